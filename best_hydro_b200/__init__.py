@@ -1,0 +1,184 @@
+"""best_hydro_b200: BEST's dense boundary-element hot path on one B200.
+
+The product is the shared library ``lib/libbestgpu.so`` (CUDA kernels for sm_100a behind the C ABI
+of ``include/best_hmatrix.h`` and ``include/best_gpu.h``).  This module is a thin ctypes mirror of
+that interface for Python callers (tests, benchmarks): it loads the in-tree library and raises if it
+is missing; there is no Python or CPU implementation of any stage behind it.
+
+    from best_hydro_b200 import BhmSolver
+    s = BhmSolver()
+    s.create(v1, v2, v3, area, afac, cg)     # bhm_create
+    x = s.incenters()                         # bhm_incenters
+    dm = s.diag_mean()                        # bhm_diag_mean
+    s.build(eps, direct, ndef, gdef, comp, xmu)   # bhm_build
+    b = s.solve(b)                            # bhm_solve
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "lib", "libbestgpu.so")
+
+BGPU_FP64 = 0
+BGPU_MIXED = 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+# name -> (restype, argtypes), as declared in include/best_hmatrix.h and include/best_gpu.h
+_SIGS = {
+    "bhm_available": (ctypes.c_int, []),
+    "bhm_create": (ctypes.c_int, [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    "bhm_incenters": (None, [_dp]),
+    "bhm_entries": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]),
+    "bhm_diag_mean": (ctypes.c_double, []),
+    "bhm_build": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _ip, _dp,
+                                 ctypes.c_int, ctypes.c_int]),
+    "bhm_solve": (ctypes.c_int, [ctypes.c_int, _dp]),
+    "bhm_log_line": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
+    "bhm_destroy": (None, []),
+    "bgpu_set_precision": (ctypes.c_int, [ctypes.c_int]),
+    "bgpu_precision": (ctypes.c_int, []),
+    "bgpu_timings": (ctypes.c_int, [_dp, ctypes.c_int]),
+    "bgpu_stream": (ctypes.c_void_p, []),
+    "bgpu_solve_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
+    "bgpu_dgetrf_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, _ip]),
+    "bgpu_dgetrs_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_int]),
+    "bgpu_dgemm_minus_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
+    "bgpu_assemble_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_int]),
+}
+
+
+class BestGpuError(RuntimeError):
+    pass
+
+
+def lib():
+    """The loaded libbestgpu (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise BestGpuError(f"libbestgpu is not built ({LIBPATH}); run python -m best_hydro_b200.build")
+        L = ctypes.CDLL(LIBPATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def log_lines():
+    """Drains the library's message queue (bhm_log_line)."""
+    L = lib()
+    out = []
+    buf = ctypes.create_string_buffer(1024)
+    while True:
+        k = L.bhm_log_line(buf, 1024)
+        if k < 0:
+            return out
+        out.append(buf.raw[:k].decode(errors="replace"))
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise BestGpuError(f"{what} failed: " + " | ".join(log_lines()))
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def timings():
+    """Stage times (ms) of the last calls: dict of bgpu_timings."""
+    v = np.zeros(7)
+    lib().bgpu_timings(_p(v), 7)
+    keys = ("create", "assemble", "factor", "solve", "build", "refine_iters", "relres")
+    return dict(zip(keys, v.tolist()))
+
+
+class BhmSolver:
+    """The nine-function seam of BEST (include/best_hmatrix.h), one solver per process."""
+
+    def __init__(self):
+        self.L = lib()
+        self.n = 0
+
+    @staticmethod
+    def available():
+        return bool(lib().bhm_available())
+
+    def create(self, v1, v2, v3, area, afac, cg=1.0):
+        """v1, v2, v3: BEST's n x 3 column-major arrays flattened (v[c*n+i]); area corrected."""
+        self._keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (v1, v2, v3, area)]
+        n = self._keep[3].size
+        _check(self.L.bhm_create(n, *(_p(a) for a in self._keep), float(afac), float(cg), 0), "bhm_create")
+        self.n = n
+
+    def incenters(self):
+        x = np.empty(3 * self.n)
+        self.L.bhm_incenters(_p(x))
+        return x
+
+    def entries(self, i0, m, j0, nc):
+        a = np.zeros((m, nc), dtype=np.float64, order="F")
+        self.L.bhm_entries(i0, m, j0, nc, a.ctypes.data_as(_dp), m)
+        return a
+
+    def diag_mean(self):
+        return float(self.L.bhm_diag_mean())
+
+    def build(self, eps=1e-4, direct=1, ndef=1, gdef=None, comp=None, xmu=None, single=0, nrhs=6):
+        gdef = np.ascontiguousarray(gdef, dtype=np.float64)
+        comp = np.ascontiguousarray(comp if comp is not None else np.ones(self.n), dtype=np.int32)
+        xmu = np.ascontiguousarray(xmu, dtype=np.float64)
+        _check(self.L.bhm_build(float(eps), int(direct), 0.1, int(ndef), _p(gdef), comp.ctypes.data_as(_ip), _p(xmu),
+                                int(single), int(nrhs)), "bhm_build")
+
+    def solve(self, b):
+        b = np.array(b, dtype=np.float64, order="F", copy=True)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        _check(self.L.bhm_solve(nrhs, _p(b)), "bhm_solve")
+        return b
+
+    def solve_device(self, d_b, nrhs, ldb):
+        _check(self.L.bgpu_solve_device(int(nrhs), ctypes.c_void_p(d_b), int(ldb)), "bgpu_solve_device")
+
+    def destroy(self):
+        self.L.bhm_destroy()
+        self.n = 0
+
+
+def set_precision(mode):
+    _check(lib().bgpu_set_precision(int(mode)), "bgpu_set_precision")
+
+
+def dgetrf_device(n, d_a, lda, d_ipiv):
+    """dgetrf on device pointers; returns info."""
+    info = ctypes.c_int(0)
+    _check(lib().bgpu_dgetrf_device(int(n), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_ipiv),
+                                    ctypes.byref(info)), "bgpu_dgetrf_device")
+    return info.value
+
+
+def dgetrs_device(n, nrhs, d_a, lda, d_ipiv, d_b, ldb):
+    _check(lib().bgpu_dgetrs_device(int(n), int(nrhs), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_ipiv),
+                                    ctypes.c_void_p(d_b), int(ldb)), "bgpu_dgetrs_device")
+
+
+def dgemm_minus_device(m, n, k, d_a, lda, d_b, ldb, d_c, ldc):
+    _check(lib().bgpu_dgemm_minus_device(int(m), int(n), int(k), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_b),
+                                         int(ldb), ctypes.c_void_p(d_c), int(ldc)), "bgpu_dgemm_minus_device")
+
+
+def assemble_device(r0, r1, c0, c1, d_out, ldo):
+    _check(lib().bgpu_assemble_device(int(r0), int(r1), int(c0), int(c1), ctypes.c_void_p(d_out), int(ldo)),
+           "bgpu_assemble_device")

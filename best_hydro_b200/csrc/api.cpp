@@ -1,0 +1,561 @@
+// libbestgpu: BEST's solver seam (include/best_hmatrix.h) and its extensions (include/best_gpu.h)
+// on one B200.
+//
+// Conventions kept from the reference's C interface (hmatrix/src/api.cpp): one solver per process
+// in a global (api.cpp:127), messages queued and pulled one at a time (api.cpp:57-67, :881-890),
+// every entry point guarded so that no exception crosses into Fortran and a failure is a nonzero
+// status after a message (api.cpp:341-351), non-finite solutions reported as errors
+// (api.cpp:681-689).  There is no CPU path: without a usable GPU, bhm_available() is 0 and every
+// other call fails with a message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <exception>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/best_gpu.h"
+#include "../../include/best_hmatrix.h"
+#include "bgpu_internal.h"
+#include "mixed.h"
+
+namespace bgpu {
+namespace {
+
+std::deque<std::string> g_log;
+
+void say(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
+void say(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_log.emplace_back(buf);
+}
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    say("error: out of host memory");
+  } catch (const std::exception& e) {
+    say("error: %s", e.what());
+  }
+  return 1;
+}
+
+// Device buffer that frees itself.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // (Re)allocates when smaller than `need`; zeroes fresh memory when `zero`.
+  void ensure(size_t need, const char* what, bool zero = false) {
+    if (bytes >= need && p) return;
+    reset();
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) {
+      size_t fr = 0, tot = 0;
+      cudaGetLastError();
+      cudaMemGetInfo(&fr, &tot);
+      throw CudaError(std::string("cannot allocate ") + what + ": " + std::to_string(need / 1e9) +
+                      " GB needed, " + std::to_string(fr / 1e9) + " GB free on the GPU");
+    }
+    bytes = need;
+    if (zero) ck(cudaMemset(p, 0, need), "cudaMemset");
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+long padded_ld(int n) { return ((long)n + 31) / 32 * 32; }
+
+struct Runtime {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  DevBuf status, info;     // device status word, dgetrf info
+  DevBuf lu_scratch;       // grid-barrier words and pivot candidates
+  DevBuf trsv_scratch;     // flags, ticket and the permuted right-hand sides
+  cudaEvent_t ev[8] = {};
+  double ms[8] = {};
+  Runtime() {
+    int count = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      throw CudaError("no CUDA device is usable");
+    }
+    ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+    status.ensure(256, "status words", true);
+    info.ensure(256, "info", true);
+    lu_scratch.ensure(lu_scratch_bytes(0), "LU scratch", true);
+  }
+  ~Runtime() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void sync(const char* what) { ck(cudaStreamSynchronize(stream), what); }
+  // Reads and clears the device status word; throws on a recorded failure.
+  void check_status(const char* what) {
+    int st = 0;
+    ck(cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, stream), "status read");
+    sync(what);
+    if (st != kOk) {
+      ck(cudaMemsetAsync(status.p, 0, sizeof(int), stream), "status clear");
+      sync(what);
+      if (st == kWaitTimeout)
+        throw CudaError(std::string(what) + ": a device-side wait ran out (kernel gave up, no result)");
+      if (st == kNotFinite) throw CudaError(std::string(what) + ": the solution is not finite (NaN or Inf)");
+      throw CudaError(std::string(what) + ": device status " + std::to_string(st));
+    }
+  }
+  void ensure_trsv(int n) { trsv_scratch.ensure(trsv_scratch_bytes(n), "solve scratch", true); }
+  float elapsed(int a, int b) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, ev[a], ev[b]);
+    return t;
+  }
+};
+
+std::unique_ptr<Runtime> g_rt;
+
+Runtime& rt() {
+  if (!g_rt) g_rt = std::make_unique<Runtime>();
+  return *g_rt;
+}
+
+struct Solver {
+  int n = 0;
+  double afac = 1.0, cg = 1.0;
+  std::vector<double> x_host;  // incenters, n x 3 column-major
+  DevBuf geo, xc, self9, diag;
+  DevBuf gr;                   // GR / its LU factors (FP64), n x ld
+  long ld = 0;
+  DevBuf ipiv, perm;
+  DevBuf gdef, comp, xmu;
+  DevBuf rhs;                  // right-hand sides, n3 x 16
+  std::unique_ptr<MixedSolver> mixed;
+  int precision = BGPU_FP64;
+  bool factored = false;
+  DevMesh mesh() const {
+    DevMesh m;
+    m.n = n;
+    m.cg = cg;
+    m.afac = afac;
+    m.geo = geo.as<double>();
+    m.xc = xc.as<double>();
+    m.self9 = self9.as<double>();
+    return m;
+  }
+};
+
+std::unique_ptr<Solver> g;
+int g_prec_override = -1;
+double g_solve_info[2] = {0, 0};  // refinement iterations, relative residual of the last solve
+
+Solver& solver() {
+  if (!g) throw std::runtime_error("bhm_create has not been called");
+  return *g;
+}
+
+int precision_for(int direct, int single) {
+  if (g_prec_override >= 0) return g_prec_override;
+  if (const char* e = std::getenv("BEST_GPU_PRECISION")) {
+    if (!std::strcmp(e, "fp64")) return BGPU_FP64;
+    if (!std::strcmp(e, "mixed")) return BGPU_MIXED;
+  }
+  if (direct && !single) return BGPU_FP64;
+  return BGPU_MIXED;
+}
+
+// Factors the FP64 matrix in s.gr (dgetrf); throws on a zero pivot.
+void factor64(Solver& s, Runtime& r) {
+  const int n3 = 3 * s.n;
+  s.ipiv.ensure(sizeof(int) * n3, "pivots");
+  s.perm.ensure(sizeof(int) * n3, "permutation");
+  LuScratch ws{r.lu_scratch.p, r.lu_scratch.bytes};
+  ck(lu64_getrf(s.gr.as<double>(), s.ld, n3, s.ipiv.as<int>(), r.info.as<int>(), r.status.as<int>(), ws, r.stream),
+     "LU");
+  ck(lu_perm_from_ipiv(s.ipiv.as<int>(), n3, s.perm.as<int>(), r.stream), "permutation");
+}
+
+void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
+  if (!s.factored) throw std::runtime_error("bhm_build has not factored GR");
+  const int n3 = 3 * s.n;
+  ck(cudaEventRecord(r.ev[6], r.stream), "event");
+  if (s.precision == BGPU_MIXED && s.mixed) {
+    MixedReport rep{};
+    s.mixed->solve(nrhs, d_b, ldb, r.stream, &rep);
+    g_solve_info[0] = rep.iterations;
+    g_solve_info[1] = rep.relres;
+  } else {
+    r.ensure_trsv(n3);
+    for (int c = 0; c < nrhs; c += 16) {
+      const int q = std::min(16, nrhs - c);
+      ck(getrs64(s.gr.as<double>(), s.ld, n3, s.perm.as<int>(), d_b + (size_t)c * ldb, ldb, q, r.trsv_scratch.p,
+                 r.status.as<int>(), r.stream),
+         "solve");
+    }
+    g_solve_info[0] = 0;
+    g_solve_info[1] = 0;
+  }
+  ck(check_finite(d_b, ldb, n3, nrhs, r.status.as<int>(), r.stream), "finite check");
+  ck(cudaEventRecord(r.ev[7], r.stream), "event");
+  r.check_status("solve");
+  r.ms[3] = r.elapsed(6, 7);
+}
+
+}  // namespace
+}  // namespace bgpu
+
+using namespace bgpu;
+
+extern "C" {
+
+int bhm_available(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return count > 0 ? 1 : 0;
+}
+
+int bhm_create(int n, const double* v1, const double* v2, const double* v3, const double* area, double afac,
+               double cg, int /*threads*/) {
+  return guarded([&] {
+    if (n < 1) {
+      say("error: the GPU solver needs at least 1 triangle");
+      return 1;
+    }
+    Runtime& r = rt();
+    auto s = std::make_unique<Solver>();
+    s->n = n;
+    s->afac = afac;
+    s->cg = cg;
+    std::vector<double> h((size_t)n * kGeoStride, 0.0);
+    for (int t = 0; t < n; ++t)
+      for (int c = 0; c < 3; ++c) {
+        h[(size_t)t * kGeoStride + c] = v1[(size_t)c * n + t];
+        h[(size_t)t * kGeoStride + 3 + c] = v2[(size_t)c * n + t];
+        h[(size_t)t * kGeoStride + 6 + c] = v3[(size_t)c * n + t];
+      }
+    for (int t = 0; t < n; ++t) h[(size_t)t * kGeoStride + 9] = area[t];
+    s->geo.ensure(h.size() * sizeof(double), "mesh");
+    s->xc.ensure((size_t)n * kXcStride * sizeof(double), "incenters");
+    s->self9.ensure((size_t)n * 9 * sizeof(double), "self blocks");
+    s->diag.ensure(256, "diagonal mean");
+    ck(cudaEventRecord(r.ev[0], r.stream), "event");
+    ck(cudaMemcpyAsync(s->geo.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, r.stream), "mesh copy");
+    ck(launch_self_blocks(s->mesh(), r.stream), "self blocks");
+    std::vector<double> xc((size_t)n * kXcStride);
+    ck(cudaMemcpyAsync(xc.data(), s->xc.p, xc.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream),
+       "incenter copy");
+    ck(cudaEventRecord(r.ev[1], r.stream), "event");
+    r.sync("bhm_create");
+    r.ms[0] = r.elapsed(0, 1);
+    s->x_host.resize((size_t)3 * n);
+    for (int t = 0; t < n; ++t)
+      for (int c = 0; c < 3; ++c) s->x_host[(size_t)c * n + t] = xc[(size_t)t * kXcStride + c];
+    g = std::move(s);
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, r.device);
+    say("GPU solver: %d triangles on %s (%d SMs, %.0f GB), dense GR %.2f GB in FP64", n, prop.name,
+        prop.multiProcessorCount, prop.totalGlobalMem / 1e9, 72.0 * n * (double)n / 1e9);
+    return 0;
+  });
+}
+
+void bhm_incenters(double* x) {
+  guarded([&] {
+    Solver& s = solver();
+    std::memcpy(x, s.x_host.data(), s.x_host.size() * sizeof(double));
+    return 0;
+  });
+}
+
+void bhm_entries(int i0, int m, int j0, int nc, double* a, int lda) {
+  guarded([&] {
+    if (m <= 0 || nc <= 0) return 0;
+    Solver& s = solver();
+    Runtime& r = rt();
+    if (i0 < 0 || j0 < 0 || (long)i0 + m > 3L * s.n || (long)j0 + nc > 3L * s.n || lda < m) {
+      say("error: bhm_entries: rows %d..%d or columns %d..%d outside GR (order %d), or lda %d < m", i0, i0 + m - 1, j0,
+          j0 + nc - 1, 3 * s.n, lda);
+      return 1;
+    }
+    const int t0 = i0 / 3, t1 = (i0 + m - 1) / 3 + 1;
+    const long rows = 3L * (t1 - t0);
+    // columns in chunks so the staging buffer stays below ~1 GB
+    const int cmax = std::max(1, (int)std::min<long>((long)s.n, (1L << 27) / std::max(1L, rows) / 3));
+    const int s0 = j0 / 3, s1 = (j0 + nc - 1) / 3 + 1;
+    DevBuf tmp;
+    tmp.ensure((size_t)rows * 3 * std::min(cmax, s1 - s0) * sizeof(double), "entry staging");
+    for (int c = s0; c < s1; c += cmax) {
+      const int ce = std::min(s1, c + cmax);
+      DevDeflation none;
+      ck(launch_assemble(s.mesh(), t0, t1, c, ce, tmp.as<double>(), rows, none, nullptr, 0, r.stream), "entries");
+      // copy the part of columns [3c, 3ce) x rows [3 t0, 3 t1) that the caller asked for
+      const int jlo = std::max(j0, 3 * c), jhi = std::min(j0 + nc, 3 * ce);
+      const double* src = tmp.as<double>() + (size_t)(jlo - 3 * c) * rows + (i0 - 3 * t0);
+      double* dst = a + (size_t)(jlo - j0) * lda;
+      ck(cudaMemcpy2DAsync(dst, (size_t)lda * sizeof(double), src, (size_t)rows * sizeof(double),
+                           (size_t)m * sizeof(double), (size_t)(jhi - jlo), cudaMemcpyDeviceToHost, r.stream),
+         "entries copy");
+      r.sync("bhm_entries");
+    }
+    return 0;
+  });
+}
+
+double bhm_diag_mean(void) {
+  double v = 0.0;
+  guarded([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    ck(launch_diag_mean(s.mesh(), s.diag.as<double>(), r.stream), "diagonal mean");
+    ck(cudaMemcpyAsync(&v, s.diag.p, sizeof(double), cudaMemcpyDeviceToHost, r.stream), "diagonal copy");
+    r.sync("bhm_diag_mean");
+    return 0;
+  });
+  return v;
+}
+
+int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double* gdef, const int* comp,
+              const double* xmu, int single, int /*nrhs*/) {
+  return guarded([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    const int n = s.n, n3 = 3 * n;
+    s.factored = false;
+    s.precision = precision_for(direct, single);
+    DevDeflation defl;
+    if (ndef >= 1) {
+      s.gdef.ensure(sizeof(double) * ndef, "deflation weights");
+      s.xmu.ensure(sizeof(double) * n3, "deflation vectors");
+      ck(cudaMemcpyAsync(s.gdef.p, gdef, sizeof(double) * ndef, cudaMemcpyHostToDevice, r.stream), "gdef copy");
+      ck(cudaMemcpyAsync(s.xmu.p, xmu, sizeof(double) * n3, cudaMemcpyHostToDevice, r.stream), "xmu copy");
+      defl.ndef = ndef;
+      defl.gdef = s.gdef.as<double>();
+      defl.xmu = s.xmu.as<double>();
+      if (ndef > 1) {
+        s.comp.ensure(sizeof(int) * n, "surface labels");
+        ck(cudaMemcpyAsync(s.comp.p, comp, sizeof(int) * n, cudaMemcpyHostToDevice, r.stream), "comp copy");
+        defl.comp = s.comp.as<int>();
+      }
+    }
+    s.ld = padded_ld(n3);
+    s.gr.ensure((size_t)s.ld * n3 * sizeof(double), "GR (FP64)");
+    ck(cudaEventRecord(r.ev[2], r.stream), "event");
+    if (s.precision == BGPU_MIXED) {
+      if (!s.mixed) s.mixed = std::make_unique<MixedSolver>();
+      s.mixed->build(s.mesh(), defl, s.gr.as<double>(), s.ld, eps, r.stream, r.ev[3], r.ev[4]);
+      ck(cudaEventRecord(r.ev[5], r.stream), "event");
+      r.check_status("bhm_build");
+    } else {
+      ck(launch_assemble(s.mesh(), 0, n, 0, n, s.gr.as<double>(), s.ld, defl, nullptr, 0, r.stream), "assembly");
+      ck(cudaEventRecord(r.ev[3], r.stream), "event");
+      factor64(s, r);
+      ck(cudaEventRecord(r.ev[5], r.stream), "event");
+      ck(cudaEventRecord(r.ev[4], r.stream), "event");
+      r.check_status("bhm_build");
+      ck(cudaEventRecord(r.ev[4], r.stream), "event");
+    }
+    r.sync("bhm_build");
+    int info = 0;
+    ck(cudaMemcpy(&info, r.info.p, sizeof(int), cudaMemcpyDeviceToHost), "info read");
+    r.ms[1] = r.elapsed(2, 3);
+    r.ms[2] = r.elapsed(3, 5);
+    r.ms[4] = r.elapsed(2, 5);
+    if (info > 0) {
+      say("error: the LU factorisation found U(%d,%d) = 0: GR is singular", info, info);
+      return 1;
+    }
+    s.factored = true;
+    say("GPU build: %s LU of order %d, assembly %.1f ms, factorisation %.1f ms (%.1f TFLOP/s)",
+        s.precision == BGPU_FP64 ? "FP64" : (s.mixed ? s.mixed->name() : "mixed"), n3, r.ms[1], r.ms[2],
+        (2.0 / 3.0) * (double)n3 * n3 * n3 / (r.ms[2] * 1e-3) / 1e12);
+    return 0;
+  });
+}
+
+int bhm_solve(int nrhs, double* b) {
+  return guarded([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    if (nrhs <= 0) return 0;
+    const int n3 = 3 * s.n;
+    s.rhs.ensure((size_t)n3 * nrhs * sizeof(double), "right-hand sides");
+    ck(cudaMemcpyAsync(s.rhs.p, b, (size_t)n3 * nrhs * sizeof(double), cudaMemcpyHostToDevice, r.stream), "b copy");
+    solve_device(s, r, nrhs, s.rhs.as<double>(), n3);
+    ck(cudaMemcpyAsync(b, s.rhs.p, (size_t)n3 * nrhs * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "x copy");
+    r.sync("bhm_solve");
+    if (s.precision == BGPU_MIXED && s.mixed)
+      say("solve: %d right-hand sides, %d refinement steps, relative residual %.1e, %.2f ms", nrhs,
+          (int)g_solve_info[0], g_solve_info[1], r.ms[3]);
+    else
+      say("solve: %d right-hand sides with the FP64 LU factors, %.2f ms", nrhs, r.ms[3]);
+    return 0;
+  });
+}
+
+int bhm_log_line(char* buf, int len) {
+  if (g_log.empty()) return -1;
+  const std::string& s = g_log.front();
+  const int k = std::min(len, (int)s.size());
+  std::memcpy(buf, s.data(), (size_t)k);
+  g_log.pop_front();
+  return k;
+}
+
+void bhm_destroy(void) {
+  g.reset();
+  g_rt.reset();
+}
+
+// ---------------------------------------------------------------------------------------------
+// best_gpu.h
+// ---------------------------------------------------------------------------------------------
+
+int bgpu_set_precision(int mode) {
+  if (mode != -1 && mode != BGPU_FP64 && mode != BGPU_MIXED) {
+    say("error: unknown precision %d", mode);
+    return 1;
+  }
+  g_prec_override = mode;
+  return 0;
+}
+
+int bgpu_precision(void) { return g ? g->precision : -1; }
+
+int bgpu_timings(double* ms, int len) {
+  if (!g_rt) return 0;
+  double v[7] = {g_rt->ms[0], g_rt->ms[1], g_rt->ms[2], g_rt->ms[3], g_rt->ms[4], g_solve_info[0], g_solve_info[1]};
+  const int k = std::min(len, 7);
+  for (int i = 0; i < k; ++i) ms[i] = v[i];
+  return k;
+}
+
+void* bgpu_stream(void) {
+  void* p = nullptr;
+  guarded([&] {
+    p = (void*)rt().stream;
+    return 0;
+  });
+  return p;
+}
+
+int bgpu_solve_device(int nrhs, double* d_b, int ldb) {
+  return guarded([&] {
+    solve_device(solver(), rt(), nrhs, d_b, ldb);
+    return 0;
+  });
+}
+
+int bgpu_dgetrf_device(int n, double* d_a, int lda, int* d_ipiv, int* info) {
+  return guarded([&] {
+    Runtime& r = rt();
+    if (n < 0 || lda < std::max(1, n) || (lda & 1) || ((uintptr_t)d_a & 15)) {
+      say("error: bgpu_dgetrf_device needs lda >= n, lda even and a 16-byte aligned matrix");
+      return 1;
+    }
+    LuScratch ws{r.lu_scratch.p, r.lu_scratch.bytes};
+    ck(cudaEventRecord(r.ev[3], r.stream), "event");
+    ck(lu64_getrf(d_a, lda, n, d_ipiv, r.info.as<int>(), r.status.as<int>(), ws, r.stream), "LU");
+    ck(cudaEventRecord(r.ev[5], r.stream), "event");
+    r.check_status("dgetrf");
+    ck(cudaMemcpy(info, r.info.p, sizeof(int), cudaMemcpyDeviceToHost), "info read");
+    r.ms[2] = r.elapsed(3, 5);
+    return 0;
+  });
+}
+
+int bgpu_dgetrs_device(int n, int nrhs, const double* d_a, int lda, const int* d_ipiv, double* d_b, int ldb) {
+  return guarded([&] {
+    Runtime& r = rt();
+    if (n <= 0 || nrhs <= 0) return 0;
+    if (nrhs > 16) {
+      say("error: bgpu_dgetrs_device takes at most 16 right-hand sides per call");
+      return 1;
+    }
+    DevBuf perm;
+    perm.ensure(sizeof(int) * n, "permutation");
+    r.ensure_trsv(n);
+    ck(cudaEventRecord(r.ev[6], r.stream), "event");
+    ck(lu_perm_from_ipiv(d_ipiv, n, perm.as<int>(), r.stream), "permutation");
+    ck(getrs64(d_a, lda, n, perm.as<int>(), d_b, ldb, nrhs, r.trsv_scratch.p, r.status.as<int>(), r.stream),
+       "solve");
+    ck(cudaEventRecord(r.ev[7], r.stream), "event");
+    r.check_status("dgetrs");
+    r.ms[3] = r.elapsed(6, 7);
+    return 0;
+  });
+}
+
+int bgpu_dgemm_minus_device(int m, int n, int k, const double* d_a, int lda, const double* d_b, int ldb, double* d_c,
+                            int ldc) {
+  return guarded([&] {
+    Runtime& r = rt();
+    if ((lda & 1) || (ldb & 1) || ((uintptr_t)d_a & 15) || ((uintptr_t)d_b & 15)) {
+      say("error: bgpu_dgemm_minus_device needs even leading dimensions and 16-byte aligned A and B");
+      return 1;
+    }
+    ck(cudaEventRecord(r.ev[6], r.stream), "event");
+    ck(dgemm_nn_minus(m, n, k, d_a, lda, d_b, ldb, d_c, ldc, r.stream), "dgemm");
+    ck(cudaEventRecord(r.ev[7], r.stream), "event");
+    r.sync("dgemm");
+    r.ms[3] = r.elapsed(6, 7);
+    return 0;
+  });
+}
+
+int bgpu_assemble_device(int r0, int r1, int c0, int c1, double* d_out, int ldo) {
+  return guarded([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    if (r0 < 0 || c0 < 0 || r1 > s.n || c1 > s.n || ldo < 3 * (r1 - r0)) {
+      say("error: bgpu_assemble_device: range outside the mesh or ldo too small");
+      return 1;
+    }
+    DevDeflation none;
+    ck(cudaEventRecord(r.ev[2], r.stream), "event");
+    ck(launch_assemble(s.mesh(), r0, r1, c0, c1, d_out, ldo, none, nullptr, 0, r.stream), "assembly");
+    ck(cudaEventRecord(r.ev[3], r.stream), "event");
+    r.sync("assembly");
+    r.ms[1] = r.elapsed(2, 3);
+    return 0;
+  });
+}
+
+}  // extern "C"

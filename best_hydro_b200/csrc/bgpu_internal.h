@@ -1,0 +1,81 @@
+// Internal declarations shared by the CUDA translation units and the C-ABI layer of libbestgpu.
+// Nothing here is part of the public interface (include/best_hmatrix.h, include/best_gpu.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+namespace bgpu {
+
+// Device status codes written by kernels into a status word (0 = ok).  Kernels never trap: a
+// bounded wait that runs out, or an index check that fails, records a code here and returns.
+enum DevStatus : int {
+  kOk = 0,
+  kWaitTimeout = 1,   // a grid barrier or a dependency flag was not reached in time
+  kBadIndex = 2,      // an index check failed (the access was skipped)
+  kNotFinite = 3,     // a result is NaN or Inf
+};
+
+// Per-triangle source geometry on the device: p1, p2, p3 (9 doubles), corrected area, 2 pad.
+constexpr int kGeoStride = 12;
+// Incenter: x, y, z, pad.
+constexpr int kXcStride = 4;
+
+struct DevMesh {
+  int n = 0;
+  double cg = 1.0;
+  double afac = 1.0;
+  const double* geo = nullptr;  // n * kGeoStride
+  double* xc = nullptr;         // n * kXcStride (written by the self-block kernel)
+  double* self9 = nullptr;      // n * 9, self block of triangle t: self9[9t + 3a + b]
+};
+
+// The normal-field deflation applied in the assembly epilogue (best/best.f:406-425):
+// GR(I,J) += (gdef[comp[J/3]-1] * xmu[J]) * xmu[I] when comp[I/3] == comp[J/3].
+struct DevDeflation {
+  int ndef = 0;  // 0: none
+  const double* gdef = nullptr;
+  const int* comp = nullptr;  // 1-based surface of each triangle (nullptr when ndef == 1)
+  const double* xmu = nullptr;
+};
+
+// assemble.cu -------------------------------------------------------------------------------
+cudaError_t launch_self_blocks(const DevMesh& m, cudaStream_t s);
+// GR rows of targets [r0,r1) x columns of sources [c0,c1) into out (column-major, ld), entry
+// (3(n1-r0)+a, 3(n2-c0)+b).  With defl.ndef > 0 the deflation term is added; with out32 != nullptr
+// a single-precision copy (rounded to nearest) is written too (leading dimension ld32).
+cudaError_t launch_assemble(const DevMesh& m, int r0, int r1, int c0, int c1, double* out, long ld,
+                            const DevDeflation& defl, float* out32, long ld32, cudaStream_t s);
+// BEST's mean of GR's diagonal (best/best.f:401-403), summed in BEST's order, into *d_out.
+cudaError_t launch_diag_mean(const DevMesh& m, double* d_out, cudaStream_t s);
+
+// lu.cu -------------------------------------------------------------------------------------
+// Scratch for the factorisation kernels (grid barrier words, pivot candidates, status).
+struct LuScratch {
+  void* base = nullptr;
+  size_t bytes = 0;
+};
+size_t lu_scratch_bytes(int n);
+// dgetrf semantics: A (n x n, column-major, lda) overwritten by L and U, ipiv 1-based row
+// interchanges, *d_info = 0 or the first exactly-zero pivot (1-based).  d_status receives a
+// DevStatus.  Host-side errors return a cudaError_t.
+cudaError_t lu64_getrf(double* A, long lda, int n, int* ipiv, int* d_info, int* d_status, const LuScratch& ws,
+                       cudaStream_t s);
+// C(m x n) -= A(m x k) B(k x n), all column-major (FP64 tensor-core path).
+cudaError_t dgemm_nn_minus(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C,
+                           long ldc, cudaStream_t s);
+
+// solve.cu ----------------------------------------------------------------------------------
+// The row permutation of a factorisation: perm[i] = original row of row i of P A (0-based).
+cudaError_t lu_perm_from_ipiv(const int* ipiv, int n, int* perm, cudaStream_t s);
+size_t trsv_scratch_bytes(int n);
+// X (n x nrhs, ldx) := A^{-1} X given the LU factors and perm, dgetrs('N') semantics.
+cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* X, long ldx, int nrhs, void* scratch,
+                    int* d_status, cudaStream_t s);
+// Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.
+cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s);
+
+}  // namespace bgpu

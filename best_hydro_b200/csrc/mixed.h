@@ -1,0 +1,34 @@
+// Mixed-precision factorisation and refined solve (internal interface of libbestgpu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bgpu_internal.h"
+
+namespace bgpu {
+
+struct MixedReport {
+  int iterations = 0;   // refinement steps of the last solve
+  double relres = 0.0;  // largest relative residual ||b - A x|| / ||b|| over the right-hand sides
+};
+
+class MixedSolver {
+ public:
+  MixedSolver();
+  ~MixedSolver();
+  MixedSolver(const MixedSolver&) = delete;
+  MixedSolver& operator=(const MixedSolver&) = delete;
+  const char* name() const;
+  // Assembles GR + deflation into gr64 (FP64, kept for the residuals) and a reduced-precision copy,
+  // records ev_assembled, factors the copy.  Throws on failure.
+  void build(const DevMesh& m, const DevDeflation& d, double* gr64, long ld, double eps, cudaStream_t s,
+             cudaEvent_t ev_assembled, cudaEvent_t ev_factored);
+  // Solves GR x = b in place (d_b: 3n x nrhs, ldb) to the relative residual of build's eps.
+  void solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedReport* rep);
+
+ private:
+  struct Impl;
+  Impl* p_;
+};
+
+}  // namespace bgpu

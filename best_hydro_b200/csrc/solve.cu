@@ -1,0 +1,322 @@
+// Solves with the LU factors for BEST's 6 (or 11) right-hand sides (dgetrs('N') semantics).
+//
+// What it replaces: dgetrs('N', n, nrhs, GR, n, ipiv, b, n, info), best/besolve.f90:132-133, and
+// the H-matrix solver's bhm_solve behind the same seam (hmatrix/best_hmatrix.h:64-66).
+//
+// The solve reads the n x n factor once (HBM-bound).  Each triangle is one persistent kernel:
+// CTAs take 64-row blocks in order from a ticket counter, stream their row of 64x64 blocks of the
+// factor against the already-solved blocks of the unknowns, and publish each finished block through
+// a readiness flag (release/acquire, with a bounded wait).  A block taken from the ticket counter
+// only ever waits on blocks taken before it by CTAs that are already running, so the scheme cannot
+// deadlock however many CTAs are resident.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "bgpu_internal.h"
+
+namespace bgpu {
+namespace {
+
+constexpr int kBs = 64;           // rows per block
+constexpr int kMaxRhs = 16;       // right-hand sides per call (kernels for 8 and 16)
+constexpr int kThreads = 256;     // 4 quarter-rows of the inner dimension x 64 rows
+constexpr unsigned kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void k_perm_init(int* perm, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) perm[i] = i;
+}
+
+// Composes the interchanges of ipiv (1-based, LAPACK order) into perm, chunk by chunk in shared
+// memory: a chunk of C interchanges touches its own C rows and at most C rows below it.
+constexpr int kPermChunk = 512;
+__global__ void __launch_bounds__(1024) k_perm_compose(const int* __restrict__ ipiv, int n, int* __restrict__ perm) {
+  __shared__ int s_ins[kPermChunk];   // perm values of the chunk's own rows
+  __shared__ int s_tgt[kPermChunk];   // target row of each interchange
+  __shared__ int s_slot[kPermChunk];  // outside target: slot of its first occurrence, else -1
+  __shared__ int s_out[kPermChunk];   // perm values of outside targets (by slot)
+  const int tid = threadIdx.x;
+  for (int j0 = 0; j0 < n; j0 += kPermChunk) {
+    const int C = min(kPermChunk, n - j0);
+    const int j1 = j0 + C;
+    if (tid < C) {
+      s_ins[tid] = perm[j0 + tid];
+      s_tgt[tid] = ipiv[j0 + tid] - 1;
+    }
+    __syncthreads();
+    if (tid < C) {
+      const int p = s_tgt[tid];
+      int slot = -1;
+      if (p >= j1) {
+        slot = tid;
+        for (int q = 0; q < tid; ++q)
+          if (s_tgt[q] == p) {
+            slot = q;
+            break;
+          }
+        if (slot == tid) s_out[tid] = perm[p];
+      }
+      s_slot[tid] = slot;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int t = 0; t < C; ++t) {
+        const int p = s_tgt[t];
+        if (p == j0 + t) continue;
+        int* a = &s_ins[t];
+        int* b = (p < j1) ? &s_ins[p - j0] : &s_out[s_slot[t]];
+        const int v = *a;
+        *a = *b;
+        *b = v;
+      }
+    }
+    __syncthreads();
+    if (tid < C) {
+      perm[j0 + tid] = s_ins[tid];
+      if (s_slot[tid] == tid) perm[s_tgt[tid]] = s_out[tid];
+    }
+    __syncthreads();
+  }
+}
+
+// Y(i, r) = X(perm[i], r)
+template <typename T>
+__global__ void k_gather_rows(const T* __restrict__ X, long ldx, const int* __restrict__ perm, int n, int nrhs,
+                              T* __restrict__ Y, long ldy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm[i];
+  for (int r = 0; r < nrhs; ++r) Y[(size_t)r * ldy + i] = X[(size_t)r * ldx + p];
+}
+
+template <typename T>
+__global__ void k_copy_cols(const T* __restrict__ Y, long ldy, int n, int nrhs, T* __restrict__ X, long ldx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int r = 0; r < nrhs; ++r) X[(size_t)r * ldx + i] = Y[(size_t)r * ldy + i];
+}
+
+// Warp 0 waits until flags[jb] == epoch, then counts how many more flags in the direction `step`
+// (+1 or -1) are ready too, up to 32 and within [lo, hi).  Returns that count (>= 1), or 0 when the
+// wait runs out (status set).  Every thread of the block must call it.
+__device__ int wait_ready(const unsigned* flags, int jb, int step, int lo, int hi, unsigned epoch, int* status,
+                          int* s_cnt) {
+  if (threadIdx.x < 32) {
+    int cnt = 0;
+    unsigned spins = 0;
+    for (;;) {
+      const int q = jb + step * (int)threadIdx.x;
+      const bool in = q >= lo && q < hi;
+      const bool rdy = in && ld_acquire_u32(flags + q) == epoch;
+      const unsigned ball = __ballot_sync(0xffffffffu, rdy);
+      if (ball & 1u) {
+        cnt = __ffs(~ball) - 1;
+        if (cnt < 0 || ball == 0xffffffffu) cnt = 32;
+        break;
+      }
+      if (++spins > kSpinLimit) {
+        if (threadIdx.x == 0) atomicExch(status, (int)kWaitTimeout);
+        break;
+      }
+      __nanosleep(32);
+    }
+    if (threadIdx.x == 0) *s_cnt = cnt;
+  }
+  __syncthreads();
+  return *s_cnt;
+}
+
+// One triangle of the solve on Y (n x nrhs <= RHS, ldy).  LOWER: unit lower L, blocks in increasing
+// order; otherwise upper U (non-unit diagonal), blocks in decreasing order.  F is the factor's type.
+template <typename F, bool LOWER, int RHS>
+__global__ void __launch_bounds__(kThreads) k_trsv(const F* __restrict__ LU, long lda, int n, double* Y, long ldy,
+                                                   int nrhs, unsigned* flags, unsigned* ticket, unsigned epoch,
+                                                   int* status) {
+  __shared__ double s_y[kBs][RHS];  // a solved block being consumed, later the block being solved
+  // the partial sums of the four quarters, then (reusing the space) the diagonal block
+  constexpr int kAccWords = 4 * kBs * RHS, kDiagWords = kBs * (kBs + 1);
+  __shared__ double s_buf[kAccWords > kDiagWords ? kAccWords : kDiagWords];
+  __shared__ int s_blk, s_cnt;
+  double(*s_acc)[kBs][RHS] = reinterpret_cast<double(*)[kBs][RHS]>(s_buf);
+  double(*s_d)[kBs + 1] = reinterpret_cast<double(*)[kBs + 1]>(s_buf);
+  const int nblk = (n + kBs - 1) / kBs;
+  const int tid = threadIdx.x, row = tid & (kBs - 1), quarter = tid >> 6;
+
+  for (;;) {
+    if (tid == 0) s_blk = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int t = s_blk;
+    if (t >= nblk) return;
+    const int blk = LOWER ? t : nblk - 1 - t;
+    const int r0 = blk * kBs, nr = min(kBs, n - r0);
+    double acc[RHS];
+#pragma unroll
+    for (int r = 0; r < RHS; ++r) acc[r] = 0.0;
+
+    // off-diagonal blocks: jb = 0 .. blk-1 (lower) or jb = nblk-1 .. blk+1 (upper)
+    const int nq = LOWER ? blk : nblk - 1 - blk;
+    int confirmed = 0;  // blocks known ready, counted along the processing order
+    for (int q = 0; q < nq; ++q) {
+      const int jb = LOWER ? q : nblk - 1 - q;
+      if (q >= confirmed) {
+        const int c = LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, &s_cnt)
+                            : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, &s_cnt);
+        if (c == 0) return;
+        confirmed = q + c;
+      }
+      const int c0 = jb * kBs, nc = min(kBs, n - c0);
+      for (int idx = tid; idx < kBs * RHS; idx += kThreads) {
+        const int rr = idx / RHS, r = idx % RHS;
+        s_y[rr][r] = (rr < nc && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + c0 + rr]) : 0.0;
+      }
+      __syncthreads();
+      if (row < nr) {
+        const F* col = LU + (size_t)(c0 + quarter * 16) * lda + r0 + row;
+#pragma unroll 4
+        for (int kk = 0; kk < 16; ++kk) {
+          const int cc = quarter * 16 + kk;
+          if (cc < nc) {
+            const double l = (double)col[(size_t)kk * lda];
+#pragma unroll
+            for (int r = 0; r < RHS; ++r) acc[r] -= l * s_y[cc][r];
+          }
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < RHS; ++r) s_acc[quarter][row][r] = acc[r];
+    __syncthreads();
+    // s_y := b - sum of the off-diagonal products
+    for (int idx = tid; idx < kBs * RHS; idx += kThreads) {
+      const int rr = idx / RHS, r = idx % RHS;
+      double v = 0.0;
+      if (rr < nr && r < nrhs)
+        v = Y[(size_t)r * ldy + r0 + rr] + ((s_acc[0][rr][r] + s_acc[1][rr][r]) + (s_acc[2][rr][r] + s_acc[3][rr][r]));
+      s_y[rr][r] = v;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kBs * kBs; idx += kThreads) {
+      const int rr = idx % kBs, cc = idx / kBs;
+      s_d[rr][cc] = (rr < nr && cc < nr) ? (double)LU[(size_t)(r0 + cc) * lda + r0 + rr] : 0.0;
+    }
+    __syncthreads();
+    // substitution inside the diagonal block, column by column
+    if (LOWER) {
+      for (int c = 0; c < nr; ++c) {
+        for (int idx = tid; idx < kBs * RHS; idx += kThreads) {
+          const int rr = idx / RHS, r = idx % RHS;
+          if (rr > c && rr < nr && r < nrhs) s_y[rr][r] -= s_d[rr][c] * s_y[c][r];
+        }
+        __syncthreads();
+      }
+    } else {
+      for (int c = nr - 1; c >= 0; --c) {
+        if (tid < nrhs) s_y[c][tid] = s_y[c][tid] / s_d[c][c];
+        __syncthreads();
+        for (int idx = tid; idx < kBs * RHS; idx += kThreads) {
+          const int rr = idx / RHS, r = idx % RHS;
+          if (rr < c && r < nrhs) s_y[rr][r] -= s_d[rr][c] * s_y[c][r];
+        }
+        __syncthreads();
+      }
+    }
+    for (int idx = tid; idx < kBs * RHS; idx += kThreads) {
+      const int rr = idx / RHS, r = idx % RHS;
+      if (rr < nr && r < nrhs) Y[(size_t)r * ldy + r0 + rr] = s_y[rr][r];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      st_release_u32(flags + blk, epoch);
+    }
+  }
+}
+
+__global__ void k_check_finite(const double* __restrict__ X, long ldx, int n, int nrhs, int* status) {
+  const long total = (long)n * nrhs;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+    const long r = idx / n, i = idx % n;
+    if (!isfinite(X[r * ldx + i])) {
+      atomicExch(status, (int)kNotFinite);
+      return;
+    }
+  }
+}
+
+struct TrsvScratch {
+  // [ticket (256 B)] [flags nblk unsigned, rounded] [Y n x kMaxRhs doubles]
+  static size_t flags_off() { return 256; }
+  static size_t y_off(int n) { return (256 + (size_t)((n + kBs - 1) / kBs) * 4 + 255) / 256 * 256; }
+  static size_t bytes(int n) { return y_off(n) + (size_t)n * kMaxRhs * sizeof(double); }
+};
+
+unsigned g_epoch = 0;
+
+}  // namespace
+
+cudaError_t lu_perm_from_ipiv(const int* ipiv, int n, int* perm, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_perm_init<<<(n + 255) / 256, 256, 0, s>>>(perm, n);
+  k_perm_compose<<<1, 1024, 0, s>>>(ipiv, n, perm);
+  return cudaGetLastError();
+}
+
+size_t trsv_scratch_bytes(int n) { return TrsvScratch::bytes(n); }
+
+// Solves in place with FP64 factors.  The scratch must hold trsv_scratch_bytes(n) bytes and be
+// zeroed once when first allocated (the flags carry an epoch; no per-call clearing is needed).
+cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* X, long ldx, int nrhs, void* scratch,
+                    int* d_status, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return cudaSuccess;
+  if (nrhs > kMaxRhs) return cudaErrorInvalidValue;
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  unsigned* ticket = reinterpret_cast<unsigned*>(base);
+  unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
+  double* Y = reinterpret_cast<double*>(base + TrsvScratch::y_off(n));
+  const long ldy = n;
+  k_gather_rows<double><<<(n + 255) / 256, 256, 0, s>>>(X, ldx, perm, n, nrhs, Y, ldy);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int nblk = (n + kBs - 1) / kBs;
+  const int grid = std::min(nblk, sms * 2);
+  // epochs: never 0 (the flags' initial value)
+  g_epoch += 2;
+  if (g_epoch == 0) g_epoch = 2;
+  cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  if (nrhs <= 8)
+    k_trsv<double, true, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
+  else
+    k_trsv<double, true, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
+  if (nrhs <= 8)
+    k_trsv<double, false, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1, d_status);
+  else
+    k_trsv<double, false, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1,
+                                                         d_status);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_copy_cols<double><<<(n + 255) / 256, 256, 0, s>>>(Y, ldy, n, nrhs, X, ldx);
+  return cudaGetLastError();
+}
+
+cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return cudaSuccess;
+  k_check_finite<<<std::min(1184, (n * nrhs + 255) / 256), 256, 0, s>>>(X, ldx, n, nrhs, d_status);
+  return cudaGetLastError();
+}
+
+}  // namespace bgpu

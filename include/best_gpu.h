@@ -1,0 +1,64 @@
+/* best_gpu.h -- extensions of libbestgpu beyond BEST's nine-function seam (best_hmatrix.h).
+ *
+ * Precision control, timings, device-pointer entry points for callers that keep their data on the
+ * GPU, and the raw FP64 factor/solve kernels with LAPACK semantics.  The reference has no GPU code,
+ * so none of these replaces a reference function one for one; each names the reference routine
+ * whose semantics it follows.  Every int-returning function returns 0 on success, or nonzero after
+ * queuing a message for bhm_log_line.  Device pointers must be 16-byte aligned and leading
+ * dimensions even.  The library works on its own non-blocking stream (bgpu_stream): data written on
+ * other streams must be complete before a call, and each call has finished with its data on return.
+ */
+#ifndef BEST_GPU_H
+#define BEST_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Factorisation precisions for bhm_build. */
+enum {
+  BGPU_FP64 = 0,   /* FP64 LU with partial pivoting (the plain path) */
+  BGPU_MIXED = 1   /* reduced-precision tensor-core LU + FP64 GMRES refinement */
+};
+
+/* Overrides the precision bhm_build derives from direct/single (-1: back to that rule). */
+int bgpu_set_precision(int mode);
+
+/* The precision of the last bhm_build. */
+int bgpu_precision(void);
+
+/* Stage times of the last calls in milliseconds, measured with CUDA events on the library's
+ * stream: ms[0] self blocks + incenters (bhm_create), ms[1] assembly + deflation, ms[2] LU,
+ * ms[3] solve (last bhm_solve or bgpu_solve_device), ms[4] bhm_build total, ms[5] refinement
+ * iterations of the last solve (count, as a double), ms[6] relative residual of the last solve.
+ * Returns the number of values written (at most len). */
+int bgpu_timings(double *ms, int len);
+
+/* The library's CUDA stream (a cudaStream_t), for callers that order their own work after it. */
+void *bgpu_stream(void);
+
+/* bhm_solve for right-hand sides already on the GPU: d_b is 3n x nrhs with leading dimension ldb. */
+int bgpu_solve_device(int nrhs, double *d_b, int ldb);
+
+/* LAPACK dgetrf semantics on a caller's device matrix (best/best.f:444): d_a (n x n, column-major,
+ * lda) is overwritten by L and U, d_ipiv receives the 1-based interchanges, *info (host) the first
+ * exactly-zero pivot (1-based) or 0. */
+int bgpu_dgetrf_device(int n, double *d_a, int lda, int *d_ipiv, int *info);
+
+/* LAPACK dgetrs('N') semantics on device data (best/besolve.f90:133): solves with the factors of
+ * bgpu_dgetrf_device for nrhs <= 16 right-hand sides d_b (n x nrhs, ldb), in place. */
+int bgpu_dgetrs_device(int n, int nrhs, const double *d_a, int lda, const int *d_ipiv, double *d_b, int ldb);
+
+/* C(m x n) -= A(m x k) B(k x n), FP64, column-major device matrices: the LU's trailing update. */
+int bgpu_dgemm_minus_device(int m, int n, int k, const double *d_a, int lda, const double *d_b, int ldb,
+                            double *d_c, int ldc);
+
+/* Assembles GR rows of triangles [r0, r1) x columns of triangles [c0, c1) of the mesh given to
+ * bhm_create into d_out (column-major, ldo), before deflation (best/tgetgr.f:33-173). */
+int bgpu_assemble_device(int r0, int r1, int c0, int c1, double *d_out, int ldo);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
