@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of BEST's dense hot path on the B200: seconds per BEST solve (assemble GR with the
+deflation, LU, solve for the 6 translation/rotation right-hand sides).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload star_f32|ellipsoid_f16|icosphere_l3] [--precision fp64|mixed|both]
+
+One JSON line on rank 0.  `value` is the device time per solve with the mesh already in HBM (CUDA
+events on the library's stream, L2 flushed between steps); `e2e` is the same solve through the C ABI
+with host buffers (bhm_create ... bhm_solve, copies included).  With N GPUs (torchrun), every rank
+solves its own replica: the path has no exchange step, so there is no collective in it.
+`--impl reference` times the reference's own CPU implementation (its kernel.cpp assembly, OpenMP,
+plus the LAPACK dgetrf/dgetrs BEST calls) on bounded samples of the same workload, scaled to a full
+solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # BASELINE configuration of the metric's target: star body at geodesic frequency 32 (N = 20,480)
+    "star_f32": dict(desc="star-shaped body r=25A(1+sum_{l=2..8} a_lm Y_lm), a_lm~N(0,(0.08/l)^2) seed 1, "
+                          "geodesic f=32", N=20480, iarea=0, gen=("star", 32)),
+    "ellipsoid_f16": dict(desc="ellipsoid 30/20/12 A, geodesic f=16, normal jitter U(+-2%) seed 0", N=5120,
+                          iarea=1, gen=("ellipsoid", 16)),
+    "icosphere_l3": dict(desc="icosphere level 3, R=20 A", N=1280, iarea=1, gen=("icosphere", 3)),
+}
+
+
+def make_mesh(name):
+    from best_hydro_b200 import meshes
+    kind, arg = WORKLOADS[name]["gen"]
+    if kind == "star":
+        return meshes.star(arg)
+    if kind == "ellipsoid":
+        return meshes.ellipsoid(arg)
+    return meshes.icosphere(arg, 20.0)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baseline: the reference's own implementation on the host cores, on bounded samples
+# ------------------------------------------------------------------------------------------------
+
+def cpu_reference_sample(tri, iarea, truearea, rows=512, n_lu=12288, seed=0):
+    """One bounded sample, scaled to a full solve: (seconds per solve, parts dict)."""
+    import ctypes
+
+    from oracle import best as ob
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    s = ob.setup(tri, iarea, truearea)
+    n = s.n
+    R = ob.ref_lib()
+    kind = "reference"
+    if R is None:
+        kind = "port"
+    v1, v2, v3 = s.colmajor()
+    rows = min(rows, n)
+    buf = np.empty((3 * rows, 3 * n), order="F")
+    dp = ctypes.POINTER(ctypes.c_double)
+    if R is not None:
+        R.ref_create(n, v1.ctypes.data_as(dp), v2.ctypes.data_as(dp), v3.ctypes.data_as(dp),
+                     s.area.ctypes.data_as(dp), s.afac, 1.0)
+        t0 = time.perf_counter()
+        R.ref_fill(0, rows, 0, n, buf.ctypes.data_as(dp), 3 * rows)
+        t_asm = time.perf_counter() - t0
+        R.ref_destroy()
+    else:
+        L = ob.lib()
+        x, self9 = ob.incenters_and_self(s)
+        t0 = time.perf_counter()
+        L.orc_gr_block(n, v1.ctypes.data_as(dp), v2.ctypes.data_as(dp), v3.ctypes.data_as(dp),
+                       s.area.ctypes.data_as(dp), 1.0, x.ctypes.data_as(dp), self9.ctypes.data_as(dp), 0, rows, 0, n,
+                       buf.ctypes.data_as(dp), 3 * rows)
+        t_asm = time.perf_counter() - t0
+    from scipy.linalg import lapack
+    n3 = 3 * n
+    nl = min(n_lu, n3)
+    rng = np.random.default_rng(seed)
+    A = np.asfortranarray(rng.standard_normal((nl, nl)) + np.sqrt(nl) * np.eye(nl))
+    B = np.asfortranarray(rng.standard_normal((nl, 6)))
+    t0 = time.perf_counter()
+    lu, piv, info = lapack.dgetrf(A, overwrite_a=1)
+    t_lu = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    lapack.dgetrs(lu, piv, B)
+    t_sv = time.perf_counter() - t0
+    asm = t_asm * n / rows
+    fac = t_lu * (n3 / nl) ** 3
+    sv = t_sv * (n3 / nl) ** 2
+    parts = dict(assembly_s=asm, lu_s=fac, solve_s=sv, threads=threads, kind=kind,
+                 sample=f"assembly of {rows} of {n} target rows ({'kernel.cpp' if R is not None else 'C port'}, "
+                        f"OpenMP {threads} threads) scaled by pairs; dgetrf+dgetrs (OpenBLAS via scipy, "
+                        f"{threads} threads) at order {nl} scaled by ({n3}/{nl})^3 and ^2")
+    return asm + fac + sv, parts
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    tri, ta, tv = make_mesh(args.workload)
+    for _ in range(args.warmup):
+        cpu_reference_sample(tri, w["iarea"], ta, rows=64, n_lu=2048)
+    vals, parts = [], None
+    for k in range(args.steps):
+        v, parts = cpu_reference_sample(tri, w["iarea"], ta, seed=k)
+        vals.append(v)
+    v = float(np.median(vals))
+    line = {
+        "impl": "reference", "metric": "s per BEST solve (assemble+LU+6 RHS)", "value": v, "unit": "s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "N": w["N"], "order": 3 * w["N"], "desc": w["desc"]},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": parts["threads"], "kind": parts["kind"],
+                         "sample": parts["sample"], "parts_s": {k: parts[k] for k in ("assembly_s", "lu_s", "solve_s")}},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------
+
+def fp64_peak_tflops(torch, dev):
+    """cuBLAS DGEMM 8192^3 (best of 3): the FP64 denominator (MEASURED_PEAKS.json has none)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import best_hydro_b200 as bh
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    w = WORKLOADS[args.workload]
+    tri, ta, tv = make_mesh(args.workload)
+    st = bh.Setup(tri, w["iarea"], ta)
+    n, n3 = st.n, 3 * st.n
+    peaks, peak_src = load_peaks()
+    p64 = fp64_peak_tflops(torch, dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    prec = {"fp64": bh.BGPU_FP64, "mixed": bh.BGPU_MIXED}.get(args.precision, bh.BGPU_FP64)
+    bh.set_precision(prec)
+    solver = bh.BhmSolver()
+    solver.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+    x = solver.incenters()
+    dm = solver.diag_mean()
+    xmu, gdef = st.deflation(dm)
+    b0 = torch.from_numpy(bh.rhs6(x)).T.contiguous().to(dev)  # rows = right-hand sides: column-major 3n x 6
+    b = torch.empty_like(b0)
+    s = torch.cuda.ExternalStream(bh.lib().bgpu_stream(), device=dev)
+
+    def step():
+        solver.build(eps=1e-10, direct=1 if prec == bh.BGPU_FP64 else 0, ndef=st.ndef, gdef=gdef, comp=st.icomp,
+                     xmu=xmu)
+        with torch.cuda.stream(s):
+            b.copy_(b0)
+        solver.solve_device(b.data_ptr(), 6, n3)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    bh.kernel_stats(enable=1)
+    sampler = ClockSampler(local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev = []
+    launches0 = bh.launch_count()
+    t_wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        step()
+        e1.record(s)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall0
+    launches = bh.launch_count() - launches0
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(c) for a, c in ev]
+    gl, gms, gflop = bh.kernel_stats(enable=0)
+    stage = bh.timings()
+    ms = sum(step_ms) / len(step_ms)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # the solution's tensors (host post-processing, not timed) for the record
+    sol = np.asfortranarray(b.T.cpu().numpy())
+    tens = bh.difco(x, st.area, sol)
+    tr = bh.traces(tens)
+
+    # e2e through the C ABI with host buffers
+    e2e = []
+    h2d = 8 * (12 * n + 3 * n + len(gdef)) + (4 * n if st.ndef > 1 else 0) + 8 * 6 * n3
+    d2h = 8 * (4 * n + 1 + 6 * n3)
+    B_host = bh.rhs6(x)
+    for k in range(0 if args.no_e2e else max(1, args.steps)):
+        solver.destroy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solver.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        xe = solver.incenters()
+        dme = solver.diag_mean()
+        xmu_e, gdef_e = st.deflation(dme)
+        solver.build(eps=1e-10, direct=1 if prec == bh.BGPU_FP64 else 0, ndef=st.ndef, gdef=gdef_e, comp=st.icomp,
+                     xmu=xmu_e)
+        solver.solve(B_host)
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e)) if e2e else float("nan")
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, parts = cpu_reference_sample(tri, w["iarea"], ta)
+        cpu = {"value": v, "unit": "s", "cores": parts["threads"], "kind": parts["kind"], "sample": parts["sample"],
+               "parts_s": {k: parts[k] for k in ("assembly_s", "lu_s", "solve_s")}}
+
+    if rank == 0:
+        gemm_avg_ms = gms / max(gl, 1)
+        achieved = (gflop / max(gl, 1)) / (gemm_avg_ms * 1e-3) / 1e12 if gl else None
+        line = {
+            "metric": "s per BEST solve (assemble+LU+6 RHS)", "value": ms / 1e3 / world, "unit": "s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == bh.BGPU_FP64 else "f32/f64-refined", "data": "synthetic",
+            "config": {"workload": args.workload, "N": n, "order": n3, "desc": w["desc"],
+                       "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "flushed (256 MB write) between timed steps; GR is 72 N^2 bytes, far above L2",
+                       "stages_ms": {k: round(v, 3) for k, v in stage.items() if k in ("assemble", "factor", "solve")},
+                       "wall_s": t_wall},
+            "roofline": {"kernel": "FP64 LU trailing-update GEMM (mma.sync f64, k_dgemm_nn_minus)", "bound": "tensor",
+                         "achieved": achieved, "peak": p64, "unit": "TFLOP/s",
+                         "frac": (achieved / p64) if achieved else None, "traffic": None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                         "launches_per_step": gl / max(args.steps, 1), "share_of_step": gms / max(sum(step_ms), 1e-9)},
+            "clocks": clocks,
+            "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "result": {"D_t_cm2_s": tr["DTRANS"], "D_r_1_s": tr["DR"]},
+            "cpu_baseline": cpu,
+            "peaks": {"source": peak_src, "hbm_gbs": peaks.get("hbm_gbs"), "bf16_tflops": peaks.get("bf16_tflops"),
+                      "fp64_tflops_cublas": p64},
+        }
+        print(json.dumps(line), flush=True)
+    solver.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="star_f32", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

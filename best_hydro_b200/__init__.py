@@ -54,6 +54,20 @@ _SIGS = {
                                                ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
     "bgpu_assemble_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_int]),
+    "bgpu_launch_count": (ctypes.c_ulonglong, []),
+    "bgpu_kernel_stats": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, _dp, _dp]),
+    # include/best_driver.h: BEST's host side around the seam
+    "bgpu_best_setup": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, _dp,
+                                       _dp, _ip, _ip, _ip, _ip]),
+    "bgpu_best_deflation": (ctypes.c_int, [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, _ip, ctypes.c_double, _dp,
+                                           _dp]),
+    "bgpu_best_rhs6": (None, [ctypes.c_int, _dp, _dp]),
+    "bgpu_best_strain5": (None, [ctypes.c_int, _dp, _dp]),
+    "bgpu_best_difco": (ctypes.c_int, [ctypes.c_int, _dp, _dp, ctypes.c_double, _dp, _dp]),
+    "bgpu_best_visco": (ctypes.c_int, [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]),
+    "bgpu_best_traces": (None, [_dp, _dp]),
+    "bgpu_best_run": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_int, _dp]),
 }
 
 
@@ -155,6 +169,115 @@ class BhmSolver:
     def destroy(self):
         self.L.bhm_destroy()
         self.n = 0
+
+
+class Setup:
+    """BEST's arrays after its set-up (best/best.f:261-337), from the C++ host driver."""
+
+    def __init__(self, tri, iarea=1, truearea=None):
+        tri = np.ascontiguousarray(tri, dtype=np.float64)
+        n = tri.shape[0]
+        self.n = n
+        self.v1, self.v2, self.v3 = (np.empty(3 * n) for _ in range(3))
+        self.area = np.empty(n)
+        self.icomp = np.empty(n, dtype=np.int32)
+        a, t = ctypes.c_double(), ctypes.c_double()
+        cen = np.empty(3)
+        nc, no, nd = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        rc = lib().bgpu_best_setup(n, _p(tri), int(iarea), float(truearea or 0.0), _p(self.v1), _p(self.v2),
+                                   _p(self.v3), _p(self.area), ctypes.byref(a), ctypes.byref(t), _p(cen),
+                                   self.icomp.ctypes.data_as(_ip), ctypes.byref(nc), ctypes.byref(no),
+                                   ctypes.byref(nd))
+        if rc:
+            raise BestGpuError("bgpu_best_setup failed")
+        self.afac, self.totarea, self.centroid = a.value, t.value, cen
+        self.ncomp, self.nopen, self.ndef = nc.value, no.value, nd.value
+
+    def deflation(self, diagm):
+        xmu = np.empty(3 * self.n)
+        gdef = np.empty(max(1, self.ndef))
+        lib().bgpu_best_deflation(self.n, _p(self.v1), _p(self.v2), _p(self.v3), _p(self.area), self.ndef,
+                                  self.icomp.ctypes.data_as(_ip), float(diagm), _p(xmu), _p(gdef))
+        return xmu, gdef
+
+
+def rhs6(x):
+    n = x.size // 3
+    b = np.empty((3 * n, 6), order="F")
+    lib().bgpu_best_rhs6(n, _p(np.ascontiguousarray(x)), b.ctypes.data_as(_dp))
+    return b
+
+
+def strain5(x):
+    n = x.size // 3
+    v = np.empty((3 * n, 5), order="F")
+    lib().bgpu_best_strain5(n, _p(np.ascontiguousarray(x)), v.ctypes.data_as(_dp))
+    return v
+
+
+TENSOR_KEYS = (("Dtt", 0, 9), ("Dtr", 9, 9), ("Drr", 18, 9), ("urc", 27, 3), ("udr", 30, 3), ("Ktt", 33, 9),
+               ("KrtCR", 42, 9), ("KrrCR", 51, 9))
+
+
+def _unpack(out):
+    return {k: (out[o:o + m].reshape(3, 3).copy() if m == 9 else out[o:o + m].copy()) for k, o, m in TENSOR_KEYS}
+
+
+def difco(x, area, b6, cg=1.0):
+    """best/difco.f on the six solutions: dict of Dtt, Dtr, Drr, urc, udr, Ktt, KrtCR, KrrCR."""
+    n = area.size
+    out = np.empty(60)
+    b6 = np.asfortranarray(b6, dtype=np.float64)
+    lib().bgpu_best_difco(n, _p(np.ascontiguousarray(x)), _p(np.ascontiguousarray(area)), float(cg),
+                          b6.ctypes.data_as(_dp), _p(out))
+    return _unpack(out)
+
+
+def visco(x, area, v5, b6, icov=0, cg=1.0):
+    """best/visco.f: (CHI', (Dx, Dy, Dz))."""
+    n = area.size
+    out = np.empty(4)
+    v5 = np.asfortranarray(v5, dtype=np.float64)
+    b6 = np.asfortranarray(b6, dtype=np.float64)
+    lib().bgpu_best_visco(n, _p(np.ascontiguousarray(x)), _p(np.ascontiguousarray(area)), float(cg), int(icov),
+                          v5.ctypes.data_as(_dp), b6.ctypes.data_as(_dp), _p(out))
+    return float(out[0]), (float(out[1]), float(out[2]), float(out[3]))
+
+
+def traces(t):
+    """best/output.f:96-130 from difco's tensors: dict trace_dtt, trace_drr, DTRANS, DR."""
+    buf = np.zeros(60)
+    for k, o, m in TENSOR_KEYS:
+        buf[o:o + m] = np.asarray(t[k]).ravel()
+    out = np.empty(4)
+    lib().bgpu_best_traces(_p(buf), _p(out))
+    return dict(trace_dtt=float(out[0]), trace_drr=float(out[1]), DTRANS=float(out[2]), DR=float(out[3]))
+
+
+def best_run(path, iarea=1, cg_zero=0, ivisco=0, icov=0, wm=0.0, precision=-1):
+    """The whole BEST program on the GPU (writes <path><flags>.be and .log); returns a dict."""
+    out = np.zeros(68)
+    _check(lib().bgpu_best_run(str(path).encode(), int(iarea), int(cg_zero), int(ivisco), int(icov), float(wm),
+                               int(precision), _p(out)), "bgpu_best_run")
+    d = _unpack(out[:60])
+    d.update(chiprime=out[60], dvisc=tuple(out[61:64]), DTRANS=out[64], DR=out[65], CHI=out[66], ETA=out[67])
+    return d
+
+
+BGPU_KERNEL_LU_GEMM64 = 0
+
+
+def kernel_stats(kernel=BGPU_KERNEL_LU_GEMM64, enable=1):
+    """(launches, ms, flops) recorded since the last call; then recording on/off."""
+    l, t, w = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+    _check(lib().bgpu_kernel_stats(int(kernel), int(enable), ctypes.byref(l), ctypes.byref(t), ctypes.byref(w)),
+           "bgpu_kernel_stats")
+    return l.value, t.value, w.value
+
+
+def launch_count():
+    """Kernel launches the library has issued (bgpu_launch_count)."""
+    return int(lib().bgpu_launch_count())
 
 
 def set_precision(mode):

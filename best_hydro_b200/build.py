@@ -25,7 +25,10 @@ SOURCES = [
     ("solve.cu", []),
     ("mixed.cu", []),
     ("api.cpp", []),
+    ("driver.cpp", []),
 ]
+# host programs linked against the library: (source, output name)
+PROGRAMS = [("best_gpu_main.cpp", "best_gpu")]
 
 
 def _headers():
@@ -64,6 +67,12 @@ def build(verbose=False):
             _run([NVCC] + ARCH + COMMON + extra + lang + ["-c", s, "-o", o], verbose)
     if _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs, verbose)
+    for src, name in PROGRAMS:
+        s = os.path.join(CSRC, src)
+        exe = os.path.join(LIBDIR, name)
+        if _newer(exe, [s, LIB] + hdrs):
+            _run(["g++", "-O2", "-std=c++17", f"-I{os.path.join(ROOT, 'include')}", "-o", exe, s, f"-L{LIBDIR}",
+                  "-lbestgpu", "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 

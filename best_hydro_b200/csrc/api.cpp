@@ -540,6 +540,25 @@ int bgpu_dgemm_minus_device(int m, int n, int k, const double* d_a, int lda, con
   });
 }
 
+unsigned long long bgpu_launch_count(void) { return g_launches; }
+
+int bgpu_kernel_stats(int kernel, int enable, int* launches, double* ms, double* work) {
+  return guarded([&] {
+    if (kernel != BGPU_KERNEL_LU_GEMM64) {
+      say("error: unknown kernel id %d", kernel);
+      return 1;
+    }
+    int l = 0;
+    double t = 0, w = 0;
+    lu_gemm_timer_read(&l, &t, &w);
+    if (launches) *launches = l;
+    if (ms) *ms = t;
+    if (work) *work = w;
+    lu_gemm_timer_enable(enable != 0);
+    return 0;
+  });
+}
+
 int bgpu_assemble_device(int r0, int r1, int c0, int c1, double* d_out, int ldo) {
   return guarded([&] {
     Solver& s = solver();

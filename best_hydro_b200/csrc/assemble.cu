@@ -3,8 +3,9 @@
 // Compiled with -fmad=false: BEST is built with -ffp-contract=off (reference Makefile:34, :40), so
 // every product and sum below must round separately, in the order the reference writes it, for the
 // entries to match the reference's bit for bit.  IEEE +, -, *, / and sqrt are correctly rounded on
-// both sides; only the transcendental functions (log here; acos, sin, cos, log in the O(N) self
-// blocks) come from CUDA's library instead of glibc.
+// both sides.  The transcendental functions of the O(N) self blocks (acos, sin, cos, log) are the
+// correctly rounded ones of ddmath.cuh, which return what glibc returns for almost every argument;
+// the pair integrals' log is CUDA's (within an ulp; it reaches the entries without cancellation).
 //
 // Kernels:
 //   k_self_blocks   one thread per triangle: incenter, normal and the exact self-integral block,
@@ -18,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "bgpu_internal.h"
+#include "ddmath.cuh"
 
 namespace bgpu {
 namespace {
@@ -47,8 +49,15 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
   return a0 * b0 + a1 * b1 + a2 * b2;
 }
 
+using dd::cr_acos;
+using dd::cr_cos;
+using dd::cr_log;
+using dd::cr_sin;
+
 // tgetgr.f:177-187
-__device__ __forceinline__ double si_fn(double x) { return 2.0 * (log((1.0 + sqrt(1.0 - x * x)) / x) - sqrt(1.0 - x * x)); }
+__device__ __forceinline__ double si_fn(double x) {
+  return 2.0 * (cr_log((1.0 + sqrt(1.0 - x * x)) / x) - sqrt(1.0 - x * x));
+}
 __device__ __forceinline__ double csi_fn(double x) { return 3.0 - 1.0 / x - 2.0 * x; }
 
 __global__ void k_self_blocks(int n, const double* __restrict__ geo, double afac, double cg, double* __restrict__ xc,
@@ -82,26 +91,26 @@ __global__ void k_self_blocks(int n, const double* __restrict__ geo, double afac
   ny = .5 * ny / area2;
   nz = .5 * nz / area2;
   // exact self integrals (:67-112)
-  const double cc = acos(cosC);
-  const double r = tin * sin(cc);
+  const double cc = cr_acos(cosC);
+  const double r = tin * cr_sin(cc);
   const double cosB = -(v21x * v32x + v21y * v32y + v21z * v32z) / a / c;
-  const double bb = acos(cosB);
+  const double bb = cr_acos(cosB);
   const double aa = pi - bb - cc;
-  const double hcos = 1. / (2. * cos(0.5 * cc));
+  const double hcos = 1. / (2. * cr_cos(0.5 * cc));
   const double dc = (a + b - c) * hcos;
   const double db = sqrt(a * a + (b - c) * (b - c) - 2. * a * (b - c) * cosC) * hcos;
   const double da = sqrt(b * b + (a - c) * (a - c) - 2. * b * (a - c) * cosC) * hcos;
   const double ha = r / da, hb = r / db, hc = r / dc;
-  const double dpa = (pi - aa) * (da - r) - 2.0 * (da * acos(ha) - r * log((1. + sqrt(1. - ha * ha)) / ha));
-  const double dpb = (pi - bb) * (db - r) - 2.0 * (db * acos(hb) - r * log((1. + sqrt(1. - hb * hb)) / hb));
-  const double dpc = (pi - cc) * (dc - r) - 2.0 * (dc * acos(hc) - r * log((1. + sqrt(1. - hc * hc)) / hc));
+  const double dpa = (pi - aa) * (da - r) - 2.0 * (da * cr_acos(ha) - r * cr_log((1. + sqrt(1. - ha * ha)) / ha));
+  const double dpb = (pi - bb) * (db - r) - 2.0 * (db * cr_acos(hb) - r * cr_log((1. + sqrt(1. - hb * hb)) / hb));
+  const double dpc = (pi - cc) * (dc - r) - 2.0 * (dc * cr_acos(hc) - r * cr_log((1. + sqrt(1. - hc * hc)) / hc));
   const double sca =
-      0.5 * r * ((cos(2.0 * cc) + cos(2.0 * bb)) * si_fn(ha) - (sin(2.0 * cc) + sin(2.0 * bb)) * csi_fn(ha));
-  const double scb = 0.5 * r * ((1. + cos(2.0 * bb)) * si_fn(hb) + sin(2.0 * bb) * csi_fn(hb));
-  const double scc = 0.5 * r * ((1. + cos(2.0 * cc)) * si_fn(hc) + sin(2.0 * cc) * csi_fn(hc));
-  const double cca = -(sin(bb - cc) * r * (cos(aa) * si_fn(ha) + sin(aa) * csi_fn(ha)));
-  const double ccb = sin(bb) * r * (cos(bb) * si_fn(hb) + sin(bb) * csi_fn(hb));
-  const double ccc = -(sin(cc) * r * (cos(cc) * si_fn(hc) + sin(cc) * csi_fn(hc)));
+      0.5 * r * ((cr_cos(2.0 * cc) + cr_cos(2.0 * bb)) * si_fn(ha) - (cr_sin(2.0 * cc) + cr_sin(2.0 * bb)) * csi_fn(ha));
+  const double scb = 0.5 * r * ((1. + cr_cos(2.0 * bb)) * si_fn(hb) + cr_sin(2.0 * bb) * csi_fn(hb));
+  const double scc = 0.5 * r * ((1. + cr_cos(2.0 * cc)) * si_fn(hc) + cr_sin(2.0 * cc) * csi_fn(hc));
+  const double cca = -(cr_sin(bb - cc) * r * (cr_cos(aa) * si_fn(ha) + cr_sin(aa) * csi_fn(ha)));
+  const double ccb = cr_sin(bb) * r * (cr_cos(bb) * si_fn(hb) + cr_sin(bb) * csi_fn(hb));
+  const double ccc = -(cr_sin(cc) * r * (cr_cos(cc) * si_fn(hc) + cr_sin(cc) * csi_fn(hc)));
   const double cor = sqrt(afac);
   // local g (1-based as in the Fortran; g(1,3) = g(2,3) = g(3,1) = g(3,2) = 0)
   double gl[4][4];
@@ -334,6 +343,7 @@ __global__ void k_diag_mean(int n, const double* __restrict__ self9, double* out
 cudaError_t launch_self_blocks(const DevMesh& m, cudaStream_t s) {
   if (m.n <= 0) return cudaSuccess;
   k_self_blocks<<<(m.n + 127) / 128, 128, 0, s>>>(m.n, m.geo, m.afac, m.cg, m.xc, m.self9);
+  BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -352,11 +362,13 @@ cudaError_t launch_assemble(const DevMesh& m, int r0, int r1, int c0, int c1, do
     return cudaSuccess;
   }
   k_assemble<<<grid, kTgtTile, 0, s>>>(m.n, m.geo, m.xc, m.self9, m.cg, r0, r1, c0, c1, out, ld, defl, out32, ld32);
+  BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
 cudaError_t launch_diag_mean(const DevMesh& m, double* d_out, cudaStream_t s) {
   k_diag_mean<<<1, 32, 0, s>>>(m.n, m.self9, d_out);
+  BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 

@@ -10,6 +10,10 @@
 
 namespace bgpu {
 
+// Kernel launches issued by the library since it was loaded (bgpu_launch_count).
+extern unsigned long long g_launches;
+#define BGPU_COUNT_LAUNCH() (++::bgpu::g_launches)
+
 // Device status codes written by kernels into a status word (0 = ok).  Kernels never trap: a
 // bounded wait that runs out, or an index check that fails, records a code here and returns.
 enum DevStatus : int {
@@ -64,6 +68,9 @@ size_t lu_scratch_bytes(int n);
 // DevStatus.  Host-side errors return a cudaError_t.
 cudaError_t lu64_getrf(double* A, long lda, int n, int* ipiv, int* d_info, int* d_status, const LuScratch& ws,
                        cudaStream_t s);
+// Opt-in CUDA-event timing of the LU's trailing-update GEMM launches.
+void lu_gemm_timer_enable(bool on);
+void lu_gemm_timer_read(int* launches, double* ms, double* flops);
 // C(m x n) -= A(m x k) B(k x n), all column-major (FP64 tensor-core path).
 cudaError_t dgemm_nn_minus(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C,
                            long ldc, cudaStream_t s);

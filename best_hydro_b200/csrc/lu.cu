@@ -18,10 +18,14 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "bgpu_internal.h"
 
 namespace bgpu {
+
+unsigned long long g_launches = 0;
+
 namespace {
 
 // ------------------------------------------------------------------------------------------
@@ -172,6 +176,7 @@ cudaError_t run_gemm(int m, int n, int k, const double* A, long lda, const doubl
   }
   dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN);
   kern<<<grid, Cfg::kThreads, Cfg::kSmem, s>>>(m, n, k, A, lda, B, ldb, C, ldc);
+  BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -457,6 +462,7 @@ cudaError_t laswp(const Ctx& c, int c0, int c1, int j0, int j1) {
   if (c1 <= c0 || j1 <= j0) return cudaSuccess;
   const int threads = 128;
   k_laswp<<<(c1 - c0 + threads - 1) / threads, threads, 0, c.s>>>(c.A, c.lda, c0, c1, c.ipiv, j0, j1);
+  BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -465,6 +471,7 @@ cudaError_t trsm_lower_unit(const double* L, long lda, int kb, double* B, int nc
   if (kb <= 0 || nc <= 0) return cudaSuccess;
   if (kb <= kTrsmLeaf) {
     k_trsm_leaf<<<(nc + kTrsmCols - 1) / kTrsmCols, kTrsmCols, 0, s>>>(L, lda, kb, B, lda, nc);
+    BGPU_COUNT_LAUNCH();
     return cudaGetLastError();
   }
   int k1 = (kb / 2 + 15) / 16 * 16;
@@ -505,9 +512,11 @@ cudaError_t leaf(const Ctx& c, int k, int w) {
     int* status = c.status;
     unsigned char* scr = c.leaf_scratch;
     void* args[] = {&P, &lda, &mm, &ww, &RR, &ip, &ro, &info, &status, &scr};
+    BGPU_COUNT_LAUNCH();
     return cudaLaunchCooperativeKernel((const void*)k_leaf, dim3(G), dim3(kLeafThreads), args, smem, c.s);
   }
   k_leaf<<<1, kLeafThreads, smem, c.s>>>(P, c.lda, m, w, R, ip, k, c.info, c.status, c.leaf_scratch);
+  BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -531,7 +540,53 @@ cudaError_t panel(const Ctx& c, int k, int w) {
   return laswp(c, k, k + w1, k + w1, k + w);
 }
 
+// Live timing of the trailing-update GEMM launches (opt-in; for the roofline report).
+struct GemmTimer {
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  size_t used = 0;
+  double flops = 0;
+  void begin(cudaStream_t s) {
+    if (!on) return;
+    if (used == ev.size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      ev.emplace_back(a, b);
+    }
+    cudaEventRecord(ev[used].first, s);
+  }
+  void end(cudaStream_t s, double f) {
+    if (!on) return;
+    cudaEventRecord(ev[used].second, s);
+    ++used;
+    flops += f;
+  }
+} g_gemm_timer;
+
 }  // namespace
+
+void lu_gemm_timer_enable(bool on) {
+  g_gemm_timer.on = on;
+  g_gemm_timer.used = 0;
+  g_gemm_timer.flops = 0;
+}
+
+// Sums the recorded launches (synchronising on the last one) and resets the counters.
+void lu_gemm_timer_read(int* launches, double* ms, double* flops) {
+  double t = 0;
+  if (g_gemm_timer.used) cudaEventSynchronize(g_gemm_timer.ev[g_gemm_timer.used - 1].second);
+  for (size_t i = 0; i < g_gemm_timer.used; ++i) {
+    float x = 0;
+    cudaEventElapsedTime(&x, g_gemm_timer.ev[i].first, g_gemm_timer.ev[i].second);
+    t += x;
+  }
+  *launches = (int)g_gemm_timer.used;
+  *ms = t;
+  *flops = g_gemm_timer.flops;
+  g_gemm_timer.used = 0;
+  g_gemm_timer.flops = 0;
+}
 
 size_t lu_scratch_bytes(int) { return LeafScratchLayout::kEnd; }
 
@@ -560,10 +615,12 @@ cudaError_t lu64_getrf(double* A, long lda, int n, int* ipiv, int* d_info, int* 
       if ((e = trsm_lower_unit(A + k + (size_t)k * lda, lda, kb, A + k + (size_t)(k + kb) * lda, n - k - kb, s)) !=
           cudaSuccess)
         return e;
+      g_gemm_timer.begin(s);
       if ((e = gemm_minus(n - k - kb, n - k - kb, kb, A + (k + kb) + (size_t)k * lda, lda,
                           A + k + (size_t)(k + kb) * lda, lda, A + (k + kb) + (size_t)(k + kb) * lda, lda, s)) !=
           cudaSuccess)
         return e;
+      g_gemm_timer.end(s, 2.0 * (double)(n - k - kb) * (double)(n - k - kb) * kb);
     }
   }
   return cudaSuccess;

@@ -268,8 +268,8 @@ unsigned g_epoch = 0;
 
 cudaError_t lu_perm_from_ipiv(const int* ipiv, int n, int* perm, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_perm_init<<<(n + 255) / 256, 256, 0, s>>>(perm, n);
-  k_perm_compose<<<1, 1024, 0, s>>>(ipiv, n, perm);
+  k_perm_init<<<(n + 255) / 256, 256, 0, s>>>(perm, n); BGPU_COUNT_LAUNCH();
+  k_perm_compose<<<1, 1024, 0, s>>>(ipiv, n, perm); BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -286,7 +286,7 @@ cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* 
   unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
   double* Y = reinterpret_cast<double*>(base + TrsvScratch::y_off(n));
   const long ldy = n;
-  k_gather_rows<double><<<(n + 255) / 256, 256, 0, s>>>(X, ldx, perm, n, nrhs, Y, ldy);
+  k_gather_rows<double><<<(n + 255) / 256, 256, 0, s>>>(X, ldx, perm, n, nrhs, Y, ldy); BGPU_COUNT_LAUNCH();
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -297,25 +297,27 @@ cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* 
   if (g_epoch == 0) g_epoch = 2;
   cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
   if (e != cudaSuccess) return e;
+  BGPU_COUNT_LAUNCH();
   if (nrhs <= 8)
     k_trsv<double, true, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
   else
     k_trsv<double, true, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
+  BGPU_COUNT_LAUNCH();
   if (nrhs <= 8)
     k_trsv<double, false, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1, d_status);
   else
     k_trsv<double, false, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1,
                                                          d_status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_copy_cols<double><<<(n + 255) / 256, 256, 0, s>>>(Y, ldy, n, nrhs, X, ldx);
+  k_copy_cols<double><<<(n + 255) / 256, 256, 0, s>>>(Y, ldy, n, nrhs, X, ldx); BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s) {
   if (n <= 0 || nrhs <= 0) return cudaSuccess;
-  k_check_finite<<<std::min(1184, (n * nrhs + 255) / 256), 256, 0, s>>>(X, ldx, n, nrhs, d_status);
+  k_check_finite<<<std::min(1184, (n * nrhs + 255) / 256), 256, 0, s>>>(X, ldx, n, nrhs, d_status); BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 

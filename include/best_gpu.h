@@ -57,6 +57,16 @@ int bgpu_dgemm_minus_device(int m, int n, int k, const double *d_a, int lda, con
  * bhm_create into d_out (column-major, ldo), before deflation (best/tgetgr.f:33-173). */
 int bgpu_assemble_device(int r0, int r1, int c0, int c1, double *d_out, int ldo);
 
+/* Kernel launches the library has issued since it was loaded. */
+unsigned long long bgpu_launch_count(void);
+
+/* Kernels whose launches can be timed live (CUDA events on the library's stream). */
+enum { BGPU_KERNEL_LU_GEMM64 = 0 /* the FP64 LU's trailing-update GEMM (DMMA) */ };
+
+/* Returns, for `kernel`, the launches recorded since the last call, their summed device time (ms) and
+ * their algorithmic work (flops), then turns recording on (enable = 1) or off (0). */
+int bgpu_kernel_stats(int kernel, int enable, int *launches, double *ms, double *work);
+
 #ifdef __cplusplus
 }
 #endif

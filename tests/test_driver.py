@@ -1,0 +1,45 @@
+"""CPU tests of the product's C++ host driver (include/best_driver.h) against the oracle's numpy
+restatement of the same Fortran: two independent restatements of best.f's set-up, COMPON, the
+deflation vectors, DIFCO, VISCO and OUTPUT's traces, fed with the oracle's LAPACK solutions."""
+import numpy as np
+import pytest
+
+import best_hydro_b200 as bh
+from oracle import best as ob
+from tests.helpers import golden_mesh
+
+
+@pytest.fixture(scope="module", params=["2eu7_02562", "1aki49_atom_01806"])
+def case(request):
+    tri, ta, tv = golden_mesh(request.param)
+    o = ob.best_run(tri, ta, tv, iarea=1, ivisco=1, icov=1, wm=30000.0)
+    return tri, ta, tv, o
+
+
+def test_setup_compon_deflation_bitwise(case):
+    tri, ta, tv, o = case
+    s = bh.Setup(tri, 1, ta)
+    v1, v2, v3 = o.setup.colmajor()
+    for a, b in ((s.v1, v1), (s.v2, v2), (s.v3, v3), (s.area, o.setup.area)):
+        assert np.array_equal(a, b)
+    assert s.afac == o.setup.afac and s.totarea == o.setup.totarea
+    assert (s.ncomp, s.nopen, s.ndef) == (o.setup.ncomp, o.setup.nopen, o.setup.ndef)
+    assert np.array_equal(s.icomp, o.setup.icomp)
+    xmu, gdef = s.deflation(o.diagm)
+    assert np.array_equal(xmu, o.xmu)
+    np.testing.assert_array_equal(gdef, o.gdef)
+
+
+def test_rhs_and_postprocessing(case):
+    tri, ta, tv, o = case
+    assert np.array_equal(bh.rhs6(o.x), ob.rhs6(o.x, o.setup.n))
+    assert np.array_equal(bh.strain5(o.x), ob.strain5(o.x, o.setup.n))
+    t = bh.difco(o.x, o.setup.area, o.B6)
+    for k in ("Dtt", "Dtr", "Drr", "urc", "udr"):
+        np.testing.assert_allclose(t[k], o.tensors[k], rtol=1e-13, atol=1e-13 * np.max(np.abs(o.tensors[k])))
+    chip, dv = bh.visco(o.x, o.setup.area, o.V5, o.B6, icov=1)
+    assert abs(chip / o.chiprime - 1) < 1e-13
+    np.testing.assert_allclose(dv, o.dvisc, rtol=1e-12)
+    tr = bh.traces(t)
+    assert abs(tr["DTRANS"] / o.report["DTRANS"] - 1) < 1e-13
+    assert abs(tr["DR"] / o.report["DR"] - 1) < 1e-13
