@@ -100,3 +100,18 @@ def test_compon_open_surface_falls_back_to_one_deflation():
     tri, ta, tv = meshes.icosphere(1, 10.0)
     s = ob.setup(tri[1:], 0, None)
     assert s.nopen > 0 and s.ndef == 1 and np.all(s.icomp == 1)
+
+
+def test_self_blocks_differ_from_glibc_only_where_glibc_misrounds():
+    """The reference's self-block arithmetic with correctly rounded acos/sin/cos/log (what the GPU
+    kernel computes) against the same arithmetic with glibc's: the few entries that differ are within
+    4 ulp of their block's largest entry (cancellation residues of glibc's misrounded calls)."""
+    from tests import crshim
+    tri, ta, tv = golden_mesh("2eu7_02562")
+    s = ob.setup(tri, 1, ta)
+    x_cr, s_cr = crshim.self_blocks_cr(s)
+    x_g, s_g = ob.incenters_and_self(s)
+    assert np.array_equal(x_cr, x_g)  # incenters use no transcendental function
+    same = np.count_nonzero(s_cr == s_g)
+    assert same >= 0.99 * s_g.size
+    assert np.max(crshim.block_scale_ulps(s_cr, s_g)) <= 4
