@@ -50,6 +50,8 @@ _SIGS = {
     "bgpu_dgetrf_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, _ip]),
     "bgpu_dgetrs_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_int]),
+    "bgpu_dgetrs_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "bgpu_dgemm_minus_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                                ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
     "bgpu_assemble_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
@@ -295,6 +297,12 @@ def dgetrf_device(n, d_a, lda, d_ipiv):
 def dgetrs_device(n, nrhs, d_a, lda, d_ipiv, d_b, ldb):
     _check(lib().bgpu_dgetrs_device(int(n), int(nrhs), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_ipiv),
                                     ctypes.c_void_p(d_b), int(ldb)), "bgpu_dgetrs_device")
+
+
+def dgetrs_noalloc(n, nrhs, d_a, lda, d_ipiv, d_b, ldb, stream=0):
+    """bgpu_dgetrs_noalloc: the solve without device allocations (see include/best_gpu.h)."""
+    _check(lib().bgpu_dgetrs_noalloc(int(n), int(nrhs), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_ipiv),
+                                     ctypes.c_void_p(d_b), int(ldb), ctypes.c_void_p(stream)), "bgpu_dgetrs_noalloc")
 
 
 def dgemm_minus_device(m, n, k, d_a, lda, d_b, ldb, d_c, ldc):

@@ -237,6 +237,9 @@ void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
 }
 
 }  // namespace
+
+void log_message(const char* msg) { g_log.emplace_back(msg); }
+
 }  // namespace bgpu
 
 using namespace bgpu;

@@ -46,6 +46,9 @@ struct DevDeflation {
   const double* xmu = nullptr;
 };
 
+// Queues a message for bhm_log_line (api.cpp).
+void log_message(const char* msg);
+
 // assemble.cu -------------------------------------------------------------------------------
 cudaError_t launch_self_blocks(const DevMesh& m, cudaStream_t s);
 // GR rows of targets [r0,r1) x columns of sources [c0,c1) into out (column-major, ld), entry

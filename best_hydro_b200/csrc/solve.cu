@@ -13,8 +13,17 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
+#include <mutex>
 
+#include "../../include/best_gpu.h"
 #include "bgpu_internal.h"
+
+// Device scratch of bgpu_dgetrs_noalloc, for callers that cannot allocate GPU memory: 16 MiB held by
+// every GPU that loads the library, until the process exits.  Host code must not use this name as
+// an address (it is a host-side stand-in); the entry point below looks the device address up with
+// cudaGetSymbolAddress once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[16u << 20];
 
 namespace bgpu {
 namespace {
@@ -321,4 +330,97 @@ cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_stat
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------------------
+// bgpu_dgetrs_noalloc: the solve without any device allocation
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocBytes = sizeof(g_noalloc_scratch);
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_base[kMaxDevices] = {};
+
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+// [0, 256) status word | trsv scratch (ticket, readiness flags, permuted right-hand sides) | perm
+size_t noalloc_bytes(int n) { return 256 + round256(trsv_scratch_bytes(n)) + round256(4 * (size_t)n); }
+
+int noalloc_max_n() {
+  int lo = 0, hi = 1 << 24;
+  while (lo < hi) {
+    const int mid = lo + (hi - lo + 1) / 2;
+    if (noalloc_bytes(mid) <= kNoAllocBytes) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Once per device, with that device current: the device address of the scratch, zeroed.
+cudaError_t noalloc_base(unsigned char** out, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_base[dev]) {
+    void* p = nullptr;
+    if ((e = cudaGetSymbolAddress(&p, g_noalloc_scratch)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(p, 0, kNoAllocBytes, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    g_noalloc_base[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_base[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
 }  // namespace bgpu
+
+using bgpu::log_message;
+
+extern "C" int bgpu_dgetrs_noalloc(int n, int nrhs, const double* d_a, int lda, const int* d_ipiv, double* d_b,
+                                   int ldb, void* stream) {
+  using namespace bgpu;
+  char msg[256];
+  if (n < 0 || nrhs < 1 || nrhs > kMaxRhs || lda < std::max(1, n) || ldb < std::max(1, n)) {
+    std::snprintf(msg, sizeof msg, "error: bgpu_dgetrs_noalloc: bad arguments (n %d, nrhs %d in 1..%d, lda %d, ldb %d)",
+                  n, nrhs, kMaxRhs, lda, ldb);
+    log_message(msg);
+    return 1;
+  }
+  const int nmax = noalloc_max_n();
+  if (n > nmax) {
+    std::snprintf(msg, sizeof msg,
+                  "error: bgpu_dgetrs_noalloc: order %d exceeds %d, the most its fixed %zu MiB device scratch holds", n,
+                  nmax, kNoAllocBytes >> 20);
+    log_message(msg);
+    return 1;
+  }
+  if (n == 0) return 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  unsigned char* base = nullptr;
+  cudaError_t e = noalloc_base(&base, s);
+  if (e == cudaSuccess) {
+    int* status = reinterpret_cast<int*>(base);
+    unsigned char* trsv = base + 256;
+    int* perm = reinterpret_cast<int*>(base + 256 + round256(trsv_scratch_bytes(n)));
+    if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) == cudaSuccess &&
+        (e = lu_perm_from_ipiv(d_ipiv, n, perm, s)) == cudaSuccess &&
+        (e = getrs64(d_a, lda, n, perm, d_b, ldb, nrhs, trsv, status, s)) == cudaSuccess &&
+        (e = check_finite(d_b, ldb, n, nrhs, status, s)) == cudaSuccess) {
+      int st = 0;
+      if ((e = cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s)) == cudaSuccess &&
+          (e = cudaStreamSynchronize(s)) == cudaSuccess) {
+        if (st == kOk) return 0;
+        std::snprintf(msg, sizeof msg, "error: bgpu_dgetrs_noalloc: %s",
+                      st == kWaitTimeout ? "a device-side wait ran out (kernel gave up, no result)"
+                                         : "the solution is not finite (NaN or Inf)");
+        log_message(msg);
+        return 1;
+      }
+    }
+  }
+  std::snprintf(msg, sizeof msg, "error: bgpu_dgetrs_noalloc: CUDA error: %s", cudaGetErrorString(e));
+  log_message(msg);
+  return 1;
+}

@@ -49,6 +49,21 @@ int bgpu_dgetrf_device(int n, double *d_a, int lda, int *d_ipiv, int *info);
  * bgpu_dgetrf_device for nrhs <= 16 right-hand sides d_b (n x nrhs, ldb), in place. */
 int bgpu_dgetrs_device(int n, int nrhs, const double *d_a, int lda, const int *d_ipiv, double *d_b, int ldb);
 
+/* The solve of bgpu_dgetrs_device for callers that cannot allocate GPU memory.  It calls no
+ * cudaMalloc, cudaFree or other allocating routine: an application that owns all device memory
+ * through its own pool allocator, or that must not let a library allocate behind its back, can still
+ * solve with the factors.  Its scratch (readiness flags, the permuted right-hand sides, the
+ * permutation, a status word) is a fixed 16 MiB array in the library's device image, which every GPU
+ * that loads the library holds until the process exits; that bounds the order: n * (8 * 16 + 4) bytes
+ * plus a few KB must fit, i.e. n <= about 127,000 (larger n is rejected with a message).  The first
+ * call on each device looks the array up and zeroes it, so make that first call before any stream
+ * capture.  stream: a cudaStream_t (NULL for the default stream); the call returns when the solve on
+ * it has finished.  Every call uses the same array: calls that overlap on the GPU (other threads,
+ * other streams of the same device) race and must be serialised by the caller.  No reference
+ * counterpart: the reference has no GPU code. */
+int bgpu_dgetrs_noalloc(int n, int nrhs, const double *d_a, int lda, const int *d_ipiv, double *d_b, int ldb,
+                        void *stream);
+
 /* C(m x n) -= A(m x k) B(k x n), FP64, column-major device matrices: the LU's trailing update. */
 int bgpu_dgemm_minus_device(int m, int n, int k, const double *d_a, int lda, const double *d_b, int ldb,
                             double *d_c, int ldc);
