@@ -44,6 +44,7 @@ _SIGS = {
     "bhm_destroy": (None, []),
     "bgpu_set_precision": (ctypes.c_int, [ctypes.c_int]),
     "bgpu_precision": (ctypes.c_int, []),
+    "bgpu_set_refinement": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "bgpu_timings": (ctypes.c_int, [_dp, ctypes.c_int]),
     "bgpu_stream": (ctypes.c_void_p, []),
     "bgpu_solve_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
@@ -54,6 +55,9 @@ _SIGS = {
                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "bgpu_dgemm_minus_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                                ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
+    "bgpu_gemm_bf16_minus_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                   ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                   ctypes.c_int]),
     "bgpu_assemble_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_int]),
     "bgpu_launch_count": (ctypes.c_ulonglong, []),
@@ -282,6 +286,10 @@ def launch_count():
     return int(lib().bgpu_launch_count())
 
 
+def set_refinement(max_restarts=8, krylov=10):
+    _check(lib().bgpu_set_refinement(int(max_restarts), int(krylov)), "bgpu_set_refinement")
+
+
 def set_precision(mode):
     _check(lib().bgpu_set_precision(int(mode)), "bgpu_set_precision")
 
@@ -308,6 +316,12 @@ def dgetrs_noalloc(n, nrhs, d_a, lda, d_ipiv, d_b, ldb, stream=0):
 def dgemm_minus_device(m, n, k, d_a, lda, d_b, ldb, d_c, ldc):
     _check(lib().bgpu_dgemm_minus_device(int(m), int(n), int(k), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_b),
                                          int(ldb), ctypes.c_void_p(d_c), int(ldc)), "bgpu_dgemm_minus_device")
+
+
+def gemm_bf16_minus_device(m, n, k, d_a, lda, d_b, ldb, d_c, ldc):
+    _check(lib().bgpu_gemm_bf16_minus_device(int(m), int(n), int(k), ctypes.c_void_p(d_a), int(lda),
+                                             ctypes.c_void_p(d_b), int(ldb), ctypes.c_void_p(d_c), int(ldc)),
+           "bgpu_gemm_bf16_minus_device")
 
 
 def assemble_device(r0, r1, c0, c1, d_out, ldo):

@@ -23,6 +23,7 @@ SOURCES = [
     ("assemble.cu", ["-fmad=false"]),
     ("lu.cu", []),
     ("solve.cu", []),
+    ("tc_gemm.cu", []),
     ("mixed.cu", []),
     ("api.cpp", []),
     ("driver.cpp", []),

@@ -164,7 +164,7 @@ struct Solver {
   long ld = 0;
   DevBuf ipiv, perm;
   DevBuf gdef, comp, xmu;
-  DevBuf rhs;                  // right-hand sides, n3 x 16
+  DevBuf rhs, rhs_keep;        // right-hand sides (host-interface staging, and a kept copy)
   std::unique_ptr<MixedSolver> mixed;
   int precision = BGPU_FP64;
   bool factored = false;
@@ -182,6 +182,7 @@ struct Solver {
 
 std::unique_ptr<Solver> g;
 int g_prec_override = -1;
+int g_refine[2] = {8, 10};  // GMRES restarts, Krylov vectors per restart
 double g_solve_info[2] = {0, 0};  // refinement iterations, relative residual of the last solve
 
 Solver& solver() {
@@ -216,9 +217,26 @@ void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
   ck(cudaEventRecord(r.ev[6], r.stream), "event");
   if (s.precision == BGPU_MIXED && s.mixed) {
     MixedReport rep{};
-    s.mixed->solve(nrhs, d_b, ldb, r.stream, &rep);
-    g_solve_info[0] = rep.iterations;
-    g_solve_info[1] = rep.relres;
+    // keep the right-hand sides: a failed refinement falls back to the FP64 LU on the same input
+    s.rhs_keep.ensure((size_t)n3 * nrhs * sizeof(double), "right-hand sides (copy)");
+    ck(cudaMemcpy2DAsync(s.rhs_keep.p, (size_t)n3 * sizeof(double), d_b, (size_t)ldb * sizeof(double),
+                         (size_t)n3 * sizeof(double), nrhs, cudaMemcpyDeviceToDevice, r.stream),
+       "rhs copy");
+    try {
+      s.mixed->solve(nrhs, d_b, ldb, r.stream, &rep);
+      g_solve_info[0] = rep.iterations;
+      g_solve_info[1] = rep.relres;
+    } catch (const MixedFailure& e) {
+      say("mixed precision: %s; factoring the FP64 matrix instead", e.what());
+      ck(cudaMemcpy2DAsync(d_b, (size_t)ldb * sizeof(double), s.rhs_keep.p, (size_t)n3 * sizeof(double),
+                           (size_t)n3 * sizeof(double), nrhs, cudaMemcpyDeviceToDevice, r.stream),
+         "rhs restore");
+      factor64(s, r);
+      r.check_status("FP64 fallback");
+      s.precision = BGPU_FP64;
+      solve_device(s, r, nrhs, d_b, ldb);
+      return;
+    }
   } else {
     r.ensure_trsv(n3);
     for (int c = 0; c < nrhs; c += 16) {
@@ -383,7 +401,14 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
     ck(cudaEventRecord(r.ev[2], r.stream), "event");
     if (s.precision == BGPU_MIXED) {
       if (!s.mixed) s.mixed = std::make_unique<MixedSolver>();
-      s.mixed->build(s.mesh(), defl, s.gr.as<double>(), s.ld, eps, r.stream, r.ev[3], r.ev[4]);
+      s.mixed->set_refinement(g_refine[0], g_refine[1]);
+      try {
+        s.mixed->build(s.mesh(), defl, s.gr.as<double>(), s.ld, eps, r.stream, r.ev[3], r.ev[4]);
+      } catch (const MixedFailure& e) {
+        say("mixed precision: %s; factoring the FP64 matrix instead", e.what());
+        s.precision = BGPU_FP64;
+        factor64(s, r);
+      }
       ck(cudaEventRecord(r.ev[5], r.stream), "event");
       r.check_status("bhm_build");
     } else {
@@ -461,6 +486,17 @@ int bgpu_set_precision(int mode) {
 }
 
 int bgpu_precision(void) { return g ? g->precision : -1; }
+
+int bgpu_set_refinement(int max_restarts, int krylov) {
+  if (max_restarts < 0 || krylov < 1 || krylov > 16) {
+    say("error: bgpu_set_refinement: restarts >= 0 and 1 <= krylov <= 16");
+    return 1;
+  }
+  g_refine[0] = max_restarts;
+  g_refine[1] = krylov;
+  if (g && g->mixed) g->mixed->set_refinement(max_restarts, krylov);
+  return 0;
+}
 
 int bgpu_timings(double* ms, int len) {
   if (!g_rt) return 0;
@@ -558,6 +594,26 @@ int bgpu_kernel_stats(int kernel, int enable, int* launches, double* ms, double*
     if (ms) *ms = t;
     if (work) *work = w;
     lu_gemm_timer_enable(enable != 0);
+    return 0;
+  });
+}
+
+int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float* d_a, int lda, const float* d_b, int ldb, float* d_c,
+                                int ldc) {
+  return guarded([&] {
+    Runtime& r = rt();
+    if (m <= 0 || n <= 0 || k <= 0) return 0;
+    const long lt = ((long)k + 63) / 64 * 64;
+    DevBuf at, bt;
+    at.ensure((size_t)m * lt * 2, "BF16 A");
+    bt.ensure((size_t)n * lt * 2, "BF16 B");
+    ck(cudaEventRecord(r.ev[6], r.stream), "event");
+    ck(cast_transpose_bf16(d_a, lda, m, k, at.p, lt, r.stream), "cast A");
+    ck(cast_bf16(d_b, ldb, k, n, bt.p, lt, r.stream), "cast B");
+    ck(gemm_bf16_tc_minus(m, n, k, at.p, lt, bt.p, lt, d_c, ldc, r.status.as<int>(), r.stream), "tensor-core GEMM");
+    ck(cudaEventRecord(r.ev[7], r.stream), "event");
+    r.check_status("tensor-core GEMM");
+    r.ms[3] = r.elapsed(6, 7);
     return 0;
   });
 }

@@ -85,7 +85,20 @@ size_t trsv_scratch_bytes(int n);
 // X (n x nrhs, ldx) := A^{-1} X given the LU factors and perm, dgetrs('N') semantics.
 cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* X, long ldx, int nrhs, void* scratch,
                     int* d_status, cudaStream_t s);
+// Y := U^-1 L^-1 Y with FP32 factors of an unpivoted LU, FP64 right-hand sides (in place).
+cudaError_t trsv_lu32(const float* LU, long lda, int n, double* Y, long ldy, int nrhs, void* scratch, int* d_status,
+                      cudaStream_t s);
 // Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s);
+
+// tc_gemm.cu ---------------------------------------------------------------------------------
+// BF16 operand copies for the tensor-core GEMM: At (m x k row-major) from A (m x k column-major
+// FP32), Bt (k x n column-major) from B (k x n column-major FP32).
+cudaError_t cast_transpose_bf16(const float* A, long lda, int m, int k, void* At, long lda_t, cudaStream_t s);
+cudaError_t cast_bf16(const float* B, long ldb, int k, int n, void* Bt, long ldb_t, cudaStream_t s);
+// C (FP32, column-major) -= A B with A given as At (m x k row-major BF16) and B as Bt (k x n
+// column-major BF16); tcgen05 kind::f16, FP32 accumulation in TMEM.
+cudaError_t gemm_bf16_tc_minus(int m, int n, int k, const void* At, long lda_t, const void* Bt, long ldb_t, float* C,
+                               long ldc, int* d_status, cudaStream_t s);
 
 }  // namespace bgpu

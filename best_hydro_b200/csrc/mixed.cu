@@ -1,21 +1,559 @@
-// Mixed-precision LU + FP64 refinement: placeholder until the tensor-core factorisation lands.
+// Mixed-precision factorisation of BEST's GR and the refined solve (BF16 tensor cores + FP64
+// GMRES iterative refinement).
+//
+// What it replaces: LAPACK dgetrf/dgetrs in FP64 (best/best.f:444, best/besolve.f90:133), or the
+// H-matrix solver's GMRES behind bhm_build/bhm_solve (hmatrix/src/api.cpp:694-771), whose outer
+// loop (several right-hand sides in lockstep, true residual at each restart) this follows.
+//
+// Factorisation: GR is assembled once in FP64 (kept for the residuals) with an FP32 copy written by
+// the same kernel; the copy is factored without pivoting (as the reference's H-LU factors GR,
+// hmatrix/src/hmatrix.cpp:1007) by recursive halving:
+//     LU(D) = [L11 0; L21 L22][U11 U12; 0 U22]:  LU(D11); U12 = L11^-1 D12; L21 = D21 U11^-1;
+//     D22 -= L21 U12; LU(D22)
+// with 128 x 128 diagonal leaves factored in one CTA, triangular solves recursive down to 128-wide
+// leaves, and every update C -= A B on the tcgen05 GEMM (BF16 operands, FP32 accumulation).
+// Deflation keeps GR far from singular (1-norm condition ~1e3 on the synthetic meshes), so BF16
+// updates are recovered by refinement in a few steps.
+//
+// Solve: restarted right-preconditioned GMRES in FP64 (preconditioner: the FP32 factors, applied
+// with FP64 accumulation), the true FP64 residual b - GR x at every restart; all right-hand sides
+// advance in lockstep.  Stops at a relative residual of tol for every column; a failure to converge
+// or a zero pivot is an error (the C ABI then factors the kept FP64 matrix instead).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
 #include <stdexcept>
+#include <string>
+#include <vector>
 
 #include "mixed.h"
 
 namespace bgpu {
+namespace {
 
-struct MixedSolver::Impl {};
-
-MixedSolver::MixedSolver() : p_(new Impl) {}
-MixedSolver::~MixedSolver() { delete p_; }
-const char* MixedSolver::name() const { return "mixed"; }
-void MixedSolver::build(const DevMesh&, const DevDeflation&, double*, long, double, cudaStream_t, cudaEvent_t,
-                        cudaEvent_t) {
-  throw std::runtime_error("the mixed-precision factorisation is not available in this build (use fp64)");
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
-void MixedSolver::solve(int, double*, long, cudaStream_t, MixedReport*) {
-  throw std::runtime_error("the mixed-precision solve is not available in this build");
+
+struct Buf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  Buf() = default;
+  Buf(const Buf&) = delete;
+  Buf& operator=(const Buf&) = delete;
+  ~Buf() {
+    if (p) cudaFree(p);
+  }
+  void ensure(size_t need, const char* what) {
+    if (p && bytes >= need) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMalloc(&p, need) != cudaSuccess) {
+      cudaGetLastError();
+      throw std::runtime_error(std::string("cannot allocate ") + what + " (" + std::to_string(need / 1e9) + " GB)");
+    }
+    bytes = need;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+constexpr int kLeaf = 128;
+constexpr int kZeroPivot = 4;  // status: a pivot of the unpivoted FP32 LU is zero or not finite
+
+long round_up(long v, long q) { return (v + q - 1) / q * q; }
+
+// ---- diagonal leaf: h x h (h <= 128) LU without pivoting, in shared memory -----------------
+__global__ void __launch_bounds__(512) k_lu32_leaf(float* __restrict__ A, long lda, int h, int* status) {
+  extern __shared__ float d[];  // column-major, leading dimension h + 1
+  const int ldd = h + 1, tid = threadIdx.x, nt = blockDim.x;
+  __shared__ int s_bad;
+  for (int i = tid; i < h * h; i += nt) {
+    const int r = i % h, c = i / h;
+    d[c * ldd + r] = A[(size_t)c * lda + r];
+  }
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int k = 0; k < h; ++k) {
+    const float p = d[k * ldd + k];
+    if (tid == 0 && !(p != 0.f && isfinite(p))) s_bad = 1;
+    const float rp = 1.0f / p;
+    for (int r = k + 1 + tid; r < h; r += nt) d[k * ldd + r] *= rp;
+    __syncthreads();
+    const int w = h - k - 1;
+    for (int i = tid; i < w * w; i += nt) {
+      const int r = k + 1 + i % w, c = k + 1 + i / w;
+      d[c * ldd + r] -= d[k * ldd + r] * d[c * ldd + k];
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < h * h; i += nt) {
+    const int r = i % h, c = i / h;
+    A[(size_t)c * lda + r] = d[c * ldd + r];
+  }
+  if (tid == 0 && s_bad) atomicExch(status, kZeroPivot);
+}
+
+// ---- triangular-solve leaves (h <= 128) ----------------------------------------------------
+// B (h x w, ldb) := L^-1 B, L unit lower (h x h, lda); one CTA per 64 columns.
+__global__ void __launch_bounds__(256) k_trsm_llu_leaf(const float* __restrict__ L, long lda, int h, float* B, long ldb,
+                                                        int w) {
+  extern __shared__ float sm[];
+  float* l = sm;                 // [h][h+1] column-major
+  float* b = sm + h * (h + 1);   // [64][h+1]: column c of the strip at b[c*(h+1)]
+  const int ldl = h + 1, tid = threadIdx.x, nt = blockDim.x;
+  const int c0 = blockIdx.x * 64, nc = min(64, w - c0);
+  for (int i = tid; i < h * h; i += nt) {
+    const int r = i % h, c = i / h;
+    l[c * ldl + r] = L[(size_t)c * lda + r];
+  }
+  for (int i = tid; i < h * nc; i += nt) {
+    const int r = i % h, c = i / h;
+    b[c * ldl + r] = B[(size_t)(c0 + c) * ldb + r];
+  }
+  __syncthreads();
+  for (int k = 0; k < h - 1; ++k) {
+    const int rows = h - k - 1;
+    for (int i = tid; i < rows * nc; i += nt) {
+      const int r = k + 1 + i % rows, c = i / rows;
+      b[c * ldl + r] -= l[k * ldl + r] * b[c * ldl + k];
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < h * nc; i += nt) {
+    const int r = i % h, c = i / h;
+    B[(size_t)(c0 + c) * ldb + r] = b[c * ldl + r];
+  }
+}
+
+// B (m x h, ldb) := B U^-1, U upper (h x h, lda); one CTA per 64 rows.
+__global__ void __launch_bounds__(256) k_trsm_ru_leaf(const float* __restrict__ U, long lda, int h, float* B, long ldb,
+                                                       int m) {
+  extern __shared__ float sm[];
+  float* u = sm;                 // [h][h+1] column-major
+  float* b = sm + h * (h + 1);   // [h][65]: column j of the strip at b[j*65]
+  const int ldu = h + 1, tid = threadIdx.x, nt = blockDim.x;
+  const int r0 = blockIdx.x * 64, nr = min(64, m - r0);
+  for (int i = tid; i < h * h; i += nt) {
+    const int r = i % h, c = i / h;
+    u[c * ldu + r] = U[(size_t)c * lda + r];
+  }
+  for (int i = tid; i < nr * h; i += nt) {
+    const int r = i % nr, c = i / nr;
+    b[c * 65 + r] = B[(size_t)c * ldb + r0 + r];
+  }
+  __syncthreads();
+  for (int j = 0; j < h; ++j) {
+    const float rp = 1.0f / u[j * ldu + j];
+    for (int r = tid; r < nr; r += nt) b[j * 65 + r] *= rp;
+    __syncthreads();
+    const int cols = h - j - 1;
+    for (int i = tid; i < nr * cols; i += nt) {
+      const int r = i % nr, c = j + 1 + i / nr;
+      b[c * 65 + r] -= b[j * 65 + r] * u[c * ldu + j];
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < nr * h; i += nt) {
+    const int r = i % nr, c = i / nr;
+    B[(size_t)c * ldb + r0 + r] = b[c * 65 + r];
+  }
+}
+
+// ---- FP64 mat-vec for the residuals: Y = beta Y + alpha A X (q <= Q columns) ----------------
+template <int Q>
+__global__ void __launch_bounds__(128) k_matvec64_part(const double* __restrict__ A, long lda, int n,
+                                                       const double* __restrict__ X, long ldx, int q, int cols_per,
+                                                       double* __restrict__ P) {
+  const int row = blockIdx.x * 128 + threadIdx.x, split = blockIdx.y;
+  const int c0 = split * cols_per, c1 = min(n, c0 + cols_per);
+  double acc[Q];
+#pragma unroll
+  for (int j = 0; j < Q; ++j) acc[j] = 0.0;
+  if (row < n) {
+    const double* a = A + row;
+#pragma unroll 4
+    for (int c = c0; c < c1; ++c) {
+      const double v = a[(size_t)c * lda];
+#pragma unroll
+      for (int j = 0; j < Q; ++j)
+        if (j < q) acc[j] += v * __ldg(&X[(size_t)j * ldx + c]);
+    }
+#pragma unroll
+    for (int j = 0; j < Q; ++j)
+      if (j < q) P[((size_t)split * Q + j) * n + row] = acc[j];
+  }
+}
+
+template <int Q>
+__global__ void k_matvec64_reduce(const double* __restrict__ P, int n, int q, int splits, double alpha, double beta,
+                                  double* Y, long ldy) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  for (int j = 0; j < q; ++j) {
+    double s = 0.0;
+    for (int t = 0; t < splits; ++t) s += P[((size_t)t * Q + j) * n + row];
+    double* y = Y + (size_t)j * ldy + row;
+    *y = (beta == 0.0 ? 0.0 : beta * *y) + alpha * s;
+  }
+}
+
+// ---- small vector kernels for GMRES (all blocks of q columns, column c at c * n) ------------
+// out[i * q + c] partial sums over a chunk of rows of V_i[c] . W[c], i < nv
+__global__ void k_dots(const double* __restrict__ V, int nv, const double* __restrict__ W, int n, int q,
+                       double* __restrict__ part) {
+  const int i = blockIdx.y;
+  __shared__ double red[16][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double acc[16];
+  for (int c = 0; c < 16; ++c) acc[c] = 0.0;
+  const double* v = V + (size_t)i * q * n;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int c = 0; c < q; ++c) acc[c] += v[(size_t)c * n + r] * W[(size_t)c * n + r];
+  for (int c = 0; c < q; ++c) {
+    double x = acc[c];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[c][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < q) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+    part[((size_t)blockIdx.x * nv + i) * q + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_dots_reduce(const double* __restrict__ part, int nparts, int count, double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  double s = 0.0;
+  for (int p = 0; p < nparts; ++p) s += part[(size_t)p * count + t];
+  out[t] = s;
+}
+
+// W[c] += sign * sum_i V_i[c] coef[i * q + c]
+__global__ void k_combine(const double* __restrict__ V, int nv, const double* __restrict__ coef, double sign, double* W,
+                          int n, int q) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int c = 0; c < q; ++c) {
+      double s = 0.0;
+      for (int i = 0; i < nv; ++i) s += V[((size_t)i * q + c) * n + r] * coef[i * q + c];
+      W[(size_t)c * n + r] += sign * s;
+    }
+}
+
+// Y[c] = X[c] * scale[c]
+__global__ void k_scale_cols(const double* __restrict__ X, const double* __restrict__ scale, double* Y, int n, int q) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int c = 0; c < q; ++c) Y[(size_t)c * n + r] = X[(size_t)c * n + r] * scale[c];
+}
+
+__global__ void k_copy_in(const double* __restrict__ B, long ldb, int n, int q, double* Y) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int c = 0; c < q; ++c) Y[(size_t)c * n + r] = B[(size_t)c * ldb + r];
+}
+__global__ void k_copy_out(const double* __restrict__ Y, int n, int q, double* B, long ldb) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int c = 0; c < q; ++c) B[(size_t)c * ldb + r] = Y[(size_t)c * n + r];
+}
+
+}  // namespace
+
+struct MixedSolver::Impl {
+  int n3 = 0;
+  long ld32 = 0;
+  double* gr64 = nullptr;  // the FP64 matrix (owned by the caller)
+  long ld64 = 0;
+  double tol = 1e-12;
+  int max_restarts = 8, krylov = 10;
+  int sms = 148;
+  Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs;
+  int* d_status() { return status.as<int>(); }
+
+  // C (m x n at c, ldc) -= A (m x k, col-major fp32) B (k x n col-major fp32) via BF16 tensor cores
+  void gemm(int m, int n, int k, const float* A, long lda, const float* B, long ldb, float* C, long ldc,
+            cudaStream_t s) {
+    if (m <= 0 || n <= 0 || k <= 0) return;
+    const long lat = round_up(k, 64), lbt = round_up(k, 64);
+    ck(cast_transpose_bf16(A, lda, m, k, at.p, lat, s), "cast A");
+    ck(cast_bf16(B, ldb, k, n, bt.p, lbt, s), "cast B");
+    ck(gemm_bf16_tc_minus(m, n, k, at.p, lat, bt.p, lbt, C, ldc, d_status(), s), "tensor-core GEMM");
+  }
+
+  static int split(int sz) {
+    int h = (sz / 2) / kLeaf * kLeaf;
+    return std::max(h, kLeaf);
+  }
+
+  // B (h x w at b) := L^-1 B, L unit lower at l (h x h); leading dimension ld32
+  void trsm_llu(const float* l, int h, float* b, int w, cudaStream_t s) {
+    if (h <= 0 || w <= 0) return;
+    if (h <= kLeaf) {
+      const size_t smem = (size_t)(h * (h + 1) + 64 * (h + 1)) * sizeof(float);
+      k_trsm_llu_leaf<<<(w + 63) / 64, 256, smem, s>>>(l, ld32, h, b, ld32, w);
+      BGPU_COUNT_LAUNCH();
+      ck(cudaGetLastError(), "trsm leaf");
+      return;
+    }
+    const int h1 = split(h);
+    trsm_llu(l, h1, b, w, s);
+    gemm(h - h1, w, h1, l + h1, ld32, b, ld32, b + h1, ld32, s);
+    trsm_llu(l + h1 + (size_t)h1 * ld32, h - h1, b + h1, w, s);
+  }
+
+  // B (m x h at b) := B U^-1, U upper at u (h x h)
+  void trsm_ru(const float* u, int h, float* b, int m, cudaStream_t s) {
+    if (h <= 0 || m <= 0) return;
+    if (h <= kLeaf) {
+      const size_t smem = (size_t)(h * (h + 1) + h * 65) * sizeof(float);
+      k_trsm_ru_leaf<<<(m + 63) / 64, 256, smem, s>>>(u, ld32, h, b, ld32, m);
+      BGPU_COUNT_LAUNCH();
+      ck(cudaGetLastError(), "trsm leaf");
+      return;
+    }
+    const int h1 = split(h);
+    trsm_ru(u, h1, b, m, s);
+    gemm(m, h - h1, h1, b, ld32, u + (size_t)h1 * ld32, ld32, b + (size_t)h1 * ld32, ld32, s);
+    trsm_ru(u + h1 + (size_t)h1 * ld32, h - h1, b + (size_t)h1 * ld32, m, s);
+  }
+
+  // factors the square block at (k0, k0) of size sz in place
+  void rlu(int k0, int sz, cudaStream_t s) {
+    float* A = lu32.as<float>();
+    float* D = A + k0 + (size_t)k0 * ld32;
+    if (sz <= kLeaf) {
+      const size_t smem = (size_t)sz * (sz + 1) * sizeof(float);
+      k_lu32_leaf<<<1, 512, smem, s>>>(D, ld32, sz, d_status());
+      BGPU_COUNT_LAUNCH();
+      ck(cudaGetLastError(), "LU leaf");
+      return;
+    }
+    const int h = split(sz), r = sz - h;
+    rlu(k0, h, s);
+    trsm_llu(D, h, D + (size_t)h * ld32, r, s);          // U12
+    trsm_ru(D, h, D + h, r, s);                          // L21
+    gemm(r, r, h, D + h, ld32, D + (size_t)h * ld32, ld32, D + h + (size_t)h * ld32, ld32, s);
+    rlu(k0 + h, r, s);
+  }
+
+  // Y (n3 x q, ldy) = beta Y + alpha GR X
+  void matvec(const double* X, long ldx, int q, double* Y, long ldy, double alpha, double beta, cudaStream_t s) {
+    const int rb = (n3 + 127) / 128;
+    const int splits = std::max(1, std::min(32, (4 * sms * 8 + rb - 1) / rb));
+    const int per = (n3 + splits - 1) / splits;
+    part.ensure((size_t)splits * 16 * n3 * sizeof(double), "residual partials");
+    if (q <= 8) {
+      k_matvec64_part<8><<<dim3(rb, splits), 128, 0, s>>>(gr64, ld64, n3, X, ldx, q, per, part.as<double>());
+      BGPU_COUNT_LAUNCH();
+      k_matvec64_reduce<8><<<(n3 + 255) / 256, 256, 0, s>>>(part.as<double>(), n3, q, splits, alpha, beta, Y, ldy);
+    } else {
+      k_matvec64_part<16><<<dim3(rb, splits), 128, 0, s>>>(gr64, ld64, n3, X, ldx, q, per, part.as<double>());
+      BGPU_COUNT_LAUNCH();
+      k_matvec64_reduce<16><<<(n3 + 255) / 256, 256, 0, s>>>(part.as<double>(), n3, q, splits, alpha, beta, Y, ldy);
+    }
+    BGPU_COUNT_LAUNCH();
+    ck(cudaGetLastError(), "FP64 residual");
+  }
+
+  // host copy of V_i[c] . W[c] for i < nv (nv x q values, row i)
+  std::vector<double> dot(const double* V, int nv, const double* W, int q, cudaStream_t s) {
+    const int blocks = std::min(4 * sms, (n3 + 255) / 256);
+    pdots.ensure((size_t)blocks * 32 * 16 * sizeof(double), "dot partials");  // nv <= 17
+    dots.ensure(32 * 16 * sizeof(double), "dots");
+    k_dots<<<dim3(blocks, nv), 256, 0, s>>>(V, nv, W, n3, q, pdots.as<double>());
+    BGPU_COUNT_LAUNCH();
+    k_dots_reduce<<<(nv * q + 127) / 128, 128, 0, s>>>(pdots.as<double>(), blocks, nv * q, dots.as<double>());
+    BGPU_COUNT_LAUNCH();
+    std::vector<double> h((size_t)nv * q);
+    ck(cudaMemcpyAsync(h.data(), dots.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "dot read");
+    ck(cudaStreamSynchronize(s), "dot sync");
+    return h;
+  }
+};
+
+MixedSolver::MixedSolver() : p_(new Impl) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&p_->sms, cudaDevAttrMultiProcessorCount, dev);
+  p_->status.ensure(256, "status");
+  ck(cudaMemset(p_->status.p, 0, 256), "status clear");
+}
+MixedSolver::~MixedSolver() { delete p_; }
+void MixedSolver::set_refinement(int max_restarts, int krylov) {
+  p_->max_restarts = std::max(0, max_restarts);
+  p_->krylov = std::min(16, std::max(1, krylov));
+}
+const char* MixedSolver::name() const { return "BF16 tensor-core (FP32 factors) + FP64 GMRES-IR"; }
+
+void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, long ld, double eps, cudaStream_t s,
+                        cudaEvent_t ev_assembled, cudaEvent_t ev_factored) {
+  Impl& P = *p_;
+  P.n3 = 3 * m.n;
+  P.ld32 = round_up(P.n3, 32);
+  P.gr64 = gr64;
+  P.ld64 = ld;
+  P.tol = std::max(1e-15, std::min(0.1 * eps, 1e-12));
+  P.lu32.ensure((size_t)P.ld32 * P.n3 * sizeof(float), "FP32 copy of GR");
+  const long half = P.n3 / 2 + 128;
+  P.at.ensure((size_t)half * round_up(half, 64) * 2, "BF16 operand A");
+  P.bt.ensure((size_t)half * round_up(half, 64) * 2, "BF16 operand B");
+  static bool attrs = false;
+  if (!attrs) {
+    const int big = 200 * 1024;
+    ck(cudaFuncSetAttribute(k_lu32_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_trsm_llu_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_trsm_ru_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    attrs = true;
+  }
+  ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
+  ck(launch_assemble(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
+  ck(cudaEventRecord(ev_assembled, s), "event");
+  P.rlu(0, P.n3, s);
+  ck(cudaEventRecord(ev_factored, s), "event");
+  int st = 0;
+  ck(cudaMemcpyAsync(&st, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
+  ck(cudaStreamSynchronize(s), "factorisation");
+  if (st != 0) {
+    ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
+    throw MixedFailure(st == kZeroPivot ? "the unpivoted FP32 factorisation met a zero or non-finite pivot"
+                                        : "a device-side wait ran out in the tensor-core factorisation");
+  }
+}
+
+void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedReport* rep) {
+  Impl& P = *p_;
+  const int n = P.n3;
+  const int m = P.krylov;           // Krylov vectors per restart
+  const int max_restarts = P.max_restarts;
+  int total_iters = 0;
+  double worst = 0.0;
+  P.trsv.ensure(trsv_scratch_bytes(n), "solve scratch");
+  for (int c0 = 0; c0 < nrhs; c0 += 16) {
+    const int q = std::min(16, nrhs - c0);
+    const size_t blk = (size_t)n * q;
+    // [B | X | R | W | V_0..V_m | Z_0..Z_{m-1}]
+    P.vecs.ensure(blk * (4 + (m + 1) + m) * sizeof(double), "GMRES vectors");
+    double* B = P.vecs.as<double>();
+    double* X = B + blk;
+    double* R = X + blk;
+    double* W = R + blk;
+    double* V = W + blk;
+    double* Z = V + (size_t)(m + 1) * blk;
+    const int grid = std::min(4 * P.sms, (n + 255) / 256);
+    k_copy_in<<<grid, 256, 0, s>>>(d_b + (size_t)c0 * ldb, ldb, n, q, B);
+    BGPU_COUNT_LAUNCH();
+    ck(cudaMemsetAsync(X, 0, blk * sizeof(double), s), "x clear");
+    std::vector<double> bn2 = P.dot(B, 1, B, q, s);
+    std::vector<double> bn(q);
+    for (int c = 0; c < q; ++c) bn[c] = std::sqrt(bn2[c]);
+    double rel = 1.0;
+    for (int restart = 0; restart <= max_restarts; ++restart) {
+      // R = B - GR X
+      ck(cudaMemcpyAsync(R, B, blk * sizeof(double), cudaMemcpyDeviceToDevice, s), "r copy");
+      if (restart > 0) P.matvec(X, n, q, R, n, -1.0, 1.0, s);
+      std::vector<double> rn2 = P.dot(R, 1, R, q, s);
+      std::vector<double> rn(q), inv(q);
+      rel = 0.0;
+      for (int c = 0; c < q; ++c) {
+        rn[c] = std::sqrt(rn2[c]);
+        const double r = bn[c] > 0 ? rn[c] / bn[c] : 0.0;
+        rel = std::max(rel, std::isnan(r) ? INFINITY : r);
+        inv[c] = rn[c] > 0 ? 1.0 / rn[c] : 0.0;
+      }
+      if (rel <= P.tol || restart == max_restarts) break;
+      ck(cudaMemcpyAsync(P.dots.p, inv.data(), q * sizeof(double), cudaMemcpyHostToDevice, s), "scale");
+      k_scale_cols<<<grid, 256, 0, s>>>(R, P.dots.as<double>(), V, n, q);
+      BGPU_COUNT_LAUNCH();
+      // Arnoldi with Givens rotations, per column
+      std::vector<std::vector<double>> H(q, std::vector<double>((size_t)(m + 1) * m, 0.0));
+      std::vector<std::vector<double>> cs(q, std::vector<double>(m)), sn(q, std::vector<double>(m));
+      std::vector<std::vector<double>> g(q, std::vector<double>(m + 1, 0.0));
+      for (int c = 0; c < q; ++c) g[c][0] = rn[c];
+      int jdone = 0;
+      std::vector<double> coef((size_t)(m + 1) * q);
+      for (int j = 0; j < m; ++j) {
+        double* Vj = V + (size_t)j * blk;
+        double* Zj = Z + (size_t)j * blk;
+        ck(cudaMemcpyAsync(Zj, Vj, blk * sizeof(double), cudaMemcpyDeviceToDevice, s), "z copy");
+        ck(trsv_lu32(P.lu32.as<float>(), P.ld32, n, Zj, n, q, P.trsv.p, P.d_status(), s), "preconditioner");
+        P.matvec(Zj, n, q, W, n, 1.0, 0.0, s);
+        // classical Gram-Schmidt, twice
+        std::vector<double> h = P.dot(V, j + 1, W, q, s);
+        ck(cudaMemcpyAsync(P.dots.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s), "coef");
+        k_combine<<<grid, 256, 0, s>>>(V, j + 1, P.dots.as<double>(), -1.0, W, n, q);
+        BGPU_COUNT_LAUNCH();
+        std::vector<double> h2 = P.dot(V, j + 1, W, q, s);
+        ck(cudaMemcpyAsync(P.dots.p, h2.data(), h2.size() * sizeof(double), cudaMemcpyHostToDevice, s), "coef");
+        k_combine<<<grid, 256, 0, s>>>(V, j + 1, P.dots.as<double>(), -1.0, W, n, q);
+        BGPU_COUNT_LAUNCH();
+        for (size_t t = 0; t < h.size(); ++t) h[t] += h2[t];
+        std::vector<double> wn2 = P.dot(W, 1, W, q, s);
+        std::vector<double> sc(q);
+        double est = 0.0;
+        for (int c = 0; c < q; ++c) {
+          const double hn = std::sqrt(wn2[c]);
+          sc[c] = hn > 0 ? 1.0 / hn : 0.0;
+          double* Hc = H[c].data();
+          for (int i = 0; i <= j; ++i) Hc[i * m + j] = h[(size_t)i * q + c];
+          Hc[(j + 1) * m + j] = hn;
+          for (int i = 0; i < j; ++i) {
+            const double a = Hc[i * m + j], b = Hc[(i + 1) * m + j];
+            Hc[i * m + j] = cs[c][i] * a + sn[c][i] * b;
+            Hc[(i + 1) * m + j] = -sn[c][i] * a + cs[c][i] * b;
+          }
+          const double a = Hc[j * m + j], b = Hc[(j + 1) * m + j];
+          const double rr = std::hypot(a, b);
+          cs[c][j] = rr > 0 ? a / rr : 1.0;
+          sn[c][j] = rr > 0 ? b / rr : 0.0;
+          Hc[j * m + j] = rr;
+          Hc[(j + 1) * m + j] = 0.0;
+          g[c][j + 1] = -sn[c][j] * g[c][j];
+          g[c][j] = cs[c][j] * g[c][j];
+          if (bn[c] > 0) est = std::max(est, std::fabs(g[c][j + 1]) / bn[c]);
+        }
+        ck(cudaMemcpyAsync(P.dots.p, sc.data(), q * sizeof(double), cudaMemcpyHostToDevice, s), "scale");
+        k_scale_cols<<<grid, 256, 0, s>>>(W, P.dots.as<double>(), V + (size_t)(j + 1) * blk, n, q);
+        BGPU_COUNT_LAUNCH();
+        ++total_iters;
+        jdone = j + 1;
+        if (est <= 0.5 * P.tol) break;
+      }
+      // y from the triangular H, then X += Z y
+      for (int c = 0; c < q; ++c) {
+        std::vector<double> y(jdone, 0.0);
+        for (int i = jdone - 1; i >= 0; --i) {
+          double v = g[c][i];
+          for (int k = i + 1; k < jdone; ++k) v -= H[c][i * m + k] * y[k];
+          y[i] = H[c][i * m + i] != 0 ? v / H[c][i * m + i] : 0.0;
+        }
+        for (int i = 0; i < jdone; ++i) coef[(size_t)i * q + c] = y[i];
+      }
+      ck(cudaMemcpyAsync(P.dots.p, coef.data(), (size_t)jdone * q * sizeof(double), cudaMemcpyHostToDevice, s),
+         "coef");
+      k_combine<<<grid, 256, 0, s>>>(Z, jdone, P.dots.as<double>(), 1.0, X, n, q);
+      BGPU_COUNT_LAUNCH();
+    }
+    int st = 0;
+    ck(cudaMemcpyAsync(&st, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
+    ck(cudaStreamSynchronize(s), "solve");
+    if (st != 0) {
+      ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
+      throw MixedFailure("a device-side wait ran out in the refined solve");
+    }
+    if (!(rel <= P.tol)) throw MixedFailure("GMRES refinement did not reach the requested residual");
+    k_copy_out<<<grid, 256, 0, s>>>(X, n, q, d_b + (size_t)c0 * ldb, ldb);
+    BGPU_COUNT_LAUNCH();
+    ck(cudaGetLastError(), "copy out");
+    worst = std::max(worst, rel);
+  }
+  if (rep) {
+    rep->iterations = total_iters;
+    rep->relres = worst;
+  }
 }
 
 }  // namespace bgpu

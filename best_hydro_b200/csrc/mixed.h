@@ -3,9 +3,17 @@
 
 #include <cuda_runtime.h>
 
+#include <stdexcept>
+
 #include "bgpu_internal.h"
 
 namespace bgpu {
+
+// The mixed path cannot deliver (zero pivot without pivoting, refinement not converging): the caller
+// falls back to the FP64 LU of the kept FP64 matrix.
+struct MixedFailure : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 struct MixedReport {
   int iterations = 0;   // refinement steps of the last solve
@@ -23,6 +31,8 @@ class MixedSolver {
   // records ev_assembled, factors the copy.  Throws on failure.
   void build(const DevMesh& m, const DevDeflation& d, double* gr64, long ld, double eps, cudaStream_t s,
              cudaEvent_t ev_assembled, cudaEvent_t ev_factored);
+  // GMRES restarts (each with a true FP64 residual) and Krylov vectors per restart.
+  void set_refinement(int max_restarts, int krylov);
   // Solves GR x = b in place (d_b: 3n x nrhs, ldb) to the relative residual of build's eps.
   void solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedReport* rep);
 

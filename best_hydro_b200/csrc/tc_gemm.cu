@@ -1,0 +1,329 @@
+// C(m x n, FP32) -= A(m x k) B(k x n) on the B200's 5th-generation tensor cores, BF16 operands with
+// FP32 accumulation: the trailing update and triangular-solve updates of the mixed-precision LU
+// (mixed.cu).  No counterpart in the reference, whose LU is LAPACK's dgetrf in FP64.
+//
+// Kernel (one 128 x 256 output tile per CTA, 192 threads, 197 KB of shared memory):
+//   warp 0, one thread   TMA producer: 128 x 64 tile of A and 256 x 64 tile of B per stage
+//                        (cp.async.bulk.tensor, 128-byte swizzle) into a 4-stage ring guarded by
+//                        full/empty mbarriers
+//   warp 1               allocates 256 TMEM columns; one thread issues tcgen05.mma kind::f16
+//                        (M 128, N 256, K 16; A and B K-major in shared memory) into the FP32
+//                        accumulator in TMEM and returns each stage with tcgen05.commit
+//   warps 2-5            epilogue: tcgen05.ld of the accumulator (each warp its 32-lane quarter),
+//                        C -= D in FP32, one row per thread (coalesced column stores)
+// Operands are BF16 copies in K-major layout (A row-major, B column-major), made by the cast
+// kernels below.  Tiles are ordered in groups of 16 row-tiles so that the CTAs resident together
+// share A and B slices in L2.  Every mbarrier wait is bounded: on expiry the thread records a status
+// and stops issuing work; all roles still reach the teardown, which frees TMEM.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "bgpu_internal.h"
+
+namespace bgpu {
+namespace {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int kThreads = 192;
+constexpr uint32_t kStageA = BM * BK * 2;  // 16 KB
+constexpr uint32_t kStageB = BN * BK * 2;  // 32 KB
+constexpr uint32_t kSmem = STAGES * (kStageA + kStageB) + 1024 + 256;
+constexpr uint32_t kTmemCols = 256;
+constexpr int kGroupM = 16;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // a wait gives up after 2 s
+
+// instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
+// both K-major (bits 15, 16 = 0), N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Bounded wait; false (status recorded) when it runs out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    for (int i = 0; i < 256; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kWaitNs) break;
+  }
+  atomicExch(status, (int)kWaitTimeout);
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)tm), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle; rows of 128 B, 8-row groups 1024 B
+// apart (stride byte offset), version 1 (bits 46-47), layout 2 = SWIZZLE_128B (bits 61-63).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)2 << 61);
+}
+// D (TMEM) (+)= A B; no output lane disabled.
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%"
+      "21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int m, int n,
+                   int k, float* __restrict__ C, long ldc, int tiles_m, int tiles_n, int* status) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + STAGES * kStageA;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * kStageB);
+  uint64_t* empty = full + STAGES;
+  uint64_t* accum = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+  __shared__ int s_abort;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // grouped tile order: groups of kGroupM row-tiles sweep all column tiles
+  const int tile = blockIdx.x;
+  const int per_group = kGroupM * tiles_n;
+  const int group = tile / per_group;
+  const int first_m = group * kGroupM;
+  const int group_m = min(tiles_m - first_m, kGroupM);
+  const int tm = first_m + (tile % per_group) % group_m;
+  const int tn = (tile % per_group) / group_m;
+  const int m0 = tm * BM, n0 = tn * BN;
+  const int ktiles = (k + BK - 1) / BK;
+
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kt = 0; kt < ktiles; ++kt) {
+        const int s = kt % STAGES;
+        if (kt >= STAGES && !mbar_wait(&empty[s], ((kt / STAGES) & 1) ^ 1, status)) {
+          s_abort = 1;
+          break;
+        }
+        if (*(volatile int*)&s_abort) break;
+        mbar_expect_tx(&full[s], kStageA + kStageB);
+        tma_load_2d(sA + s * kStageA, &tmA, kt * BK, m0, &full[s]);
+        tma_load_2d(sB + s * kStageB, &tmB, kt * BK, n0, &full[s]);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      bool ok = true;
+      for (int kt = 0; kt < ktiles; ++kt) {
+        const int s = kt % STAGES;
+        if (!mbar_wait(&full[s], (kt / STAGES) & 1, status)) {
+          s_abort = 1;
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk)
+          mma_bf16(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
+        mma_commit(&empty[s]);
+      }
+      (void)ok;
+      mma_commit(accum);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 = tile rows
+    const int q = warp & 3;
+    const bool ok = mbar_wait(accum, 0, status) && !*(volatile int*)&s_abort;
+    tc_fence_after();
+    if (ok) {
+      const int row = m0 + q * 32 + lane;
+#pragma unroll 1
+      for (int c = 0; c < BN / 32; ++c) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 32), v);
+        if (row < m) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = n0 + c * 32 + j;
+            if (col < n) {
+              float* p = C + (size_t)col * ldc + row;
+              *p = *p - v[j];
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// BF16 operand copies
+// ------------------------------------------------------------------------------------------
+// At (m x k row-major, lda_t) = bf16(A), A m x k column-major FP32 (lda): transposed through a
+// 32 x 32 shared tile so both sides are coalesced.
+__global__ void k_cast_transpose_bf16(const float* __restrict__ A, long lda, int m, int k, __nv_bfloat16* __restrict__ At,
+                                      long lda_t) {
+  __shared__ float t[32][33];
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int kk = k0 + r, i = i0 + threadIdx.x;
+    t[r][threadIdx.x] = (kk < k && i < m) ? A[(size_t)kk * lda + i] : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, kk = k0 + threadIdx.x;
+    if (i < m && kk < k) At[(size_t)i * lda_t + kk] = __float2bfloat16_rn(t[threadIdx.x][r]);
+  }
+}
+
+// Bt (k x n column-major, ldb_t) = bf16(B), B k x n column-major FP32 (ldb); 32 x 32 tiles.
+__global__ void k_cast_bf16(const float* __restrict__ B, long ldb, int k, int n, __nv_bfloat16* __restrict__ Bt,
+                            long ldb_t) {
+  const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const int kk = k0 + threadIdx.x;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r;
+    if (kk < k && j < n) Bt[(size_t)j * ldb_t + kk] = __float2bfloat16_rn(B[(size_t)j * ldb + kk]);
+  }
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+// 2-D BF16 tensor map: `rows` rows of `cols` elements (row pitch ld elements), box 64 x box_rows,
+// 128-byte swizzle, zero fill outside.
+bool make_map(CUtensorMap* tm, const void* base, int rows, int cols, long ld, int box_rows) {
+  EncodeTiled fn = encoder();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+cudaError_t cast_transpose_bf16(const float* A, long lda, int m, int k, void* At, long lda_t, cudaStream_t s) {
+  if (m <= 0 || k <= 0) return cudaSuccess;
+  dim3 grid((m + 31) / 32, (k + 31) / 32);
+  k_cast_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(A, lda, m, k, static_cast<__nv_bfloat16*>(At), lda_t);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t cast_bf16(const float* B, long ldb, int k, int n, void* Bt, long ldb_t, cudaStream_t s) {
+  if (k <= 0 || n <= 0) return cudaSuccess;
+  dim3 grid((k + 31) / 32, (n + 31) / 32);
+  k_cast_bf16<<<grid, dim3(32, 8), 0, s>>>(B, ldb, k, n, static_cast<__nv_bfloat16*>(Bt), ldb_t);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// C (m x n FP32, ldc) -= At^T-major A (m x k, row-major BF16, lda_t) * B (k x n column-major BF16,
+// ldb_t).  lda_t and ldb_t: multiples of 8 elements; At and Bt 16-byte aligned.
+cudaError_t gemm_bf16_tc_minus(int m, int n, int k, const void* At, long lda_t, const void* Bt, long ldb_t, float* C,
+                               long ldc, int* d_status, cudaStream_t s) {
+  if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  if ((lda_t % 8) || (ldb_t % 8) || ((uintptr_t)At & 15) || ((uintptr_t)Bt & 15)) return cudaErrorInvalidValue;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, At, m, k, lda_t, BM) || !make_map(&tb, Bt, n, k, ldb_t, BN)) return cudaErrorInvalidValue;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  k_gemm_bf16_tc<<<tiles_m * tiles_n, kThreads, kSmem, s>>>(ta, tb, m, n, k, C, ldc, tiles_m, tiles_n, d_status);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+}  // namespace bgpu

@@ -27,6 +27,11 @@ int bgpu_set_precision(int mode);
 /* The precision of the last bhm_build. */
 int bgpu_precision(void);
 
+/* Refinement of the mixed path: at most max_restarts GMRES restarts (each starting from the true
+ * FP64 residual) of krylov <= 16 vectors; defaults 8 and 10.  When the refinement does not reach its
+ * tolerance, bhm_solve factors the kept FP64 matrix on the GPU and solves with it instead (logged). */
+int bgpu_set_refinement(int max_restarts, int krylov);
+
 /* Stage times of the last calls in milliseconds, measured with CUDA events on the library's
  * stream: ms[0] self blocks + incenters (bhm_create), ms[1] assembly + deflation, ms[2] LU,
  * ms[3] solve (last bhm_solve or bgpu_solve_device), ms[4] bhm_build total, ms[5] refinement
@@ -67,6 +72,11 @@ int bgpu_dgetrs_noalloc(int n, int nrhs, const double *d_a, int lda, const int *
 /* C(m x n) -= A(m x k) B(k x n), FP64, column-major device matrices: the LU's trailing update. */
 int bgpu_dgemm_minus_device(int m, int n, int k, const double *d_a, int lda, const double *d_b, int ldb,
                             double *d_c, int ldc);
+
+/* C(m x n) -= A(m x k) B(k x n) with A, B rounded to BF16 and FP32 accumulation on the tcgen05
+ * tensor cores (column-major FP32 device matrices): the mixed-precision LU's update. */
+int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float *d_a, int lda, const float *d_b, int ldb, float *d_c,
+                                int ldc);
 
 /* Assembles GR rows of triangles [r0, r1) x columns of triangles [c0, c1) of the mesh given to
  * bhm_create into d_out (column-major, ldo), before deflation (best/tgetgr.f:33-173). */

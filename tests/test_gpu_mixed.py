@@ -1,0 +1,110 @@
+"""GPU tests of the mixed-precision path: the tcgen05 BF16 GEMM against an FP64 product of the
+same BF16-rounded operands, and the refined solve (BF16 tensor-core LU + FP64 GMRES-IR) through
+BEST's seam against the oracle.  Bars: GEMM within 1e-6 of k max|A| max|B| (FP32 accumulation);
+D_t, D_r, D_tr, centres and CHI' within 1e-8 relative of the FP64 oracle (the metric's bar); golden
+results at their 2e-4; a refinement that cannot converge falls back to the FP64 LU on the GPU."""
+import numpy as np
+import pytest
+
+import best_hydro_b200 as bh
+from oracle import best as ob
+from best_hydro_b200 import BhmSolver, meshes
+from tests.helpers import expected_cases, golden_mesh, rel, run_gpu, value_for_label
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-8
+
+
+def _torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 256, 64), (300, 500, 70), (1000, 1000, 1000), (4096, 2048, 512),
+                                   (129, 257, 65), (2000, 64, 4000)])
+def test_tc_gemm_bf16(m, n, k):
+    torch = _torch()
+    g = torch.Generator().manual_seed(m + n + k)
+    A = torch.randn(k, m, generator=g, dtype=torch.float32)  # column-major m x k: A.T
+    B = torch.randn(n, k, generator=g, dtype=torch.float32)  # column-major k x n: B.T
+    C = torch.randn(n, m, generator=g, dtype=torch.float32)  # column-major m x n: C.T
+    dA, dB, dC = A.cuda(), B.cuda(), C.cuda()
+    torch.cuda.synchronize()
+    bh.gemm_bf16_minus_device(m, n, k, dA.data_ptr(), m, dB.data_ptr(), k, dC.data_ptr(), m)
+    got = dC.cpu().double().T
+    Ab = A.T.bfloat16().double()
+    Bb = B.T.bfloat16().double()
+    want = C.T.double() - Ab @ Bb
+    err = (got - want).abs().max().item() / (Ab.abs().max().item() * Bb.abs().max().item() * k)
+    assert err < 1e-6, err
+
+
+def compare(g, o, tol=TOL):
+    for key in ("Dtt", "Drr"):
+        assert rel(g["tensors"][key], o.tensors[key]) < tol, key
+    scale = np.sqrt(np.max(np.abs(o.tensors["Dtt"])) * np.max(np.abs(o.tensors["Drr"])))
+    assert np.max(np.abs(g["tensors"]["Dtr"] - o.tensors["Dtr"])) / scale < tol
+    size = np.sqrt(np.mean(o.x.reshape(3, -1) ** 2) * 3)
+    for key in ("urc", "udr"):
+        assert np.max(np.abs(g["tensors"][key] - o.tensors[key])) / size < tol
+    if o.chiprime is not None:
+        assert abs(g["chiprime"] / o.chiprime - 1) < tol
+
+
+@pytest.mark.parametrize("case", ["icosphere_1280", "ellipsoid_5120", "star_f16"])
+def test_mixed_solve_vs_oracle(case):
+    if case == "icosphere_1280":
+        (tri, ta, tv), iarea = meshes.icosphere(3, 20.0), 1
+    elif case == "ellipsoid_5120":
+        (tri, ta, tv), iarea = meshes.ellipsoid(16), 1
+    else:
+        (tri, ta, tv), iarea = meshes.star(16), 0
+    bh.set_precision(bh.BGPU_MIXED)
+    try:
+        solver = BhmSolver()
+        g = run_gpu(solver, tri, ta, iarea=iarea, direct=0, eps=1e-10, ivisco=1, truevol=tv)
+        logs = bh.log_lines()
+        t = bh.timings()
+        solver.destroy()
+    finally:
+        bh.set_precision(-1)
+    print(f"\n{case}: {t} | {' / '.join(l for l in logs if 'solve' in l or 'build' in l)}")
+    assert not any("instead" in l for l in logs), logs
+    assert 0 < t["refine_iters"] <= 40 and t["relres"] <= 1e-12
+    o = ob.best_run(tri, ta, tv, iarea=iarea, ivisco=1)
+    compare(g, o)
+
+
+def test_mixed_golden_2eu7():
+    c = expected_cases()["2eu7"]
+    tri, ta, tv = golden_mesh(c["mesh"])
+    bh.set_precision(bh.BGPU_MIXED)
+    try:
+        solver = BhmSolver()
+        g = run_gpu(solver, tri, ta, iarea=1, direct=0, eps=1e-10, ivisco=1, truevol=tv, wm=c["wm"])
+        solver.destroy()
+    finally:
+        bh.set_precision(-1)
+    for e in c["expected"]:
+        got = value_for_label(g["report"], e["label"])
+        assert abs(got - e["value"]) <= e["tol"] * abs(e["value"]), (e["label"], got)
+    compare(g, ob.best_run(tri, ta, tv, iarea=1, ivisco=1, wm=c["wm"]))
+
+
+def test_mixed_falls_back_to_fp64_when_refinement_cannot_converge():
+    """No restarts allowed: the refinement cannot reach its tolerance, so bhm_solve factors the kept
+    FP64 matrix on the GPU and returns the FP64 solution (a host-side failure, no GPU fault)."""
+    tri, ta, tv = meshes.icosphere(2, 20.0)
+    bh.set_precision(bh.BGPU_MIXED)
+    bh.set_refinement(0, 10)
+    try:
+        solver = BhmSolver()
+        g = run_gpu(solver, tri, ta, iarea=1, direct=0, eps=1e-10)
+        logs = bh.log_lines()
+        solver.destroy()
+    finally:
+        bh.set_precision(-1)
+        bh.set_refinement(8, 10)
+    assert any("factoring the FP64 matrix instead" in l for l in logs), logs
+    compare(g, ob.best_run(tri, ta, tv, iarea=1), tol=1e-10)
