@@ -162,7 +162,7 @@ struct Solver {
   DevBuf geo, xc, self9, diag;
   DevBuf gr;                   // GR / its LU factors (FP64), n x ld
   long ld = 0;
-  DevBuf ipiv, perm;
+  DevBuf ipiv, perm, dl64, du64;  // pivots, composed permutation, diagonal-block inverses
   DevBuf gdef, comp, xmu;
   DevBuf rhs, rhs_keep;        // right-hand sides (host-interface staging, and a kept copy)
   std::unique_ptr<MixedSolver> mixed;
@@ -209,6 +209,10 @@ void factor64(Solver& s, Runtime& r) {
   ck(lu64_getrf(s.gr.as<double>(), s.ld, n3, s.ipiv.as<int>(), r.info.as<int>(), r.status.as<int>(), ws, r.stream),
      "LU");
   ck(lu_perm_from_ipiv(s.ipiv.as<int>(), n3, s.perm.as<int>(), r.stream), "permutation");
+  s.dl64.ensure(diag_inverse_elems(n3) * sizeof(double), "diagonal-block inverses (L)");
+  s.du64.ensure(diag_inverse_elems(n3) * sizeof(double), "diagonal-block inverses (U)");
+  ck(diag_inverses64(s.gr.as<double>(), s.ld, n3, s.dl64.as<double>(), s.du64.as<double>(), r.stream),
+     "diagonal inverses");
 }
 
 void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
@@ -241,8 +245,8 @@ void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
     r.ensure_trsv(n3);
     for (int c = 0; c < nrhs; c += 16) {
       const int q = std::min(16, nrhs - c);
-      ck(getrs64(s.gr.as<double>(), s.ld, n3, s.perm.as<int>(), d_b + (size_t)c * ldb, ldb, q, r.trsv_scratch.p,
-                 r.status.as<int>(), r.stream),
+      ck(getrs64_inv(s.gr.as<double>(), s.ld, s.dl64.as<double>(), s.du64.as<double>(), n3, s.perm.as<int>(),
+                     d_b + (size_t)c * ldb, ldb, q, r.trsv_scratch.p, r.status.as<int>(), r.stream),
          "solve");
     }
     g_solve_info[0] = 0;
@@ -431,6 +435,8 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
       return 1;
     }
     s.factored = true;
+    if (s.mixed)
+      for (auto& line : s.mixed->profile_report()) say("%s", line.c_str());
     say("GPU build: %s LU of order %d, assembly %.1f ms, factorisation %.1f ms (%.1f TFLOP/s)",
         s.precision == BGPU_FP64 ? "FP64" : (s.mixed ? s.mixed->name() : "mixed"), n3, r.ms[1], r.ms[2],
         (2.0 / 3.0) * (double)n3 * n3 * n3 / (r.ms[2] * 1e-3) / 1e12);
@@ -449,6 +455,8 @@ int bhm_solve(int nrhs, double* b) {
     solve_device(s, r, nrhs, s.rhs.as<double>(), n3);
     ck(cudaMemcpyAsync(b, s.rhs.p, (size_t)n3 * nrhs * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "x copy");
     r.sync("bhm_solve");
+    if (s.precision == BGPU_MIXED && s.mixed)
+      for (auto& line : s.mixed->profile_report()) say("%s", line.c_str());
     if (s.precision == BGPU_MIXED && s.mixed)
       say("solve: %d right-hand sides, %d refinement steps, relative residual %.1e, %.2f ms", nrhs,
           (int)g_solve_info[0], g_solve_info[1], r.ms[3]);

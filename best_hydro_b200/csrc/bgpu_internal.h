@@ -88,6 +88,16 @@ cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* 
 // Y := U^-1 L^-1 Y with FP32 factors of an unpivoted LU, FP64 right-hand sides (in place).
 cudaError_t trsv_lu32(const float* LU, long lda, int n, double* Y, long ldy, int nrhs, void* scratch, int* d_status,
                       cudaStream_t s);
+// Inverses of the 128 x 128 diagonal blocks of LU factors (DL: unit-lower parts, DU: upper parts),
+// each diag_inverse_elems(n) elements; and the solves that use them.
+size_t diag_inverse_elems(int n);
+cudaError_t diag_inverses64(const double* LU, long lda, int n, double* DL, double* DU, cudaStream_t s);
+// (FP32: nb blocks starting at block b0)
+cudaError_t diag_inverses32(const float* LU, long lda, int n, int b0, int nb, float* DL, float* DU, cudaStream_t s);
+cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
+                        double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s);
+cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, double* Y, long ldy,
+                          int nrhs, void* scratch, int* d_status, cudaStream_t s);
 // Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s);
 
@@ -100,5 +110,13 @@ cudaError_t cast_bf16(const float* B, long ldb, int k, int n, void* Bt, long ldb
 // column-major BF16); tcgen05 kind::f16, FP32 accumulation in TMEM.
 cudaError_t gemm_bf16_tc_minus(int m, int n, int k, const void* At, long lda_t, const void* Bt, long ldb_t, float* C,
                                long ldc, int* d_status, cudaStream_t s);
+// Tensor maps (two opaque 128-byte CUtensorMap objects) over whole operand buffers, built once; and
+// the GEMM on them (A = leading m rows of the A buffer, B = leading n rows of the B buffer).
+constexpr int kTensorMapBytes = 128;
+cudaError_t tc_gemm_prepare();  // kernel attributes, once, before any capture
+bool tc_operand_maps(const void* At, int rows_a, long lda_t, const void* Bt, int rows_b, long ldb_t, void* map_a,
+                     void* map_b);
+cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, const void* map_b, float* C, long ldc,
+                                    int* d_status, cudaStream_t s);
 
 }  // namespace bgpu

@@ -10,8 +10,9 @@
 // hmatrix/src/hmatrix.cpp:1007) by recursive halving:
 //     LU(D) = [L11 0; L21 L22][U11 U12; 0 U22]:  LU(D11); U12 = L11^-1 D12; L21 = D21 U11^-1;
 //     D22 -= L21 U12; LU(D22)
-// with 128 x 128 diagonal leaves factored in one CTA, triangular solves recursive down to 128-wide
-// leaves, and every update C -= A B on the tcgen05 GEMM (BF16 operands, FP32 accumulation).
+// with 128 x 128 diagonal leaves factored in one CTA and inverted right away, triangular solves
+// recursive down to 128-wide leaves that multiply by those inverses (FP32), and every other update
+// C -= A B on the tcgen05 GEMM (BF16 operands, FP32 accumulation).
 // Deflation keeps GR far from singular (1-norm condition ~1e3 on the synthetic meshes), so BF16
 // updates are recovered by refinement in a few steps.
 //
@@ -23,6 +24,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -67,125 +71,208 @@ constexpr int kZeroPivot = 4;  // status: a pivot of the unpivoted FP32 LU is ze
 
 long round_up(long v, long q) { return (v + q - 1) / q * q; }
 
-// ---- diagonal leaf: h x h (h <= 128) LU without pivoting, in shared memory -----------------
-__global__ void __launch_bounds__(512) k_lu32_leaf(float* __restrict__ A, long lda, int h, int* status) {
-  extern __shared__ float d[];  // column-major, leading dimension h + 1
-  const int ldd = h + 1, tid = threadIdx.x, nt = blockDim.x;
+// ---- diagonal leaf: h x h (h <= 128) LU without pivoting and the inverses of both triangles ----
+// 512 threads.  Factorisation: threads as 32 (rows) x 16 (columns) over the trailing block, one
+// barrier per step; the multipliers (a_rk / a_kk) are formed on the fly and column k is scaled after
+// the barrier (nothing reads it again).  Inverses: four consecutive lanes per column c, the
+// substitution's sums split four ways and combined by shuffles; L^-1 (unit lower) and U^-1 are
+// written to DL, DU (128 x 128 column-major, zero outside the h x h block).
+constexpr int kLdS = 129;
+__global__ void __launch_bounds__(512) k_lu32_leaf_inv(float* __restrict__ A, long lda, int h, float* __restrict__ DL,
+                                                        float* __restrict__ DU, int* status) {
+  extern __shared__ float sm[];
+  float* d = sm;                    // d[c * kLdS + r] = A(r, c), then L\U
+  float* li = sm + 128 * kLdS;      // li[c * kLdS + i] = (L^-1)(i, c)
+  float* ui = li + 128 * kLdS;      // ui[c * kLdS + i] = (U^-1)(i, c)
   __shared__ int s_bad;
-  for (int i = tid; i < h * h; i += nt) {
-    const int r = i % h, c = i / h;
-    d[c * ldd + r] = A[(size_t)c * lda + r];
-  }
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  for (int c = ty; c < h; c += 16)
+    for (int r = tx; r < h; r += 32) d[c * kLdS + r] = A[(size_t)c * lda + r];
   if (tid == 0) s_bad = 0;
   __syncthreads();
   for (int k = 0; k < h; ++k) {
-    const float p = d[k * ldd + k];
+    const float p = d[k * kLdS + k];
     if (tid == 0 && !(p != 0.f && isfinite(p))) s_bad = 1;
     const float rp = 1.0f / p;
-    for (int r = k + 1 + tid; r < h; r += nt) d[k * ldd + r] *= rp;
-    __syncthreads();
-    const int w = h - k - 1;
-    for (int i = tid; i < w * w; i += nt) {
-      const int r = k + 1 + i % w, c = k + 1 + i / w;
-      d[c * ldd + r] -= d[k * ldd + r] * d[c * ldd + k];
+    for (int c = k + 1 + ty; c < h; c += 16) {
+      const float u = d[c * kLdS + k];
+      for (int r = k + 1 + tx; r < h; r += 32) d[c * kLdS + r] -= (d[k * kLdS + r] * rp) * u;
     }
     __syncthreads();
+    for (int r = k + 1 + tid; r < h; r += 512) d[k * kLdS + r] *= rp;
   }
-  for (int i = tid; i < h * h; i += nt) {
-    const int r = i % h, c = i / h;
-    A[(size_t)c * lda + r] = d[c * ldd + r];
+  // initial columns of the inverses
+  const int c = tid >> 2, q = tid & 3;
+  for (int i = q; i < 128; i += 4) {
+    li[c * kLdS + i] = (i == c && c < h) ? 1.f : 0.f;
+    ui[c * kLdS + i] = 0.f;
   }
+  __syncthreads();
+  if (c < h && q == 0) ui[c * kLdS + c] = 1.0f / d[c * kLdS + c];
+  __syncwarp();
+  const int lane = tid & 31;
+  const int cmin = (tid >> 5) * 8, cmax = min(cmin + 7, h - 1);
+  if (cmin < h) {
+    // L^-1: x_i = -sum_{j < i} L(i, j) x_j for i > c (x_j = 0 for j < c, x_c = 1)
+    for (int i = cmin + 1; i < h; ++i) {
+      float part = 0.f;
+      for (int j = cmin + q; j < i; j += 4) part += d[j * kLdS + i] * li[c * kLdS + j];
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      part += __shfl_xor_sync(0xffffffffu, part, 2);
+      if (q == 0 && c < h && i > c) li[c * kLdS + i] = -part;
+      __syncwarp();
+    }
+    // U^-1: x_i = -(sum_{j > i} U(i, j) x_j) / U(i, i) for i < c (x_j = 0 for j > c)
+    for (int i = cmax - 1; i >= 0; --i) {
+      float part = 0.f;
+      for (int j = i + 1 + q; j <= cmax; j += 4) part += d[j * kLdS + i] * ui[c * kLdS + j];
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      part += __shfl_xor_sync(0xffffffffu, part, 2);
+      if (q == 0 && c < h && i < c) ui[c * kLdS + i] = -part / d[i * kLdS + i];
+      __syncwarp();
+    }
+  }
+  (void)lane;
+  __syncthreads();
+  for (int cc = ty; cc < h; cc += 16)
+    for (int r = tx; r < h; r += 32) A[(size_t)cc * lda + r] = d[cc * kLdS + r];
+  for (int cc = ty; cc < 128; cc += 16)
+    for (int r = tx; r < 128; r += 32) {
+      DL[(size_t)cc * 128 + r] = li[cc * kLdS + r];
+      DU[(size_t)cc * 128 + r] = ui[cc * kLdS + r];
+    }
   if (tid == 0 && s_bad) atomicExch(status, kZeroPivot);
 }
 
-// ---- triangular-solve leaves (h <= 128) ----------------------------------------------------
-// B (h x w, ldb) := L^-1 B, L unit lower (h x h, lda); one CTA per 64 columns.
-__global__ void __launch_bounds__(256) k_trsm_llu_leaf(const float* __restrict__ L, long lda, int h, float* B, long ldb,
-                                                        int w) {
-  extern __shared__ float sm[];
-  float* l = sm;                 // [h][h+1] column-major
-  float* b = sm + h * (h + 1);   // [64][h+1]: column c of the strip at b[c*(h+1)]
-  const int ldl = h + 1, tid = threadIdx.x, nt = blockDim.x;
+// ---- triangular-solve leaves (h <= 128): products with the inverted diagonal block ----------
+// B (h x w, ldb) := Dinv B, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h);
+// one CTA per 64 columns, 256 threads each computing 4 rows x 8 columns, FP32.
+constexpr int kLdI = 132, kLdB = 68;
+__global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict__ Dinv, int h, float* B, long ldb,
+                                                         int w) {
+  extern __shared__ __align__(16) float sm[];
+  float* li = sm;                 // li[k * kLdI + r] = Dinv(r, k)
+  float* bs = sm + 128 * kLdI;    // bs[k * kLdB + c] = B(k, c0 + c)
+  const int tid = threadIdx.x;
   const int c0 = blockIdx.x * 64, nc = min(64, w - c0);
-  for (int i = tid; i < h * h; i += nt) {
-    const int r = i % h, c = i / h;
-    l[c * ldl + r] = L[(size_t)c * lda + r];
+  for (int i = tid; i < 128 * 128; i += 256) {
+    const int r = i & 127, k = i >> 7;
+    li[k * kLdI + r] = Dinv[(size_t)k * 128 + r];
   }
-  for (int i = tid; i < h * nc; i += nt) {
-    const int r = i % h, c = i / h;
-    b[c * ldl + r] = B[(size_t)(c0 + c) * ldb + r];
+  for (int i = tid; i < 128 * 64; i += 256) {
+    const int k = i & 127, cc = i >> 7;
+    bs[k * kLdB + cc] = (k < h && cc < nc) ? B[(size_t)(c0 + cc) * ldb + k] : 0.f;
   }
   __syncthreads();
-  for (int k = 0; k < h - 1; ++k) {
-    const int rows = h - k - 1;
-    for (int i = tid; i < rows * nc; i += nt) {
-      const int r = k + 1 + i % rows, c = i / rows;
-      b[c * ldl + r] -= l[k * ldl + r] * b[c * ldl + k];
-    }
-    __syncthreads();
+  const int tr = tid & 31, tc = tid >> 5;  // rows 4 tr .. 4 tr + 3, columns 8 tc .. 8 tc + 7
+  float acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+  for (int k = 0; k < h; ++k) {
+    const float4 a = *reinterpret_cast<const float4*>(&li[k * kLdI + 4 * tr]);
+    const float4 b0 = *reinterpret_cast<const float4*>(&bs[k * kLdB + 8 * tc]);
+    const float4 b1 = *reinterpret_cast<const float4*>(&bs[k * kLdB + 8 * tc + 4]);
+    const float av[4] = {a.x, a.y, a.z, a.w};
+    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] += av[i] * bv[j];
   }
-  for (int i = tid; i < h * nc; i += nt) {
-    const int r = i % h, c = i / h;
-    B[(size_t)(c0 + c) * ldb + r] = b[c * ldl + r];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int cc = 8 * tc + j;
+    if (cc < nc)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = 4 * tr + i;
+        if (r < h) B[(size_t)(c0 + cc) * ldb + r] = acc[i][j];
+      }
   }
 }
 
-// B (m x h, ldb) := B U^-1, U upper (h x h, lda); one CTA per 64 rows.
-__global__ void __launch_bounds__(256) k_trsm_ru_leaf(const float* __restrict__ U, long lda, int h, float* B, long ldb,
-                                                       int m) {
-  extern __shared__ float sm[];
-  float* u = sm;                 // [h][h+1] column-major
-  float* b = sm + h * (h + 1);   // [h][65]: column j of the strip at b[j*65]
-  const int ldu = h + 1, tid = threadIdx.x, nt = blockDim.x;
+// B (m x h, ldb) := B Dinv, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h);
+// one CTA per 64 rows, 256 threads each computing 4 rows x 8 columns, FP32.
+__global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict__ Dinv, int h, float* B, long ldb,
+                                                          int m) {
+  extern __shared__ __align__(16) float sm[];
+  float* us = sm;                 // us[k * kLdI + c] = Dinv(k, c)
+  float* bs = sm + 128 * kLdI;    // bs[k * kLdB + rr] = B(r0 + rr, k)
+  const int tid = threadIdx.x;
   const int r0 = blockIdx.x * 64, nr = min(64, m - r0);
-  for (int i = tid; i < h * h; i += nt) {
-    const int r = i % h, c = i / h;
-    u[c * ldu + r] = U[(size_t)c * lda + r];
+  for (int i = tid; i < 128 * 128; i += 256) {
+    const int k = i & 127, cc = i >> 7;
+    us[k * kLdI + cc] = Dinv[(size_t)cc * 128 + k];
   }
-  for (int i = tid; i < nr * h; i += nt) {
-    const int r = i % nr, c = i / nr;
-    b[c * 65 + r] = B[(size_t)c * ldb + r0 + r];
+  for (int i = tid; i < 64 * 128; i += 256) {
+    const int rr = i & 63, k = i >> 6;
+    bs[k * kLdB + rr] = (k < h && rr < nr) ? B[(size_t)k * ldb + r0 + rr] : 0.f;
   }
   __syncthreads();
-  for (int j = 0; j < h; ++j) {
-    const float rp = 1.0f / u[j * ldu + j];
-    for (int r = tid; r < nr; r += nt) b[j * 65 + r] *= rp;
-    __syncthreads();
-    const int cols = h - j - 1;
-    for (int i = tid; i < nr * cols; i += nt) {
-      const int r = i % nr, c = j + 1 + i / nr;
-      b[c * 65 + r] -= b[j * 65 + r] * u[c * ldu + j];
-    }
-    __syncthreads();
+  const int tr = tid & 15, tc = tid >> 4;  // rows 4 tr .. 4 tr + 3, columns 8 tc .. 8 tc + 7
+  float acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+  for (int k = 0; k < h; ++k) {
+    const float4 a = *reinterpret_cast<const float4*>(&bs[k * kLdB + 4 * tr]);
+    const float4 b0 = *reinterpret_cast<const float4*>(&us[k * kLdI + 8 * tc]);
+    const float4 b1 = *reinterpret_cast<const float4*>(&us[k * kLdI + 8 * tc + 4]);
+    const float av[4] = {a.x, a.y, a.z, a.w};
+    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] += av[i] * bv[j];
   }
-  for (int i = tid; i < nr * h; i += nt) {
-    const int r = i % nr, c = i / nr;
-    B[(size_t)c * ldb + r0 + r] = b[c * 65 + r];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int cc = 8 * tc + j;
+    if (cc < h)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int rr = 4 * tr + i;
+        if (rr < nr) B[(size_t)cc * ldb + r0 + rr] = acc[i][j];
+      }
   }
 }
 
 // ---- FP64 mat-vec for the residuals: Y = beta Y + alpha A X (q <= Q columns) ----------------
+// Two rows per thread (16-byte loads; the leading dimension is even and the rows start even), the
+// columns split over blockIdx.y into partial sums P, reduced in a fixed order afterwards.
 template <int Q>
 __global__ void __launch_bounds__(128) k_matvec64_part(const double* __restrict__ A, long lda, int n,
                                                        const double* __restrict__ X, long ldx, int q, int cols_per,
                                                        double* __restrict__ P) {
-  const int row = blockIdx.x * 128 + threadIdx.x, split = blockIdx.y;
+  const int row = 2 * (blockIdx.x * 128 + threadIdx.x), split = blockIdx.y;
   const int c0 = split * cols_per, c1 = min(n, c0 + cols_per);
-  double acc[Q];
+  double a0[Q], a1[Q];
 #pragma unroll
-  for (int j = 0; j < Q; ++j) acc[j] = 0.0;
+  for (int j = 0; j < Q; ++j) a0[j] = a1[j] = 0.0;
   if (row < n) {
     const double* a = A + row;
-#pragma unroll 4
+#pragma unroll 8
     for (int c = c0; c < c1; ++c) {
-      const double v = a[(size_t)c * lda];
+      const double2 v = *reinterpret_cast<const double2*>(a + (size_t)c * lda);
 #pragma unroll
       for (int j = 0; j < Q; ++j)
-        if (j < q) acc[j] += v * __ldg(&X[(size_t)j * ldx + c]);
+        if (j < q) {
+          const double x = __ldg(&X[(size_t)j * ldx + c]);
+          a0[j] += v.x * x;
+          a1[j] += v.y * x;
+        }
     }
 #pragma unroll
     for (int j = 0; j < Q; ++j)
-      if (j < q) P[((size_t)split * Q + j) * n + row] = acc[j];
+      if (j < q) {
+        P[((size_t)split * Q + j) * n + row] = a0[j];
+        if (row + 1 < n) P[((size_t)split * Q + j) * n + row + 1] = a1[j];
+      }
   }
 }
 
@@ -261,9 +348,78 @@ __global__ void k_copy_out(const double* __restrict__ Y, int n, int q, double* B
     for (int c = 0; c < q; ++c) B[(size_t)c * ldb + r] = Y[(size_t)c * n + r];
 }
 
+// Optional per-call timing (BEST_GPU_PROFILE=1): CUDA events around each GEMM, cast and leaf,
+// summed per category and (for GEMMs) per size class, reported as log lines after the build.
+struct CallProfile {
+  bool on = false;
+  struct Rec {
+    std::string key;
+    cudaEvent_t a, b;
+    double flops;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  cudaEvent_t ev() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void begin(const std::string& key, double flops, cudaStream_t s) {
+    if (!on) return;
+    Rec r{key, ev(), ev(), flops};
+    cudaEventRecord(r.a, s);
+    recs.push_back(r);
+  }
+  void end(cudaStream_t s) {
+    if (on) cudaEventRecord(recs.back().b, s);
+  }
+  std::vector<std::string> report() {
+    std::vector<std::string> out;
+    if (!on || recs.empty()) return out;
+    cudaEventSynchronize(recs.back().b);
+    std::map<std::string, std::pair<int, std::pair<double, double>>> agg;
+    for (auto& r : recs) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      auto& a = agg[r.key];
+      a.first += 1;
+      a.second.first += ms;
+      a.second.second += r.flops;
+    }
+    for (auto& kv : agg) {
+      char buf[256];
+      std::snprintf(buf, sizeof buf, "profile: %-28s %6d calls %9.2f ms %8.1f TFLOP/s", kv.first.c_str(),
+                    kv.second.first, kv.second.second.first,
+                    kv.second.second.second / std::max(1e-9, kv.second.second.first * 1e-3) / 1e12);
+      out.emplace_back(buf);
+    }
+    recs.clear();
+    used = 0;
+    return out;
+  }
+};
+
+std::string size_class(int m, int n, int k) {
+  auto c = [](int v) { return v <= 256 ? "S" : (v <= 2048 ? "M" : "L"); };
+  return std::string("gemm ") + c(m) + c(n) + c(k);
+}
+
 }  // namespace
 
 struct MixedSolver::Impl {
+  CallProfile prof;
+  alignas(64) unsigned char map_a[kTensorMapBytes], map_b[kTensorMapBytes];
+  long op_ld = 0;      // leading dimension of both BF16 operand buffers (elements)
+  int op_rows = 0;     // rows of both operand buffers
+  const void* map_key[2] = {};      // the buffers the tensor maps describe
+  cudaGraphExec_t graph = nullptr;  // the captured factorisation
+  const void* graph_key[5] = {};
+  int graph_n = 0;
+  size_t graph_kernels = 0;
   int n3 = 0;
   long ld32 = 0;
   double* gr64 = nullptr;  // the FP64 matrix (owned by the caller)
@@ -271,17 +427,21 @@ struct MixedSolver::Impl {
   double tol = 1e-12;
   int max_restarts = 8, krylov = 10;
   int sms = 148;
-  Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs;
+  Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs, dl32, du32;
   int* d_status() { return status.as<int>(); }
 
   // C (m x n at c, ldc) -= A (m x k, col-major fp32) B (k x n col-major fp32) via BF16 tensor cores
   void gemm(int m, int n, int k, const float* A, long lda, const float* B, long ldb, float* C, long ldc,
             cudaStream_t s) {
     if (m <= 0 || n <= 0 || k <= 0) return;
-    const long lat = round_up(k, 64), lbt = round_up(k, 64);
-    ck(cast_transpose_bf16(A, lda, m, k, at.p, lat, s), "cast A");
-    ck(cast_bf16(B, ldb, k, n, bt.p, lbt, s), "cast B");
-    ck(gemm_bf16_tc_minus(m, n, k, at.p, lat, bt.p, lbt, C, ldc, d_status(), s), "tensor-core GEMM");
+    if (m > op_rows || n > op_rows || round_up(k, 64) > op_ld) throw std::runtime_error("GEMM larger than its operand buffers");
+    prof.begin("casts", 0, s);
+    ck(cast_transpose_bf16(A, lda, m, k, at.p, op_ld, s), "cast A");
+    ck(cast_bf16(B, ldb, k, n, bt.p, op_ld, s), "cast B");
+    prof.end(s);
+    prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
+    ck(gemm_bf16_tc_minus_maps(m, n, k, map_a, map_b, C, ldc, d_status(), s), "tensor-core GEMM");
+    prof.end(s);
   }
 
   static int split(int sz) {
@@ -289,60 +449,71 @@ struct MixedSolver::Impl {
     return std::max(h, kLeaf);
   }
 
-  // B (h x w at b) := L^-1 B, L unit lower at l (h x h); leading dimension ld32
-  void trsm_llu(const float* l, int h, float* b, int w, cudaStream_t s) {
+  float* at_(int r, int c) const { return lu32.as<float>() + r + (size_t)c * ld32; }
+
+  // rows [kd, kd+h) x columns [c0, c0+w) := L^-1 (that block), L the unit lower triangle at (kd, kd)
+  void trsm_llu(int kd, int h, int c0, int w, cudaStream_t s) {
     if (h <= 0 || w <= 0) return;
     if (h <= kLeaf) {
-      const size_t smem = (size_t)(h * (h + 1) + 64 * (h + 1)) * sizeof(float);
-      k_trsm_llu_leaf<<<(w + 63) / 64, 256, smem, s>>>(l, ld32, h, b, ld32, w);
+      const size_t smem = (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float);
+      prof.begin("trsm leaf (left)", 2.0 * h * h * w, s);
+      k_apply_inv_left<<<(w + 63) / 64, 256, smem, s>>>(dl32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf, h,
+                                                       at_(kd, c0), ld32, w);
+      prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
       return;
     }
     const int h1 = split(h);
-    trsm_llu(l, h1, b, w, s);
-    gemm(h - h1, w, h1, l + h1, ld32, b, ld32, b + h1, ld32, s);
-    trsm_llu(l + h1 + (size_t)h1 * ld32, h - h1, b + h1, w, s);
+    trsm_llu(kd, h1, c0, w, s);
+    gemm(h - h1, w, h1, at_(kd + h1, kd), ld32, at_(kd, c0), ld32, at_(kd + h1, c0), ld32, s);
+    trsm_llu(kd + h1, h - h1, c0, w, s);
   }
 
-  // B (m x h at b) := B U^-1, U upper at u (h x h)
-  void trsm_ru(const float* u, int h, float* b, int m, cudaStream_t s) {
+  // rows [r0, r0+m) x columns [kd, kd+h) := (that block) U^-1, U the upper triangle at (kd, kd)
+  void trsm_ru(int kd, int h, int r0, int m, cudaStream_t s) {
     if (h <= 0 || m <= 0) return;
     if (h <= kLeaf) {
-      const size_t smem = (size_t)(h * (h + 1) + h * 65) * sizeof(float);
-      k_trsm_ru_leaf<<<(m + 63) / 64, 256, smem, s>>>(u, ld32, h, b, ld32, m);
+      const size_t smem = (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float);
+      prof.begin("trsm leaf (right)", 2.0 * h * h * m, s);
+      k_apply_inv_right<<<(m + 63) / 64, 256, smem, s>>>(du32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf, h,
+                                                        at_(r0, kd), ld32, m);
+      prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
       return;
     }
     const int h1 = split(h);
-    trsm_ru(u, h1, b, m, s);
-    gemm(m, h - h1, h1, b, ld32, u + (size_t)h1 * ld32, ld32, b + (size_t)h1 * ld32, ld32, s);
-    trsm_ru(u + h1 + (size_t)h1 * ld32, h - h1, b + (size_t)h1 * ld32, m, s);
+    trsm_ru(kd, h1, r0, m, s);
+    gemm(m, h - h1, h1, at_(r0, kd), ld32, at_(kd, kd + h1), ld32, at_(r0, kd + h1), ld32, s);
+    trsm_ru(kd + h1, h - h1, r0, m, s);
   }
 
-  // factors the square block at (k0, k0) of size sz in place
+  // factors the square block at (k0, k0) of size sz in place; each 128 x 128 diagonal leaf is
+  // inverted (both triangles) right after it is factored, for the triangular-solve leaves above it
   void rlu(int k0, int sz, cudaStream_t s) {
-    float* A = lu32.as<float>();
-    float* D = A + k0 + (size_t)k0 * ld32;
     if (sz <= kLeaf) {
-      const size_t smem = (size_t)sz * (sz + 1) * sizeof(float);
-      k_lu32_leaf<<<1, 512, smem, s>>>(D, ld32, sz, d_status());
+      const size_t smem = (size_t)3 * 128 * kLdS * sizeof(float);
+      const size_t off = (size_t)(k0 / kLeaf) * kLeaf * kLeaf;
+      prof.begin("LU leaf + inverses", 0, s);
+      k_lu32_leaf_inv<<<1, 512, smem, s>>>(at_(k0, k0), ld32, sz, dl32.as<float>() + off, du32.as<float>() + off,
+                                           d_status());
+      prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "LU leaf");
       return;
     }
     const int h = split(sz), r = sz - h;
     rlu(k0, h, s);
-    trsm_llu(D, h, D + (size_t)h * ld32, r, s);          // U12
-    trsm_ru(D, h, D + h, r, s);                          // L21
-    gemm(r, r, h, D + h, ld32, D + (size_t)h * ld32, ld32, D + h + (size_t)h * ld32, ld32, s);
+    trsm_llu(k0, h, k0 + h, r, s);   // U12
+    trsm_ru(k0, h, k0 + h, r, s);    // L21
+    gemm(r, r, h, at_(k0 + h, k0), ld32, at_(k0, k0 + h), ld32, at_(k0 + h, k0 + h), ld32, s);
     rlu(k0 + h, r, s);
   }
 
   // Y (n3 x q, ldy) = beta Y + alpha GR X
   void matvec(const double* X, long ldx, int q, double* Y, long ldy, double alpha, double beta, cudaStream_t s) {
-    const int rb = (n3 + 127) / 128;
+    const int rb = (n3 + 255) / 256;
     const int splits = std::max(1, std::min(32, (4 * sms * 8 + rb - 1) / rb));
     const int per = (n3 + splits - 1) / splits;
     part.ensure((size_t)splits * 16 * n3 * sizeof(double), "residual partials");
@@ -375,14 +546,21 @@ struct MixedSolver::Impl {
   }
 };
 
+std::vector<std::string> MixedSolver::profile_report() { return p_->prof.report(); }
+
 MixedSolver::MixedSolver() : p_(new Impl) {
+  const char* e = std::getenv("BEST_GPU_PROFILE");
+  p_->prof.on = e && *e && std::string(e) != "0";
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&p_->sms, cudaDevAttrMultiProcessorCount, dev);
   p_->status.ensure(256, "status");
   ck(cudaMemset(p_->status.p, 0, 256), "status clear");
 }
-MixedSolver::~MixedSolver() { delete p_; }
+MixedSolver::~MixedSolver() {
+  if (p_->graph) cudaGraphExecDestroy(p_->graph);
+  delete p_;
+}
 void MixedSolver::set_refinement(int max_restarts, int krylov) {
   p_->max_restarts = std::max(0, max_restarts);
   p_->krylov = std::min(16, std::max(1, krylov));
@@ -398,21 +576,67 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   P.ld64 = ld;
   P.tol = std::max(1e-15, std::min(0.1 * eps, 1e-12));
   P.lu32.ensure((size_t)P.ld32 * P.n3 * sizeof(float), "FP32 copy of GR");
+  P.dl32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (L)");
+  P.du32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (U)");
   const long half = P.n3 / 2 + 128;
-  P.at.ensure((size_t)half * round_up(half, 64) * 2, "BF16 operand A");
-  P.bt.ensure((size_t)half * round_up(half, 64) * 2, "BF16 operand B");
+  const long op_ld = round_up(half, 64);
+  P.at.ensure((size_t)half * op_ld * 2, "BF16 operand A");
+  P.bt.ensure((size_t)half * op_ld * 2, "BF16 operand B");
+  if (P.op_ld != op_ld || P.op_rows != (int)half || P.map_key[0] != P.at.p || P.map_key[1] != P.bt.p) {
+    if (!tc_operand_maps(P.at.p, (int)half, op_ld, P.bt.p, (int)half, op_ld, P.map_a, P.map_b))
+      throw std::runtime_error("cannot build the tensor maps of the BF16 operands");
+    P.op_ld = op_ld;
+    P.op_rows = (int)half;
+    P.map_key[0] = P.at.p;
+    P.map_key[1] = P.bt.p;
+  }
+  ck(tc_gemm_prepare(), "tensor-core GEMM attributes");
   static bool attrs = false;
   if (!attrs) {
     const int big = 200 * 1024;
-    ck(cudaFuncSetAttribute(k_lu32_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
-    ck(cudaFuncSetAttribute(k_trsm_llu_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
-    ck(cudaFuncSetAttribute(k_trsm_ru_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_lu32_leaf_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_left, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_right, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
     attrs = true;
   }
   ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
   ck(launch_assemble(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
   ck(cudaEventRecord(ev_assembled, s), "event");
-  P.rlu(0, P.n3, s);
+  if (P.prof.on) {
+    P.rlu(0, P.n3, s);  // direct launches, each timed
+  } else {
+    // the recursion's launches depend only on the order and the buffers: capture them once as a
+    // CUDA graph and replay it
+    const void* key[5] = {P.lu32.p, P.at.p, P.bt.p, P.dl32.p, P.du32.p};
+    if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 5, P.graph_key)) {
+      if (P.graph) cudaGraphExecDestroy(P.graph);
+      P.graph = nullptr;
+      cudaStream_t cs;
+      ck(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+      cudaGraph_t g = nullptr;
+      const unsigned long long launches0 = g_launches;  // captured launches do not run now
+      ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+      try {
+        P.rlu(0, P.n3, cs);
+      } catch (...) {
+        cudaStreamEndCapture(cs, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cs);
+        g_launches = launches0;
+        throw;
+      }
+      ck(cudaStreamEndCapture(cs, &g), "end capture");
+      P.graph_kernels = (size_t)(g_launches - launches0);
+      g_launches = launches0;
+      ck(cudaGraphInstantiate(&P.graph, g, 0), "graph instantiate");
+      cudaGraphDestroy(g);
+      cudaStreamDestroy(cs);
+      std::copy(key, key + 5, P.graph_key);
+      P.graph_n = P.n3;
+    }
+    ck(cudaGraphLaunch(P.graph, s), "graph launch");
+    g_launches += P.graph_kernels;
+  }
   ck(cudaEventRecord(ev_factored, s), "event");
   int st = 0;
   ck(cudaMemcpyAsync(&st, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
@@ -454,7 +678,11 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
     for (int restart = 0; restart <= max_restarts; ++restart) {
       // R = B - GR X
       ck(cudaMemcpyAsync(R, B, blk * sizeof(double), cudaMemcpyDeviceToDevice, s), "r copy");
-      if (restart > 0) P.matvec(X, n, q, R, n, -1.0, 1.0, s);
+      if (restart > 0) {
+        P.prof.begin("FP64 mat-vec", 2.0 * n * (double)n * q, s);
+        P.matvec(X, n, q, R, n, -1.0, 1.0, s);
+        P.prof.end(s);
+      }
       std::vector<double> rn2 = P.dot(R, 1, R, q, s);
       std::vector<double> rn(q), inv(q);
       rel = 0.0;
@@ -479,8 +707,14 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
         double* Vj = V + (size_t)j * blk;
         double* Zj = Z + (size_t)j * blk;
         ck(cudaMemcpyAsync(Zj, Vj, blk * sizeof(double), cudaMemcpyDeviceToDevice, s), "z copy");
-        ck(trsv_lu32(P.lu32.as<float>(), P.ld32, n, Zj, n, q, P.trsv.p, P.d_status(), s), "preconditioner");
+        P.prof.begin("preconditioner solve", 0, s);
+        ck(trsv_lu32_inv(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), n, Zj, n, q, P.trsv.p,
+                         P.d_status(), s),
+           "preconditioner");
+        P.prof.end(s);
+        P.prof.begin("FP64 mat-vec", 2.0 * n * (double)n * q, s);
         P.matvec(Zj, n, q, W, n, 1.0, 0.0, s);
+        P.prof.end(s);
         // classical Gram-Schmidt, twice
         std::vector<double> h = P.dot(V, j + 1, W, q, s);
         ck(cudaMemcpyAsync(P.dots.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s), "coef");

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <stdexcept>
+#include <string>
+#include <vector>
 
 #include "bgpu_internal.h"
 
@@ -31,6 +33,8 @@ class MixedSolver {
   // records ev_assembled, factors the copy.  Throws on failure.
   void build(const DevMesh& m, const DevDeflation& d, double* gr64, long ld, double eps, cudaStream_t s,
              cudaEvent_t ev_assembled, cudaEvent_t ev_factored);
+  // With BEST_GPU_PROFILE=1: per-category times of the calls since the last report (log lines).
+  std::vector<std::string> profile_report();
   // GMRES restarts (each with a true FP64 residual) and Krylov vectors per restart.
   void set_refinement(int max_restarts, int krylov);
   // Solves GR x = b in place (d_b: 3n x nrhs, ldb) to the relative residual of build's eps.

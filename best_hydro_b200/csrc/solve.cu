@@ -324,6 +324,247 @@ cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* 
   return cudaGetLastError();
 }
 
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// Triangular solves with inverted diagonal blocks (128 rows): the in-block step is a 128 x 128
+// mat-vec instead of a 128-step substitution, which shortens the block-to-block dependency chain.
+// ---------------------------------------------------------------------------------------------
+constexpr int kIb = 128;  // rows per block
+constexpr int kIrhs = 8;  // right-hand sides per pass
+
+// Inverses of the 128 x 128 diagonal blocks of an LU factor (F = double or float): block b of DL is
+// L_bb^-1 (unit lower), of DU U_bb^-1, column-major 128 x 128 (the last block padded with zeros);
+// one CTA per block, one thread per column, FP64 arithmetic.
+template <typename F, typename FI>
+__global__ void __launch_bounds__(kIb) k_diag_inverses(const F* __restrict__ LU, long lda, int n, int b0,
+                                                       FI* __restrict__ DL, FI* __restrict__ DU) {
+  extern __shared__ double sdi[];  // sdi[c * (kIb + 1) + r] = factor entry (r, c) of the block
+  const int b = b0 + blockIdx.x, r0 = b * kIb, h = min(kIb, n - r0), c = threadIdx.x;
+  auto sl = [&](int col, int r) -> double { return sdi[col * (kIb + 1) + r]; };
+  for (int i = 0; i < h; ++i)
+    if (c < h) sdi[c * (kIb + 1) + i] = (double)LU[(size_t)(r0 + c) * lda + r0 + i];
+  __syncthreads();
+  FI* dl = DL + (size_t)b * kIb * kIb;
+  FI* du = DU + (size_t)b * kIb * kIb;
+  // column c of L^-1: x_c = 1, x_i = -sum_{c <= j < i} L_ij x_j  (i > c); and of U^-1:
+  // x_c = 1/U_cc, x_i = -(sum_{i < j <= c} U_ij x_j) / U_ii (i < c)
+  double x[kIb];
+  for (int i = 0; i < kIb; ++i) x[i] = 0.0;
+  if (c < h) {
+    x[c] = 1.0;
+    for (int i = c + 1; i < h; ++i) {
+      double s0 = 0.0, s1 = 0.0;
+      int j = c;
+      for (; j + 1 < i; j += 2) {
+        s0 += sl(j, i) * x[j];
+        s1 += sl(j + 1, i) * x[j + 1];
+      }
+      if (j < i) s0 += sl(j, i) * x[j];
+      x[i] = -(s0 + s1);
+    }
+  }
+  for (int i = 0; i < kIb; ++i) dl[(size_t)c * kIb + i] = (FI)((c < h && i < h) ? x[i] : 0.0);
+  for (int i = 0; i < kIb; ++i) x[i] = 0.0;
+  if (c < h) {
+    x[c] = 1.0 / sl(c, c);
+    for (int i = c - 1; i >= 0; --i) {
+      double s0 = 0.0, s1 = 0.0;
+      int j = i + 1;
+      for (; j + 1 <= c; j += 2) {
+        s0 += sl(j, i) * x[j];
+        s1 += sl(j + 1, i) * x[j + 1];
+      }
+      if (j <= c) s0 += sl(j, i) * x[j];
+      x[i] = -(s0 + s1) / sl(i, i);
+    }
+  }
+  for (int i = 0; i < kIb; ++i) du[(size_t)c * kIb + i] = (FI)((c < h && i < h) ? x[i] : 0.0);
+}
+
+// One triangle on Y (n x nrhs <= kIrhs, ldy): LOWER = unit lower L with block inverses DI, blocks in
+// increasing order; otherwise upper U, decreasing.  256 threads: row = t % 128, half = t / 128 of
+// the 128-wide inner dimension.  Each thread loads its 64 factor entries of the next block into
+// registers before waiting for that block's unknowns, so the factor streams while the chain of
+// dependencies advances.
+template <typename F, typename FI, bool LOWER>
+__global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
+                                                  double* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
+                                                  unsigned epoch, int* status) {
+  __shared__ double s_y[kIb][kIrhs];
+  __shared__ double s_acc[2][kIb][kIrhs];
+  __shared__ int s_blk, s_cnt;
+  const int nblk = (n + kIb - 1) / kIb;
+  const int tid = threadIdx.x, row = tid & (kIb - 1), half = tid >> 7;
+  for (;;) {
+    if (tid == 0) s_blk = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int t = s_blk;
+    if (t >= nblk) return;
+    const int blk = LOWER ? t : nblk - 1 - t;
+    const int r0 = blk * kIb, nr = min(kIb, n - r0);
+    const bool live = row < nr;
+    double acc[kIrhs];
+#pragma unroll
+    for (int r = 0; r < kIrhs; ++r) acc[r] = 0.0;
+    const int nq = LOWER ? blk : nblk - 1 - blk;
+    int confirmed = 0;
+    for (int q = 0; q < nq; ++q) {
+      const int jb = LOWER ? q : nblk - 1 - q;
+      const int c0 = jb * kIb, nc = min(kIb, n - c0);
+      // this thread's 64 entries of block (blk, jb), loaded before the wait
+      const F* col = LU + (size_t)(c0 + half * 64) * lda + r0 + row;
+      F lv[64];
+#pragma unroll
+      for (int kk = 0; kk < 64; ++kk)
+        lv[kk] = (live && half * 64 + kk < nc) ? col[(size_t)kk * lda] : (F)0;
+      if (q >= confirmed) {
+        const int cnt = LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, &s_cnt)
+                              : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, &s_cnt);
+        if (cnt == 0) return;
+        confirmed = q + cnt;
+      }
+      for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+        const int rr = idx / kIrhs, r = idx % kIrhs;
+        s_y[rr][r] = (rr < nc && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + c0 + rr]) : 0.0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < 64; ++kk) {
+        const double l = (double)lv[kk];
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) acc[r] -= l * s_y[half * 64 + kk][r];
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
+    // this thread's row of the inverse block
+    const FI* di = DI + (size_t)blk * kIb * kIb + row;
+    __syncthreads();
+    // right-hand side of the block: b - off-diagonal sums
+    for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+      const int rr = idx / kIrhs, r = idx % kIrhs;
+      s_y[rr][r] = (rr < nr && r < nrhs) ? Y[(size_t)r * ldy + r0 + rr] + (s_acc[0][rr][r] + s_acc[1][rr][r]) : 0.0;
+    }
+    __syncthreads();
+    // x = D^-1 (b - ...): each half does 64 of the 128 products
+#pragma unroll
+    for (int r = 0; r < kIrhs; ++r) acc[r] = 0.0;
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      double dv[32];
+#pragma unroll
+      for (int kk = 0; kk < 32; ++kk) dv[kk] = (double)di[(size_t)(half * 64 + b * 32 + kk) * kIb];
+#pragma unroll
+      for (int kk = 0; kk < 32; ++kk) {
+        const int cc = half * 64 + b * 32 + kk;
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) acc[r] += dv[kk] * s_y[cc][r];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
+    __syncthreads();
+    for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+      const int rr = idx / kIrhs, r = idx % kIrhs;
+      if (rr < nr && r < nrhs) Y[(size_t)r * ldy + r0 + rr] = s_acc[0][rr][r] + s_acc[1][rr][r];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      st_release_u32(flags + blk, epoch);
+    }
+  }
+}
+
+template <typename F, typename FI>
+cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int n, double* Y, long ldy, int nrhs,
+                          void* scratch, int* d_status, cudaStream_t s) {
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  unsigned* ticket = reinterpret_cast<unsigned*>(base);
+  unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int nblk = (n + kIb - 1) / kIb;
+  const int grid = std::min(nblk, sms * 3);
+  for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
+    const int q = std::min(kIrhs, nrhs - c0);
+    double* Yc = Y + (size_t)c0 * ldy;
+    g_epoch += 2;
+    if (g_epoch == 0) g_epoch = 2;
+    cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
+    if (e != cudaSuccess) return e;
+    k_trsv_inv<F, FI, true><<<grid, 256, 0, s>>>(LU, lda, DL, n, Yc, ldy, q, flags, ticket, g_epoch, d_status);
+    BGPU_COUNT_LAUNCH();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
+    k_trsv_inv<F, FI, false><<<grid, 256, 0, s>>>(LU, lda, DU, n, Yc, ldy, q, flags, ticket, g_epoch + 1, d_status);
+    BGPU_COUNT_LAUNCH();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+size_t diag_inverse_elems(int n) { return (size_t)((n + kIb - 1) / kIb) * kIb * kIb; }
+
+constexpr size_t kDiagInvSmem = (size_t)kIb * (kIb + 1) * sizeof(double);
+
+cudaError_t diag_inverses64(const double* LU, long lda, int n, double* DL, double* DU, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_diag_inverses<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kDiagInvSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_diag_inverses<double, double><<<(n + kIb - 1) / kIb, kIb, kDiagInvSmem, s>>>(LU, lda, n, 0, DL, DU);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t diag_inverses32(const float* LU, long lda, int n, int b0, int nb, float* DL, float* DU, cudaStream_t s) {
+  if (n <= 0 || nb <= 0) return cudaSuccess;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_diag_inverses<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kDiagInvSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_diag_inverses<float, float><<<nb, kIb, kDiagInvSmem, s>>>(LU, lda, n, b0, DL, DU);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// dgetrs('N') with FP64 factors and their diagonal-block inverses: X := A^-1 X (in place).
+cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
+                        double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return cudaSuccess;
+  if (nrhs > kMaxRhs) return cudaErrorInvalidValue;
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  double* Y = reinterpret_cast<double*>(base + TrsvScratch::y_off(n));
+  const long ldy = n;
+  k_gather_rows<double><<<(n + 255) / 256, 256, 0, s>>>(X, ldx, perm, n, nrhs, Y, ldy);
+  BGPU_COUNT_LAUNCH();
+  cudaError_t e = trsv_inv_pair<double, double>(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
+  if (e != cudaSuccess) return e;
+  k_copy_cols<double><<<(n + 255) / 256, 256, 0, s>>>(Y, ldy, n, nrhs, X, ldx);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// Y := U^-1 L^-1 Y with FP32 factors of an unpivoted LU and their FP32 diagonal-block inverses.
+cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, double* Y, long ldy,
+                          int nrhs, void* scratch, int* d_status, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return cudaSuccess;
+  return trsv_inv_pair<float, float>(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
+}
+
 // Y := U^-1 L^-1 Y in place with FP32 factors of an unpivoted LU (the mixed-precision
 // preconditioner); Y is FP64 and the sums are accumulated in FP64.
 cudaError_t trsv_lu32(const float* LU, long lda, int n, double* Y, long ldy, int nrhs, void* scratch, int* d_status,

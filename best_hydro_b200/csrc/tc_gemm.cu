@@ -232,8 +232,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ------------------------------------------------------------------------------------------
 // At (m x k row-major, lda_t) = bf16(A), A m x k column-major FP32 (lda): transposed through a
 // 32 x 32 shared tile so both sides are coalesced.
-__global__ void k_cast_transpose_bf16(const float* __restrict__ A, long lda, int m, int k, __nv_bfloat16* __restrict__ At,
-                                      long lda_t) {
+// Columns [k, kpad) of At are written as zeros (the GEMM reads whole 64-wide K tiles).
+__global__ void k_cast_transpose_bf16(const float* __restrict__ A, long lda, int m, int k, int kpad,
+                                      __nv_bfloat16* __restrict__ At, long lda_t) {
   __shared__ float t[32][33];
   const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
@@ -243,18 +244,19 @@ __global__ void k_cast_transpose_bf16(const float* __restrict__ A, long lda, int
   __syncthreads();
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int i = i0 + r, kk = k0 + threadIdx.x;
-    if (i < m && kk < k) At[(size_t)i * lda_t + kk] = __float2bfloat16_rn(t[threadIdx.x][r]);
+    if (i < m && kk < kpad) At[(size_t)i * lda_t + kk] = __float2bfloat16_rn(t[threadIdx.x][r]);
   }
 }
 
-// Bt (k x n column-major, ldb_t) = bf16(B), B k x n column-major FP32 (ldb); 32 x 32 tiles.
-__global__ void k_cast_bf16(const float* __restrict__ B, long ldb, int k, int n, __nv_bfloat16* __restrict__ Bt,
-                            long ldb_t) {
+// Bt (k x n column-major, ldb_t) = bf16(B), B k x n column-major FP32 (ldb); 32 x 32 tiles; rows
+// [k, kpad) of Bt are written as zeros.
+__global__ void k_cast_bf16(const float* __restrict__ B, long ldb, int k, int kpad, int n,
+                            __nv_bfloat16* __restrict__ Bt, long ldb_t) {
   const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
   const int kk = k0 + threadIdx.x;
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int j = j0 + r;
-    if (kk < k && j < n) Bt[(size_t)j * ldb_t + kk] = __float2bfloat16_rn(B[(size_t)j * ldb + kk]);
+    if (kk < kpad && j < n) Bt[(size_t)j * ldb_t + kk] = __float2bfloat16_rn(kk < k ? B[(size_t)j * ldb + kk] : 0.f);
   }
 }
 
@@ -292,16 +294,46 @@ bool make_map(CUtensorMap* tm, const void* base, int rows, int cols, long ld, in
 
 cudaError_t cast_transpose_bf16(const float* A, long lda, int m, int k, void* At, long lda_t, cudaStream_t s) {
   if (m <= 0 || k <= 0) return cudaSuccess;
-  dim3 grid((m + 31) / 32, (k + 31) / 32);
-  k_cast_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(A, lda, m, k, static_cast<__nv_bfloat16*>(At), lda_t);
+  const int kpad = (k + BK - 1) / BK * BK;
+  if (kpad > lda_t) return cudaErrorInvalidValue;
+  dim3 grid((m + 31) / 32, (kpad + 31) / 32);
+  k_cast_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(A, lda, m, k, kpad, static_cast<__nv_bfloat16*>(At), lda_t);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
 cudaError_t cast_bf16(const float* B, long ldb, int k, int n, void* Bt, long ldb_t, cudaStream_t s) {
   if (k <= 0 || n <= 0) return cudaSuccess;
-  dim3 grid((k + 31) / 32, (n + 31) / 32);
-  k_cast_bf16<<<grid, dim3(32, 8), 0, s>>>(B, ldb, k, n, static_cast<__nv_bfloat16*>(Bt), ldb_t);
+  const int kpad = (k + BK - 1) / BK * BK;
+  if (kpad > ldb_t) return cudaErrorInvalidValue;
+  dim3 grid((kpad + 31) / 32, (n + 31) / 32);
+  k_cast_bf16<<<grid, dim3(32, 8), 0, s>>>(B, ldb, k, kpad, n, static_cast<__nv_bfloat16*>(Bt), ldb_t);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// Tensor maps over whole BF16 operand buffers (rows x ld elements), built once per buffer: a GEMM
+// on a leading part of the buffer reads rows beyond m or n (never stored) and K padding (zeroed by
+// the casts).
+bool tc_operand_maps(const void* At, int rows_a, long lda_t, const void* Bt, int rows_b, long ldb_t, void* map_a,
+                     void* map_b) {
+  if ((lda_t % 8) || (ldb_t % 8) || ((uintptr_t)At & 15) || ((uintptr_t)Bt & 15)) return false;
+  return make_map(static_cast<CUtensorMap*>(map_a), At, rows_a, (int)lda_t, lda_t, BM) &&
+         make_map(static_cast<CUtensorMap*>(map_b), Bt, rows_b, (int)ldb_t, ldb_t, BN);
+}
+
+cudaError_t tc_gemm_prepare() {
+  return cudaFuncSetAttribute(k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+}
+
+// (tc_gemm_prepare must have run: the launch may be captured into a graph)
+cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, const void* map_b, float* C, long ldc,
+                                    int* d_status, cudaStream_t s) {
+  if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  k_gemm_bf16_tc<<<tiles_m * tiles_n, kThreads, kSmem, s>>>(*static_cast<const CUtensorMap*>(map_a),
+                                                            *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc,
+                                                            tiles_m, tiles_n, d_status);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
