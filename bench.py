@@ -3,11 +3,14 @@
 deflation, LU, solve for the 6 translation/rotation right-hand sides).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload star_f32|ellipsoid_f16|icosphere_l3] [--precision fp64|mixed|both]
+                    [--workload star_f32|ellipsoid_f16|icosphere_l3] [--precision mixed|fp64]
 
-One JSON line on rank 0.  `value` is the device time per solve with the mesh already in HBM (CUDA
-events on the library's stream, L2 flushed between steps); `e2e` is the same solve through the C ABI
-with host buffers (bhm_create ... bhm_solve, copies included).  With N GPUs (torchrun), every rank
+One JSON line on rank 0.  `value` is the device time per solve of the timed path (default: the
+mixed-precision factorisation + FP64 GMRES refinement) with the mesh already in HBM (CUDA events on
+the library's stream, L2 flushed between steps); `fp64_path` is the plain FP64 path timed the same
+way, and `accuracy` the relative differences of D_t, D_r and [eta] (11-RHS solves) between the two.
+`e2e` is the timed path through the C ABI with host buffers (bhm_create ... bhm_solve, copies
+included).  With N GPUs (torchrun), every rank
 solves its own replica: the path has no exchange step, so there is no collective in it.
 `--impl reference` times the reference's own CPU implementation (its kernel.cpp assembly, OpenMP,
 plus the LAPACK dgetrf/dgetrs BEST calls) on bounded samples of the same workload, scaled to a full
@@ -29,6 +32,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+
+METRIC = "s per BEST solve (assemble+LU+6 RHS), mixed vs FP64 GPU at rel err<=1e-8"
 
 WORKLOADS = {
     # BASELINE configuration of the metric's target: star body at geodesic frequency 32 (N = 20,480)
@@ -182,7 +187,7 @@ def run_reference(args, rank):
         vals.append(v)
     v = float(np.median(vals))
     line = {
-        "impl": "reference", "metric": "s per BEST solve (assemble+LU+6 RHS)", "value": v, "unit": "s",
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "N": w["N"], "order": 3 * w["N"], "desc": w["desc"]},
@@ -216,6 +221,21 @@ def fp64_peak_tflops(torch, dev):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
+def tensors_of(solver, x, st, bh):
+    """D_t, D_r traces and CHI' (proportional to [eta]) from an 11-RHS solve with the current factors
+    (untimed): best/difco.f on the 6 flows, best/visco.f on the 5 strain flows."""
+    B = solver.solve(np.hstack([bh.rhs6(x), bh.strain5(x)]))
+    t = bh.difco(x, st.area, B[:, :6])
+    chip, _ = bh.visco(x, st.area, B[:, 6:], B[:, :6])
+    tr = bh.traces(t)
+    return dict(D_t=tr["DTRANS"], D_r=tr["DR"], chiprime=chip, Dtt=t["Dtt"], Drr=t["Drr"])
+
+
+def relerr(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import best_hydro_b200 as bh
@@ -229,16 +249,21 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
 
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     w = WORKLOADS[args.workload]
     tri, ta, tv = make_mesh(args.workload)
     st = bh.Setup(tri, w["iarea"], ta)
     n, n3 = st.n, 3 * st.n
     peaks, peak_src = load_peaks()
-    p64 = fp64_peak_tflops(torch, dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    modes = {"fp64": bh.BGPU_FP64, "mixed": bh.BGPU_MIXED}
 
-    prec = {"fp64": bh.BGPU_FP64, "mixed": bh.BGPU_MIXED}.get(args.precision, bh.BGPU_FP64)
-    bh.set_precision(prec)
     solver = bh.BhmSolver()
     solver.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
     x = solver.incenters()
@@ -248,58 +273,66 @@ def run_ours(args, rank, world, local_rank):
     b = torch.empty_like(b0)
     s = torch.cuda.ExternalStream(bh.lib().bgpu_stream(), device=dev)
 
-    def step():
-        solver.build(eps=1e-10, direct=1 if prec == bh.BGPU_FP64 else 0, ndef=st.ndef, gdef=gdef, comp=st.icomp,
-                     xmu=xmu)
+    def step(prec):
+        solver.build(eps=1e-10, direct=1 if prec == "fp64" else 0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
         with torch.cuda.stream(s):
             b.copy_(b0)
         solver.solve_device(b.data_ptr(), 6, n3)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    bh.kernel_stats(enable=1)
-    sampler = ClockSampler(local_rank)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    ev = []
-    launches0 = bh.launch_count()
-    t_wall0 = time.perf_counter()
-    for k in range(args.steps):
-        flush.zero_()
+    def timed(prec, warmup, steps, stats_kernel=None, clocks=False):
+        """Device ms per solve (CUDA events on the library's stream, L2 flushed before each step)."""
+        bh.set_precision(modes[prec])
+        for _ in range(warmup):
+            step(prec)
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        step()
-        e1.record(s)
-        ev.append((e0, e1))
-    torch.cuda.synchronize()
-    t_wall = time.perf_counter() - t_wall0
-    launches = bh.launch_count() - launches0
-    clocks = sampler.stop()
-    step_ms = [a.elapsed_time(c) for a, c in ev]
-    gl, gms, gflop = bh.kernel_stats(enable=0)
-    stage = bh.timings()
-    ms = sum(step_ms) / len(step_ms)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+        if stats_kernel is not None:
+            bh.kernel_stats(stats_kernel, enable=1)
+        sampler = ClockSampler(local_rank) if clocks else None
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        ev, stages = [], []
+        launches0 = bh.launch_count()
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            step(prec)
+            e1.record(s)
+            ev.append((e0, e1))
+            stages.append(bh.timings())
+        torch.cuda.synchronize()
+        launches = bh.launch_count() - launches0
+        clk = sampler.stop() if sampler else None
+        step_ms = [a.elapsed_time(c) for a, c in ev]
+        kst = bh.kernel_stats(stats_kernel, enable=0) if stats_kernel is not None else None
+        ms = max_over_ranks(sum(step_ms) / len(step_ms))
+        st_ms = {k: round(float(np.mean([d[k] for d in stages])), 3) for k in ("assemble", "factor", "solve")}
+        return dict(ms=ms, step_ms=step_ms, launches=launches, clocks=clk, kstats=kst, stages_ms=st_ms,
+                    refine_iters=stages[-1]["refine_iters"], relres=stages[-1]["relres"])
 
-    # the solution's tensors (host post-processing, not timed) for the record
-    sol = np.asfortranarray(b.T.cpu().numpy())
-    tens = bh.difco(x, st.area, sol)
-    tr = bh.traces(tens)
+    head = args.precision
+    head_kernel = bh.BGPU_KERNEL_TC_GEMM if head == "mixed" else bh.BGPU_KERNEL_LU_GEMM64
+    H = timed(head, args.warmup, args.steps, stats_kernel=head_kernel, clocks=True)
+    acc_head = tensors_of(solver, x, st, bh)
 
-    # e2e through the C ABI with host buffers
+    # the plain FP64 path beside the mixed one: its time per solve and its tensors (the reference
+    # for the mixed path's errors)
+    F = acc_fp64 = None
+    if head == "mixed" and not args.no_fp64:
+        F = timed("fp64", 1, max(1, min(args.steps, 2)))
+        acc_fp64 = tensors_of(solver, x, st, bh)
+
+    # e2e through the C ABI with host buffers (create ... solve, copies included)
+    bh.set_precision(modes[head])
     e2e = []
     h2d = 8 * (12 * n + 3 * n + len(gdef)) + (4 * n if st.ndef > 1 else 0) + 8 * 6 * n3
     d2h = 8 * (4 * n + 1 + 6 * n3)
     B_host = bh.rhs6(x)
-    for k in range(0 if args.no_e2e else max(1, args.steps)):
+    for _ in range(0 if args.no_e2e else max(1, args.steps)):
         solver.destroy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -307,15 +340,11 @@ def run_ours(args, rank, world, local_rank):
         xe = solver.incenters()
         dme = solver.diag_mean()
         xmu_e, gdef_e = st.deflation(dme)
-        solver.build(eps=1e-10, direct=1 if prec == bh.BGPU_FP64 else 0, ndef=st.ndef, gdef=gdef_e, comp=st.icomp,
+        solver.build(eps=1e-10, direct=1 if head == "fp64" else 0, ndef=st.ndef, gdef=gdef_e, comp=st.icomp,
                      xmu=xmu_e)
         solver.solve(B_host)
         e2e.append(time.perf_counter() - t0)
-    e2e_s = float(np.median(e2e)) if e2e else float("nan")
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(float(np.median(e2e))) if e2e else float("nan")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -324,30 +353,52 @@ def run_ours(args, rank, world, local_rank):
                "parts_s": {k: parts[k] for k in ("assembly_s", "lu_s", "solve_s")}}
 
     if rank == 0:
-        gemm_avg_ms = gms / max(gl, 1)
-        achieved = (gflop / max(gl, 1)) / (gemm_avg_ms * 1e-3) / 1e12 if gl else None
+        gl, gms, gflop = H["kstats"]
+        achieved = (gflop / max(gl, 1)) / (gms / max(gl, 1) * 1e-3) / 1e12 if gl else None
+        if head == "mixed":
+            peak = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+            roof = {"kernel": "k_gemm_bf16_tc (tcgen05.mma kind::f16, TMA, TMEM accumulators): every update of "
+                              "the mixed LU", "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": (achieved / peak) if achieved else None, "traffic": None,
+                    "peak_source": f"{peak_src} bf16 sustained (MEASURED_PEAKS.json; the GEMM runs inside a long step)",
+                    "traffic_note": "launch shapes vary from 128x128x128 to 30720^3; per-shape DRAM bytes of "
+                                    "captured launches in profiles/"}
+        else:
+            p64 = fp64_peak_tflops(torch, dev)
+            roof = {"kernel": "FP64 LU trailing-update GEMM (mma.sync f64, k_dgemm_nn_minus)", "bound": "tensor",
+                    "achieved": achieved, "peak": p64, "unit": "TFLOP/s", "frac": (achieved / p64) if achieved else None,
+                    "traffic": None,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)"}
+        roof.update(launches_per_step=gl / max(args.steps, 1), share_of_step=gms / max(sum(H["step_ms"]), 1e-9))
+        accuracy = None
+        if acc_fp64 is not None:
+            accuracy = {"vs": "plain FP64 GPU path (partial-pivoting LU), same mesh, 11 RHS",
+                        "D_t": relerr(acc_head["D_t"], acc_fp64["D_t"]), "D_r": relerr(acc_head["D_r"], acc_fp64["D_r"]),
+                        "eta": relerr(acc_head["chiprime"], acc_fp64["chiprime"]),
+                        "Dtt_tensor": relerr(acc_head["Dtt"], acc_fp64["Dtt"]),
+                        "Drr_tensor": relerr(acc_head["Drr"], acc_fp64["Drr"]), "bar": 1e-8,
+                        "refine_iterations": H["refine_iters"], "relres": H["relres"]}
         line = {
-            "metric": "s per BEST solve (assemble+LU+6 RHS)", "value": ms / 1e3 / world, "unit": "s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if prec == bh.BGPU_FP64 else "f32/f64-refined", "data": "synthetic",
-            "config": {"workload": args.workload, "N": n, "order": n3, "desc": w["desc"],
-                       "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "metric": METRIC,
+            "value": H["ms"] / 1e3 / world, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": H["ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if head == "fp64" else "bf16 LU (f32 accumulate) + f64 refinement", "data": "synthetic",
+            "config": {"workload": args.workload, "N": n, "order": n3, "desc": w["desc"], "precision": head,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB write) between timed steps; GR is 72 N^2 bytes, far above L2",
-                       "stages_ms": {k: round(v, 3) for k, v in stage.items() if k in ("assemble", "factor", "solve")},
-                       "wall_s": t_wall},
-            "roofline": {"kernel": "FP64 LU trailing-update GEMM (mma.sync f64, k_dgemm_nn_minus)", "bound": "tensor",
-                         "achieved": achieved, "peak": p64, "unit": "TFLOP/s",
-                         "frac": (achieved / p64) if achieved else None, "traffic": None,
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                         "launches_per_step": gl / max(args.steps, 1), "share_of_step": gms / max(sum(step_ms), 1e-9)},
-            "clocks": clocks,
+                       "stages_ms": H["stages_ms"]},
+            "roofline": roof,
+            "clocks": H["clocks"],
             "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches,
-            "result": {"D_t_cm2_s": tr["DTRANS"], "D_r_1_s": tr["DR"]},
+            "gpu_launches": H["launches"],
+            "fp64_path": None if F is None else {"value": F["ms"] / 1e3, "unit": "s", "steps": len(F["step_ms"]),
+                                                 "warmup": 1, "stages_ms": F["stages_ms"],
+                                                 "speedup_mixed_vs_fp64": F["ms"] / H["ms"]},
+            "accuracy": accuracy,
+            "result": {"D_t_cm2_s": acc_head["D_t"], "D_r_1_s": acc_head["D_r"], "chiprime": acc_head["chiprime"]},
             "cpu_baseline": cpu,
             "peaks": {"source": peak_src, "hbm_gbs": peaks.get("hbm_gbs"), "bf16_tflops": peaks.get("bf16_tflops"),
-                      "fp64_tflops_cublas": p64},
+                      "bf16_tflops_sustained": peaks.get("bf16_tflops_sustained")},
         }
         print(json.dumps(line), flush=True)
     solver.destroy()
@@ -363,7 +414,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="star_f32", choices=list(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="the timed path (mixed: its FP64 comparison runs beside it)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     args = ap.parse_args()

@@ -271,6 +271,7 @@ def best_run(path, iarea=1, cg_zero=0, ivisco=0, icov=0, wm=0.0, precision=-1):
 
 
 BGPU_KERNEL_LU_GEMM64 = 0
+BGPU_KERNEL_TC_GEMM = 1
 
 
 def kernel_stats(kernel=BGPU_KERNEL_LU_GEMM64, enable=1):

@@ -591,17 +591,18 @@ unsigned long long bgpu_launch_count(void) { return g_launches; }
 
 int bgpu_kernel_stats(int kernel, int enable, int* launches, double* ms, double* work) {
   return guarded([&] {
-    if (kernel != BGPU_KERNEL_LU_GEMM64) {
+    if (kernel < 0 || kernel >= kTimedKernels) {
       say("error: unknown kernel id %d", kernel);
       return 1;
     }
     int l = 0;
     double t = 0, w = 0;
-    lu_gemm_timer_read(&l, &t, &w);
+    KernelTimer& kt = kernel_timer(kernel);
+    kt.read(&l, &t, &w);
     if (launches) *launches = l;
     if (ms) *ms = t;
     if (work) *work = w;
-    lu_gemm_timer_enable(enable != 0);
+    kt.enable(enable != 0);
     return 0;
   });
 }

@@ -7,6 +7,8 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <utility>
+#include <vector>
 
 namespace bgpu {
 
@@ -46,6 +48,22 @@ struct DevDeflation {
   const double* xmu = nullptr;
 };
 
+// Opt-in live timing of one kernel's launches: CUDA events recorded around each launch on its
+// stream, summed on read (bgpu_kernel_stats).  Ids as in best_gpu.h (BGPU_KERNEL_*).
+struct KernelTimer {
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  size_t used = 0;
+  double work = 0;
+  void begin(cudaStream_t s);
+  void end(cudaStream_t s, double w);
+  void enable(bool v);
+  // launches recorded, their summed device time (ms) and work, then reset (synchronises)
+  void read(int* launches, double* ms, double* w);
+};
+constexpr int kTimedKernels = 2;
+KernelTimer& kernel_timer(int id);
+
 // Queues a message for bhm_log_line (api.cpp).
 void log_message(const char* msg);
 
@@ -71,9 +89,6 @@ size_t lu_scratch_bytes(int n);
 // DevStatus.  Host-side errors return a cudaError_t.
 cudaError_t lu64_getrf(double* A, long lda, int n, int* ipiv, int* d_info, int* d_status, const LuScratch& ws,
                        cudaStream_t s);
-// Opt-in CUDA-event timing of the LU's trailing-update GEMM launches.
-void lu_gemm_timer_enable(bool on);
-void lu_gemm_timer_read(int* launches, double* ms, double* flops);
 // C(m x n) -= A(m x k) B(k x n), all column-major (FP64 tensor-core path).
 cudaError_t dgemm_nn_minus(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C,
                            long ldc, cudaStream_t s);

@@ -540,52 +540,52 @@ cudaError_t panel(const Ctx& c, int k, int w) {
   return laswp(c, k, k + w1, k + w1, k + w);
 }
 
-// Live timing of the trailing-update GEMM launches (opt-in; for the roofline report).
-struct GemmTimer {
-  bool on = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
-  size_t used = 0;
-  double flops = 0;
-  void begin(cudaStream_t s) {
-    if (!on) return;
-    if (used == ev.size()) {
-      cudaEvent_t a, b;
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      ev.emplace_back(a, b);
-    }
-    cudaEventRecord(ev[used].first, s);
-  }
-  void end(cudaStream_t s, double f) {
-    if (!on) return;
-    cudaEventRecord(ev[used].second, s);
-    ++used;
-    flops += f;
-  }
-} g_gemm_timer;
-
 }  // namespace
 
-void lu_gemm_timer_enable(bool on) {
-  g_gemm_timer.on = on;
-  g_gemm_timer.used = 0;
-  g_gemm_timer.flops = 0;
+// Live timing of kernel launches (opt-in; for the roofline report).
+
+void KernelTimer::begin(cudaStream_t s) {
+  if (!on) return;
+  if (used == ev.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    ev.emplace_back(a, b);
+  }
+  cudaEventRecord(ev[used].first, s);
 }
 
-// Sums the recorded launches (synchronising on the last one) and resets the counters.
-void lu_gemm_timer_read(int* launches, double* ms, double* flops) {
+void KernelTimer::end(cudaStream_t s, double w) {
+  if (!on) return;
+  cudaEventRecord(ev[used].second, s);
+  ++used;
+  work += w;
+}
+
+void KernelTimer::enable(bool v) {
+  on = v;
+  used = 0;
+  work = 0;
+}
+
+void KernelTimer::read(int* launches, double* ms, double* w) {
   double t = 0;
-  if (g_gemm_timer.used) cudaEventSynchronize(g_gemm_timer.ev[g_gemm_timer.used - 1].second);
-  for (size_t i = 0; i < g_gemm_timer.used; ++i) {
+  if (used) cudaEventSynchronize(ev[used - 1].second);
+  for (size_t i = 0; i < used; ++i) {
     float x = 0;
-    cudaEventElapsedTime(&x, g_gemm_timer.ev[i].first, g_gemm_timer.ev[i].second);
+    cudaEventElapsedTime(&x, ev[i].first, ev[i].second);
     t += x;
   }
-  *launches = (int)g_gemm_timer.used;
+  *launches = (int)used;
   *ms = t;
-  *flops = g_gemm_timer.flops;
-  g_gemm_timer.used = 0;
-  g_gemm_timer.flops = 0;
+  *w = work;
+  used = 0;
+  work = 0;
+}
+
+KernelTimer& kernel_timer(int id) {
+  static KernelTimer timers[kTimedKernels];
+  return timers[id < 0 || id >= kTimedKernels ? 0 : id];
 }
 
 size_t lu_scratch_bytes(int) { return LeafScratchLayout::kEnd; }
@@ -615,12 +615,12 @@ cudaError_t lu64_getrf(double* A, long lda, int n, int* ipiv, int* d_info, int* 
       if ((e = trsm_lower_unit(A + k + (size_t)k * lda, lda, kb, A + k + (size_t)(k + kb) * lda, n - k - kb, s)) !=
           cudaSuccess)
         return e;
-      g_gemm_timer.begin(s);
+      kernel_timer(0).begin(s);
       if ((e = gemm_minus(n - k - kb, n - k - kb, kb, A + (k + kb) + (size_t)k * lda, lda,
                           A + k + (size_t)(k + kb) * lda, lda, A + (k + kb) + (size_t)(k + kb) * lda, lda, s)) !=
           cudaSuccess)
         return e;
-      g_gemm_timer.end(s, 2.0 * (double)(n - k - kb) * (double)(n - k - kb) * kb);
+      kernel_timer(0).end(s, 2.0 * (double)(n - k - kb) * (double)(n - k - kb) * kb);
     }
   }
   return cudaSuccess;

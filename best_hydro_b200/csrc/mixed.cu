@@ -440,7 +440,10 @@ struct MixedSolver::Impl {
     ck(cast_bf16(B, ldb, k, n, bt.p, op_ld, s), "cast B");
     prof.end(s);
     prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
+    KernelTimer& kt = kernel_timer(1);
+    kt.begin(s);
     ck(gemm_bf16_tc_minus_maps(m, n, k, map_a, map_b, C, ldc, d_status(), s), "tensor-core GEMM");
+    kt.end(s, 2.0 * m * n * k);
     prof.end(s);
   }
 
@@ -602,7 +605,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
   ck(launch_assemble(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
   ck(cudaEventRecord(ev_assembled, s), "event");
-  if (P.prof.on) {
+  if (P.prof.on || kernel_timer(1).on) {
     P.rlu(0, P.n3, s);  // direct launches, each timed
   } else {
     // the recursion's launches depend only on the order and the buffers: capture them once as a

@@ -1,0 +1,79 @@
+"""Single-kernel cases for profiling (one warm-up launch, then the launch to capture).
+
+    python -m best_hydro_b200.kernel_cases tc_gemm M N K     # C -= A B, BF16 tcgen05 (FP32 C)
+    python -m best_hydro_b200.kernel_cases dgemm M N K       # C -= A B, FP64 DMMA
+    python -m best_hydro_b200.kernel_cases assemble F        # GR of the ellipsoid at geodesic frequency F
+    python -m best_hydro_b200.kernel_cases mixed F           # mixed build + solve, ellipsoid frequency F
+
+Each case launches its kernel twice (the second launch is the one to capture: `ncu -k <kernel>
+-s 1 -c 1`) and prints the CUDA-event time of the second launch.
+"""
+import sys
+
+
+def _ev(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def main(argv):
+    import torch
+
+    import best_hydro_b200 as bh
+    case = argv[0]
+    dev = torch.device("cuda", 0)
+    if case in ("tc_gemm", "dgemm"):
+        m, n, k = (int(v) for v in argv[1:4])
+        dt = torch.float32 if case == "tc_gemm" else torch.float64
+        g = torch.Generator(device=dev).manual_seed(0)
+        a = torch.randn(k, m, dtype=dt, device=dev, generator=g)  # a[j] = column j: column-major m x k
+        b = torch.randn(n, k, dtype=dt, device=dev, generator=g)
+        c = torch.randn(n, m, dtype=dt, device=dev, generator=g)
+        fn = bh.gemm_bf16_minus_device if case == "tc_gemm" else bh.dgemm_minus_device
+        times = []
+        for _ in range(2):
+            e0, e1 = _ev(torch)
+            torch.cuda.synchronize()
+            e0.record()
+            fn(m, n, k, a.data_ptr(), m, b.data_ptr(), k, c.data_ptr(), m)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        print(f"{case} {m}x{n}x{k}: {times[-1]:.3f} ms (including the BF16 casts)" if case == "tc_gemm" else
+              f"{case} {m}x{n}x{k}: {times[-1]:.3f} ms, {2.0 * m * n * k / times[-1] / 1e9:.1f} TFLOP/s")
+        return 0
+    if case in ("assemble", "mixed"):
+        f = int(argv[1])
+        from best_hydro_b200 import meshes
+        tri, ta, tv = meshes.ellipsoid(f)
+        st = bh.Setup(tri, 1, ta)
+        s = bh.BhmSolver()
+        s.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        n3 = 3 * st.n
+        if case == "assemble":
+            out = torch.empty((n3, n3), dtype=torch.float64, device=dev)
+            for _ in range(2):
+                e0, e1 = _ev(torch)
+                torch.cuda.synchronize()
+                e0.record()
+                bh.assemble_device(0, st.n, 0, st.n, out.data_ptr(), n3)
+                e1.record()
+                torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            print(f"assemble N={st.n}: {ms:.3f} ms, {st.n * (st.n - 1) / ms / 1e6:.3f} Gpairs/s")
+            return 0
+        x = s.incenters()
+        xmu, gdef = st.deflation(s.diag_mean())
+        bh.set_precision(bh.BGPU_MIXED)
+        for _ in range(2):
+            s.build(eps=1e-10, direct=0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+            s.solve(bh.rhs6(x))
+        t = bh.timings()
+        print(f"mixed N={st.n}: factor {t['factor']:.2f} ms, solve {t['solve']:.2f} ms, "
+              f"{int(t['refine_iters'])} iterations, residual {t['relres']:.2e}")
+        return 0
+    print(__doc__)
+    return 2
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

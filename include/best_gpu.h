@@ -86,10 +86,14 @@ int bgpu_assemble_device(int r0, int r1, int c0, int c1, double *d_out, int ldo)
 unsigned long long bgpu_launch_count(void);
 
 /* Kernels whose launches can be timed live (CUDA events on the library's stream). */
-enum { BGPU_KERNEL_LU_GEMM64 = 0 /* the FP64 LU's trailing-update GEMM (DMMA) */ };
+enum {
+  BGPU_KERNEL_LU_GEMM64 = 0, /* the FP64 LU's trailing-update GEMM (DMMA) */
+  BGPU_KERNEL_TC_GEMM = 1    /* the mixed LU's tcgen05 BF16 GEMM (every update of the factorisation) */
+};
 
 /* Returns, for `kernel`, the launches recorded since the last call, their summed device time (ms) and
- * their algorithmic work (flops), then turns recording on (enable = 1) or off (0). */
+ * their algorithmic work (flops), then turns recording on (enable = 1) or off (0).  While the mixed
+ * LU's GEMM is recorded, its factorisation is launched directly instead of replayed from its graph. */
 int bgpu_kernel_stats(int kernel, int enable, int *launches, double *ms, double *work);
 
 #ifdef __cplusplus
