@@ -42,12 +42,18 @@ WORKLOADS = {
     "ellipsoid_f16": dict(desc="ellipsoid 30/20/12 A, geodesic f=16, normal jitter U(+-2%) seed 0", N=5120,
                           iarea=1, gen=("ellipsoid", 16)),
     "icosphere_l3": dict(desc="icosphere level 3, R=20 A", N=1280, iarea=1, gen=("icosphere", 3)),
+    # BASELINE batching configuration: the ellipsoid at eight geodesic frequencies, solved as one series
+    "ellipsoid_series": dict(desc="ellipsoid 30/20/12 A, normal jitter U(+-2%) seed 0, geodesic f = 11, 12, 14, "
+                                  "16, 18, 20, 22, 23 (one series, FP64)", N=49080, iarea=1,
+                             gen=("series", (11, 12, 14, 16, 18, 20, 22, 23))),
 }
 
 
 def make_mesh(name):
     from best_hydro_b200 import meshes
     kind, arg = WORKLOADS[name]["gen"]
+    if kind == "series":
+        return [meshes.ellipsoid(f) for f in arg]
     if kind == "star":
         return meshes.star(arg)
     if kind == "ellipsoid":
@@ -407,6 +413,81 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_series(args, rank, world, local_rank):
+    """The series workload: every mesh assembled, factored (FP64) and solved for 11 right-hand sides
+    through bgpu_series_* (one CUDA graph per build), against the same meshes solved one after the
+    other through the single-mesh seam; results and their 1/N extrapolation."""
+    import torch
+    import best_hydro_b200 as bh
+
+    torch.cuda.set_device(local_rank)
+    w = WORKLOADS[args.workload]
+    setups = [bh.Setup(tri, w["iarea"], ta) for tri, ta, tv in make_mesh(args.workload)]
+    bh.set_precision(bh.BGPU_FP64)
+    S = bh.Series()
+    S.create(setups)
+    xs = S.incenters()
+    defl = []
+    for st, dm in zip(setups, S.diag_means()):
+        xmu, gdef = st.deflation(dm)
+        defl.append((st.ndef, gdef, st.icomp, xmu))
+    rhs = [np.hstack([bh.rhs6(x), bh.strain5(x)]) for x in xs]
+    S.build(defl, tune=1)  # tuning pass + first graph build (warm-up)
+    tune_ms = S.timings()["tune"]
+    for _ in range(max(0, args.warmup - 1)):
+        S.build(defl)
+    launches0 = bh.launch_count()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S.build(defl)
+        sols = S.solve(rhs)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    launches = bh.launch_count() - launches0
+    dev_ms = S.timings()
+    # the same meshes one after the other through the single-mesh seam
+    seq, seq_sols = [], []
+    for k in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        out = []
+        for st in setups:
+            s1 = bh.BhmSolver()
+            s1.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+            x = s1.incenters()
+            xmu, gdef = st.deflation(s1.diag_mean())
+            s1.build(eps=1e-10, direct=1, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+            out.append(s1.solve(np.hstack([bh.rhs6(x), bh.strain5(x)])))
+            s1.destroy()
+        seq.append(time.perf_counter() - t0)
+        seq_sols = out
+    same = all(np.array_equal(a.view(np.int64), b.view(np.int64)) for a, b in zip(sols, seq_sols))
+    per = []
+    for st, x, B in zip(setups, xs, sols):
+        tr = bh.traces(bh.difco(x, st.area, B[:, :6]))
+        chip, _ = bh.visco(x, st.area, B[:, 6:], B[:, :6])
+        per.append(dict(N=st.n, D_t=tr["DTRANS"], D_r=tr["DR"], chiprime=chip))
+    ns = [d["N"] for d in per]
+    ext = {k: bh.extrapolate(ns, [d[k] for d in per])[0] for k in ("D_t", "D_r", "chiprime")}
+    v = float(np.median(times))
+    line = {
+        "metric": "s per series solve (8 meshes: assemble + FP64 LU + 11 RHS each)", "value": v, "unit": "s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "N": ns, "desc": w["desc"]},
+        "device_ms": {"build_graph": dev_ms["build"], "solve": dev_ms["solve"], "tuning_pass": tune_ms},
+        "sequential_single_solves_s": float(np.median(seq)), "speedup_vs_sequential": float(np.median(seq)) / v,
+        "bitwise_equal_to_single_solves": bool(same), "clocks": clocks, "gpu_launches": launches,
+        "per_mesh": per, "extrapolated_1_over_N": ext, "autotune": bh.autotune_table(),
+    }
+    S.destroy()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,6 +506,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if WORKLOADS[args.workload]["gen"][0] == "series":
+        run_series(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 

@@ -60,6 +60,14 @@ _SIGS = {
                                                    ctypes.c_int]),
     "bgpu_assemble_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_int]),
+    "bgpu_series_create": (ctypes.c_int, [ctypes.c_int, _ip, _dp, _dp, _dp, _dp, _dp, ctypes.c_double]),
+    "bgpu_series_incenters": (ctypes.c_int, [_dp]),
+    "bgpu_series_diag_mean": (ctypes.c_int, [_dp]),
+    "bgpu_series_build": (ctypes.c_int, [_ip, _dp, _ip, _dp, ctypes.c_int]),
+    "bgpu_series_solve": (ctypes.c_int, [ctypes.c_int, _dp]),
+    "bgpu_series_timings": (ctypes.c_int, [_dp, ctypes.c_int]),
+    "bgpu_series_destroy": (None, []),
+    "bgpu_autotune_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "bgpu_launch_count": (ctypes.c_ulonglong, []),
     "bgpu_kernel_stats": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, _dp, _dp]),
     # include/best_driver.h: BEST's host side around the seam
@@ -72,6 +80,7 @@ _SIGS = {
     "bgpu_best_difco": (ctypes.c_int, [ctypes.c_int, _dp, _dp, ctypes.c_double, _dp, _dp]),
     "bgpu_best_visco": (ctypes.c_int, [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]),
     "bgpu_best_traces": (None, [_dp, _dp]),
+    "bgpu_best_extrapolate": (ctypes.c_double, [ctypes.c_int, _ip, _dp, _dp]),
     "bgpu_best_run": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_double, ctypes.c_int, _dp]),
 }
@@ -272,6 +281,120 @@ def best_run(path, iarea=1, cg_zero=0, ivisco=0, icov=0, wm=0.0, precision=-1):
 
 BGPU_KERNEL_LU_GEMM64 = 0
 BGPU_KERNEL_TC_GEMM = 1
+
+
+def extrapolate(n, y):
+    """bgpu_best_extrapolate: (value at 1/N -> 0, slope) of the least-squares line y = y0 + slope / N."""
+    n = np.ascontiguousarray(n, dtype=np.int32)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    slope = ctypes.c_double()
+    y0 = lib().bgpu_best_extrapolate(int(n.size), n.ctypes.data_as(_ip), _p(y), ctypes.byref(slope))
+    return float(y0), slope.value
+
+
+class Series:
+    """A series of meshes solved together (include/best_gpu.h, bgpu_series_*): one assembly launch,
+    a batched FP64 LU replayed from one CUDA graph, and per-mesh results equal to single solves."""
+
+    def __init__(self):
+        self.L = lib()
+        self.n = None
+
+    def create(self, setups, cg=1.0):
+        """setups: Setup objects (one per mesh, BEST's set-up already applied)."""
+        self.setups = list(setups)
+        self.n = np.array([st.n for st in self.setups], dtype=np.int32)
+        v1 = np.concatenate([st.v1 for st in self.setups])
+        v2 = np.concatenate([st.v2 for st in self.setups])
+        v3 = np.concatenate([st.v3 for st in self.setups])
+        area = np.concatenate([st.area for st in self.setups])
+        afac = np.array([st.afac for st in self.setups], dtype=np.float64)
+        _check(self.L.bgpu_series_create(len(self.setups), self.n.ctypes.data_as(_ip), _p(v1), _p(v2), _p(v3),
+                                         _p(area), _p(afac), float(cg)), "bgpu_series_create")
+
+    def _split(self, a, per):
+        out, o = [], 0
+        for k in self.n:
+            out.append(a[o:o + per * int(k)])
+            o += per * int(k)
+        return out
+
+    def incenters(self):
+        x = np.empty(3 * int(self.n.sum()))
+        _check(self.L.bgpu_series_incenters(_p(x)), "bgpu_series_incenters")
+        return self._split(x, 3)
+
+    def diag_means(self):
+        dm = np.empty(self.n.size)
+        _check(self.L.bgpu_series_diag_mean(_p(dm)), "bgpu_series_diag_mean")
+        return dm
+
+    def build(self, deflations, tune=0):
+        """deflations: (ndef, gdef, comp, xmu) per mesh."""
+        ndef = np.array([d[0] for d in deflations], dtype=np.int32)
+        gdef = np.concatenate([np.asarray(d[1], dtype=np.float64)[:max(0, int(d[0]))] for d in deflations])
+        comp = np.concatenate([np.asarray(d[2], dtype=np.int32) for d in deflations])
+        xmu = np.concatenate([np.asarray(d[3], dtype=np.float64) for d in deflations])
+        gdef = np.ascontiguousarray(gdef if gdef.size else np.zeros(1))
+        _check(self.L.bgpu_series_build(ndef.ctypes.data_as(_ip), _p(gdef), comp.ctypes.data_as(_ip), _p(xmu),
+                                        int(tune)), "bgpu_series_build")
+
+    def solve(self, blocks):
+        """blocks: one 3 n_i x nrhs array per mesh (same nrhs); returns the solutions likewise."""
+        nrhs = blocks[0].shape[1]
+        b = np.concatenate([np.asfortranarray(x, dtype=np.float64).ravel(order="F") for x in blocks])
+        _check(self.L.bgpu_series_solve(int(nrhs), _p(b)), "bgpu_series_solve")
+        out, o = [], 0
+        for k in self.n:
+            m = 3 * int(k) * nrhs
+            out.append(b[o:o + m].reshape((3 * int(k), nrhs), order="F"))
+            o += m
+        return out
+
+    def timings(self):
+        v = np.zeros(4)
+        self.L.bgpu_series_timings(_p(v), 4)
+        return dict(zip(("build", "assemble", "solve", "tune"), v.tolist()))
+
+    def destroy(self):
+        self.L.bgpu_series_destroy()
+
+
+def autotune_table():
+    """The DGEMM autotuner's choices (bgpu_autotune_table), one line per size class."""
+    k = lib().bgpu_autotune_table(None, 0)
+    buf = ctypes.create_string_buffer(k + 1)
+    lib().bgpu_autotune_table(buf, k + 1)
+    return [ln for ln in buf.value.decode().split("\n") if ln]
+
+
+def series_run(setups, tune=0, ivisco=1, cg=1.0):
+    """BEST on every mesh of a series through bgpu_series_*: per mesh D_t, D_r, CHI' (11 right-hand
+    sides with ivisco), then their linear extrapolation in 1/N.  Returns (per-mesh list, extrapolated)."""
+    S = Series()
+    S.create(setups, cg)
+    xs = S.incenters()
+    dms = S.diag_means()
+    defl = []
+    for st, dm in zip(setups, dms):
+        xmu, gdef = st.deflation(dm)
+        defl.append((st.ndef, gdef, st.icomp, xmu))
+    S.build(defl, tune=tune)
+    rhs = [np.hstack([rhs6(x), strain5(x)]) if ivisco else rhs6(x) for x in xs]
+    sols = S.solve(rhs)
+    per = []
+    for st, x, B in zip(setups, xs, sols):
+        t = difco(x, st.area, B[:, :6], cg)
+        tr = traces(t)
+        d = dict(N=st.n, D_t=tr["DTRANS"], D_r=tr["DR"], tensors=t, solution=B)
+        if ivisco:
+            d["chiprime"], _ = visco(x, st.area, B[:, 6:], B[:, :6], 0, cg)
+        per.append(d)
+    n = [d["N"] for d in per]
+    ext = {k: extrapolate(n, [d[k] for d in per])[0] for k in (("D_t", "D_r", "chiprime") if ivisco else ("D_t", "D_r"))}
+    timings = S.timings()
+    S.destroy()
+    return per, ext, timings
 
 
 def kernel_stats(kernel=BGPU_KERNEL_LU_GEMM64, enable=1):

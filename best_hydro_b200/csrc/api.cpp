@@ -143,7 +143,10 @@ struct Runtime {
   void ensure_trsv(int n) { trsv_scratch.ensure(trsv_scratch_bytes(n), "solve scratch", true); }
   float elapsed(int a, int b) {
     float t = 0.f;
-    cudaEventElapsedTime(&t, ev[a], ev[b]);
+    if (cudaEventElapsedTime(&t, ev[a], ev[b]) != cudaSuccess) {
+      cudaGetLastError();
+      t = 0.f;
+    }
     return t;
   }
 };
@@ -258,6 +261,99 @@ void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
   r.ms[3] = r.elapsed(6, 7);
 }
 
+// host mesh arrays (v1, v2, v3: n x 3 column-major; area) in the device layout, kGeoStride per triangle
+std::vector<double> geo_host(int n, const double* v1, const double* v2, const double* v3, const double* area) {
+  std::vector<double> h((size_t)n * kGeoStride, 0.0);
+  for (int t = 0; t < n; ++t) {
+    for (int c = 0; c < 3; ++c) {
+      h[(size_t)t * kGeoStride + c] = v1[(size_t)c * n + t];
+      h[(size_t)t * kGeoStride + 3 + c] = v2[(size_t)c * n + t];
+      h[(size_t)t * kGeoStride + 6 + c] = v3[(size_t)c * n + t];
+    }
+    h[(size_t)t * kGeoStride + 9] = area[t];
+  }
+  return h;
+}
+
+// A series of meshes of one body (BEST's workflow of results extrapolated in 1/N, best/best.f:154-157),
+// assembled, factored (FP64, partial pivoting) and solved together.  Mesh i's arrays sit in
+// concatenated buffers from triangle t0[i]; its GR (order 3 n_i, leading dimension ld[i]) from gr0[i].
+struct Series {
+  int count = 0;
+  double cg = 1.0;
+  std::vector<int> n;
+  std::vector<long> t0;        // first triangle of each mesh
+  std::vector<double> afac;
+  std::vector<double> x_host;  // incenters: mesh i's n_i x 3 column-major block at 3 t0[i]
+  DevBuf geo, xc, self9, diag;
+  std::vector<int> ndef;
+  std::vector<long> gdef0;     // first deflation weight of each mesh
+  DevBuf gdef, comp, xmu;
+  std::vector<long> ld;
+  std::vector<size_t> gr0, inv0;
+  DevBuf gr, ipiv, perm, dl, du, info, rhs;
+  cudaGraphExec_t graph = nullptr;  // assembly + LU + permutations + diagonal inverses of the series
+  unsigned long long graph_kernels = 0;
+  bool graph_tried = false, factored = false;
+  double ms[4] = {};  // build (graph), of which assembly; last solve; tuning pass
+  ~Series() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
+  DevMesh mesh(int i) const {
+    DevMesh m;
+    m.n = n[i];
+    m.cg = cg;
+    m.afac = afac[i];
+    m.geo = geo.as<double>() + (size_t)t0[i] * kGeoStride;
+    m.xc = xc.as<double>() + (size_t)t0[i] * kXcStride;
+    m.self9 = self9.as<double>() + (size_t)t0[i] * 9;
+    return m;
+  }
+  long rows() const { return 3 * (t0[count - 1] + n[count - 1]); }
+};
+
+std::unique_ptr<Series> g_series;
+
+Series& series() {
+  if (!g_series) throw std::runtime_error("bgpu_series_create has not been called");
+  return *g_series;
+}
+
+// every device step of a series build, on stream st (run directly, or captured into the graph);
+// ev_assembled (direct runs only) is recorded after the assembly
+void series_record(Series& S, Runtime& r, cudaStream_t st, cudaEvent_t ev_assembled = nullptr) {
+  SeriesAssembly sa;
+  sa.count = S.count;
+  for (int i = 0; i < S.count; ++i) {
+    sa.mesh[i] = S.mesh(i);
+    DevDeflation d;
+    if (S.ndef[i] >= 1) {
+      d.ndef = S.ndef[i];
+      d.gdef = S.gdef.as<double>() + S.gdef0[i];
+      d.xmu = S.xmu.as<double>() + 3 * S.t0[i];
+      if (S.ndef[i] > 1) d.comp = S.comp.as<int>() + S.t0[i];
+    }
+    sa.defl[i] = d;
+    sa.out[i] = S.gr.as<double>() + S.gr0[i];
+    sa.ld[i] = S.ld[i];
+  }
+  ck(launch_assemble_series(sa, st), "series assembly");
+  if (ev_assembled) ck(cudaEventRecord(ev_assembled, st), "event");
+  std::vector<LuItem> items(S.count);
+  for (int i = 0; i < S.count; ++i)
+    items[i] = LuItem{S.gr.as<double>() + S.gr0[i], S.ld[i], 3 * S.n[i], S.ipiv.as<int>() + 3 * S.t0[i],
+                      S.info.as<int>() + i};
+  LuScratch ws{r.lu_scratch.p, r.lu_scratch.bytes};
+  ck(lu64_getrf_batch(items.data(), S.count, r.status.as<int>(), ws, st), "series LU");
+  for (int i = 0; i < S.count; ++i) {
+    const int n3 = 3 * S.n[i];
+    ck(lu_perm_from_ipiv(S.ipiv.as<int>() + 3 * S.t0[i], n3, S.perm.as<int>() + 3 * S.t0[i], st), "permutation");
+    ck(diag_inverses64(S.gr.as<double>() + S.gr0[i], S.ld[i], n3, S.dl.as<double>() + S.inv0[i],
+                       S.du.as<double>() + S.inv0[i], st),
+       "diagonal inverses");
+  }
+}
+
 }  // namespace
 
 void log_message(const char* msg) { g_log.emplace_back(msg); }
@@ -289,14 +385,7 @@ int bhm_create(int n, const double* v1, const double* v2, const double* v3, cons
     s->n = n;
     s->afac = afac;
     s->cg = cg;
-    std::vector<double> h((size_t)n * kGeoStride, 0.0);
-    for (int t = 0; t < n; ++t)
-      for (int c = 0; c < 3; ++c) {
-        h[(size_t)t * kGeoStride + c] = v1[(size_t)c * n + t];
-        h[(size_t)t * kGeoStride + 3 + c] = v2[(size_t)c * n + t];
-        h[(size_t)t * kGeoStride + 6 + c] = v3[(size_t)c * n + t];
-      }
-    for (int t = 0; t < n; ++t) h[(size_t)t * kGeoStride + 9] = area[t];
+    std::vector<double> h = geo_host(n, v1, v2, v3, area);
     s->geo.ensure(h.size() * sizeof(double), "mesh");
     s->xc.ensure((size_t)n * kXcStride * sizeof(double), "incenters");
     s->self9.ensure((size_t)n * 9 * sizeof(double), "self blocks");
@@ -506,6 +595,257 @@ int bgpu_set_refinement(int max_restarts, int krylov) {
   return 0;
 }
 
+int bgpu_series_create(int count, const int* n, const double* v1, const double* v2, const double* v3,
+                       const double* area, const double* afac, double cg) {
+  return guarded([&] {
+    if (count < 1 || count > kMaxSeries) {
+      say("error: bgpu_series_create: %d meshes (1 to %d)", count, kMaxSeries);
+      return 1;
+    }
+    for (int i = 0; i < count; ++i)
+      if (n[i] < 1) {
+        say("error: bgpu_series_create: mesh %d has no triangles", i);
+        return 1;
+      }
+    Runtime& r = rt();
+    g_series.reset();
+    auto S = std::make_unique<Series>();
+    S->count = count;
+    S->cg = cg;
+    long tot = 0;
+    for (int i = 0; i < count; ++i) {
+      S->n.push_back(n[i]);
+      S->t0.push_back(tot);
+      S->afac.push_back(afac[i]);
+      tot += n[i];
+    }
+    std::vector<double> h;
+    h.reserve((size_t)tot * kGeoStride);
+    for (int i = 0; i < count; ++i) {
+      const long o = S->t0[i];
+      std::vector<double> g = geo_host(n[i], v1 + 3 * o, v2 + 3 * o, v3 + 3 * o, area + o);
+      h.insert(h.end(), g.begin(), g.end());
+    }
+    S->geo.ensure(h.size() * sizeof(double), "series meshes");
+    S->xc.ensure((size_t)tot * kXcStride * sizeof(double), "series incenters");
+    S->self9.ensure((size_t)tot * 9 * sizeof(double), "series self blocks");
+    S->diag.ensure(sizeof(double) * count, "series diagonal means");
+    ck(cudaMemcpyAsync(S->geo.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, r.stream), "mesh copy");
+    for (int i = 0; i < count; ++i) {
+      ck(launch_self_blocks(S->mesh(i), r.stream), "self blocks");
+      ck(launch_diag_mean(S->mesh(i), S->diag.as<double>() + i, r.stream), "diagonal mean");
+    }
+    std::vector<double> xc((size_t)tot * kXcStride);
+    ck(cudaMemcpyAsync(xc.data(), S->xc.p, xc.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream),
+       "incenter copy");
+    r.sync("bgpu_series_create");
+    S->x_host.resize((size_t)3 * tot);
+    for (int i = 0; i < count; ++i)
+      for (int t = 0; t < n[i]; ++t)
+        for (int c = 0; c < 3; ++c)
+          S->x_host[3 * S->t0[i] + (size_t)c * n[i] + t] = xc[(size_t)(S->t0[i] + t) * kXcStride + c];
+    g_series = std::move(S);
+    return 0;
+  });
+}
+
+int bgpu_series_incenters(double* x) {
+  return guarded([&] {
+    Series& S = series();
+    std::memcpy(x, S.x_host.data(), S.x_host.size() * sizeof(double));
+    return 0;
+  });
+}
+
+int bgpu_series_diag_mean(double* dm) {
+  return guarded([&] {
+    Series& S = series();
+    Runtime& r = rt();
+    ck(cudaMemcpyAsync(dm, S.diag.p, sizeof(double) * S.count, cudaMemcpyDeviceToHost, r.stream), "diag copy");
+    r.sync("bgpu_series_diag_mean");
+    return 0;
+  });
+}
+
+int bgpu_series_build(const int* ndef, const double* gdef, const int* comp, const double* xmu, int tune) {
+  return guarded([&] {
+    Series& S = series();
+    Runtime& r = rt();
+    S.factored = false;
+    const long tot = S.t0[S.count - 1] + S.n[S.count - 1];
+    // deflation data
+    S.ndef.assign(ndef, ndef + S.count);
+    S.gdef0.clear();
+    long ng = 0;
+    bool any_comp = false;
+    for (int i = 0; i < S.count; ++i) {
+      S.gdef0.push_back(ng);
+      ng += std::max(0, S.ndef[i]);
+      any_comp = any_comp || S.ndef[i] > 1;
+    }
+    if (ng > 0) {
+      S.gdef.ensure(sizeof(double) * ng, "deflation weights");
+      S.xmu.ensure(sizeof(double) * 3 * tot, "deflation vectors");
+      ck(cudaMemcpyAsync(S.gdef.p, gdef, sizeof(double) * ng, cudaMemcpyHostToDevice, r.stream), "gdef copy");
+      ck(cudaMemcpyAsync(S.xmu.p, xmu, sizeof(double) * 3 * tot, cudaMemcpyHostToDevice, r.stream), "xmu copy");
+    }
+    if (any_comp) {
+      S.comp.ensure(sizeof(int) * tot, "surface labels");
+      ck(cudaMemcpyAsync(S.comp.p, comp, sizeof(int) * tot, cudaMemcpyHostToDevice, r.stream), "comp copy");
+    }
+    // matrices and factors
+    if (S.gr0.empty()) {
+      size_t g0 = 0, i0 = 0;
+      for (int i = 0; i < S.count; ++i) {
+        const int n3 = 3 * S.n[i];
+        S.ld.push_back(padded_ld(n3));
+        S.gr0.push_back(g0);
+        S.inv0.push_back(i0);
+        g0 += (size_t)S.ld[i] * n3;
+        i0 += diag_inverse_elems(n3);
+      }
+      S.gr.ensure(g0 * sizeof(double), "series GR (FP64)");
+      S.dl.ensure(i0 * sizeof(double), "diagonal-block inverses (L)");
+      S.du.ensure(i0 * sizeof(double), "diagonal-block inverses (U)");
+      S.ipiv.ensure(sizeof(int) * 3 * tot, "pivots");
+      S.perm.ensure(sizeof(int) * 3 * tot, "permutations");
+      S.info.ensure(sizeof(int) * kMaxSeries, "info", true);
+    }
+    ck(lu_prepare(), "LU kernel attributes");
+    if (tune) {
+      // a first build with the DGEMM autotuner on (direct launches; the result is overwritten below)
+      ck(cudaEventRecord(r.ev[0], r.stream), "event");
+      lu_autotune(true);
+      try {
+        series_record(S, r, r.stream, r.ev[3]);
+      } catch (...) {
+        lu_autotune(false);
+        throw;
+      }
+      lu_autotune(false);
+      ck(cudaEventRecord(r.ev[1], r.stream), "event");
+      r.check_status("series tuning");
+      S.ms[3] = r.elapsed(0, 1);
+      S.ms[1] = r.elapsed(0, 3);
+      std::string table = lu_autotune_table();
+      size_t a = 0;
+      while (a < table.size()) {
+        size_t b = table.find('\n', a);
+        if (b == std::string::npos) b = table.size();
+        say("autotune: %s", table.substr(a, b - a).c_str());
+        a = b + 1;
+      }
+      if (S.graph) {  // shapes may have changed: capture again
+        cudaGraphExecDestroy(S.graph);
+        S.graph = nullptr;
+        S.graph_tried = false;
+      }
+    }
+    if (!S.graph && !S.graph_tried) {
+      S.graph_tried = true;
+      cudaStream_t cs;
+      ck(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+      cudaGraph_t gph = nullptr;
+      const unsigned long long launches0 = g_launches;
+      bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      std::string why;
+      if (ok) {
+        try {
+          series_record(S, r, cs);
+        } catch (const std::exception& e) {
+          why = e.what();
+          ok = false;
+        }
+        if (cudaStreamEndCapture(cs, &gph) != cudaSuccess) ok = false;
+      }
+      const unsigned long long captured = g_launches - launches0;
+      g_launches = launches0;
+      if (ok && gph && cudaGraphInstantiate(&S.graph, gph, 0) == cudaSuccess) {
+        S.graph_kernels = captured;
+      } else {
+        S.graph = nullptr;
+        say("series: graph capture unavailable (%s); launching directly", why.empty() ? "capture failed" : why.c_str());
+      }
+      if (gph) cudaGraphDestroy(gph);
+      cudaGetLastError();
+      cudaStreamDestroy(cs);
+    }
+    ck(cudaEventRecord(r.ev[2], r.stream), "event");
+    if (S.graph) {
+      ck(cudaGraphLaunch(S.graph, r.stream), "series graph");
+      g_launches += S.graph_kernels;
+    } else {
+      series_record(S, r, r.stream, r.ev[3]);
+    }
+    ck(cudaEventRecord(r.ev[4], r.stream), "event");
+    r.check_status("bgpu_series_build");
+    S.ms[0] = r.elapsed(2, 4);
+    if (!S.graph) S.ms[1] = r.elapsed(2, 3);
+    std::vector<int> info(S.count);
+    ck(cudaMemcpy(info.data(), S.info.p, sizeof(int) * S.count, cudaMemcpyDeviceToHost), "info read");
+    for (int i = 0; i < S.count; ++i)
+      if (info[i] > 0) {
+        say("error: series mesh %d: the LU factorisation found U(%d,%d) = 0: GR is singular", i, info[i], info[i]);
+        return 1;
+      }
+    S.factored = true;
+    say("GPU series build: %d meshes (N = %d .. %d), %s, %.1f ms", S.count, *std::min_element(S.n.begin(), S.n.end()),
+        *std::max_element(S.n.begin(), S.n.end()), S.graph ? "one CUDA graph" : "direct launches", S.ms[0]);
+    return 0;
+  });
+}
+
+int bgpu_series_solve(int nrhs, double* b) {
+  return guarded([&] {
+    Series& S = series();
+    Runtime& r = rt();
+    if (!S.factored) throw std::runtime_error("bgpu_series_build has not factored the series");
+    if (nrhs <= 0) return 0;
+    const long rows = S.rows();
+    S.rhs.ensure((size_t)rows * nrhs * sizeof(double), "series right-hand sides");
+    ck(cudaMemcpyAsync(S.rhs.p, b, (size_t)rows * nrhs * sizeof(double), cudaMemcpyHostToDevice, r.stream), "b copy");
+    ck(cudaEventRecord(r.ev[5], r.stream), "event");
+    long maxn = 0;
+    for (int i = 0; i < S.count; ++i) maxn = std::max<long>(maxn, 3L * S.n[i]);
+    r.ensure_trsv((int)maxn);
+    for (int i = 0; i < S.count; ++i) {
+      const int n3 = 3 * S.n[i];
+      double* bi = S.rhs.as<double>() + (size_t)3 * S.t0[i] * nrhs;
+      for (int c = 0; c < nrhs; c += 16) {
+        const int q = std::min(16, nrhs - c);
+        ck(getrs64_inv(S.gr.as<double>() + S.gr0[i], S.ld[i], S.dl.as<double>() + S.inv0[i],
+                       S.du.as<double>() + S.inv0[i], n3, S.perm.as<int>() + 3 * S.t0[i], bi + (size_t)c * n3, n3, q,
+                       r.trsv_scratch.p, r.status.as<int>(), r.stream),
+           "series solve");
+      }
+      ck(check_finite(bi, n3, n3, nrhs, r.status.as<int>(), r.stream), "finite check");
+    }
+    ck(cudaEventRecord(r.ev[6], r.stream), "event");
+    ck(cudaMemcpyAsync(b, S.rhs.p, (size_t)rows * nrhs * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "x copy");
+    r.check_status("bgpu_series_solve");
+    S.ms[2] = r.elapsed(5, 6);
+    return 0;
+  });
+}
+
+int bgpu_series_timings(double* ms, int len) {
+  if (!g_series) return 0;
+  const int k = std::min(len, 4);
+  for (int i = 0; i < k; ++i) ms[i] = g_series->ms[i];
+  return k;
+}
+
+void bgpu_series_destroy(void) { g_series.reset(); }
+
+int bgpu_autotune_table(char* buf, int len) {
+  const std::string t = lu_autotune_table();
+  if (len <= 0) return (int)t.size();
+  const int k = std::min<int>(len - 1, (int)t.size());
+  std::memcpy(buf, t.data(), k);
+  buf[k] = 0;
+  return (int)t.size();
+}
+
 int bgpu_timings(double* ms, int len) {
   if (!g_rt) return 0;
   double v[7] = {g_rt->ms[0], g_rt->ms[1], g_rt->ms[2], g_rt->ms[3], g_rt->ms[4], g_solve_info[0], g_solve_info[1]};
@@ -619,7 +959,10 @@ int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float* d_a, int lda, 
     ck(cudaEventRecord(r.ev[6], r.stream), "event");
     ck(cast_transpose_bf16(d_a, lda, m, k, at.p, lt, r.stream), "cast A");
     ck(cast_bf16(d_b, ldb, k, n, bt.p, lt, r.stream), "cast B");
+    KernelTimer& kt = kernel_timer(BGPU_KERNEL_TC_GEMM);
+    kt.begin(r.stream);
     ck(gemm_bf16_tc_minus(m, n, k, at.p, lt, bt.p, lt, d_c, ldc, r.status.as<int>(), r.stream), "tensor-core GEMM");
+    kt.end(r.stream, 2.0 * m * n * (double)k);
     ck(cudaEventRecord(r.ev[7], r.stream), "event");
     r.check_status("tensor-core GEMM");
     r.ms[3] = r.elapsed(6, 7);

@@ -15,6 +15,7 @@
 //                   shared memory with their target-independent differences and dot products.
 //                   best/triangleint.f:1-247 (kernel.cpp:148-249); epilogue: the deflation term of
 //                   best/best.f:406-425 and an optional FP32 copy for the mixed-precision LU.
+//   k_assemble_series  the same tiles for every mesh of a series (up to 16) in one launch
 //   k_diag_mean     best/best.f:401-403, summed in BEST's order (one thread: the order is the spec).
 #include <cuda_runtime.h>
 
@@ -26,6 +27,9 @@ namespace {
 
 constexpr double kPi = 3.1415926535897932385;  // tgetgr.f:17
 constexpr int kTgtTile = 128;                   // targets per block (threads)
+#ifndef BGPU_ASM_MIN_BLOCKS
+#define BGPU_ASM_MIN_BLOCKS 4                   // resident blocks per SM the register budget allows
+#endif
 constexpr int kSrcTile = 16;                    // source triangles per block
 
 // 21-point Gauss-Legendre abscissae and weights on [0,1]: the decimal literals of
@@ -144,17 +148,17 @@ __global__ void k_self_blocks(int n, const double* __restrict__ geo, double afac
     }
 }
 
-__global__ void __launch_bounds__(kTgtTile) k_assemble(int n, const double* __restrict__ geo,
-                                                       const double* __restrict__ xc,
-                                                       const double* __restrict__ self9, double cg, int r0, int r1,
-                                                       int c0, int c1, double* __restrict__ out, long ld,
-                                                       DevDeflation defl, float* __restrict__ out32, long ld32) {
+// One tile: targets [r0 + 128 bx, +128) x sources [c0 + 16 by, +16) of one mesh.
+__device__ __forceinline__ void assemble_tile(int bx, int by, const double* __restrict__ geo,
+                                              const double* __restrict__ xc, const double* __restrict__ self9,
+                                              double cg, int r0, int r1, int c0, int c1, double* __restrict__ out,
+                                              long ld, const DevDeflation& defl, float* __restrict__ out32, long ld32) {
   __shared__ double s_p[kSrcTile][9];     // p1, p2, p3
   __shared__ double s_v[kSrcTile][9];     // v21, v31, v32
   __shared__ double s_d[kSrcTile][8];     // d2121 d2131 d2132 d3131 d3232 d3231 s21 area
   __shared__ int s_comp[kSrcTile];
 
-  const int sbase = c0 + blockIdx.y * kSrcTile;
+  const int sbase = c0 + by * kSrcTile;
   const int ns = min(kSrcTile, c1 - sbase);
   if (threadIdx.x < ns) {
     const int t = sbase + threadIdx.x;
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(kTgtTile) k_assemble(int n, const double* __re
   }
   __syncthreads();
 
-  const int n1 = r0 + blockIdx.x * kTgtTile + threadIdx.x;
+  const int n1 = r0 + bx * kTgtTile + threadIdx.x;
   if (n1 >= r1) return;
   const double xcx = xc[(size_t)n1 * kXcStride + 0];
   const double xcy = xc[(size_t)n1 * kXcStride + 1];
@@ -331,6 +335,25 @@ __global__ void __launch_bounds__(kTgtTile) k_assemble(int n, const double* __re
   }
 }
 
+__global__ void __launch_bounds__(kTgtTile, BGPU_ASM_MIN_BLOCKS)
+    k_assemble(const double* __restrict__ geo, const double* __restrict__ xc, const double* __restrict__ self9,
+               double cg, int r0, int r1, int c0, int c1, double* __restrict__ out, long ld, DevDeflation defl,
+               float* __restrict__ out32, long ld32) {
+  assemble_tile(blockIdx.x, blockIdx.y, geo, xc, self9, cg, r0, r1, c0, c1, out, ld, defl, out32, ld32);
+}
+
+// Every mesh of a series in one launch: block b belongs to the mesh whose tile range holds it.
+__global__ void __launch_bounds__(kTgtTile, BGPU_ASM_MIN_BLOCKS) k_assemble_series(const __grid_constant__ SeriesAssembly sa) {
+  const int b = blockIdx.x;
+  int i = 0;
+  while (i + 1 < sa.count && b >= sa.tile0[i + 1]) ++i;
+  const int local = b - sa.tile0[i];
+  const int tx = (sa.mesh[i].n + kTgtTile - 1) / kTgtTile;
+  const DevMesh& m = sa.mesh[i];
+  assemble_tile(local % tx, local / tx, m.geo, m.xc, m.self9, m.cg, 0, m.n, 0, m.n, sa.out[i], sa.ld[i], sa.defl[i],
+                nullptr, 0);
+}
+
 __global__ void k_diag_mean(int n, const double* __restrict__ self9, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double s = 0.0;
@@ -361,7 +384,22 @@ cudaError_t launch_assemble(const DevMesh& m, int r0, int r1, int c0, int c1, do
     }
     return cudaSuccess;
   }
-  k_assemble<<<grid, kTgtTile, 0, s>>>(m.n, m.geo, m.xc, m.self9, m.cg, r0, r1, c0, c1, out, ld, defl, out32, ld32);
+  k_assemble<<<grid, kTgtTile, 0, s>>>(m.geo, m.xc, m.self9, m.cg, r0, r1, c0, c1, out, ld, defl, out32, ld32);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_assemble_series(const SeriesAssembly& sa, cudaStream_t s) {
+  if (sa.count <= 0) return cudaSuccess;
+  SeriesAssembly a = sa;
+  long total = 0;
+  for (int i = 0; i < a.count; ++i) {
+    a.tile0[i] = (int)total;
+    const long tx = (a.mesh[i].n + kTgtTile - 1) / kTgtTile, ty = (a.mesh[i].n + kSrcTile - 1) / kSrcTile;
+    total += tx * ty;
+  }
+  if (total > 0x7fffffffL) return cudaErrorInvalidValue;
+  k_assemble_series<<<(unsigned)total, kTgtTile, 0, s>>>(a);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }

@@ -74,6 +74,17 @@ cudaError_t launch_self_blocks(const DevMesh& m, cudaStream_t s);
 // a single-precision copy (rounded to nearest) is written too (leading dimension ld32).
 cudaError_t launch_assemble(const DevMesh& m, int r0, int r1, int c0, int c1, double* out, long ld,
                             const DevDeflation& defl, float* out32, long ld32, cudaStream_t s);
+// Every mesh of a series at once (whole GR of each, with its deflation): mesh i into out[i] (ld[i]).
+constexpr int kMaxSeries = 16;
+struct SeriesAssembly {
+  int count = 0;
+  DevMesh mesh[kMaxSeries];
+  DevDeflation defl[kMaxSeries];
+  double* out[kMaxSeries] = {};
+  long ld[kMaxSeries] = {};
+  int tile0[kMaxSeries] = {};  // (filled by the launcher)
+};
+cudaError_t launch_assemble_series(const SeriesAssembly& sa, cudaStream_t s);
 // BEST's mean of GR's diagonal (best/best.f:401-403), summed in BEST's order, into *d_out.
 cudaError_t launch_diag_mean(const DevMesh& m, double* d_out, cudaStream_t s);
 
@@ -89,6 +100,23 @@ size_t lu_scratch_bytes(int n);
 // DevStatus.  Host-side errors return a cudaError_t.
 cudaError_t lu64_getrf(double* A, long lda, int n, int* ipiv, int* d_info, int* d_status, const LuScratch& ws,
                        cudaStream_t s);
+// The same on up to 16 independent matrices at once: each step's leaves, interchanges, triangular
+// solves and updates of all matrices run as one launch each (the matrices' results are those of
+// factoring each alone).
+struct LuItem {
+  double* A;
+  long lda;
+  int n;
+  int* ipiv;  // device, n entries
+  int* info;  // device, one int
+};
+cudaError_t lu64_getrf_batch(const LuItem* items, int count, int* d_status, const LuScratch& ws, cudaStream_t s);
+// DGEMM tile-shape autotuner: on = tune the shapes of new GEMM sizes as they are met (outside stream
+// capture); the table of choices as text.
+void lu_autotune(bool on);
+std::string lu_autotune_table();
+// kernel attributes of the LU, once, before any stream capture
+cudaError_t lu_prepare();
 // C(m x n) -= A(m x k) B(k x n), all column-major (FP64 tensor-core path).
 cudaError_t dgemm_nn_minus(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C,
                            long ldc, cudaStream_t s);
@@ -111,6 +139,9 @@ cudaError_t diag_inverses64(const double* LU, long lda, int n, double* DL, doubl
 cudaError_t diag_inverses32(const float* LU, long lda, int n, int b0, int nb, float* DL, float* DU, cudaStream_t s);
 cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
                         double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s);
+// dgetrs('T'): X := A^-T X with the same factors (the adjoint solve).
+cudaError_t getrs64_trans_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
+                              double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s);
 cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, double* Y, long ldy,
                           int nrhs, void* scratch, int* d_status, cudaStream_t s);
 // Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -126,19 +127,25 @@ void compon(int n, const double* v1, const double* v2, const double* v3, int* ic
   *nopen = open;
 }
 
+inline double re(double x) { return x; }
+inline double re(const std::complex<double>& x) { return x.real(); }
+
 // best/matin3.f: inverse of a 3x3 by Crout LU with implicit scaling.  a[i][j] = A(i+1, j+1).
-int matin3(const Mat3 A, Mat3 Y) {
-  double a[3][3];
-  std::memcpy(a, A, sizeof a);
+// T is double, or std::complex<double> for complex-step derivatives (pivoting on the real parts).
+template <class T>
+int matin3_t(const T A[3][3], T Y[3][3]) {
+  T a[3][3];
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) Y[i][j] = (i == j) ? 1.0 : 0.0;
+    for (int j = 0; j < 3; ++j) a[i][j] = A[i][j];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Y[i][j] = (i == j) ? T(1.0) : T(0.0);
   const int n = 3;
   double vv[3];
   int ierr = 0;
   for (int i = 0; i < n; ++i) {
     double aamax = 0.0;
     for (int j = 0; j < n; ++j)
-      if (std::fabs(a[i][j]) > aamax) aamax = std::fabs(a[i][j]);
+      if (std::fabs(re(a[i][j])) > aamax) aamax = std::fabs(re(a[i][j]));
     if (aamax == 0.0) {
       ierr = 1;
       aamax = 1.0;
@@ -149,7 +156,7 @@ int matin3(const Mat3 A, Mat3 Y) {
   int indx[3] = {0, 0, 0}, imax = 0;
   for (int j = 0; j < n; ++j) {
     for (int i = 0; i < j; ++i) {
-      double s = a[i][j];
+      T s = a[i][j];
       if (i > 0) {
         for (int k = 0; k < i; ++k) s = s - a[i][k] * a[k][j];
         a[i][j] = s;
@@ -157,12 +164,12 @@ int matin3(const Mat3 A, Mat3 Y) {
     }
     double aamax = 0.0;
     for (int i = j; i < n; ++i) {
-      double s = a[i][j];
+      T s = a[i][j];
       if (j > 0) {
         for (int k = 0; k < j; ++k) s = s - a[i][k] * a[k][j];
         a[i][j] = s;
       }
-      const double dum = vv[i] * std::fabs(s);
+      const double dum = vv[i] * std::fabs(re(s));
       if (dum >= aamax) {
         imax = i;
         aamax = dum;
@@ -174,28 +181,28 @@ int matin3(const Mat3 A, Mat3 Y) {
     }
     indx[j] = imax;
     if (j != n - 1) {
-      if (a[j][j] == 0.0) a[j][j] = 1e-20;
-      const double dum = 1.0 / a[j][j];
+      if (re(a[j][j]) == 0.0) a[j][j] = 1e-20;
+      const T dum = 1.0 / a[j][j];
       for (int i = j + 1; i < n; ++i) a[i][j] = a[i][j] * dum;
     }
   }
-  if (a[n - 1][n - 1] == 0.0) a[n - 1][n - 1] = 1e-20;
+  if (re(a[n - 1][n - 1]) == 0.0) a[n - 1][n - 1] = 1e-20;
   for (int col = 0; col < n; ++col) {
-    double b[3] = {Y[0][col], Y[1][col], Y[2][col]};
+    T b[3] = {Y[0][col], Y[1][col], Y[2][col]};
     int ii = -1;
     for (int i = 0; i < n; ++i) {
       const int ll = indx[i];
-      double s = b[ll];
+      T s = b[ll];
       b[ll] = b[i];
       if (ii != -1) {
         for (int j = ii; j < i; ++j) s = s - a[i][j] * b[j];
-      } else if (s != 0.0) {
+      } else if (re(s) != 0.0) {
         ii = i;
       }
       b[i] = s;
     }
     for (int i = n - 1; i >= 0; --i) {
-      double s = b[i];
+      T s = b[i];
       for (int j = i + 1; j < n; ++j) s = s - a[i][j] * b[j];
       b[i] = s / a[i][i];
     }
@@ -203,6 +210,8 @@ int matin3(const Mat3 A, Mat3 Y) {
   }
   return 0;
 }
+
+int matin3(const Mat3 A, Mat3 Y) { return matin3_t<double>(A, Y); }
 
 void antisym(const double u[3], Mat3 uu) {
   uu[2][0] = -u[1];
@@ -286,6 +295,132 @@ void jacobi3(const Mat3 A, double d[3]) {
 }
 
 }  // namespace
+
+template <class T>
+void antisym_t(const T u[3], T uu[3][3]) {
+  uu[2][0] = -u[1];
+  uu[2][1] = u[0];
+  uu[0][1] = -u[2];
+  uu[1][0] = -uu[0][1];
+  uu[1][2] = -uu[2][1];
+  uu[0][2] = -uu[2][0];
+  uu[0][0] = uu[1][1] = uu[2][2] = T(0.0);
+}
+
+// best/difco.f:104-401 from the four raw friction blocks (Ktt, Ktr, Krt, Krr, as summed in
+// difco.f:53-103): the centre of resistance, the diffusion tensors and the centre of diffusion.  T is
+// double, or std::complex<double> for complex-step derivatives.  out as bgpu_best_difco's.
+template <class T>
+void difco_post(T Ktt[3][3], T Ktr[3][3], T Krt[3][3], T Krr[3][3], double cg, T out[60]) {
+  T uu[3][3], aux[3][3];
+  uu[0][0] = Ktt[1][1] + Ktt[2][2];
+  uu[1][1] = Ktt[0][0] + Ktt[2][2];
+  uu[2][2] = Ktt[1][1] + Ktt[0][0];
+  uu[0][1] = -Ktt[0][1];
+  uu[0][2] = -Ktt[0][2];
+  uu[2][1] = -Ktt[1][2];
+  uu[1][0] = uu[0][1];
+  uu[1][2] = uu[2][1];
+  uu[2][0] = uu[0][2];
+  Krt[0][2] = (Krt[0][2] + Ktr[2][0]) * 0.5;
+  Krt[2][0] = (Krt[2][0] + Ktr[0][2]) * 0.5;
+  Krt[0][1] = (Krt[0][1] + Ktr[1][0]) * 0.5;
+  Krt[1][0] = (Krt[1][0] + Ktr[0][1]) * 0.5;
+  Krt[1][2] = (Krt[1][2] + Ktr[2][1]) * 0.5;
+  Krt[2][1] = (Krt[2][1] + Ktr[1][2]) * 0.5;
+  Krt[0][0] = (Krt[0][0] + Ktr[0][0]) * 0.5;
+  Krt[1][1] = (Krt[1][1] + Ktr[1][1]) * 0.5;
+  Krt[2][2] = (Krt[2][2] + Ktr[2][2]) * 0.5;
+  T sur1 = -Krt[2][1] + Krt[1][2];
+  T sur2 = -Krt[0][2] + Krt[2][0];
+  T sur3 = -Krt[1][0] + Krt[0][1];
+  matin3_t<T>(uu, aux);
+  T urc[3], udr[3];
+  for (int j = 0; j < 3; ++j) urc[j] = aux[j][0] * sur1 + aux[j][1] * sur2 + aux[j][2] * sur3;
+  antisym_t<T>(urc, uu);
+  T Krr2[3][3], Krt2[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      T temp = 0.0;
+      for (int k = 0; k < 3; ++k)
+        temp = temp + uu[i][k] * (Ktt[k][0] * uu[0][j] + Ktt[k][1] * uu[1][j] + Ktt[k][2] * uu[2][j]);
+      const T temp1 = Krt[0][i] * uu[0][j] + Krt[1][i] * uu[1][j] + Krt[2][i] * uu[2][j];
+      const T temp2 = uu[i][0] * Krt[0][j] + uu[i][1] * Krt[1][j] + uu[i][2] * Krt[2][j];
+      Krr2[i][j] = Krr[i][j] - temp + temp1 - temp2;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Krt2[i][j] = Krt[i][j] + Ktt[i][0] * uu[0][j] + Ktt[i][1] * uu[1][j] + Ktt[i][2] * uu[2][j];
+  T Kttinv[3][3], M[3][3], Drr[3][3], Dtr[3][3], Dtt[3][3];
+  matin3_t<T>(Ktt, Kttinv);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      T temp = 0.0;
+      for (int k = 0; k < 3; ++k)
+        temp = temp + Krt2[i][k] * (Kttinv[k][0] * Krt2[j][0] + Kttinv[k][1] * Krt2[j][1] + Kttinv[k][2] * Krt2[j][2]);
+      M[i][j] = Krr2[i][j] - temp;
+    }
+  matin3_t<T>(M, Drr);
+  if (cg == 0)
+    for (auto& r : Drr)
+      for (T& v : r) v = 4.0 * v / 3.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      T temp = 0.0;
+      for (int k = 0; k < 3; ++k)
+        temp = temp + Kttinv[i][k] * (Krt2[0][k] * Drr[0][j] + Krt2[1][k] * Drr[1][j] + Krt2[2][k] * Drr[2][j]);
+      Dtr[i][j] = -temp;
+      if (cg == 0) Dtr[i][j] = 4.0 * Dtr[i][j] / 3.0;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      T temp = 0.0;
+      for (int k = 0; k < 3; ++k)
+        temp = temp + Kttinv[i][k] * (Krt2[0][k] * Dtr[j][0] + Krt2[1][k] * Dtr[j][1] + Krt2[2][k] * Dtr[j][2]);
+      Dtt[i][j] = Kttinv[i][j] - temp;
+      if (cg == 0) Dtt[i][j] = 4.0 * Dtt[i][j] / 3.0;
+    }
+  uu[0][0] = Drr[1][1] + Drr[2][2];
+  uu[1][1] = Drr[0][0] + Drr[2][2];
+  uu[2][2] = Drr[1][1] + Drr[0][0];
+  uu[0][1] = -Drr[0][1];
+  uu[0][2] = -Drr[0][2];
+  uu[2][1] = -Drr[2][1];
+  uu[1][0] = uu[0][1];
+  uu[1][2] = uu[2][1];
+  uu[2][0] = uu[0][2];
+  sur1 = Dtr[2][1] - Dtr[1][2];
+  sur2 = Dtr[0][2] - Dtr[2][0];
+  sur3 = Dtr[1][0] - Dtr[0][1];
+  matin3_t<T>(uu, aux);
+  for (int j = 0; j < 3; ++j) udr[j] = aux[j][0] * sur1 + aux[j][1] * sur2 + aux[j][2] * sur3;
+  antisym_t<T>(udr, uu);
+  T Dtt2[3][3], Dtr2[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      T temp = 0.0;
+      for (int k = 0; k < 3; ++k)
+        temp = temp + uu[i][k] * Drr[k][0] * uu[0][j] + uu[i][k] * Drr[k][1] * uu[1][j] + uu[i][k] * Drr[k][2] * uu[2][j];
+      const T temp1 = Dtr[i][0] * uu[0][j] + Dtr[i][1] * uu[1][j] + Dtr[i][2] * uu[2][j];
+      const T temp2 = -uu[i][0] * Dtr[j][0] - uu[i][1] * Dtr[j][1] - uu[i][2] * Dtr[j][2];
+      Dtt2[i][j] = Dtt[i][j] - temp + temp1 + temp2;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Dtr2[i][j] = Dtr[i][j] - uu[i][0] * Drr[0][j] - uu[i][1] * Drr[1][j] - uu[i][2] * Drr[2][j];
+  auto put = [&](int off, const T m[3][3]) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out[off + 3 * i + j] = m[i][j];
+  };
+  put(0, Dtt2);
+  put(9, Dtr2);
+  put(18, Drr);
+  for (int j = 0; j < 3; ++j) {
+    out[27 + j] = urc[j];
+    out[30 + j] = udr[j];
+  }
+  put(33, Ktt);
+  put(42, Krt2);
+  put(51, Krr2);
+}
 
 extern "C" {
 
@@ -400,114 +535,7 @@ int bgpu_best_difco(int n, const double* x, const double* area, double cg, const
       }
     }
   }
-  Mat3 uu, aux;
-  uu[0][0] = Ktt[1][1] + Ktt[2][2];
-  uu[1][1] = Ktt[0][0] + Ktt[2][2];
-  uu[2][2] = Ktt[1][1] + Ktt[0][0];
-  uu[0][1] = -Ktt[0][1];
-  uu[0][2] = -Ktt[0][2];
-  uu[2][1] = -Ktt[1][2];
-  uu[1][0] = uu[0][1];
-  uu[1][2] = uu[2][1];
-  uu[2][0] = uu[0][2];
-  Krt[0][2] = (Krt[0][2] + Ktr[2][0]) * 0.5;
-  Krt[2][0] = (Krt[2][0] + Ktr[0][2]) * 0.5;
-  Krt[0][1] = (Krt[0][1] + Ktr[1][0]) * 0.5;
-  Krt[1][0] = (Krt[1][0] + Ktr[0][1]) * 0.5;
-  Krt[1][2] = (Krt[1][2] + Ktr[2][1]) * 0.5;
-  Krt[2][1] = (Krt[2][1] + Ktr[1][2]) * 0.5;
-  Krt[0][0] = (Krt[0][0] + Ktr[0][0]) * 0.5;
-  Krt[1][1] = (Krt[1][1] + Ktr[1][1]) * 0.5;
-  Krt[2][2] = (Krt[2][2] + Ktr[2][2]) * 0.5;
-  double sur1 = -Krt[2][1] + Krt[1][2];
-  double sur2 = -Krt[0][2] + Krt[2][0];
-  double sur3 = -Krt[1][0] + Krt[0][1];
-  matin3(uu, aux);
-  double urc[3], udr[3];
-  for (int j = 0; j < 3; ++j) urc[j] = aux[j][0] * sur1 + aux[j][1] * sur2 + aux[j][2] * sur3;
-  antisym(urc, uu);
-  Mat3 Krr2, Krt2;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double temp = 0.0;
-      for (int k = 0; k < 3; ++k)
-        temp = temp + uu[i][k] * (Ktt[k][0] * uu[0][j] + Ktt[k][1] * uu[1][j] + Ktt[k][2] * uu[2][j]);
-      const double temp1 = Krt[0][i] * uu[0][j] + Krt[1][i] * uu[1][j] + Krt[2][i] * uu[2][j];
-      const double temp2 = uu[i][0] * Krt[0][j] + uu[i][1] * Krt[1][j] + uu[i][2] * Krt[2][j];
-      Krr2[i][j] = Krr[i][j] - temp + temp1 - temp2;
-    }
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) Krt2[i][j] = Krt[i][j] + Ktt[i][0] * uu[0][j] + Ktt[i][1] * uu[1][j] + Ktt[i][2] * uu[2][j];
-  Mat3 Kttinv, M, Drr, Dtr, Dtt;
-  matin3(Ktt, Kttinv);
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double temp = 0.0;
-      for (int k = 0; k < 3; ++k)
-        temp = temp + Krt2[i][k] * (Kttinv[k][0] * Krt2[j][0] + Kttinv[k][1] * Krt2[j][1] + Kttinv[k][2] * Krt2[j][2]);
-      M[i][j] = Krr2[i][j] - temp;
-    }
-  matin3(M, Drr);
-  if (cg == 0)
-    for (auto& r : Drr)
-      for (double& v : r) v = 4.0 * v / 3.0;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double temp = 0.0;
-      for (int k = 0; k < 3; ++k)
-        temp = temp + Kttinv[i][k] * (Krt2[0][k] * Drr[0][j] + Krt2[1][k] * Drr[1][j] + Krt2[2][k] * Drr[2][j]);
-      Dtr[i][j] = -temp;
-      if (cg == 0) Dtr[i][j] = 4.0 * Dtr[i][j] / 3.0;
-    }
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double temp = 0.0;
-      for (int k = 0; k < 3; ++k)
-        temp = temp + Kttinv[i][k] * (Krt2[0][k] * Dtr[j][0] + Krt2[1][k] * Dtr[j][1] + Krt2[2][k] * Dtr[j][2]);
-      Dtt[i][j] = Kttinv[i][j] - temp;
-      if (cg == 0) Dtt[i][j] = 4.0 * Dtt[i][j] / 3.0;
-    }
-  uu[0][0] = Drr[1][1] + Drr[2][2];
-  uu[1][1] = Drr[0][0] + Drr[2][2];
-  uu[2][2] = Drr[1][1] + Drr[0][0];
-  uu[0][1] = -Drr[0][1];
-  uu[0][2] = -Drr[0][2];
-  uu[2][1] = -Drr[2][1];
-  uu[1][0] = uu[0][1];
-  uu[1][2] = uu[2][1];
-  uu[2][0] = uu[0][2];
-  sur1 = Dtr[2][1] - Dtr[1][2];
-  sur2 = Dtr[0][2] - Dtr[2][0];
-  sur3 = Dtr[1][0] - Dtr[0][1];
-  matin3(uu, aux);
-  for (int j = 0; j < 3; ++j) udr[j] = aux[j][0] * sur1 + aux[j][1] * sur2 + aux[j][2] * sur3;
-  antisym(udr, uu);
-  Mat3 Dtt2, Dtr2;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double temp = 0.0;
-      for (int k = 0; k < 3; ++k)
-        temp = temp + uu[i][k] * Drr[k][0] * uu[0][j] + uu[i][k] * Drr[k][1] * uu[1][j] + uu[i][k] * Drr[k][2] * uu[2][j];
-      const double temp1 = Dtr[i][0] * uu[0][j] + Dtr[i][1] * uu[1][j] + Dtr[i][2] * uu[2][j];
-      const double temp2 = -uu[i][0] * Dtr[j][0] - uu[i][1] * Dtr[j][1] - uu[i][2] * Dtr[j][2];
-      Dtt2[i][j] = Dtt[i][j] - temp + temp1 + temp2;
-    }
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) Dtr2[i][j] = Dtr[i][j] - uu[i][0] * Drr[0][j] - uu[i][1] * Drr[1][j] - uu[i][2] * Drr[2][j];
-  auto put = [&](int off, const Mat3 m) {
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) out[off + 3 * i + j] = m[i][j];
-  };
-  put(0, Dtt2);
-  put(9, Dtr2);
-  put(18, Drr);
-  for (int j = 0; j < 3; ++j) {
-    out[27 + j] = urc[j];
-    out[30 + j] = udr[j];
-  }
-  put(33, Ktt);
-  put(42, Krt2);
-  put(51, Krr2);
+  difco_post<double>(Ktt, Ktr, Krt, Krr, cg, out);
   return 0;
 }
 
@@ -637,6 +665,31 @@ void bgpu_best_traces(const double* tensors, double* out) {
   out[3] = runit * out[1];
 }
 
+
+// Least squares of y against 1/N (the reference gives no formula beyond "extrapolated linearly in
+// 1/N", README.md:12-16): centred sums, so that the intercept is not the difference of large terms.
+double bgpu_best_extrapolate(int count, const int* n, const double* y, double* slope) {
+  if (count < 2) {
+    if (slope) *slope = 0.0;
+    return count == 1 ? y[0] : 0.0;
+  }
+  double mx = 0.0, my = 0.0;
+  for (int i = 0; i < count; ++i) {
+    mx += 1.0 / n[i];
+    my += y[i];
+  }
+  mx /= count;
+  my /= count;
+  double sxx = 0.0, sxy = 0.0;
+  for (int i = 0; i < count; ++i) {
+    const double dx = 1.0 / n[i] - mx;
+    sxx += dx * dx;
+    sxy += dx * (y[i] - my);
+  }
+  const double b = sxx > 0.0 ? sxy / sxx : 0.0;
+  if (slope) *slope = b;
+  return my - b * mx;
+}
 
 }  // extern "C"
 

@@ -18,6 +18,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "bgpu_internal.h"
@@ -27,6 +30,10 @@ namespace bgpu {
 unsigned long long g_launches = 0;
 
 namespace {
+
+// The LU works on a batch of independent matrices at once (one matrix is a batch of one): every
+// kernel below takes per-matrix pointers and extents and finds its matrix from its block index.
+constexpr int kMaxBatch = 16;
 
 // ------------------------------------------------------------------------------------------
 // small PTX helpers
@@ -68,17 +75,38 @@ struct GemmCfg {
   static constexpr size_t kSmem = (size_t)STAGES * (kAStage + kBStage) * sizeof(double);
 };
 
+// A batch of independent products C_i -= A_i B_i with a common k (the same step of several LUs):
+// blockIdx.z selects the product; CTAs outside a product's tiles return at once.
+struct GemmItem {
+  const double* A;
+  const double* B;
+  double* C;
+  long lda, ldb, ldc;
+  int m, n;
+};
+struct GemmBatch {
+  int k;
+  int count;
+  GemmItem it[kMaxBatch];
+};
+
 template <int BM, int BN, int BK, int WM, int WN, int STAGES>
 __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::kThreads)
-    k_dgemm_nn_minus(int m, int n, int k, const double* __restrict__ A, long lda, const double* __restrict__ B,
-                     long ldb, double* __restrict__ C, long ldc) {
+    k_dgemm_nn_minus(const __grid_constant__ GemmBatch gb) {
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
   extern __shared__ __align__(16) double smem[];
+  const GemmItem& g = gb.it[blockIdx.z];
+  const int m = g.m, n = g.n, k = gb.k;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (m0 >= m || n0 >= n) return;
+  const double* __restrict__ A = g.A;
+  const double* __restrict__ B = g.B;
+  double* __restrict__ C = g.C;
+  const long lda = g.lda, ldb = g.ldb, ldc = g.ldc;
   double* As = smem;
   double* Bs = smem + STAGES * Cfg::kAStage;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm0 = (warp % Cfg::kWarpsM) * WM, wn0 = (warp / Cfg::kWarpsM) * WN;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int ktiles = (k + BK - 1) / BK;
 
   auto load_stage = [&](int stage, int kt) {
@@ -160,28 +188,157 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::kThreads)
   }
 }
 
-using GemmBig = GemmCfg<128, 128, 16, 32, 64, 4>;
-using GemmSmall = GemmCfg<64, 64, 16, 32, 32, 4>;
-
+// the kernel's shared-memory attribute, once (before any stream capture)
 template <int BM, int BN, int BK, int WM, int WN, int ST>
-cudaError_t run_gemm(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C, long ldc,
-                     cudaStream_t s) {
+cudaError_t gemm_attr() {
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, ST>;
   static bool attr_set = false;
-  auto kern = k_dgemm_nn_minus<BM, BN, BK, WM, WN, ST>;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_dgemm_nn_minus<BM, BN, BK, WM, WN, ST>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN);
-  kern<<<grid, Cfg::kThreads, Cfg::kSmem, s>>>(m, n, k, A, lda, B, ldb, C, ldc);
+  return cudaSuccess;
+}
+
+template <int BM, int BN, int BK, int WM, int WN, int ST>
+cudaError_t run_gemm(const GemmBatch& gb, cudaStream_t s) {
+  using Cfg = GemmCfg<BM, BN, BK, WM, WN, ST>;
+  auto kern = k_dgemm_nn_minus<BM, BN, BK, WM, WN, ST>;
+  cudaError_t e0 = gemm_attr<BM, BN, BK, WM, WN, ST>();
+  if (e0 != cudaSuccess) return e0;
+  int mm = 0, nn = 0;
+  for (int i = 0; i < gb.count; ++i) {
+    mm = std::max(mm, gb.it[i].m);
+    nn = std::max(nn, gb.it[i].n);
+  }
+  dim3 grid((mm + BM - 1) / BM, (nn + BN - 1) / BN, gb.count);
+  kern<<<grid, Cfg::kThreads, Cfg::kSmem, s>>>(gb);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
+// The DGEMM tile shapes the autotuner chooses from (all K steps of 16, 4 cp.async stages).
+enum GemmShape { kShapeBig = 0, kShapeSmall, kShapeTall, kShapeWide, kNumShapes };
+const char* const kShapeNames[kNumShapes] = {"128x128", "64x64", "128x64", "64x128"};
+
+cudaError_t run_shape(int shape, const GemmBatch& gb, cudaStream_t s) {
+  switch (shape) {
+    case kShapeBig: return run_gemm<128, 128, 16, 32, 64, 4>(gb, s);
+    case kShapeSmall: return run_gemm<64, 64, 16, 32, 32, 4>(gb, s);
+    case kShapeTall: return run_gemm<128, 64, 16, 32, 32, 4>(gb, s);
+    default: return run_gemm<64, 128, 16, 32, 64, 4>(gb, s);
+  }
+}
+
 // ------------------------------------------------------------------------------------------
-// Leaf panel factorisation: m x w (w <= 32), partial pivoting, cooperative over G CTAs
+// Autotuner of the DGEMM tile shape.  Key: (ceil log2 of the largest m, of the largest n, k, batch
+// count).  While tuning is on, the first product with a new key (outside stream capture) is split
+// into kNumShapes slices of its columns (or rows, when it is narrow), each computed with one shape
+// and timed with CUDA events; the fastest shape is kept for the key.  The product is still
+// computed exactly once, and the result does not depend on the shape (every shape accumulates each
+// entry over k in the same order), so tuning changes times only.  Untuned keys use the fixed rule
+// (128 x 64 when that gives at least one tile per SM, else 64 x 64; the tuner's choices on B200).
+// ------------------------------------------------------------------------------------------
+struct Tuner {
+  bool on = false;
+  std::map<unsigned long long, int> choice;
+  std::map<unsigned long long, std::vector<float>> times;
+  cudaEvent_t ev[kNumShapes + 1] = {};
+};
+Tuner& tuner() {
+  static Tuner t;
+  return t;
+}
+int ceil_log2(int v) {
+  int r = 0;
+  while ((1 << r) < v) ++r;
+  return r;
+}
+unsigned long long tune_key(int mm, int nn, int k, int count) {
+  return ((unsigned long long)ceil_log2(mm) << 40) | ((unsigned long long)ceil_log2(nn) << 32) |
+         ((unsigned long long)k << 8) | (unsigned long long)count;
+}
+
+bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &st);
+  return st != cudaStreamCaptureStatusNone;
+}
+
+cudaError_t gemm_batch(const GemmBatch& gb0, cudaStream_t s) {
+  GemmBatch gb;
+  gb.k = gb0.k;
+  gb.count = 0;
+  int mm = 0, nn = 0;
+  for (int i = 0; i < gb0.count; ++i)
+    if (gb0.it[i].m > 0 && gb0.it[i].n > 0) {
+      gb.it[gb.count++] = gb0.it[i];
+      mm = std::max(mm, gb0.it[i].m);
+      nn = std::max(nn, gb0.it[i].n);
+    }
+  if (gb.count == 0 || gb.k <= 0) return cudaSuccess;
+  Tuner& T = tuner();
+  const unsigned long long key = tune_key(mm, nn, gb.k, gb.count);
+  auto found = T.choice.find(key);
+  if (found != T.choice.end()) return run_shape(found->second, gb, s);
+  const bool by_cols = nn >= kNumShapes * 128, by_rows = !by_cols && mm >= kNumShapes * 128;
+  if (T.on && (by_cols || by_rows) && !capturing(s)) {
+    for (int q = 0; q <= kNumShapes; ++q)
+      if (!T.ev[q]) cudaEventCreate(&T.ev[q]);
+    cudaError_t e = cudaEventRecord(T.ev[0], s);
+    for (int sh = 0; sh < kNumShapes && e == cudaSuccess; ++sh) {
+      GemmBatch part = gb;
+      for (int i = 0; i < gb.count; ++i) {
+        GemmItem& it = part.it[i];
+        const int ext = by_cols ? it.n : it.m;
+        const int chunk = (ext + kNumShapes - 1) / kNumShapes;
+        const int lo = std::min(ext, sh * chunk), hi = std::min(ext, lo + chunk);
+        if (by_cols) {
+          it.B += (size_t)lo * it.ldb;
+          it.C += (size_t)lo * it.ldc;
+          it.n = hi - lo;
+        } else {
+          it.A += lo;
+          it.C += lo;
+          it.m = hi - lo;
+        }
+      }
+      bool any = false;
+      for (int i = 0; i < part.count; ++i) any = any || (part.it[i].m > 0 && part.it[i].n > 0);
+      if (any) e = run_shape(sh, part, s);
+      if (e == cudaSuccess) e = cudaEventRecord(T.ev[sh + 1], s);
+    }
+    if (e != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(T.ev[kNumShapes])) != cudaSuccess) return e;
+    std::vector<float> ms(kNumShapes);
+    int best = 0;
+    for (int sh = 0; sh < kNumShapes; ++sh) {
+      cudaEventElapsedTime(&ms[sh], T.ev[sh], T.ev[sh + 1]);
+      if (ms[sh] < ms[best]) best = sh;
+    }
+    T.choice[key] = best;
+    T.times[key] = ms;
+    return cudaSuccess;
+  }
+  const long tiles_tall = (long)((mm + 127) / 128) * ((nn + 63) / 64) * gb.count;
+  return run_shape(tiles_tall >= 148 ? kShapeTall : kShapeSmall, gb, s);
+}
+
+cudaError_t gemm_minus(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C, long ldc,
+                       cudaStream_t s) {
+  if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  GemmBatch gb;
+  gb.k = k;
+  gb.count = 1;
+  gb.it[0] = GemmItem{A, B, C, lda, ldb, ldc, m, n};
+  return gemm_batch(gb, s);
+}
+
+// ------------------------------------------------------------------------------------------
+// Leaf panel factorisation: for each matrix of the batch, an m x w panel (w <= 32) with partial
+// pivoting, cooperative over G CTAs per matrix (one grid for the whole batch)
 // ------------------------------------------------------------------------------------------
 constexpr int kLeafW = 32;
 constexpr int kLeafThreads = 256;
@@ -191,10 +348,10 @@ struct LeafScratchLayout {
   // offsets in bytes from the scratch base
   static constexpr size_t kBarrier = 0;                    // unsigned counter
   static constexpr size_t kCand = 256;                     // [2][kMaxCta] {double val; long long idx}
-  static constexpr int kMaxCta = 256;
-  static constexpr size_t kCandRows = kCand + 2 * kMaxCta * 16;           // [2][kMaxCta][kLeafW] double
-  static constexpr size_t kRowJ = kCandRows + 2 * kMaxCta * kLeafW * 8;   // [2][kLeafW] double
-  static constexpr size_t kEnd = kRowJ + 2 * kLeafW * 8;
+  static constexpr int kMaxCta = 512;
+  static constexpr size_t kCandRows = kCand + 2 * kMaxCta * 16;                         // [2][kMaxCta][kLeafW]
+  static constexpr size_t kRowJ = kCandRows + 2 * (size_t)kMaxCta * kLeafW * 8;         // [2][kMaxBatch][kLeafW]
+  static constexpr size_t kEnd = kRowJ + 2 * (size_t)kMaxBatch * kLeafW * 8;
 };
 
 // Waits until every CTA of the grid has arrived here `round` times.  Returns false, with the status
@@ -227,9 +384,25 @@ struct Cand {
   long long idx;
 };
 
-// rows of the leaf held by each CTA: R (the last CTA may hold fewer); shared: sp[c * R + r]
-__global__ void __launch_bounds__(kLeafThreads) k_leaf(double* __restrict__ P, long lda, int m, int w, int R,
-                                                       int* __restrict__ ipiv, int rowoff, int* info, int* status,
+struct LeafItem {
+  double* P;   // the panel's (0, 0): A(k, k)
+  long lda;
+  int m;       // rows of the panel
+  int* ipiv;   // ipiv + k
+  int* info;
+  int cta0;    // first CTA of this matrix and the number of its CTAs
+  int G;
+};
+struct LeafBatch {
+  int count;
+  int w;       // panel width (common)
+  int R;       // rows per CTA (common)
+  int rowoff;  // k (common)
+  LeafItem it[kMaxBatch];
+};
+
+// CTA c of matrix i holds rows [c R, c R + R) of its panel in shared memory: sp[col * R + r]
+__global__ void __launch_bounds__(kLeafThreads) k_leaf(const __grid_constant__ LeafBatch lb, int* status,
                                                        unsigned char* scratch) {
   extern __shared__ __align__(16) double sp[];
   __shared__ double s_prow[kLeafW];
@@ -240,12 +413,21 @@ __global__ void __launch_bounds__(kLeafThreads) k_leaf(double* __restrict__ P, l
   __shared__ int s_win;
   __shared__ double s_pval;
 
-  const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gcta = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int item = 0;
+  for (int i = 0; i < lb.count; ++i)
+    if (gcta >= lb.it[i].cta0 && gcta < lb.it[i].cta0 + lb.it[i].G) item = i;
+  const LeafItem& L = lb.it[item];
+  double* __restrict__ P = L.P;
+  const long lda = L.lda;
+  const int m = L.m, w = lb.w, R = lb.R, G = L.G, cta0 = L.cta0, cta = gcta - cta0;
+  const int total = gridDim.x;
   unsigned* counter = reinterpret_cast<unsigned*>(scratch + LeafScratchLayout::kBarrier);
   Cand* cand = reinterpret_cast<Cand*>(scratch + LeafScratchLayout::kCand);
   double* cand_rows = reinterpret_cast<double*>(scratch + LeafScratchLayout::kCandRows);
-  double* rowj = reinterpret_cast<double*>(scratch + LeafScratchLayout::kRowJ);
+  double* rowj = reinterpret_cast<double*>(scratch + LeafScratchLayout::kRowJ) + (size_t)item * kLeafW;
   constexpr int kMax = LeafScratchLayout::kMaxCta;
+  constexpr size_t kRowjPar = (size_t)kMaxBatch * kLeafW;
 
   const int rbeg = cta * R;
   const int nr = max(0, min(m, rbeg + R) - rbeg);
@@ -256,20 +438,22 @@ __global__ void __launch_bounds__(kLeafThreads) k_leaf(double* __restrict__ P, l
   __syncthreads();
 
   unsigned rounds = 0;
-  for (int j = 0; j < w && j < m; ++j) {
+  for (int j = 0; j < w; ++j) {
     const int par = j & 1;
+    const bool live = j < m;  // (uniform for a matrix; every CTA still takes every barrier)
     // local candidate: max |P(i, j)| over rows i >= j, first index on ties
     double bv = -1.0;
     long long bi = 0x7fffffffffffffffLL;
-    for (int r = tid; r < nr; r += kLeafThreads) {
-      const int i = rbeg + r;
-      if (i < j) continue;
-      const double v = fabs(sp[j * R + r]);
-      if (v > bv || (v == bv && i < bi)) {
-        bv = v;
-        bi = i;
+    if (live)
+      for (int r = tid; r < nr; r += kLeafThreads) {
+        const int i = rbeg + r;
+        if (i < j) continue;
+        const double v = fabs(sp[j * R + r]);
+        if (v > bv || (v == bv && i < bi)) {
+          bv = v;
+          bi = i;
+        }
       }
-    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -297,28 +481,30 @@ __global__ void __launch_bounds__(kLeafThreads) k_leaf(double* __restrict__ P, l
     bv = s_rv[0];
     bi = s_ri[0];
 
-    if (G > 1) {
+    if (total > 1) {
       // publish the candidate, its row, and (owner of row j) row j; then one barrier
       if (tid == 0) {
-        cand[par * kMax + cta].val = bv;
-        cand[par * kMax + cta].idx = bi;
+        cand[par * kMax + gcta].val = bv;
+        cand[par * kMax + gcta].idx = bi;
       }
-      if (tid < w && bi != 0x7fffffffffffffffLL) cand_rows[((size_t)par * kMax + cta) * kLeafW + tid] = sp[tid * R + (int)(bi - rbeg)];
-      if (j >= rbeg && j < rbeg + nr && tid < w) rowj[par * kLeafW + tid] = sp[tid * R + (j - rbeg)];
+      if (tid < w && bi != 0x7fffffffffffffffLL)
+        cand_rows[((size_t)par * kMax + gcta) * kLeafW + tid] = sp[tid * R + (int)(bi - rbeg)];
+      if (live && j >= rbeg && j < rbeg + nr && tid < w) rowj[par * kRowjPar + tid] = sp[tid * R + (j - rbeg)];
       ++rounds;
-      if (!grid_barrier(counter, rounds * (unsigned)G, status)) return;
-      // global pivot
+      if (!grid_barrier(counter, rounds * (unsigned)total, status)) return;
+      if (!live) continue;
+      // this matrix's pivot: the best of its G candidates
       if (warp == 0) {
         double gv = -1.0;
         long long gi = 0x7fffffffffffffffLL;
         int gw = 0;
         for (int q = lane; q < G; q += 32) {
-          const double v = __ldcg(&cand[par * kMax + q].val);
-          const long long i = __ldcg(&cand[par * kMax + q].idx);
+          const double v = __ldcg(&cand[par * kMax + cta0 + q].val);
+          const long long i = __ldcg(&cand[par * kMax + cta0 + q].idx);
           if (v > gv || (v == gv && i < gi)) {
             gv = v;
             gi = i;
-            gw = q;
+            gw = cta0 + q;
           }
         }
 #pragma unroll
@@ -340,9 +526,10 @@ __global__ void __launch_bounds__(kLeafThreads) k_leaf(double* __restrict__ P, l
       __syncthreads();
       if (tid < w) {
         s_prow[tid] = __ldcg(&cand_rows[((size_t)par * kMax + s_win) * kLeafW + tid]);
-        s_rowj[tid] = __ldcg(&rowj[par * kLeafW + tid]);
+        s_rowj[tid] = __ldcg(&rowj[par * kRowjPar + tid]);
       }
     } else {
+      if (!live) break;
       if (tid == 0) s_piv = bi;
       __syncthreads();
       if (tid < w) {
@@ -354,8 +541,8 @@ __global__ void __launch_bounds__(kLeafThreads) k_leaf(double* __restrict__ P, l
     const int p = (int)s_piv;
     if (tid == 0) s_pval = s_prow[j];
     if (cta == 0 && tid == 0) {
-      ipiv[j] = rowoff + p + 1;
-      if (s_prow[j] == 0.0) atomicCAS(info, 0, rowoff + j + 1);
+      L.ipiv[j] = lb.rowoff + p + 1;
+      if (s_prow[j] == 0.0) atomicCAS(L.info, 0, lb.rowoff + j + 1);
     }
     __syncthreads();
     const double pv = s_pval;
@@ -385,15 +572,27 @@ __global__ void __launch_bounds__(kLeafThreads) k_leaf(double* __restrict__ P, l
 }
 
 // ------------------------------------------------------------------------------------------
-// Row interchanges on columns [c0, c1): for j in [j0, j1) swap rows j and ipiv[j]-1 (in order)
+// Row interchanges on columns [c0, c1_i) of each matrix: for j in [j0, j1) swap rows j and
+// ipiv[j]-1 (in order); blockIdx.y selects the matrix
 // ------------------------------------------------------------------------------------------
-__global__ void k_laswp(double* __restrict__ A, long lda, int c0, int c1, const int* __restrict__ ipiv, int j0,
-                        int j1) {
+struct SwapItem {
+  double* A;
+  long lda;
+  const int* ipiv;
+  int c1;
+};
+struct SwapBatch {
+  int count;
+  SwapItem it[kMaxBatch];
+};
+__global__ void k_laswp(const __grid_constant__ SwapBatch sb, int c0, int j0, int j1) {
+  const SwapItem& S = sb.it[blockIdx.y];
   const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = c < c1;
-  double* col = A + (size_t)(act ? c : c0) * lda;
+  if (c0 + (int)(blockIdx.x * blockDim.x) >= S.c1) return;
+  const bool act = c < S.c1;
+  double* col = S.A + (size_t)(act ? c : c0) * S.lda;
   for (int j = j0; j < j1; ++j) {
-    const int p = ipiv[j] - 1;  // uniform across the block: no divergence
+    const int p = S.ipiv[j] - 1;  // uniform across the block: no divergence
     if (p != j && act) {
       const double t = col[j];
       col[j] = col[p];
@@ -403,23 +602,35 @@ __global__ void k_laswp(double* __restrict__ A, long lda, int c0, int c1, const 
 }
 
 // ------------------------------------------------------------------------------------------
-// TRSM leaf: B(kb x nc) := L^-1 B, L unit lower kb x kb (kb <= 32); one CTA per 64 columns
+// TRSM leaf: B(kb x nc) := L^-1 B, L unit lower kb x kb (kb <= 32), per matrix (blockIdx.y);
+// one CTA per 64 columns
 // ------------------------------------------------------------------------------------------
 constexpr int kTrsmLeaf = 32;
 constexpr int kTrsmCols = 64;
-__global__ void __launch_bounds__(kTrsmCols) k_trsm_leaf(const double* __restrict__ L, long ldl, int kb,
-                                                          double* __restrict__ B, long ldb, int nc) {
+struct TriItem {
+  const double* L;  // the unit lower triangle's (0, 0)
+  double* B;        // the right-hand block's (0, 0)
+  long ld;          // leading dimension of both
+  int nc;           // columns of B
+};
+struct TriBatch {
+  int count;
+  TriItem it[kMaxBatch];
+};
+__global__ void __launch_bounds__(kTrsmCols) k_trsm_leaf(const __grid_constant__ TriBatch tb, int kb) {
   __shared__ double sl[kTrsmLeaf][kTrsmLeaf + 1];
+  const TriItem& T = tb.it[blockIdx.y];
+  if ((int)(blockIdx.x * kTrsmCols) >= T.nc) return;
   const int tid = threadIdx.x;
   for (int idx = tid; idx < kb * kb; idx += kTrsmCols) {
     const int r = idx % kb, c = idx / kb;
-    sl[r][c] = L[(size_t)c * ldl + r];
+    sl[r][c] = T.L[(size_t)c * T.ld + r];
   }
   __syncthreads();
   const int col = blockIdx.x * kTrsmCols + tid;
-  if (col >= nc) return;
+  if (col >= T.nc) return;
   double x[kTrsmLeaf];
-  double* b = B + (size_t)col * ldb;
+  double* b = T.B + (size_t)col * T.ld;
 #pragma unroll
   for (int r = 0; r < kTrsmLeaf; ++r)
     if (r < kb) x[r] = b[r];
@@ -438,106 +649,229 @@ __global__ void __launch_bounds__(kTrsmCols) k_trsm_leaf(const double* __restric
     if (r < kb) b[r] = x[r];
 }
 
+// ------------------------------------------------------------------------------------------
+// Host side: the blocked recursive LU over a batch of matrices
+// ------------------------------------------------------------------------------------------
 struct Ctx {
-  double* A;
-  long lda;
-  int n;
-  int* ipiv;
-  int* info;
+  LuItem items[kMaxBatch];
+  int count;
   int* status;
   unsigned char* leaf_scratch;
   int num_sms;
   cudaStream_t s;
 };
+// the matrices worked on together (indices into Ctx::items)
+struct Group {
+  int n = 0;
+  int idx[kMaxBatch];
+};
 
-cudaError_t gemm_minus(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C, long ldc,
-                       cudaStream_t s) {
-  if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
-  const long tiles_big = (long)((m + 127) / 128) * ((n + 127) / 128);
-  if (tiles_big >= 148) return run_gemm<128, 128, 16, 32, 64, 4>(m, n, k, A, lda, B, ldb, C, ldc, s);
-  return run_gemm<64, 64, 16, 32, 32, 4>(m, n, k, A, lda, B, ldb, C, ldc, s);
-}
-
-cudaError_t laswp(const Ctx& c, int c0, int c1, int j0, int j1) {
-  if (c1 <= c0 || j1 <= j0) return cudaSuccess;
-  const int threads = 128;
-  k_laswp<<<(c1 - c0 + threads - 1) / threads, threads, 0, c.s>>>(c.A, c.lda, c0, c1, c.ipiv, j0, j1);
-  BGPU_COUNT_LAUNCH();
-  return cudaGetLastError();
-}
-
-// B(kb x nc) := L^-1 B with L unit lower (both inside A, leading dimension lda)
-cudaError_t trsm_lower_unit(const double* L, long lda, int kb, double* B, int nc, cudaStream_t s) {
-  if (kb <= 0 || nc <= 0) return cudaSuccess;
+// B_i(kb x nc_i) := L_i^-1 B_i for every item (L unit lower, both inside the matrix)
+cudaError_t trsm_lower_unit(const TriBatch& tb, int kb, cudaStream_t s) {
+  if (kb <= 0 || tb.count == 0) return cudaSuccess;
+  int ncmax = 0;
+  for (int i = 0; i < tb.count; ++i) ncmax = std::max(ncmax, tb.it[i].nc);
+  if (ncmax <= 0) return cudaSuccess;
   if (kb <= kTrsmLeaf) {
-    k_trsm_leaf<<<(nc + kTrsmCols - 1) / kTrsmCols, kTrsmCols, 0, s>>>(L, lda, kb, B, lda, nc);
+    k_trsm_leaf<<<dim3((ncmax + kTrsmCols - 1) / kTrsmCols, tb.count), kTrsmCols, 0, s>>>(tb, kb);
     BGPU_COUNT_LAUNCH();
     return cudaGetLastError();
   }
   int k1 = (kb / 2 + 15) / 16 * 16;
   if (k1 >= kb) k1 = kb / 2;
-  cudaError_t e = trsm_lower_unit(L, lda, k1, B, nc, s);
+  cudaError_t e = trsm_lower_unit(tb, k1, s);
   if (e != cudaSuccess) return e;
-  e = gemm_minus(kb - k1, nc, k1, L + k1, lda, B, lda, B + k1, lda, s);
-  if (e != cudaSuccess) return e;
-  return trsm_lower_unit(L + k1 + (size_t)k1 * lda, lda, kb - k1, B + k1, nc, s);
+  GemmBatch gb;
+  gb.k = k1;
+  gb.count = tb.count;
+  TriBatch t2 = tb;
+  for (int i = 0; i < tb.count; ++i) {
+    const TriItem& t = tb.it[i];
+    gb.it[i] = GemmItem{t.L + k1, t.B, t.B + k1, t.ld, t.ld, t.ld, kb - k1, t.nc};
+    t2.it[i].L = t.L + k1 + (size_t)k1 * t.ld;
+    t2.it[i].B = t.B + k1;
+  }
+  if ((e = gemm_batch(gb, s)) != cudaSuccess) return e;
+  return trsm_lower_unit(t2, kb - k1, s);
 }
 
-cudaError_t leaf(const Ctx& c, int k, int w) {
-  const int m = c.n - k;
-  int G = std::max(1, std::min(c.num_sms, (m + 255) / 256));
-  G = std::min(G, LeafScratchLayout::kMaxCta);
-  int R = (m + G - 1) / G;
-  size_t smem = (size_t)R * w * sizeof(double);
-  while (smem > 200 * 1024 && G < std::min(c.num_sms, LeafScratchLayout::kMaxCta)) {
-    ++G;
-    R = (m + G - 1) / G;
-    smem = (size_t)R * w * sizeof(double);
+// row interchanges j0..j1 on columns [c0, c1_i) with c1_i = to_n ? n_i : c1
+cudaError_t laswp(const Ctx& c, const Group& g, int c0, int c1, bool to_n, int j0, int j1) {
+  if (j1 <= j0) return cudaSuccess;
+  SwapBatch sb;
+  sb.count = 0;
+  int span = 0;
+  for (int q = 0; q < g.n; ++q) {
+    const LuItem& it = c.items[g.idx[q]];
+    const int e1 = to_n ? it.n : c1;
+    if (e1 <= c0) continue;
+    sb.it[sb.count++] = SwapItem{it.A, it.lda, it.ipiv, e1};
+    span = std::max(span, e1 - c0);
   }
-  if (smem > 220 * 1024) return cudaErrorInvalidValue;
+  if (sb.count == 0) return cudaSuccess;
+  const int threads = 128;
+  k_laswp<<<dim3((span + threads - 1) / threads, sb.count), threads, 0, c.s>>>(sb, c0, j0, j1);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// the leaves (columns [k, k + w), rows [k, n_i)) of every item of g, in as few cooperative launches
+// as the co-residency of their CTAs allows
+cudaError_t leaf_attr() {
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  double* P = c.A + k + (size_t)k * c.lda;
-  int* ip = c.ipiv + k;
-  if (G > 1) {
-    cudaError_t e = cudaMemsetAsync(c.leaf_scratch + LeafScratchLayout::kBarrier, 0, 4, c.s);
-    if (e != cudaSuccess) return e;
-    long lda = c.lda;
-    int mm = m, ww = w, RR = R, ro = k;
-    int* info = c.info;
-    int* status = c.status;
-    unsigned char* scr = c.leaf_scratch;
-    void* args[] = {&P, &lda, &mm, &ww, &RR, &ip, &ro, &info, &status, &scr};
-    BGPU_COUNT_LAUNCH();
-    return cudaLaunchCooperativeKernel((const void*)k_leaf, dim3(G), dim3(kLeafThreads), args, smem, c.s);
-  }
-  k_leaf<<<1, kLeafThreads, smem, c.s>>>(P, c.lda, m, w, R, ip, k, c.info, c.status, c.leaf_scratch);
-  BGPU_COUNT_LAUNCH();
-  return cudaGetLastError();
+  return cudaSuccess;
 }
 
-// columns [k, k + w), rows [k, n)
-cudaError_t panel(const Ctx& c, int k, int w) {
-  if (w <= kLeafW) return leaf(c, k, w);
+cudaError_t leaf(const Ctx& c, const Group& g, int k, int w) {
+  if (g.n == 0) return cudaSuccess;
+  cudaError_t e0 = leaf_attr();
+  if (e0 != cudaSuccess) return e0;
+  long total_rows = 0;
+  for (int q = 0; q < g.n; ++q) total_rows += c.items[g.idx[q]].n - k;
+  // rows per CTA: at least 256, enough that the CTAs fit on the GPU at once
+  int R = (int)std::max<long>(256, (total_rows + c.num_sms - 1) / c.num_sms);
+  for (;;) {
+    const size_t smem = (size_t)R * w * sizeof(double);
+    if (smem > 220 * 1024) break;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf, kLeafThreads, smem) != cudaSuccess) per_sm = 1;
+    long ctas = 0;
+    for (int q = 0; q < g.n; ++q) ctas += (c.items[g.idx[q]].n - k + R - 1) / R;
+    if (ctas <= (long)per_sm * c.num_sms && ctas <= LeafScratchLayout::kMaxCta) {
+      LeafBatch lb;
+      lb.count = g.n;
+      lb.w = w;
+      lb.R = R;
+      lb.rowoff = k;
+      int cta = 0;
+      for (int q = 0; q < g.n; ++q) {
+        const LuItem& it = c.items[g.idx[q]];
+        const int m = it.n - k;
+        const int G = (m + R - 1) / R;
+        lb.it[q] = LeafItem{it.A + k + (size_t)k * it.lda, it.lda, m, it.ipiv + k, it.info, cta, G};
+        cta += G;
+      }
+      int* status = c.status;
+      unsigned char* scr = c.leaf_scratch;
+      if (cta > 1) {
+        cudaError_t e = cudaMemsetAsync(c.leaf_scratch + LeafScratchLayout::kBarrier, 0, 4, c.s);
+        if (e != cudaSuccess) return e;
+        void* args[] = {&lb, &status, &scr};
+        BGPU_COUNT_LAUNCH();
+        return cudaLaunchCooperativeKernel((const void*)k_leaf, dim3(cta), dim3(kLeafThreads), args, smem, c.s);
+      }
+      k_leaf<<<1, kLeafThreads, smem, c.s>>>(lb, status, scr);
+      BGPU_COUNT_LAUNCH();
+      return cudaGetLastError();
+    }
+    R += 32;
+  }
+  // too many rows for one co-resident grid: halves of the group, one after the other
+  if (g.n == 1) return cudaErrorInvalidValue;
+  Group a, b;
+  for (int q = 0; q < g.n; ++q) {
+    Group& t = (q < g.n / 2) ? a : b;
+    t.idx[t.n++] = g.idx[q];
+  }
+  cudaError_t e = leaf(c, a, k, w);
+  if (e != cudaSuccess) return e;
+  return leaf(c, b, k, w);
+}
+
+// columns [k, k + w), rows [k, n_i) of every item of g
+cudaError_t panel(const Ctx& c, const Group& g, int k, int w) {
+  if (w <= kLeafW) return leaf(c, g, k, w);
   int w1 = (w / 2) / 8 * 8;
   if (w1 < 8) w1 = w / 2;
-  cudaError_t e = panel(c, k, w1);
+  cudaError_t e = panel(c, g, k, w1);
   if (e != cudaSuccess) return e;
-  if ((e = laswp(c, k + w1, k + w, k, k + w1)) != cudaSuccess) return e;
-  double* A = c.A;
-  const long lda = c.lda;
-  if ((e = trsm_lower_unit(A + k + (size_t)k * lda, lda, w1, A + k + (size_t)(k + w1) * lda, w - w1, c.s)) !=
-      cudaSuccess)
-    return e;
-  if ((e = gemm_minus(c.n - k - w1, w - w1, w1, A + (k + w1) + (size_t)k * lda, lda, A + k + (size_t)(k + w1) * lda,
-                      lda, A + (k + w1) + (size_t)(k + w1) * lda, lda, c.s)) != cudaSuccess)
-    return e;
-  if ((e = panel(c, k + w1, w - w1)) != cudaSuccess) return e;
-  return laswp(c, k, k + w1, k + w1, k + w);
+  if ((e = laswp(c, g, k + w1, k + w, false, k, k + w1)) != cudaSuccess) return e;
+  TriBatch tb;
+  tb.count = g.n;
+  GemmBatch gb;
+  gb.k = w1;
+  gb.count = g.n;
+  for (int q = 0; q < g.n; ++q) {
+    const LuItem& it = c.items[g.idx[q]];
+    double* A = it.A;
+    const long lda = it.lda;
+    tb.it[q] = TriItem{A + k + (size_t)k * lda, A + k + (size_t)(k + w1) * lda, lda, w - w1};
+    gb.it[q] = GemmItem{A + (k + w1) + (size_t)k * lda, A + k + (size_t)(k + w1) * lda,
+                        A + (k + w1) + (size_t)(k + w1) * lda, lda, lda, lda, it.n - k - w1, w - w1};
+  }
+  if ((e = trsm_lower_unit(tb, w1, c.s)) != cudaSuccess) return e;
+  if ((e = gemm_batch(gb, c.s)) != cudaSuccess) return e;
+  if ((e = panel(c, g, k + w1, w - w1)) != cudaSuccess) return e;
+  return laswp(c, g, k, k + w1, false, k + w1, k + w);
+}
+
+// one block column of width kb at k for the items of g (n_i - k >= kb for all of them)
+cudaError_t block_step(const Ctx& c, const Group& g, int k, int kb) {
+  cudaError_t e;
+  if ((e = panel(c, g, k, kb)) != cudaSuccess) return e;
+  if ((e = laswp(c, g, k + kb, 0, true, k, k + kb)) != cudaSuccess) return e;
+  if ((e = laswp(c, g, 0, k, false, k, k + kb)) != cudaSuccess) return e;
+  TriBatch tb;
+  tb.count = 0;
+  GemmBatch gb;
+  gb.k = kb;
+  gb.count = 0;
+  double flops = 0;
+  for (int q = 0; q < g.n; ++q) {
+    const LuItem& it = c.items[g.idx[q]];
+    const int rest = it.n - k - kb;
+    if (rest <= 0) continue;
+    double* A = it.A;
+    const long lda = it.lda;
+    tb.it[tb.count++] = TriItem{A + k + (size_t)k * lda, A + k + (size_t)(k + kb) * lda, lda, rest};
+    gb.it[gb.count++] = GemmItem{A + (k + kb) + (size_t)k * lda, A + k + (size_t)(k + kb) * lda,
+                                 A + (k + kb) + (size_t)(k + kb) * lda, lda, lda, lda, rest, rest};
+    flops += 2.0 * rest * (double)rest * kb;
+  }
+  if (tb.count == 0) return cudaSuccess;
+  if ((e = trsm_lower_unit(tb, kb, c.s)) != cudaSuccess) return e;
+  kernel_timer(0).begin(c.s);
+  if ((e = gemm_batch(gb, c.s)) != cudaSuccess) return e;
+  kernel_timer(0).end(c.s, flops);
+  return cudaSuccess;
+}
+
+constexpr int kBlock = 256;  // block-column width nb
+
+cudaError_t getrf_batch(Ctx& c) {
+  cudaError_t e;
+  for (int i = 0; i < c.count; ++i)
+    if ((e = cudaMemsetAsync(c.items[i].info, 0, sizeof(int), c.s)) != cudaSuccess) return e;
+  int nmax = 0;
+  for (int i = 0; i < c.count; ++i) nmax = std::max(nmax, c.items[i].n);
+  for (int k = 0; k < nmax; k += kBlock) {
+    // the items with a whole block column at k go together; an item's last, narrower block column
+    // is factored on its own (so every item sees the same blocking as when factored alone)
+    Group full;
+    for (int i = 0; i < c.count; ++i)
+      if (c.items[i].n - k >= kBlock) full.idx[full.n++] = i;
+    if (full.n && (e = block_step(c, full, k, kBlock)) != cudaSuccess) return e;
+    for (int i = 0; i < c.count; ++i) {
+      const int kb = c.items[i].n - k;
+      if (kb <= 0 || kb >= kBlock) continue;
+      Group one;
+      one.idx[one.n++] = i;
+      if ((e = block_step(c, one, k, kb)) != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+int device_sms() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms > 0 ? sms : 148;
 }
 
 }  // namespace
@@ -592,38 +926,64 @@ size_t lu_scratch_bytes(int) { return LeafScratchLayout::kEnd; }
 
 cudaError_t dgemm_nn_minus(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C,
                            long ldc, cudaStream_t s) {
-  return gemm_minus(m, n, k, A, lda, B, ldb, C, ldc, s);
+  kernel_timer(0).begin(s);
+  const cudaError_t e = gemm_minus(m, n, k, A, lda, B, ldb, C, ldc, s);
+  kernel_timer(0).end(s, 2.0 * m * n * (double)k);
+  return e;
 }
 
 cudaError_t lu64_getrf(double* A, long lda, int n, int* ipiv, int* d_info, int* d_status, const LuScratch& ws,
                        cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  if (ws.bytes < LeafScratchLayout::kEnd) return cudaErrorInvalidValue;
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  Ctx c{A, lda, n, ipiv, d_info, d_status, static_cast<unsigned char*>(ws.base), sms, s};
-  cudaError_t e = cudaMemsetAsync(d_info, 0, sizeof(int), s);
-  if (e != cudaSuccess) return e;
-  const int nb = 256;
-  for (int k = 0; k < n; k += nb) {
-    const int kb = std::min(nb, n - k);
-    if ((e = panel(c, k, kb)) != cudaSuccess) return e;
-    if ((e = laswp(c, k + kb, n, k, k + kb)) != cudaSuccess) return e;
-    if ((e = laswp(c, 0, k, k, k + kb)) != cudaSuccess) return e;
-    if (k + kb < n) {
-      if ((e = trsm_lower_unit(A + k + (size_t)k * lda, lda, kb, A + k + (size_t)(k + kb) * lda, n - k - kb, s)) !=
-          cudaSuccess)
-        return e;
-      kernel_timer(0).begin(s);
-      if ((e = gemm_minus(n - k - kb, n - k - kb, kb, A + (k + kb) + (size_t)k * lda, lda,
-                          A + k + (size_t)(k + kb) * lda, lda, A + (k + kb) + (size_t)(k + kb) * lda, lda, s)) !=
-          cudaSuccess)
-        return e;
-      kernel_timer(0).end(s, 2.0 * (double)(n - k - kb) * (double)(n - k - kb) * kb);
+  LuItem it{A, lda, n, ipiv, d_info};
+  return lu64_getrf_batch(&it, 1, d_status, ws, s);
+}
+
+cudaError_t lu64_getrf_batch(const LuItem* items, int count, int* d_status, const LuScratch& ws, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  if (count > kMaxBatch || ws.bytes < LeafScratchLayout::kEnd) return cudaErrorInvalidValue;
+  Ctx c;
+  c.count = 0;
+  for (int i = 0; i < count; ++i)
+    if (items[i].n > 0) c.items[c.count++] = items[i];
+  c.status = d_status;
+  c.leaf_scratch = static_cast<unsigned char*>(ws.base);
+  c.num_sms = device_sms();
+  c.s = s;
+  return getrf_batch(c);
+}
+
+void lu_autotune(bool on) { tuner().on = on; }
+
+cudaError_t lu_prepare() {
+  cudaError_t e;
+  if ((e = gemm_attr<128, 128, 16, 32, 64, 4>()) != cudaSuccess) return e;
+  if ((e = gemm_attr<64, 64, 16, 32, 32, 4>()) != cudaSuccess) return e;
+  if ((e = gemm_attr<128, 64, 16, 32, 32, 4>()) != cudaSuccess) return e;
+  if ((e = gemm_attr<64, 128, 16, 32, 64, 4>()) != cudaSuccess) return e;
+  return leaf_attr();
+}
+
+std::string lu_autotune_table() {
+  std::string out;
+  for (auto& kv : tuner().choice) {
+    char buf[256];
+    const unsigned long long key = kv.first;
+    std::snprintf(buf, sizeof buf, "m<=2^%llu n<=2^%llu k=%llu batch=%llu: %s", (key >> 40) & 0xff, (key >> 32) & 0xff,
+                  (key >> 8) & 0xffffff, key & 0xff, kShapeNames[kv.second]);
+    out += buf;
+    auto t = tuner().times.find(key);
+    if (t != tuner().times.end()) {
+      out += " (ms";
+      for (float v : t->second) {
+        std::snprintf(buf, sizeof buf, " %.3f", v);
+        out += buf;
+      }
+      out += ")";
     }
+    out += "\n";
   }
-  return cudaSuccess;
+  return out;
 }
 
 }  // namespace bgpu

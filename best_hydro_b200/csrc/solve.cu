@@ -387,7 +387,10 @@ __global__ void __launch_bounds__(kIb) k_diag_inverses(const F* __restrict__ LU,
 // the 128-wide inner dimension.  Each thread loads its 64 factor entries of the next block into
 // registers before waiting for that block's unknowns, so the factor streams while the chain of
 // dependencies advances.
-template <typename F, typename FI, bool LOWER>
+// TRANS: the triangle is the transpose of the stored one (U^T, lower, with DI = DU; or L^T, upper,
+// with DI = DL): entry (i, j) is read from LU(j, i) and the block inverses are applied transposed;
+// each thread then reads 64 consecutive entries of one stored column.
+template <typename F, typename FI, bool LOWER, bool TRANS = false>
 __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
                                                   double* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
                                                   unsigned epoch, int* status) {
@@ -413,11 +416,16 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
       const int jb = LOWER ? q : nblk - 1 - q;
       const int c0 = jb * kIb, nc = min(kIb, n - c0);
       // this thread's 64 entries of block (blk, jb), loaded before the wait
-      const F* col = LU + (size_t)(c0 + half * 64) * lda + r0 + row;
       F lv[64];
+      if (TRANS) {
+        const F* rowp = LU + (size_t)(r0 + row) * lda + c0 + half * 64;
 #pragma unroll
-      for (int kk = 0; kk < 64; ++kk)
-        lv[kk] = (live && half * 64 + kk < nc) ? col[(size_t)kk * lda] : (F)0;
+        for (int kk = 0; kk < 64; ++kk) lv[kk] = (live && half * 64 + kk < nc) ? rowp[kk] : (F)0;
+      } else {
+        const F* col = LU + (size_t)(c0 + half * 64) * lda + r0 + row;
+#pragma unroll
+        for (int kk = 0; kk < 64; ++kk) lv[kk] = (live && half * 64 + kk < nc) ? col[(size_t)kk * lda] : (F)0;
+      }
       if (q >= confirmed) {
         const int cnt = LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, &s_cnt)
                               : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, &s_cnt);
@@ -439,8 +447,9 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     }
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
-    // this thread's row of the inverse block
-    const FI* di = DI + (size_t)blk * kIb * kIb + row;
+    // this thread's row of the inverse block (its column, transposed)
+    const FI* di = TRANS ? DI + (size_t)blk * kIb * kIb + (size_t)row * kIb : DI + (size_t)blk * kIb * kIb + row;
+    const long dstride = TRANS ? 1 : kIb;
     __syncthreads();
     // right-hand side of the block: b - off-diagonal sums
     for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
@@ -455,7 +464,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     for (int b = 0; b < 2; ++b) {
       double dv[32];
 #pragma unroll
-      for (int kk = 0; kk < 32; ++kk) dv[kk] = (double)di[(size_t)(half * 64 + b * 32 + kk) * kIb];
+      for (int kk = 0; kk < 32; ++kk) dv[kk] = (double)di[(size_t)(half * 64 + b * 32 + kk) * dstride];
 #pragma unroll
       for (int kk = 0; kk < 32; ++kk) {
         const int cc = half * 64 + b * 32 + kk;
@@ -507,7 +516,66 @@ cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int
   return cudaSuccess;
 }
 
+// Y := U^-T Y, then L^-T Y (the transposed solve, FP64 factors)
+cudaError_t trsv_inv_pair_trans(const double* LU, long lda, const double* DL, const double* DU, int n, double* Y,
+                                long ldy, int nrhs, void* scratch, int* d_status, cudaStream_t s) {
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  unsigned* ticket = reinterpret_cast<unsigned*>(base);
+  unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int nblk = (n + kIb - 1) / kIb;
+  const int grid = std::min(nblk, sms * 3);
+  for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
+    const int q = std::min(kIrhs, nrhs - c0);
+    double* Yc = Y + (size_t)c0 * ldy;
+    g_epoch += 2;
+    if (g_epoch == 0) g_epoch = 2;
+    cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
+    if (e != cudaSuccess) return e;
+    k_trsv_inv<double, double, true, true><<<grid, 256, 0, s>>>(LU, lda, DU, n, Yc, ldy, q, flags, ticket, g_epoch,
+                                                                 d_status);
+    BGPU_COUNT_LAUNCH();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
+    k_trsv_inv<double, double, false, true><<<grid, 256, 0, s>>>(LU, lda, DL, n, Yc, ldy, q, flags, ticket,
+                                                                  g_epoch + 1, d_status);
+    BGPU_COUNT_LAUNCH();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// X[perm[i]] = Y[i] (the inverse of k_gather_rows)
+template <typename T>
+__global__ void k_scatter_rows(const T* __restrict__ Y, long ldy, const int* __restrict__ perm, int n, int nrhs,
+                               T* __restrict__ X, long ldx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm[i];
+  for (int r = 0; r < nrhs; ++r) X[(size_t)r * ldx + p] = Y[(size_t)r * ldy + i];
+}
+
 }  // namespace
+
+// dgetrs('T') with FP64 factors and their diagonal-block inverses: X := A^-T X (in place).
+// A = P^T L U, so A^T x = b is U^T L^T (P x) = b: two transposed triangular solves, then x = P^T z.
+cudaError_t getrs64_trans_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
+                              double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return cudaSuccess;
+  if (nrhs > kMaxRhs) return cudaErrorInvalidValue;
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  double* Y = reinterpret_cast<double*>(base + TrsvScratch::y_off(n));
+  const long ldy = n;
+  k_copy_cols<double><<<(n + 255) / 256, 256, 0, s>>>(X, ldx, n, nrhs, Y, ldy);
+  BGPU_COUNT_LAUNCH();
+  cudaError_t e = trsv_inv_pair_trans(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
+  if (e != cudaSuccess) return e;
+  k_scatter_rows<double><<<(n + 255) / 256, 256, 0, s>>>(Y, ldy, perm, n, nrhs, X, ldx);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
 
 size_t diag_inverse_elems(int n) { return (size_t)((n + kIb - 1) / kIb) * kIb * kIb; }
 

@@ -2,19 +2,23 @@
 // FP32 accumulation: the trailing update and triangular-solve updates of the mixed-precision LU
 // (mixed.cu).  No counterpart in the reference, whose LU is LAPACK's dgetrf in FP64.
 //
-// Kernel (one 128 x 256 output tile per CTA, 192 threads, 197 KB of shared memory):
+// Persistent kernel: one CTA per SM (320 threads, 197 KB of shared memory) walks the 128 x 256
+// output tiles blockIdx.x, blockIdx.x + gridDim.x, ... with
 //   warp 0, one thread   TMA producer: 128 x 64 tile of A and 256 x 64 tile of B per stage
 //                        (cp.async.bulk.tensor, 128-byte swizzle) into a 4-stage ring guarded by
-//                        full/empty mbarriers
-//   warp 1               allocates 256 TMEM columns; one thread issues tcgen05.mma kind::f16
-//                        (M 128, N 256, K 16; A and B K-major in shared memory) into the FP32
-//                        accumulator in TMEM and returns each stage with tcgen05.commit
-//   warps 2-5            epilogue: tcgen05.ld of the accumulator (each warp its 32-lane quarter),
-//                        C -= D in FP32, one row per thread (coalesced column stores)
-// Operands are BF16 copies in K-major layout (A row-major, B column-major), made by the cast
-// kernels below.  Tiles are ordered in groups of 16 row-tiles so that the CTAs resident together
-// share A and B slices in L2.  Every mbarrier wait is bounded: on expiry the thread records a status
-// and stops issuing work; all roles still reach the teardown, which frees TMEM.
+//                        full/empty mbarriers; the ring runs on across tiles
+//   warp 1               allocates all 512 TMEM columns (two 256-column FP32 accumulators); one
+//                        thread issues tcgen05.mma kind::f16 (M 128, N 256, K 16; A and B K-major in
+//                        shared memory), returns each stage with tcgen05.commit and hands a finished
+//                        accumulator to the epilogue with another commit
+//   warps 2-9            epilogue: tcgen05.ld of an accumulator (warp w reads TMEM lanes
+//                        32 (w % 4) .. +31 = tile rows, half of the 256 columns), C -= D in FP32 with
+//                        the next 32 columns of C already loaded; then the accumulator is released
+// so the epilogue of one tile runs under the main loop of the next.  Operands are BF16 copies in
+// K-major layout (A row-major, B column-major), made by the cast kernels below.  Tiles are ordered
+// in groups of 16 row-tiles so that the CTAs resident together share A and B slices in L2.  Every
+// mbarrier wait is bounded: on expiry the thread records a status and stops issuing work; all roles
+// still reach the teardown, which frees TMEM.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -28,11 +32,12 @@ namespace bgpu {
 namespace {
 
 constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kStageA = BM * BK * 2;  // 16 KB
 constexpr uint32_t kStageB = BN * BK * 2;  // 32 KB
 constexpr uint32_t kSmem = STAGES * (kStageA + kStageB) + 1024 + 256;
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;        // two accumulators of BN columns
 constexpr int kGroupM = 16;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a wait gives up after 2 s
 
@@ -117,6 +122,16 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// tile index -> (row tile, column tile) in the grouped order
+__device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int& tm, int& tn) {
+  const int per_group = kGroupM * tiles_n;
+  const int group = tile / per_group;
+  const int first_m = group * kGroupM;
+  const int group_m = min(tiles_m - first_m, kGroupM);
+  tm = first_m + (tile % per_group) % group_m;
+  tn = (tile % per_group) / group_m;
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int m, int n,
                    int k, float* __restrict__ C, long ldc, int tiles_m, int tiles_n, int* status) {
@@ -126,20 +141,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t* sB = smem + STAGES * kStageA;
   uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * kStageB);
   uint64_t* empty = full + STAGES;
-  uint64_t* accum = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+  uint64_t* acc_full = empty + STAGES;   // [2]
+  uint64_t* acc_empty = acc_full + 2;    // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   __shared__ int s_abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // grouped tile order: groups of kGroupM row-tiles sweep all column tiles
-  const int tile = blockIdx.x;
-  const int per_group = kGroupM * tiles_n;
-  const int group = tile / per_group;
-  const int first_m = group * kGroupM;
-  const int group_m = min(tiles_m - first_m, kGroupM);
-  const int tm = first_m + (tile % per_group) % group_m;
-  const int tn = (tile % per_group) / group_m;
-  const int m0 = tm * BM, n0 = tn * BN;
+  const int ntiles = tiles_m * tiles_n;
   const int ktiles = (k + BK - 1) / BK;
 
   if (threadIdx.x == 0) {
@@ -148,7 +156,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accum, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], kEpiWarps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 1) {
@@ -163,60 +174,93 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      for (int kt = 0; kt < ktiles; ++kt) {
-        const int s = kt % STAGES;
-        if (kt >= STAGES && !mbar_wait(&empty[s], ((kt / STAGES) & 1) ^ 1, status)) {
-          s_abort = 1;
-          break;
+      uint32_t it = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !*(volatile int*)&s_abort; tile += gridDim.x) {
+        int tm, tn;
+        tile_coords(tile, tiles_m, tiles_n, tm, tn);
+        for (int kt = 0; kt < ktiles; ++kt, ++it) {
+          const uint32_t s = it % STAGES;
+          if (it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) & 1) ^ 1, status)) {
+            s_abort = 1;
+            break;
+          }
+          if (*(volatile int*)&s_abort) break;
+          mbar_expect_tx(&full[s], kStageA + kStageB);
+          tma_load_2d(sA + s * kStageA, &tmA, kt * BK, tm * BM, &full[s]);
+          tma_load_2d(sB + s * kStageB, &tmB, kt * BK, tn * BN, &full[s]);
         }
-        if (*(volatile int*)&s_abort) break;
-        mbar_expect_tx(&full[s], kStageA + kStageB);
-        tma_load_2d(sA + s * kStageA, &tmA, kt * BK, m0, &full[s]);
-        tma_load_2d(sB + s * kStageB, &tmB, kt * BK, n0, &full[s]);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      bool ok = true;
-      for (int kt = 0; kt < ktiles; ++kt) {
-        const int s = kt % STAGES;
-        if (!mbar_wait(&full[s], (kt / STAGES) & 1, status)) {
+      uint32_t it = 0, local = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
+        const uint32_t b = local & 1, use = local >> 1;
+        if (use >= 1 && !mbar_wait(&acc_empty[b], (use - 1) & 1, status)) {
           s_abort = 1;
-          ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
+        const uint32_t acc = tmem + b * BN;
+        bool ok = true;
+        for (int kt = 0; kt < ktiles; ++kt, ++it) {
+          const uint32_t s = it % STAGES;
+          if (!mbar_wait(&full[s], (it / STAGES) & 1, status)) {
+            s_abort = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
 #pragma unroll
-        for (int kk = 0; kk < BK / 16; ++kk)
-          mma_bf16(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
-        mma_commit(&empty[s]);
+          for (int kk = 0; kk < BK / 16; ++kk)
+            mma_bf16(acc, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
+          mma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[b]);
       }
-      (void)ok;
-      mma_commit(accum);
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 = tile rows
-    const int q = warp & 3;
-    const bool ok = mbar_wait(accum, 0, status) && !*(volatile int*)&s_abort;
-    tc_fence_after();
-    if (ok) {
-      const int row = m0 + q * 32 + lane;
-#pragma unroll 1
-      for (int c = 0; c < BN / 32; ++c) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 32), v);
-        if (row < m) {
+    // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (tile rows), columns [half * 128, half * 128 + 128)
+    const int q = warp & 3, half = (warp - 2) >> 2;
+    uint32_t local = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
+      const uint32_t b = local & 1, use = local >> 1;
+      int tm, tn;
+      tile_coords(tile, tiles_m, tiles_n, tm, tn);
+      const int row = tm * BM + q * 32 + lane;
+      const int cbase = tn * BN + half * (BN / 2);
+      const bool rok = row < m;
+      float* crow = C + row;
+      // C of the first 32 columns, loaded before the accumulator is ready
+      float cv[32];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = n0 + c * 32 + j;
-            if (col < n) {
-              float* p = C + (size_t)col * ldc + row;
-              *p = *p - v[j];
-            }
-          }
+      for (int j = 0; j < 32; ++j) cv[j] = (rok && cbase + j < n) ? __ldcs(crow + (size_t)(cbase + j) * ldc) : 0.f;
+      if (!mbar_wait(&acc_full[b], use & 1, status) || *(volatile int*)&s_abort) break;
+      tc_fence_after();
+#pragma unroll 1
+      for (int c = 0; c < BN / 2 / 32; ++c) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * BN + (uint32_t)(half * (BN / 2) + c * 32), v);
+        float nv[32];
+        const int c0 = cbase + c * 32, c1 = c0 + 32;
+        if (c + 1 < BN / 2 / 32) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) nv[j] = (rok && c1 + j < n) ? __ldcs(crow + (size_t)(c1 + j) * ldc) : 0.f;
         }
+        if (rok) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (c0 + j < n) __stcs(crow + (size_t)(c0 + j) * ldc, cv[j] - v[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) cv[j] = nv[j];
       }
+      // every tcgen05.ld of this warp has completed (tmem_ld32 waits): release the accumulator
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acc_empty[b])) : "memory");
     }
   }
   tc_fence_before();
@@ -290,6 +334,18 @@ bool make_map(CUtensorMap* tm, const void* base, int rows, int cols, long ld, in
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// one CTA per SM (at most one per tile)
+int persistent_grid(int tiles) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return std::min(tiles, sms);
+}
+
 }  // namespace
 
 cudaError_t cast_transpose_bf16(const float* A, long lda, int m, int k, void* At, long lda_t, cudaStream_t s) {
@@ -331,9 +387,9 @@ cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, cons
                                     int* d_status, cudaStream_t s) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  k_gemm_bf16_tc<<<tiles_m * tiles_n, kThreads, kSmem, s>>>(*static_cast<const CUtensorMap*>(map_a),
-                                                            *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc,
-                                                            tiles_m, tiles_n, d_status);
+  k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
+      *static_cast<const CUtensorMap*>(map_a), *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m,
+      tiles_n, d_status);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -353,7 +409,8 @@ cudaError_t gemm_bf16_tc_minus(int m, int n, int k, const void* At, long lda_t, 
     attr = true;
   }
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  k_gemm_bf16_tc<<<tiles_m * tiles_n, kThreads, kSmem, s>>>(ta, tb, m, n, k, C, ldc, tiles_m, tiles_n, d_status);
+  k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(ta, tb, m, n, k, C, ldc, tiles_m,
+                                                                              tiles_n, d_status);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }

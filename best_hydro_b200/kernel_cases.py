@@ -29,17 +29,25 @@ def main(argv):
         b = torch.randn(n, k, dtype=dt, device=dev, generator=g)
         c = torch.randn(n, m, dtype=dt, device=dev, generator=g)
         fn = bh.gemm_bf16_minus_device if case == "tc_gemm" else bh.dgemm_minus_device
-        times = []
-        for _ in range(2):
-            e0, e1 = _ev(torch)
-            torch.cuda.synchronize()
-            e0.record()
+        kid = bh.BGPU_KERNEL_TC_GEMM if case == "tc_gemm" else bh.BGPU_KERNEL_LU_GEMM64
+        reps = int(argv[4]) if len(argv) > 4 else 1
+        fn(m, n, k, a.data_ptr(), m, b.data_ptr(), k, c.data_ptr(), m)
+        torch.cuda.synchronize()
+        bh.kernel_stats(kid, enable=1)
+        e0, e1 = _ev(torch)
+        e0.record()
+        for _ in range(reps):
             fn(m, n, k, a.data_ptr(), m, b.data_ptr(), k, c.data_ptr(), m)
-            e1.record()
-            torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1))
-        print(f"{case} {m}x{n}x{k}: {times[-1]:.3f} ms (including the BF16 casts)" if case == "tc_gemm" else
-              f"{case} {m}x{n}x{k}: {times[-1]:.3f} ms, {2.0 * m * n * k / times[-1] / 1e9:.1f} TFLOP/s")
+        e1.record()
+        torch.cuda.synchronize()
+        launches, kms, work = bh.kernel_stats(kid, enable=0)
+        call = e0.elapsed_time(e1) / reps
+        if launches:
+            kms /= launches
+            print(f"{case} {m}x{n}x{k}: kernel {kms:.3f} ms, {2.0 * m * n * k / kms / 1e9:.1f} TFLOP/s "
+                  f"(whole call {call:.3f} ms)")
+        else:
+            print(f"{case} {m}x{n}x{k}: call {call:.3f} ms, {2.0 * m * n * k / call / 1e9:.1f} TFLOP/s")
         return 0
     if case in ("assemble", "mixed"):
         f = int(argv[1])
@@ -70,6 +78,8 @@ def main(argv):
         t = bh.timings()
         print(f"mixed N={st.n}: factor {t['factor']:.2f} ms, solve {t['solve']:.2f} ms, "
               f"{int(t['refine_iters'])} iterations, residual {t['relres']:.2e}")
+        for line in bh.log_lines():
+            print(line)
         return 0
     print(__doc__)
     return 2

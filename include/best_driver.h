@@ -40,6 +40,11 @@ int bgpu_best_visco(int n, const double *x, const double *area, double cg, int i
  * out[3] D_r (1/s), from bgpu_best_difco's tensors. */
 void bgpu_best_traces(const double *tensors, double *out);
 
+/* The linear extrapolation in 1/N of a series of results (BEST's workflow with rcoal, best/best.f:154-157,
+ * README.md:12-16): the least-squares line y = y0 + slope / N through (1/n[i], y[i]), i < count
+ * (count >= 2).  Returns y0 (the value at an infinite number of triangles); *slope may be NULL. */
+double bgpu_best_extrapolate(int count, const int *n, const double *y, double *slope);
+
 /* The whole program (best/best.f:184-510 through the seam, as with -hm): reads the mesh file, solves,
  * writes <infile><flags>.be and .log.  precision: 0 FP64 LU, 1 mixed, -1 BEST's rule.  results
  * (may be NULL, 68 doubles): bgpu_best_difco's 60, then CHI', Dx, Dy, Dz, D_t, D_r, CHI, ETA. */

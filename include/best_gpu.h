@@ -82,6 +82,47 @@ int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float *d_a, int lda, 
  * bhm_create into d_out (column-major, ldo), before deflation (best/tgetgr.f:33-173). */
 int bgpu_assemble_device(int r0, int r1, int c0, int c1, double *d_out, int ldo);
 
+/* ---- Series of meshes (BEST's workflow of results extrapolated linearly in 1/N: rcoal makes a
+ * series of triangulations of one surface, best/best.f:154-157, README.md:12-16) ---------------
+ * Up to 16 meshes are assembled, factored (FP64 LU with partial pivoting, the plain path) and solved
+ * together: one launch assembles all of them, and each step of the blocked LU runs as one launch per
+ * kernel for every mesh at once; the whole build is captured once as a CUDA graph and replayed.
+ * Each mesh's factors and solutions are those of factoring it alone (bhm_build with direct = 1).
+ * Arrays of several meshes are concatenated: mesh i's block follows mesh i-1's, in the layout of
+ * the single-mesh call (v1, v2, v3: n_i x 3 column-major; x: n_i x 3; xmu: 3 n_i; comp: n_i;
+ * gdef: ndef_i values; b: 3 n_i x nrhs column-major). */
+
+/* Copies the meshes (set-up done by the caller, as for bhm_create) and computes incenters and self
+ * blocks.  n: triangles of each mesh; afac: each mesh's area correction factor. */
+int bgpu_series_create(int count, const int *n, const double *v1, const double *v2, const double *v3,
+                       const double *area, const double *afac, double cg);
+
+/* The meshes' incenters (concatenated n_i x 3 blocks), as bhm_incenters. */
+int bgpu_series_incenters(double *x);
+
+/* BEST's mean of GR's diagonal for each mesh (count values), as bhm_diag_mean. */
+int bgpu_series_diag_mean(double *dm);
+
+/* Assembles every GR with its deflation (best/best.f:406-425) and factors it.  tune = 1 first runs
+ * the build once with the DGEMM tile-shape autotuner on (its choices are logged and kept for the
+ * process), then builds again from the tuned graph.  Nonzero on a zero pivot (the message names the
+ * mesh), as bhm_build. */
+int bgpu_series_build(const int *ndef, const double *gdef, const int *comp, const double *xmu, int tune);
+
+/* Solves every mesh's system for nrhs right-hand sides in place (concatenated blocks). */
+int bgpu_series_solve(int nrhs, double *b);
+
+/* ms[0] last series build (graph replay), ms[1] the assembly of the last direct (tuning or
+ * uncaptured) build, ms[2] last series solve, ms[3] the tuning pass (0 when not tuned).  Returns
+ * the number of values written. */
+int bgpu_series_timings(double *ms, int len);
+
+void bgpu_series_destroy(void);
+
+/* The DGEMM autotuner's choices so far as text, one line per size class (NUL-terminated in buf of
+ * len bytes); returns the full length. */
+int bgpu_autotune_table(char *buf, int len);
+
 /* Kernel launches the library has issued since it was loaded. */
 unsigned long long bgpu_launch_count(void);
 

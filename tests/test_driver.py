@@ -43,3 +43,16 @@ def test_rhs_and_postprocessing(case):
     tr = bh.traces(t)
     assert abs(tr["DTRANS"] / o.report["DTRANS"] - 1) < 1e-13
     assert abs(tr["DR"] / o.report["DR"] - 1) < 1e-13
+
+
+def test_extrapolation_in_one_over_n():
+    """bgpu_best_extrapolate: least squares of y on 1/N, exact on a line, equal to numpy's fit."""
+    n = [2420, 2880, 3920, 5120, 6480, 8000, 9680, 10580]
+    y = [1.5 - 7.0 / k for k in n]
+    y0, slope = bh.extrapolate(n, y)
+    assert abs(y0 - 1.5) < 1e-13 and abs(slope + 7.0) < 1e-9
+    rng = np.random.default_rng(3)
+    y = 1.0 + 50.0 / np.array(n) + 1e-6 * rng.standard_normal(len(n))
+    s_np, y_np = np.polyfit(1.0 / np.array(n, dtype=float), y, 1)
+    y0, slope = bh.extrapolate(n, y)
+    assert abs(y0 - y_np) < 1e-12 and abs(slope - s_np) < 1e-6 * abs(s_np)
