@@ -68,6 +68,7 @@ _SIGS = {
     "bgpu_series_timings": (ctypes.c_int, [_dp, ctypes.c_int]),
     "bgpu_series_destroy": (None, []),
     "bgpu_autotune_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
+    "bgpu_best_gradient": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
     "bgpu_launch_count": (ctypes.c_ulonglong, []),
     "bgpu_kernel_stats": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, _dp, _dp]),
     # include/best_driver.h: BEST's host side around the seam
@@ -180,6 +181,16 @@ class BhmSolver:
 
     def solve_device(self, d_b, nrhs, ldb):
         _check(self.L.bgpu_solve_device(int(nrhs), ctypes.c_void_p(d_b), int(ldb)), "bgpu_solve_device")
+
+    def gradient(self, iarea=1, truearea=0.0, wm=0.0):
+        """bgpu_best_gradient: (values [D_t, D_r, [eta] or CHI'], gradients (3 results, N triangles,
+        3 corners, 3 coordinates)) with respect to the corners as read (before the centroid shift)."""
+        n = self.n
+        vals = np.zeros(3)
+        g = np.zeros(27 * n)
+        _check(self.L.bgpu_best_gradient(int(iarea), float(truearea or 0.0), float(wm), _p(vals), _p(g)),
+               "bgpu_best_gradient")
+        return vals, g.reshape(3, 3, 3, n).transpose(0, 3, 1, 2).copy()
 
     def destroy(self):
         self.L.bhm_destroy()

@@ -25,6 +25,7 @@ SOURCES = [
     ("solve.cu", []),
     ("tc_gemm.cu", []),
     ("mixed.cu", []),
+    ("adjoint.cu", []),
     ("api.cpp", []),
     ("driver.cpp", []),
 ]

@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/best_driver.h"
 #include "../../include/best_gpu.h"
 #include "../../include/best_hmatrix.h"
 #include "bgpu_internal.h"
@@ -162,6 +163,10 @@ struct Solver {
   int n = 0;
   double afac = 1.0, cg = 1.0;
   std::vector<double> x_host;  // incenters, n x 3 column-major
+  std::vector<double> v_host[3], area_host;  // the mesh as given (corners, corrected areas)
+  int ndef = 0;                               // deflation of the last build (host copies)
+  std::vector<double> gdef_host, xmu_host;
+  std::vector<int> comp_host;
   DevBuf geo, xc, self9, diag;
   DevBuf gr;                   // GR / its LU factors (FP64), n x ld
   long ld = 0;
@@ -386,6 +391,10 @@ int bhm_create(int n, const double* v1, const double* v2, const double* v3, cons
     s->afac = afac;
     s->cg = cg;
     std::vector<double> h = geo_host(n, v1, v2, v3, area);
+    s->v_host[0].assign(v1, v1 + 3 * (size_t)n);
+    s->v_host[1].assign(v2, v2 + 3 * (size_t)n);
+    s->v_host[2].assign(v3, v3 + 3 * (size_t)n);
+    s->area_host.assign(area, area + n);
     s->geo.ensure(h.size() * sizeof(double), "mesh");
     s->xc.ensure((size_t)n * kXcStride * sizeof(double), "incenters");
     s->self9.ensure((size_t)n * 9 * sizeof(double), "self blocks");
@@ -475,6 +484,10 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
     s.factored = false;
     s.precision = precision_for(direct, single);
     DevDeflation defl;
+    s.ndef = std::max(0, ndef);
+    s.gdef_host.assign(gdef, gdef + s.ndef);
+    s.xmu_host.assign(xmu, xmu + (ndef >= 1 ? n3 : 0));
+    s.comp_host.assign(comp, comp + (ndef > 1 ? n : 0));
     if (ndef >= 1) {
       s.gdef.ensure(sizeof(double) * ndef, "deflation weights");
       s.xmu.ensure(sizeof(double) * n3, "deflation vectors");
@@ -844,6 +857,289 @@ int bgpu_autotune_table(char* buf, int len) {
   std::memcpy(buf, t.data(), k);
   buf[k] = 0;
   return (int)t.size();
+}
+
+int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, double* grad) {
+  return guarded([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    if (!s.factored || s.precision != BGPU_FP64) {
+      say("error: bgpu_best_gradient needs the FP64 LU of the last bhm_build (direct = 1, or "
+          "bgpu_set_precision(BGPU_FP64))");
+      return 1;
+    }
+    const int n = s.n;
+    const size_t n3 = 3 * (size_t)n;
+    const double* x = s.x_host.data();
+    const double* area = s.area_host.data();
+    const double cg = s.cg, afac = s.afac;
+    constexpr int K = 3, C = 17;  // results D_t, D_r, [eta]; adjoint columns 6 + 6 + 5
+    ck(cudaEventRecord(r.ev[0], r.stream), "event");
+    // 1. the solutions of the six flows and the five strain flows (best/difco.f:28-44, visco.f:216-243)
+    std::vector<double> F(n3 * 11);
+    bgpu_best_rhs6(n, x, F.data());
+    bgpu_best_strain5(n, x, F.data() + 6 * n3);
+    DevBuf dF;
+    dF.ensure(F.size() * sizeof(double), "gradient right-hand sides");
+    ck(cudaMemcpyAsync(dF.p, F.data(), F.size() * sizeof(double), cudaMemcpyHostToDevice, r.stream), "b copy");
+    solve_device(s, r, 11, dF.as<double>(), (long)n3);
+    ck(cudaMemcpyAsync(F.data(), dF.p, F.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "x copy");
+    r.sync("gradient solve");
+    auto fv = [&](int col, int t, int c) { return F[(size_t)col * n3 + 3 * (size_t)t + c]; };
+    auto xv = [&](int t, int c) { return x[(size_t)c * n + t]; };
+    // 2. the results and their seeds: d/dF, d/dX and d/d(area) of the post-processing
+    double tens[60], tr[4], vis[4];
+    bgpu_best_difco(n, x, area, cg, F.data(), tens);
+    bgpu_best_traces(tens, tr);
+    bgpu_best_visco(n, x, area, cg, 0, F.data() + 6 * n3, F.data(), vis);
+    const double eta_f = wm > 0 ? 0.602214 / wm : 1.0;
+    values[0] = tr[2];
+    values[1] = tr[3];
+    values[2] = vis[0] * eta_f;
+    double Kraw[4][9] = {};
+    for (int mx = 0; mx < 6; ++mx) {
+      const int i = mx % 3, bf = mx < 3 ? 0 : 2;
+      for (int t = 0; t < n; ++t) {
+        const double F1 = fv(mx, t, 0), F2 = fv(mx, t, 1), F3 = fv(mx, t, 2), X = xv(t, 0), Y = xv(t, 1), Z = xv(t, 2);
+        const double T[3] = {Y * F3 - Z * F2, Z * F1 - X * F3, X * F2 - Y * F1}, Fv[3] = {F1, F2, F3};
+        for (int j = 0; j < 3; ++j) {
+          Kraw[bf][3 * j + i] += area[t] * Fv[j];
+          Kraw[bf + 1][3 * j + i] += area[t] * T[j];
+        }
+      }
+    }
+    double gK[2][4][9];
+    difco_post_gradient(Kraw, cg, gK[0], gK[1]);
+    std::vector<double> Fbar(n3 * C, 0.0), Xbar((size_t)K * n * 3, 0.0), Abar((size_t)K * n, 0.0);
+    auto XB = [&](int k, int t, int c) -> double& { return Xbar[((size_t)k * n + t) * 3 + c]; };
+    for (int k = 0; k < 2; ++k)
+      for (int mx = 0; mx < 6; ++mx) {
+        const int i = mx % 3, bf = mx < 3 ? 0 : 2;
+        const double gF[3] = {gK[k][bf][i], gK[k][bf][3 + i], gK[k][bf][6 + i]};
+        const double gT[3] = {gK[k][bf + 1][i], gK[k][bf + 1][3 + i], gK[k][bf + 1][6 + i]};
+        for (int t = 0; t < n; ++t) {
+          const double f[3] = {fv(mx, t, 0), fv(mx, t, 1), fv(mx, t, 2)}, X[3] = {xv(t, 0), xv(t, 1), xv(t, 2)};
+          const double A = area[t];
+          // K += A F (forces), A X x F (torques)
+          const double TxX[3] = {gT[1] * X[2] - gT[2] * X[1], gT[2] * X[0] - gT[0] * X[2], gT[0] * X[1] - gT[1] * X[0]};
+          const double FxT[3] = {f[1] * gT[2] - f[2] * gT[1], f[2] * gT[0] - f[0] * gT[2], f[0] * gT[1] - f[1] * gT[0]};
+          const double XxF[3] = {X[1] * f[2] - X[2] * f[1], X[2] * f[0] - X[0] * f[2], X[0] * f[1] - X[1] * f[0]};
+          for (int c = 0; c < 3; ++c) {
+            Fbar[(size_t)(6 * k + mx) * n3 + 3 * (size_t)t + c] = A * (gF[c] + TxX[c]);
+            XB(k, t, c) += A * FxT[c];
+          }
+          Abar[(size_t)k * n + t] += f[0] * gF[0] + f[1] * gF[1] + f[2] * gF[2] + XxF[0] * gT[0] + XxF[1] * gT[1] +
+                                     XxF[2] * gT[2];
+        }
+      }
+    {
+      // CHI' (best/visco.f:192-213 with icov = 0) is linear in the strain solutions: per column l and
+      // component c, the coordinate it is multiplied by and its coefficient
+      const double pi = 3.1415926535897932385;
+      const double f8 = eta_f * 8 * pi * (cg == 0 ? 0.75 : 1.0);
+      const int xi[5][3] = {{1, 0, -1}, {2, -1, 0}, {-1, 2, 1}, {0, 1, 2}, {0, 1, 2}};
+      const double cf[5][3] = {{0.1, 0.1, 0}, {0.1, 0, 0.1}, {0, 0.1, 0.1}, {1 / 15., -2 / 15., 1 / 15.},
+                               {1 / 15., 1 / 15., -2 / 15.}};
+      for (int l = 0; l < 5; ++l)
+        for (int c = 0; c < 3; ++c) {
+          if (xi[l][c] < 0) continue;
+          const double co = f8 * cf[l][c];
+          for (int t = 0; t < n; ++t) {
+            const double A = area[t], X = xv(t, xi[l][c]), V = fv(6 + l, t, c);
+            Fbar[(size_t)(12 + l) * n3 + 3 * (size_t)t + c] = co * A * X;
+            XB(2, t, xi[l][c]) += co * A * V;
+            Abar[2 * (size_t)n + t] += co * V * X;
+          }
+        }
+    }
+    // 3. the adjoint solve, lambda = GR^-T dJ/dF, with the same LU
+    DevBuf dL;
+    dL.ensure(Fbar.size() * sizeof(double), "adjoint vectors");
+    ck(cudaMemcpyAsync(dL.p, Fbar.data(), Fbar.size() * sizeof(double), cudaMemcpyHostToDevice, r.stream), "copy");
+    r.ensure_trsv(3 * n);
+    for (int c = 0; c < C; c += 16) {
+      const int q = std::min(16, C - c);
+      ck(getrs64_trans_inv(s.gr.as<double>(), s.ld, s.dl64.as<double>(), s.du64.as<double>(), (int)n3, s.perm.as<int>(),
+                           dL.as<double>() + (size_t)c * n3, (long)n3, q, r.trsv_scratch.p, r.status.as<int>(),
+                           r.stream),
+         "adjoint solve");
+    }
+    std::vector<double> lam(n3 * C);
+    ck(cudaMemcpyAsync(lam.data(), dL.p, lam.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "copy");
+    r.check_status("adjoint solve");
+    auto lv = [&](int col, int t, int c) { return lam[(size_t)col * n3 + 3 * (size_t)t + c]; };
+    // the F column each adjoint column pairs with, and its result
+    int fcol[C], cout_[C];
+    for (int c = 0; c < C; ++c) {
+      fcol[c] = c < 6 ? c : (c < 12 ? c - 6 : 6 + (c - 12));
+      cout_[c] = c < 6 ? 0 : (c < 12 ? 1 : 2);
+    }
+    // 4. the right-hand sides' dependence on the incenters: rotations e_i x X, strains
+    for (int k = 0; k < 2; ++k)
+      for (int t = 0; t < n; ++t)
+        for (int i = 0; i < 3; ++i) {
+          const double a0 = lv(6 * k + 3 + i, t, 0), a1 = lv(6 * k + 3 + i, t, 1), a2 = lv(6 * k + 3 + i, t, 2);
+          // lambda . (e_i x dX) = dX . (lambda x e_i)
+          const double ax[3][3] = {{0.0, a2, -a1}, {-a2, 0.0, a0}, {a1, -a0, 0.0}};
+          for (int c = 0; c < 3; ++c) XB(k, t, c) += ax[i][c];
+        }
+    for (int t = 0; t < n; ++t) {
+      const int b = 12;
+      XB(2, t, 1) += 0.5 * lv(b + 0, t, 0);
+      XB(2, t, 0) += 0.5 * lv(b + 0, t, 1);
+      XB(2, t, 2) += 0.5 * lv(b + 1, t, 0);
+      XB(2, t, 0) += 0.5 * lv(b + 1, t, 2);
+      XB(2, t, 2) += 0.5 * lv(b + 2, t, 1);
+      XB(2, t, 1) += 0.5 * lv(b + 2, t, 2);
+      XB(2, t, 0) += 0.5 * lv(b + 3, t, 0);
+      XB(2, t, 1) -= 0.5 * lv(b + 3, t, 1);
+      XB(2, t, 0) += 0.5 * lv(b + 4, t, 0);
+      XB(2, t, 2) -= 0.5 * lv(b + 4, t, 2);
+    }
+    // 5. the pair integrals' adjoint on the GPU (GR recomputed, contracted on the fly)
+    std::vector<double> lamT(n3 * C), fsT(n3 * C);
+    for (int t = 0; t < n; ++t)
+      for (int c = 0; c < C; ++c)
+        for (int a = 0; a < 3; ++a) {
+          lamT[((size_t)t * C + c) * 3 + a] = lv(c, t, a);
+          fsT[((size_t)t * C + c) * 3 + a] = fv(fcol[c], t, a);
+        }
+    DevBuf dlamT, dfsT, dxb, dqb, dscr;
+    dlamT.ensure(lamT.size() * sizeof(double), "adjoint vectors (by triangle)");
+    dfsT.ensure(fsT.size() * sizeof(double), "solutions (by triangle)");
+    dxb.ensure((size_t)n * 3 * K * sizeof(double), "incenter gradients");
+    dqb.ensure((size_t)n * 10 * K * sizeof(double), "corner gradients");
+    dscr.ensure(pair_adjoint_scratch_bytes(n, K), "adjoint partial sums");
+    ck(cudaMemcpyAsync(dlamT.p, lamT.data(), lamT.size() * sizeof(double), cudaMemcpyHostToDevice, r.stream), "copy");
+    ck(cudaMemcpyAsync(dfsT.p, fsT.data(), fsT.size() * sizeof(double), cudaMemcpyHostToDevice, r.stream), "copy");
+    ck(cudaEventRecord(r.ev[1], r.stream), "event");
+    ck(launch_pair_adjoint(s.mesh(), K, dlamT.as<double>(), dfsT.as<double>(), C, cout_, dxb.as<double>(),
+                           dqb.as<double>(), dscr.p, r.stream),
+       "pair adjoint");
+    ck(cudaEventRecord(r.ev[2], r.stream), "event");
+    std::vector<double> xb((size_t)n * 3 * K), qb((size_t)n * 10 * K), self9((size_t)n * 9);
+    ck(cudaMemcpyAsync(xb.data(), dxb.p, xb.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "copy");
+    ck(cudaMemcpyAsync(qb.data(), dqb.p, qb.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "copy");
+    ck(cudaMemcpyAsync(self9.data(), s.self9.p, self9.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream),
+       "copy");
+    r.check_status("pair adjoint");
+    r.ms[5] = r.elapsed(1, 2);
+    for (int k = 0; k < K; ++k)
+      for (int t = 0; t < n; ++t) {
+        for (int c = 0; c < 3; ++c) XB(k, t, c) += xb[(size_t)t * 3 * K + 3 * k + c];
+        Abar[(size_t)k * n + t] += qb[(size_t)t * 10 * K + 10 * k + 9];
+      }
+    // 6. the self blocks' weights
+    std::vector<double> Ws((size_t)K * n * 9, 0.0);
+    for (int c = 0; c < C; ++c)
+      for (int t = 0; t < n; ++t)
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b)
+            Ws[((size_t)cout_[c] * n + t) * 9 + 3 * a + b] -= lv(c, t, a) * fv(fcol[c], t, b);
+    // 7. the deflation (best/best.f:406-425): GR += GDEF_d XMU XMU^T on each surface d, GDEF_d =
+    // DIAGM / |XMU_d|^2, XMU = area * unit normal, DIAGM the mean of the self blocks' diagonals
+    std::vector<double> nbar((size_t)K * n * 3, 0.0);
+    if (s.ndef >= 1) {
+      const int nd = s.ndef;
+      auto surf = [&](int t) { return nd > 1 ? s.comp_host[t] - 1 : 0; };
+      const double* xmu = s.xmu_host.data();
+      std::vector<double> Q(nd, 0.0);
+      for (int t = 0; t < n; ++t)
+        Q[surf(t)] += xmu[3 * t] * xmu[3 * t] + xmu[3 * t + 1] * xmu[3 * t + 1] + xmu[3 * t + 2] * xmu[3 * t + 2];
+      const double diagm = s.gdef_host[0] * Q[0];
+      std::vector<double> xmub((size_t)K * n3, 0.0);
+      for (int k = 0; k < K; ++k) {
+        std::vector<double> gG(nd, 0.0);
+        for (int c = 0; c < C; ++c) {
+          if (cout_[c] != k) continue;
+          std::vector<double> u(nd, 0.0), w(nd, 0.0);
+          for (int t = 0; t < n; ++t)
+            for (int a = 0; a < 3; ++a) {
+              u[surf(t)] += lv(c, t, a) * xmu[3 * t + a];
+              w[surf(t)] += xmu[3 * t + a] * fv(fcol[c], t, a);
+            }
+          for (int d = 0; d < nd; ++d) gG[d] -= u[d] * w[d];
+          for (int t = 0; t < n; ++t) {
+            const int d = surf(t);
+            for (int a = 0; a < 3; ++a)
+              xmub[(size_t)k * n3 + 3 * t + a] -= s.gdef_host[d] * (lv(c, t, a) * w[d] + fv(fcol[c], t, a) * u[d]);
+          }
+        }
+        double gdiag = 0.0;
+        for (int d = 0; d < nd; ++d) {
+          gdiag += gG[d] / Q[d];
+          const double gQ = -gG[d] * diagm / (Q[d] * Q[d]);
+          for (int t = 0; t < n; ++t)
+            if (surf(t) == d)
+              for (int a = 0; a < 3; ++a) xmub[(size_t)k * n3 + 3 * t + a] += 2.0 * gQ * xmu[3 * t + a];
+        }
+        for (int t = 0; t < n; ++t)
+          for (int a = 0; a < 3; ++a) Ws[((size_t)k * n + t) * 9 + 4 * a] += gdiag / (double)n3;
+        // XMU_t = area_t * unit normal_t
+        for (int t = 0; t < n; ++t) {
+          double dotp = 0.0;
+          for (int a = 0; a < 3; ++a) {
+            const double nh = xmu[3 * t + a] / area[t];
+            dotp += xmub[(size_t)k * n3 + 3 * t + a] * nh;
+            nbar[((size_t)k * n + t) * 3 + a] = area[t] * xmub[(size_t)k * n3 + 3 * t + a];
+          }
+          Abar[(size_t)k * n + t] += dotp;
+        }
+      }
+    }
+    // 8. corrected area = AFAC * raw area; AFAC = TRUEAREA / total raw area when iarea (best.f:286-298);
+    // the self blocks scale with sqrt(AFAC) (tgetgr.f:106)
+    double totraw = 0.0;
+    for (int t = 0; t < n; ++t) totraw += area[t] / afac;
+    std::vector<double> cot((size_t)n * K * 16, 0.0);
+    for (int k = 0; k < K; ++k) {
+      double gafac = 0.0;
+      if (iarea) {
+        for (int t = 0; t < n; ++t) {
+          gafac += (area[t] / afac) * Abar[(size_t)k * n + t];
+          for (int e = 0; e < 9; ++e) gafac += Ws[((size_t)k * n + t) * 9 + e] * self9[9 * (size_t)t + e] / (2.0 * afac);
+        }
+      }
+      const double gtot = iarea ? -gafac * afac / totraw : 0.0;
+      for (int t = 0; t < n; ++t) {
+        double* ct = cot.data() + ((size_t)t * K + k) * 16;
+        for (int e = 0; e < 9; ++e) ct[e] = Ws[((size_t)k * n + t) * 9 + e];
+        for (int c = 0; c < 3; ++c) ct[9 + c] = XB(k, t, c);
+        ct[12] = afac * Abar[(size_t)k * n + t] + gtot;
+        for (int c = 0; c < 3; ++c) ct[13 + c] = nbar[((size_t)k * n + t) * 3 + c];
+      }
+    }
+    // 9. the per-triangle geometry's adjoint on the GPU
+    DevBuf dcot, dvb;
+    dcot.ensure(cot.size() * sizeof(double), "triangle cotangents");
+    dvb.ensure((size_t)n * K * 9 * sizeof(double), "triangle gradients");
+    ck(cudaMemcpyAsync(dcot.p, cot.data(), cot.size() * sizeof(double), cudaMemcpyHostToDevice, r.stream), "copy");
+    ck(launch_tri_adjoint(s.mesh(), K, dcot.as<double>(), dvb.as<double>(), r.stream), "triangle adjoint");
+    std::vector<double> vb((size_t)n * K * 9);
+    ck(cudaMemcpyAsync(vb.data(), dvb.p, vb.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "copy");
+    ck(cudaEventRecord(r.ev[3], r.stream), "event");
+    r.check_status("triangle adjoint");
+    r.ms[6] = r.elapsed(0, 3);
+    // 10. the corners as given: the centroid of the triangle centroids is subtracted first
+    // (best.f:261-272), so every corner's gradient loses the mean over all corners
+    for (int k = 0; k < K; ++k) {
+      double mean[3] = {0, 0, 0};
+      for (int t = 0; t < n; ++t)
+        for (int corner = 0; corner < 3; ++corner)
+          for (int c = 0; c < 3; ++c) {
+            const double g = vb[((size_t)t * K + k) * 9 + 3 * corner + c] + qb[(size_t)t * 10 * K + 10 * k + 3 * corner + c];
+            grad[(size_t)k * 9 * n + (size_t)corner * 3 * n + (size_t)c * n + t] = g;
+            mean[c] += g;
+          }
+      for (int c = 0; c < 3; ++c) mean[c] /= 3.0 * n;
+      for (int corner = 0; corner < 3; ++corner)
+        for (int c = 0; c < 3; ++c)
+          for (int t = 0; t < n; ++t) grad[(size_t)k * 9 * n + (size_t)corner * 3 * n + (size_t)c * n + t] -= mean[c];
+    }
+    say("gradient: D_t %.6e, D_r %.6e, %s %.6e; pair adjoint %.1f ms, total %.1f ms", values[0], values[1],
+        wm > 0 ? "[eta]" : "CHI'", values[2], r.ms[5], r.ms[6]);
+    return 0;
+  });
 }
 
 int bgpu_timings(double* ms, int len) {

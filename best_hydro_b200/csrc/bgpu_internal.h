@@ -64,6 +64,9 @@ struct KernelTimer {
 constexpr int kTimedKernels = 2;
 KernelTimer& kernel_timer(int id);
 
+// driver.cpp: d(D_t, D_r)/d(raw friction blocks Ktt, Ktr, Krt, Krr), each row-major [j][i].
+void difco_post_gradient(const double K[4][9], double cg, double dDt[4][9], double dDr[4][9]);
+
 // Queues a message for bhm_log_line (api.cpp).
 void log_message(const char* msg);
 
@@ -146,6 +149,16 @@ cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const floa
                           int nrhs, void* scratch, int* d_status, cudaStream_t s);
 // Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s);
+
+// adjoint.cu ---------------------------------------------------------------------------------
+// Pair integrals' adjoint: lam, fs [t][C][3] (adjoint vectors and solutions per column), col_out[c]
+// = the result (0..K-1) column c belongs to.  xbar (n x 3K): d/d incenter; qbar (n x 10K): d/d
+// corners (9) and d/d corrected area, summed over all pairs (the weight is -sum_c lam_c F_c^T).
+size_t pair_adjoint_scratch_bytes(int n, int K);
+cudaError_t launch_pair_adjoint(const DevMesh& m, int K, const double* lam, const double* fs, int C,
+                                const int* col_out, double* xbar, double* qbar, void* scratch, cudaStream_t s);
+// Per-triangle geometry's adjoint: cot [t][K][16] (self9, incenter, raw area, unit normal) -> vbar [t][K][9].
+cudaError_t launch_tri_adjoint(const DevMesh& m, int K, const double* cot, double* vbar, cudaStream_t s);
 
 // tc_gemm.cu ---------------------------------------------------------------------------------
 // BF16 operand copies for the tensor-core GEMM: At (m x k row-major) from A (m x k column-major

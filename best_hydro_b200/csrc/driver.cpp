@@ -29,6 +29,7 @@
 #include "../../include/best_driver.h"
 #include "../../include/best_gpu.h"
 #include "../../include/best_hmatrix.h"
+#include "bgpu_internal.h"
 
 namespace {
 
@@ -421,6 +422,36 @@ void difco_post(T Ktt[3][3], T Ktr[3][3], T Krt[3][3], T Krr[3][3], double cg, T
   put(42, Krt2);
   put(51, Krr2);
 }
+
+namespace bgpu {
+
+// The derivatives of BEST's D_t and D_r (best/output.f:96-130: TUNIT and RUNIT times a third of
+// the traces of Dtt and Drr; the sum of the Jacobi eigenvalues is the trace) with respect to the four
+// raw friction blocks K[0..3] = Ktt, Ktr, Krt, Krr (row-major [j][i], as summed in
+// best/difco.f:53-103), by complex-step differentiation of difco_post: exact to rounding, since
+// the tensors are analytic in K (matin3 pivots on the real parts).
+void difco_post_gradient(const double K[4][9], double cg, double dDt[4][9], double dDr[4][9]) {
+  const double temperature = 293.15, eta = 0.01002, pi = 3.141592653;
+  const double tunit = (1.38066E-16) * temperature * 1.0E8 / (8.0 * eta * pi);
+  const double runit = tunit * 1.0e16;
+  double scale = 0.0;
+  for (int b = 0; b < 4; ++b)
+    for (int e = 0; e < 9; ++e) scale = std::max(scale, std::fabs(K[b][e]));
+  const double h = 1e-20 * (scale > 0.0 ? scale : 1.0);
+  using C = std::complex<double>;
+  for (int b = 0; b < 4; ++b)
+    for (int e = 0; e < 9; ++e) {
+      C Kc[4][3][3];
+      for (int bb = 0; bb < 4; ++bb)
+        for (int ee = 0; ee < 9; ++ee) Kc[bb][ee / 3][ee % 3] = C(K[bb][ee], (bb == b && ee == e) ? h : 0.0);
+      C out[60];
+      difco_post<C>(Kc[0], Kc[1], Kc[2], Kc[3], cg, out);
+      dDt[b][e] = tunit * (out[0].imag() + out[4].imag() + out[8].imag()) / 3.0 / h;
+      dDr[b][e] = runit * (out[18].imag() + out[22].imag() + out[26].imag()) / 3.0 / h;
+    }
+}
+
+}  // namespace bgpu
 
 extern "C" {
 

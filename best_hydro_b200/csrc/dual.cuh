@@ -8,6 +8,13 @@
 
 namespace bgpu {
 
+// the plain double functions stay visible beside the Dual overloads below
+using ::acos;
+using ::cos;
+using ::log;
+using ::sin;
+using ::sqrt;
+
 template <int N>
 struct Dual {
   double v;

@@ -138,6 +138,12 @@ def ellipsoid(freq=16, axes=(30.0, 20.0, 12.0), jitter=0.02, seed=0):
     """Configuration C2/C4: geodesic sphere mapped to the ellipsoid, each vertex moved along the
     ellipsoid normal by U(-jitter, +jitter) of its distance from the centre (numpy default_rng(seed)).
     truearea is the smooth ellipsoid's area (quadrature), truevol 4/3 pi a b c."""
+    p, f, ta, tv = ellipsoid_vf(freq, axes, jitter, seed)
+    return to_triangles(p, f), ta, tv
+
+
+def ellipsoid_vf(freq=16, axes=(30.0, 20.0, 12.0), jitter=0.02, seed=0):
+    """ellipsoid() as shared vertices and faces: (vertices (nv, 3), faces (N, 3), truearea, truevol)."""
     a, b, c = axes
     v, f = geodesic_unit(freq)
     p = v * np.array(axes)
@@ -146,7 +152,16 @@ def ellipsoid(freq=16, axes=(30.0, 20.0, 12.0), jitter=0.02, seed=0):
     rng = np.random.default_rng(seed)
     d = rng.uniform(-jitter, jitter, size=len(p)) * np.linalg.norm(p, axis=1)
     p = p + d[:, None] * nrm
-    return to_triangles(p, f), ellipsoid_area(a, b, c), 4 * math.pi * a * b * c / 3
+    return p, f, ellipsoid_area(a, b, c), 4 * math.pi * a * b * c / 3
+
+
+def corner_to_vertex(grad, faces, nverts):
+    """Sums per-corner gradients (..., N, 3 corners, 3) onto shared vertices: (..., nverts, 3)."""
+    grad = np.asarray(grad)
+    out = np.zeros(grad.shape[:-3] + (nverts, 3))
+    for corner in range(3):
+        np.add.at(out, (Ellipsis, faces[:, corner], slice(None)), grad[..., :, corner, :])
+    return out
 
 
 def _real_ylm(l, m, theta, phi):

@@ -123,6 +123,19 @@ void bgpu_series_destroy(void);
  * len bytes); returns the full length. */
 int bgpu_autotune_table(char *buf, int len);
 
+/* ---- Gradients (the adjoint method) --------------------------------------------------------
+ * BEST's D_t and D_r (best/output.f:96-130) and [eta] (best/visco.f with icov = 0) of the mesh given
+ * to bhm_create, and their gradients with respect to every corner coordinate of every triangle.  It
+ * needs the FP64 LU of the last bhm_build, solves the 6 + 5 flows itself, solves the transposed
+ * systems with the same factors, and recomputes GR's entries on the GPU (never stored) to contract
+ * their derivatives.  The whole set-up is differentiated: the centroid shift (best.f:261-272), the
+ * area correction AFAC (iarea = 1: TRUEAREA / the total area), the deflation (best.f:384-425) and the
+ * self blocks.  wm: molecular weight ([eta] = CHI' 0.602214 / wm cm^3/g); wm <= 0 gives CHI' (A^3).
+ * values[3]: D_t (cm^2/s), D_r (1/s), [eta].  grad (27 n doubles): for each result k, 9 n values
+ * d values[k] / d(V1, V2, V3) (three n x 3 column-major blocks, per Angstrom, the coordinates as
+ * read, before the centroid shift).  No reference counterpart: the reference has no derivatives. */
+int bgpu_best_gradient(int iarea, double truearea, double wm, double *values, double *grad);
+
 /* Kernel launches the library has issued since it was loaded. */
 unsigned long long bgpu_launch_count(void);
 
