@@ -43,6 +43,10 @@ WORKLOADS = {
                           iarea=1, gen=("ellipsoid", 16)),
     "icosphere_l3": dict(desc="icosphere level 3, R=20 A", N=1280, iarea=1, gen=("icosphere", 3)),
     # BASELINE batching configuration: the ellipsoid at eight geodesic frequencies, solved as one series
+    # BASELINE differentiation configuration: gradients of the ellipsoid at frequency 16 (N = 5,120)
+    "ellipsoid_adjoint": dict(desc="ellipsoid 30/20/12 A, geodesic f=16, normal jitter U(+-2%) seed 0: adjoint "
+                                   "gradients w.r.t. all 3 x 2562 vertex coordinates", N=5120, iarea=1,
+                              gen=("adjoint", 16)),
     "ellipsoid_series": dict(desc="ellipsoid 30/20/12 A, normal jitter U(+-2%) seed 0, geodesic f = 11, 12, 14, "
                                   "16, 18, 20, 22, 23 (one series, FP64)", N=49080, iarea=1,
                              gen=("series", (11, 12, 14, 16, 18, 20, 22, 23))),
@@ -54,6 +58,8 @@ def make_mesh(name):
     kind, arg = WORKLOADS[name]["gen"]
     if kind == "series":
         return [meshes.ellipsoid(f) for f in arg]
+    if kind == "adjoint":
+        return meshes.ellipsoid(arg)
     if kind == "star":
         return meshes.star(arg)
     if kind == "ellipsoid":
@@ -413,6 +419,97 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_adjoint(args, rank, world, local_rank):
+    """The differentiation workload: adjoint gradients of D_t, D_r and [eta] (CHI') with respect to
+    every vertex coordinate, checked against central differences (h = 1e-4 A) on 64 random vertices
+    (seed 2), then a 20-step descent on vertex normal displacements that brings D_t 3% below its
+    initial value (mesh's own area, BEST's -na, for the fit)."""
+    import torch
+    import best_hydro_b200 as bh
+    from best_hydro_b200 import meshes
+
+    torch.cuda.set_device(local_rank)
+    w = WORKLOADS[args.workload]
+    verts, faces, ta, tv = meshes.ellipsoid_vf(w["gen"][1])
+    nv = len(verts)
+
+    def forward(vx, iarea):
+        st = bh.Setup(meshes.to_triangles(vx, faces), iarea, ta)
+        s = bh.BhmSolver()
+        s.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        x = s.incenters()
+        xmu, gdef = st.deflation(s.diag_mean())
+        s.build(eps=1e-10, direct=1, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+        B = s.solve(np.hstack([bh.rhs6(x), bh.strain5(x)]))
+        tr = bh.traces(bh.difco(x, st.area, B[:, :6]))
+        chip, _ = bh.visco(x, st.area, B[:, 6:], B[:, :6])
+        return np.array([tr["DTRANS"], tr["DR"], chip]), s
+
+    bh.set_precision(bh.BGPU_FP64)
+    for _ in range(max(1, args.warmup)):
+        forward(verts, 1)[1].gradient(iarea=1, truearea=ta)
+    t_fwd, t_grad = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        v0, s = forward(verts, 1)
+        t1 = time.perf_counter()
+        vals, g = s.gradient(iarea=1, truearea=ta)
+        t2 = time.perf_counter()
+        t_fwd.append(t1 - t0)
+        t_grad.append(t2 - t1)
+    gv = meshes.corner_to_vertex(g, faces, nv)
+    # central differences on 64 random vertices
+    rng = np.random.default_rng(2)
+    picks = rng.choice(nv, 64, replace=False)
+    h = 1e-4
+    scale = np.abs(gv).reshape(3, -1).max(axis=1)
+    worst = np.zeros(3)
+    t0 = time.perf_counter()
+    for v in picks:
+        for c in range(3):
+            vp, vm = verts.copy(), verts.copy()
+            vp[v, c] += h
+            vm[v, c] -= h
+            fd = (forward(vp, 1)[0] - forward(vm, 1)[0]) / (2 * h)
+            worst = np.maximum(worst, np.abs(fd - gv[:, v, c]) / scale)
+    t_fd = time.perf_counter() - t0
+    # descent on normal displacements s_i (v_i + s_i n_i, n_i the outward unit normal at the vertex)
+    nrm = np.zeros_like(verts)
+    for f in faces:
+        e = np.cross(verts[f[1]] - verts[f[0]], verts[f[2]] - verts[f[0]])
+        nrm[f] += e
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    d0 = forward(verts, 0)[0][0]
+    target = 0.97 * d0
+    sdisp = np.zeros(nv)
+    history = []
+    for it in range(20):
+        vals_k, sk = forward(verts + sdisp[:, None] * nrm, 0)
+        _, gk = sk.gradient(iarea=0)
+        gs = (meshes.corner_to_vertex(gk, faces, nv)[0] * nrm).sum(axis=1)  # dD_t / ds_i
+        r = (vals_k[0] - target) / target
+        history.append(float(r))
+        # steepest descent on r^2 / 2 with the step that zeroes the linearised residual
+        sdisp -= (r * target) * gs / float(gs @ gs)
+    bh.set_precision(-1)
+    line = {
+        "metric": "s per adjoint gradient (D_t, D_r, [eta] w.r.t. 3 x 2562 vertex coordinates)",
+        "value": float(np.median(t_grad)), "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(np.median(t_grad)) * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "N": len(faces), "vertices": nv, "desc": w["desc"]},
+        "forward_solve_s": float(np.median(t_fwd)), "values": {"D_t": vals[0], "D_r": vals[1], "chiprime": vals[2]},
+        "fd_check": {"vertices": 64, "seed": 2, "h_A": h, "worst_abs_err_over_max_grad": worst.tolist(),
+                     "seconds": t_fd},
+        "fit": {"target": "D_t 3% below initial (mesh's own area)", "relative_residual_per_step": history,
+                "max_normal_displacement_A": float(np.abs(sdisp).max())},
+        "log": [ln for ln in bh.log_lines() if ln.startswith("gradient")][-1:],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_series(args, rank, world, local_rank):
     """The series workload: every mesh assembled, factored (FP64) and solved for 11 right-hand sides
     through bgpu_series_* (one CUDA graph per build), against the same meshes solved one after the
@@ -509,6 +606,9 @@ def main():
         return
     if WORKLOADS[args.workload]["gen"][0] == "series":
         run_series(args, rank, world, local_rank)
+        return
+    if WORKLOADS[args.workload]["gen"][0] == "adjoint":
+        run_adjoint(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 

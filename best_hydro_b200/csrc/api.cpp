@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -874,6 +875,10 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
     const double* area = s.area_host.data();
     const double cg = s.cg, afac = s.afac;
     constexpr int K = 3, C = 17;  // results D_t, D_r, [eta]; adjoint columns 6 + 6 + 5
+    using Clock = std::chrono::steady_clock;
+    const auto h0 = Clock::now();
+    auto since = [&](Clock::time_point a) { return std::chrono::duration<double, std::milli>(Clock::now() - a).count(); };
+    double hms[6] = {};
     ck(cudaEventRecord(r.ev[0], r.stream), "event");
     // 1. the solutions of the six flows and the five strain flows (best/difco.f:28-44, visco.f:216-243)
     std::vector<double> F(n3 * 11);
@@ -885,6 +890,7 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
     solve_device(s, r, 11, dF.as<double>(), (long)n3);
     ck(cudaMemcpyAsync(F.data(), dF.p, F.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "x copy");
     r.sync("gradient solve");
+    hms[0] = since(h0);
     auto fv = [&](int col, int t, int c) { return F[(size_t)col * n3 + 3 * (size_t)t + c]; };
     auto xv = [&](int t, int c) { return x[(size_t)c * n + t]; };
     // 2. the results and their seeds: d/dF, d/dX and d/d(area) of the post-processing
@@ -952,6 +958,7 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
           }
         }
     }
+    hms[1] = since(h0);
     // 3. the adjoint solve, lambda = GR^-T dJ/dF, with the same LU
     DevBuf dL;
     dL.ensure(Fbar.size() * sizeof(double), "adjoint vectors");
@@ -967,6 +974,7 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
     std::vector<double> lam(n3 * C);
     ck(cudaMemcpyAsync(lam.data(), dL.p, lam.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "copy");
     r.check_status("adjoint solve");
+    hms[2] = since(h0);
     auto lv = [&](int col, int t, int c) { return lam[(size_t)col * n3 + 3 * (size_t)t + c]; };
     // the F column each adjoint column pairs with, and its result
     int fcol[C], cout_[C];
@@ -1024,6 +1032,7 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
        "copy");
     r.check_status("pair adjoint");
     r.ms[5] = r.elapsed(1, 2);
+    hms[3] = since(h0);
     for (int k = 0; k < K; ++k)
       for (int t = 0; t < n; ++t) {
         for (int c = 0; c < 3; ++c) XB(k, t, c) += xb[(size_t)t * 3 * K + 3 * k + c];
@@ -1118,6 +1127,7 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
     std::vector<double> vb((size_t)n * K * 9);
     ck(cudaMemcpyAsync(vb.data(), dvb.p, vb.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "copy");
     ck(cudaEventRecord(r.ev[3], r.stream), "event");
+    hms[4] = since(h0);
     r.check_status("triangle adjoint");
     r.ms[6] = r.elapsed(0, 3);
     // 10. the corners as given: the centroid of the triangle centroids is subtracted first
@@ -1136,8 +1146,11 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
         for (int c = 0; c < 3; ++c)
           for (int t = 0; t < n; ++t) grad[(size_t)k * 9 * n + (size_t)corner * 3 * n + (size_t)c * n + t] -= mean[c];
     }
-    say("gradient: D_t %.6e, D_r %.6e, %s %.6e; pair adjoint %.1f ms, total %.1f ms", values[0], values[1],
-        wm > 0 ? "[eta]" : "CHI'", values[2], r.ms[5], r.ms[6]);
+    hms[5] = since(h0);
+    say("gradient: D_t %.6e, D_r %.6e, %s %.6e; pair adjoint %.1f ms (GPU); host clock: solves %.1f, seeds %.1f, "
+        "adjoint solve %.1f, pair adjoint %.1f, deflation/area/triangles %.1f, total %.1f ms",
+        values[0], values[1], wm > 0 ? "[eta]" : "CHI'", values[2], r.ms[5], hms[0], hms[1] - hms[0], hms[2] - hms[1],
+        hms[3] - hms[2], hms[4] - hms[3], hms[5]);
     return 0;
   });
 }

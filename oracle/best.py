@@ -80,11 +80,20 @@ def ref_lib():
 
 
 def _seqsum(v):
-    """Left-to-right sum, as a Fortran DO loop accumulates (0.0 + v1 + v2 + ...)."""
-    v = np.asarray(v, dtype=np.float64)
+    """Left-to-right sum, as a Fortran DO loop accumulates (0.0 + v1 + v2 + ...).  Complex input
+    (the complex-step reference gradient, gradref.py) is summed the same way."""
+    v = np.asarray(v)
+    if not np.iscomplexobj(v):
+        v = v.astype(np.float64, copy=False)
     if v.size == 0:
         return 0.0
-    return float(np.add.accumulate(np.concatenate([[0.0], v]))[-1])
+    r = np.add.accumulate(np.concatenate([[0.0], v]))[-1]
+    return complex(r) if np.iscomplexobj(r) else float(r)
+
+
+def _re(z):
+    """The real part (pivoting and zero tests of complex-step runs follow the real computation)."""
+    return z.real if isinstance(z, (complex, np.complexfloating)) else z
 
 
 # ----------------------------------------------------------------------------------------------
@@ -359,7 +368,8 @@ def strain5(x, n):
 def matin3(A):
     """matin3.f: 3x3 inverse by Crout LU with implicit scaling (LUDCMP3) and back substitution
     (LUBKSB3).  A is indexed A[i][j] for Fortran A(i+1,j+1).  Returns (Y, ierr)."""
-    a = [[float(A[i][j]) for j in range(3)] for i in range(3)]
+    cv = complex if np.iscomplexobj(np.asarray(A)) else float
+    a = [[cv(A[i][j]) for j in range(3)] for i in range(3)]
     Y = [[1.0 if i == j else 0.0 for j in range(3)] for i in range(3)]
     n = 3
     TINY = 1e-20
@@ -368,8 +378,8 @@ def matin3(A):
     for i in range(n):
         aamax = 0.0
         for j in range(n):
-            if abs(a[i][j]) > aamax:
-                aamax = abs(a[i][j])
+            if abs(_re(a[i][j])) > aamax:
+                aamax = abs(_re(a[i][j]))
         if aamax == 0.0:
             ierr = 1
             aamax = 1.0
@@ -393,7 +403,7 @@ def matin3(A):
                 for k in range(j):
                     s = s - a[i][k] * a[k][j]
                 a[i][j] = s
-            dum = vv[i] * abs(s)
+            dum = vv[i] * abs(_re(s))
             if dum >= aamax:
                 imax = i
                 aamax = dum
@@ -402,12 +412,12 @@ def matin3(A):
             vv[imax] = vv[j]
         indx[j] = imax
         if j != n - 1:
-            if a[j][j] == 0.0:
+            if _re(a[j][j]) == 0.0:
                 a[j][j] = TINY
             dum = 1.0 / a[j][j]
             for i in range(j + 1, n):
                 a[i][j] = a[i][j] * dum
-    if a[n - 1][n - 1] == 0.0:
+    if _re(a[n - 1][n - 1]) == 0.0:
         a[n - 1][n - 1] = TINY
     for col in range(n):
         b = [Y[r][col] for r in range(n)]
@@ -419,7 +429,7 @@ def matin3(A):
             if ii != -1:
                 for j in range(ii, i):
                     s = s - a[i][j] * b[j]
-            elif s != 0.0:
+            elif _re(s) != 0.0:
                 ii = i
             b[i] = s
         for i in range(n - 1, -1, -1):
@@ -447,7 +457,8 @@ def difco(B, x, area, n, cg=1.0):
     """difco.f:53-401 on the six solutions B (3n x 6).  Returns a dict of the friction and
     diffusion tensors (internal units) and the centre vectors."""
     X = x.reshape(3, n)
-    Ktt = np.zeros((3, 3)); Ktr = np.zeros((3, 3)); Krt = np.zeros((3, 3)); Krr = np.zeros((3, 3))
+    dt = np.result_type(B, x, area)
+    Ktt = np.zeros((3, 3), dtype=dt); Ktr = np.zeros((3, 3), dtype=dt); Krt = np.zeros((3, 3), dtype=dt); Krr = np.zeros((3, 3), dtype=dt)
     for mx in range(6):
         F = [B[0::3, mx], B[1::3, mx], B[2::3, mx]]
         TQ = [X[1] * F[2] - X[2] * F[1], X[2] * F[0] - X[0] * F[2], X[0] * F[1] - X[1] * F[0]]
@@ -466,7 +477,7 @@ def difco(B, x, area, n, cg=1.0):
                 Krt[j, i] = -fto[j] * temp
                 Krr[j, i] = -tto[j] * temp
     raw = dict(Ktt=Ktt.copy(), Ktr=Ktr.copy(), Krt=Krt.copy(), Krr=Krr.copy())
-    uu = np.zeros((3, 3))
+    uu = np.zeros((3, 3), dtype=dt)
     uu[0, 0] = Ktt[1, 1] + Ktt[2, 2]
     uu[1, 1] = Ktt[0, 0] + Ktt[2, 2]
     uu[2, 2] = Ktt[1, 1] + Ktt[0, 0]
@@ -491,7 +502,7 @@ def difco(B, x, area, n, cg=1.0):
     aux, ierr = matin3(uu)
     urc = np.array([aux[j, 0] * sur1 + aux[j, 1] * sur2 + aux[j, 2] * sur3 for j in range(3)])
     uu = _antisym(urc)
-    Krr_new = np.zeros((3, 3))
+    Krr_new = np.zeros((3, 3), dtype=dt)
     for i in range(3):
         for j in range(3):
             temp = 0.0
@@ -501,14 +512,14 @@ def difco(B, x, area, n, cg=1.0):
             temp2 = uu[i, 0] * Krt[0, j] + uu[i, 1] * Krt[1, j] + uu[i, 2] * Krt[2, j]
             Krr_new[i, j] = Krr[i, j] - temp + temp1 - temp2
     Krr = Krr_new
-    Krt_new = np.zeros((3, 3))
+    Krt_new = np.zeros((3, 3), dtype=dt)
     for i in range(3):
         for j in range(3):
             Krt_new[i, j] = Krt[i, j] + Ktt[i, 0] * uu[0, j] + Ktt[i, 1] * uu[1, j] + Ktt[i, 2] * uu[2, j]
     Krt = Krt_new
     Kttinv, _ = matin3(Ktt)
     KrrCR = Krr.copy()
-    M = np.zeros((3, 3))
+    M = np.zeros((3, 3), dtype=dt)
     for i in range(3):
         for j in range(3):
             temp = 0.0
@@ -518,7 +529,7 @@ def difco(B, x, area, n, cg=1.0):
     Drr, _ = matin3(M)
     if cg == 0:
         Drr = 4.0 * Drr / 3.0
-    Dtr = np.zeros((3, 3))
+    Dtr = np.zeros((3, 3), dtype=dt)
     for i in range(3):
         for j in range(3):
             temp = 0.0
@@ -527,7 +538,7 @@ def difco(B, x, area, n, cg=1.0):
             Dtr[i, j] = -temp
             if cg == 0:
                 Dtr[i, j] = 4.0 * Dtr[i, j] / 3.0
-    Dtt = np.zeros((3, 3))
+    Dtt = np.zeros((3, 3), dtype=dt)
     for i in range(3):
         for j in range(3):
             temp = 0.0
@@ -536,7 +547,7 @@ def difco(B, x, area, n, cg=1.0):
             Dtt[i, j] = Kttinv[i, j] - temp
             if cg == 0:
                 Dtt[i, j] = 4.0 * Dtt[i, j] / 3.0
-    uu = np.zeros((3, 3))
+    uu = np.zeros((3, 3), dtype=dt)
     uu[0, 0] = Drr[1, 1] + Drr[2, 2]
     uu[1, 1] = Drr[0, 0] + Drr[2, 2]
     uu[2, 2] = Drr[1, 1] + Drr[0, 0]
@@ -552,7 +563,7 @@ def difco(B, x, area, n, cg=1.0):
     aux, _ = matin3(uu)
     udr = np.array([aux[j, 0] * sur1 + aux[j, 1] * sur2 + aux[j, 2] * sur3 for j in range(3)])
     uu = _antisym(udr)
-    Dtt_new = np.zeros((3, 3))
+    Dtt_new = np.zeros((3, 3), dtype=dt)
     for i in range(3):
         for j in range(3):
             temp = 0.0
@@ -562,7 +573,7 @@ def difco(B, x, area, n, cg=1.0):
             temp2 = -uu[i, 0] * Dtr[j, 0] - uu[i, 1] * Dtr[j, 1] - uu[i, 2] * Dtr[j, 2]
             Dtt_new[i, j] = Dtt[i, j] - temp + temp1 + temp2
     Dtt = Dtt_new
-    Dtr_new = np.zeros((3, 3))
+    Dtr_new = np.zeros((3, 3), dtype=dt)
     for i in range(3):
         for j in range(3):
             Dtr_new[i, j] = Dtr[i, j] - uu[i, 0] * Drr[0, j] - uu[i, 1] * Drr[1, j] - uu[i, 2] * Drr[2, j]
@@ -571,7 +582,7 @@ def difco(B, x, area, n, cg=1.0):
 
 
 def _antisym(u):
-    uu = np.zeros((3, 3))
+    uu = np.zeros((3, 3), dtype=np.result_type(*[np.asarray(v) for v in u]))
     uu[2, 0] = -u[1]
     uu[2, 1] = u[0]
     uu[0, 1] = -u[2]

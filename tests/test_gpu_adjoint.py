@@ -81,3 +81,40 @@ def test_gradient_needs_the_fp64_factors():
     with pytest.raises(bh.BestGpuError):
         s.gradient(iarea=1, truearea=ta)
     s.destroy()
+
+
+def test_adjoint_matches_the_cpu_reference_gradient():
+    """Against the complex-step derivatives of the CPU oracle (oracle/gradref.py): both are exact up
+    to rounding, so they agree far below the finite differences' accuracy."""
+    from oracle import gradref
+    verts, faces, ta, tv = meshes.ellipsoid_vf(6)
+    tri = meshes.to_triangles(verts, faces)
+    _, s, st = values_of(tri, ta, 1)
+    vals, g = s.gradient(iarea=1, truearea=ta)
+    bh.set_precision(-1)
+    gv = meshes.corner_to_vertex(g, faces, len(verts))
+    rng = np.random.default_rng(2)
+    picks = [(int(v), int(c)) for v in rng.choice(len(verts), 4, replace=False) for c in range(3)]
+    ref = gradref.gradient(verts, faces, 1, ta, picks)
+    got = np.array([[gv[k, v, c] for (v, c) in picks] for k in range(3)])
+    err = np.abs(got - ref).max(axis=1) / np.abs(gv).reshape(3, -1).max(axis=1)
+    print(f"\nadjoint vs complex-step CPU reference: D_t {err[0]:.1e}, D_r {err[1]:.1e}, CHI' {err[2]:.1e}")
+    assert np.all(err < 1e-9), err
+
+
+def test_torch_autograd_wrapper():
+    """The adjoint through torch.autograd (tests/torch_best.py): a scalar loss of the three results
+    back-propagates to the vertices as the chain rule of the adjoint gradients says."""
+    import torch
+    from tests.torch_best import BestValues
+    verts, faces, ta, tv = meshes.ellipsoid_vf(4)
+    v = torch.tensor(verts, dtype=torch.float64, requires_grad=True)
+    vals = BestValues.apply(v, faces, ta, 1)
+    w = torch.tensor([1e6, 1e-7, 1e-4], dtype=torch.float64)
+    (w * vals).sum().backward()
+    _, s, st = values_of(meshes.to_triangles(verts, faces), ta, 1)
+    _, g = s.gradient(iarea=1, truearea=ta)
+    bh.set_precision(-1)
+    gv = meshes.corner_to_vertex(g, faces, len(verts))
+    expect = np.einsum("k,kvc->vc", w.numpy(), gv)
+    assert np.allclose(v.grad.numpy(), expect, rtol=1e-12, atol=1e-12 * np.abs(expect).max())
