@@ -27,7 +27,7 @@ namespace {
 constexpr double kPi = 3.1415926535897932385;  // best/tgetgr.f:17
 constexpr int kSrcBlock = 128;                  // sources per block (threads)
 constexpr int kTgtTile = 16;                    // targets staged per step
-constexpr int kTgtChunk = 256;                  // targets per block (grid.y splits the rest)
+constexpr int kTgtChunkMax = 256;               // targets per block at most (grid.y splits the rest)
 constexpr int kMaxCols = 17;                    // adjoint columns (6 + 6 + 5)
 
 // 21-point Gauss-Legendre rule on [0,1] (best/triangleint.f:66-108), as in the assembly
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kSrcBlock) k_pair_adjoint(int n, const double*
                                                             const double* __restrict__ xc, double cg,
                                                             const double* __restrict__ lam,
                                                             const double* __restrict__ fs, int C, ColMap cols,
-                                                            double* __restrict__ xbar_part,
+                                                            int tgt_chunk, double* __restrict__ xbar_part,
                                                             double* __restrict__ qbar_part) {
   extern __shared__ double sm[];
   const int stride = 3 * C;
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kSrcBlock) k_pair_adjoint(int n, const double*
   for (int k = 0; k < K; ++k)
 #pragma unroll
     for (int i = 0; i < 10; ++i) qacc[k][i] = 0.0;
-  const int p_lo = blockIdx.y * kTgtChunk, p_hi = min(n, p_lo + kTgtChunk);
+  const int p_lo = blockIdx.y * tgt_chunk, p_hi = min(n, p_lo + tgt_chunk);
   for (int t0 = p_lo; t0 < p_hi; t0 += kTgtTile) {
     const int nt = min(kTgtTile, p_hi - t0);
     __syncthreads();
@@ -504,18 +504,31 @@ __global__ void __launch_bounds__(64) k_tri_adjoint(int n, const double* __restr
   }
 }
 
+// targets per block: at most kTgtChunkMax, and few enough that the grid has two blocks per SM
+int tgt_chunk(int n) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int gx = (n + kSrcBlock - 1) / kSrcBlock;
+  const int gy = std::max(1, (2 * sms + gx - 1) / gx);
+  int chunk = (n + gy - 1) / gy;
+  chunk = (chunk + kTgtTile - 1) / kTgtTile * kTgtTile;
+  return std::max(kTgtTile, std::min(kTgtChunkMax, chunk));
+}
+
 template <int K>
 cudaError_t run_pair(const DevMesh& m, const double* lam, const double* fs, int C, const int* col_out, double* xbar,
                      double* qbar, double* scratch, cudaStream_t s) {
   ColMap cols{};
   for (int c = 0; c < C; ++c) cols.out[c] = col_out[c];
-  const int gx = (m.n + kSrcBlock - 1) / kSrcBlock, gy = (m.n + kTgtChunk - 1) / kTgtChunk;
+  const int gx = (m.n + kSrcBlock - 1) / kSrcBlock, chunk = tgt_chunk(m.n), gy = (m.n + chunk - 1) / chunk;
   const size_t smem = (size_t)(kSrcBlock * 3 * C + kTgtTile * (3 + 3 * C) + 4 * kTgtTile * 3 * K) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(k_pair_adjoint<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   double* xpart = scratch;
   double* qpart = scratch + (size_t)gx * m.n * 3 * K;
-  k_pair_adjoint<K><<<dim3(gx, gy), kSrcBlock, smem, s>>>(m.n, m.geo, m.xc, m.cg, lam, fs, C, cols, xpart, qpart);
+  k_pair_adjoint<K><<<dim3(gx, gy), kSrcBlock, smem, s>>>(m.n, m.geo, m.xc, m.cg, lam, fs, C, cols, chunk, xpart,
+                                                           qpart);
   BGPU_COUNT_LAUNCH();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const size_t lx = (size_t)m.n * 3 * K, lq = (size_t)m.n * 10 * K;
@@ -529,7 +542,7 @@ cudaError_t run_pair(const DevMesh& m, const double* lam, const double* fs, int 
 }  // namespace
 
 size_t pair_adjoint_scratch_bytes(int n, int K) {
-  const size_t gx = (n + kSrcBlock - 1) / kSrcBlock, gy = (n + kTgtChunk - 1) / kTgtChunk;
+  const size_t gx = (n + kSrcBlock - 1) / kSrcBlock, chunk = tgt_chunk(n), gy = (n + chunk - 1) / chunk;
   return (gx * n * 3 * K + gy * n * 10 * K) * sizeof(double);
 }
 

@@ -4,6 +4,7 @@
     python -m best_hydro_b200.kernel_cases dgemm M N K       # C -= A B, FP64 DMMA
     python -m best_hydro_b200.kernel_cases assemble F        # GR of the ellipsoid at geodesic frequency F
     python -m best_hydro_b200.kernel_cases mixed F           # mixed build + solve, ellipsoid frequency F
+    python -m best_hydro_b200.kernel_cases adjoint F         # FP64 build + adjoint gradients (k_pair_adjoint)
 
 Each case launches its kernel twice (the second launch is the one to capture: `ncu -k <kernel>
 -s 1 -c 1`) and prints the CUDA-event time of the second launch.
@@ -48,6 +49,20 @@ def main(argv):
                   f"(whole call {call:.3f} ms)")
         else:
             print(f"{case} {m}x{n}x{k}: call {call:.3f} ms, {2.0 * m * n * k / call / 1e9:.1f} TFLOP/s")
+        return 0
+    if case == "adjoint":
+        from best_hydro_b200 import meshes
+        f = int(argv[1])
+        tri, ta, tv = meshes.ellipsoid(f)
+        st = bh.Setup(tri, 1, ta)
+        s = bh.BhmSolver()
+        s.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        xmu, gdef = st.deflation(s.diag_mean())
+        bh.set_precision(bh.BGPU_FP64)
+        s.build(eps=1e-10, direct=1, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+        for _ in range(2):
+            s.gradient(iarea=1, truearea=ta)
+        print([ln for ln in bh.log_lines() if ln.startswith("gradient")][-1])
         return 0
     if case in ("assemble", "mixed"):
         f = int(argv[1])
