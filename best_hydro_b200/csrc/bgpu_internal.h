@@ -177,5 +177,11 @@ bool tc_operand_maps(const void* At, int rows_a, long lda_t, const void* Bt, int
                      void* map_b);
 cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, const void* map_b, float* C, long ldc,
                                     int* d_status, cudaStream_t s);
+// Maps over whole-matrix BF16 mirrors (Am row-major, Bm column-major, n x n, ld ldm) and the GEMM on
+// blocks of them named by position (A at rows a_row.., columns a_k..; B at columns b_row..,
+// rows b_k..).
+bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a, void* map_b);
+cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
+                                  int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s);
 
 }  // namespace bgpu

@@ -20,6 +20,7 @@
 // with FP64 accumulation), the true FP64 residual b - GR x at every restart; all right-hand sides
 // advance in lockstep.  Stops at a relative residual of tol for every column; a failure to converge
 // or a zero pivot is an error (the C ABI then factors the kept FP64 matrix instead).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,97 +73,301 @@ constexpr int kZeroPivot = 4;  // status: a pivot of the unpivoted FP32 LU is ze
 long round_up(long v, long q) { return (v + q - 1) / q * q; }
 
 // ---- diagonal leaf: h x h (h <= 128) LU without pivoting and the inverses of both triangles ----
-// 512 threads.  Factorisation: threads as 32 (rows) x 16 (columns) over the trailing block, one
-// barrier per step; the multipliers (a_rk / a_kk) are formed on the fly and column k is scaled after
-// the barrier (nothing reads it again).  Inverses: four consecutive lanes per column c, the
-// substitution's sums split four ways and combined by shuffles; L^-1 (unit lower) and U^-1 are
-// written to DL, DU (128 x 128 column-major, zero outside the h x h block).
+// 512 threads = 16 warps x 32 lanes; warp w owns rows 8w .. 8w+7 and lane l columns 4l .. 4l+3 of
+// the 128 x 128 block, as an 8 x 4 register tile (rows and columns beyond h hold the identity, so
+// the padded part factors to itself).  Each of the 128 right-looking steps is one barrier: the
+// owners of column k and of row k publish them in a double-buffered shared row/column, and every
+// thread applies the rank-1 update to its tile.  The inverses then run the same way (L^-1 forward,
+// then U^-1 backward, 128 steps each) from the factors kept in shared memory; L^-1 (unit lower) and
+// U^-1 are written to DL, DU (128 x 128 column-major, zero outside the h x h block).
 constexpr int kLdS = 129;
-__global__ void __launch_bounds__(512) k_lu32_leaf_inv(float* __restrict__ A, long lda, int h, float* __restrict__ DL,
-                                                        float* __restrict__ DU, int* status) {
+__global__ void __launch_bounds__(512, 1) k_lu32_leaf_inv(float* __restrict__ A, long lda, int h, float* __restrict__ DL,
+                                                           float* __restrict__ DU, int* status) {
   extern __shared__ float sm[];
-  float* d = sm;                    // d[c * kLdS + r] = A(r, c), then L\U
-  float* li = sm + 128 * kLdS;      // li[c * kLdS + i] = (L^-1)(i, c)
-  float* ui = li + 128 * kLdS;      // ui[c * kLdS + i] = (U^-1)(i, c)
+  float* d = sm;                       // d[c * kLdS + r] = block entry (r, c)
+  float* rowb = sm + 128 * kLdS;       // [2][128]
+  float* colb = rowb + 2 * 128;        // [2][128]
   __shared__ int s_bad;
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-  for (int c = ty; c < h; c += 16)
-    for (int r = tx; r < h; r += 32) d[c * kLdS + r] = A[(size_t)c * lda + r];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = 8 * warp, c0 = 4 * lane;
+  for (int c = warp; c < 128; c += 16)
+    for (int r = lane; r < 128; r += 32)
+      d[c * kLdS + r] = (r < h && c < h) ? A[(size_t)c * lda + r] : (r == c ? 1.f : 0.f);
   if (tid == 0) s_bad = 0;
   __syncthreads();
-  for (int k = 0; k < h; ++k) {
-    const float p = d[k * kLdS + k];
-    if (tid == 0 && !(p != 0.f && isfinite(p))) s_bad = 1;
-    const float rp = 1.0f / p;
-    for (int c = k + 1 + ty; c < h; c += 16) {
-      const float u = d[c * kLdS + k];
-      for (int r = k + 1 + tx; r < h; r += 32) d[c * kLdS + r] -= (d[k * kLdS + r] * rp) * u;
+  float a[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) a[i][j] = d[(c0 + j) * kLdS + r0 + i];
+  // LU without pivoting.  The multipliers (column k of L) go to shared memory as they are formed
+  // (lane 0 of each warp); a tile keeps only the entries still being updated, so warps whose rows
+  // are all above the pivot sit the step out, and columns left of the pivot are never masked (they
+  // are not read again).
+#pragma unroll 1
+  for (int k = 0; k < 128; ++k) {
+    const int par = k & 1;
+    float* rb = rowb + par * 128;
+    float* cb = colb + par * 128;
+    // (selects, not indexing: the register tiles must stay in registers)
+    if (lane == (k >> 2)) {
+      const int jk = k & 3;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        cb[r0 + i] = jk == 0 ? a[i][0] : (jk == 1 ? a[i][1] : (jk == 2 ? a[i][2] : a[i][3]));
+    }
+    if (warp == (k >> 3)) {
+      const int ik = k & 7;
+      float4 v = make_float4(a[0][0], a[0][1], a[0][2], a[0][3]);
+#pragma unroll
+      for (int i = 1; i < 8; ++i)
+        if (i == ik) v = make_float4(a[i][0], a[i][1], a[i][2], a[i][3]);
+      *reinterpret_cast<float4*>(&rb[c0]) = v;
     }
     __syncthreads();
-    for (int r = k + 1 + tid; r < h; r += 512) d[k * kLdS + r] *= rp;
-  }
-  // initial columns of the inverses
-  const int c = tid >> 2, q = tid & 3;
-  for (int i = q; i < 128; i += 4) {
-    li[c * kLdS + i] = (i == c && c < h) ? 1.f : 0.f;
-    ui[c * kLdS + i] = 0.f;
+    if (tid == 0 && !(rb[k] != 0.f && isfinite(rb[k]))) s_bad = 1;
+    if (r0 + 7 > k) {
+      const float rp = 1.0f / rb[k];
+      float l[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) l[i] = (r0 + i > k) ? cb[r0 + i] * rp : 0.f;
+      if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          if (r0 + i > k) d[k * kLdS + r0 + i] = l[i];
+      }
+      const float4 u = *reinterpret_cast<const float4*>(&rb[c0]);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        a[i][0] -= l[i] * u.x;
+        a[i][1] -= l[i] * u.y;
+        a[i][2] -= l[i] * u.z;
+        a[i][3] -= l[i] * u.w;
+      }
+    }
   }
   __syncthreads();
-  if (c < h && q == 0) ui[c * kLdS + c] = 1.0f / d[c * kLdS + c];
-  __syncwarp();
-  const int lane = tid & 31;
-  const int cmin = (tid >> 5) * 8, cmax = min(cmin + 7, h - 1);
-  if (cmin < h) {
-    // L^-1: x_i = -sum_{j < i} L(i, j) x_j for i > c (x_j = 0 for j < c, x_c = 1)
-    for (int i = cmin + 1; i < h; ++i) {
-      float part = 0.f;
-      for (int j = cmin + q; j < i; j += 4) part += d[j * kLdS + i] * li[c * kLdS + j];
-      part += __shfl_xor_sync(0xffffffffu, part, 1);
-      part += __shfl_xor_sync(0xffffffffu, part, 2);
-      if (q == 0 && c < h && i > c) li[c * kLdS + i] = -part;
-      __syncwarp();
-    }
-    // U^-1: x_i = -(sum_{j > i} U(i, j) x_j) / U(i, i) for i < c (x_j = 0 for j > c)
-    for (int i = cmax - 1; i >= 0; --i) {
-      float part = 0.f;
-      for (int j = i + 1 + q; j <= cmax; j += 4) part += d[j * kLdS + i] * ui[c * kLdS + j];
-      part += __shfl_xor_sync(0xffffffffu, part, 1);
-      part += __shfl_xor_sync(0xffffffffu, part, 2);
-      if (q == 0 && c < h && i < c) ui[c * kLdS + i] = -part / d[i * kLdS + i];
-      __syncwarp();
-    }
-  }
-  (void)lane;
+  // the U part from the tiles (the L part is already in shared memory)
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (r0 + i <= c0 + j) d[(c0 + j) * kLdS + r0 + i] = a[i][j];
   __syncthreads();
-  for (int cc = ty; cc < h; cc += 16)
-    for (int r = tx; r < h; r += 32) A[(size_t)cc * lda + r] = d[cc * kLdS + r];
-  for (int cc = ty; cc < 128; cc += 16)
-    for (int r = tx; r < 128; r += 32) {
-      DL[(size_t)cc * 128 + r] = li[cc * kLdS + r];
-      DU[(size_t)cc * 128 + r] = ui[cc * kLdS + r];
+  for (int c = warp; c < h; c += 16)
+    for (int r = lane; r < h; r += 32) A[(size_t)c * lda + r] = d[c * kLdS + r];
+  // inverses from the factors in shared memory: X = L^-1 forward (steps k = 0..127), then
+  // X = U^-1 backward (k = 127..0), each one barrier per step
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool lower = pass == 0;
+    float x[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[i][j] = (r0 + i == c0 + j) ? 1.f : 0.f;
+#pragma unroll 1
+    for (int st = 0; st < 128; ++st) {
+      const int k = lower ? st : 127 - st;
+      float* xb = (st & 1) ? colb : rowb;
+      if (warp == (k >> 3)) {
+        const float rd = lower ? 1.f : 1.0f / d[k * kLdS + k];
+        const int ik = k & 7;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float sc = i == ik ? rd : 1.f;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) x[i][j] *= sc;
+          if (i == ik) v = make_float4(x[i][0], x[i][1], x[i][2], x[i][3]);
+        }
+        *reinterpret_cast<float4*>(&xb[c0]) = v;
+      }
+      __syncthreads();
+      if (lower ? r0 + 7 > k : r0 < k) {
+        const float4 xr = *reinterpret_cast<const float4*>(&xb[c0]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int r = r0 + i;
+          const float cf = (lower ? r > k : r < k) ? d[k * kLdS + r] : 0.f;
+          x[i][0] -= cf * xr.x;
+          x[i][1] -= cf * xr.y;
+          x[i][2] -= cf * xr.z;
+          x[i][3] -= cf * xr.w;
+        }
+      }
     }
+    float* D = lower ? DL : DU;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int i = 0; i < 8; ++i) D[(size_t)(c0 + j) * 128 + r0 + i] = (r0 + i < h && c0 + j < h) ? x[i][j] : 0.f;
+    __syncthreads();
+  }
   if (tid == 0 && s_bad) atomicExch(status, kZeroPivot);
 }
 
 // ---- triangular-solve leaves (h <= 128): products with the inverted diagonal block ----------
+// LEFT:  B (h x w, ldb) := Dinv B;  otherwise B (m x h, ldb) := B Dinv.  Dinv is an inverted
+// diagonal block (128 x 128, ld 128, zero outside h).  One CTA per 128 columns (LEFT) or rows of B:
+// both 128 x 128 operands go to shared memory (k-major), then 256 threads each accumulate an 8 x 8
+// tile over the 128-long inner dimension in FP32, and write it back in place (each CTA owns its
+// tile).  With mir != nullptr the results are also written, rounded to BF16, to the matrix's BF16
+// mirror at the same place: column-major for LEFT (the U part), row-major otherwise (the L part).
+// 16-byte asynchronous copy global -> shared; fewer than 16 source bytes are zero-filled
+__device__ __forceinline__ void cp16(void* sdst, const void* gsrc, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+constexpr int kLm = 132;  // row stride of the shared operands (floats)
+constexpr int kWideLeaf = 8192;  // from this many columns (rows) on, k_leaf_mult; below, 64 per CTA
+template <bool LEFT>
+__global__ void __launch_bounds__(256, 1) k_leaf_mult(const float* __restrict__ Dinv, int h, float* B, long ldb,
+                                                      int len, __nv_bfloat16* __restrict__ mir, long ldm) {
+  extern __shared__ __align__(16) float sm[];
+  float* As = sm;               // As[k * kLm + i]: the left factor's (i, k)
+  float* Bs = sm + 128 * kLm;   // Bs[k * kLm + j]: the right factor's (k, j)
+  const int tid = threadIdx.x;
+  const int t0 = blockIdx.x * 128, nt = min(128, len - t0);  // this CTA's columns (LEFT) or rows of B
+  // operands in: rows of shared memory that are contiguous in global memory by 16-byte asynchronous
+  // copies, transposed ones by float4 loads (all issued before any is used)
+  const float* tsrc;  // the operand stored transposed: element (k, x) at tsrc[x * tld + k]
+  long tld;
+  int tk, tx_lim;     // its valid k and x ranges
+  float* tdst;
+  if (LEFT) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {  // Dinv column k -> As row k
+      const int e = tid + 256 * q, k = e >> 5, i4 = (e & 31) * 4;
+      cp16(&As[k * kLm + i4], &Dinv[(size_t)k * 128 + i4], 16);
+    }
+    tsrc = B + (size_t)t0 * ldb;  // B (k, t0 + j) at B[(t0 + j) ldb + k]
+    tld = ldb;
+    tk = h;
+    tx_lim = nt;
+    tdst = Bs;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {  // B (t0 + i, k), i contiguous -> As row k
+      const int e = tid + 256 * q, k = e >> 5, i4 = (e & 31) * 4;
+      const int valid = (k < h) ? max(0, min(4, nt - i4)) * 4 : 0;
+      cp16(&As[k * kLm + i4], valid ? (const void*)&B[(size_t)k * ldb + t0 + i4] : (const void*)B, valid);
+    }
+    tsrc = Dinv;  // Dinv (k, j) at Dinv[j * 128 + k]
+    tld = 128;
+    tk = 128;
+    tx_lim = 128;
+    tdst = Bs;
+  }
+  {
+    float4 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = tid + 256 * q, k4 = (e & 31) * 4, x = e >> 5;
+      v[q] = (x < tx_lim && k4 < tk) ? *reinterpret_cast<const float4*>(&tsrc[(size_t)x * tld + k4])
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = tid + 256 * q, k4 = (e & 31) * 4, x = e >> 5;
+      tdst[(k4 + 0) * kLm + x] = k4 + 0 < tk ? v[q].x : 0.f;
+      tdst[(k4 + 1) * kLm + x] = k4 + 1 < tk ? v[q].y : 0.f;
+      tdst[(k4 + 2) * kLm + x] = k4 + 2 < tk ? v[q].z : 0.f;
+      tdst[(k4 + 3) * kLm + x] = k4 + 3 < tk ? v[q].w : 0.f;
+    }
+  }
+  cp_wait_all();
+  __syncthreads();
+  const int ty = tid >> 4, tx = tid & 15;  // rows 8 ty .. +7, columns 4 tx .. +3 and 64 + 4 tx .. +3
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+#pragma unroll 4
+  for (int k = 0; k < 128; ++k) {
+    const float4 a0 = *reinterpret_cast<const float4*>(&As[k * kLm + 8 * ty]);
+    const float4 a1 = *reinterpret_cast<const float4*>(&As[k * kLm + 8 * ty + 4]);
+    const float4 b0 = *reinterpret_cast<const float4*>(&Bs[k * kLm + 4 * tx]);
+    const float4 b1 = *reinterpret_cast<const float4*>(&Bs[k * kLm + 64 + 4 * tx]);
+    const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] += av[i] * bv[j];
+  }
+  // results through shared memory (Cs[jj * kLm + ii]: local row ii, local column jj of B's block),
+  // then coalesced stores
+  __syncthreads();
+  float* Cs = sm;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int jj = j < 4 ? 4 * tx + j : 64 + 4 * tx + (j - 4);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) Cs[jj * kLm + 8 * ty + i] = acc[i][j];
+  }
+  __syncthreads();
+  if (LEFT) {
+    // B rows ii < h, columns t0 + jj (jj < nt); mirror column-major
+    for (int e = tid; e < 128 * 128; e += 256) {
+      const int ii = e & 127, jj = e >> 7;
+      if (ii < h && jj < nt) {
+        const float v = Cs[jj * kLm + ii];
+        B[(size_t)(t0 + jj) * ldb + ii] = v;
+        if (mir) mir[(size_t)(t0 + jj) * ldm + ii] = __float2bfloat16_rn(v);
+      }
+    }
+  } else {
+    // B rows t0 + ii (ii < nt), columns jj < h; mirror row-major
+    for (int e = tid; e < 128 * 128; e += 256) {
+      const int ii = e & 127, jj = e >> 7;
+      if (ii < nt && jj < h) B[(size_t)jj * ldb + t0 + ii] = Cs[jj * kLm + ii];
+    }
+    if (mir)
+      for (int e = tid; e < 128 * 128; e += 256) {
+        const int jj = e & 127, ii = e >> 7;
+        if (ii < nt && jj < h) mir[(size_t)(t0 + ii) * ldm + jj] = __float2bfloat16_rn(Cs[jj * kLm + ii]);
+      }
+  }
+}
+
 // B (h x w, ldb) := Dinv B, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h);
 // one CTA per 64 columns, 256 threads each computing 4 rows x 8 columns, FP32.
 constexpr int kLdI = 132, kLdB = 68;
+// (the narrow leaves: 64 columns per CTA; mirror writes as k_leaf_mult's)
 __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict__ Dinv, int h, float* B, long ldb,
-                                                         int w) {
+                                                         int w, __nv_bfloat16* __restrict__ mir, long ldm) {
   extern __shared__ __align__(16) float sm[];
   float* li = sm;                 // li[k * kLdI + r] = Dinv(r, k)
   float* bs = sm + 128 * kLdI;    // bs[k * kLdB + c] = B(k, c0 + c)
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * 64, nc = min(64, w - c0);
-  for (int i = tid; i < 128 * 128; i += 256) {
-    const int r = i & 127, k = i >> 7;
-    li[k * kLdI + r] = Dinv[(size_t)k * 128 + r];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {  // Dinv column k -> li row k (16-byte asynchronous copies)
+    const int e = tid + 256 * q, k = e >> 5, r4 = (e & 31) * 4;
+    cp16(&li[k * kLdI + r4], &Dinv[(size_t)k * 128 + r4], 16);
   }
-  for (int i = tid; i < 128 * 64; i += 256) {
-    const int k = i & 127, cc = i >> 7;
-    bs[k * kLdB + cc] = (k < h && cc < nc) ? B[(size_t)(c0 + cc) * ldb + k] : 0.f;
+  {
+    float4 v[8];  // B (k, c0 + cc), k contiguous in memory: float4 loads, transposed into bs
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      v[q] = (cc < nc && k4 < h) ? *reinterpret_cast<const float4*>(&B[(size_t)(c0 + cc) * ldb + k4])
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      bs[(k4 + 0) * kLdB + cc] = k4 + 0 < h ? v[q].x : 0.f;
+      bs[(k4 + 1) * kLdB + cc] = k4 + 1 < h ? v[q].y : 0.f;
+      bs[(k4 + 2) * kLdB + cc] = k4 + 2 < h ? v[q].z : 0.f;
+      bs[(k4 + 3) * kLdB + cc] = k4 + 3 < h ? v[q].w : 0.f;
+    }
   }
+  cp_wait_all();
   __syncthreads();
   const int tr = tid & 31, tc = tid >> 5;  // rows 4 tr .. 4 tr + 3, columns 8 tc .. 8 tc + 7
   float acc[4][8];
@@ -189,7 +394,10 @@ __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict_
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int r = 4 * tr + i;
-        if (r < h) B[(size_t)(c0 + cc) * ldb + r] = acc[i][j];
+        if (r < h) {
+          B[(size_t)(c0 + cc) * ldb + r] = acc[i][j];
+          if (mir) mir[(size_t)(c0 + cc) * ldm + r] = __float2bfloat16_rn(acc[i][j]);
+        }
       }
   }
 }
@@ -197,20 +405,35 @@ __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict_
 // B (m x h, ldb) := B Dinv, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h);
 // one CTA per 64 rows, 256 threads each computing 4 rows x 8 columns, FP32.
 __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict__ Dinv, int h, float* B, long ldb,
-                                                          int m) {
+                                                          int m, __nv_bfloat16* __restrict__ mir, long ldm) {
   extern __shared__ __align__(16) float sm[];
   float* us = sm;                 // us[k * kLdI + c] = Dinv(k, c)
   float* bs = sm + 128 * kLdI;    // bs[k * kLdB + rr] = B(r0 + rr, k)
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * 64, nr = min(64, m - r0);
-  for (int i = tid; i < 128 * 128; i += 256) {
-    const int k = i & 127, cc = i >> 7;
-    us[k * kLdI + cc] = Dinv[(size_t)cc * 128 + k];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {  // B (r0 + rr, k), rr contiguous -> bs row k (16-byte copies)
+    const int e = tid + 256 * q, k = e >> 4, rr4 = (e & 15) * 4;
+    const int valid = (k < h) ? max(0, min(4, nr - rr4)) * 4 : 0;
+    cp16(&bs[k * kLdB + rr4], valid ? (const void*)&B[(size_t)k * ldb + r0 + rr4] : (const void*)B, valid);
   }
-  for (int i = tid; i < 64 * 128; i += 256) {
-    const int rr = i & 63, k = i >> 6;
-    bs[k * kLdB + rr] = (k < h && rr < nr) ? B[(size_t)k * ldb + r0 + rr] : 0.f;
+  {
+    float4 v[16];  // Dinv (k, cc) at Dinv[cc * 128 + k]: float4 loads along k, transposed into us
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      v[q] = *reinterpret_cast<const float4*>(&Dinv[(size_t)cc * 128 + k4]);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      us[(k4 + 0) * kLdI + cc] = v[q].x;
+      us[(k4 + 1) * kLdI + cc] = v[q].y;
+      us[(k4 + 2) * kLdI + cc] = v[q].z;
+      us[(k4 + 3) * kLdI + cc] = v[q].w;
+    }
   }
+  cp_wait_all();
   __syncthreads();
   const int tr = tid & 15, tc = tid >> 4;  // rows 4 tr .. 4 tr + 3, columns 8 tc .. 8 tc + 7
   float acc[4][8];
@@ -239,6 +462,17 @@ __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict
         const int rr = 4 * tr + i;
         if (rr < nr) B[(size_t)cc * ldb + r0 + rr] = acc[i][j];
       }
+  }
+  if (mir) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int rr = 4 * tr + i;
+      if (rr >= nr) continue;
+      __nv_bfloat16* dst = mir + (size_t)(r0 + rr) * ldm + 8 * tc;
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (8 * tc + j < h) dst[j] = __float2bfloat16_rn(acc[i][j]);
+    }
   }
 }
 
@@ -428,21 +662,40 @@ struct MixedSolver::Impl {
   int max_restarts = 8, krylov = 10;
   int sms = 148;
   Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs, dl32, du32;
+  // BF16 mirrors of the factors (L part row-major, U part column-major), written by the triangular
+  // solve leaves as the entries become final; the GEMMs read their operands there by position, so no
+  // operand copies are made.  Used when the GPU has room for them (4 n^2 bytes), else copies.
+  Buf am, bm;
+  bool mirrors = false;
+  long ldm = 0;
+  alignas(64) unsigned char map_am[kTensorMapBytes], map_bm[kTensorMapBytes];
+  const void* mirror_key[2] = {};
   int* d_status() { return status.as<int>(); }
+  __nv_bfloat16* am_at(int r, int c) const { return am.as<__nv_bfloat16>() + (size_t)r * ldm + c; }
+  __nv_bfloat16* bm_at(int r, int c) const { return bm.as<__nv_bfloat16>() + (size_t)c * ldm + r; }
 
-  // C (m x n at c, ldc) -= A (m x k, col-major fp32) B (k x n col-major fp32) via BF16 tensor cores
-  void gemm(int m, int n, int k, const float* A, long lda, const float* B, long ldb, float* C, long ldc,
-            cudaStream_t s) {
+  // C = block (cr, cc) of the matrix, m x n, -= A (block (ar, ac), m x k) B (block (br, bc), k x n),
+  // BF16 tensor cores: operands from the mirrors by position, or copied into the operand buffers
+  void gemm(int m, int n, int k, int ar, int ac, int br, int bc, int cr, int cc, cudaStream_t s) {
     if (m <= 0 || n <= 0 || k <= 0) return;
+    float* C = at_(cr, cc);
+    KernelTimer& kt = kernel_timer(1);
+    if (mirrors) {
+      prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
+      kt.begin(s);
+      ck(gemm_bf16_tc_minus_at(m, n, k, map_am, ar, ac, map_bm, bc, br, C, ld32, d_status(), s), "tensor-core GEMM");
+      kt.end(s, 2.0 * m * n * k);
+      prof.end(s);
+      return;
+    }
     if (m > op_rows || n > op_rows || round_up(k, 64) > op_ld) throw std::runtime_error("GEMM larger than its operand buffers");
     prof.begin("casts", 0, s);
-    ck(cast_transpose_bf16(A, lda, m, k, at.p, op_ld, s), "cast A");
-    ck(cast_bf16(B, ldb, k, n, bt.p, op_ld, s), "cast B");
+    ck(cast_transpose_bf16(at_(ar, ac), ld32, m, k, at.p, op_ld, s), "cast A");
+    ck(cast_bf16(at_(br, bc), ld32, k, n, bt.p, op_ld, s), "cast B");
     prof.end(s);
     prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
-    KernelTimer& kt = kernel_timer(1);
     kt.begin(s);
-    ck(gemm_bf16_tc_minus_maps(m, n, k, map_a, map_b, C, ldc, d_status(), s), "tensor-core GEMM");
+    ck(gemm_bf16_tc_minus_maps(m, n, k, map_a, map_b, C, ld32, d_status(), s), "tensor-core GEMM");
     kt.end(s, 2.0 * m * n * k);
     prof.end(s);
   }
@@ -458,10 +711,15 @@ struct MixedSolver::Impl {
   void trsm_llu(int kd, int h, int c0, int w, cudaStream_t s) {
     if (h <= 0 || w <= 0) return;
     if (h <= kLeaf) {
-      const size_t smem = (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float);
-      prof.begin("trsm leaf (left)", 2.0 * h * h * w, s);
-      k_apply_inv_left<<<(w + 63) / 64, 256, smem, s>>>(dl32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf, h,
-                                                       at_(kd, c0), ld32, w);
+      const float* dinv = dl32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf;
+      __nv_bfloat16* mir = mirrors ? bm_at(kd, c0) : nullptr;
+      prof.begin(w >= kWideLeaf ? "trsm leaf (left, wide)" : "trsm leaf (left)", 2.0 * h * h * w, s);
+      if (w >= kWideLeaf)
+        k_leaf_mult<true><<<(w + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(dinv, h, at_(kd, c0), ld32,
+                                                                                           w, mir, ldm);
+      else
+        k_apply_inv_left<<<(w + 63) / 64, 256, (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float), s>>>(
+            dinv, h, at_(kd, c0), ld32, w, mir, ldm);
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
@@ -469,7 +727,7 @@ struct MixedSolver::Impl {
     }
     const int h1 = split(h);
     trsm_llu(kd, h1, c0, w, s);
-    gemm(h - h1, w, h1, at_(kd + h1, kd), ld32, at_(kd, c0), ld32, at_(kd + h1, c0), ld32, s);
+    gemm(h - h1, w, h1, kd + h1, kd, kd, c0, kd + h1, c0, s);
     trsm_llu(kd + h1, h - h1, c0, w, s);
   }
 
@@ -477,10 +735,15 @@ struct MixedSolver::Impl {
   void trsm_ru(int kd, int h, int r0, int m, cudaStream_t s) {
     if (h <= 0 || m <= 0) return;
     if (h <= kLeaf) {
-      const size_t smem = (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float);
-      prof.begin("trsm leaf (right)", 2.0 * h * h * m, s);
-      k_apply_inv_right<<<(m + 63) / 64, 256, smem, s>>>(du32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf, h,
-                                                        at_(r0, kd), ld32, m);
+      const float* dinv = du32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf;
+      __nv_bfloat16* mir = mirrors ? am_at(r0, kd) : nullptr;
+      prof.begin(m >= kWideLeaf ? "trsm leaf (right, wide)" : "trsm leaf (right)", 2.0 * h * h * m, s);
+      if (m >= kWideLeaf)
+        k_leaf_mult<false><<<(m + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(dinv, h, at_(r0, kd),
+                                                                                            ld32, m, mir, ldm);
+      else
+        k_apply_inv_right<<<(m + 63) / 64, 256, (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float), s>>>(
+            dinv, h, at_(r0, kd), ld32, m, mir, ldm);
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
@@ -488,7 +751,7 @@ struct MixedSolver::Impl {
     }
     const int h1 = split(h);
     trsm_ru(kd, h1, r0, m, s);
-    gemm(m, h - h1, h1, at_(r0, kd), ld32, at_(kd, kd + h1), ld32, at_(r0, kd + h1), ld32, s);
+    gemm(m, h - h1, h1, r0, kd, kd, kd + h1, r0, kd + h1, s);
     trsm_ru(kd + h1, h - h1, r0, m, s);
   }
 
@@ -496,7 +759,7 @@ struct MixedSolver::Impl {
   // inverted (both triangles) right after it is factored, for the triangular-solve leaves above it
   void rlu(int k0, int sz, cudaStream_t s) {
     if (sz <= kLeaf) {
-      const size_t smem = (size_t)3 * 128 * kLdS * sizeof(float);
+      const size_t smem = (size_t)(128 * kLdS + 4 * 128) * sizeof(float);
       const size_t off = (size_t)(k0 / kLeaf) * kLeaf * kLeaf;
       prof.begin("LU leaf + inverses", 0, s);
       k_lu32_leaf_inv<<<1, 512, smem, s>>>(at_(k0, k0), ld32, sz, dl32.as<float>() + off, du32.as<float>() + off,
@@ -510,7 +773,7 @@ struct MixedSolver::Impl {
     rlu(k0, h, s);
     trsm_llu(k0, h, k0 + h, r, s);   // U12
     trsm_ru(k0, h, k0 + h, r, s);    // L21
-    gemm(r, r, h, at_(k0 + h, k0), ld32, at_(k0, k0 + h), ld32, at_(k0 + h, k0 + h), ld32, s);
+    gemm(r, r, h, k0 + h, k0, k0, k0 + h, k0 + h, k0 + h, s);
     rlu(k0 + h, r, s);
   }
 
@@ -574,30 +837,55 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
                         cudaEvent_t ev_assembled, cudaEvent_t ev_factored) {
   Impl& P = *p_;
   P.n3 = 3 * m.n;
+  // columns 128-byte aligned, but not a multiple of 1 KB apart: the triangular solves read 64
+  // columns at once, and a power-of-two-like stride puts them all on the same memory partitions
   P.ld32 = round_up(P.n3, 32);
+  if ((P.ld32 * 4) % 1024 == 0) P.ld32 += 32;
   P.gr64 = gr64;
   P.ld64 = ld;
   P.tol = std::max(1e-15, std::min(0.1 * eps, 1e-12));
-  P.lu32.ensure((size_t)P.ld32 * P.n3 * sizeof(float), "FP32 copy of GR");
+  // (+256 bytes: the solve leaves read whole 16-byte groups at the end of the last column)
+  P.lu32.ensure((size_t)P.ld32 * P.n3 * sizeof(float) + 256, "FP32 copy of GR");
   P.dl32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (L)");
   P.du32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (U)");
-  const long half = P.n3 / 2 + 128;
-  const long op_ld = round_up(half, 64);
-  P.at.ensure((size_t)half * op_ld * 2, "BF16 operand A");
-  P.bt.ensure((size_t)half * op_ld * 2, "BF16 operand B");
-  if (P.op_ld != op_ld || P.op_rows != (int)half || P.map_key[0] != P.at.p || P.map_key[1] != P.bt.p) {
-    if (!tc_operand_maps(P.at.p, (int)half, op_ld, P.bt.p, (int)half, op_ld, P.map_a, P.map_b))
-      throw std::runtime_error("cannot build the tensor maps of the BF16 operands");
-    P.op_ld = op_ld;
-    P.op_rows = (int)half;
-    P.map_key[0] = P.at.p;
-    P.map_key[1] = P.bt.p;
+  // BF16 mirrors when they fit with 4 GB to spare, else operand copies per product
+  const long ldm = round_up(P.n3, 64);
+  const size_t mirror_bytes = (size_t)P.n3 * ldm * 2;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t held = (P.am.p ? P.am.bytes : 0) + (P.bm.p ? P.bm.bytes : 0);
+  P.mirrors = free_b + held >= 2 * mirror_bytes + ((size_t)4 << 30) && std::getenv("BEST_GPU_NO_MIRRORS") == nullptr;
+  if (P.mirrors) {
+    P.am.ensure(mirror_bytes, "BF16 mirror (L)");
+    P.bm.ensure(mirror_bytes, "BF16 mirror (U)");
+    if (P.ldm != ldm || P.mirror_key[0] != P.am.p || P.mirror_key[1] != P.bm.p) {
+      if (!tc_mirror_maps(P.am.p, P.bm.p, P.n3, ldm, P.map_am, P.map_bm))
+        throw std::runtime_error("cannot build the tensor maps of the BF16 mirrors");
+      P.ldm = ldm;
+      P.mirror_key[0] = P.am.p;
+      P.mirror_key[1] = P.bm.p;
+    }
+  } else {
+    const long half = P.n3 / 2 + 128;
+    const long op_ld = round_up(half, 64);
+    P.at.ensure((size_t)half * op_ld * 2, "BF16 operand A");
+    P.bt.ensure((size_t)half * op_ld * 2, "BF16 operand B");
+    if (P.op_ld != op_ld || P.op_rows != (int)half || P.map_key[0] != P.at.p || P.map_key[1] != P.bt.p) {
+      if (!tc_operand_maps(P.at.p, (int)half, op_ld, P.bt.p, (int)half, op_ld, P.map_a, P.map_b))
+        throw std::runtime_error("cannot build the tensor maps of the BF16 operands");
+      P.op_ld = op_ld;
+      P.op_rows = (int)half;
+      P.map_key[0] = P.at.p;
+      P.map_key[1] = P.bt.p;
+    }
   }
   ck(tc_gemm_prepare(), "tensor-core GEMM attributes");
   static bool attrs = false;
   if (!attrs) {
     const int big = 200 * 1024;
     ck(cudaFuncSetAttribute(k_lu32_leaf_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024), "attr");
+    ck(cudaFuncSetAttribute(k_leaf_mult<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_leaf_mult<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
     ck(cudaFuncSetAttribute(k_apply_inv_left, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
     ck(cudaFuncSetAttribute(k_apply_inv_right, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
     attrs = true;
@@ -610,7 +898,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   } else {
     // the recursion's launches depend only on the order and the buffers: capture them once as a
     // CUDA graph and replay it
-    const void* key[5] = {P.lu32.p, P.at.p, P.bt.p, P.dl32.p, P.du32.p};
+    const void* key[5] = {P.lu32.p, P.mirrors ? P.am.p : P.at.p, P.mirrors ? P.bm.p : P.bt.p, P.dl32.p, P.du32.p};
     if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 5, P.graph_key)) {
       if (P.graph) cudaGraphExecDestroy(P.graph);
       P.graph = nullptr;
@@ -658,7 +946,9 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
   const int max_restarts = P.max_restarts;
   int total_iters = 0;
   double worst = 0.0;
+  const bool fresh_scratch = !P.trsv.p || P.trsv.bytes < trsv_scratch_bytes(n);
   P.trsv.ensure(trsv_scratch_bytes(n), "solve scratch");
+  if (fresh_scratch) ck(cudaMemsetAsync(P.trsv.p, 0, P.trsv.bytes, s), "solve scratch clear");  // flags start at 0
   for (int c0 = 0; c0 < nrhs; c0 += 16) {
     const int q = std::min(16, nrhs - c0);
     const size_t blk = (size_t)n * q;

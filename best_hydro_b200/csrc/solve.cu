@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <vector>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -115,6 +117,14 @@ __global__ void k_copy_cols(const T* __restrict__ Y, long ldy, int n, int nrhs, 
   if (i >= n) return;
   for (int r = 0; r < nrhs; ++r) X[(size_t)r * ldx + i] = Y[(size_t)r * ldy + i];
 }
+
+// asynchronous copy of one element global -> shared (4 or 8 bytes)
+template <int B>
+__device__ __forceinline__ void cp_async_elem(void* sdst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Warp 0 waits until flags[jb] == epoch, then counts how many more flags in the direction `step`
 // (+1 or -1) are ready too, up to 32 and within [lo, hi).  Returns that count (>= 1), or 0 when the
@@ -282,7 +292,7 @@ cudaError_t lu_perm_from_ipiv(const int* ipiv, int n, int* perm, cudaStream_t s)
   return cudaGetLastError();
 }
 
-size_t trsv_scratch_bytes(int n) { return TrsvScratch::bytes(n); }
+size_t trsv_scratch_bytes(int n);  // (below: the base scratch and the split solves' area)
 
 // Solves in place with FP64 factors.  The scratch must hold trsv_scratch_bytes(n) bytes and be
 // zeroed once when first allocated (the flags carry an epoch; no per-call clearing is needed).
@@ -382,37 +392,97 @@ __global__ void __launch_bounds__(kIb) k_diag_inverses(const F* __restrict__ LU,
   for (int i = 0; i < kIb; ++i) du[(size_t)c * kIb + i] = (FI)((c < h && i < h) ? x[i] : 0.0);
 }
 
-// One triangle on Y (n x nrhs <= kIrhs, ldy): LOWER = unit lower L with block inverses DI, blocks in
-// increasing order; otherwise upper U, decreasing.  256 threads: row = t % 128, half = t / 128 of
-// the 128-wide inner dimension.  Each thread loads its 64 factor entries of the next block into
-// registers before waiting for that block's unknowns, so the factor streams while the chain of
-// dependencies advances.
-// TRANS: the triangle is the transpose of the stored one (U^T, lower, with DI = DU; or L^T, upper,
-// with DI = DL): entry (i, j) is read from LU(j, i) and the block inverses are applied transposed;
-// each thread then reads 64 consecutive entries of one stored column.
+// One triangle on Y (n x nrhs <= kIrhs, ldy) with the block inverses DI: LOWER = unit lower L, block
+// rows in increasing order; otherwise upper U, decreasing.  TRANS: the triangle is the transpose of
+// the stored one (U^T, lower, with DI = DU; or L^T, upper, with DI = DL): entry (i, j) is read from
+// LU(j, i) and the block inverses are applied transposed.
+//
+// Work is split in tasks taken in ticket order by persistent CTAs.  In the order of the solve
+// (q-space: q = block row for LOWER, nblk-1-block row otherwise), row i's final task F(i) does its
+// last kLead off-diagonal blocks [i - kLead, i), adds the partial sums of the blocks before them in a
+// fixed order (so results do not depend on scheduling), applies the inverted diagonal block and
+// publishes x_i.  The blocks before are cut, walking away from the diagonal, into chunks of 2, 4,
+// 8 and then kChunk blocks, each a partial task P(i, s) that streams its blocks into a slot of its
+// own.  A chunk is issued right after the final task of its newest block row (the last x it needs):
+// the chunks near the diagonal, which become ready last, are short, so they finish within the few
+// rows the chain advances meanwhile, and the far ones, ready long before, stream the bulk of the
+// factor.  The host builds the task list (every task after all tasks it waits for, so the waits
+// always end; each is bounded anyway) and CTAs take it in ticket order.
+constexpr int kChunk = 16;
+constexpr int kLead = 2;
+
 template <typename F, typename FI, bool LOWER, bool TRANS = false>
 __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
                                                   double* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
-                                                  unsigned epoch, int* status) {
+                                                  unsigned epoch, int* status, unsigned* __restrict__ cnt,
+                                                  double* __restrict__ part, int smax, const int4* __restrict__ tasks,
+                                                  int ntasks) {
   __shared__ double s_y[kIb][kIrhs];
+  __shared__ double s_b[kIb][kIrhs];
   __shared__ double s_acc[2][kIb][kIrhs];
-  __shared__ int s_blk, s_cnt;
+  __shared__ int s_task[4], s_cnt;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  FI* s_di = reinterpret_cast<FI*>(s_dyn);  // the inverted diagonal block, stride kIb + 1
   const int nblk = (n + kIb - 1) / kIb;
   const int tid = threadIdx.x, row = tid & (kIb - 1), half = tid >> 7;
   for (;;) {
-    if (tid == 0) s_blk = (int)atomicAdd(ticket, 1u);
+    // task: x = slot (partial task) or -1 - number of partial tasks (final task); y = row; [z, w) blocks
+    if (tid == 0) {
+      const unsigned t = atomicAdd(ticket, 1u);
+      const int4 tk = t < (unsigned)ntasks ? tasks[t] : make_int4(0, -1, 0, 0);
+      s_task[0] = tk.x;
+      s_task[1] = tk.y;
+      s_task[2] = tk.z;
+      s_task[3] = tk.w;
+    }
     __syncthreads();
-    const int t = s_blk;
-    if (t >= nblk) return;
-    const int blk = LOWER ? t : nblk - 1 - t;
+    const int code = s_task[0], i = s_task[1], q0 = s_task[2], q1 = s_task[3];
+    if (i < 0) return;
+    const int kind = code < 0 ? 1 : 0, sidx = code;
+    const bool fin = kind == 1;
+    const int blk = LOWER ? i : nblk - 1 - i;
     const int r0 = blk * kIb, nr = min(kIb, n - r0);
     const bool live = row < nr;
     double acc[kIrhs];
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) acc[r] = 0.0;
-    const int nq = LOWER ? blk : nblk - 1 - blk;
-    int confirmed = 0;
-    for (int q = 0; q < nq; ++q) {
+    if (fin) {
+      // before any wait: the inverted diagonal block into shared memory (asynchronous copies), the
+      // block's right-hand sides, and the partial sums of the earlier chunks
+      const FI* dblk = DI + (size_t)blk * kIb * kIb;
+      for (int e = tid; e < kIb * kIb; e += 256) cp_async_elem<sizeof(FI)>(s_di + (e >> 7) * (kIb + 1) + (e & 127), dblk + e);
+      for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+        const int rr = idx / kIrhs, r = idx % kIrhs;
+        s_b[rr][r] = (rr < nr && r < nrhs) ? Y[(size_t)r * ldy + r0 + rr] : 0.0;
+      }
+      const int nparts = -1 - code;
+      if (tid == 0) {
+        int ok = 1;
+        unsigned spins = 0;
+        while (nparts > 0 && ld_acquire_u32(cnt + i) < (unsigned)nparts) {
+          if (++spins > kSpinLimit) {
+            atomicExch(status, (int)kWaitTimeout);
+            ok = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+        s_cnt = ok;
+      }
+      __syncthreads();
+      if (!s_cnt) {
+        cp_async_wait_all();
+        return;
+      }
+      if (half == 0) {
+        const double* p = part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs;
+        for (int sp = 0; sp < nparts; ++sp)
+#pragma unroll
+          for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + (size_t)sp * kIb * kIrhs + r);
+      }
+    }
+    int confirmed = q0;
+    for (int q = q0; q < q1; ++q) {
       const int jb = LOWER ? q : nblk - 1 - q;
       const int c0 = jb * kIb, nc = min(kIb, n - c0);
       // this thread's 64 entries of block (blk, jb), loaded before the wait
@@ -427,10 +497,13 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
         for (int kk = 0; kk < 64; ++kk) lv[kk] = (live && half * 64 + kk < nc) ? col[(size_t)kk * lda] : (F)0;
       }
       if (q >= confirmed) {
-        const int cnt = LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, &s_cnt)
-                              : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, &s_cnt);
-        if (cnt == 0) return;
-        confirmed = q + cnt;
+        const int c = LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, &s_cnt)
+                            : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, &s_cnt);
+        if (c == 0) {
+          cp_async_wait_all();
+          return;
+        }
+        confirmed = q + c;
       }
       for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
         const int rr = idx / kIrhs, r = idx % kIrhs;
@@ -447,30 +520,37 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     }
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
-    // this thread's row of the inverse block (its column, transposed)
-    const FI* di = TRANS ? DI + (size_t)blk * kIb * kIb + (size_t)row * kIb : DI + (size_t)blk * kIb * kIb + row;
-    const long dstride = TRANS ? 1 : kIb;
     __syncthreads();
-    // right-hand side of the block: b - off-diagonal sums
+    if (!fin) {
+      double* slot = part + ((size_t)i * smax + sidx) * kIb * kIrhs;
+      for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+        const int rr = idx / kIrhs, r = idx % kIrhs;
+        slot[idx] = s_acc[0][rr][r] + s_acc[1][rr][r];
+      }
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        atomicAdd(cnt + i, 1u);
+      }
+      continue;
+    }
+    // final task: right-hand side b + (negative) off-diagonal sums, then x = D^-1 (...)
     for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
       const int rr = idx / kIrhs, r = idx % kIrhs;
-      s_y[rr][r] = (rr < nr && r < nrhs) ? Y[(size_t)r * ldy + r0 + rr] + (s_acc[0][rr][r] + s_acc[1][rr][r]) : 0.0;
+      s_y[rr][r] = s_b[rr][r] + (s_acc[0][rr][r] + s_acc[1][rr][r]);
     }
+    cp_async_wait_all();
     __syncthreads();
-    // x = D^-1 (b - ...): each half does 64 of the 128 products
+    // each half does 64 of the 128 products; D^-1 (row, c) at s_di[c * 129 + row] (transposed:
+    // the other way round)
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) acc[r] = 0.0;
+#pragma unroll 8
+    for (int kk = 0; kk < 64; ++kk) {
+      const int cc = half * 64 + kk;
+      const double dv = TRANS ? (double)s_di[row * (kIb + 1) + cc] : (double)s_di[cc * (kIb + 1) + row];
 #pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      double dv[32];
-#pragma unroll
-      for (int kk = 0; kk < 32; ++kk) dv[kk] = (double)di[(size_t)(half * 64 + b * 32 + kk) * dstride];
-#pragma unroll
-      for (int kk = 0; kk < 32; ++kk) {
-        const int cc = half * 64 + b * 32 + kk;
-#pragma unroll
-        for (int r = 0; r < kIrhs; ++r) acc[r] += dv[kk] * s_y[cc][r];
-      }
+      for (int r = 0; r < kIrhs; ++r) acc[r] += dv * s_y[cc][r];
     }
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
@@ -487,31 +567,91 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
   }
 }
 
-template <typename F, typename FI>
-cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int n, double* Y, long ldy, int nrhs,
-                          void* scratch, int* d_status, cudaStream_t s) {
+// Scratch of the split solves, after the base scratch: per-row partial-task counters, the partial
+// sums [nblk][smax][128][kIrhs], and the task list.
+struct SplitScratch {
+  static int nblk(int n) { return (n + kIb - 1) / kIb; }
+  static int smax(int n) { return 4 + nblk(n) / kChunk; }
+  static size_t max_tasks(int n) { return (size_t)nblk(n) * (1 + smax(n)); }
+  static size_t base(int n) { return (TrsvScratch::bytes(n) + 255) / 256 * 256; }
+  static size_t part_off(int n) { return base(n) + ((size_t)nblk(n) * 4 + 255) / 256 * 256; }
+  static size_t task_off(int n) { return part_off(n) + (size_t)nblk(n) * smax(n) * kIb * kIrhs * sizeof(double); }
+  static size_t bytes(int n) { return task_off(n) + max_tasks(n) * sizeof(int4); }
+};
+
+// The task list of a triangle with nblk block rows (see k_trsv_inv), built once per size.
+const std::vector<int4>& split_tasks(int nblk) {
+  static std::map<int, std::vector<int4>> cache;
+  auto it = cache.find(nblk);
+  if (it != cache.end()) return it->second;
+  std::vector<std::vector<int4>> after(nblk);  // partial tasks issued after F(b)
+  std::vector<int> nparts(nblk, 0);
+  for (int i = 0; i < nblk; ++i) {
+    int e = i - kLead, w = 2, sidx = 0;
+    while (e > 0) {
+      const int lo = std::max(0, e - w);
+      after[e - 1].push_back(make_int4(sidx, i, lo, e));
+      e = lo;
+      w = std::min(2 * w, kChunk);
+      ++sidx;
+    }
+    nparts[i] = sidx;
+  }
+  std::vector<int4> list;
+  for (int b = 0; b < nblk; ++b) {
+    list.push_back(make_int4(-1 - nparts[b], b, std::max(0, b - kLead), b));
+    for (const int4& t : after[b]) list.push_back(t);
+  }
+  return cache.emplace(nblk, std::move(list)).first->second;
+}
+
+// one triangle: ticket, counters and task list set, then the persistent launch (one CTA per SM)
+template <typename F, typename FI, bool LOWER, bool TRANS>
+cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, double* Yc, long ldy, int q, void* scratch,
+                     unsigned epoch, int* d_status, cudaStream_t s) {
   unsigned char* base = static_cast<unsigned char*>(scratch);
   unsigned* ticket = reinterpret_cast<unsigned*>(base);
   unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
+  unsigned* cnt = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
+  double* part = reinterpret_cast<double*>(base + SplitScratch::part_off(n));
+  int4* tasks = reinterpret_cast<int4*>(base + SplitScratch::task_off(n));
+  const std::vector<int4>& list = split_tasks(SplitScratch::nblk(n));
+  if (list.size() > SplitScratch::max_tasks(n)) return cudaErrorInvalidValue;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int nblk = (n + kIb - 1) / kIb;
-  const int grid = std::min(nblk, sms * 3);
+  cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(cnt, 0, (size_t)SplitScratch::nblk(n) * 4, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(tasks, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return e;
+  const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(FI);
+  static bool attr = false;
+  if (!attr) {
+    if ((e = cudaFuncSetAttribute(k_trsv_inv<F, FI, LOWER, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dsmem)) != cudaSuccess)
+      return e;
+    attr = true;
+  }
+  k_trsv_inv<F, FI, LOWER, TRANS><<<sms, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
+                                                          cnt, part, SplitScratch::smax(n), tasks, (int)list.size());
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+template <typename F, typename FI>
+cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int n, double* Y, long ldy, int nrhs,
+                          void* scratch, int* d_status, cudaStream_t s) {
   for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
     const int q = std::min(kIrhs, nrhs - c0);
     double* Yc = Y + (size_t)c0 * ldy;
     g_epoch += 2;
     if (g_epoch == 0) g_epoch = 2;
-    cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
+    cudaError_t e = trsv_one<F, FI, true, false>(LU, lda, DL, n, Yc, ldy, q, scratch, g_epoch, d_status, s);
     if (e != cudaSuccess) return e;
-    k_trsv_inv<F, FI, true><<<grid, 256, 0, s>>>(LU, lda, DL, n, Yc, ldy, q, flags, ticket, g_epoch, d_status);
-    BGPU_COUNT_LAUNCH();
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
-    k_trsv_inv<F, FI, false><<<grid, 256, 0, s>>>(LU, lda, DU, n, Yc, ldy, q, flags, ticket, g_epoch + 1, d_status);
-    BGPU_COUNT_LAUNCH();
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = trsv_one<F, FI, false, false>(LU, lda, DU, n, Yc, ldy, q, scratch, g_epoch + 1, d_status, s)) !=
+        cudaSuccess)
+      return e;
   }
   return cudaSuccess;
 }
@@ -519,30 +659,16 @@ cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int
 // Y := U^-T Y, then L^-T Y (the transposed solve, FP64 factors)
 cudaError_t trsv_inv_pair_trans(const double* LU, long lda, const double* DL, const double* DU, int n, double* Y,
                                 long ldy, int nrhs, void* scratch, int* d_status, cudaStream_t s) {
-  unsigned char* base = static_cast<unsigned char*>(scratch);
-  unsigned* ticket = reinterpret_cast<unsigned*>(base);
-  unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int nblk = (n + kIb - 1) / kIb;
-  const int grid = std::min(nblk, sms * 3);
   for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
     const int q = std::min(kIrhs, nrhs - c0);
     double* Yc = Y + (size_t)c0 * ldy;
     g_epoch += 2;
     if (g_epoch == 0) g_epoch = 2;
-    cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
+    cudaError_t e = trsv_one<double, double, true, true>(LU, lda, DU, n, Yc, ldy, q, scratch, g_epoch, d_status, s);
     if (e != cudaSuccess) return e;
-    k_trsv_inv<double, double, true, true><<<grid, 256, 0, s>>>(LU, lda, DU, n, Yc, ldy, q, flags, ticket, g_epoch,
-                                                                 d_status);
-    BGPU_COUNT_LAUNCH();
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
-    k_trsv_inv<double, double, false, true><<<grid, 256, 0, s>>>(LU, lda, DL, n, Yc, ldy, q, flags, ticket,
-                                                                  g_epoch + 1, d_status);
-    BGPU_COUNT_LAUNCH();
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = trsv_one<double, double, false, true>(LU, lda, DL, n, Yc, ldy, q, scratch, g_epoch + 1, d_status, s)) !=
+        cudaSuccess)
+      return e;
   }
   return cudaSuccess;
 }
@@ -576,6 +702,8 @@ cudaError_t getrs64_trans_inv(const double* LU, long lda, const double* DL, cons
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
+
+size_t trsv_scratch_bytes(int n) { return SplitScratch::bytes(n); }
 
 size_t diag_inverse_elems(int n) { return (size_t)((n + kIb - 1) / kIb) * kIb * kIb; }
 
@@ -686,7 +814,7 @@ unsigned char* g_noalloc_base[kMaxDevices] = {};
 size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 
 // [0, 256) status word | trsv scratch (ticket, readiness flags, permuted right-hand sides) | perm
-size_t noalloc_bytes(int n) { return 256 + round256(trsv_scratch_bytes(n)) + round256(4 * (size_t)n); }
+size_t noalloc_bytes(int n) { return 256 + round256(TrsvScratch::bytes(n)) + round256(4 * (size_t)n); }
 
 int noalloc_max_n() {
   int lo = 0, hi = 1 << 24;
@@ -746,7 +874,7 @@ extern "C" int bgpu_dgetrs_noalloc(int n, int nrhs, const double* d_a, int lda, 
   if (e == cudaSuccess) {
     int* status = reinterpret_cast<int*>(base);
     unsigned char* trsv = base + 256;
-    int* perm = reinterpret_cast<int*>(base + 256 + round256(trsv_scratch_bytes(n)));
+    int* perm = reinterpret_cast<int*>(base + 256 + round256(TrsvScratch::bytes(n)));
     if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) == cudaSuccess &&
         (e = lu_perm_from_ipiv(d_ipiv, n, perm, s)) == cudaSuccess &&
         (e = getrs64(d_a, lda, n, perm, d_b, ldb, nrhs, trsv, status, s)) == cudaSuccess &&

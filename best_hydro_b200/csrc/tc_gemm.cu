@@ -132,9 +132,12 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
   tn = (tile % per_group) / group_m;
 }
 
+// A's tiles start at row a_y0, column (K) a_x0 of its tensor map; B's at row b_y0, column b_x0 of its
+// (both 0 for operand buffers that hold just this product).
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int m, int n,
-                   int k, float* __restrict__ C, long ldc, int tiles_m, int tiles_n, int* status) {
+                   int k, float* __restrict__ C, long ldc, int tiles_m, int tiles_n, int* status, int a_y0, int a_x0,
+                   int b_y0, int b_x0) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;
@@ -186,8 +189,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           if (*(volatile int*)&s_abort) break;
           mbar_expect_tx(&full[s], kStageA + kStageB);
-          tma_load_2d(sA + s * kStageA, &tmA, kt * BK, tm * BM, &full[s]);
-          tma_load_2d(sB + s * kStageB, &tmB, kt * BK, tn * BN, &full[s]);
+          tma_load_2d(sA + s * kStageA, &tmA, a_x0 + kt * BK, a_y0 + tm * BM, &full[s]);
+          tma_load_2d(sB + s * kStageB, &tmB, b_x0 + kt * BK, b_y0 + tn * BN, &full[s]);
         }
       }
     }
@@ -389,7 +392,30 @@ cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, cons
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
   k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
       *static_cast<const CUtensorMap*>(map_a), *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m,
-      tiles_n, d_status);
+      tiles_n, d_status, 0, 0, 0, 0);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// Tensor maps over two n x n BF16 mirrors of a matrix (Am row-major, Bm column-major, leading
+// dimension ldm elements): a product then names its operands by position, with no copies.
+bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a, void* map_b) {
+  if ((ldm % 8) || ((uintptr_t)Am & 15) || ((uintptr_t)Bm & 15)) return false;
+  return make_map(static_cast<CUtensorMap*>(map_a), Am, n, n, ldm, BM) &&
+         make_map(static_cast<CUtensorMap*>(map_b), Bm, n, n, ldm, BN);
+}
+
+// C (m x n) -= A B with A at (a_row, a_k) of map_a's matrix and B at (b_row = first column of B,
+// b_k = first row of B) of map_b's (column-major) matrix; a_k and b_k multiples of 8, k a multiple
+// of 64.
+cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
+                                  int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s) {
+  if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  if ((a_k % 8) || (b_k % 8) || (k % BK)) return cudaErrorInvalidValue;
+  const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
+      *static_cast<const CUtensorMap*>(map_a), *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m,
+      tiles_n, d_status, a_row, a_k, b_row, b_k);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -410,7 +436,7 @@ cudaError_t gemm_bf16_tc_minus(int m, int n, int k, const void* At, long lda_t, 
   }
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
   k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(ta, tb, m, n, k, C, ldc, tiles_m,
-                                                                              tiles_n, d_status);
+                                                                              tiles_n, d_status, 0, 0, 0, 0);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
