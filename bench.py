@@ -39,6 +39,8 @@ WORKLOADS = {
     # BASELINE configuration of the metric's target: star body at geodesic frequency 32 (N = 20,480)
     "star_f32": dict(desc="star-shaped body r=25A(1+sum_{l=2..8} a_lm Y_lm), a_lm~N(0,(0.08/l)^2) seed 1, "
                           "geodesic f=32", N=20480, iarea=0, gen=("star", 32)),
+    "star_f45": dict(desc="star-shaped body as star_f32, geodesic f=45 (the FP32 factor fits beside the FP64 GR)",
+                     N=40500, iarea=0, gen=("star", 45)),
     "ellipsoid_f16": dict(desc="ellipsoid 30/20/12 A, geodesic f=16, normal jitter U(+-2%) seed 0", N=5120,
                           iarea=1, gen=("ellipsoid", 16)),
     "icosphere_l3": dict(desc="icosphere level 3, R=20 A", N=1280, iarea=1, gen=("icosphere", 3)),

@@ -688,16 +688,26 @@ struct MixedSolver::Impl {
       prof.end(s);
       return;
     }
-    if (m > op_rows || n > op_rows || round_up(k, 64) > op_ld) throw std::runtime_error("GEMM larger than its operand buffers");
-    prof.begin("casts", 0, s);
-    ck(cast_transpose_bf16(at_(ar, ac), ld32, m, k, at.p, op_ld, s), "cast A");
-    ck(cast_bf16(at_(br, bc), ld32, k, n, bt.p, op_ld, s), "cast B");
-    prof.end(s);
-    prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
-    kt.begin(s);
-    ck(gemm_bf16_tc_minus_maps(m, n, k, map_a, map_b, C, ld32, d_status(), s), "tensor-core GEMM");
-    kt.end(s, 2.0 * m * n * k);
-    prof.end(s);
+    if (round_up(k, 64) > op_ld) throw std::runtime_error("GEMM deeper than its operand buffers");
+    // operand buffers of op_rows rows: products with more rows or columns go in blocks of that size
+    for (int m0 = 0; m0 < m; m0 += op_rows) {
+      const int mm = std::min(op_rows, m - m0);
+      prof.begin("casts", 0, s);
+      ck(cast_transpose_bf16(at_(ar + m0, ac), ld32, mm, k, at.p, op_ld, s), "cast A");
+      prof.end(s);
+      for (int n0 = 0; n0 < n; n0 += op_rows) {
+        const int nn = std::min(op_rows, n - n0);
+        prof.begin("casts", 0, s);
+        ck(cast_bf16(at_(br, bc + n0), ld32, k, nn, bt.p, op_ld, s), "cast B");
+        prof.end(s);
+        prof.begin(size_class(mm, nn, k), 2.0 * mm * nn * k, s);
+        kt.begin(s);
+        ck(gemm_bf16_tc_minus_maps(mm, nn, k, map_a, map_b, at_(cr + m0, cc + n0), ld32, d_status(), s),
+           "tensor-core GEMM");
+        kt.end(s, 2.0 * mm * nn * k);
+        prof.end(s);
+      }
+    }
   }
 
   static int split(int sz) {
@@ -866,15 +876,23 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       P.mirror_key[1] = P.bm.p;
     }
   } else {
+    // K of any product is at most about n/2; rows per buffer as many as fit beside everything else
+    // (3 GB kept for the solve's scratch and vectors), at most n/2
     const long half = P.n3 / 2 + 128;
     const long op_ld = round_up(half, 64);
-    P.at.ensure((size_t)half * op_ld * 2, "BF16 operand A");
-    P.bt.ensure((size_t)half * op_ld * 2, "BF16 operand B");
-    if (P.op_ld != op_ld || P.op_rows != (int)half || P.map_key[0] != P.at.p || P.map_key[1] != P.bt.p) {
-      if (!tc_operand_maps(P.at.p, (int)half, op_ld, P.bt.p, (int)half, op_ld, P.map_a, P.map_b))
+    const size_t held_ops = (P.at.p ? P.at.bytes : 0) + (P.bt.p ? P.bt.bytes : 0);
+    const size_t avail = free_b + held_ops > ((size_t)3 << 30) ? free_b + held_ops - ((size_t)3 << 30) : 0;
+    long rows = std::min<long>(half, (long)(avail / 2 / ((size_t)op_ld * 2)));
+    if (const char* e = std::getenv("BEST_GPU_OPERAND_ROWS")) rows = std::min<long>(rows, std::max(256L, atol(e)));
+    rows = rows >= half ? half : rows / 256 * 256;
+    if (rows < 256) throw std::runtime_error("no room on the GPU for the BF16 operand buffers");
+    P.at.ensure((size_t)rows * op_ld * 2, "BF16 operand A");
+    P.bt.ensure((size_t)rows * op_ld * 2, "BF16 operand B");
+    if (P.op_ld != op_ld || P.op_rows != (int)rows || P.map_key[0] != P.at.p || P.map_key[1] != P.bt.p) {
+      if (!tc_operand_maps(P.at.p, (int)rows, op_ld, P.bt.p, (int)rows, op_ld, P.map_a, P.map_b))
         throw std::runtime_error("cannot build the tensor maps of the BF16 operands");
       P.op_ld = op_ld;
-      P.op_rows = (int)half;
+      P.op_rows = (int)rows;
       P.map_key[0] = P.at.p;
       P.map_key[1] = P.bt.p;
     }

@@ -76,6 +76,26 @@ def test_mixed_solve_vs_oracle(case):
     compare(g, o)
 
 
+def test_mixed_operand_copies_in_blocks(monkeypatch):
+    """The path without BF16 mirrors (when the GPU has no room for them): operands copied per
+    product into buffers of capped rows, so the large products run in blocks."""
+    monkeypatch.setenv("BEST_GPU_NO_MIRRORS", "1")
+    monkeypatch.setenv("BEST_GPU_OPERAND_ROWS", "1024")
+    tri, ta, tv = meshes.ellipsoid(12)
+    bh.set_precision(bh.BGPU_MIXED)
+    try:
+        solver = BhmSolver()
+        g = run_gpu(solver, tri, ta, iarea=1, direct=0, eps=1e-10, ivisco=1, truevol=tv)
+        logs = bh.log_lines()
+        t = bh.timings()
+        solver.destroy()
+    finally:
+        bh.set_precision(-1)
+    assert not any("instead" in l for l in logs), logs
+    assert 0 < t["refine_iters"] <= 40 and t["relres"] <= 1e-12
+    compare(g, ob.best_run(tri, ta, tv, iarea=1, ivisco=1))
+
+
 def test_mixed_golden_2eu7():
     c = expected_cases()["2eu7"]
     tri, ta, tv = golden_mesh(c["mesh"])
