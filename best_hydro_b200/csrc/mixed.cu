@@ -75,24 +75,59 @@ long round_up(long v, long q) { return (v + q - 1) / q * q; }
 // ---- diagonal leaf: h x h (h <= 128) LU without pivoting and the inverses of both triangles ----
 // 512 threads = 16 warps x 32 lanes; warp w owns rows 8w .. 8w+7 and lane l columns 4l .. 4l+3 of
 // the 128 x 128 block, as an 8 x 4 register tile (rows and columns beyond h hold the identity, so
-// the padded part factors to itself).  Each of the 128 right-looking steps is one barrier: the
-// owners of column k and of row k publish them in a double-buffered shared row/column, and every
-// thread applies the rank-1 update to its tile.  The inverses then run the same way (L^-1 forward,
-// then U^-1 backward, 128 steps each) from the factors kept in shared memory; L^-1 (unit lower) and
-// U^-1 are written to DL, DU (128 x 128 column-major, zero outside the h x h block).
+// the padded part factors to itself).  The factorisation goes 4 columns per step (32 steps, one
+// barrier each): the thread holding the 4 x 4 diagonal block (warp K/2, lane K) factors it and its
+// warp forms the 4 rows of U to its right (the block's L comes by shuffles); after the barrier, the
+// lane K of every warp below forms its rows of the 4 columns of L, passes them to its warp by
+// shuffles, and every such thread applies the rank-4 update to its tile.  The inverses run the same
+// way, L^-1 forward and U^-1 backward in the same 32 steps, from the factors in shared memory.
+// L^-1 (unit lower) and U^-1 are written to DL, DU (128 x 128 column-major, zero outside h x h).
 constexpr int kLdS = 129;
+
+// rows q0 .. q0+3 of an 8 x 4 tile, as a 4 x 4 array (q0 = 0 or 4; selects keep it in registers)
+__device__ __forceinline__ void get4(const float (&a)[8][4], bool hi, float (&b)[4][4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[i][j] = hi ? a[4 + i][j] : a[i][j];
+}
+__device__ __forceinline__ void put4(float (&a)[8][4], bool hi, const float (&b)[4][4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      a[i][j] = hi ? a[i][j] : b[i][j];
+      a[4 + i][j] = hi ? b[i][j] : a[4 + i][j];
+    }
+}
+
 __global__ void __launch_bounds__(512, 1) k_lu32_leaf_inv(float* __restrict__ A, long lda, int h, float* __restrict__ DL,
                                                            float* __restrict__ DU, int* status) {
   extern __shared__ float sm[];
-  float* d = sm;                       // d[c * kLdS + r] = block entry (r, c)
-  float* rowb = sm + 128 * kLdS;       // [2][128]
-  float* colb = rowb + 2 * 128;        // [2][128]
+  float* d = sm;                     // d[c * kLdS + r] = block entry (r, c)
+  float* ub = sm + 128 * kLdS;       // [2][4][128]: the 4 rows of U of a step (then rows of X)
+  float* db = ub + 2 * 4 * 128;      // [2][20]: the factored 4 x 4 diagonal block, row-major, and
+                                     // the reciprocals of its 4 pivots
+  float* yb = db + 2 * 20;           // [2][4][128]: rows of U^-1 of an inverse step
+  float* rdiag = yb + 2 * 4 * 128;   // [128]: reciprocals of the pivots
   __shared__ int s_bad;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int r0 = 8 * warp, c0 = 4 * lane;
-  for (int c = warp; c < 128; c += 16)
-    for (int r = lane; r < 128; r += 32)
-      d[c * kLdS + r] = (r < h && c < h) ? A[(size_t)c * lda + r] : (r == c ? 1.f : 0.f);
+  if (h == 128) {
+    // full block: one float4 per lane per column, all 8 loads in flight
+    float4 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = *reinterpret_cast<const float4*>(A + (size_t)(warp + 16 * q) * lda + 4 * lane);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      float* dc = d + (warp + 16 * q) * kLdS + 4 * lane;
+      dc[0] = v[q].x, dc[1] = v[q].y, dc[2] = v[q].z, dc[3] = v[q].w;
+    }
+  } else {
+    for (int c = warp; c < 128; c += 16)
+      for (int r = lane; r < 128; r += 32)
+        d[c * kLdS + r] = (r < h && c < h) ? A[(size_t)c * lda + r] : (r == c ? 1.f : 0.f);
+  }
   if (tid == 0) s_bad = 0;
   __syncthreads();
   float a[8][4];
@@ -100,120 +135,233 @@ __global__ void __launch_bounds__(512, 1) k_lu32_leaf_inv(float* __restrict__ A,
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) a[i][j] = d[(c0 + j) * kLdS + r0 + i];
-  // LU without pivoting.  The multipliers (column k of L) go to shared memory as they are formed
-  // (lane 0 of each warp); a tile keeps only the entries still being updated, so warps whose rows
-  // are all above the pivot sit the step out, and columns left of the pivot are never masked (they
-  // are not read again).
 #pragma unroll 1
-  for (int k = 0; k < 128; ++k) {
-    const int par = k & 1;
-    float* rb = rowb + par * 128;
-    float* cb = colb + par * 128;
-    // (selects, not indexing: the register tiles must stay in registers)
-    if (lane == (k >> 2)) {
-      const int jk = k & 3;
+  for (int K = 0; K < 32; ++K) {
+    const int k = 4 * K, par = K & 1;
+    const bool hi = K & 1;  // the step's rows are rows 4..7 of the owning warp's tile
+    float* ubp = ub + par * 4 * 128;
+    float* dbp = db + par * 20;
+    if (warp == (K >> 1)) {
+      // the 4 x 4 diagonal block (lane K), factored, its L passed to the warp
+      float D[4][4];
+      get4(a, hi, D);
+      if (lane == K) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
-        cb[r0 + i] = jk == 0 ? a[i][0] : (jk == 1 ? a[i][1] : (jk == 2 ? a[i][2] : a[i][3]));
-    }
-    if (warp == (k >> 3)) {
-      const int ik = k & 7;
-      float4 v = make_float4(a[0][0], a[0][1], a[0][2], a[0][3]);
+        for (int t = 0; t < 4; ++t) {
+          const float p = D[t][t];
+          if (!(p != 0.f && isfinite(p))) s_bad = 1;
+          const float rp = 1.0f / p;
+          dbp[16 + t] = rp;
+          rdiag[k + t] = rp;
 #pragma unroll
-      for (int i = 1; i < 8; ++i)
-        if (i == ik) v = make_float4(a[i][0], a[i][1], a[i][2], a[i][3]);
-      *reinterpret_cast<float4*>(&rb[c0]) = v;
+          for (int r = t + 1; r < 4; ++r) {
+            D[r][t] *= rp;
+#pragma unroll
+            for (int c = t + 1; c < 4; ++c) D[r][c] -= D[r][t] * D[t][c];
+          }
+        }
+        put4(a, hi, D);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) dbp[e] = D[e >> 2][e & 3];
+      }
+      float l10 = __shfl_sync(0xffffffffu, D[1][0], K), l20 = __shfl_sync(0xffffffffu, D[2][0], K);
+      float l21 = __shfl_sync(0xffffffffu, D[2][1], K), l30 = __shfl_sync(0xffffffffu, D[3][0], K);
+      float l31 = __shfl_sync(0xffffffffu, D[3][1], K), l32 = __shfl_sync(0xffffffffu, D[3][2], K);
+      if (lane > K) {
+        // U rows k..k+3 in this lane's columns: U = L_D^-1 A
+        float U[4][4];
+        get4(a, hi, U);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          U[1][j] -= l10 * U[0][j];
+          U[2][j] -= l20 * U[0][j] + l21 * U[1][j];
+          U[3][j] -= l30 * U[0][j] + l31 * U[1][j] + l32 * U[2][j];
+        }
+        put4(a, hi, U);
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          *reinterpret_cast<float4*>(&ubp[t * 128 + c0]) = make_float4(U[t][0], U[t][1], U[t][2], U[t][3]);
+      }
     }
     __syncthreads();
-    if (tid == 0 && !(rb[k] != 0.f && isfinite(rb[k]))) s_bad = 1;
-    if (r0 + 7 > k) {
-      const float rp = 1.0f / rb[k];
-      float l[8];
+    if (r0 + 7 > k + 3) {
+      // rows below the block: lane K forms their 4 columns of L (only rows > k + 3), then the
+      // rank-4 update of every column right of the block
+      float l[8][4];
+      if (lane == K) {
+        float Ud[4][4], rp[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) l[i] = (r0 + i > k) ? cb[r0 + i] * rp : 0.f;
-      if (lane == 0) {
+        for (int e = 0; e < 16; ++e) Ud[e >> 2][e & 3] = dbp[e];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) rp[t] = dbp[16 + t];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const bool below = r0 + i > k + 3;
+          float x0 = a[i][0], x1 = a[i][1], x2 = a[i][2], x3 = a[i][3];
+          x0 = x0 * rp[0];
+          x1 = (x1 - x0 * Ud[0][1]) * rp[1];
+          x2 = (x2 - x0 * Ud[0][2] - x1 * Ud[1][2]) * rp[2];
+          x3 = (x3 - x0 * Ud[0][3] - x1 * Ud[1][3] - x2 * Ud[2][3]) * rp[3];
+          a[i][0] = below ? x0 : a[i][0];
+          a[i][1] = below ? x1 : a[i][1];
+          a[i][2] = below ? x2 : a[i][2];
+          a[i][3] = below ? x3 : a[i][3];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const float v = __shfl_sync(0xffffffffu, a[i][t], K);
+          l[i][t] = (r0 + i > k + 3) ? v : 0.f;
+        }
+      if (lane > K) {
+        float4 u[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) u[t] = *reinterpret_cast<const float4*>(&ubp[t * 128 + c0]);
 #pragma unroll
         for (int i = 0; i < 8; ++i)
-          if (r0 + i > k) d[k * kLdS + r0 + i] = l[i];
-      }
-      const float4 u = *reinterpret_cast<const float4*>(&rb[c0]);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        a[i][0] -= l[i] * u.x;
-        a[i][1] -= l[i] * u.y;
-        a[i][2] -= l[i] * u.z;
-        a[i][3] -= l[i] * u.w;
+          for (int t = 0; t < 4; ++t) {
+            a[i][0] -= l[i][t] * u[t].x;
+            a[i][1] -= l[i][t] * u[t].y;
+            a[i][2] -= l[i][t] * u[t].z;
+            a[i][3] -= l[i][t] * u[t].w;
+          }
       }
     }
   }
   __syncthreads();
-  // the U part from the tiles (the L part is already in shared memory)
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if (r0 + i <= c0 + j) d[(c0 + j) * kLdS + r0 + i] = a[i][j];
+    for (int j = 0; j < 4; ++j) d[(c0 + j) * kLdS + r0 + i] = a[i][j];
   __syncthreads();
-  for (int c = warp; c < h; c += 16)
-    for (int r = lane; r < h; r += 32) A[(size_t)c * lda + r] = d[c * kLdS + r];
-  // inverses from the factors in shared memory: X = L^-1 forward (steps k = 0..127), then
-  // X = U^-1 backward (k = 127..0), each one barrier per step
+  if (h == 128) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float* dc = d + (warp + 16 * q) * kLdS + 4 * lane;
+      *reinterpret_cast<float4*>(A + (size_t)(warp + 16 * q) * lda + 4 * lane) = make_float4(dc[0], dc[1], dc[2], dc[3]);
+    }
+  } else {
+    for (int c = warp; c < h; c += 16)
+      for (int r = lane; r < h; r += 32) A[(size_t)c * lda + r] = d[c * kLdS + r];
+  }
+  // inverses, 4 rows per step: X = L^-1 forward (step s: rows 4s..4s+3), Y = U^-1 backward
+  // (rows 4(31-s)..+3); the owning warp finishes its 4 rows by substitution within the 4 x 4
+  // diagonal block, publishes them, and the warps of the other rows apply the rank-4 update
+  float x[8][4], y[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[i][j] = y[i][j] = (r0 + i == c0 + j) ? 1.f : 0.f;
 #pragma unroll 1
-  for (int pass = 0; pass < 2; ++pass) {
-    const bool lower = pass == 0;
-    float x[8][4];
+  for (int st = 0; st < 32; ++st) {
+    const int KL = st, KU = 31 - st, kl = 4 * KL, ku = 4 * KU, par = st & 1;
+    float* xb = ub + par * 4 * 128;
+    float* ybp = yb + par * 4 * 128;
+    if (warp == (KL >> 1)) {
+      const bool hi = KL & 1;
+      float X[4][4];
+      get4(x, hi, X);
+      const float l10 = d[kl * kLdS + kl + 1], l20 = d[kl * kLdS + kl + 2], l30 = d[kl * kLdS + kl + 3];
+      const float l21 = d[(kl + 1) * kLdS + kl + 2], l31 = d[(kl + 1) * kLdS + kl + 3];
+      const float l32 = d[(kl + 2) * kLdS + kl + 3];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) x[i][j] = (r0 + i == c0 + j) ? 1.f : 0.f;
-#pragma unroll 1
-    for (int st = 0; st < 128; ++st) {
-      const int k = lower ? st : 127 - st;
-      float* xb = (st & 1) ? colb : rowb;
-      if (warp == (k >> 3)) {
-        const float rd = lower ? 1.f : 1.0f / d[k * kLdS + k];
-        const int ik = k & 7;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const float sc = i == ik ? rd : 1.f;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) x[i][j] *= sc;
-          if (i == ik) v = make_float4(x[i][0], x[i][1], x[i][2], x[i][3]);
-        }
-        *reinterpret_cast<float4*>(&xb[c0]) = v;
+      for (int j = 0; j < 4; ++j) {
+        X[1][j] -= l10 * X[0][j];
+        X[2][j] -= l20 * X[0][j] + l21 * X[1][j];
+        X[3][j] -= l30 * X[0][j] + l31 * X[1][j] + l32 * X[2][j];
       }
-      __syncthreads();
-      if (lower ? r0 + 7 > k : r0 < k) {
-        const float4 xr = *reinterpret_cast<const float4*>(&xb[c0]);
+      put4(x, hi, X);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int r = r0 + i;
-          const float cf = (lower ? r > k : r < k) ? d[k * kLdS + r] : 0.f;
-          x[i][0] -= cf * xr.x;
-          x[i][1] -= cf * xr.y;
-          x[i][2] -= cf * xr.z;
-          x[i][3] -= cf * xr.w;
+      for (int t = 0; t < 4; ++t)
+        *reinterpret_cast<float4*>(&xb[t * 128 + c0]) = make_float4(X[t][0], X[t][1], X[t][2], X[t][3]);
+    }
+    if (warp == (KU >> 1)) {
+      const bool hi = KU & 1;
+      float Y[4][4];
+      get4(y, hi, Y);
+      float U[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) U[r][c] = d[(ku + c) * kLdS + ku + r];
+      const float q0 = rdiag[ku], q1 = rdiag[ku + 1], q2 = rdiag[ku + 2], q3 = rdiag[ku + 3];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        Y[3][j] = Y[3][j] * q3;
+        Y[2][j] = (Y[2][j] - U[2][3] * Y[3][j]) * q2;
+        Y[1][j] = (Y[1][j] - U[1][2] * Y[2][j] - U[1][3] * Y[3][j]) * q1;
+        Y[0][j] = (Y[0][j] - U[0][1] * Y[1][j] - U[0][2] * Y[2][j] - U[0][3] * Y[3][j]) * q0;
+      }
+      put4(y, hi, Y);
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        *reinterpret_cast<float4*>(&ybp[t * 128 + c0]) = make_float4(Y[t][0], Y[t][1], Y[t][2], Y[t][3]);
+    }
+    __syncthreads();
+    if (r0 + 7 > kl + 3) {
+      float4 xr[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) xr[t] = *reinterpret_cast<const float4*>(&xb[t * 128 + c0]);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int r = r0 + i;
+        if (r > kl + 3) {
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const float lc = d[(kl + t) * kLdS + r];
+            x[i][0] -= lc * xr[t].x;
+            x[i][1] -= lc * xr[t].y;
+            x[i][2] -= lc * xr[t].z;
+            x[i][3] -= lc * xr[t].w;
+          }
         }
       }
     }
-    float* D = lower ? DL : DU;
+    if (r0 < ku) {
+      float4 yr[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+      for (int t = 0; t < 4; ++t) yr[t] = *reinterpret_cast<const float4*>(&ybp[t * 128 + c0]);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) D[(size_t)(c0 + j) * 128 + r0 + i] = (r0 + i < h && c0 + j < h) ? x[i][j] : 0.f;
+      for (int i = 0; i < 8; ++i) {
+        const int r = r0 + i;
+        if (r < ku) {
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const float uc = d[(ku + t) * kLdS + r];
+            y[i][0] -= uc * yr[t].x;
+            y[i][1] -= uc * yr[t].y;
+            y[i][2] -= uc * yr[t].z;
+            y[i][3] -= uc * yr[t].w;
+          }
+        }
+      }
+    }
+  }
+  // L^-1 and U^-1 through shared memory, so each column goes out as 32 float4 stores
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
     __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool in = r0 + i < h && c0 + j < h;
+        d[(c0 + j) * kLdS + r0 + i] = in ? (pass ? y[i][j] : x[i][j]) : 0.f;
+      }
+    __syncthreads();
+    float* D = pass ? DU : DL;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float* dc = d + (warp + 16 * q) * kLdS + 4 * lane;
+      *reinterpret_cast<float4*>(D + (size_t)(warp + 16 * q) * 128 + 4 * lane) = make_float4(dc[0], dc[1], dc[2], dc[3]);
+    }
   }
   if (tid == 0 && s_bad) atomicExch(status, kZeroPivot);
 }
 
-// ---- triangular-solve leaves (h <= 128): products with the inverted diagonal block ----------
-// LEFT:  B (h x w, ldb) := Dinv B;  otherwise B (m x h, ldb) := B Dinv.  Dinv is an inverted
-// diagonal block (128 x 128, ld 128, zero outside h).  One CTA per 128 columns (LEFT) or rows of B:
-// both 128 x 128 operands go to shared memory (k-major), then 256 threads each accumulate an 8 x 8
-// tile over the 128-long inner dimension in FP32, and write it back in place (each CTA owns its
-// tile).  With mir != nullptr the results are also written, rounded to BF16, to the matrix's BF16
-// mirror at the same place: column-major for LEFT (the U part), row-major otherwise (the L part).
 // 16-byte asynchronous copy global -> shared; fewer than 16 source bytes are zero-filled
 __device__ __forceinline__ void cp16(void* sdst, const void* gsrc, int src_bytes) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
@@ -661,6 +809,12 @@ struct MixedSolver::Impl {
   double tol = 1e-12;
   int max_restarts = 8, krylov = 10;
   int sms = 148;
+  // second stream and fork/join events: the two triangular-solve chains of each recursion step
+  // (U12 and L21) write disjoint blocks and run side by side; not with operand copies, whose
+  // buffers the products of both chains would share
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool fork = false;
   Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs, dl32, du32;
   // BF16 mirrors of the factors (L part row-major, U part column-major), written by the triangular
   // solve leaves as the entries become final; the GEMMs read their operands there by position, so no
@@ -769,7 +923,7 @@ struct MixedSolver::Impl {
   // inverted (both triangles) right after it is factored, for the triangular-solve leaves above it
   void rlu(int k0, int sz, cudaStream_t s) {
     if (sz <= kLeaf) {
-      const size_t smem = (size_t)(128 * kLdS + 4 * 128) * sizeof(float);
+      const size_t smem = (size_t)(128 * kLdS + 2 * 4 * 128 + 2 * 20 + 2 * 4 * 128 + 128) * sizeof(float);
       const size_t off = (size_t)(k0 / kLeaf) * kLeaf * kLeaf;
       prof.begin("LU leaf + inverses", 0, s);
       k_lu32_leaf_inv<<<1, 512, smem, s>>>(at_(k0, k0), ld32, sz, dl32.as<float>() + off, du32.as<float>() + off,
@@ -781,8 +935,17 @@ struct MixedSolver::Impl {
     }
     const int h = split(sz), r = sz - h;
     rlu(k0, h, s);
-    trsm_llu(k0, h, k0 + h, r, s);   // U12
-    trsm_ru(k0, h, k0 + h, r, s);    // L21
+    if (fork) {
+      ck(cudaEventRecord(ev_fork, s), "fork");
+      ck(cudaStreamWaitEvent(side, ev_fork, 0), "fork");
+      trsm_llu(k0, h, k0 + h, r, s);     // U12
+      trsm_ru(k0, h, k0 + h, r, side);   // L21
+      ck(cudaEventRecord(ev_join, side), "join");
+      ck(cudaStreamWaitEvent(s, ev_join, 0), "join");
+    } else {
+      trsm_llu(k0, h, k0 + h, r, s);   // U12
+      trsm_ru(k0, h, k0 + h, r, s);    // L21
+    }
     gemm(r, r, h, k0 + h, k0, k0, k0 + h, k0 + h, k0 + h, s);
     rlu(k0 + h, r, s);
   }
@@ -835,6 +998,9 @@ MixedSolver::MixedSolver() : p_(new Impl) {
 }
 MixedSolver::~MixedSolver() {
   if (p_->graph) cudaGraphExecDestroy(p_->graph);
+  if (p_->side) cudaStreamDestroy(p_->side);
+  if (p_->ev_fork) cudaEventDestroy(p_->ev_fork);
+  if (p_->ev_join) cudaEventDestroy(p_->ev_join);
   delete p_;
 }
 void MixedSolver::set_refinement(int max_restarts, int krylov) {
@@ -911,8 +1077,14 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
   ck(launch_assemble(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
   ck(cudaEventRecord(ev_assembled, s), "event");
+  if (!P.side) {
+    ck(cudaStreamCreateWithFlags(&P.side, cudaStreamNonBlocking), "side stream");
+    ck(cudaEventCreateWithFlags(&P.ev_fork, cudaEventDisableTiming), "fork event");
+    ck(cudaEventCreateWithFlags(&P.ev_join, cudaEventDisableTiming), "join event");
+  }
   if (P.prof.on || kernel_timer(1).on) {
-    P.rlu(0, P.n3, s);  // direct launches, each timed
+    P.fork = false;
+    P.rlu(0, P.n3, s);  // direct launches in order, each timed
   } else {
     // the recursion's launches depend only on the order and the buffers: capture them once as a
     // CUDA graph and replay it
@@ -925,6 +1097,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       cudaGraph_t g = nullptr;
       const unsigned long long launches0 = g_launches;  // captured launches do not run now
       ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+      P.fork = P.mirrors && std::getenv("BEST_GPU_ONE_STREAM") == nullptr;
       try {
         P.rlu(0, P.n3, cs);
       } catch (...) {
