@@ -145,7 +145,8 @@ cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const doub
 // dgetrs('T'): X := A^-T X with the same factors (the adjoint solve).
 cudaError_t getrs64_trans_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
                               double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s);
-cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, double* Y, long ldy,
+// Y := U^-1 L^-1 Y, FP32 factors, right-hand sides and sums (the mixed path's preconditioner)
+cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, float* Y, long ldy,
                           int nrhs, void* scratch, int* d_status, cudaStream_t s);
 // Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s);

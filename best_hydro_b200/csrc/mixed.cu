@@ -721,6 +721,16 @@ __global__ void k_scale_cols(const double* __restrict__ X, const double* __restr
     for (int c = 0; c < q; ++c) Y[(size_t)c * n + r] = X[(size_t)c * n + r] * scale[c];
 }
 
+// the preconditioner's FP32 copy of n x q FP64 vectors (ld n both), and back
+__global__ void k_to_f32(const double* __restrict__ X, size_t len, float* __restrict__ Y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < len; i += (size_t)gridDim.x * blockDim.x)
+    Y[i] = (float)X[i];
+}
+__global__ void k_to_f64(const float* __restrict__ X, size_t len, double* __restrict__ Y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < len; i += (size_t)gridDim.x * blockDim.x)
+    Y[i] = (double)X[i];
+}
+
 __global__ void k_copy_in(const double* __restrict__ B, long ldb, int n, int q, double* Y) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
     for (int c = 0; c < q; ++c) Y[(size_t)c * n + r] = B[(size_t)c * ldb + r];
@@ -815,7 +825,7 @@ struct MixedSolver::Impl {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool fork = false;
-  Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs, dl32, du32;
+  Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs, dl32, du32, zf;
   // BF16 mirrors of the factors (L part row-major, U part column-major), written by the triangular
   // solve leaves as the entries become final; the GEMMs read their operands there by position, so no
   // operand copies are made.  Used when the GPU has room for them (4 n^2 bytes), else copies.
@@ -1145,6 +1155,7 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
     const size_t blk = (size_t)n * q;
     // [B | X | R | W | V_0..V_m | Z_0..Z_{m-1}]
     P.vecs.ensure(blk * (4 + (m + 1) + m) * sizeof(double), "GMRES vectors");
+    P.zf.ensure(blk * sizeof(float), "preconditioner vectors (FP32)");
     double* B = P.vecs.as<double>();
     double* X = B + blk;
     double* R = X + blk;
@@ -1190,11 +1201,14 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
       for (int j = 0; j < m; ++j) {
         double* Vj = V + (size_t)j * blk;
         double* Zj = Z + (size_t)j * blk;
-        ck(cudaMemcpyAsync(Zj, Vj, blk * sizeof(double), cudaMemcpyDeviceToDevice, s), "z copy");
         P.prof.begin("preconditioner solve", 0, s);
-        ck(trsv_lu32_inv(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), n, Zj, n, q, P.trsv.p,
-                         P.d_status(), s),
+        k_to_f32<<<grid, 256, 0, s>>>(Vj, blk, P.zf.as<float>());
+        BGPU_COUNT_LAUNCH();
+        ck(trsv_lu32_inv(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), n, P.zf.as<float>(), n,
+                         q, P.trsv.p, P.d_status(), s),
            "preconditioner");
+        k_to_f64<<<grid, 256, 0, s>>>(P.zf.as<float>(), blk, Zj);
+        BGPU_COUNT_LAUNCH();
         P.prof.end(s);
         P.prof.begin("FP64 mat-vec", 2.0 * n * (double)n * q, s);
         P.matvec(Zj, n, q, W, n, 1.0, 0.0, s);

@@ -411,15 +411,16 @@ __global__ void __launch_bounds__(kIb) k_diag_inverses(const F* __restrict__ LU,
 constexpr int kChunk = 16;
 constexpr int kLead = 2;
 
-template <typename F, typename FI, bool LOWER, bool TRANS = false>
+// V is the type of the right-hand sides and of every sum (double; float for the FP32 preconditioner).
+template <typename F, typename FI, bool LOWER, bool TRANS = false, typename V = double>
 __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
-                                                  double* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
+                                                  V* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
                                                   unsigned epoch, int* status, unsigned* __restrict__ cnt,
-                                                  double* __restrict__ part, int smax, const int4* __restrict__ tasks,
+                                                  V* __restrict__ part, int smax, const int4* __restrict__ tasks,
                                                   int ntasks) {
-  __shared__ double s_y[kIb][kIrhs];
-  __shared__ double s_b[kIb][kIrhs];
-  __shared__ double s_acc[2][kIb][kIrhs];
+  __shared__ V s_y[kIb][kIrhs];
+  __shared__ V s_b[kIb][kIrhs];
+  __shared__ V s_acc[2][kIb][kIrhs];
   __shared__ int s_task[4], s_cnt;
   extern __shared__ __align__(16) unsigned char s_dyn[];
   FI* s_di = reinterpret_cast<FI*>(s_dyn);  // the inverted diagonal block, stride kIb + 1
@@ -443,9 +444,9 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     const int blk = LOWER ? i : nblk - 1 - i;
     const int r0 = blk * kIb, nr = min(kIb, n - r0);
     const bool live = row < nr;
-    double acc[kIrhs];
+    V acc[kIrhs];
 #pragma unroll
-    for (int r = 0; r < kIrhs; ++r) acc[r] = 0.0;
+    for (int r = 0; r < kIrhs; ++r) acc[r] = (V)0;
     if (fin) {
       // before any wait: the inverted diagonal block into shared memory (asynchronous copies), the
       // block's right-hand sides, and the partial sums of the earlier chunks
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
       for (int e = tid; e < kIb * kIb; e += 256) cp_async_elem<sizeof(FI)>(s_di + (e >> 7) * (kIb + 1) + (e & 127), dblk + e);
       for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
         const int rr = idx / kIrhs, r = idx % kIrhs;
-        s_b[rr][r] = (rr < nr && r < nrhs) ? Y[(size_t)r * ldy + r0 + rr] : 0.0;
+        s_b[rr][r] = (rr < nr && r < nrhs) ? Y[(size_t)r * ldy + r0 + rr] : (V)0;
       }
       const int nparts = -1 - code;
       if (tid == 0) {
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
         return;
       }
       if (half == 0) {
-        const double* p = part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs;
+        const V* p = part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs;
         for (int sp = 0; sp < nparts; ++sp)
 #pragma unroll
           for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + (size_t)sp * kIb * kIrhs + r);
@@ -507,12 +508,12 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
       }
       for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
         const int rr = idx / kIrhs, r = idx % kIrhs;
-        s_y[rr][r] = (rr < nc && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + c0 + rr]) : 0.0;
+        s_y[rr][r] = (rr < nc && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + c0 + rr]) : (V)0;
       }
       __syncthreads();
 #pragma unroll
       for (int kk = 0; kk < 64; ++kk) {
-        const double l = (double)lv[kk];
+        const V l = (V)lv[kk];
 #pragma unroll
         for (int r = 0; r < kIrhs; ++r) acc[r] -= l * s_y[half * 64 + kk][r];
       }
@@ -522,7 +523,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
     __syncthreads();
     if (!fin) {
-      double* slot = part + ((size_t)i * smax + sidx) * kIb * kIrhs;
+      V* slot = part + ((size_t)i * smax + sidx) * kIb * kIrhs;
       for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
         const int rr = idx / kIrhs, r = idx % kIrhs;
         slot[idx] = s_acc[0][rr][r] + s_acc[1][rr][r];
@@ -544,11 +545,11 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     // each half does 64 of the 128 products; D^-1 (row, c) at s_di[c * 129 + row] (transposed:
     // the other way round)
 #pragma unroll
-    for (int r = 0; r < kIrhs; ++r) acc[r] = 0.0;
+    for (int r = 0; r < kIrhs; ++r) acc[r] = (V)0;
 #pragma unroll 8
     for (int kk = 0; kk < 64; ++kk) {
       const int cc = half * 64 + kk;
-      const double dv = TRANS ? (double)s_di[row * (kIb + 1) + cc] : (double)s_di[cc * (kIb + 1) + row];
+      const V dv = TRANS ? (V)s_di[row * (kIb + 1) + cc] : (V)s_di[cc * (kIb + 1) + row];
 #pragma unroll
       for (int r = 0; r < kIrhs; ++r) acc[r] += dv * s_y[cc][r];
     }
@@ -606,14 +607,14 @@ const std::vector<int4>& split_tasks(int nblk) {
 }
 
 // one triangle: ticket, counters and task list set, then the persistent launch (one CTA per SM)
-template <typename F, typename FI, bool LOWER, bool TRANS>
-cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, double* Yc, long ldy, int q, void* scratch,
+template <typename F, typename FI, bool LOWER, bool TRANS, typename V = double>
+cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, V* Yc, long ldy, int q, void* scratch,
                      unsigned epoch, int* d_status, cudaStream_t s) {
   unsigned char* base = static_cast<unsigned char*>(scratch);
   unsigned* ticket = reinterpret_cast<unsigned*>(base);
   unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
   unsigned* cnt = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
-  double* part = reinterpret_cast<double*>(base + SplitScratch::part_off(n));
+  V* part = reinterpret_cast<V*>(base + SplitScratch::part_off(n));
   int4* tasks = reinterpret_cast<int4*>(base + SplitScratch::task_off(n));
   const std::vector<int4>& list = split_tasks(SplitScratch::nblk(n));
   if (list.size() > SplitScratch::max_tasks(n)) return cudaErrorInvalidValue;
@@ -628,28 +629,28 @@ cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, double* Yc, lon
   const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(FI);
   static bool attr = false;
   if (!attr) {
-    if ((e = cudaFuncSetAttribute(k_trsv_inv<F, FI, LOWER, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = cudaFuncSetAttribute(k_trsv_inv<F, FI, LOWER, TRANS, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)dsmem)) != cudaSuccess)
       return e;
     attr = true;
   }
-  k_trsv_inv<F, FI, LOWER, TRANS><<<sms, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
+  k_trsv_inv<F, FI, LOWER, TRANS, V><<<sms, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
                                                           cnt, part, SplitScratch::smax(n), tasks, (int)list.size());
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
-template <typename F, typename FI>
-cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int n, double* Y, long ldy, int nrhs,
+template <typename F, typename FI, typename V = double>
+cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int n, V* Y, long ldy, int nrhs,
                           void* scratch, int* d_status, cudaStream_t s) {
   for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
     const int q = std::min(kIrhs, nrhs - c0);
-    double* Yc = Y + (size_t)c0 * ldy;
+    V* Yc = Y + (size_t)c0 * ldy;
     g_epoch += 2;
     if (g_epoch == 0) g_epoch = 2;
-    cudaError_t e = trsv_one<F, FI, true, false>(LU, lda, DL, n, Yc, ldy, q, scratch, g_epoch, d_status, s);
+    cudaError_t e = trsv_one<F, FI, true, false, V>(LU, lda, DL, n, Yc, ldy, q, scratch, g_epoch, d_status, s);
     if (e != cudaSuccess) return e;
-    if ((e = trsv_one<F, FI, false, false>(LU, lda, DU, n, Yc, ldy, q, scratch, g_epoch + 1, d_status, s)) !=
+    if ((e = trsv_one<F, FI, false, false, V>(LU, lda, DU, n, Yc, ldy, q, scratch, g_epoch + 1, d_status, s)) !=
         cudaSuccess)
       return e;
   }
@@ -754,11 +755,13 @@ cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const doub
   return cudaGetLastError();
 }
 
-// Y := U^-1 L^-1 Y with FP32 factors of an unpivoted LU and their FP32 diagonal-block inverses.
-cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, double* Y, long ldy,
+// Y := U^-1 L^-1 Y with FP32 factors of an unpivoted LU and their FP32 diagonal-block inverses,
+// FP32 right-hand sides and sums (the preconditioner of the refined solve, whose result only
+// steers the iteration: the FP64 products and residuals fix the accuracy)
+cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, float* Y, long ldy,
                           int nrhs, void* scratch, int* d_status, cudaStream_t s) {
   if (n <= 0 || nrhs <= 0) return cudaSuccess;
-  return trsv_inv_pair<float, float>(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
+  return trsv_inv_pair<float, float, float>(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
 }
 
 // Y := U^-1 L^-1 Y in place with FP32 factors of an unpivoted LU (the mixed-precision
