@@ -634,7 +634,17 @@ cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, V* Yc, long ldy
       return e;
     attr = true;
   }
-  k_trsv_inv<F, FI, LOWER, TRANS, V><<<sms, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
+  // as many CTAs as fit (tasks are taken in ticket order and wait only on earlier tickets, so any
+  // grid size completes)
+  static int per_sm = 0;
+  if (!per_sm) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trsv_inv<F, FI, LOWER, TRANS, V>, 256, dsmem) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    per_sm = std::min(per_sm, 2);
+  }
+  k_trsv_inv<F, FI, LOWER, TRANS, V><<<sms * per_sm, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
                                                           cnt, part, SplitScratch::smax(n), tasks, (int)list.size());
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
