@@ -346,19 +346,28 @@ def run_ours(args, rank, world, local_rank):
     h2d = 8 * (12 * n + 3 * n + len(gdef)) + (4 * n if st.ndef > 1 else 0) + 8 * 6 * n3
     d2h = 8 * (4 * n + 1 + 6 * n3)
     B_host = bh.rhs6(x)
+    phases = []
     for _ in range(0 if args.no_e2e else max(1, args.steps)):
         solver.destroy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         solver.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        t1 = time.perf_counter()
         xe = solver.incenters()
         dme = solver.diag_mean()
         xmu_e, gdef_e = st.deflation(dme)
+        t2 = time.perf_counter()
         solver.build(eps=1e-10, direct=1 if head == "fp64" else 0, ndef=st.ndef, gdef=gdef_e, comp=st.icomp,
                      xmu=xmu_e)
+        t3 = time.perf_counter()
         solver.solve(B_host)
-        e2e.append(time.perf_counter() - t0)
+        t4 = time.perf_counter()
+        e2e.append(t4 - t0)
+        phases.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
     e2e_s = max_over_ranks(float(np.median(e2e))) if e2e else float("nan")
+    e2e_phases = ({k: round(1e3 * float(np.median([p[i] for p in phases])), 2)
+                   for i, k in enumerate(("create", "incenters_deflation", "build", "solve"))} if phases else None)
+    host_notes = [ln for ln in bh.log_lines() if "host side" in ln][-2:]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -400,7 +409,8 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": args.workload, "N": n, "order": n3, "desc": w["desc"], "precision": head,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB write) between timed steps; GR is 72 N^2 bytes, far above L2",
-                       "stages_ms": H["stages_ms"]},
+                       "stages_ms": H["stages_ms"], "e2e_phases_ms": e2e_phases,
+                       "e2e_host_notes": host_notes},
             "roofline": roof,
             "clocks": H["clocks"],
             "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

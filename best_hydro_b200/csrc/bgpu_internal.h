@@ -60,6 +60,15 @@ struct KernelTimer {
   void enable(bool v);
   // launches recorded, their summed device time (ms) and work, then reset (synchronises)
   void read(int* launches, double* ms, double* w);
+  // launches timed by other means (device stamps inside a graph), added to the next read
+  int extra_launches = 0;
+  double extra_ms = 0;
+  void add(int launches, double ms, double w) {
+    if (!on) return;
+    extra_launches += launches;
+    extra_ms += ms;
+    work += w;
+  }
 };
 constexpr int kTimedKernels = 2;
 KernelTimer& kernel_timer(int id);
@@ -176,13 +185,17 @@ constexpr int kTensorMapBytes = 128;
 cudaError_t tc_gemm_prepare();  // kernel attributes, once, before any capture
 bool tc_operand_maps(const void* At, int rows_a, long lda_t, const void* Bt, int rows_b, long ldb_t, void* map_a,
                      void* map_b);
+// stamp (optional, here and below): 2 words per launch, set to [~0, 0] by stamps_reset; the kernel
+// leaves its first start and last end (global timer, ns) there
 cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, const void* map_b, float* C, long ldc,
-                                    int* d_status, cudaStream_t s);
+                                    int* d_status, cudaStream_t s, unsigned long long* stamp = nullptr);
+cudaError_t stamps_reset(unsigned long long* stamps, int slots, cudaStream_t s);
 // Maps over whole-matrix BF16 mirrors (Am row-major, Bm column-major, n x n, ld ldm) and the GEMM on
 // blocks of them named by position (A at rows a_row.., columns a_k..; B at columns b_row..,
 // rows b_k..).
 bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a, void* map_b);
 cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
-                                  int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s);
+                                  int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s,
+                                  unsigned long long* stamp = nullptr);
 
 }  // namespace bgpu

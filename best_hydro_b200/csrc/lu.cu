@@ -900,6 +900,8 @@ void KernelTimer::enable(bool v) {
   on = v;
   used = 0;
   work = 0;
+  extra_launches = 0;
+  extra_ms = 0;
 }
 
 void KernelTimer::read(int* launches, double* ms, double* w) {
@@ -910,11 +912,13 @@ void KernelTimer::read(int* launches, double* ms, double* w) {
     cudaEventElapsedTime(&x, ev[i].first, ev[i].second);
     t += x;
   }
-  *launches = (int)used;
-  *ms = t;
+  *launches = (int)used + extra_launches;
+  *ms = t + extra_ms;
   *w = work;
   used = 0;
   work = 0;
+  extra_launches = 0;
+  extra_ms = 0;
 }
 
 KernelTimer& kernel_timer(int id) {

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -482,62 +483,87 @@ __global__ void __launch_bounds__(256, 1) k_leaf_mult(const float* __restrict__ 
   }
 }
 
-// B (h x w, ldb) := Dinv B, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h);
-// one CTA per 64 columns, 256 threads each computing 4 rows x 8 columns, FP32.
-constexpr int kLdI = 132, kLdB = 68;
-// (the narrow leaves: 64 columns per CTA; mirror writes as k_leaf_mult's)
+// The narrow leaves (fewer than kWideLeaf columns or rows), FP32, 256 threads, NB = 64, 32 or 16
+// columns (rows) of B per CTA, each thread 4 rows x NB/8 columns of the result; the narrower
+// the leaf, the fewer per CTA, so that the grid still covers every SM.  Mirror writes as
+// k_leaf_mult's.
+constexpr int kLdI = 132;
+template <int NB>
+struct NarrowLeaf {
+  static constexpr int kCpt = NB / 8;    // result columns per thread
+  static constexpr int kLdB = NB + 4;    // row stride of the staged B block (floats)
+  static constexpr size_t smem() { return (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float); }
+};
+
+// kCpt consecutive floats of shared memory (kCpt = 8, 4 or 2; 8-byte aligned at least)
+template <int C>
+__device__ __forceinline__ void lds_n(const float* p, float (&v)[C]) {
+  if constexpr (C == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    v[0] = t.x, v[1] = t.y;
+  } else {
+#pragma unroll
+    for (int q = 0; q < C / 4; ++q) {
+      const float4 t = *reinterpret_cast<const float4*>(p + 4 * q);
+      v[4 * q] = t.x, v[4 * q + 1] = t.y, v[4 * q + 2] = t.z, v[4 * q + 3] = t.w;
+    }
+  }
+}
+
+// B (h x w, ldb) := Dinv B, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h)
+template <int NB>
 __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict__ Dinv, int h, float* B, long ldb,
                                                          int w, __nv_bfloat16* __restrict__ mir, long ldm) {
+  using L = NarrowLeaf<NB>;
+  constexpr int C = L::kCpt, ldb_s = L::kLdB;
   extern __shared__ __align__(16) float sm[];
   float* li = sm;                 // li[k * kLdI + r] = Dinv(r, k)
-  float* bs = sm + 128 * kLdI;    // bs[k * kLdB + c] = B(k, c0 + c)
+  float* bs = sm + 128 * kLdI;    // bs[k * ldb_s + c] = B(k, c0 + c)
   const int tid = threadIdx.x;
-  const int c0 = blockIdx.x * 64, nc = min(64, w - c0);
+  const int c0 = blockIdx.x * NB, nc = min(NB, w - c0);
 #pragma unroll
   for (int q = 0; q < 16; ++q) {  // Dinv column k -> li row k (16-byte asynchronous copies)
     const int e = tid + 256 * q, k = e >> 5, r4 = (e & 31) * 4;
     cp16(&li[k * kLdI + r4], &Dinv[(size_t)k * 128 + r4], 16);
   }
   {
-    float4 v[8];  // B (k, c0 + cc), k contiguous in memory: float4 loads, transposed into bs
+    float4 v[NB / 8];  // B (k, c0 + cc), k contiguous in memory: float4 loads, transposed into bs
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < NB / 8; ++q) {
       const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
       v[q] = (cc < nc && k4 < h) ? *reinterpret_cast<const float4*>(&B[(size_t)(c0 + cc) * ldb + k4])
                                  : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < NB / 8; ++q) {
       const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
-      bs[(k4 + 0) * kLdB + cc] = k4 + 0 < h ? v[q].x : 0.f;
-      bs[(k4 + 1) * kLdB + cc] = k4 + 1 < h ? v[q].y : 0.f;
-      bs[(k4 + 2) * kLdB + cc] = k4 + 2 < h ? v[q].z : 0.f;
-      bs[(k4 + 3) * kLdB + cc] = k4 + 3 < h ? v[q].w : 0.f;
+      bs[(k4 + 0) * ldb_s + cc] = k4 + 0 < h ? v[q].x : 0.f;
+      bs[(k4 + 1) * ldb_s + cc] = k4 + 1 < h ? v[q].y : 0.f;
+      bs[(k4 + 2) * ldb_s + cc] = k4 + 2 < h ? v[q].z : 0.f;
+      bs[(k4 + 3) * ldb_s + cc] = k4 + 3 < h ? v[q].w : 0.f;
     }
   }
   cp_wait_all();
   __syncthreads();
-  const int tr = tid & 31, tc = tid >> 5;  // rows 4 tr .. 4 tr + 3, columns 8 tc .. 8 tc + 7
-  float acc[4][8];
+  const int tr = tid & 31, tc = tid >> 5;  // rows 4 tr .. 4 tr + 3, columns C tc .. C tc + C - 1
+  float acc[4][C];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+    for (int j = 0; j < C; ++j) acc[i][j] = 0.f;
   for (int k = 0; k < h; ++k) {
     const float4 a = *reinterpret_cast<const float4*>(&li[k * kLdI + 4 * tr]);
-    const float4 b0 = *reinterpret_cast<const float4*>(&bs[k * kLdB + 8 * tc]);
-    const float4 b1 = *reinterpret_cast<const float4*>(&bs[k * kLdB + 8 * tc + 4]);
+    float bv[C];
+    lds_n<C>(&bs[k * ldb_s + C * tc], bv);
     const float av[4] = {a.x, a.y, a.z, a.w};
-    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] += av[i] * bv[j];
+      for (int j = 0; j < C; ++j) acc[i][j] += av[i] * bv[j];
   }
-  __syncthreads();
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int cc = 8 * tc + j;
+  for (int j = 0; j < C; ++j) {
+    const int cc = C * tc + j;
     if (cc < nc)
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -550,20 +576,22 @@ __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict_
   }
 }
 
-// B (m x h, ldb) := B Dinv, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h);
-// one CTA per 64 rows, 256 threads each computing 4 rows x 8 columns, FP32.
+// B (m x h, ldb) := B Dinv, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h)
+template <int NB>
 __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict__ Dinv, int h, float* B, long ldb,
                                                           int m, __nv_bfloat16* __restrict__ mir, long ldm) {
+  using L = NarrowLeaf<NB>;
+  constexpr int C = L::kCpt, ldb_s = L::kLdB, RG = NB / 4;  // RG row groups of 4
   extern __shared__ __align__(16) float sm[];
   float* us = sm;                 // us[k * kLdI + c] = Dinv(k, c)
-  float* bs = sm + 128 * kLdI;    // bs[k * kLdB + rr] = B(r0 + rr, k)
+  float* bs = sm + 128 * kLdI;    // bs[k * ldb_s + rr] = B(r0 + rr, k)
   const int tid = threadIdx.x;
-  const int r0 = blockIdx.x * 64, nr = min(64, m - r0);
+  const int r0 = blockIdx.x * NB, nr = min(NB, m - r0);
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {  // B (r0 + rr, k), rr contiguous -> bs row k (16-byte copies)
-    const int e = tid + 256 * q, k = e >> 4, rr4 = (e & 15) * 4;
+  for (int q = 0; q < NB / 8; ++q) {  // B (r0 + rr, k), rr contiguous -> bs row k (16-byte copies)
+    const int e = tid + 256 * q, k = e / RG, rr4 = (e % RG) * 4;
     const int valid = (k < h) ? max(0, min(4, nr - rr4)) * 4 : 0;
-    cp16(&bs[k * kLdB + rr4], valid ? (const void*)&B[(size_t)k * ldb + r0 + rr4] : (const void*)B, valid);
+    cp16(&bs[k * ldb_s + rr4], valid ? (const void*)&B[(size_t)k * ldb + r0 + rr4] : (const void*)B, valid);
   }
   {
     float4 v[16];  // Dinv (k, cc) at Dinv[cc * 128 + k]: float4 loads along k, transposed into us
@@ -583,27 +611,25 @@ __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict
   }
   cp_wait_all();
   __syncthreads();
-  const int tr = tid & 15, tc = tid >> 4;  // rows 4 tr .. 4 tr + 3, columns 8 tc .. 8 tc + 7
-  float acc[4][8];
+  const int tr = tid % RG, tc = tid / RG;  // rows 4 tr .. 4 tr + 3, columns C tc .. C tc + C - 1
+  float acc[4][C];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+    for (int j = 0; j < C; ++j) acc[i][j] = 0.f;
   for (int k = 0; k < h; ++k) {
-    const float4 a = *reinterpret_cast<const float4*>(&bs[k * kLdB + 4 * tr]);
-    const float4 b0 = *reinterpret_cast<const float4*>(&us[k * kLdI + 8 * tc]);
-    const float4 b1 = *reinterpret_cast<const float4*>(&us[k * kLdI + 8 * tc + 4]);
+    const float4 a = *reinterpret_cast<const float4*>(&bs[k * ldb_s + 4 * tr]);
+    float bv[C];
+    lds_n<C>(&us[k * kLdI + C * tc], bv);
     const float av[4] = {a.x, a.y, a.z, a.w};
-    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] += av[i] * bv[j];
+      for (int j = 0; j < C; ++j) acc[i][j] += av[i] * bv[j];
   }
-  __syncthreads();
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int cc = 8 * tc + j;
+  for (int j = 0; j < C; ++j) {
+    const int cc = C * tc + j;
     if (cc < h)
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -616,12 +642,32 @@ __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict
     for (int i = 0; i < 4; ++i) {
       const int rr = 4 * tr + i;
       if (rr >= nr) continue;
-      __nv_bfloat16* dst = mir + (size_t)(r0 + rr) * ldm + 8 * tc;
+      __nv_bfloat16* dst = mir + (size_t)(r0 + rr) * ldm + C * tc;
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (8 * tc + j < h) dst[j] = __float2bfloat16_rn(acc[i][j]);
+      for (int j = 0; j < C; ++j)
+        if (C * tc + j < h) dst[j] = __float2bfloat16_rn(acc[i][j]);
     }
   }
+}
+
+// one narrow leaf: the per-CTA width that gives at least two CTAs per SM where it can
+template <bool LEFT>
+void launch_narrow_leaf(const float* dinv, int h, float* B, long ldb, int len, __nv_bfloat16* mir, long ldm,
+                        int sms, cudaStream_t s) {
+  const int nb = len <= 2 * sms * 16 ? 16 : len <= 2 * sms * 32 ? 32 : 64;
+#define BGPU_NARROW(NB)                                                                                  \
+  if (LEFT)                                                                                              \
+    k_apply_inv_left<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm); \
+  else                                                                                                   \
+    k_apply_inv_right<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm)
+  if (nb == 16) {
+    BGPU_NARROW(16);
+  } else if (nb == 32) {
+    BGPU_NARROW(32);
+  } else {
+    BGPU_NARROW(64);
+  }
+#undef BGPU_NARROW
 }
 
 // ---- FP64 mat-vec for the residuals: Y = beta Y + alpha A X (q <= Q columns) ----------------
@@ -809,9 +855,22 @@ struct MixedSolver::Impl {
   int op_rows = 0;     // rows of both operand buffers
   const void* map_key[2] = {};      // the buffers the tensor maps describe
   cudaGraphExec_t graph = nullptr;  // the captured factorisation
-  const void* graph_key[5] = {};
+  const void* graph_key[6] = {};
   int graph_n = 0;
   size_t graph_kernels = 0;
+  // per-launch device stamps of the GEMMs (live timing that works inside the graph): slots taken in
+  // launch order as the recursion runs (or is captured), with each launch's flops
+  std::string host_note;  // host-side times of the last build (allocations, graph capture)
+  Buf stamps;
+  int slot_cap = 0, nslots = 0;
+  double slot_work = 0;
+  int graph_slots = 0;
+  double graph_work = 0;
+  unsigned long long* next_stamp(double flops) {
+    if (nslots >= slot_cap) return nullptr;
+    slot_work += flops;
+    return stamps.as<unsigned long long>() + 2 * (size_t)nslots++;
+  }
   int n3 = 0;
   long ld32 = 0;
   double* gr64 = nullptr;  // the FP64 matrix (owned by the caller)
@@ -843,12 +902,11 @@ struct MixedSolver::Impl {
   void gemm(int m, int n, int k, int ar, int ac, int br, int bc, int cr, int cc, cudaStream_t s) {
     if (m <= 0 || n <= 0 || k <= 0) return;
     float* C = at_(cr, cc);
-    KernelTimer& kt = kernel_timer(1);
     if (mirrors) {
       prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
-      kt.begin(s);
-      ck(gemm_bf16_tc_minus_at(m, n, k, map_am, ar, ac, map_bm, bc, br, C, ld32, d_status(), s), "tensor-core GEMM");
-      kt.end(s, 2.0 * m * n * k);
+      ck(gemm_bf16_tc_minus_at(m, n, k, map_am, ar, ac, map_bm, bc, br, C, ld32, d_status(), s,
+                               next_stamp(2.0 * m * n * k)),
+         "tensor-core GEMM");
       prof.end(s);
       return;
     }
@@ -865,10 +923,9 @@ struct MixedSolver::Impl {
         ck(cast_bf16(at_(br, bc + n0), ld32, k, nn, bt.p, op_ld, s), "cast B");
         prof.end(s);
         prof.begin(size_class(mm, nn, k), 2.0 * mm * nn * k, s);
-        kt.begin(s);
-        ck(gemm_bf16_tc_minus_maps(mm, nn, k, map_a, map_b, at_(cr + m0, cc + n0), ld32, d_status(), s),
+        ck(gemm_bf16_tc_minus_maps(mm, nn, k, map_a, map_b, at_(cr + m0, cc + n0), ld32, d_status(), s,
+                                   next_stamp(2.0 * mm * nn * k)),
            "tensor-core GEMM");
-        kt.end(s, 2.0 * mm * nn * k);
         prof.end(s);
       }
     }
@@ -892,8 +949,7 @@ struct MixedSolver::Impl {
         k_leaf_mult<true><<<(w + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(dinv, h, at_(kd, c0), ld32,
                                                                                            w, mir, ldm);
       else
-        k_apply_inv_left<<<(w + 63) / 64, 256, (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float), s>>>(
-            dinv, h, at_(kd, c0), ld32, w, mir, ldm);
+        launch_narrow_leaf<true>(dinv, h, at_(kd, c0), ld32, w, mir, ldm, sms, s);
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
@@ -916,8 +972,7 @@ struct MixedSolver::Impl {
         k_leaf_mult<false><<<(m + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(dinv, h, at_(r0, kd),
                                                                                             ld32, m, mir, ldm);
       else
-        k_apply_inv_right<<<(m + 63) / 64, 256, (size_t)(128 * kLdI + 128 * kLdB) * sizeof(float), s>>>(
-            dinv, h, at_(r0, kd), ld32, m, mir, ldm);
+        launch_narrow_leaf<false>(dinv, h, at_(r0, kd), ld32, m, mir, ldm, sms, s);
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
@@ -995,7 +1050,12 @@ struct MixedSolver::Impl {
   }
 };
 
-std::vector<std::string> MixedSolver::profile_report() { return p_->prof.report(); }
+std::vector<std::string> MixedSolver::profile_report() {
+  std::vector<std::string> out = p_->prof.report();
+  if (!p_->host_note.empty()) out.push_back(p_->host_note);
+  p_->host_note.clear();
+  return out;
+}
 
 MixedSolver::MixedSolver() : p_(new Impl) {
   const char* e = std::getenv("BEST_GPU_PROFILE");
@@ -1022,6 +1082,12 @@ const char* MixedSolver::name() const { return "BF16 tensor-core (FP32 factors) 
 void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, long ld, double eps, cudaStream_t s,
                         cudaEvent_t ev_assembled, cudaEvent_t ev_factored) {
   Impl& P = *p_;
+  using clk = std::chrono::steady_clock;
+  const auto ms_since = [](clk::time_point t) {
+    return std::chrono::duration<double, std::milli>(clk::now() - t).count();
+  };
+  const clk::time_point t_begin = clk::now();
+  double ms_alloc = 0, ms_capture = 0, ms_inst = 0;
   P.n3 = 3 * m.n;
   // columns 128-byte aligned, but not a multiple of 1 KB apart: the triangular solves read 64
   // columns at once, and a power-of-two-like stride puts them all on the same memory partitions
@@ -1080,26 +1146,47 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     ck(cudaFuncSetAttribute(k_lu32_leaf_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024), "attr");
     ck(cudaFuncSetAttribute(k_leaf_mult<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
     ck(cudaFuncSetAttribute(k_leaf_mult<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
-    ck(cudaFuncSetAttribute(k_apply_inv_left, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
-    ck(cudaFuncSetAttribute(k_apply_inv_right, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_left<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_left<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_left<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_right<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_right<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+    ck(cudaFuncSetAttribute(k_apply_inv_right<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
     attrs = true;
   }
   ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
+  ms_alloc = ms_since(t_begin);
   ck(launch_assemble(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
   ck(cudaEventRecord(ev_assembled, s), "event");
+  // GEMM stamp slots: far more than the recursion's launches (about 8 per 128-row leaf with the
+  // mirrors; the blocked products without them add a few per leaf)
+  const int cap = 64 * ((P.n3 + kLeaf - 1) / kLeaf) + 4096;
+  if (P.slot_cap < cap || !P.stamps.p) {
+    P.stamps.ensure((size_t)cap * 2 * sizeof(unsigned long long), "GEMM timing stamps");
+    P.slot_cap = cap;
+  }
   if (!P.side) {
     ck(cudaStreamCreateWithFlags(&P.side, cudaStreamNonBlocking), "side stream");
     ck(cudaEventCreateWithFlags(&P.ev_fork, cudaEventDisableTiming), "fork event");
     ck(cudaEventCreateWithFlags(&P.ev_join, cudaEventDisableTiming), "join event");
   }
-  if (P.prof.on || kernel_timer(1).on) {
+  int used_slots = 0;
+  double used_work = 0;
+  if (P.prof.on) {
     P.fork = false;
+    P.nslots = 0;
+    P.slot_work = 0;
+    ck(stamps_reset(P.stamps.as<unsigned long long>(), P.slot_cap, s), "stamps");
     P.rlu(0, P.n3, s);  // direct launches in order, each timed
+    used_slots = P.nslots;
+    used_work = P.slot_work;
   } else {
     // the recursion's launches depend only on the order and the buffers: capture them once as a
     // CUDA graph and replay it
-    const void* key[5] = {P.lu32.p, P.mirrors ? P.am.p : P.at.p, P.mirrors ? P.bm.p : P.bt.p, P.dl32.p, P.du32.p};
-    if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 5, P.graph_key)) {
+    const void* key[6] = {P.lu32.p, P.mirrors ? P.am.p : P.at.p, P.mirrors ? P.bm.p : P.bt.p,
+                          P.dl32.p, P.du32.p, P.stamps.p};
+    if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 6, P.graph_key)) {
+      const clk::time_point t_cap = clk::now();
       if (P.graph) cudaGraphExecDestroy(P.graph);
       P.graph = nullptr;
       cudaStream_t cs;
@@ -1108,6 +1195,8 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       const unsigned long long launches0 = g_launches;  // captured launches do not run now
       ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
       P.fork = P.mirrors && std::getenv("BEST_GPU_ONE_STREAM") == nullptr;
+      P.nslots = 0;
+      P.slot_work = 0;
       try {
         P.rlu(0, P.n3, cs);
       } catch (...) {
@@ -1120,19 +1209,45 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       ck(cudaStreamEndCapture(cs, &g), "end capture");
       P.graph_kernels = (size_t)(g_launches - launches0);
       g_launches = launches0;
+      ms_capture = ms_since(t_cap);
+      const clk::time_point t_inst = clk::now();
       ck(cudaGraphInstantiate(&P.graph, g, 0), "graph instantiate");
+      ms_inst = ms_since(t_inst);
       cudaGraphDestroy(g);
       cudaStreamDestroy(cs);
-      std::copy(key, key + 5, P.graph_key);
+      std::copy(key, key + 6, P.graph_key);
       P.graph_n = P.n3;
+      P.graph_slots = P.nslots;
+      P.graph_work = P.slot_work;
     }
+    ck(stamps_reset(P.stamps.as<unsigned long long>(), P.graph_slots, s), "stamps");
     ck(cudaGraphLaunch(P.graph, s), "graph launch");
     g_launches += P.graph_kernels;
+    used_slots = P.graph_slots;
+    used_work = P.graph_work;
   }
   ck(cudaEventRecord(ev_factored, s), "event");
   int st = 0;
   ck(cudaMemcpyAsync(&st, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
   ck(cudaStreamSynchronize(s), "factorisation");
+  {
+    char note[256];
+    std::snprintf(note, sizeof note,
+                  "mixed build, host side: allocations %.1f ms, graph capture %.1f ms, instantiation %.1f ms, "
+                  "whole call %.1f ms",
+                  ms_alloc, ms_capture, ms_inst, ms_since(t_begin));
+    P.host_note = note;
+  }
+  KernelTimer& kt = kernel_timer(1);
+  if (kt.on && used_slots > 0) {
+    // live GEMM time of this factorisation: each launch's last end minus its first start
+    std::vector<unsigned long long> h((size_t)2 * used_slots);
+    ck(cudaMemcpy(h.data(), P.stamps.p, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stamps");
+    double ns = 0;
+    for (int i = 0; i < used_slots; ++i)
+      if (h[2 * i + 1] >= h[2 * i]) ns += (double)(h[2 * i + 1] - h[2 * i]);
+    kt.add(used_slots, ns * 1e-6, used_work);
+  }
   if (st != 0) {
     ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
     throw MixedFailure(st == kZeroPivot ? "the unpivoted FP32 factorisation met a zero or non-finite pivot"
@@ -1147,6 +1262,9 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
   const int max_restarts = P.max_restarts;
   int total_iters = 0;
   double worst = 0.0;
+  using clk = std::chrono::steady_clock;
+  const clk::time_point t_begin = clk::now();
+  double ms_alloc = 0;
   const bool fresh_scratch = !P.trsv.p || P.trsv.bytes < trsv_scratch_bytes(n);
   P.trsv.ensure(trsv_scratch_bytes(n), "solve scratch");
   if (fresh_scratch) ck(cudaMemsetAsync(P.trsv.p, 0, P.trsv.bytes, s), "solve scratch clear");  // flags start at 0
@@ -1156,6 +1274,7 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
     // [B | X | R | W | V_0..V_m | Z_0..Z_{m-1}]
     P.vecs.ensure(blk * (4 + (m + 1) + m) * sizeof(double), "GMRES vectors");
     P.zf.ensure(blk * sizeof(float), "preconditioner vectors (FP32)");
+    if (c0 == 0) ms_alloc = std::chrono::duration<double, std::milli>(clk::now() - t_begin).count();
     double* B = P.vecs.as<double>();
     double* X = B + blk;
     double* R = X + blk;
@@ -1286,6 +1405,10 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
     rep->iterations = total_iters;
     rep->relres = worst;
   }
+  char note[160];
+  std::snprintf(note, sizeof note, "mixed solve, host side: allocations %.1f ms, whole call %.1f ms", ms_alloc,
+                std::chrono::duration<double, std::milli>(clk::now() - t_begin).count());
+  P.host_note = note;
 }
 
 }  // namespace bgpu

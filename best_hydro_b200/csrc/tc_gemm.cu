@@ -133,11 +133,14 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 }
 
 // A's tiles start at row a_y0, column (K) a_x0 of its tensor map; B's at row b_y0, column b_x0 of its
-// (both 0 for operand buffers that hold just this product).
+// (both 0 for operand buffers that hold just this product).  stamp (optional): the launch's first
+// CTA start and last CTA end on the global nanosecond timer, as atomic min into stamp[0] and max into
+// stamp[1] (live per-launch timing that also works inside a CUDA graph).
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int m, int n,
                    int k, float* __restrict__ C, long ldc, int tiles_m, int tiles_n, int* status, int a_y0, int a_x0,
-                   int b_y0, int b_x0) {
+                   int b_y0, int b_x0, unsigned long long* stamp) {
+  if (stamp && threadIdx.x == 0) atomicMin(stamp, global_ns());
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;
@@ -272,6 +275,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 1) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
   }
+  if (stamp && threadIdx.x == 0) {
+    __threadfence();
+    atomicMax(stamp + 1, global_ns());
+  }
+}
+
+__global__ void k_stamps_reset(unsigned long long* stamps, int slots) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < slots; i += gridDim.x * blockDim.x) {
+    stamps[2 * i] = ~0ull;
+    stamps[2 * i + 1] = 0ull;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -387,12 +401,19 @@ cudaError_t tc_gemm_prepare() {
 
 // (tc_gemm_prepare must have run: the launch may be captured into a graph)
 cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, const void* map_b, float* C, long ldc,
-                                    int* d_status, cudaStream_t s) {
+                                    int* d_status, cudaStream_t s, unsigned long long* stamp) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
   k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
       *static_cast<const CUtensorMap*>(map_a), *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m,
-      tiles_n, d_status, 0, 0, 0, 0);
+      tiles_n, d_status, 0, 0, 0, 0, stamp);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t stamps_reset(unsigned long long* stamps, int slots, cudaStream_t s) {
+  if (slots <= 0) return cudaSuccess;
+  k_stamps_reset<<<(slots + 255) / 256, 256, 0, s>>>(stamps, slots);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -409,13 +430,14 @@ bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a
 // b_k = first row of B) of map_b's (column-major) matrix; a_k and b_k multiples of 8, k a multiple
 // of 64.
 cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
-                                  int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s) {
+                                  int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s,
+                                  unsigned long long* stamp) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   if ((a_k % 8) || (b_k % 8) || (k % BK)) return cudaErrorInvalidValue;
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
   k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
       *static_cast<const CUtensorMap*>(map_a), *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m,
-      tiles_n, d_status, a_row, a_k, b_row, b_k);
+      tiles_n, d_status, a_row, a_k, b_row, b_k, stamp);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -436,7 +458,7 @@ cudaError_t gemm_bf16_tc_minus(int m, int n, int k, const void* At, long lda_t, 
   }
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
   k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(ta, tb, m, n, k, C, ldc, tiles_m,
-                                                                              tiles_n, d_status, 0, 0, 0, 0);
+                                                                              tiles_n, d_status, 0, 0, 0, 0, nullptr);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
