@@ -60,6 +60,8 @@ _SIGS = {
                                                    ctypes.c_int]),
     "bgpu_assemble_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_int]),
+    "bgpu_assemble_device_mixed": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_void_p, ctypes.c_int]),
     "bgpu_series_create": (ctypes.c_int, [ctypes.c_int, _ip, _dp, _dp, _dp, _dp, _dp, ctypes.c_double]),
     "bgpu_series_incenters": (ctypes.c_int, [_dp]),
     "bgpu_series_diag_mean": (ctypes.c_int, [_dp]),
@@ -459,6 +461,7 @@ def gemm_bf16_minus_device(m, n, k, d_a, lda, d_b, ldb, d_c, ldc):
            "bgpu_gemm_bf16_minus_device")
 
 
-def assemble_device(r0, r1, c0, c1, d_out, ldo):
-    _check(lib().bgpu_assemble_device(int(r0), int(r1), int(c0), int(c1), ctypes.c_void_p(d_out), int(ldo)),
-           "bgpu_assemble_device")
+def assemble_device(r0, r1, c0, c1, d_out, ldo, mixed=False):
+    """GR block (before deflation) into device memory; mixed=True: the mixed path's assembly."""
+    fn = lib().bgpu_assemble_device_mixed if mixed else lib().bgpu_assemble_device
+    _check(fn(int(r0), int(r1), int(c0), int(c1), ctypes.c_void_p(d_out), int(ldo)), "bgpu_assemble_device")

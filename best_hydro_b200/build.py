@@ -21,6 +21,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", f"-I{CSRC
 # (source, extra flags)
 SOURCES = [
     ("assemble.cu", ["-fmad=false"]),
+    ("assemble_fast.cu", []),
     ("lu.cu", []),
     ("solve.cu", []),
     ("tc_gemm.cu", []),

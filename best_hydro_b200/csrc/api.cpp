@@ -1279,7 +1279,7 @@ int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float* d_a, int lda, 
   });
 }
 
-int bgpu_assemble_device(int r0, int r1, int c0, int c1, double* d_out, int ldo) {
+static int assemble_device(bool fast, int r0, int r1, int c0, int c1, double* d_out, int ldo) {
   return guarded([&] {
     Solver& s = solver();
     Runtime& r = rt();
@@ -1289,12 +1289,23 @@ int bgpu_assemble_device(int r0, int r1, int c0, int c1, double* d_out, int ldo)
     }
     DevDeflation none;
     ck(cudaEventRecord(r.ev[2], r.stream), "event");
-    ck(launch_assemble(s.mesh(), r0, r1, c0, c1, d_out, ldo, none, nullptr, 0, r.stream), "assembly");
+    if (fast)
+      ck(launch_assemble_fast(s.mesh(), r0, r1, c0, c1, d_out, ldo, none, nullptr, 0, r.stream), "assembly");
+    else
+      ck(launch_assemble(s.mesh(), r0, r1, c0, c1, d_out, ldo, none, nullptr, 0, r.stream), "assembly");
     ck(cudaEventRecord(r.ev[3], r.stream), "event");
     r.sync("assembly");
     r.ms[1] = r.elapsed(2, 3);
     return 0;
   });
+}
+
+int bgpu_assemble_device(int r0, int r1, int c0, int c1, double* d_out, int ldo) {
+  return assemble_device(false, r0, r1, c0, c1, d_out, ldo);
+}
+
+int bgpu_assemble_device_mixed(int r0, int r1, int c0, int c1, double* d_out, int ldo) {
+  return assemble_device(true, r0, r1, c0, c1, d_out, ldo);
 }
 
 }  // extern "C"

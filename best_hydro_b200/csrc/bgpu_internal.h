@@ -86,6 +86,10 @@ cudaError_t launch_self_blocks(const DevMesh& m, cudaStream_t s);
 // a single-precision copy (rounded to nearest) is written too (leading dimension ld32).
 cudaError_t launch_assemble(const DevMesh& m, int r0, int r1, int c0, int c1, double* out, long ld,
                             const DevDeflation& defl, float* out32, long ld32, cudaStream_t s);
+// The same matrix for the mixed path with fewer FP64 operations (assemble_fast.cu): entries within a
+// few ulp of launch_assemble's, not bit-compatible with the reference.
+cudaError_t launch_assemble_fast(const DevMesh& m, int r0, int r1, int c0, int c1, double* out, long ld,
+                                 const DevDeflation& defl, float* out32, long ld32, cudaStream_t s);
 // Every mesh of a series at once (whole GR of each, with its deflation): mesh i into out[i] (ld[i]).
 constexpr int kMaxSeries = 16;
 struct SeriesAssembly {

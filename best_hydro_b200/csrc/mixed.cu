@@ -1156,7 +1156,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   }
   ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
   ms_alloc = ms_since(t_begin);
-  ck(launch_assemble(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
+  ck(launch_assemble_fast(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
   ck(cudaEventRecord(ev_assembled, s), "event");
   // GEMM stamp slots: far more than the recursion's launches (about 8 per 128-row leaf with the
   // mirrors; the blocked products without them add a few per leaf)

@@ -81,6 +81,10 @@ int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float *d_a, int lda, 
 /* Assembles GR rows of triangles [r0, r1) x columns of triangles [c0, c1) of the mesh given to
  * bhm_create into d_out (column-major, ldo), before deflation (best/tgetgr.f:33-173). */
 int bgpu_assemble_device(int r0, int r1, int c0, int c1, double *d_out, int ldo);
+/* The same block with the mixed-precision path's assembly: fewer FP64 operations (rsqrt, shared
+ * reciprocals, FMA contraction); entries within a few ulp of bgpu_assemble_device's, not
+ * bit-compatible with the reference. */
+int bgpu_assemble_device_mixed(int r0, int r1, int c0, int c1, double *d_out, int ldo);
 
 /* ---- Series of meshes (BEST's workflow of results extrapolated linearly in 1/N: rcoal makes a
  * series of triangulations of one surface, best/best.f:154-157, README.md:12-16) ---------------

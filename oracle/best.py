@@ -290,6 +290,71 @@ def assemble_ref(s: Setup, cg=1.0, rows=None, cols=None):
     return gr, x, dm
 
 
+# 21-point Gauss-Legendre rule of best/triangleint.f:66-108 (decimal literals)
+_GY = (3.1239146898052499e-3, 1.6386580716846853e-2, 3.9950332924799586e-2, 7.3318317708341358e-2,
+       0.1157800182621610, 0.1664305979012938, 0.2241905820563901, 0.2878289398962806,
+       0.3559893415987995, 0.4272190729195525, 0.5, 0.5727809270804476,
+       0.6440106584012005, 0.7121710601037194, 0.7758094179436099, 0.8335694020987062,
+       0.8842199817378390, 0.9266816822916586, 0.9600496670752004, 0.9836134192831531,
+       0.9968760853101948)
+_GW = (1.601722825777433e-2, 3.695378977085249e-2, 5.713442542685720e-2, 7.610011362837930e-2,
+       9.344442345603390e-2, 0.1087972991671484, 0.1218314160537285, 0.1322689386333375,
+       0.1398873947910731, 0.1445244039899701, 0.1460811336496904, 0.1445244039899701,
+       0.1398873947910731, 0.1322689386333375, 0.1218314160537285, 0.1087972991671484,
+       9.344442345603390e-2, 7.610011362837930e-2, 5.713442542685720e-2, 3.695378977085249e-2,
+       1.601722825777433e-2)
+
+
+def pair_blocks_ld(s: Setup, x, rows, cols, cg=1.0):
+    """The 3x3 pair blocks GR(target rows[k], source cols[k]) (rows != cols) of best/triangleint.f:1-247
+    evaluated in numpy's long double (x86 80-bit, 64-bit significand): a reference value about 2^11
+    times more precise than any FP64 evaluation, for judging FP64 variants of the quadrature.
+    x: incenters as incenters_and_self returns them.  Returns (k, 3, 3) float64."""
+    T = np.longdouble
+    X = np.asarray(x, dtype=np.float64).reshape(3, -1).T[rows].astype(T)
+    P1, P2, P3 = (v[cols].astype(T) for v in (s.v1, s.v2, s.v3))
+    area = s.area[cols].astype(T)
+
+    def dot(a, b):
+        return a[:, 0] * b[:, 0] + a[:, 1] * b[:, 1] + a[:, 2] * b[:, 2]
+
+    v21, v31, v32 = P2 - P1, P3 - P1, P3 - P2
+    v1c, v2c, v3c = P1 - X, P2 - X, P3 - X
+    d2121, d2131, d2132 = dot(v21, v21), dot(v21, v31), dot(v21, v32)
+    d3131, d3232, d3231 = dot(v31, v31), dot(v32, v32), dot(v32, v31)
+    s21 = np.sqrt(d2121)
+    d211c, d212c, d322c = dot(v21, v1c), dot(v21, v2c), dot(v32, v2c)
+    d1c1c, d1c31, d2c2c, d2c1c = dot(v1c, v1c), dot(v1c, v31), dot(v2c, v2c), dot(v2c, v1c)
+    d3c31, d3c32, d3c3c = dot(v3c, v31), dot(v3c, v32), dot(v3c, v3c)
+    S = [np.zeros_like(d2121) for _ in range(7)]
+    for y, w in zip(_GY, _GW):
+        y, w = T(y), T(w)
+        q1 = np.sqrt(d1c1c + 2 * y * d1c31 + y * y * d3131)
+        q2 = np.sqrt(d2c2c + 2 * y * d322c + y * y * d3232)
+        hv = np.log((d212c + d2132 * y + s21 * q2) / (d211c + d2131 * y + s21 * q1)) / s21
+        hyc = (d211c * d211c - d1c1c * d2121 - 2 * y * d1c31 * d2121 + 2 * y * d211c * d2131 +
+               y * y * d2131 * d2131 - y * y * d2121 * d3131)
+        hyv = ((d211c + y * d2131) / q1 - (y * d2132 + d212c) / q2) / hyc
+        hxyv = (q1 + (y * d211c - d2c1c - 2 * y * d1c31 - y * d2131 - y * y * d3231) / q2) / (-hyc)
+        hxa = (-d1c31 - y * d2131) / np.sqrt(d1c1c + 2 * y * d211c + y * y * d2121)
+        hxb = (d3c31 - y * d3231) / np.sqrt(y * y * d3232 - 2 * y * d3c32 + d3c3c)
+        hxc = (d1c1c * d3131 - d1c31 * d1c31 + 2 * y * (d211c * d3131 - d1c31 * d2131) +
+               y * y * (d2121 * d3131 - d2131 * d2131))
+        hxv = (hxa + hxb) / hxc
+        for k, v in enumerate((w * hv, w * hyv, w * hxyv, w * y * hyv, w * y * hxyv, w * y * y * hyv, w * y * y * hxv)):
+            S[k] = S[k] + v
+    t0, s0, sx, sy, sxy, syy, sxx = (v / 2 for v in S)
+    out = np.empty((len(rows), 3, 3), dtype=np.float64)
+    for a in range(3):
+        for b in range(3):
+            tt = (v1c[:, a] * v1c[:, b] * s0 + (v1c[:, a] * v21[:, b] + v21[:, a] * v1c[:, b]) * sx +
+                  (v31[:, a] * v1c[:, b] + v1c[:, a] * v31[:, b]) * sy +
+                  (v21[:, a] * v31[:, b] + v31[:, a] * v21[:, b]) * sxy +
+                  v21[:, a] * v21[:, b] * sxx + v31[:, a] * v31[:, b] * syy)
+            out[:, a, b] = (2 * area * ((t0 if a == b else 0) + T(cg) * tt)).astype(np.float64)
+    return out
+
+
 def diag_mean(self9, n):
     return lib().orc_diag_mean(n, _ptr(self9))
 

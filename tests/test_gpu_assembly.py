@@ -125,3 +125,47 @@ def test_bhm_entries_ranges():
         a = solver.entries(i0, m, j0, nc)
         check_block(a, s, 1.0, i0, j0, label=f"entries({i0},{m},{j0},{nc})")
     solver.destroy()
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_mixed_assembly_entries(case):
+    """The mixed path's assembly (rsqrt, shared reciprocals, FMA contraction) against the bit-exact
+    kernel on the same mesh.  Self blocks are identical.  The pair quadrature loses accuracy on
+    ill-conditioned pairs in both forms: a target nearly in the plane of a source triangle and near
+    the line of its edge 1-2, where the numerator and the denominator of hy (triangleint.f:222-234)
+    both vanish; the reference's own FP64 formula errs by up to ~1e-9 of the row scale there.  So the
+    bar is set against the truth: on the 40 blocks where the two kernels differ most, a long-double
+    evaluation shows the mixed kernel's worst and median errors within 4x the exact kernel's (plus
+    1e-13 of the row scale); everywhere the two differ by < 1e-8 of the row scale."""
+    torch = _torch()
+    (tri, ta, tv), iarea, cg = CASES[case]()
+    s = ob.setup(tri, iarea, ta)
+    solver, gr = gpu_gr(s, cg)
+    n3 = 3 * s.n
+    d = torch.empty((n3, n3), dtype=torch.float64, device="cuda")
+    assemble_device(0, s.n, 0, s.n, d.data_ptr(), n3, mixed=True)
+    torch.cuda.synchronize()
+    fast = d.cpu().numpy().reshape(n3, n3).T
+    x = solver.incenters()
+    solver.destroy()
+    mask = self_mask(n3)
+    assert np.array_equal(fast[mask], gr[mask])
+    scale = np.abs(gr).max(axis=1, keepdims=True)
+    err = np.abs(fast - gr) / scale
+    assert err.max() < 1e-8
+    blk = err.reshape(s.n, 3, s.n, 3).max(axis=(1, 3))
+    np.fill_diagonal(blk, 0.0)
+    worst = np.argsort(blk, axis=None)[-40:]
+    rows, cols = np.unravel_index(worst, blk.shape)
+    truth = ob.pair_blocks_ld(s, x, rows, cols, cg)
+    sc = scale.reshape(s.n, 3).max(axis=1)[rows][:, None, None]
+    gf = fast.reshape(s.n, 3, s.n, 3)[rows, :, cols, :]
+    ge = gr.reshape(s.n, 3, s.n, 3)[rows, :, cols, :]
+    e_fast = (np.abs(gf - truth) / sc).max(axis=(1, 2))
+    e_exact = (np.abs(ge - truth) / sc).max(axis=(1, 2))
+    h, w = ob.ulp_hist(fast[~mask], gr[~mask])
+    print(f"\n{case}: mixed vs exact entries, ulp histogram 0..6,>6: {h.tolist()}; largest difference "
+          f"{err.max():.2e} of the row scale; on those blocks, error vs long double: mixed {e_fast.max():.2e}, "
+          f"exact {e_exact.max():.2e}")
+    assert e_fast.max() <= 4 * e_exact.max() + 1e-13
+    assert np.median(e_fast) <= 4 * np.median(e_exact) + 1e-13

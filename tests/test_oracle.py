@@ -115,3 +115,22 @@ def test_self_blocks_differ_from_glibc_only_where_glibc_misrounds():
     same = np.count_nonzero(s_cr == s_g)
     assert same >= 0.99 * s_g.size
     assert np.max(crshim.block_scale_ulps(s_cr, s_g)) <= 4
+
+
+def test_pair_blocks_long_double():
+    """The long-double pair blocks (the reference value the mixed assembly is judged against) agree
+    with the FP64 restatement within the FP64 formula's own error: 1e-10 of the row scale."""
+    tri, ta, tv = golden_mesh("2eu7_02562")
+    s = ob.setup(tri, 1, ta)
+    x, _ = ob.incenters_and_self(s, 1.0)
+    gr, _, _ = ob.assemble(s, 1.0, rows=(0, 40), cols=(0, s.n))
+    rng = np.random.default_rng(3)
+    rows = rng.integers(0, 40, 200)
+    cols = rng.integers(0, s.n, 200)
+    keep = rows != cols
+    rows, cols = rows[keep], cols[keep]
+    t = ob.pair_blocks_ld(s, x, rows, cols, 1.0)
+    scale = np.abs(gr).reshape(40, 3, -1).max(axis=(1, 2))
+    for k, (r, c) in enumerate(zip(rows, cols)):
+        g = gr[3 * r:3 * r + 3, 3 * c:3 * c + 3]
+        assert np.abs(g - t[k]).max() / scale[r] < 1e-10
