@@ -2,7 +2,8 @@
 
     python -m best_hydro_b200.kernel_cases tc_gemm M N K     # C -= A B, BF16 tcgen05 (FP32 C)
     python -m best_hydro_b200.kernel_cases dgemm M N K       # C -= A B, FP64 DMMA
-    python -m best_hydro_b200.kernel_cases assemble F        # GR of the ellipsoid at geodesic frequency F
+    python -m best_hydro_b200.kernel_cases assemble F [mixed]  # GR of the ellipsoid at geodesic frequency F
+                                                             # (mixed: the mixed path's assembly)
     python -m best_hydro_b200.kernel_cases mixed F           # mixed build + solve, ellipsoid frequency F
     python -m best_hydro_b200.kernel_cases adjoint F         # FP64 build + adjoint gradients (k_pair_adjoint)
 
@@ -78,11 +79,12 @@ def main(argv):
                 e0, e1 = _ev(torch)
                 torch.cuda.synchronize()
                 e0.record()
-                bh.assemble_device(0, st.n, 0, st.n, out.data_ptr(), n3)
+                bh.assemble_device(0, st.n, 0, st.n, out.data_ptr(), n3, mixed=len(argv) > 2 and argv[2] == "mixed")
                 e1.record()
                 torch.cuda.synchronize()
             ms = e0.elapsed_time(e1)
-            print(f"assemble N={st.n}: {ms:.3f} ms, {st.n * (st.n - 1) / ms / 1e6:.3f} Gpairs/s")
+            kind = "mixed" if len(argv) > 2 and argv[2] == "mixed" else "exact"
+            print(f"assemble ({kind}) N={st.n}: {ms:.3f} ms, {st.n * (st.n - 1) / ms / 1e6:.3f} Gpairs/s")
             return 0
         x = s.incenters()
         xmu, gdef = st.deflation(s.diag_mean())
