@@ -331,6 +331,7 @@ def run_ours(args, rank, world, local_rank):
     head = args.precision
     head_kernel = bh.BGPU_KERNEL_TC_GEMM if head == "mixed" else bh.BGPU_KERNEL_LU_GEMM64
     H = timed(head, args.warmup, args.steps, stats_kernel=head_kernel, clocks=True)
+    timeline = [ln.split("; ", 1)[1] for ln in bh.log_lines() if "factorisation timeline" in ln]
     acc_head = tensors_of(solver, x, st, bh)
 
     # the plain FP64 path beside the mixed one: its time per solve and its tensors (the reference
@@ -409,7 +410,8 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": args.workload, "N": n, "order": n3, "desc": w["desc"], "precision": head,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB write) between timed steps; GR is 72 N^2 bytes, far above L2",
-                       "stages_ms": H["stages_ms"], "e2e_phases_ms": e2e_phases,
+                       "stages_ms": H["stages_ms"], "factor_timeline": timeline[-1] if timeline else None,
+                       "e2e_phases_ms": e2e_phases,
                        "e2e_host_notes": host_notes},
             "roofline": roof,
             "clocks": H["clocks"],

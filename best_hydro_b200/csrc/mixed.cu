@@ -85,6 +85,26 @@ long round_up(long v, long q) { return (v + q - 1) / q * q; }
 // L^-1 (unit lower) and U^-1 are written to DL, DU (128 x 128 column-major, zero outside h x h).
 constexpr int kLdS = 129;
 
+// Optional launch stamps (as the GEMM's): the earliest CTA start into st[0], the latest CTA end into
+// st[1], global timer in ns.  st is a kernel argument, so the branch is uniform.
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void stamp_begin(unsigned long long* st) {
+  if (st && threadIdx.x == 0) atomicMin(st, gtimer_ns());
+}
+__device__ __forceinline__ void stamp_end(unsigned long long* st) {
+  if (st) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicMax(st + 1, gtimer_ns());
+    }
+  }
+}
+
 // rows q0 .. q0+3 of an 8 x 4 tile, as a 4 x 4 array (q0 = 0 or 4; selects keep it in registers)
 __device__ __forceinline__ void get4(const float (&a)[8][4], bool hi, float (&b)[4][4]) {
 #pragma unroll
@@ -103,7 +123,9 @@ __device__ __forceinline__ void put4(float (&a)[8][4], bool hi, const float (&b)
 }
 
 __global__ void __launch_bounds__(512, 1) k_lu32_leaf_inv(float* __restrict__ A, long lda, int h, float* __restrict__ DL,
-                                                           float* __restrict__ DU, int* status) {
+                                                           float* __restrict__ DU, int* status,
+                                                           unsigned long long* stamp) {
+  stamp_begin(stamp);
   extern __shared__ float sm[];
   float* d = sm;                     // d[c * kLdS + r] = block entry (r, c)
   float* ub = sm + 128 * kLdS;       // [2][4][128]: the 4 rows of U of a step (then rows of X)
@@ -361,6 +383,7 @@ __global__ void __launch_bounds__(512, 1) k_lu32_leaf_inv(float* __restrict__ A,
     }
   }
   if (tid == 0 && s_bad) atomicExch(status, kZeroPivot);
+  stamp_end(stamp);
 }
 
 // 16-byte asynchronous copy global -> shared; fewer than 16 source bytes are zero-filled
@@ -374,7 +397,9 @@ constexpr int kLm = 132;  // row stride of the shared operands (floats)
 constexpr int kWideLeaf = 8192;  // from this many columns (rows) on, k_leaf_mult; below, 64 per CTA
 template <bool LEFT>
 __global__ void __launch_bounds__(256, 1) k_leaf_mult(const float* __restrict__ Dinv, int h, float* B, long ldb,
-                                                      int len, __nv_bfloat16* __restrict__ mir, long ldm) {
+                                                      int len, __nv_bfloat16* __restrict__ mir, long ldm,
+                                                      unsigned long long* stamp) {
+  stamp_begin(stamp);
   extern __shared__ __align__(16) float sm[];
   float* As = sm;               // As[k * kLm + i]: the left factor's (i, k)
   float* Bs = sm + 128 * kLm;   // Bs[k * kLm + j]: the right factor's (k, j)
@@ -481,6 +506,7 @@ __global__ void __launch_bounds__(256, 1) k_leaf_mult(const float* __restrict__ 
         if (ii < nt && jj < h) mir[(size_t)(t0 + ii) * ldm + jj] = __float2bfloat16_rn(Cs[jj * kLm + ii]);
       }
   }
+  stamp_end(stamp);
 }
 
 // The narrow leaves (fewer than kWideLeaf columns or rows), FP32, 256 threads, NB = 64, 32 or 16
@@ -513,7 +539,9 @@ __device__ __forceinline__ void lds_n(const float* p, float (&v)[C]) {
 // B (h x w, ldb) := Dinv B, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h)
 template <int NB>
 __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict__ Dinv, int h, float* B, long ldb,
-                                                         int w, __nv_bfloat16* __restrict__ mir, long ldm) {
+                                                         int w, __nv_bfloat16* __restrict__ mir, long ldm,
+                                                         unsigned long long* stamp) {
+  stamp_begin(stamp);
   using L = NarrowLeaf<NB>;
   constexpr int C = L::kCpt, ldb_s = L::kLdB;
   extern __shared__ __align__(16) float sm[];
@@ -574,12 +602,15 @@ __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict_
         }
       }
   }
+  stamp_end(stamp);
 }
 
 // B (m x h, ldb) := B Dinv, Dinv an inverse diagonal block (128 x 128, ld 128, zero outside h)
 template <int NB>
 __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict__ Dinv, int h, float* B, long ldb,
-                                                          int m, __nv_bfloat16* __restrict__ mir, long ldm) {
+                                                          int m, __nv_bfloat16* __restrict__ mir, long ldm,
+                                                          unsigned long long* stamp) {
+  stamp_begin(stamp);
   using L = NarrowLeaf<NB>;
   constexpr int C = L::kCpt, ldb_s = L::kLdB, RG = NB / 4;  // RG row groups of 4
   extern __shared__ __align__(16) float sm[];
@@ -648,18 +679,19 @@ __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict
         if (C * tc + j < h) dst[j] = __float2bfloat16_rn(acc[i][j]);
     }
   }
+  stamp_end(stamp);
 }
 
 // one narrow leaf: the per-CTA width that gives at least two CTAs per SM where it can
 template <bool LEFT>
 void launch_narrow_leaf(const float* dinv, int h, float* B, long ldb, int len, __nv_bfloat16* mir, long ldm,
-                        int sms, cudaStream_t s) {
+                        int sms, cudaStream_t s, unsigned long long* st) {
   const int nb = len <= 2 * sms * 16 ? 16 : len <= 2 * sms * 32 ? 32 : 64;
 #define BGPU_NARROW(NB)                                                                                  \
   if (LEFT)                                                                                              \
-    k_apply_inv_left<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm); \
+    k_apply_inv_left<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm, st); \
   else                                                                                                   \
-    k_apply_inv_right<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm)
+    k_apply_inv_right<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm, st)
   if (nb == 16) {
     BGPU_NARROW(16);
   } else if (nb == 32) {
@@ -841,6 +873,40 @@ struct CallProfile {
   }
 };
 
+// kinds of the factorisation's stamped launches
+constexpr unsigned char kSlotGemm = 0, kSlotLuLeaf = 1, kSlotSolveLeaf = 2;
+
+// The factorisation's timeline from its launch stamps: how long some kernel ran, a GEMM ran, only
+// leaves ran (LU leaves among them), and nothing ran, between the first start and the last end.
+std::string timeline_note(const std::vector<unsigned long long>& h, const std::vector<unsigned char>& kind, int n) {
+  std::vector<std::pair<unsigned long long, int>> ev;  // (time, +-(1 + kind))
+  for (int i = 0; i < n; ++i)
+    if (h[2 * i + 1] >= h[2 * i]) {
+      ev.emplace_back(h[2 * i], 1 + kind[i]);
+      ev.emplace_back(h[2 * i + 1], -(1 + kind[i]));
+    }
+  if (ev.empty()) return "";
+  std::sort(ev.begin(), ev.end());
+  int cnt[3] = {0, 0, 0};
+  double busy = 0, gemm = 0, leaves_only = 0, lu_only = 0;
+  for (size_t i = 0; i + 1 < ev.size(); ++i) {
+    const int k = std::abs(ev[i].second) - 1;
+    cnt[k] += ev[i].second > 0 ? 1 : -1;
+    const double dt = (double)(ev[i + 1].first - ev[i].first) * 1e-6;
+    if (cnt[0] + cnt[1] + cnt[2] > 0) busy += dt;
+    if (cnt[0] > 0) gemm += dt;
+    if (cnt[0] == 0 && cnt[1] + cnt[2] > 0) leaves_only += dt;
+    if (cnt[0] == 0 && cnt[1] > 0) lu_only += dt;
+  }
+  const double span = (double)(ev.back().first - ev.front().first) * 1e-6;
+  char note[256];
+  std::snprintf(note, sizeof note,
+                "factorisation timeline: %.1f ms from first start to last end; a GEMM running %.1f ms, only leaves "
+                "%.1f ms (an LU leaf %.1f ms), nothing %.1f ms",
+                span, gemm, leaves_only, lu_only, span - busy);
+  return note;
+}
+
 std::string size_class(int m, int n, int k) {
   auto c = [](int v) { return v <= 256 ? "S" : (v <= 2048 ? "M" : "L"); };
   return std::string("gemm ") + c(m) + c(n) + c(k);
@@ -863,12 +929,14 @@ struct MixedSolver::Impl {
   std::string host_note;  // host-side times of the last build (allocations, graph capture)
   Buf stamps;
   int slot_cap = 0, nslots = 0;
-  double slot_work = 0;
+  double slot_work = 0;  // GEMM flops
+  std::vector<unsigned char> slot_kind;  // kSlot* of each slot, in launch order
   int graph_slots = 0;
   double graph_work = 0;
-  unsigned long long* next_stamp(double flops) {
+  unsigned long long* next_stamp(double flops, unsigned char kind = kSlotGemm) {
     if (nslots >= slot_cap) return nullptr;
-    slot_work += flops;
+    if (kind == kSlotGemm) slot_work += flops;
+    slot_kind.push_back(kind);
     return stamps.as<unsigned long long>() + 2 * (size_t)nslots++;
   }
   int n3 = 0;
@@ -946,10 +1014,11 @@ struct MixedSolver::Impl {
       __nv_bfloat16* mir = mirrors ? bm_at(kd, c0) : nullptr;
       prof.begin(w >= kWideLeaf ? "trsm leaf (left, wide)" : "trsm leaf (left)", 2.0 * h * h * w, s);
       if (w >= kWideLeaf)
-        k_leaf_mult<true><<<(w + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(dinv, h, at_(kd, c0), ld32,
-                                                                                           w, mir, ldm);
+        k_leaf_mult<true><<<(w + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(
+            dinv, h, at_(kd, c0), ld32, w, mir, ldm, next_stamp(2.0 * h * h * w, kSlotSolveLeaf));
       else
-        launch_narrow_leaf<true>(dinv, h, at_(kd, c0), ld32, w, mir, ldm, sms, s);
+        launch_narrow_leaf<true>(dinv, h, at_(kd, c0), ld32, w, mir, ldm, sms, s,
+                                 next_stamp(2.0 * h * h * w, kSlotSolveLeaf));
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
@@ -969,10 +1038,11 @@ struct MixedSolver::Impl {
       __nv_bfloat16* mir = mirrors ? am_at(r0, kd) : nullptr;
       prof.begin(m >= kWideLeaf ? "trsm leaf (right, wide)" : "trsm leaf (right)", 2.0 * h * h * m, s);
       if (m >= kWideLeaf)
-        k_leaf_mult<false><<<(m + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(dinv, h, at_(r0, kd),
-                                                                                            ld32, m, mir, ldm);
+        k_leaf_mult<false><<<(m + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(
+            dinv, h, at_(r0, kd), ld32, m, mir, ldm, next_stamp(2.0 * h * h * m, kSlotSolveLeaf));
       else
-        launch_narrow_leaf<false>(dinv, h, at_(r0, kd), ld32, m, mir, ldm, sms, s);
+        launch_narrow_leaf<false>(dinv, h, at_(r0, kd), ld32, m, mir, ldm, sms, s,
+                                  next_stamp(2.0 * h * h * m, kSlotSolveLeaf));
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "trsm leaf");
@@ -992,7 +1062,7 @@ struct MixedSolver::Impl {
       const size_t off = (size_t)(k0 / kLeaf) * kLeaf * kLeaf;
       prof.begin("LU leaf + inverses", 0, s);
       k_lu32_leaf_inv<<<1, 512, smem, s>>>(at_(k0, k0), ld32, sz, dl32.as<float>() + off, du32.as<float>() + off,
-                                           d_status());
+                                           d_status(), next_stamp(0, kSlotLuLeaf));
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "LU leaf");
@@ -1176,6 +1246,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     P.fork = false;
     P.nslots = 0;
     P.slot_work = 0;
+    P.slot_kind.clear();
     ck(stamps_reset(P.stamps.as<unsigned long long>(), P.slot_cap, s), "stamps");
     P.rlu(0, P.n3, s);  // direct launches in order, each timed
     used_slots = P.nslots;
@@ -1197,6 +1268,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       P.fork = P.mirrors && std::getenv("BEST_GPU_ONE_STREAM") == nullptr;
       P.nslots = 0;
       P.slot_work = 0;
+      P.slot_kind.clear();
       try {
         P.rlu(0, P.n3, cs);
       } catch (...) {
@@ -1244,9 +1316,15 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     std::vector<unsigned long long> h((size_t)2 * used_slots);
     ck(cudaMemcpy(h.data(), P.stamps.p, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stamps");
     double ns = 0;
+    int gemms = 0;
     for (int i = 0; i < used_slots; ++i)
-      if (h[2 * i + 1] >= h[2 * i]) ns += (double)(h[2 * i + 1] - h[2 * i]);
-    kt.add(used_slots, ns * 1e-6, used_work);
+      if (P.slot_kind[i] == kSlotGemm && h[2 * i + 1] >= h[2 * i]) {
+        ns += (double)(h[2 * i + 1] - h[2 * i]);
+        ++gemms;
+      }
+    kt.add(gemms, ns * 1e-6, used_work);
+    const std::string tl = timeline_note(h, P.slot_kind, used_slots);
+    if (!tl.empty()) P.host_note += "; " + tl;
   }
   if (st != 0) {
     ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
