@@ -933,6 +933,19 @@ struct MixedSolver::Impl {
   std::vector<unsigned char> slot_kind;  // kSlot* of each slot, in launch order
   int graph_slots = 0;
   double graph_work = 0;
+  // the solve's buffers for q right-hand sides per pass (GMRES vectors, FP32 preconditioner
+  // vectors, split-solve scratch, mat-vec partials, dot partials)
+  void reserve_solve(int q, cudaStream_t s) {
+    const size_t blk = (size_t)n3 * q;
+    const bool fresh = !trsv.p || trsv.bytes < trsv_scratch_bytes(n3);
+    trsv.ensure(trsv_scratch_bytes(n3), "solve scratch");
+    if (fresh) ck(cudaMemsetAsync(trsv.p, 0, trsv.bytes, s), "solve scratch clear");  // flags start at 0
+    vecs.ensure(blk * (4 + (krylov + 1) + krylov) * sizeof(double), "GMRES vectors");
+    zf.ensure(blk * sizeof(float), "preconditioner vectors (FP32)");
+    part.ensure((size_t)32 * 16 * n3 * sizeof(double), "residual partials");
+    pdots.ensure((size_t)std::min(4 * sms, (n3 + 255) / 256) * 32 * 16 * sizeof(double), "dot partials");
+    dots.ensure(32 * 16 * sizeof(double), "dots");
+  }
   unsigned long long* next_stamp(double flops, unsigned char kind = kSlotGemm) {
     if (nslots >= slot_cap) return nullptr;
     if (kind == kSlotGemm) slot_work += flops;
@@ -1087,6 +1100,7 @@ struct MixedSolver::Impl {
 
   // Y (n3 x q, ldy) = beta Y + alpha GR X
   void matvec(const double* X, long ldx, int q, double* Y, long ldy, double alpha, double beta, cudaStream_t s) {
+    // 128 threads per block, two rows each (larger blocks measured slower on B200)
     const int rb = (n3 + 255) / 256;
     const int splits = std::max(1, std::min(32, (4 * sms * 8 + rb - 1) / rb));
     const int per = (n3 + splits - 1) / splits;
@@ -1168,6 +1182,11 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   P.tol = std::max(1e-15, std::min(0.1 * eps, 1e-12));
   // (+256 bytes: the solve leaves read whole 16-byte groups at the end of the last column)
   P.lu32.ensure((size_t)P.ld32 * P.n3 * sizeof(float) + 256, "FP32 copy of GR");
+  ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
+  ck(launch_assemble_fast(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
+  ck(cudaEventRecord(ev_assembled, s), "event");
+  // everything else is allocated while the GPU assembles: the factorisation's buffers and the
+  // solve's scratch (for up to 16 right-hand sides per pass)
   P.dl32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (L)");
   P.du32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (U)");
   // BF16 mirrors when they fit with 4 GB to spare, else operand copies per product
@@ -1224,10 +1243,8 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     ck(cudaFuncSetAttribute(k_apply_inv_right<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
     attrs = true;
   }
-  ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");
+  P.reserve_solve(16, s);
   ms_alloc = ms_since(t_begin);
-  ck(launch_assemble_fast(m, 0, m.n, 0, m.n, gr64, ld, d, P.lu32.as<float>(), P.ld32, s), "assembly");
-  ck(cudaEventRecord(ev_assembled, s), "event");
   // GEMM stamp slots: far more than the recursion's launches (about 8 per 128-row leaf with the
   // mirrors; the blocked products without them add a few per leaf)
   const int cap = 64 * ((P.n3 + kLeaf - 1) / kLeaf) + 4096;
