@@ -168,22 +168,35 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::kThreads)
     }
   }
   cp_async_wait<0>();
-  // epilogue: C -= acc; fragment element (row lane/4, cols 2*(lane%4) + {0,1})
+  __syncthreads();
+  // epilogue through shared memory (the pipeline's buffers, free now): the tile column-major
+  // (stride BM + 2; fragment element (row lane/4, cols 2*(lane%4) + {0,1})), then C -= tile with
+  // each column read and written by consecutive threads in 16-byte pieces
+  double* ct = smem;
+  constexpr int kCs = BM + 2;
+  static_assert((size_t)BN * kCs <= (size_t)STAGES * (Cfg::kAStage + Cfg::kBStage), "C tile must fit");
 #pragma unroll
-  for (int i = 0; i < Cfg::kFm; ++i) {
-    const int gr = m0 + wm0 + i * 8 + (lane >> 2);
-    if (gr >= m) continue;
+  for (int i = 0; i < Cfg::kFm; ++i)
 #pragma unroll
     for (int j = 0; j < Cfg::kFn; ++j) {
-      const int gc = n0 + wn0 + j * 8 + 2 * (lane & 3);
-      if (gc < n) {
-        double* p = C + (size_t)gc * ldc + gr;
-        *p = *p - acc[i][j][0];
-      }
-      if (gc + 1 < n) {
-        double* p = C + (size_t)(gc + 1) * ldc + gr;
-        *p = *p - acc[i][j][1];
-      }
+      const int r = wm0 + i * 8 + (lane >> 2), c = wn0 + j * 8 + 2 * (lane & 3);
+      ct[c * kCs + r] = acc[i][j][0];
+      ct[(c + 1) * kCs + r] = acc[i][j][1];
+    }
+  __syncthreads();
+  const bool full = m0 + BM <= m && n0 + BN <= n && (ldc % 2) == 0 && ((uintptr_t)C & 15) == 0;
+  for (int e = tid; e < BN * (BM / 2); e += Cfg::kThreads) {
+    const int c = e / (BM / 2), r = (e % (BM / 2)) * 2;
+    const int gr = m0 + r, gc = n0 + c;
+    if (full) {
+      double2* p = reinterpret_cast<double2*>(C + (size_t)gc * ldc + gr);
+      double2 v = *p;
+      v.x = v.x - ct[c * kCs + r];
+      v.y = v.y - ct[c * kCs + r + 1];
+      *p = v;
+    } else if (gc < n) {
+      if (gr < m) C[(size_t)gc * ldc + gr] = C[(size_t)gc * ldc + gr] - ct[c * kCs + r];
+      if (gr + 1 < m) C[(size_t)gc * ldc + gr + 1] = C[(size_t)gc * ldc + gr + 1] - ct[c * kCs + r + 1];
     }
   }
 }
@@ -227,7 +240,7 @@ cudaError_t run_shape(int shape, const GemmBatch& gb, cudaStream_t s) {
   switch (shape) {
     case kShapeBig: return run_gemm<128, 128, 16, 32, 64, 4>(gb, s);
     case kShapeSmall: return run_gemm<64, 64, 16, 32, 32, 4>(gb, s);
-    case kShapeTall: return run_gemm<128, 64, 16, 32, 32, 4>(gb, s);
+    case kShapeTall: return run_gemm<128, 64, 16, 32, 32, 3>(gb, s);
     default: return run_gemm<64, 128, 16, 32, 64, 4>(gb, s);
   }
 }
@@ -963,7 +976,7 @@ cudaError_t lu_prepare() {
   cudaError_t e;
   if ((e = gemm_attr<128, 128, 16, 32, 64, 4>()) != cudaSuccess) return e;
   if ((e = gemm_attr<64, 64, 16, 32, 32, 4>()) != cudaSuccess) return e;
-  if ((e = gemm_attr<128, 64, 16, 32, 32, 4>()) != cudaSuccess) return e;
+  if ((e = gemm_attr<128, 64, 16, 32, 32, 3>()) != cudaSuccess) return e;
   if ((e = gemm_attr<64, 128, 16, 32, 64, 4>()) != cudaSuccess) return e;
   return leaf_attr();
 }
