@@ -154,17 +154,28 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::kThreads)
     }
     const double* as = As + (kt % STAGES) * Cfg::kAStage;
     const double* bs = Bs + (kt % STAGES) * Cfg::kBStage;
+    // fragments double-buffered in registers: the next k4 step's loads are issued before this
+    // step's DMMAs (the accumulation order over k is the same for every tile shape)
+    double af[2][Cfg::kFm], bf[2][Cfg::kFn];
+#pragma unroll
+    for (int i = 0; i < Cfg::kFm; ++i) af[0][i] = as[(lane & 3) * Cfg::kAStride + wm0 + i * 8 + (lane >> 2)];
+#pragma unroll
+    for (int j = 0; j < Cfg::kFn; ++j) bf[0][j] = bs[(wn0 + j * 8 + (lane >> 2)) * Cfg::kBStride + (lane & 3)];
 #pragma unroll
     for (int k4 = 0; k4 < BK; k4 += 4) {
-      double af[Cfg::kFm], bf[Cfg::kFn];
+      const int cur = (k4 / 4) & 1, nxt = cur ^ 1;
+      if (k4 + 4 < BK) {
 #pragma unroll
-      for (int i = 0; i < Cfg::kFm; ++i) af[i] = as[(k4 + (lane & 3)) * Cfg::kAStride + wm0 + i * 8 + (lane >> 2)];
+        for (int i = 0; i < Cfg::kFm; ++i)
+          af[nxt][i] = as[(k4 + 4 + (lane & 3)) * Cfg::kAStride + wm0 + i * 8 + (lane >> 2)];
 #pragma unroll
-      for (int j = 0; j < Cfg::kFn; ++j) bf[j] = bs[(wn0 + j * 8 + (lane >> 2)) * Cfg::kBStride + k4 + (lane & 3)];
+        for (int j = 0; j < Cfg::kFn; ++j)
+          bf[nxt][j] = bs[(wn0 + j * 8 + (lane >> 2)) * Cfg::kBStride + k4 + 4 + (lane & 3)];
+      }
 #pragma unroll
       for (int i = 0; i < Cfg::kFm; ++i)
 #pragma unroll
-        for (int j = 0; j < Cfg::kFn; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        for (int j = 0; j < Cfg::kFn; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[cur][i], bf[cur][j]);
     }
   }
   cp_async_wait<0>();
@@ -240,7 +251,7 @@ cudaError_t run_shape(int shape, const GemmBatch& gb, cudaStream_t s) {
   switch (shape) {
     case kShapeBig: return run_gemm<128, 128, 16, 32, 64, 4>(gb, s);
     case kShapeSmall: return run_gemm<64, 64, 16, 32, 32, 4>(gb, s);
-    case kShapeTall: return run_gemm<128, 64, 16, 32, 32, 3>(gb, s);
+    case kShapeTall: return run_gemm<128, 64, 32, 32, 32, 2>(gb, s);
     default: return run_gemm<64, 128, 16, 32, 64, 4>(gb, s);
   }
 }
@@ -976,7 +987,7 @@ cudaError_t lu_prepare() {
   cudaError_t e;
   if ((e = gemm_attr<128, 128, 16, 32, 64, 4>()) != cudaSuccess) return e;
   if ((e = gemm_attr<64, 64, 16, 32, 32, 4>()) != cudaSuccess) return e;
-  if ((e = gemm_attr<128, 64, 16, 32, 32, 3>()) != cudaSuccess) return e;
+  if ((e = gemm_attr<128, 64, 32, 32, 32, 2>()) != cudaSuccess) return e;
   if ((e = gemm_attr<64, 128, 16, 32, 64, 4>()) != cudaSuccess) return e;
   return leaf_attr();
 }
