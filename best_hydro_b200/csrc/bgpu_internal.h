@@ -144,15 +144,10 @@ size_t trsv_scratch_bytes(int n);
 // X (n x nrhs, ldx) := A^{-1} X given the LU factors and perm, dgetrs('N') semantics.
 cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* X, long ldx, int nrhs, void* scratch,
                     int* d_status, cudaStream_t s);
-// Y := U^-1 L^-1 Y with FP32 factors of an unpivoted LU, FP64 right-hand sides (in place).
-cudaError_t trsv_lu32(const float* LU, long lda, int n, double* Y, long ldy, int nrhs, void* scratch, int* d_status,
-                      cudaStream_t s);
 // Inverses of the 128 x 128 diagonal blocks of LU factors (DL: unit-lower parts, DU: upper parts),
 // each diag_inverse_elems(n) elements; and the solves that use them.
 size_t diag_inverse_elems(int n);
 cudaError_t diag_inverses64(const double* LU, long lda, int n, double* DL, double* DU, cudaStream_t s);
-// (FP32: nb blocks starting at block b0)
-cudaError_t diag_inverses32(const float* LU, long lda, int n, int b0, int nb, float* DL, float* DU, cudaStream_t s);
 cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
                         double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s);
 // dgetrs('T'): X := A^-T X with the same factors (the adjoint solve).

@@ -734,20 +734,6 @@ cudaError_t diag_inverses64(const double* LU, long lda, int n, double* DL, doubl
   return cudaGetLastError();
 }
 
-cudaError_t diag_inverses32(const float* LU, long lda, int n, int b0, int nb, float* DL, float* DU, cudaStream_t s) {
-  if (n <= 0 || nb <= 0) return cudaSuccess;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_diag_inverses<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kDiagInvSmem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  k_diag_inverses<float, float><<<nb, kIb, kDiagInvSmem, s>>>(LU, lda, n, b0, DL, DU);
-  BGPU_COUNT_LAUNCH();
-  return cudaGetLastError();
-}
-
 // dgetrs('N') with FP64 factors and their diagonal-block inverses: X := A^-1 X (in place).
 cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
                         double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s) {
@@ -772,40 +758,6 @@ cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const floa
                           int nrhs, void* scratch, int* d_status, cudaStream_t s) {
   if (n <= 0 || nrhs <= 0) return cudaSuccess;
   return trsv_inv_pair<float, float, float>(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
-}
-
-// Y := U^-1 L^-1 Y in place with FP32 factors of an unpivoted LU (the mixed-precision
-// preconditioner); Y is FP64 and the sums are accumulated in FP64.
-cudaError_t trsv_lu32(const float* LU, long lda, int n, double* Y, long ldy, int nrhs, void* scratch, int* d_status,
-                      cudaStream_t s) {
-  if (n <= 0 || nrhs <= 0) return cudaSuccess;
-  if (nrhs > kMaxRhs) return cudaErrorInvalidValue;
-  unsigned char* base = static_cast<unsigned char*>(scratch);
-  unsigned* ticket = reinterpret_cast<unsigned*>(base);
-  unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int nblk = (n + kBs - 1) / kBs;
-  const int grid = std::min(nblk, sms * 2);
-  g_epoch += 2;
-  if (g_epoch == 0) g_epoch = 2;
-  cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
-  if (e != cudaSuccess) return e;
-  BGPU_COUNT_LAUNCH();
-  if (nrhs <= 8)
-    k_trsv<float, true, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
-  else
-    k_trsv<float, true, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
-  BGPU_COUNT_LAUNCH();
-  if (nrhs <= 8)
-    k_trsv<float, false, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1, d_status);
-  else
-    k_trsv<float, false, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1,
-                                                        d_status);
-  return cudaGetLastError();
 }
 
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s) {
