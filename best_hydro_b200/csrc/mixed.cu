@@ -436,16 +436,18 @@ __global__ void __launch_bounds__(256, 1) k_leaf_mult(const float* __restrict__ 
     tdst = Bs;
   }
   {
+    // lanes along x: the transposed stores of a warp hit 32 consecutive words (no bank conflicts)
     float4 v[16];
+    const int x = tid & 127;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int e = tid + 256 * q, k4 = (e & 31) * 4, x = e >> 5;
+      const int k4 = ((tid >> 7) + 2 * q) * 4;
       v[q] = (x < tx_lim && k4 < tk) ? *reinterpret_cast<const float4*>(&tsrc[(size_t)x * tld + k4])
                                      : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int e = tid + 256 * q, k4 = (e & 31) * 4, x = e >> 5;
+      const int k4 = ((tid >> 7) + 2 * q) * 4;
       tdst[(k4 + 0) * kLm + x] = k4 + 0 < tk ? v[q].x : 0.f;
       tdst[(k4 + 1) * kLm + x] = k4 + 1 < tk ? v[q].y : 0.f;
       tdst[(k4 + 2) * kLm + x] = k4 + 2 < tk ? v[q].z : 0.f;
@@ -555,16 +557,18 @@ __global__ void __launch_bounds__(256) k_apply_inv_left(const float* __restrict_
     cp16(&li[k * kLdI + r4], &Dinv[(size_t)k * 128 + r4], 16);
   }
   {
-    float4 v[NB / 8];  // B (k, c0 + cc), k contiguous in memory: float4 loads, transposed into bs
+    // B (k, c0 + cc), k contiguous in memory: float4 loads, transposed into bs with the lanes along
+    // cc (no bank conflicts on the stores)
+    float4 v[NB / 8];
 #pragma unroll
     for (int q = 0; q < NB / 8; ++q) {
-      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      const int e = tid + 256 * q, cc = e % NB, k4 = (e / NB) * 4;
       v[q] = (cc < nc && k4 < h) ? *reinterpret_cast<const float4*>(&B[(size_t)(c0 + cc) * ldb + k4])
                                  : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 #pragma unroll
     for (int q = 0; q < NB / 8; ++q) {
-      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      const int e = tid + 256 * q, cc = e % NB, k4 = (e / NB) * 4;
       bs[(k4 + 0) * ldb_s + cc] = k4 + 0 < h ? v[q].x : 0.f;
       bs[(k4 + 1) * ldb_s + cc] = k4 + 1 < h ? v[q].y : 0.f;
       bs[(k4 + 2) * ldb_s + cc] = k4 + 2 < h ? v[q].z : 0.f;
@@ -625,15 +629,18 @@ __global__ void __launch_bounds__(256) k_apply_inv_right(const float* __restrict
     cp16(&bs[k * ldb_s + rr4], valid ? (const void*)&B[(size_t)k * ldb + r0 + rr4] : (const void*)B, valid);
   }
   {
-    float4 v[16];  // Dinv (k, cc) at Dinv[cc * 128 + k]: float4 loads along k, transposed into us
+    // Dinv (k, cc) at Dinv[cc * 128 + k]: float4 loads along k, transposed into us with the lanes
+    // along cc (no bank conflicts on the stores)
+    float4 v[16];
+    const int cc = tid & 127;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      const int k4 = ((tid >> 7) + 2 * q) * 4;
       v[q] = *reinterpret_cast<const float4*>(&Dinv[(size_t)cc * 128 + k4]);
     }
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int e = tid + 256 * q, k4 = (e & 31) * 4, cc = e >> 5;
+      const int k4 = ((tid >> 7) + 2 * q) * 4;
       us[(k4 + 0) * kLdI + cc] = v[q].x;
       us[(k4 + 1) * kLdI + cc] = v[q].y;
       us[(k4 + 2) * kLdI + cc] = v[q].z;
