@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 METRIC = "s per BEST solve (assemble+LU+6 RHS), mixed vs FP64 GPU at rel err<=1e-8"
 
 WORKLOADS = {
-    # BASELINE configuration of the metric's target: star body at geodesic frequency 32 (N = 20,480)
+    # the headline workload: star body at geodesic frequency 32 (N = 20,480)
     "star_f32": dict(desc="star-shaped body r=25A(1+sum_{l=2..8} a_lm Y_lm), a_lm~N(0,(0.08/l)^2) seed 1, "
                           "geodesic f=32", N=20480, iarea=0, gen=("star", 32)),
     "star_f45": dict(desc="star-shaped body as star_f32, geodesic f=45 (the FP32 factor fits beside the FP64 GR)",
@@ -44,8 +44,8 @@ WORKLOADS = {
     "ellipsoid_f16": dict(desc="ellipsoid 30/20/12 A, geodesic f=16, normal jitter U(+-2%) seed 0", N=5120,
                           iarea=1, gen=("ellipsoid", 16)),
     "icosphere_l3": dict(desc="icosphere level 3, R=20 A", N=1280, iarea=1, gen=("icosphere", 3)),
-    # BASELINE batching configuration: the ellipsoid at eight geodesic frequencies, solved as one series
-    # BASELINE differentiation configuration: gradients of the ellipsoid at frequency 16 (N = 5,120)
+    # the batching workload: the ellipsoid at eight geodesic frequencies, solved as one series
+    # the differentiation workload: gradients of the ellipsoid at frequency 16 (N = 5,120)
     "ellipsoid_adjoint": dict(desc="ellipsoid 30/20/12 A, geodesic f=16, normal jitter U(+-2%) seed 0: adjoint "
                                    "gradients w.r.t. all 3 x 2562 vertex coordinates", N=5120, iarea=1,
                               gen=("adjoint", 16)),

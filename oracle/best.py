@@ -1,6 +1,6 @@
 """ORACLE (test infrastructure only): a CPU restatement of BEST's dense path.
 
-This module is the checker for the CUDA path.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+This module is the oracle for the CUDA path.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
 CPU-baseline leg of ``bench.py`` may import it; the product never does.
 
 It restates, in numpy, the reference's driver arithmetic around the hot path, and calls the C

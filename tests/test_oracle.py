@@ -118,7 +118,7 @@ def test_self_blocks_differ_from_glibc_only_where_glibc_misrounds():
 
 
 def test_pair_blocks_long_double():
-    """The long-double pair blocks (the reference value the mixed assembly is judged against) agree
+    """The long-double pair blocks (the reference value the mixed assembly is compared with) agree
     with the FP64 restatement within the FP64 formula's own error: 1e-10 of the row scale."""
     tri, ta, tv = golden_mesh("2eu7_02562")
     s = ob.setup(tri, 1, ta)
