@@ -250,6 +250,24 @@ def relerr(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
+def max_over_ranks(v, dist=None, device="cpu"):
+    """The largest v over the ranks of the default process group (v itself without one): every rank
+    times its own replica, and the job is as fast as its slowest rank."""
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seconds(ms_per_solve, world):
+    """Whole-job seconds per solve when each of `world` ranks solves its own replica: the slowest
+    rank's time per solve divided by the number of solves done at once (aggregate throughput)."""
+    return ms_per_solve / 1e3 / world
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import best_hydro_b200 as bh
@@ -262,13 +280,6 @@ def run_ours(args, rank, world, local_rank):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     w = WORKLOADS[args.workload]
     tri, ta, tv = make_mesh(args.workload)
@@ -323,7 +334,7 @@ def run_ours(args, rank, world, local_rank):
         clk = sampler.stop() if sampler else None
         step_ms = [a.elapsed_time(c) for a, c in ev]
         kst = bh.kernel_stats(stats_kernel, enable=0) if stats_kernel is not None else None
-        ms = max_over_ranks(sum(step_ms) / len(step_ms))
+        ms = max_over_ranks(sum(step_ms) / len(step_ms), dist, dev)
         st_ms = {k: round(float(np.mean([d[k] for d in stages])), 3) for k in ("assemble", "factor", "solve")}
         return dict(ms=ms, step_ms=step_ms, launches=launches, clocks=clk, kstats=kst, stages_ms=st_ms,
                     refine_iters=stages[-1]["refine_iters"], relres=stages[-1]["relres"])
@@ -365,7 +376,7 @@ def run_ours(args, rank, world, local_rank):
         t4 = time.perf_counter()
         e2e.append(t4 - t0)
         phases.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
-    e2e_s = max_over_ranks(float(np.median(e2e))) if e2e else float("nan")
+    e2e_s = max_over_ranks(float(np.median(e2e)), dist, dev) if e2e else float("nan")
     e2e_phases = ({k: round(1e3 * float(np.median([p[i] for p in phases])), 2)
                    for i, k in enumerate(("create", "incenters_deflation", "build", "solve"))} if phases else None)
     host_notes = [ln for ln in bh.log_lines() if "host side" in ln][-2:]
@@ -404,7 +415,7 @@ def run_ours(args, rank, world, local_rank):
                         "refine_iterations": H["refine_iters"], "relres": H["relres"]}
         line = {
             "metric": METRIC,
-            "value": H["ms"] / 1e3 / world, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "value": replica_seconds(H["ms"], world), "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": H["ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if head == "fp64" else "bf16 LU (f32 accumulate) + f64 refinement", "data": "synthetic",
             "config": {"workload": args.workload, "N": n, "order": n3, "desc": w["desc"], "precision": head,
@@ -415,7 +426,7 @@ def run_ours(args, rank, world, local_rank):
                        "e2e_host_notes": host_notes},
             "roofline": roof,
             "clocks": H["clocks"],
-            "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": replica_seconds(1e3 * e2e_s, world), "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": H["launches"],
             "fp64_path": None if F is None else {"value": F["ms"] / 1e3, "unit": "s", "steps": len(F["step_ms"]),
                                                  "warmup": 1, "stages_ms": F["stages_ms"],
