@@ -172,8 +172,8 @@ __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __re
         }
       } else {
         // 1/sqrt as rsqrt (q = a rsqrt(a)); the denominators of hy and hxy (exact negatives of each
-        // other in triangleint.f) and of hx as quadratics in y with per-pair coefficients, one
-        // reciprocal shared by hy and hxy; 1/s21 once per source triangle
+        // other in triangleint.f) and of hx as quadratics in y with per-pair coefficients; one
+        // reciprocal per quadrature point for all three quotients; 1/s21 once per source triangle
         const double inv_s21 = D[8];
         const double cy0 = d211c * d211c - d1c1c * d2121;
         const double cy1 = 2.0 * (d211c * d2131 - d1c31 * d2121);
@@ -189,12 +189,17 @@ __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __re
           const double a4 = d3c3c + y * (y * d3232 - 2.0 * d3c32);
           const double r1 = rsqrt(a1), r2 = rsqrt(a2);
           const double q1 = a1 * r1, q2 = a2 * r2;
-          const double hv = log((d212c + d2132 * y + s21 * q2) / (d211c + d2131 * y + s21 * q1)) * inv_s21;
-          const double ry = 1.0 / (cy0 + y * (cy1 + y * cy2));
+          // the three quotients (log argument, hy/hxy, hx) from one reciprocal of the product of
+          // their denominators
+          const double den = d211c + d2131 * y + s21 * q1;
+          const double dy = cy0 + y * (cy1 + y * cy2), dx = cx0 + y * (cx1 - y * cy2);
+          const double dyx = dy * dx;
+          const double r = 1.0 / (dyx * den);
+          const double ry = dx * den * r, rx = dy * den * r, rden = dyx * r;
+          const double hv = log((d212c + d2132 * y + s21 * q2) * rden) * inv_s21;
           const double hyv = ((d211c + y * d2131) * r1 - (y * d2132 + d212c) * r2) * ry;
           const double hxyv = -(q1 + (y * d211c - d2c1c - 2.0 * y * d1c31 - y * d2131 - y * y * d3231) * r2) * ry;
-          const double hxv = ((-d1c31 - y * d2131) * rsqrt(a3) + (d3c31 - y * d3231) * rsqrt(a4)) /
-                             (cx0 + y * (cx1 - y * cy2));
+          const double hxv = ((-d1c31 - y * d2131) * rsqrt(a3) + (d3c31 - y * d3231) * rsqrt(a4)) * rx;
           const double wy = w * y, wyy = wy * y;
           t0 = t0 + w * hv;
           s0 = s0 + w * hyv;
