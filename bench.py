@@ -13,8 +13,9 @@ way, and `accuracy` the relative differences of D_t, D_r and [eta] (11-RHS solve
 included).  With N GPUs (torchrun), every rank
 solves its own replica: the path has no exchange step, so there is no collective in it.
 `--impl reference` times the reference's own CPU implementation (its kernel.cpp assembly, OpenMP,
-plus the LAPACK dgetrf/dgetrs BEST calls) on bounded samples of the same workload, scaled to a full
-solve.
+the deflation, and the LAPACK dgetrf/dgetrs BEST calls) on complete solves of the same workload: as
+many as fit in --ref-budget-s seconds, at least one; `steps` is the number run.  The GPU arm's
+`cpu_baseline` is one such complete solve, whose tensors are the oracle of `accuracy`.
 """
 from __future__ import annotations
 
@@ -188,25 +189,107 @@ def cpu_reference_sample(tri, iarea, truearea, rows=512, n_lu=12288, seed=0):
     return asm + fac + sv, parts
 
 
+def host_bytes_available():
+    try:
+        import psutil
+        return int(psutil.virtual_memory().available)
+    except Exception:
+        return None
+
+
+def cpu_reference_solve(tri, iarea, truearea):
+    """One complete BEST solve on the host cores with the reference's own code: the reference's
+    kernel.cpp assembly of every entry of GR (oracle/_ref, OpenMP over source columns; the oracle's C
+    restatement, equal to it bit for bit, when _ref is absent), BEST's deflation (best.f:406-425),
+    LAPACK dgetrf (best.f:444) and dgetrs for the 6 flows (besolve.f90:133; OpenBLAS via scipy, all
+    host threads).  Timed part by part with a monotonic clock; then, untimed, the 5 strain flows and
+    DIFCO/VISCO for the tensors.  Returns (seconds, parts, tensors)."""
+    import ctypes
+
+    from oracle import best as ob
+    threads = os.cpu_count() or 1
+    s = ob.setup(tri, iarea, truearea)
+    n, n3 = s.n, 3 * s.n
+    R = ob.ref_lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    t0 = time.perf_counter()
+    if R is not None:
+        v1, v2, v3 = s.colmajor()
+        R.ref_create(n, v1.ctypes.data_as(dp), v2.ctypes.data_as(dp), v3.ctypes.data_as(dp),
+                     s.area.ctypes.data_as(dp), s.afac, 1.0)
+        gr = np.empty((n3, n3), dtype=np.float64, order="F")
+        R.ref_fill(0, n, 0, n, gr.ctypes.data_as(dp), n3)
+        x = np.empty(n3)
+        R.ref_incenters(x.ctypes.data_as(dp))
+        dm = R.ref_diag_mean()
+        R.ref_destroy()
+    else:
+        gr, x, self9 = ob.assemble(s)
+        dm = ob.diag_mean(self9, n)
+    t1 = time.perf_counter()
+    xmu, gdef = ob.deflation_vectors(s, dm)
+    ob.deflate(s, gr, xmu, gdef)
+    t2 = time.perf_counter()
+    lu, ipiv, info = ob.getrf(gr)
+    t3 = time.perf_counter()
+    B6, _ = ob.getrs(lu, ipiv, ob.rhs6(x, n))
+    t4 = time.perf_counter()
+    V5, _ = ob.getrs(lu, ipiv, ob.strain5(x, n))
+    del lu, gr
+    t = ob.difco(B6, x, s.area, n)
+    chip, _ = ob.visco(V5, B6, x, s.area, n, 0)
+    rep = ob.report(t, chip)
+    parts = dict(assembly_s=t1 - t0, deflation_s=t2 - t1, lu_s=t3 - t2, solve_s=t4 - t3, threads=threads,
+                 kind="reference" if R is not None else "port", info=int(info),
+                 sample=f"complete solve at N={n} (order {n3}): {'the reference kernel.cpp' if R is not None else 'the C port'}"
+                        f" assembly of all {n * n} pairs (OpenMP, {threads} threads), deflation, dgetrf + dgetrs "
+                        f"(OpenBLAS via scipy, {threads} threads) on that matrix; nothing scaled")
+    tens = dict(D_t=rep["DTRANS"], D_r=rep["DR"], chiprime=chip, Dtt=t["Dtt"], Drr=t["Drr"], Dtr=t["Dtr"],
+                urc=t["urc"], udr=t["udr"])
+    return t4 - t0, parts, tens
+
+
+def full_solve_fits(n):
+    """Whether a complete host solve fits in host memory: GR is 72 N^2 bytes, plus room to spare."""
+    avail = host_bytes_available()
+    return avail is None or avail > 72.0 * n * n * 1.15 + 4e9
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
     w = WORKLOADS[args.workload]
     tri, ta, tv = make_mesh(args.workload)
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    # warm-up: small bounded samples (thread pools, library loading), not complete solves
     for _ in range(args.warmup):
-        cpu_reference_sample(tri, w["iarea"], ta, rows=64, n_lu=2048)
+        cpu_reference_sample(tri, w["iarea"], ta, rows=16, n_lu=1024)
     vals, parts = [], None
-    for k in range(args.steps):
-        v, parts = cpu_reference_sample(tri, w["iarea"], ta, seed=k)
-        vals.append(v)
-    v = float(np.median(vals))
+    if full_solve_fits(w["N"]):
+        t_start = time.perf_counter()
+        while len(vals) < max(1, args.steps):
+            v, parts, _ = cpu_reference_solve(tri, w["iarea"], ta)
+            vals.append(v)
+            if time.perf_counter() - t_start + v > args.ref_budget_s:
+                break
+        v = float(np.median(vals))
+        sample = parts["sample"]
+    else:
+        v, parts = cpu_reference_sample(tri, w["iarea"], ta)
+        vals = [v]
+        sample = ("host memory too small for a complete solve (72 N^2 bytes); " + parts["sample"])
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "n_gpus": args.gpus, "steps": len(vals), "steps_requested": args.steps, "warmup": args.warmup,
+        "ms_per_step": v * 1e3, "step_s": vals,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "N": w["N"], "order": 3 * w["N"], "desc": w["desc"]},
+        "config": {"workload": args.workload, "N": w["N"], "order": 3 * w["N"], "desc": w["desc"],
+                   "warmup_kind": "bounded samples (16 assembly rows, order-1024 LU), not complete solves",
+                   "budget_s": args.ref_budget_s},
         "cpu_baseline": {"value": v, "unit": "s", "cores": parts["threads"], "kind": parts["kind"],
-                         "sample": parts["sample"], "parts_s": {k: parts[k] for k in ("assembly_s", "lu_s", "solve_s")}},
+                         "sample": sample,
+                         "parts_s": {k: parts[k] for k in ("assembly_s", "deflation_s", "lu_s", "solve_s") if k in parts}},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -242,7 +325,25 @@ def tensors_of(solver, x, st, bh):
     t = bh.difco(x, st.area, B[:, :6])
     chip, _ = bh.visco(x, st.area, B[:, 6:], B[:, :6])
     tr = bh.traces(t)
-    return dict(D_t=tr["DTRANS"], D_r=tr["DR"], chiprime=chip, Dtt=t["Dtt"], Drr=t["Drr"])
+    return dict(D_t=tr["DTRANS"], D_r=tr["DR"], chiprime=chip, Dtt=t["Dtt"], Drr=t["Drr"], Dtr=t["Dtr"],
+                urc=t["urc"], udr=t["udr"])
+
+
+def tensor_errors(got, want):
+    """Relative differences of BEST's results: D_t, D_r traces and CHI' ([eta] is proportional); the
+    full D_tt, D_rr tensors; D_tr relative to sqrt(|D_tt| |D_rr|); the centres of resistance and
+    diffusion relative to the body's size (the largest of the two centres' and 1 A)."""
+    out = {"D_t": relerr(got["D_t"], want["D_t"]), "D_r": relerr(got["D_r"], want["D_r"]),
+           "eta": relerr(got["chiprime"], want["chiprime"]), "Dtt_tensor": relerr(got["Dtt"], want["Dtt"]),
+           "Drr_tensor": relerr(got["Drr"], want["Drr"])}
+    if "Dtr" in got and "Dtr" in want:
+        sc = np.sqrt(np.max(np.abs(want["Dtt"])) * np.max(np.abs(want["Drr"])))
+        out["Dtr_tensor"] = float(np.max(np.abs(np.asarray(got["Dtr"]) - want["Dtr"])) / sc)
+    for k in ("urc", "udr"):
+        if k in got and k in want:
+            sc = max(1.0, float(np.max(np.abs(want[k]))))
+            out[k] = float(np.max(np.abs(np.asarray(got[k]) - want[k])) / sc)
+    return out
 
 
 def relerr(a, b):
@@ -381,11 +482,17 @@ def run_ours(args, rank, world, local_rank):
                    for i, k in enumerate(("create", "incenters_deflation", "build", "solve"))} if phases else None)
     host_notes = [ln for ln in bh.log_lines() if "host side" in ln][-2:]
 
-    cpu = None
+    cpu = cpu_tens = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, parts = cpu_reference_sample(tri, w["iarea"], ta)
-        cpu = {"value": v, "unit": "s", "cores": parts["threads"], "kind": parts["kind"], "sample": parts["sample"],
-               "parts_s": {k: parts[k] for k in ("assembly_s", "lu_s", "solve_s")}}
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        if full_solve_fits(n):
+            v, parts, cpu_tens = cpu_reference_solve(tri, w["iarea"], ta)
+            sample = parts["sample"]
+        else:
+            v, parts = cpu_reference_sample(tri, w["iarea"], ta)
+            sample = "host memory too small for a complete solve (72 N^2 bytes); " + parts["sample"]
+        cpu = {"value": v, "unit": "s", "cores": parts["threads"], "kind": parts["kind"], "sample": sample,
+               "parts_s": {k: parts[k] for k in ("assembly_s", "deflation_s", "lu_s", "solve_s") if k in parts}}
 
     if rank == 0:
         gl, gms, gflop = H["kstats"]
@@ -406,13 +513,18 @@ def run_ours(args, rank, world, local_rank):
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)"}
         roof.update(launches_per_step=gl / max(args.steps, 1), share_of_step=gms / max(sum(H["step_ms"]), 1e-9))
         accuracy = None
-        if acc_fp64 is not None:
-            accuracy = {"vs": "plain FP64 GPU path (partial-pivoting LU), same mesh, 11 RHS",
-                        "D_t": relerr(acc_head["D_t"], acc_fp64["D_t"]), "D_r": relerr(acc_head["D_r"], acc_fp64["D_r"]),
-                        "eta": relerr(acc_head["chiprime"], acc_fp64["chiprime"]),
-                        "Dtt_tensor": relerr(acc_head["Dtt"], acc_fp64["Dtt"]),
-                        "Drr_tensor": relerr(acc_head["Drr"], acc_fp64["Drr"]), "bar": 1e-8,
-                        "refine_iterations": H["refine_iters"], "relres": H["relres"]}
+        if acc_fp64 is not None or cpu_tens is not None:
+            accuracy = {"refine_iterations": H["refine_iters"], "relres": H["relres"]}
+            if cpu_tens is not None:
+                accuracy["vs"] = ("the reference's CPU solve at this size (kernel.cpp assembly + LAPACK dgetrf/"
+                                  "dgetrs, DIFCO/VISCO; cpu_baseline), 11 RHS")
+                accuracy[head] = tensor_errors(acc_head, cpu_tens)
+                accuracy[head]["bar"] = 1e-8 if head == "mixed" else 1e-10
+                if acc_fp64 is not None:
+                    accuracy["fp64"] = tensor_errors(acc_fp64, cpu_tens)
+                    accuracy["fp64"]["bar"] = 1e-10
+            if acc_fp64 is not None:
+                accuracy["mixed_vs_fp64_gpu"] = tensor_errors(acc_head, acc_fp64)
         line = {
             "metric": METRIC,
             "value": replica_seconds(H["ms"], world), "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -622,6 +734,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--ref-budget-s", type=float, default=420.0,
+                    help="--impl reference: run complete solves until this many seconds would be exceeded")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

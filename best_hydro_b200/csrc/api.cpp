@@ -33,16 +33,39 @@
 namespace bgpu {
 namespace {
 
-std::deque<std::string> g_log;
+// Messages for the caller's log (BEST appends them to its .log, best/besolve.f90:281-292): the
+// library posts them, bhm_log_line hands them out oldest first, one per call.
+class MessageQueue {
+ public:
+  void post(std::string m) { q_.push_back(std::move(m)); }
+  // The oldest message, cut to `cap` bytes and without a terminator, removed from the queue; -1 when
+  // the queue is empty.
+  int take(char* out, int cap) {
+    if (q_.empty()) return -1;
+    std::string m = std::move(q_.front());
+    q_.pop_front();
+    const size_t len = std::min(m.size(), (size_t)std::max(cap, 0));
+    if (len > 0) std::memcpy(out, m.data(), len);
+    return (int)len;
+  }
 
-void say(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
-void say(const char* fmt, ...) {
-  char buf[512];
-  va_list ap;
+ private:
+  std::deque<std::string> q_;
+};
+MessageQueue g_messages;
+
+// Posts a printf-style message.
+void note(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
+void note(const char* fmt, ...) {
+  va_list ap, ap2;
   va_start(ap, fmt);
-  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_copy(ap2, ap);
+  const int len = std::vsnprintf(nullptr, 0, fmt, ap);
   va_end(ap);
-  g_log.emplace_back(buf);
+  std::string m(len > 0 ? (size_t)len : 0, '\0');
+  if (len > 0) std::vsnprintf(&m[0], m.size() + 1, fmt, ap2);
+  va_end(ap2);
+  g_messages.post(std::move(m));
 }
 
 struct CudaError : std::runtime_error {
@@ -53,15 +76,21 @@ void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
 
-template <class F>
-int guarded(F&& f) {
+// The exception boundary of every entry point: the body's status, or 1 with the reason posted when
+// it throws, so that no C++ exception reaches the Fortran caller.
+template <class Body>
+int status_of(Body&& body) {
+  std::string why;
   try {
-    return f();
+    return body();
   } catch (const std::bad_alloc&) {
-    say("error: out of host memory");
+    why = "host memory exhausted";
   } catch (const std::exception& e) {
-    say("error: %s", e.what());
+    why = e.what();
+  } catch (...) {
+    why = "unexpected failure";
   }
+  note("error: %s", why.c_str());
   return 1;
 }
 
@@ -240,7 +269,7 @@ void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
       g_solve_info[0] = rep.iterations;
       g_solve_info[1] = rep.relres;
     } catch (const MixedFailure& e) {
-      say("mixed precision: %s; factoring the FP64 matrix instead", e.what());
+      note("mixed precision: %s; factoring the FP64 matrix instead", e.what());
       ck(cudaMemcpy2DAsync(d_b, (size_t)ldb * sizeof(double), s.rhs_keep.p, (size_t)n3 * sizeof(double),
                            (size_t)n3 * sizeof(double), nrhs, cudaMemcpyDeviceToDevice, r.stream),
          "rhs restore");
@@ -362,7 +391,7 @@ void series_record(Series& S, Runtime& r, cudaStream_t st, cudaEvent_t ev_assemb
 
 }  // namespace
 
-void log_message(const char* msg) { g_log.emplace_back(msg); }
+void log_message(const char* msg) { g_messages.post(msg); }
 
 }  // namespace bgpu
 
@@ -381,9 +410,9 @@ int bhm_available(void) {
 
 int bhm_create(int n, const double* v1, const double* v2, const double* v3, const double* area, double afac,
                double cg, int /*threads*/) {
-  return guarded([&] {
+  return status_of([&] {
     if (n < 1) {
-      say("error: the GPU solver needs at least 1 triangle");
+      note("error: the GPU solver needs at least 1 triangle");
       return 1;
     }
     Runtime& r = rt();
@@ -415,14 +444,14 @@ int bhm_create(int n, const double* v1, const double* v2, const double* v3, cons
     g = std::move(s);
     cudaDeviceProp prop{};
     cudaGetDeviceProperties(&prop, r.device);
-    say("GPU solver: %d triangles on %s (%d SMs, %.0f GB), dense GR %.2f GB in FP64", n, prop.name,
+    note("GPU solver: %d triangles on %s (%d SMs, %.0f GB), dense GR %.2f GB in FP64", n, prop.name,
         prop.multiProcessorCount, prop.totalGlobalMem / 1e9, 72.0 * n * (double)n / 1e9);
     return 0;
   });
 }
 
 void bhm_incenters(double* x) {
-  guarded([&] {
+  status_of([&] {
     Solver& s = solver();
     std::memcpy(x, s.x_host.data(), s.x_host.size() * sizeof(double));
     return 0;
@@ -430,12 +459,12 @@ void bhm_incenters(double* x) {
 }
 
 void bhm_entries(int i0, int m, int j0, int nc, double* a, int lda) {
-  guarded([&] {
+  status_of([&] {
     if (m <= 0 || nc <= 0) return 0;
     Solver& s = solver();
     Runtime& r = rt();
     if (i0 < 0 || j0 < 0 || (long)i0 + m > 3L * s.n || (long)j0 + nc > 3L * s.n || lda < m) {
-      say("error: bhm_entries: rows %d..%d or columns %d..%d outside GR (order %d), or lda %d < m", i0, i0 + m - 1, j0,
+      note("error: bhm_entries: rows %d..%d or columns %d..%d outside GR (order %d), or lda %d < m", i0, i0 + m - 1, j0,
           j0 + nc - 1, 3 * s.n, lda);
       return 1;
     }
@@ -465,7 +494,7 @@ void bhm_entries(int i0, int m, int j0, int nc, double* a, int lda) {
 
 double bhm_diag_mean(void) {
   double v = 0.0;
-  guarded([&] {
+  status_of([&] {
     Solver& s = solver();
     Runtime& r = rt();
     ck(launch_diag_mean(s.mesh(), s.diag.as<double>(), r.stream), "diagonal mean");
@@ -478,7 +507,7 @@ double bhm_diag_mean(void) {
 
 int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double* gdef, const int* comp,
               const double* xmu, int single, int /*nrhs*/) {
-  return guarded([&] {
+  return status_of([&] {
     Solver& s = solver();
     Runtime& r = rt();
     const int n = s.n, n3 = 3 * n;
@@ -512,7 +541,7 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
       try {
         s.mixed->build(s.mesh(), defl, s.gr.as<double>(), s.ld, eps, r.stream, r.ev[3], r.ev[4]);
       } catch (const MixedFailure& e) {
-        say("mixed precision: %s; factoring the FP64 matrix instead", e.what());
+        note("mixed precision: %s; factoring the FP64 matrix instead", e.what());
         s.precision = BGPU_FP64;
         factor64(s, r);
       }
@@ -534,13 +563,13 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
     r.ms[2] = r.elapsed(3, 5);
     r.ms[4] = r.elapsed(2, 5);
     if (info > 0) {
-      say("error: the LU factorisation found U(%d,%d) = 0: GR is singular", info, info);
+      note("error: the LU factorisation found U(%d,%d) = 0: GR is singular", info, info);
       return 1;
     }
     s.factored = true;
     if (s.mixed)
-      for (auto& line : s.mixed->profile_report()) say("%s", line.c_str());
-    say("GPU build: %s LU of order %d, assembly %.1f ms, factorisation %.1f ms (%.1f TFLOP/s)",
+      for (auto& line : s.mixed->profile_report()) note("%s", line.c_str());
+    note("GPU build: %s LU of order %d, assembly %.1f ms, factorisation %.1f ms (%.1f TFLOP/s)",
         s.precision == BGPU_FP64 ? "FP64" : (s.mixed ? s.mixed->name() : "mixed"), n3, r.ms[1], r.ms[2],
         (2.0 / 3.0) * (double)n3 * n3 * n3 / (r.ms[2] * 1e-3) / 1e12);
     return 0;
@@ -548,7 +577,7 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
 }
 
 int bhm_solve(int nrhs, double* b) {
-  return guarded([&] {
+  return status_of([&] {
     Solver& s = solver();
     Runtime& r = rt();
     if (nrhs <= 0) return 0;
@@ -559,24 +588,17 @@ int bhm_solve(int nrhs, double* b) {
     ck(cudaMemcpyAsync(b, s.rhs.p, (size_t)n3 * nrhs * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "x copy");
     r.sync("bhm_solve");
     if (s.precision == BGPU_MIXED && s.mixed)
-      for (auto& line : s.mixed->profile_report()) say("%s", line.c_str());
+      for (auto& line : s.mixed->profile_report()) note("%s", line.c_str());
     if (s.precision == BGPU_MIXED && s.mixed)
-      say("solve: %d right-hand sides, %d refinement steps, relative residual %.1e, %.2f ms", nrhs,
+      note("solve: %d right-hand sides, %d refinement steps, relative residual %.1e, %.2f ms", nrhs,
           (int)g_solve_info[0], g_solve_info[1], r.ms[3]);
     else
-      say("solve: %d right-hand sides with the FP64 LU factors, %.2f ms", nrhs, r.ms[3]);
+      note("solve: %d right-hand sides with the FP64 LU factors, %.2f ms", nrhs, r.ms[3]);
     return 0;
   });
 }
 
-int bhm_log_line(char* buf, int len) {
-  if (g_log.empty()) return -1;
-  const std::string& s = g_log.front();
-  const int k = std::min(len, (int)s.size());
-  std::memcpy(buf, s.data(), (size_t)k);
-  g_log.pop_front();
-  return k;
-}
+int bhm_log_line(char* buf, int len) { return g_messages.take(buf, len); }
 
 void bhm_destroy(void) {
   g.reset();
@@ -589,7 +611,7 @@ void bhm_destroy(void) {
 
 int bgpu_set_precision(int mode) {
   if (mode != -1 && mode != BGPU_FP64 && mode != BGPU_MIXED) {
-    say("error: unknown precision %d", mode);
+    note("error: unknown precision %d", mode);
     return 1;
   }
   g_prec_override = mode;
@@ -600,7 +622,7 @@ int bgpu_precision(void) { return g ? g->precision : -1; }
 
 int bgpu_set_refinement(int max_restarts, int krylov) {
   if (max_restarts < 0 || krylov < 1 || krylov > 16) {
-    say("error: bgpu_set_refinement: restarts >= 0 and 1 <= krylov <= 16");
+    note("error: bgpu_set_refinement: restarts >= 0 and 1 <= krylov <= 16");
     return 1;
   }
   g_refine[0] = max_restarts;
@@ -611,14 +633,14 @@ int bgpu_set_refinement(int max_restarts, int krylov) {
 
 int bgpu_series_create(int count, const int* n, const double* v1, const double* v2, const double* v3,
                        const double* area, const double* afac, double cg) {
-  return guarded([&] {
+  return status_of([&] {
     if (count < 1 || count > kMaxSeries) {
-      say("error: bgpu_series_create: %d meshes (1 to %d)", count, kMaxSeries);
+      note("error: bgpu_series_create: %d meshes (1 to %d)", count, kMaxSeries);
       return 1;
     }
     for (int i = 0; i < count; ++i)
       if (n[i] < 1) {
-        say("error: bgpu_series_create: mesh %d has no triangles", i);
+        note("error: bgpu_series_create: mesh %d has no triangles", i);
         return 1;
       }
     Runtime& r = rt();
@@ -664,7 +686,7 @@ int bgpu_series_create(int count, const int* n, const double* v1, const double* 
 }
 
 int bgpu_series_incenters(double* x) {
-  return guarded([&] {
+  return status_of([&] {
     Series& S = series();
     std::memcpy(x, S.x_host.data(), S.x_host.size() * sizeof(double));
     return 0;
@@ -672,7 +694,7 @@ int bgpu_series_incenters(double* x) {
 }
 
 int bgpu_series_diag_mean(double* dm) {
-  return guarded([&] {
+  return status_of([&] {
     Series& S = series();
     Runtime& r = rt();
     ck(cudaMemcpyAsync(dm, S.diag.p, sizeof(double) * S.count, cudaMemcpyDeviceToHost, r.stream), "diag copy");
@@ -682,7 +704,7 @@ int bgpu_series_diag_mean(double* dm) {
 }
 
 int bgpu_series_build(const int* ndef, const double* gdef, const int* comp, const double* xmu, int tune) {
-  return guarded([&] {
+  return status_of([&] {
     Series& S = series();
     Runtime& r = rt();
     S.factored = false;
@@ -746,7 +768,7 @@ int bgpu_series_build(const int* ndef, const double* gdef, const int* comp, cons
       while (a < table.size()) {
         size_t b = table.find('\n', a);
         if (b == std::string::npos) b = table.size();
-        say("autotune: %s", table.substr(a, b - a).c_str());
+        note("autotune: %s", table.substr(a, b - a).c_str());
         a = b + 1;
       }
       if (S.graph) {  // shapes may have changed: capture again
@@ -778,7 +800,7 @@ int bgpu_series_build(const int* ndef, const double* gdef, const int* comp, cons
         S.graph_kernels = captured;
       } else {
         S.graph = nullptr;
-        say("series: graph capture unavailable (%s); launching directly", why.empty() ? "capture failed" : why.c_str());
+        note("series: graph capture unavailable (%s); launching directly", why.empty() ? "capture failed" : why.c_str());
       }
       if (gph) cudaGraphDestroy(gph);
       cudaGetLastError();
@@ -799,18 +821,18 @@ int bgpu_series_build(const int* ndef, const double* gdef, const int* comp, cons
     ck(cudaMemcpy(info.data(), S.info.p, sizeof(int) * S.count, cudaMemcpyDeviceToHost), "info read");
     for (int i = 0; i < S.count; ++i)
       if (info[i] > 0) {
-        say("error: series mesh %d: the LU factorisation found U(%d,%d) = 0: GR is singular", i, info[i], info[i]);
+        note("error: series mesh %d: the LU factorisation found U(%d,%d) = 0: GR is singular", i, info[i], info[i]);
         return 1;
       }
     S.factored = true;
-    say("GPU series build: %d meshes (N = %d .. %d), %s, %.1f ms", S.count, *std::min_element(S.n.begin(), S.n.end()),
+    note("GPU series build: %d meshes (N = %d .. %d), %s, %.1f ms", S.count, *std::min_element(S.n.begin(), S.n.end()),
         *std::max_element(S.n.begin(), S.n.end()), S.graph ? "one CUDA graph" : "direct launches", S.ms[0]);
     return 0;
   });
 }
 
 int bgpu_series_solve(int nrhs, double* b) {
-  return guarded([&] {
+  return status_of([&] {
     Series& S = series();
     Runtime& r = rt();
     if (!S.factored) throw std::runtime_error("bgpu_series_build has not factored the series");
@@ -861,11 +883,11 @@ int bgpu_autotune_table(char* buf, int len) {
 }
 
 int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, double* grad) {
-  return guarded([&] {
+  return status_of([&] {
     Solver& s = solver();
     Runtime& r = rt();
     if (!s.factored || s.precision != BGPU_FP64) {
-      say("error: bgpu_best_gradient needs the FP64 LU of the last bhm_build (direct = 1, or "
+      note("error: bgpu_best_gradient needs the FP64 LU of the last bhm_build (direct = 1, or "
           "bgpu_set_precision(BGPU_FP64))");
       return 1;
     }
@@ -1147,7 +1169,7 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
           for (int t = 0; t < n; ++t) grad[(size_t)k * 9 * n + (size_t)corner * 3 * n + (size_t)c * n + t] -= mean[c];
     }
     hms[5] = since(h0);
-    say("gradient: D_t %.6e, D_r %.6e, %s %.6e; pair adjoint %.1f ms (GPU); host clock: solves %.1f, seeds %.1f, "
+    note("gradient: D_t %.6e, D_r %.6e, %s %.6e; pair adjoint %.1f ms (GPU); host clock: solves %.1f, seeds %.1f, "
         "adjoint solve %.1f, pair adjoint %.1f, deflation/area/triangles %.1f, total %.1f ms",
         values[0], values[1], wm > 0 ? "[eta]" : "CHI'", values[2], r.ms[5], hms[0], hms[1] - hms[0], hms[2] - hms[1],
         hms[3] - hms[2], hms[4] - hms[3], hms[5]);
@@ -1165,7 +1187,7 @@ int bgpu_timings(double* ms, int len) {
 
 void* bgpu_stream(void) {
   void* p = nullptr;
-  guarded([&] {
+  status_of([&] {
     p = (void*)rt().stream;
     return 0;
   });
@@ -1173,17 +1195,17 @@ void* bgpu_stream(void) {
 }
 
 int bgpu_solve_device(int nrhs, double* d_b, int ldb) {
-  return guarded([&] {
+  return status_of([&] {
     solve_device(solver(), rt(), nrhs, d_b, ldb);
     return 0;
   });
 }
 
 int bgpu_dgetrf_device(int n, double* d_a, int lda, int* d_ipiv, int* info) {
-  return guarded([&] {
+  return status_of([&] {
     Runtime& r = rt();
     if (n < 0 || lda < std::max(1, n) || (lda & 1) || ((uintptr_t)d_a & 15)) {
-      say("error: bgpu_dgetrf_device needs lda >= n, lda even and a 16-byte aligned matrix");
+      note("error: bgpu_dgetrf_device needs lda >= n, lda even and a 16-byte aligned matrix");
       return 1;
     }
     LuScratch ws{r.lu_scratch.p, r.lu_scratch.bytes};
@@ -1198,11 +1220,11 @@ int bgpu_dgetrf_device(int n, double* d_a, int lda, int* d_ipiv, int* info) {
 }
 
 int bgpu_dgetrs_device(int n, int nrhs, const double* d_a, int lda, const int* d_ipiv, double* d_b, int ldb) {
-  return guarded([&] {
+  return status_of([&] {
     Runtime& r = rt();
     if (n <= 0 || nrhs <= 0) return 0;
     if (nrhs > 16) {
-      say("error: bgpu_dgetrs_device takes at most 16 right-hand sides per call");
+      note("error: bgpu_dgetrs_device takes at most 16 right-hand sides per call");
       return 1;
     }
     DevBuf perm;
@@ -1221,10 +1243,10 @@ int bgpu_dgetrs_device(int n, int nrhs, const double* d_a, int lda, const int* d
 
 int bgpu_dgemm_minus_device(int m, int n, int k, const double* d_a, int lda, const double* d_b, int ldb, double* d_c,
                             int ldc) {
-  return guarded([&] {
+  return status_of([&] {
     Runtime& r = rt();
     if ((lda & 1) || (ldb & 1) || ((uintptr_t)d_a & 15) || ((uintptr_t)d_b & 15)) {
-      say("error: bgpu_dgemm_minus_device needs even leading dimensions and 16-byte aligned A and B");
+      note("error: bgpu_dgemm_minus_device needs even leading dimensions and 16-byte aligned A and B");
       return 1;
     }
     ck(cudaEventRecord(r.ev[6], r.stream), "event");
@@ -1239,9 +1261,9 @@ int bgpu_dgemm_minus_device(int m, int n, int k, const double* d_a, int lda, con
 unsigned long long bgpu_launch_count(void) { return g_launches; }
 
 int bgpu_kernel_stats(int kernel, int enable, int* launches, double* ms, double* work) {
-  return guarded([&] {
+  return status_of([&] {
     if (kernel < 0 || kernel >= kTimedKernels) {
-      say("error: unknown kernel id %d", kernel);
+      note("error: unknown kernel id %d", kernel);
       return 1;
     }
     int l = 0;
@@ -1258,7 +1280,7 @@ int bgpu_kernel_stats(int kernel, int enable, int* launches, double* ms, double*
 
 int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float* d_a, int lda, const float* d_b, int ldb, float* d_c,
                                 int ldc) {
-  return guarded([&] {
+  return status_of([&] {
     Runtime& r = rt();
     if (m <= 0 || n <= 0 || k <= 0) return 0;
     const long lt = ((long)k + 63) / 64 * 64;
@@ -1280,11 +1302,11 @@ int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float* d_a, int lda, 
 }
 
 static int assemble_device(bool fast, int r0, int r1, int c0, int c1, double* d_out, int ldo) {
-  return guarded([&] {
+  return status_of([&] {
     Solver& s = solver();
     Runtime& r = rt();
     if (r0 < 0 || c0 < 0 || r1 > s.n || c1 > s.n || ldo < 3 * (r1 - r0)) {
-      say("error: bgpu_assemble_device: range outside the mesh or ldo too small");
+      note("error: bgpu_assemble_device: range outside the mesh or ldo too small");
       return 1;
     }
     DevDeflation none;

@@ -2,10 +2,13 @@
 //
 // Compiled with -fmad=false: BEST is built with -ffp-contract=off (reference Makefile:34, :40), so
 // every product and sum below must round separately, in the order the reference writes it, for the
-// entries to match the reference's bit for bit.  IEEE +, -, *, / and sqrt are correctly rounded on
-// both sides.  The transcendental functions of the O(N) self blocks (acos, sin, cos, log) are the
-// correctly rounded ones of ddmath.cuh, which return what glibc returns for almost every argument;
-// the pair integrals' log is CUDA's (within an ulp; it reaches the entries without cancellation).
+// entries to follow the reference's operation sequence exactly.  IEEE +, -, *, / and sqrt are
+// correctly rounded on both sides; every transcendental function (acos, sin, cos, log of the O(N)
+// self blocks, and the 21 logs of each pair integral) is the correctly rounded one of ddmath.cuh.
+// The entries therefore equal TGETGR's arithmetic with correctly rounded functions bit for bit.
+// glibc's log, which the reference calls, is not correctly rounded on about 0.15 % of arguments, so
+// about 0.06 % of the reference's entries differ from these by an ulp or a few; each such entry is
+// one whose pair meets such an argument.
 //
 // Kernels:
 //   k_self_blocks   one thread per triangle: incenter, normal and the exact self-integral block,
@@ -126,7 +129,9 @@ __global__ void __launch_bounds__(kTgtTile, BGPU_ASM_MIN_BLOCKS)
     k_assemble(const double* __restrict__ geo, const double* __restrict__ xc, const double* __restrict__ self9,
                double cg, int r0, int r1, int c0, int c1, double* __restrict__ out, long ld, DevDeflation defl,
                float* __restrict__ out32, long ld32) {
-  assemble_tile<false>(blockIdx.x, blockIdx.y, geo, xc, self9, cg, r0, r1, c0, c1, out, ld, defl, out32, ld32);
+  __shared__ double s_logtab[3 * dd::kLogTabN];
+  assemble_tile<false>(blockIdx.x, blockIdx.y, geo, xc, self9, cg, r0, r1, c0, c1, out, ld, defl, out32, ld32,
+                       s_logtab);
 }
 
 // Every mesh of a series in one launch: block b belongs to the mesh whose tile range holds it.
@@ -137,8 +142,9 @@ __global__ void __launch_bounds__(kTgtTile, BGPU_ASM_MIN_BLOCKS) k_assemble_seri
   const int local = b - sa.tile0[i];
   const int tx = (sa.mesh[i].n + kTgtTile - 1) / kTgtTile;
   const DevMesh& m = sa.mesh[i];
+  __shared__ double s_logtab[3 * dd::kLogTabN];
   assemble_tile<false>(local % tx, local / tx, m.geo, m.xc, m.self9, m.cg, 0, m.n, 0, m.n, sa.out[i], sa.ld[i], sa.defl[i],
-                nullptr, 0);
+                       nullptr, 0, s_logtab);
 }
 
 __global__ void k_diag_mean(int n, const double* __restrict__ self9, double* out) {

@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(kTgtTile, BGPU_ASM_FAST_MIN_BLOCKS)
     k_assemble_fast(const double* __restrict__ geo, const double* __restrict__ xc, const double* __restrict__ self9,
                     double cg, int r0, int r1, int c0, int c1, double* __restrict__ out, long ld, DevDeflation defl,
                     float* __restrict__ out32, long ld32) {
-  assemble_tile<true>(blockIdx.x, blockIdx.y, geo, xc, self9, cg, r0, r1, c0, c1, out, ld, defl, out32, ld32);
+  assemble_tile<true>(blockIdx.x, blockIdx.y, geo, xc, self9, cg, r0, r1, c0, c1, out, ld, defl, out32, ld32, nullptr);
 }
 
 }  // namespace

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "bgpu_internal.h"
+#include "ddmath.cuh"
 
 namespace bgpu {
 namespace {
@@ -38,13 +39,16 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
 }
 
 // One tile: targets [r0 + 128 bx, +128) x sources [c0 + 16 by, +16) of one mesh.  Fast = false:
-// triangleint.f's operations in its order (bit-compatible entries; the including file is compiled
-// with -fmad=false); Fast = true: the same integrals with fewer FP64 operations, for the mixed path.
+// triangleint.f's operations in its order with a correctly rounded log (bit for bit TGETGR's
+// arithmetic with correctly rounded functions; the including file is compiled with -fmad=false);
+// s_logtab: the block's shared copy of the log's reduction table, filled here.  Fast = true: the same
+// integrals with fewer FP64 operations and the hardware log, for the mixed path (s_logtab unused).
 template <bool Fast>
 __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __restrict__ geo,
                                               const double* __restrict__ xc, const double* __restrict__ self9,
                                               double cg, int r0, int r1, int c0, int c1, double* __restrict__ out,
-                                              long ld, const DevDeflation& defl, float* __restrict__ out32, long ld32) {
+                                              long ld, const DevDeflation& defl, float* __restrict__ out32, long ld32,
+                                              double* s_logtab) {
   __shared__ double s_p[kSrcTile][9];     // p1, p2, p3
   __shared__ double s_v[kSrcTile][9];     // v21, v31, v32
   __shared__ double s_d[kSrcTile][9];     // d2121 d2131 d2132 d3131 d3232 d3231 s21 area 1/s21
@@ -81,6 +85,9 @@ __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __re
     s_d[threadIdx.x][7] = gp[9];
     if constexpr (Fast) s_d[threadIdx.x][8] = 1.0 / s_d[threadIdx.x][6];
     s_comp[threadIdx.x] = (defl.ndef > 1) ? defl.comp[t] : 1;
+  }
+  if constexpr (!Fast) {
+    for (int q = threadIdx.x; q < 3 * dd::kLogTabN; q += blockDim.x) s_logtab[q] = dd::kLogTab[q];
   }
   __syncthreads();
 
@@ -140,8 +147,9 @@ __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __re
           const double q1 = sqrt(d1c1c + y2 * d1c31 + yy * d3131);
           const double q2 = sqrt(d2c2c + y2 * d322c + yy * d3232);
           // h (triangleint.f:198-206): the denominator's root is d1c1c + (2 d1c31) y + (d3131 y) y
-          const double hv = log((d212c + d2132 * y + s21 * q2) /
-                                (d211c + d2131 * y + s21 * sqrt(d1c1c + 2 * d1c31 * y + d3131 * y * y))) /
+          const double hv = dd::cr_log_tab((d212c + d2132 * y + s21 * q2) /
+                                               (d211c + d2131 * y + s21 * sqrt(d1c1c + 2 * d1c31 * y + d3131 * y * y)),
+                                           s_logtab) /
                             s21;
           // hy (:222-234)
           const double hya = (d211c + y * d2131) / q1;

@@ -12,7 +12,7 @@
 //     trsm      U12 = L11^-1 A12, recursive: 32-row leaves (k_trsm_leaf) + GEMM updates
 //     gemm      A22 -= L21 U12 on the FP64 tensor cores (mma.sync m8n8k4 f64, cp.async pipeline)
 // tcgen05 has no FP64 kind, so the FP64 trailing update runs on DMMA; the mixed-precision path
-// (lu_mixed.cu) puts its trailing update on tcgen05.
+// (mixed.cu, with tc_gemm.cu) puts its updates on tcgen05.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 

@@ -17,7 +17,8 @@
 // updates are recovered by refinement in a few steps.
 //
 // Solve: restarted right-preconditioned GMRES in FP64 (preconditioner: the FP32 factors, applied
-// with FP64 accumulation), the true FP64 residual b - GR x at every restart; all right-hand sides
+// entirely in FP32 -- vectors, partial sums and diagonal-block products; its result only steers the
+// iteration), the true FP64 residual b - GR x at every restart; all right-hand sides
 // advance in lockstep.  Stops at a relative residual of tol for every column; a failure to converge
 // or a zero pivot is an error (the C ABI then factors the kept FP64 matrix instead).
 #include <cuda_bf16.h>

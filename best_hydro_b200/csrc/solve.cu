@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <vector>
 #include <cstdint>
@@ -281,7 +282,16 @@ struct TrsvScratch {
   static size_t bytes(int n) { return y_off(n) + (size_t)n * kMaxRhs * sizeof(double); }
 };
 
-unsigned g_epoch = 0;
+// Epochs of the readiness flags, shared by every solve of the process (any thread): each solve takes
+// two consecutive values, never 0 (the flags' initial value).
+std::atomic<unsigned> g_epoch{0};
+unsigned next_epochs() {
+  unsigned e;
+  do {
+    e = g_epoch.fetch_add(2) + 2;
+  } while (e == 0);
+  return e;
+}
 
 }  // namespace
 
@@ -311,23 +321,21 @@ cudaError_t getrs64(const double* LU, long lda, int n, const int* perm, double* 
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int nblk = (n + kBs - 1) / kBs;
   const int grid = std::min(nblk, sms * 2);
-  // epochs: never 0 (the flags' initial value)
-  g_epoch += 2;
-  if (g_epoch == 0) g_epoch = 2;
+  const unsigned epoch = next_epochs();
   cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
   if (e != cudaSuccess) return e;
   BGPU_COUNT_LAUNCH();
   if (nrhs <= 8)
-    k_trsv<double, true, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
+    k_trsv<double, true, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, epoch, d_status);
   else
-    k_trsv<double, true, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch, d_status);
+    k_trsv<double, true, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, epoch, d_status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(ticket, 0, 4, s)) != cudaSuccess) return e;
   BGPU_COUNT_LAUNCH();
   if (nrhs <= 8)
-    k_trsv<double, false, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1, d_status);
+    k_trsv<double, false, 8><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, epoch + 1, d_status);
   else
-    k_trsv<double, false, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, g_epoch + 1,
+    k_trsv<double, false, 16><<<grid, kThreads, 0, s>>>(LU, lda, n, Y, ldy, nrhs, flags, ticket, epoch + 1,
                                                          d_status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_copy_cols<double><<<(n + 255) / 256, 256, 0, s>>>(Y, ldy, n, nrhs, X, ldx); BGPU_COUNT_LAUNCH();
@@ -656,11 +664,10 @@ cudaError_t trsv_inv_pair(const F* LU, long lda, const FI* DL, const FI* DU, int
   for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
     const int q = std::min(kIrhs, nrhs - c0);
     V* Yc = Y + (size_t)c0 * ldy;
-    g_epoch += 2;
-    if (g_epoch == 0) g_epoch = 2;
-    cudaError_t e = trsv_one<F, FI, true, false, V>(LU, lda, DL, n, Yc, ldy, q, scratch, g_epoch, d_status, s);
+    const unsigned epoch = next_epochs();
+    cudaError_t e = trsv_one<F, FI, true, false, V>(LU, lda, DL, n, Yc, ldy, q, scratch, epoch, d_status, s);
     if (e != cudaSuccess) return e;
-    if ((e = trsv_one<F, FI, false, false, V>(LU, lda, DU, n, Yc, ldy, q, scratch, g_epoch + 1, d_status, s)) !=
+    if ((e = trsv_one<F, FI, false, false, V>(LU, lda, DU, n, Yc, ldy, q, scratch, epoch + 1, d_status, s)) !=
         cudaSuccess)
       return e;
   }
@@ -673,11 +680,10 @@ cudaError_t trsv_inv_pair_trans(const double* LU, long lda, const double* DL, co
   for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
     const int q = std::min(kIrhs, nrhs - c0);
     double* Yc = Y + (size_t)c0 * ldy;
-    g_epoch += 2;
-    if (g_epoch == 0) g_epoch = 2;
-    cudaError_t e = trsv_one<double, double, true, true>(LU, lda, DU, n, Yc, ldy, q, scratch, g_epoch, d_status, s);
+    const unsigned epoch = next_epochs();
+    cudaError_t e = trsv_one<double, double, true, true>(LU, lda, DU, n, Yc, ldy, q, scratch, epoch, d_status, s);
     if (e != cudaSuccess) return e;
-    if ((e = trsv_one<double, double, false, true>(LU, lda, DL, n, Yc, ldy, q, scratch, g_epoch + 1, d_status, s)) !=
+    if ((e = trsv_one<double, double, false, true>(LU, lda, DL, n, Yc, ldy, q, scratch, epoch + 1, d_status, s)) !=
         cudaSuccess)
       return e;
   }
@@ -814,6 +820,50 @@ cudaError_t noalloc_base(unsigned char** out, cudaStream_t s) {
 
 using bgpu::log_message;
 
+namespace bgpu {
+namespace {
+
+// The solve on the fixed scratch at `base`; *st receives the device status word.
+cudaError_t noalloc_solve(unsigned char* base, int n, int nrhs, const double* d_a, int lda, const int* d_ipiv,
+                          double* d_b, int ldb, cudaStream_t s, int* st) {
+  int* status = reinterpret_cast<int*>(base);
+  unsigned char* trsv = base + 256;
+  int* perm = reinterpret_cast<int*>(base + 256 + round256(TrsvScratch::bytes(n)));
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return e;
+  if ((e = lu_perm_from_ipiv(d_ipiv, n, perm, s)) != cudaSuccess) return e;
+  if ((e = getrs64(d_a, lda, n, perm, d_b, ldb, nrhs, trsv, status, s)) != cudaSuccess) return e;
+  if ((e = check_finite(d_b, ldb, n, nrhs, status, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(st, status, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);
+}
+
+// The warm-up call (n = 0): looks the array up and runs every kernel of the solve once, on a 1 x 1
+// system placed in the array itself (both widths of the triangular solve), so that the module's code
+// and the array are resident on this device before the caller's allocator takes the memory.
+cudaError_t noalloc_warm_up(unsigned char* base, cudaStream_t s, int* st) {
+  const size_t off = 1u << 20;  // beyond what an order-1 solve uses of the array
+  double* a = reinterpret_cast<double*>(base + off);
+  int* ipiv = reinterpret_cast<int*>(base + off + 256);
+  double* b = reinterpret_cast<double*>(base + off + 512);
+  const double one = 1.0;
+  const int piv = 1;
+  double rhs[kMaxRhs];
+  for (double& v : rhs) v = 1.0;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(a, &one, sizeof one, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(ipiv, &piv, sizeof piv, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(b, rhs, sizeof rhs, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  for (int nrhs : {1, kMaxRhs}) {
+    if ((e = noalloc_solve(base, 1, nrhs, a, 1, ipiv, b, 1, s, st)) != cudaSuccess) return e;
+    if (*st != kOk) return cudaSuccess;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace bgpu
+
 extern "C" int bgpu_dgetrs_noalloc(int n, int nrhs, const double* d_a, int lda, const int* d_ipiv, double* d_b,
                                    int ldb, void* stream) {
   using namespace bgpu;
@@ -832,29 +882,19 @@ extern "C" int bgpu_dgetrs_noalloc(int n, int nrhs, const double* d_a, int lda, 
     log_message(msg);
     return 1;
   }
-  if (n == 0) return 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   unsigned char* base = nullptr;
+  int st = kOk;
   cudaError_t e = noalloc_base(&base, s);
+  if (e == cudaSuccess)
+    e = (n == 0) ? noalloc_warm_up(base, s, &st) : noalloc_solve(base, n, nrhs, d_a, lda, d_ipiv, d_b, ldb, s, &st);
   if (e == cudaSuccess) {
-    int* status = reinterpret_cast<int*>(base);
-    unsigned char* trsv = base + 256;
-    int* perm = reinterpret_cast<int*>(base + 256 + round256(TrsvScratch::bytes(n)));
-    if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) == cudaSuccess &&
-        (e = lu_perm_from_ipiv(d_ipiv, n, perm, s)) == cudaSuccess &&
-        (e = getrs64(d_a, lda, n, perm, d_b, ldb, nrhs, trsv, status, s)) == cudaSuccess &&
-        (e = check_finite(d_b, ldb, n, nrhs, status, s)) == cudaSuccess) {
-      int st = 0;
-      if ((e = cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s)) == cudaSuccess &&
-          (e = cudaStreamSynchronize(s)) == cudaSuccess) {
-        if (st == kOk) return 0;
-        std::snprintf(msg, sizeof msg, "error: bgpu_dgetrs_noalloc: %s",
-                      st == kWaitTimeout ? "a device-side wait ran out (kernel gave up, no result)"
-                                         : "the solution is not finite (NaN or Inf)");
-        log_message(msg);
-        return 1;
-      }
-    }
+    if (st == kOk) return 0;
+    std::snprintf(msg, sizeof msg, "error: bgpu_dgetrs_noalloc: %s",
+                  st == kWaitTimeout ? "a device-side wait ran out (kernel gave up, no result)"
+                                     : "the solution is not finite (NaN or Inf)");
+    log_message(msg);
+    return 1;
   }
   std::snprintf(msg, sizeof msg, "error: bgpu_dgetrs_noalloc: CUDA error: %s", cudaGetErrorString(e));
   log_message(msg);

@@ -59,13 +59,19 @@ int bgpu_dgetrs_device(int n, int nrhs, const double *d_a, int lda, const int *d
  * through its own pool allocator, or that must not let a library allocate behind its back, can still
  * solve with the factors.  Its scratch (readiness flags, the permuted right-hand sides, the
  * permutation, a status word) is a fixed 16 MiB array in the library's device image, which every GPU
- * that loads the library holds until the process exits; that bounds the order: n * (8 * 16 + 4) bytes
- * plus a few KB must fit, i.e. n <= about 127,000 (larger n is rejected with a message).  The first
- * call on each device looks the array up and zeroes it, so make that first call before any stream
- * capture.  stream: a cudaStream_t (NULL for the default stream); the call returns when the solve on
- * it has finished.  Every call uses the same array: calls that overlap on the GPU (other threads,
- * other streams of the same device) race and must be serialised by the caller.  No reference
- * counterpart: the reference has no GPU code. */
+ * that uses it holds until the process exits; that bounds the order: n * (8 * 16 + 4) bytes plus a
+ * few KB must fit, i.e. n <= about 127,000 (larger n is rejected with a message).
+ * The array gets its device memory when the library's module is loaded on the device, which under
+ * CUDA's default lazy loading happens at the first call, not when the library is loaded: make a
+ * first call -- n = 0 is a warm-up that only looks the array up and runs the solve's kernels once on
+ * a 1 x 1 system inside it -- on each device, with that device current, before the application's
+ * allocator reserves the memory, and before any stream capture.  Later calls touch no memory beyond
+ * the array and their arguments.
+ * stream: a cudaStream_t (NULL for the default stream); the call waits for the solve on it to finish
+ * and returns 0, or nonzero after a message.  Every call uses the same array, which keeps the last
+ * call's contents: calls that overlap on the GPU (other threads, other streams of the same device)
+ * race and must be serialised by the caller.  No reference counterpart: the reference has no GPU
+ * code. */
 int bgpu_dgetrs_noalloc(int n, int nrhs, const double *d_a, int lda, const int *d_ipiv, double *d_b, int ldb,
                         void *stream);
 

@@ -12,7 +12,7 @@ has it; the GPU box uses the committed files).
       computed by the reference's own kernel.cpp (oracle/_ref): the first 96 rows and columns and
       4096 entries at seeded random positions.
 
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import gzip
 import json
@@ -70,4 +70,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT")
+    main(sys.argv[1])

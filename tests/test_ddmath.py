@@ -120,3 +120,55 @@ def test_acos_correctly_rounded(shim):
     want = np.array([float(d_acos(v)) for v in x])
     assert np.array_equal(y, want)
     assert np.count_nonzero(y != np.array([math.acos(v) for v in x])) <= 2
+
+
+def _pairs(L, name, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    hi, lo = np.empty_like(x), np.empty_like(x)
+    dp = ctypes.POINTER(ctypes.c_double)
+    getattr(L, name)(x.size, x.ctypes.data_as(dp), hi.ctypes.data_as(dp), lo.ctypes.data_as(dp))
+    return hi, lo
+
+
+def _log_samples(n, seed):
+    """Arguments that stress the table-driven log: the pair integrals' range (ratios of sums near
+    1..2), a wide exponent range, points next to 1 and next to every subinterval boundary."""
+    rng = np.random.default_rng(seed)
+    near1 = 1.0 + rng.uniform(-2.0 ** -9, 2.0 ** -9, n // 8) * np.exp2(-rng.integers(0, 40, n // 8))
+    # bit patterns on both sides of the 256 subinterval boundaries (kLogOff = 0x3FE5F80000000000)
+    off = 0x3FE5F80000000000
+    b = off + (np.arange(256, dtype=np.uint64) << np.uint64(44))
+    bnd = np.concatenate([(b + d).view(np.float64) for d in (np.uint64(0), np.uint64(1))] +
+                         [(b - np.uint64(d)).view(np.float64) for d in (1, 2)])
+    return np.concatenate([rng.uniform(1.0, 2.0, n // 2), np.exp(rng.uniform(-700, 700, n // 8)),
+                           rng.uniform(0.3, 3.0, n // 8), near1, bnd, 2.0 ** np.arange(-1070, 1020, 7.0),
+                           [1.0, 2.0, 0.5, 5e-324, 2.2250738585072014e-308, 1.7976931348623157e308]])
+
+
+def test_log_tab_fast_phase_error_bound(shim):
+    """The fast phase of cr_log_tab is within 2^-74 of log x (relative), measured against the
+    accurate phase (2^-100); its rounding test uses 2^-72."""
+    x = _log_samples(400000, 11)
+    x = x[(x > 2.3e-308) & (x != 1.0)]
+    fh, fl = _pairs(shim, "dd_log_fast_v", x)
+    ah, al = _pairs(shim, "dd_log_acc_v", x)
+    err = np.abs((fh - ah) + (fl - al)) / np.abs(ah)
+    assert float(np.max(err)) < 2.0 ** -74, np.log2(np.max(err))
+
+
+def test_log_tab_correctly_rounded(shim):
+    """cr_log_tab equals the correctly rounded log (Decimal at 60 digits) and cr_log."""
+    x = _log_samples(200000, 12)
+    y = call(shim, "dd_log_tab_v", x)
+    assert np.array_equal(y, call(shim, "dd_log_v", x))
+    sub = np.random.default_rng(13).choice(x.size, 3000, replace=False)
+    want = np.array([float(Decimal(float(v)).ln()) for v in x[sub]])
+    assert np.array_equal(y[sub], want)
+
+
+def test_log_tab_special_values(shim):
+    x = np.array([0.0, -0.0, -1.0, np.inf, np.nan, 1.0, 5e-324])
+    y = call(shim, "dd_log_tab_v", x)
+    assert y[0] == -np.inf and y[1] == -np.inf and np.isnan(y[2]) and y[3] == np.inf and np.isnan(y[4])
+    assert y[5] == 0.0 and not np.signbit(y[5])
+    assert y[6] == float(Decimal(5e-324).ln())

@@ -2,14 +2,16 @@
 
 Bars, per entry of GR (the oracle's C restatement is pinned bit for bit to the reference's
 kernel.cpp by the CPU tests):
-  * pair integrals (off the 3x3 diagonal blocks): within 4 ulp of the reference (only the pair
-    integrals' log is CUDA's; the histogram is printed);
-  * self blocks: bit for bit equal to the reference's arithmetic evaluated with correctly rounded
-    acos/sin/cos/log (tests/native/tgetgr_cr_shim.cpp), and within 4 ulp of each block's largest
-    entry of the reference's own values (they differ only where glibc's result is not the correctly
-    rounded one, which the rotation's cancellation amplifies);
+  * every entry (pair integrals and self blocks) bit for bit equal to the reference's arithmetic
+    evaluated with correctly rounded acos/sin/cos/log (tests/native/tgetgr_cr_shim.cpp);
+  * against the reference's own values (glibc's functions): pair entries within 4 ulp, self-block
+    entries within 4 ulp of each block's largest entry (they differ only where glibc's result is not
+    the correctly rounded one, which the self blocks' rotation amplifies; tests/test_cr_parity.py
+    accounts for every such entry);
   * incenters bit for bit (no transcendental function); DIAGM bit for bit against the correctly
-    rounded evaluation.
+    rounded evaluation;
+  * BEST's own GR check (best/besolve.f90:245-277) on 2eu7_02562 reports exactly the committed list
+    of entries where glibc is not correctly rounded, and 0 of the incenter coordinates.
 """
 import numpy as np
 import pytest
@@ -53,6 +55,11 @@ def self_mask(n3, i0=0, j0=0, m=None, nc=None):
 def check_block(got, s, cg, i0, j0, label=""):
     """Checks a block of GPU entries starting at (i0, j0) against both oracles; returns histograms."""
     m, nc = got.shape
+    cr, _, _ = crshim.assemble_cr(s, cg)
+    cr = cr[i0:i0 + m, j0:j0 + nc]
+    ndiff = int(np.count_nonzero(got.view(np.int64) != cr.view(np.int64)))
+    print(f"\n{label} entries differing from the correctly rounded evaluation: {ndiff} of {got.size}")
+    assert ndiff == 0
     ref, _, self9 = ob.assemble(s, cg)
     ref = ref[i0:i0 + m, j0:j0 + nc]
     mask = self_mask(3 * s.n, i0, j0, m, nc)
@@ -95,6 +102,40 @@ def test_entries_match_reference(case):
     _, s_cr = crshim.self_blocks_cr(s, cg)
     assert solver.diag_mean() == ob.diag_mean(s_cr, s.n)
     assert abs(solver.diag_mean() - ob.diag_mean(self9, s.n)) <= 4 * np.spacing(ob.diag_mean(self9, s.n))
+    solver.destroy()
+
+
+def test_hmcheck_2eu7():
+    """BEST_HMATRIX_CHECK=1 as the reference's test runs it (test/run_tests.sh:79-95): bhm_entries
+    fetched in blocks of 768 columns (best/besolve.f90:245-277) against TGETGR (the oracle, equal to
+    the reference's kernel.cpp bit for bit).  The differing entries are exactly those where glibc's
+    functions are not correctly rounded (committed list); none differ from the correctly rounded
+    evaluation; no incenter coordinate differs."""
+    tri, ta, tv = golden_mesh("2eu7_02562")
+    s = ob.setup(tri, 1, ta)
+    v1, v2, v3 = s.colmajor()
+    solver = BhmSolver()
+    solver.create(v1, v2, v3, s.area, s.afac, 1.0)
+    n3 = 3 * s.n
+    ref, x_ref, _ = ob.assemble(s, 1.0)
+    cr, _, _ = crshim.assemble_cr(s, 1.0)
+    nc = 3 * min(s.n, 256)
+    diff = []
+    ncr = 0
+    for j0 in range(0, n3, nc):
+        c = solver.entries(0, n3, j0, min(nc, n3 - j0))
+        r = ref[:, j0:j0 + c.shape[1]]
+        rows, cols = np.nonzero(c.view(np.int64) != r.view(np.int64))
+        diff.append(np.stack([rows, cols + j0], axis=1))
+        ncr += int(np.count_nonzero(c.view(np.int64) != cr[:, j0:j0 + c.shape[1]].view(np.int64)))
+    diff = np.concatenate(diff).astype(np.int32)
+    nx = int(np.count_nonzero(solver.incenters().view(np.int64) != x_ref.view(np.int64)))
+    print(f"\nGR check: {len(diff)} of {n3 * n3} entries and {nx} of {n3} incenter coordinates differ from "
+          f"TGETGR's (with glibc); {ncr} differ from the correctly rounded evaluation")
+    g = np.load(f"{ob.HERE}/../tests/golden/hmcheck_glibc_misrounds.npz")
+    order = np.lexsort((diff[:, 1], diff[:, 0]))
+    assert np.array_equal(diff[order], g["2eu7_02562"])
+    assert ncr == 0 and nx == 0
     solver.destroy()
 
 
