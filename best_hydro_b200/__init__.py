@@ -71,6 +71,10 @@ _SIGS = {
     "bgpu_series_destroy": (None, []),
     "bgpu_autotune_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "bgpu_best_gradient": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
+    "bgpu_create_from_triangles": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                  _dp, _ip]),
+    "bgpu_build_prepared": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "bgpu_prepared_arrays": (ctypes.c_int, [_dp, _dp, _dp, _dp, _ip, _dp, _dp]),
     "bgpu_launch_count": (ctypes.c_ulonglong, []),
     "bgpu_kernel_stats": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, _dp, _dp]),
     # include/best_driver.h: BEST's host side around the seam
@@ -193,6 +197,35 @@ class BhmSolver:
         _check(self.L.bgpu_best_gradient(int(iarea), float(truearea or 0.0), float(wm), _p(vals), _p(g)),
                "bgpu_best_gradient")
         return vals, g.reshape(3, 3, 3, n).transpose(0, 3, 1, 2).copy()
+
+    def create_from_triangles(self, tri, iarea=1, truearea=None, cg=1.0):
+        """bgpu_create_from_triangles: BEST's set-up and COMPON on the GPU from the triangles as read
+        (n x 9).  Returns (info {afac, totarea, centroid}, counts {ncomp, nopen, ndef})."""
+        tri = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1, 9)
+        n = tri.shape[0]
+        info = np.zeros(5)
+        counts = np.zeros(3, dtype=np.int32)
+        _check(self.L.bgpu_create_from_triangles(n, _p(tri), int(iarea), float(truearea or 0.0), float(cg), _p(info),
+                                                 counts.ctypes.data_as(_ip)), "bgpu_create_from_triangles")
+        self.n = n
+        return (dict(afac=float(info[0]), totarea=float(info[1]), centroid=info[2:5].copy()),
+                dict(ncomp=int(counts[0]), nopen=int(counts[1]), ndef=int(counts[2])))
+
+    def build_prepared(self, eps=1e-4, direct=1, single=0, nrhs=6):
+        """bgpu_build_prepared: the deflation on the GPU, then the build."""
+        _check(self.L.bgpu_build_prepared(float(eps), int(direct), int(single), int(nrhs)), "bgpu_build_prepared")
+
+    def prepared_arrays(self, ndef):
+        """bgpu_prepared_arrays: (v1, v2, v3, area, icomp, xmu, gdef) of the device set-up."""
+        n = self.n
+        v = [np.zeros(3 * n) for _ in range(3)]
+        area = np.zeros(n)
+        icomp = np.zeros(n, dtype=np.int32)
+        xmu = np.zeros(3 * n)
+        gdef = np.zeros(max(1, ndef))
+        _check(self.L.bgpu_prepared_arrays(_p(v[0]), _p(v[1]), _p(v[2]), _p(area), icomp.ctypes.data_as(_ip), _p(xmu),
+                                           _p(gdef)), "bgpu_prepared_arrays")
+        return v[0], v[1], v[2], area, icomp, xmu, gdef[:max(1, ndef)]
 
     def destroy(self):
         self.L.bhm_destroy()

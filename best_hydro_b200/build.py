@@ -22,6 +22,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", f"-I{CSRC
 SOURCES = [
     ("assemble.cu", ["-fmad=false"]),
     ("assemble_fast.cu", []),
+    ("geometry.cu", ["-fmad=false"]),
     ("lu.cu", []),
     ("solve.cu", []),
     ("tc_gemm.cu", []),

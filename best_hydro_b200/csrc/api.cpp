@@ -203,6 +203,12 @@ struct Solver {
   DevBuf ipiv, perm, dl64, du64;  // pivots, composed permutation, diagonal-block inverses
   DevBuf gdef, comp, xmu;
   DevBuf rhs, rhs_keep;        // right-hand sides (host-interface staging, and a kept copy)
+  // set up on the device (bgpu_create_from_triangles): the triangles as read, BEST's V1/V2/V3 and
+  // areas, {AFAC, total area, centroid}, {surfaces, open edges, NDEF}, scratch of the hash tables
+  bool prepared = false;
+  int counts_host[3] = {0, 0, 0};
+  double scal_host[5] = {0, 0, 0, 0, 0};
+  DevBuf tri, vset, area, scal, counts, setup_scratch;
   std::unique_ptr<MixedSolver> mixed;
   int precision = BGPU_FP64;
   bool factored = false;
@@ -389,6 +395,55 @@ void series_record(Series& S, Runtime& r, cudaStream_t st, cudaEvent_t ev_assemb
   }
 }
 
+// Assembly (with the deflation defl, on the device), factorisation and the host-side report: the
+// part of bhm_build after the deflation vectors are in place.
+int build_common(Solver& s, Runtime& r, double eps, int direct, int single, const DevDeflation& defl) {
+  const int n = s.n, n3 = 3 * n;
+  s.factored = false;
+  s.precision = precision_for(direct, single);
+  s.ld = padded_ld(n3);
+  s.gr.ensure((size_t)s.ld * n3 * sizeof(double), "GR (FP64)");
+  ck(cudaEventRecord(r.ev[2], r.stream), "event");
+  if (s.precision == BGPU_MIXED) {
+    if (!s.mixed) s.mixed = std::make_unique<MixedSolver>();
+    s.mixed->set_refinement(g_refine[0], g_refine[1]);
+    try {
+      s.mixed->build(s.mesh(), defl, s.gr.as<double>(), s.ld, eps, r.stream, r.ev[3], r.ev[4]);
+    } catch (const MixedFailure& e) {
+      note("mixed precision: %s; factoring the FP64 matrix instead", e.what());
+      s.precision = BGPU_FP64;
+      factor64(s, r);
+    }
+    ck(cudaEventRecord(r.ev[5], r.stream), "event");
+    r.check_status("bhm_build");
+  } else {
+    ck(launch_assemble(s.mesh(), 0, n, 0, n, s.gr.as<double>(), s.ld, defl, nullptr, 0, r.stream), "assembly");
+    ck(cudaEventRecord(r.ev[3], r.stream), "event");
+    factor64(s, r);
+    ck(cudaEventRecord(r.ev[5], r.stream), "event");
+    ck(cudaEventRecord(r.ev[4], r.stream), "event");
+    r.check_status("bhm_build");
+    ck(cudaEventRecord(r.ev[4], r.stream), "event");
+  }
+  r.sync("bhm_build");
+  int info = 0;
+  ck(cudaMemcpy(&info, r.info.p, sizeof(int), cudaMemcpyDeviceToHost), "info read");
+  r.ms[1] = r.elapsed(2, 3);
+  r.ms[2] = r.elapsed(3, 5);
+  r.ms[4] = r.elapsed(2, 5);
+  if (info > 0) {
+    note("error: the LU factorisation found U(%d,%d) = 0: GR is singular", info, info);
+    return 1;
+  }
+  s.factored = true;
+  if (s.mixed)
+    for (auto& line : s.mixed->profile_report()) note("%s", line.c_str());
+  note("GPU build: %s LU of order %d, assembly %.1f ms, factorisation %.1f ms (%.1f TFLOP/s)",
+       s.precision == BGPU_FP64 ? "FP64" : (s.mixed ? s.mixed->name() : "mixed"), n3, r.ms[1], r.ms[2],
+       (2.0 / 3.0) * (double)n3 * n3 * n3 / (r.ms[2] * 1e-3) / 1e12);
+  return 0;
+}
+
 }  // namespace
 
 void log_message(const char* msg) { g_messages.post(msg); }
@@ -446,6 +501,126 @@ int bhm_create(int n, const double* v1, const double* v2, const double* v3, cons
     cudaGetDeviceProperties(&prop, r.device);
     note("GPU solver: %d triangles on %s (%d SMs, %.0f GB), dense GR %.2f GB in FP64", n, prop.name,
         prop.multiProcessorCount, prop.totalGlobalMem / 1e9, 72.0 * n * (double)n / 1e9);
+    return 0;
+  });
+}
+
+int bgpu_create_from_triangles(int n, const double* tri, int iarea, double truearea, double cg, double* info,
+                               int* counts) {
+  return status_of([&] {
+    if (n < 1) {
+      note("error: the GPU solver needs at least 1 triangle");
+      return 1;
+    }
+    Runtime& r = rt();
+    auto s = std::make_unique<Solver>();
+    s->n = n;
+    s->cg = cg;
+    s->prepared = true;
+    s->tri.ensure((size_t)9 * n * sizeof(double), "triangles");
+    s->geo.ensure((size_t)n * kGeoStride * sizeof(double), "mesh");
+    s->vset.ensure((size_t)9 * n * sizeof(double), "centred corners");
+    s->area.ensure((size_t)n * sizeof(double), "areas");
+    s->scal.ensure(8 * sizeof(double), "set-up scalars");
+    s->counts.ensure(4 * sizeof(int), "surface counts");
+    s->comp.ensure((size_t)n * sizeof(int), "surface labels");
+    s->setup_scratch.ensure(setup_scratch_bytes(n), "set-up hash tables");
+    s->xc.ensure((size_t)n * kXcStride * sizeof(double), "incenters");
+    s->self9.ensure((size_t)n * 9 * sizeof(double), "self blocks");
+    s->diag.ensure(256, "diagonal mean");
+    ck(cudaEventRecord(r.ev[0], r.stream), "event");
+    ck(cudaMemcpyAsync(s->tri.p, tri, (size_t)9 * n * sizeof(double), cudaMemcpyHostToDevice, r.stream), "mesh copy");
+    SetupOut o;
+    o.geo = s->geo.as<double>();
+    o.v = s->vset.as<double>();
+    o.area = s->area.as<double>();
+    o.scal = s->scal.as<double>();
+    o.icomp = s->comp.as<int>();
+    o.counts = s->counts.as<int>();
+    ck(setup_device(n, s->tri.as<double>(), iarea, truearea, o, s->setup_scratch.p, r.status.as<int>(), r.stream),
+       "set-up on the device");
+    ck(cudaMemcpyAsync(s->scal_host, s->scal.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "set-up copy");
+    ck(cudaMemcpyAsync(s->counts_host, s->counts.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, r.stream), "counts copy");
+    // what bhm_create does with a mesh given by the caller: self blocks, incenters, DIAGM
+    ck(launch_self_blocks(s->mesh(), r.stream), "self blocks");
+    ck(launch_diag_mean(s->mesh(), s->diag.as<double>(), r.stream), "diagonal mean");
+    std::vector<double> xc((size_t)n * kXcStride), v((size_t)9 * n);
+    s->area_host.resize(n);
+    ck(cudaMemcpyAsync(xc.data(), s->xc.p, xc.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream),
+       "incenter copy");
+    ck(cudaMemcpyAsync(v.data(), s->vset.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "corner copy");
+    ck(cudaMemcpyAsync(s->area_host.data(), s->area.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, r.stream),
+       "area copy");
+    ck(cudaEventRecord(r.ev[1], r.stream), "event");
+    r.sync("bgpu_create_from_triangles");
+    r.check_status("bgpu_create_from_triangles");
+    r.ms[0] = r.elapsed(0, 1);
+    s->afac = s->scal_host[0];
+    for (int c = 0; c < 3; ++c) s->v_host[c].assign(v.begin() + (size_t)c * 3 * n, v.begin() + (size_t)(c + 1) * 3 * n);
+    s->x_host.resize((size_t)3 * n);
+    for (int t = 0; t < n; ++t)
+      for (int c = 0; c < 3; ++c) s->x_host[(size_t)c * n + t] = xc[(size_t)t * kXcStride + c];
+    if (info)
+      for (int q = 0; q < 5; ++q) info[q] = s->scal_host[q];
+    if (counts)
+      for (int q = 0; q < 3; ++q) counts[q] = s->counts_host[q];
+    note("GPU set-up: %d triangles, %d surface(s), %d open edge(s), NDEF %d, AFAC %.15g (%.2f ms on the device)", n,
+         s->counts_host[0], s->counts_host[1], s->counts_host[2], s->afac, r.ms[0]);
+    g = std::move(s);
+    return 0;
+  });
+}
+
+int bgpu_build_prepared(double eps, int direct, int single, int /*nrhs*/) {
+  return status_of([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    if (!s.prepared) {
+      note("error: bgpu_build_prepared needs a mesh set up by bgpu_create_from_triangles");
+      return 1;
+    }
+    const int n = s.n, n3 = 3 * n, ndef = s.counts_host[2];
+    s.ndef = ndef;
+    s.gdef.ensure(sizeof(double) * std::max(ndef, 1), "deflation weights");
+    s.xmu.ensure(sizeof(double) * n3, "deflation vectors");
+    ck(deflation_device(n, ndef, s.geo.as<double>(), s.comp.as<int>(), s.diag.as<double>(), s.xmu.as<double>(),
+                        s.gdef.as<double>(), r.stream),
+       "deflation on the device");
+    s.gdef_host.resize(ndef);
+    s.xmu_host.resize(n3);
+    s.comp_host.resize(ndef > 1 ? n : 0);
+    ck(cudaMemcpyAsync(s.gdef_host.data(), s.gdef.p, sizeof(double) * ndef, cudaMemcpyDeviceToHost, r.stream), "gdef");
+    ck(cudaMemcpyAsync(s.xmu_host.data(), s.xmu.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, r.stream), "xmu");
+    if (ndef > 1)
+      ck(cudaMemcpyAsync(s.comp_host.data(), s.comp.p, sizeof(int) * n, cudaMemcpyDeviceToHost, r.stream), "comp");
+    DevDeflation defl;
+    defl.ndef = ndef;
+    defl.gdef = s.gdef.as<double>();
+    defl.xmu = s.xmu.as<double>();
+    defl.comp = ndef > 1 ? s.comp.as<int>() : nullptr;
+    return build_common(s, r, eps, direct, single, defl);
+  });
+}
+
+int bgpu_prepared_arrays(double* v1, double* v2, double* v3, double* area, int* icomp, double* xmu, double* gdef) {
+  return status_of([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    if (!s.prepared) {
+      note("error: bgpu_prepared_arrays needs a mesh set up by bgpu_create_from_triangles");
+      return 1;
+    }
+    const size_t n = (size_t)s.n;
+    double* vs[3] = {v1, v2, v3};
+    for (int c = 0; c < 3; ++c)
+      if (vs[c]) std::memcpy(vs[c], s.v_host[c].data(), 3 * n * sizeof(double));
+    if (area) std::memcpy(area, s.area_host.data(), n * sizeof(double));
+    if (icomp) {
+      ck(cudaMemcpyAsync(icomp, s.comp.p, n * sizeof(int), cudaMemcpyDeviceToHost, r.stream), "labels");
+      r.sync("bgpu_prepared_arrays");
+    }
+    if (xmu && s.xmu_host.size() == 3 * n) std::memcpy(xmu, s.xmu_host.data(), 3 * n * sizeof(double));
+    if (gdef) std::memcpy(gdef, s.gdef_host.data(), s.gdef_host.size() * sizeof(double));
     return 0;
   });
 }
@@ -511,8 +686,6 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
     Solver& s = solver();
     Runtime& r = rt();
     const int n = s.n, n3 = 3 * n;
-    s.factored = false;
-    s.precision = precision_for(direct, single);
     DevDeflation defl;
     s.ndef = std::max(0, ndef);
     s.gdef_host.assign(gdef, gdef + s.ndef);
@@ -532,47 +705,7 @@ int bhm_build(double eps, int direct, double /*eps_pre*/, int ndef, const double
         defl.comp = s.comp.as<int>();
       }
     }
-    s.ld = padded_ld(n3);
-    s.gr.ensure((size_t)s.ld * n3 * sizeof(double), "GR (FP64)");
-    ck(cudaEventRecord(r.ev[2], r.stream), "event");
-    if (s.precision == BGPU_MIXED) {
-      if (!s.mixed) s.mixed = std::make_unique<MixedSolver>();
-      s.mixed->set_refinement(g_refine[0], g_refine[1]);
-      try {
-        s.mixed->build(s.mesh(), defl, s.gr.as<double>(), s.ld, eps, r.stream, r.ev[3], r.ev[4]);
-      } catch (const MixedFailure& e) {
-        note("mixed precision: %s; factoring the FP64 matrix instead", e.what());
-        s.precision = BGPU_FP64;
-        factor64(s, r);
-      }
-      ck(cudaEventRecord(r.ev[5], r.stream), "event");
-      r.check_status("bhm_build");
-    } else {
-      ck(launch_assemble(s.mesh(), 0, n, 0, n, s.gr.as<double>(), s.ld, defl, nullptr, 0, r.stream), "assembly");
-      ck(cudaEventRecord(r.ev[3], r.stream), "event");
-      factor64(s, r);
-      ck(cudaEventRecord(r.ev[5], r.stream), "event");
-      ck(cudaEventRecord(r.ev[4], r.stream), "event");
-      r.check_status("bhm_build");
-      ck(cudaEventRecord(r.ev[4], r.stream), "event");
-    }
-    r.sync("bhm_build");
-    int info = 0;
-    ck(cudaMemcpy(&info, r.info.p, sizeof(int), cudaMemcpyDeviceToHost), "info read");
-    r.ms[1] = r.elapsed(2, 3);
-    r.ms[2] = r.elapsed(3, 5);
-    r.ms[4] = r.elapsed(2, 5);
-    if (info > 0) {
-      note("error: the LU factorisation found U(%d,%d) = 0: GR is singular", info, info);
-      return 1;
-    }
-    s.factored = true;
-    if (s.mixed)
-      for (auto& line : s.mixed->profile_report()) note("%s", line.c_str());
-    note("GPU build: %s LU of order %d, assembly %.1f ms, factorisation %.1f ms (%.1f TFLOP/s)",
-        s.precision == BGPU_FP64 ? "FP64" : (s.mixed ? s.mixed->name() : "mixed"), n3, r.ms[1], r.ms[2],
-        (2.0 / 3.0) * (double)n3 * n3 * n3 / (r.ms[2] * 1e-3) / 1e12);
-    return 0;
+    return build_common(s, r, eps, direct, single, defl);
   });
 }
 

@@ -104,6 +104,25 @@ cudaError_t launch_assemble_series(const SeriesAssembly& sa, cudaStream_t s);
 // BEST's mean of GR's diagonal (best/best.f:401-403), summed in BEST's order, into *d_out.
 cudaError_t launch_diag_mean(const DevMesh& m, double* d_out, cudaStream_t s);
 
+// BEST's input set-up on the device (geometry.cu): from the triangles as read (n x 9, device), the
+// centred mesh in the solver's layout and as BEST's V1, V2, V3 (v: 9 n doubles, v1 | v2 | v3, each n x 3
+// column-major), the corrected areas, scal = {AFAC, total area, centroid x, y, z}, COMPON's
+// 1-based surfaces and counts = {surfaces, open edges, NDEF}.
+struct SetupOut {
+  double* geo = nullptr;
+  double* v = nullptr;
+  double* area = nullptr;
+  double* scal = nullptr;
+  int* icomp = nullptr;
+  int* counts = nullptr;
+};
+size_t setup_scratch_bytes(int n);
+cudaError_t setup_device(int n, const double* tri, int iarea, double truearea, const SetupOut& o, void* scratch,
+                         int* status, cudaStream_t s);
+// XMU (3 n) and GDEF (ndef) from the mesh, the surfaces and the device's DIAGM (*diagm).
+cudaError_t deflation_device(int n, int ndef, const double* geo, const int* icomp, const double* diagm, double* xmu,
+                             double* gdef, cudaStream_t s);
+
 // lu.cu -------------------------------------------------------------------------------------
 // Scratch for the factorisation kernels (grid barrier words, pivot candidates, status).
 struct LuScratch {

@@ -84,6 +84,22 @@ int bgpu_dgemm_minus_device(int m, int n, int k, const double *d_a, int lda, con
 int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float *d_a, int lda, const float *d_b, int ldb, float *d_c,
                                 int ldc);
 
+/* ---- Input set-up on the GPU (BEST's driver does it on the host: best/best.f:261-337 and COMPON,
+ * best/compon.f90:19-116; the deflation, best/best.f:384-404 and DEFGAM, compon.f90:185-197) ------
+ * bgpu_create_from_triangles takes the triangles as read (tri: n x 9, row t = v1 v2 v3, host memory)
+ * and does on the device what BEST does before bhm_create -- centroid shift, areas, the area
+ * correction (iarea, truearea), COMPON's surfaces and open edges, NDEF -- and then what bhm_create
+ * does.  info (5 doubles, may be NULL): AFAC, total area, centroid; counts (3 ints, may be NULL):
+ * surfaces, open edges, NDEF.  Every value equals bgpu_best_setup's bit for bit (the sums are taken
+ * in BEST's order).  bgpu_build_prepared then forms XMU and GDEF from DIAGM on the device and
+ * builds as bhm_build does with them (eps, direct, single as there).  bgpu_prepared_arrays copies
+ * the set-up out (any pointer may be NULL): V1, V2, V3 (n x 3 column-major, centred), corrected
+ * areas, surface labels, and after bgpu_build_prepared XMU (3n) and GDEF (NDEF). */
+int bgpu_create_from_triangles(int n, const double *tri, int iarea, double truearea, double cg, double *info,
+                               int *counts);
+int bgpu_build_prepared(double eps, int direct, int single, int nrhs);
+int bgpu_prepared_arrays(double *v1, double *v2, double *v3, double *area, int *icomp, double *xmu, double *gdef);
+
 /* Assembles GR rows of triangles [r0, r1) x columns of triangles [c0, c1) of the mesh given to
  * bhm_create into d_out (column-major, ldo), before deflation (best/tgetgr.f:33-173). */
 int bgpu_assemble_device(int r0, int r1, int c0, int c1, double *d_out, int ldo);
