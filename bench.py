@@ -373,6 +373,8 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import best_hydro_b200 as bh
 
+    t_start = time.perf_counter()
+
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     dist = None
@@ -482,6 +484,15 @@ def run_ours(args, rank, world, local_rank):
                    for i, k in enumerate(("create", "incenters_deflation", "build", "solve"))} if phases else None)
     host_notes = [ln for ln in bh.log_lines() if "host side" in ln][-2:]
 
+    # the other workloads' records (GPU), with the headline's buffers released first
+    solver.destroy()
+    del b, b0
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    records = None
+    if rank == 0 and world == 1 and not args.no_records and args.workload == "star_f32":
+        records = collect_records(args, local_rank, t_start)
+
     cpu = cpu_tens = None
     if rank == 0 and world == 1 and not args.no_cpu:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
@@ -546,28 +557,26 @@ def run_ours(args, rank, world, local_rank):
             "accuracy": accuracy,
             "result": {"D_t_cm2_s": acc_head["D_t"], "D_r_1_s": acc_head["D_r"], "chiprime": acc_head["chiprime"]},
             "cpu_baseline": cpu,
+            "records": records,
             "peaks": {"source": peak_src, "hbm_gbs": peaks.get("hbm_gbs"), "bf16_tflops": peaks.get("bf16_tflops"),
                       "bf16_tflops_sustained": peaks.get("bf16_tflops_sustained")},
         }
         print(json.dumps(line), flush=True)
-    solver.destroy()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def run_adjoint(args, rank, world, local_rank):
+def adjoint_record(steps, warmup, fd_vertices=64, fit_steps=20, freq=16):
     """The differentiation workload: adjoint gradients of D_t, D_r and [eta] (CHI') with respect to
-    every vertex coordinate, checked against central differences (h = 1e-4 A) on 64 random vertices
-    (seed 2), then a 20-step descent on vertex normal displacements that brings D_t 3% below its
-    initial value (mesh's own area, BEST's -na, for the fit)."""
+    every vertex coordinate, timed; checked against central differences (h = 1e-4 A) on fd_vertices
+    random vertices (seed 2); then a fit_steps-step descent on vertex normal displacements that
+    brings D_t 3% below its initial value (mesh's own area, BEST's -na, for the fit)."""
     import torch
     import best_hydro_b200 as bh
     from best_hydro_b200 import meshes
 
-    torch.cuda.set_device(local_rank)
-    w = WORKLOADS[args.workload]
-    verts, faces, ta, tv = meshes.ellipsoid_vf(w["gen"][1])
+    verts, faces, ta, tv = meshes.ellipsoid_vf(freq)
     nv = len(verts)
 
     def forward(vx, iarea):
@@ -583,10 +592,10 @@ def run_adjoint(args, rank, world, local_rank):
         return np.array([tr["DTRANS"], tr["DR"], chip]), s
 
     bh.set_precision(bh.BGPU_FP64)
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         forward(verts, 1)[1].gradient(iarea=1, truearea=ta)
     t_fwd, t_grad = [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         v0, s = forward(verts, 1)
@@ -596,9 +605,9 @@ def run_adjoint(args, rank, world, local_rank):
         t_fwd.append(t1 - t0)
         t_grad.append(t2 - t1)
     gv = meshes.corner_to_vertex(g, faces, nv)
-    # central differences on 64 random vertices
+    # central differences on random vertices
     rng = np.random.default_rng(2)
-    picks = rng.choice(nv, 64, replace=False)
+    picks = rng.choice(nv, fd_vertices, replace=False)
     h = 1e-4
     scale = np.abs(gv).reshape(3, -1).max(axis=1)
     worst = np.zeros(3)
@@ -611,52 +620,71 @@ def run_adjoint(args, rank, world, local_rank):
             fd = (forward(vp, 1)[0] - forward(vm, 1)[0]) / (2 * h)
             worst = np.maximum(worst, np.abs(fd - gv[:, v, c]) / scale)
     t_fd = time.perf_counter() - t0
-    # descent on normal displacements s_i (v_i + s_i n_i, n_i the outward unit normal at the vertex)
-    nrm = np.zeros_like(verts)
-    for f in faces:
-        e = np.cross(verts[f[1]] - verts[f[0]], verts[f[2]] - verts[f[0]])
-        nrm[f] += e
-    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
-    d0 = forward(verts, 0)[0][0]
-    target = 0.97 * d0
-    sdisp = np.zeros(nv)
     history = []
-    for it in range(20):
-        vals_k, sk = forward(verts + sdisp[:, None] * nrm, 0)
-        _, gk = sk.gradient(iarea=0)
-        gs = (meshes.corner_to_vertex(gk, faces, nv)[0] * nrm).sum(axis=1)  # dD_t / ds_i
-        r = (vals_k[0] - target) / target
-        history.append(float(r))
-        # steepest descent on r^2 / 2 with the step that zeroes the linearised residual
-        sdisp -= (r * target) * gs / float(gs @ gs)
+    sdisp = np.zeros(nv)
+    if fit_steps:
+        # descent on normal displacements s_i (v_i + s_i n_i, n_i the outward unit normal at the vertex)
+        nrm = np.zeros_like(verts)
+        for f in faces:
+            e = np.cross(verts[f[1]] - verts[f[0]], verts[f[2]] - verts[f[0]])
+            nrm[f] += e
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        d0 = forward(verts, 0)[0][0]
+        target = 0.97 * d0
+        for it in range(fit_steps):
+            vals_k, sk = forward(verts + sdisp[:, None] * nrm, 0)
+            _, gk = sk.gradient(iarea=0)
+            gs = (meshes.corner_to_vertex(gk, faces, nv)[0] * nrm).sum(axis=1)  # dD_t / ds_i
+            r = (vals_k[0] - target) / target
+            history.append(float(r))
+            # steepest descent on r^2 / 2 with the step that zeroes the linearised residual
+            sdisp -= (r * target) * gs / float(gs @ gs)
     bh.set_precision(-1)
-    line = {
-        "metric": "s per adjoint gradient (D_t, D_r, [eta] w.r.t. 3 x 2562 vertex coordinates)",
-        "value": float(np.median(t_grad)), "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": float(np.median(t_grad)) * 1e3, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "N": len(faces), "vertices": nv, "desc": w["desc"]},
-        "forward_solve_s": float(np.median(t_fwd)), "values": {"D_t": vals[0], "D_r": vals[1], "chiprime": vals[2]},
-        "fd_check": {"vertices": 64, "seed": 2, "h_A": h, "worst_abs_err_over_max_grad": worst.tolist(),
+    return {
+        "value": float(np.median(t_grad)), "unit": "s", "steps": steps, "warmup": warmup,
+        "N": len(faces), "vertices": nv, "forward_solve_s": float(np.median(t_fwd)),
+        "values": {"D_t": vals[0], "D_r": vals[1], "chiprime": vals[2]},
+        "fd_check": {"vertices": fd_vertices, "seed": 2, "h_A": h, "worst_abs_err_over_max_grad": worst.tolist(),
                      "seconds": t_fd},
         "fit": {"target": "D_t 3% below initial (mesh's own area)", "relative_residual_per_step": history,
                 "max_normal_displacement_A": float(np.abs(sdisp).max())},
         "log": [ln for ln in bh.log_lines() if ln.startswith("gradient")][-1:],
     }
+
+
+def run_adjoint(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    w = WORKLOADS[args.workload]
+    rec = adjoint_record(args.steps, args.warmup, freq=w["gen"][1])
+    line = {
+        "metric": "s per adjoint gradient (D_t, D_r, [eta] w.r.t. 3 x 2562 vertex coordinates)",
+        "value": rec["value"], "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": rec["value"] * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "N": rec["N"], "vertices": rec["vertices"], "desc": w["desc"]},
+    }
+    line.update({k: rec[k] for k in ("forward_solve_s", "values", "fd_check", "fit", "log")})
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def run_series(args, rank, world, local_rank):
+SERIES_FREQS = (11, 12, 14, 16, 18, 20, 22, 23)
+
+
+def series_record(steps, warmup, local_rank=0, sequential_passes=1):
     """The series workload: every mesh assembled, factored (FP64) and solved for 11 right-hand sides
     through bgpu_series_* (one CUDA graph per build), against the same meshes solved one after the
     other through the single-mesh seam; results and their 1/N extrapolation."""
     import torch
     import best_hydro_b200 as bh
+    from best_hydro_b200 import meshes
 
-    torch.cuda.set_device(local_rank)
-    w = WORKLOADS[args.workload]
-    setups = [bh.Setup(tri, w["iarea"], ta) for tri, ta, tv in make_mesh(args.workload)]
+    setups = []
+    for f in SERIES_FREQS:
+        tri, ta, tv = meshes.ellipsoid(f)
+        setups.append(bh.Setup(tri, 1, ta))
     bh.set_precision(bh.BGPU_FP64)
     S = bh.Series()
     S.create(setups)
@@ -668,13 +696,13 @@ def run_series(args, rank, world, local_rank):
     rhs = [np.hstack([bh.rhs6(x), bh.strain5(x)]) for x in xs]
     S.build(defl, tune=1)  # tuning pass + first graph build (warm-up)
     tune_ms = S.timings()["tune"]
-    for _ in range(max(0, args.warmup - 1)):
+    for _ in range(max(0, warmup - 1)):
         S.build(defl)
     launches0 = bh.launch_count()
     sampler = ClockSampler(local_rank)
     sampler.start()
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         S.build(defl)
@@ -685,7 +713,7 @@ def run_series(args, rank, world, local_rank):
     dev_ms = S.timings()
     # the same meshes one after the other through the single-mesh seam
     seq, seq_sols = [], []
-    for k in range(max(1, min(args.steps, 2))):
+    for k in range(sequential_passes):
         t0 = time.perf_counter()
         out = []
         for st in setups:
@@ -707,19 +735,95 @@ def run_series(args, rank, world, local_rank):
     ns = [d["N"] for d in per]
     ext = {k: bh.extrapolate(ns, [d[k] for d in per])[0] for k in ("D_t", "D_r", "chiprime")}
     v = float(np.median(times))
-    line = {
-        "metric": "s per series solve (8 meshes: assemble + FP64 LU + 11 RHS each)", "value": v, "unit": "s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "N": ns, "desc": w["desc"]},
+    S.destroy()
+    bh.set_precision(-1)
+    return {
+        "value": v, "unit": "s", "steps": steps, "warmup": warmup, "N": ns,
         "device_ms": {"build_graph": dev_ms["build"], "solve": dev_ms["solve"], "tuning_pass": tune_ms},
         "sequential_single_solves_s": float(np.median(seq)), "speedup_vs_sequential": float(np.median(seq)) / v,
         "bitwise_equal_to_single_solves": bool(same), "clocks": clocks, "gpu_launches": launches,
         "per_mesh": per, "extrapolated_1_over_N": ext, "autotune": bh.autotune_table(),
     }
-    S.destroy()
+
+
+def run_series(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    w = WORKLOADS[args.workload]
+    rec = series_record(args.steps, args.warmup, local_rank, sequential_passes=max(1, min(args.steps, 2)))
+    line = {
+        "metric": "s per series solve (8 meshes: assemble + FP64 LU + 11 RHS each)", "value": rec["value"],
+        "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec["value"] * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "N": rec["N"], "desc": w["desc"]},
+    }
+    line.update({k: rec[k] for k in rec if k not in ("value", "unit", "steps", "warmup", "N")})
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def star45_record(warmup=1, steps=1, fp64=True):
+    """The precision workload at N = 40,500 (order 121,500): the mixed path's device seconds per solve
+    (build + 6-RHS solve) and, with fp64, the plain FP64 path's on the same matrix and the relative
+    differences of D_t, D_r, CHI' and the tensors between the two (11-RHS solves)."""
+    import torch
+    import best_hydro_b200 as bh
+
+    tri, ta, tv = make_mesh("star_f45")
+    st = bh.Setup(tri, WORKLOADS["star_f45"]["iarea"], ta)
+    s = bh.BhmSolver()
+    s.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+    x = s.incenters()
+    xmu, gdef = st.deflation(s.diag_mean())
+    rhs6 = bh.rhs6(x)
+    out, acc = {}, {}
+    legs = (("mixed", bh.BGPU_MIXED, warmup, steps),) + ((("fp64", bh.BGPU_FP64, 0, 1),) if fp64 else ())
+    for name, prec, w, k in legs:
+        bh.set_precision(prec)
+        ts = []
+        for it in range(w + k):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.build(eps=1e-10, direct=1 if prec == bh.BGPU_FP64 else 0, ndef=st.ndef, gdef=gdef, comp=st.icomp,
+                    xmu=xmu)
+            s.solve(rhs6)
+            if it >= w:
+                ts.append(time.perf_counter() - t0)
+        stages = bh.timings()
+        acc[name] = tensors_of(s, x, st, bh)
+        out[name] = {"value": float(np.median(ts)), "unit": "s", "steps": k, "warmup": w,
+                     "stages_ms": {kk: round(float(stages[kk]), 2) for kk in ("assemble", "factor", "solve")},
+                     "note": "host wall time of bhm_build + bhm_solve (6 RHS, host buffers)"}
+    bh.set_precision(-1)
+    s.destroy()
+    rec = {"N": st.n, "order": 3 * st.n, "legs": out}
+    if fp64:
+        rec["accuracy_mixed_vs_fp64"] = tensor_errors(acc["mixed"], acc["fp64"])
+        rec["speedup_mixed_vs_fp64"] = out["fp64"]["value"] / out["mixed"]["value"]
+    return rec
+
+
+def collect_records(args, local_rank, t_start):
+    """The other workloads' records in the default run (each guarded; skipped past the time budget)."""
+    import torch
+
+    recs = {}
+    for name, fn in (("ellipsoid_series", lambda: series_record(1, 1, local_rank)),
+                     ("ellipsoid_adjoint", lambda: adjoint_record(1, 1, fd_vertices=4, fit_steps=0)),
+                     ("star_f45", lambda: star45_record())):
+        if time.perf_counter() - t_start > args.records_budget_s:
+            recs[name] = {"skipped": f"bench time budget of {args.records_budget_s:.0f} s reached"}
+            continue
+        try:
+            t0 = time.perf_counter()
+            recs[name] = fn()
+            recs[name]["record_wall_s"] = time.perf_counter() - t0
+        except Exception as e:  # a record must never cost the headline line
+            recs[name] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return recs
 
 
 def main():
@@ -734,6 +838,10 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-records", action="store_true",
+                    help="skip the records of the series, adjoint and N = 40,500 workloads in the default run")
+    ap.add_argument("--records-budget-s", type=float, default=600.0,
+                    help="start no further record once the run has taken this many seconds")
     ap.add_argument("--ref-budget-s", type=float, default=420.0,
                     help="--impl reference: run complete solves until this many seconds would be exceeded")
     args = ap.parse_args()

@@ -71,6 +71,8 @@ _SIGS = {
     "bgpu_series_destroy": (None, []),
     "bgpu_autotune_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "bgpu_best_gradient": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
+    "bgpu_lu32_leaf_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p]),
     "bgpu_create_from_triangles": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                   _dp, _ip]),
     "bgpu_build_prepared": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
@@ -481,6 +483,12 @@ def dgetrs_noalloc(n, nrhs, d_a, lda, d_ipiv, d_b, ldb, stream=0):
     """bgpu_dgetrs_noalloc: the solve without device allocations (see include/best_gpu.h)."""
     _check(lib().bgpu_dgetrs_noalloc(int(n), int(nrhs), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_ipiv),
                                      ctypes.c_void_p(d_b), int(ldb), ctypes.c_void_p(stream)), "bgpu_dgetrs_noalloc")
+
+
+def lu32_leaf_device(h, d_a, lda, d_linv, d_uinv):
+    """bgpu_lu32_leaf_device: the mixed LU's 128 x 128 diagonal leaf (see include/best_gpu.h)."""
+    _check(lib().bgpu_lu32_leaf_device(int(h), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_linv),
+                                       ctypes.c_void_p(d_uinv)), "bgpu_lu32_leaf_device")
 
 
 def dgemm_minus_device(m, n, k, d_a, lda, d_b, ldb, d_c, ldc):

@@ -1434,6 +1434,19 @@ int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float* d_a, int lda, 
   });
 }
 
+int bgpu_lu32_leaf_device(int h, float* d_a, int lda, float* d_linv, float* d_uinv) {
+  return status_of([&] {
+    Runtime& r = rt();
+    if (h < 1 || h > 128 || lda < h) {
+      note("error: bgpu_lu32_leaf_device: h %d outside 1..128 or lda %d < h", h, lda);
+      return 1;
+    }
+    ck(lu32_leaf(d_a, lda, h, d_linv, d_uinv, r.status.as<int>(), r.stream), "LU leaf");
+    r.check_status("LU leaf");
+    return 0;
+  });
+}
+
 static int assemble_device(bool fast, int r0, int r1, int c0, int c1, double* d_out, int ldo) {
   return status_of([&] {
     Solver& s = solver();

@@ -75,16 +75,17 @@ constexpr int kZeroPivot = 4;  // status: a pivot of the unpivoted FP32 LU is ze
 long round_up(long v, long q) { return (v + q - 1) / q * q; }
 
 // ---- diagonal leaf: h x h (h <= 128) LU without pivoting and the inverses of both triangles ----
-// 512 threads = 16 warps x 32 lanes; warp w owns rows 8w .. 8w+7 and lane l columns 4l .. 4l+3 of
-// the 128 x 128 block, as an 8 x 4 register tile (rows and columns beyond h hold the identity, so
-// the padded part factors to itself).  The factorisation goes 4 columns per step (32 steps, one
-// barrier each): the thread holding the 4 x 4 diagonal block (warp K/2, lane K) factors it and its
-// warp forms the 4 rows of U to its right (the block's L comes by shuffles); after the barrier, the
-// lane K of every warp below forms its rows of the 4 columns of L, passes them to its warp by
-// shuffles, and every such thread applies the rank-4 update to its tile.  The inverses run the same
-// way, L^-1 forward and U^-1 backward in the same 32 steps, from the factors in shared memory.
-// L^-1 (unit lower) and U^-1 are written to DL, DU (128 x 128 column-major, zero outside h x h).
-constexpr int kLdS = 129;
+// One CTA of 512 threads, everything in shared memory: M (the block, becoming L\U), LI = L^-1 and
+// UI = U^-1, column-major with stride kS (rows and columns beyond h hold the identity, so the padded
+// part factors to itself).  Recursive halving, as the factorisation around it:
+//   LU(D) = [L11 0; L21 L22][U11 U12; 0 U22]:  LU(D11) with LI11, UI11;  U12 = LI11 D12 and
+//   L21 = D21 UI11 (two thread groups at once);  D22 -= L21 U12;  LU(D22) with LI22, UI22;
+//   LI21 = -LI22 (L21 LI11),  UI12 = -(UI11 U12) UI22  (the block inverse of a triangular matrix).
+// 128 -> 64 -> 32; a 32 x 32 block is factored by one warp (lane i holds row i; row k of U goes to
+// the other lanes by shuffles), and its two inverses by two warps (lane c forms column c by
+// substitution).  Every product of the 64 and 128 levels is a small shared-memory matrix product
+// with register tiles.  The serial part is 4 warp-sized factorisations; the rest is parallel.
+constexpr int kS = 132;  // column stride (floats): 16-byte aligned columns
 
 // Optional launch stamps (as the GEMM's): the earliest CTA start into st[0], the latest CTA end into
 // st[1], global timer in ns.  st is a kernel argument, so the branch is uniform.
@@ -106,283 +107,204 @@ __device__ __forceinline__ void stamp_end(unsigned long long* st) {
   }
 }
 
-// rows q0 .. q0+3 of an 8 x 4 tile, as a 4 x 4 array (q0 = 0 or 4; selects keep it in registers)
-__device__ __forceinline__ void get4(const float (&a)[8][4], bool hi, float (&b)[4][4]) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) b[i][j] = hi ? a[4 + i][j] : a[i][j];
+// group-local barrier (named barrier id, nthreads of the group)
+__device__ __forceinline__ void group_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
 }
-__device__ __forceinline__ void put4(float (&a)[8][4], bool hi, const float (&b)[4][4]) {
+
+// C = A B (MODE 0), C = -A B (MODE 1), C -= A B (MODE 2) for H x H blocks (stride kS), by the NT
+// threads t of a group.  C may alias A or B: every thread's products are finished (group barrier
+// bar) before any is stored.  bar < 0: no aliasing, no barrier.
+template <int H, int NT, int MODE>
+__device__ __forceinline__ void small_mm(const float* A, const float* B, float* C, int t, int bar) {
+  constexpr int OUT = H * H / NT;
+  constexpr int TR = OUT >= 4 ? 4 : OUT;
+  constexpr int TC = OUT / TR;
+  constexpr int RG = H / TR;
+  const int r0 = (t % RG) * TR, c0 = (t / RG) * TC;
+  float acc[TR][TC];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < TR; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      a[i][j] = hi ? a[i][j] : b[i][j];
-      a[4 + i][j] = hi ? b[i][j] : a[4 + i][j];
+    for (int j = 0; j < TC; ++j) acc[i][j] = 0.f;
+#pragma unroll 8
+  for (int k = 0; k < H; ++k) {
+    float a[TR], b[TC];
+    if constexpr (TR == 4) {
+      const float4 v = *reinterpret_cast<const float4*>(A + k * kS + r0);
+      a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < TR; ++i) a[i] = A[k * kS + r0 + i];
     }
+#pragma unroll
+    for (int j = 0; j < TC; ++j) b[j] = B[(c0 + j) * kS + k];
+#pragma unroll
+    for (int i = 0; i < TR; ++i)
+#pragma unroll
+      for (int j = 0; j < TC; ++j) acc[i][j] += a[i] * b[j];
+  }
+  if (bar >= 0) group_bar(bar, NT);
+#pragma unroll
+  for (int i = 0; i < TR; ++i)
+#pragma unroll
+    for (int j = 0; j < TC; ++j) {
+      float* c = C + (c0 + j) * kS + r0 + i;
+      if constexpr (MODE == 0) *c = acc[i][j];
+      if constexpr (MODE == 1) *c = -acc[i][j];
+      if constexpr (MODE == 2) *c -= acc[i][j];
+    }
+}
+
+// The 32 x 32 diagonal block at (o, o): LU by warp 0, then L^-1 by warp 0 and U^-1 by warp 1.
+// Called by all threads (it ends with a block barrier).
+__device__ __noinline__ void leaf_base32(float* M, float* LI, float* UI, int o, int* bad) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) {
+    float r[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) r[j] = M[(o + j) * kS + o + lane];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const float ukk = __shfl_sync(0xffffffffu, r[k], k);
+      if (lane == 0 && !(ukk != 0.f && isfinite(ukk))) *bad = 1;
+      const float l = r[k] * (1.0f / ukk);
+      if (lane > k) r[k] = l;
+#pragma unroll
+      for (int j = k + 1; j < 32; ++j) {
+        const float ukj = __shfl_sync(0xffffffffu, r[j], k);
+        if (lane > k) r[j] -= l * ukj;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) M[(o + j) * kS + o + lane] = r[j];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // column c = lane of L^-1: x_c = 1, x_i = -sum_{j < i} L_ij x_j (x_j = 0 for j < c)
+    float x[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      float sum = 0.f;
+#pragma unroll
+      for (int j = 0; j < i; ++j) sum += M[(o + j) * kS + o + i] * x[j];
+      x[i] = (i == lane) ? 1.f : (i > lane ? -sum : 0.f);
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) LI[(o + lane) * kS + o + i] = x[i];
+  } else if (warp == 1) {
+    // column c = lane of U^-1: x_i = (delta_ic - sum_{j > i} U_ij x_j) / U_ii, i = 31 .. 0
+    float x[32];
+#pragma unroll
+    for (int i = 31; i >= 0; --i) {
+      float sum = 0.f;
+#pragma unroll
+      for (int j = i + 1; j < 32; ++j) sum += M[(o + j) * kS + o + i] * x[j];
+      x[i] = ((i == lane ? 1.f : 0.f) - sum) / M[(o + i) * kS + o + i];
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) UI[(o + lane) * kS + o + i] = x[i];
+  }
+  __syncthreads();
+}
+
+// One level of the recursion: the H x H diagonal block at (o, o) from its two halves (h = H / 2).
+// Thread groups: warps 0-7 (id 1) and 8-15 (id 2), 256 threads each.
+template <int H>
+__device__ __forceinline__ void leaf_level(float* M, float* LI, float* UI, int o, int* bad) {
+  constexpr int h = H / 2;
+  if constexpr (h == 32) {
+    leaf_base32(M, LI, UI, o, bad);
+  } else {
+    leaf_level<h>(M, LI, UI, o, bad);
+  }
+  const int tid = threadIdx.x, grp = tid >> 8, t = tid & 255;
+  const int p = o + h;  // second half
+  float* M11 = M + o * kS + o;
+  float* M12 = M + p * kS + o;
+  float* M21 = M + o * kS + p;
+  float* M22 = M + p * kS + p;
+  // U12 = LI11 D12 (group 1), L21 = D21 UI11 (group 2), in place
+  if (grp == 0)
+    small_mm<h, 256, 0>(LI + o * kS + o, M12, M12, t, 1);
+  else
+    small_mm<h, 256, 0>(M21, UI + o * kS + o, M21, t, 2);
+  __syncthreads();
+  small_mm<h, 512, 2>(M21, M12, M22, tid, -1);  // D22 -= L21 U12
+  __syncthreads();
+  if constexpr (h == 32) {
+    leaf_base32(M, LI, UI, p, bad);
+  } else {
+    leaf_level<h>(M, LI, UI, p, bad);
+  }
+  // LI21 = -LI22 (L21 LI11) (group 1), UI12 = -(UI11 U12) UI22 (group 2)
+  float* LI21 = LI + o * kS + p;
+  float* UI12 = UI + p * kS + o;
+  if (grp == 0) {
+    small_mm<h, 256, 0>(M21, LI + o * kS + o, LI21, t, -1);
+    group_bar(1, 256);
+    small_mm<h, 256, 1>(LI + p * kS + p, LI21, LI21, t, 1);
+  } else {
+    small_mm<h, 256, 0>(UI + o * kS + o, M12, UI12, t, -1);
+    group_bar(2, 256);
+    small_mm<h, 256, 1>(UI12, UI + p * kS + p, UI12, t, 2);
+  }
+  __syncthreads();
+  (void)M11;
 }
 
 __global__ void __launch_bounds__(512, 1) k_lu32_leaf_inv(float* __restrict__ A, long lda, int h, float* __restrict__ DL,
                                                            float* __restrict__ DU, int* status,
                                                            unsigned long long* stamp) {
   stamp_begin(stamp);
-  extern __shared__ float sm[];
-  float* d = sm;                     // d[c * kLdS + r] = block entry (r, c)
-  float* ub = sm + 128 * kLdS;       // [2][4][128]: the 4 rows of U of a step (then rows of X)
-  float* db = ub + 2 * 4 * 128;      // [2][20]: the factored 4 x 4 diagonal block, row-major, and
-                                     // the reciprocals of its 4 pivots
-  float* yb = db + 2 * 20;           // [2][4][128]: rows of U^-1 of an inverse step
-  float* rdiag = yb + 2 * 4 * 128;   // [128]: reciprocals of the pivots
+  extern __shared__ __align__(16) float sm[];
+  float* M = sm;
+  float* LI = sm + 128 * kS;
+  float* UI = sm + 2 * 128 * kS;
   __shared__ int s_bad;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int r0 = 8 * warp, c0 = 4 * lane;
+  if (tid == 0) s_bad = 0;
   if (h == 128) {
-    // full block: one float4 per lane per column, all 8 loads in flight
     float4 v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = *reinterpret_cast<const float4*>(A + (size_t)(warp + 16 * q) * lda + 4 * lane);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      float* dc = d + (warp + 16 * q) * kLdS + 4 * lane;
-      dc[0] = v[q].x, dc[1] = v[q].y, dc[2] = v[q].z, dc[3] = v[q].w;
-    }
+    for (int q = 0; q < 8; ++q) *reinterpret_cast<float4*>(M + (warp + 16 * q) * kS + 4 * lane) = v[q];
   } else {
     for (int c = warp; c < 128; c += 16)
       for (int r = lane; r < 128; r += 32)
-        d[c * kLdS + r] = (r < h && c < h) ? A[(size_t)c * lda + r] : (r == c ? 1.f : 0.f);
+        M[c * kS + r] = (r < h && c < h) ? A[(size_t)c * lda + r] : (r == c ? 1.f : 0.f);
   }
-  if (tid == 0) s_bad = 0;
+  // LI and UI start at zero (the blocks above / below their diagonals stay zero)
+  for (int e = tid; e < 2 * 128 * kS / 4; e += 512) reinterpret_cast<float4*>(LI)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
-  float a[8][4];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) a[i][j] = d[(c0 + j) * kLdS + r0 + i];
-#pragma unroll 1
-  for (int K = 0; K < 32; ++K) {
-    const int k = 4 * K, par = K & 1;
-    const bool hi = K & 1;  // the step's rows are rows 4..7 of the owning warp's tile
-    float* ubp = ub + par * 4 * 128;
-    float* dbp = db + par * 20;
-    if (warp == (K >> 1)) {
-      // the 4 x 4 diagonal block (lane K), factored, its L passed to the warp
-      float D[4][4];
-      get4(a, hi, D);
-      if (lane == K) {
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const float p = D[t][t];
-          if (!(p != 0.f && isfinite(p))) s_bad = 1;
-          const float rp = 1.0f / p;
-          dbp[16 + t] = rp;
-          rdiag[k + t] = rp;
-#pragma unroll
-          for (int r = t + 1; r < 4; ++r) {
-            D[r][t] *= rp;
-#pragma unroll
-            for (int c = t + 1; c < 4; ++c) D[r][c] -= D[r][t] * D[t][c];
-          }
-        }
-        put4(a, hi, D);
-#pragma unroll
-        for (int e = 0; e < 16; ++e) dbp[e] = D[e >> 2][e & 3];
-      }
-      float l10 = __shfl_sync(0xffffffffu, D[1][0], K), l20 = __shfl_sync(0xffffffffu, D[2][0], K);
-      float l21 = __shfl_sync(0xffffffffu, D[2][1], K), l30 = __shfl_sync(0xffffffffu, D[3][0], K);
-      float l31 = __shfl_sync(0xffffffffu, D[3][1], K), l32 = __shfl_sync(0xffffffffu, D[3][2], K);
-      if (lane > K) {
-        // U rows k..k+3 in this lane's columns: U = L_D^-1 A
-        float U[4][4];
-        get4(a, hi, U);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          U[1][j] -= l10 * U[0][j];
-          U[2][j] -= l20 * U[0][j] + l21 * U[1][j];
-          U[3][j] -= l30 * U[0][j] + l31 * U[1][j] + l32 * U[2][j];
-        }
-        put4(a, hi, U);
-#pragma unroll
-        for (int t = 0; t < 4; ++t)
-          *reinterpret_cast<float4*>(&ubp[t * 128 + c0]) = make_float4(U[t][0], U[t][1], U[t][2], U[t][3]);
-      }
-    }
-    __syncthreads();
-    if (r0 + 7 > k + 3) {
-      // rows below the block: lane K forms their 4 columns of L (only rows > k + 3), then the
-      // rank-4 update of every column right of the block
-      float l[8][4];
-      if (lane == K) {
-        float Ud[4][4], rp[4];
-#pragma unroll
-        for (int e = 0; e < 16; ++e) Ud[e >> 2][e & 3] = dbp[e];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) rp[t] = dbp[16 + t];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const bool below = r0 + i > k + 3;
-          float x0 = a[i][0], x1 = a[i][1], x2 = a[i][2], x3 = a[i][3];
-          x0 = x0 * rp[0];
-          x1 = (x1 - x0 * Ud[0][1]) * rp[1];
-          x2 = (x2 - x0 * Ud[0][2] - x1 * Ud[1][2]) * rp[2];
-          x3 = (x3 - x0 * Ud[0][3] - x1 * Ud[1][3] - x2 * Ud[2][3]) * rp[3];
-          a[i][0] = below ? x0 : a[i][0];
-          a[i][1] = below ? x1 : a[i][1];
-          a[i][2] = below ? x2 : a[i][2];
-          a[i][3] = below ? x3 : a[i][3];
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const float v = __shfl_sync(0xffffffffu, a[i][t], K);
-          l[i][t] = (r0 + i > k + 3) ? v : 0.f;
-        }
-      if (lane > K) {
-        float4 u[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) u[t] = *reinterpret_cast<const float4*>(&ubp[t * 128 + c0]);
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            a[i][0] -= l[i][t] * u[t].x;
-            a[i][1] -= l[i][t] * u[t].y;
-            a[i][2] -= l[i][t] * u[t].z;
-            a[i][3] -= l[i][t] * u[t].w;
-          }
-      }
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) d[(c0 + j) * kLdS + r0 + i] = a[i][j];
-  __syncthreads();
+  leaf_level<128>(M, LI, UI, 0, &s_bad);
   if (h == 128) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float* dc = d + (warp + 16 * q) * kLdS + 4 * lane;
-      *reinterpret_cast<float4*>(A + (size_t)(warp + 16 * q) * lda + 4 * lane) = make_float4(dc[0], dc[1], dc[2], dc[3]);
-    }
+    for (int q = 0; q < 8; ++q)
+      *reinterpret_cast<float4*>(A + (size_t)(warp + 16 * q) * lda + 4 * lane) =
+          *reinterpret_cast<const float4*>(M + (warp + 16 * q) * kS + 4 * lane);
   } else {
     for (int c = warp; c < h; c += 16)
-      for (int r = lane; r < h; r += 32) A[(size_t)c * lda + r] = d[c * kLdS + r];
+      for (int r = lane; r < h; r += 32) A[(size_t)c * lda + r] = M[c * kS + r];
   }
-  // inverses, 4 rows per step: X = L^-1 forward (step s: rows 4s..4s+3), Y = U^-1 backward
-  // (rows 4(31-s)..+3); the owning warp finishes its 4 rows by substitution within the 4 x 4
-  // diagonal block, publishes them, and the warps of the other rows apply the rank-4 update
-  float x[8][4], y[8][4];
+  // L^-1 and U^-1, 128 x 128 column-major, zero outside h x h
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) x[i][j] = y[i][j] = (r0 + i == c0 + j) ? 1.f : 0.f;
-#pragma unroll 1
-  for (int st = 0; st < 32; ++st) {
-    const int KL = st, KU = 31 - st, kl = 4 * KL, ku = 4 * KU, par = st & 1;
-    float* xb = ub + par * 4 * 128;
-    float* ybp = yb + par * 4 * 128;
-    if (warp == (KL >> 1)) {
-      const bool hi = KL & 1;
-      float X[4][4];
-      get4(x, hi, X);
-      const float l10 = d[kl * kLdS + kl + 1], l20 = d[kl * kLdS + kl + 2], l30 = d[kl * kLdS + kl + 3];
-      const float l21 = d[(kl + 1) * kLdS + kl + 2], l31 = d[(kl + 1) * kLdS + kl + 3];
-      const float l32 = d[(kl + 2) * kLdS + kl + 3];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        X[1][j] -= l10 * X[0][j];
-        X[2][j] -= l20 * X[0][j] + l21 * X[1][j];
-        X[3][j] -= l30 * X[0][j] + l31 * X[1][j] + l32 * X[2][j];
-      }
-      put4(x, hi, X);
-#pragma unroll
-      for (int t = 0; t < 4; ++t)
-        *reinterpret_cast<float4*>(&xb[t * 128 + c0]) = make_float4(X[t][0], X[t][1], X[t][2], X[t][3]);
+  for (int q = 0; q < 8; ++q) {
+    const int c = warp + 16 * q, r = 4 * lane;
+    float4 l = *reinterpret_cast<const float4*>(LI + c * kS + r);
+    float4 u = *reinterpret_cast<const float4*>(UI + c * kS + r);
+    if (h < 128) {
+      const bool cin = c < h;
+      l.x = (cin && r < h) ? l.x : 0.f, l.y = (cin && r + 1 < h) ? l.y : 0.f;
+      l.z = (cin && r + 2 < h) ? l.z : 0.f, l.w = (cin && r + 3 < h) ? l.w : 0.f;
+      u.x = (cin && r < h) ? u.x : 0.f, u.y = (cin && r + 1 < h) ? u.y : 0.f;
+      u.z = (cin && r + 2 < h) ? u.z : 0.f, u.w = (cin && r + 3 < h) ? u.w : 0.f;
     }
-    if (warp == (KU >> 1)) {
-      const bool hi = KU & 1;
-      float Y[4][4];
-      get4(y, hi, Y);
-      float U[4][4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) U[r][c] = d[(ku + c) * kLdS + ku + r];
-      const float q0 = rdiag[ku], q1 = rdiag[ku + 1], q2 = rdiag[ku + 2], q3 = rdiag[ku + 3];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        Y[3][j] = Y[3][j] * q3;
-        Y[2][j] = (Y[2][j] - U[2][3] * Y[3][j]) * q2;
-        Y[1][j] = (Y[1][j] - U[1][2] * Y[2][j] - U[1][3] * Y[3][j]) * q1;
-        Y[0][j] = (Y[0][j] - U[0][1] * Y[1][j] - U[0][2] * Y[2][j] - U[0][3] * Y[3][j]) * q0;
-      }
-      put4(y, hi, Y);
-#pragma unroll
-      for (int t = 0; t < 4; ++t)
-        *reinterpret_cast<float4*>(&ybp[t * 128 + c0]) = make_float4(Y[t][0], Y[t][1], Y[t][2], Y[t][3]);
-    }
-    __syncthreads();
-    if (r0 + 7 > kl + 3) {
-      float4 xr[4];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) xr[t] = *reinterpret_cast<const float4*>(&xb[t * 128 + c0]);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int r = r0 + i;
-        if (r > kl + 3) {
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const float lc = d[(kl + t) * kLdS + r];
-            x[i][0] -= lc * xr[t].x;
-            x[i][1] -= lc * xr[t].y;
-            x[i][2] -= lc * xr[t].z;
-            x[i][3] -= lc * xr[t].w;
-          }
-        }
-      }
-    }
-    if (r0 < ku) {
-      float4 yr[4];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) yr[t] = *reinterpret_cast<const float4*>(&ybp[t * 128 + c0]);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int r = r0 + i;
-        if (r < ku) {
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const float uc = d[(ku + t) * kLdS + r];
-            y[i][0] -= uc * yr[t].x;
-            y[i][1] -= uc * yr[t].y;
-            y[i][2] -= uc * yr[t].z;
-            y[i][3] -= uc * yr[t].w;
-          }
-        }
-      }
-    }
+    *reinterpret_cast<float4*>(DL + (size_t)c * 128 + r) = l;
+    *reinterpret_cast<float4*>(DU + (size_t)c * 128 + r) = u;
   }
-  // L^-1 and U^-1 through shared memory, so each column goes out as 32 float4 stores
-#pragma unroll 1
-  for (int pass = 0; pass < 2; ++pass) {
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const bool in = r0 + i < h && c0 + j < h;
-        d[(c0 + j) * kLdS + r0 + i] = in ? (pass ? y[i][j] : x[i][j]) : 0.f;
-      }
-    __syncthreads();
-    float* D = pass ? DU : DL;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float* dc = d + (warp + 16 * q) * kLdS + 4 * lane;
-      *reinterpret_cast<float4*>(D + (size_t)(warp + 16 * q) * 128 + 4 * lane) = make_float4(dc[0], dc[1], dc[2], dc[3]);
-    }
-  }
+  __syncthreads();
   if (tid == 0 && s_bad) atomicExch(status, kZeroPivot);
   stamp_end(stamp);
 }
@@ -1079,7 +1001,7 @@ struct MixedSolver::Impl {
   // inverted (both triangles) right after it is factored, for the triangular-solve leaves above it
   void rlu(int k0, int sz, cudaStream_t s) {
     if (sz <= kLeaf) {
-      const size_t smem = (size_t)(128 * kLdS + 2 * 4 * 128 + 2 * 20 + 2 * 4 * 128 + 128) * sizeof(float);
+      const size_t smem = (size_t)3 * 128 * kS * sizeof(float);
       const size_t off = (size_t)(k0 / kLeaf) * kLeaf * kLeaf;
       prof.begin("LU leaf + inverses", 0, s);
       k_lu32_leaf_inv<<<1, 512, smem, s>>>(at_(k0, k0), ld32, sz, dl32.as<float>() + off, du32.as<float>() + off,
@@ -1141,6 +1063,20 @@ struct MixedSolver::Impl {
     return h;
   }
 };
+
+cudaError_t lu32_leaf(float* A, long lda, int h, float* DL, float* DU, int* status, cudaStream_t s) {
+  if (h <= 0 || h > 128 || lda < h) return cudaErrorInvalidValue;
+  static bool attr = false;
+  const size_t smem = (size_t)3 * 128 * kS * sizeof(float);
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_lu32_leaf_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_lu32_leaf_inv<<<1, 512, smem, s>>>(A, lda, h, DL, DU, status, nullptr);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
 
 std::vector<std::string> MixedSolver::profile_report() {
   std::vector<std::string> out = p_->prof.report();

@@ -22,6 +22,11 @@ struct MixedReport {
   double relres = 0.0;  // largest relative residual ||b - A x|| / ||b|| over the right-hand sides
 };
 
+// The mixed LU's diagonal leaf on one h x h block (h <= 128) of A (column-major, lda): LU without
+// pivoting in place, L^-1 into DL and U^-1 into DU (128 x 128 column-major each, zero outside h x h).
+// A zero or non-finite pivot sets *status to a nonzero code.
+cudaError_t lu32_leaf(float* A, long lda, int h, float* DL, float* DU, int* status, cudaStream_t s);
+
 class MixedSolver {
  public:
   MixedSolver();

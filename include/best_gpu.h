@@ -100,6 +100,12 @@ int bgpu_create_from_triangles(int n, const double *tri, int iarea, double truea
 int bgpu_build_prepared(double eps, int direct, int single, int nrhs);
 int bgpu_prepared_arrays(double *v1, double *v2, double *v3, double *area, int *icomp, double *xmu, double *gdef);
 
+/* The mixed-precision LU's diagonal leaf (FP32, device memory): the h x h block d_a (h <= 128,
+ * column-major, lda) factored without pivoting in place (unit L below, U on and above the diagonal),
+ * L^-1 into d_linv and U^-1 into d_uinv (128 x 128 column-major each, zero outside h x h).  A zero
+ * or non-finite pivot is an error. */
+int bgpu_lu32_leaf_device(int h, float *d_a, int lda, float *d_linv, float *d_uinv);
+
 /* Assembles GR rows of triangles [r0, r1) x columns of triangles [c0, c1) of the mesh given to
  * bhm_create into d_out (column-major, ldo), before deflation (best/tgetgr.f:33-173). */
 int bgpu_assemble_device(int r0, int r1, int c0, int c1, double *d_out, int ldo);

@@ -40,6 +40,35 @@ def test_tc_gemm_bf16(m, n, k):
     assert err < 1e-6, err
 
 
+@pytest.mark.parametrize("h", [128, 100, 42, 1])
+def test_lu32_leaf(h):
+    """The mixed LU's diagonal leaf: L U = A, L L^-1 = I and U U^-1 = I to FP32 accuracy (2e-5 of
+    the scales, computed in FP64 from the FP32 results), the inverses zero outside h x h, and the
+    padded block (ragged last leaf) handled."""
+    torch = _torch()
+    rng = np.random.default_rng(h)
+    lda = 132
+    A = np.zeros((lda, h), dtype=np.float32)  # column-major h x h with leading dimension lda: A[:h].T
+    A[:h, :h] = (rng.standard_normal((h, h)) + 2.0 * np.sqrt(h) * np.eye(h)).astype(np.float32)
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    dL = torch.full((128, 128), 7.0, dtype=torch.float32, device="cuda")
+    dU = torch.full((128, 128), 7.0, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    bh.lu32_leaf_device(h, dA.data_ptr(), lda, dL.data_ptr(), dU.data_ptr())
+    out = dA.cpu().numpy().T[:h, :h].astype(np.float64)
+    LI = dL.cpu().numpy().T.astype(np.float64)  # column-major 128 x 128
+    UI = dU.cpu().numpy().T.astype(np.float64)
+    L = np.tril(out, -1) + np.eye(h)
+    U = np.triu(out)
+    A64 = A[:h, :h].astype(np.float64)
+    assert np.max(np.abs(L @ U - A64)) / np.max(np.abs(A64)) < 2e-5
+    assert np.max(np.abs(L @ LI[:h, :h] - np.eye(h))) < 2e-5
+    assert np.max(np.abs(U @ UI[:h, :h] - np.eye(h))) < 2e-5
+    assert np.all(np.diag(LI[:h, :h]) == 1)
+    assert np.all(np.triu(LI[:h, :h], 1) == 0) and np.all(np.tril(UI[:h, :h], -1) == 0)
+    assert np.all(LI[h:, :] == 0) and np.all(LI[:, h:] == 0) and np.all(UI[h:, :] == 0) and np.all(UI[:, h:] == 0)
+
+
 def compare(g, o, tol=TOL):
     for key in ("Dtt", "Drr"):
         assert rel(g["tensors"][key], o.tensors[key]) < tol, key
