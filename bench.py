@@ -727,22 +727,54 @@ def series_record(steps, warmup, local_rank=0, sequential_passes=1):
         seq.append(time.perf_counter() - t0)
         seq_sols = out
     same = all(np.array_equal(a.view(np.int64), b.view(np.int64)) for a, b in zip(sols, seq_sols))
-    per = []
-    for st, x, B in zip(setups, xs, sols):
-        tr = bh.traces(bh.difco(x, st.area, B[:, :6]))
-        chip, _ = bh.visco(x, st.area, B[:, 6:], B[:, :6])
-        per.append(dict(N=st.n, D_t=tr["DTRANS"], D_r=tr["DR"], chiprime=chip))
+
+    def results(solutions):
+        out = []
+        for st, x, B in zip(setups, xs, solutions):
+            tr = bh.traces(bh.difco(x, st.area, B[:, :6]))
+            chip, _ = bh.visco(x, st.area, B[:, 6:], B[:, :6])
+            out.append(dict(N=st.n, D_t=tr["DTRANS"], D_r=tr["DR"], chiprime=chip))
+        return out
+
+    per = results(sols)
     ns = [d["N"] for d in per]
     ext = {k: bh.extrapolate(ns, [d[k] for d in per])[0] for k in ("D_t", "D_r", "chiprime")}
     v = float(np.median(times))
     S.destroy()
+    # the same series with every mesh's factorisation on the tensor cores, side by side
+    mixed = None
+    try:
+        M = bh.Series()
+        M.create(setups)
+        M.set_precision(bh.BGPU_MIXED)
+        M.build(defl)  # warm-up: allocations and graph captures
+        mt = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            M.build(defl)
+            msols = M.solve(rhs)
+            mt.append(time.perf_counter() - t0)
+        mdev = M.timings()
+        mper = results(msols)
+        mext = {k: bh.extrapolate(ns, [d[k] for d in mper])[0] for k in ("D_t", "D_r", "chiprime")}
+        errs = {k: max(abs(a[k] / b[k] - 1) for a, b in zip(mper, per)) for k in ("D_t", "D_r", "chiprime")}
+        mv = float(np.median(mt))
+        mixed = {"value": mv, "unit": "s", "device_ms": {"build": mdev["build"], "solve": mdev["solve"]},
+                 "speedup_vs_sequential": float(np.median(seq)) / mv,
+                 "max_rel_err_vs_fp64_per_mesh": errs,
+                 "extrapolated_rel_err_vs_fp64": {k: abs(mext[k] / ext[k] - 1) for k in ext},
+                 "log": [ln for ln in bh.log_lines() if "series" in ln][-1:]}
+        M.destroy()
+    except Exception as e:
+        mixed = {"error": f"{type(e).__name__}: {e}"}
     bh.set_precision(-1)
     return {
         "value": v, "unit": "s", "steps": steps, "warmup": warmup, "N": ns,
         "device_ms": {"build_graph": dev_ms["build"], "solve": dev_ms["solve"], "tuning_pass": tune_ms},
         "sequential_single_solves_s": float(np.median(seq)), "speedup_vs_sequential": float(np.median(seq)) / v,
         "bitwise_equal_to_single_solves": bool(same), "clocks": clocks, "gpu_launches": launches,
-        "per_mesh": per, "extrapolated_1_over_N": ext, "autotune": bh.autotune_table(),
+        "per_mesh": per, "extrapolated_1_over_N": ext, "autotune": bh.autotune_table(), "mixed_series": mixed,
     }
 
 

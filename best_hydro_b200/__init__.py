@@ -69,6 +69,7 @@ _SIGS = {
     "bgpu_series_solve": (ctypes.c_int, [ctypes.c_int, _dp]),
     "bgpu_series_timings": (ctypes.c_int, [_dp, ctypes.c_int]),
     "bgpu_series_destroy": (None, []),
+    "bgpu_series_set_precision": (ctypes.c_int, [ctypes.c_int]),
     "bgpu_autotune_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "bgpu_best_gradient": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
     "bgpu_lu32_leaf_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
@@ -399,6 +400,11 @@ class Series:
             o += m
         return out
 
+    def set_precision(self, mode):
+        """bgpu_series_set_precision: BGPU_FP64 (batched FP64 LU) or BGPU_MIXED (per-mesh tensor-core
+        factorisations side by side, FP64 GMRES-IR) for the next build."""
+        _check(self.L.bgpu_series_set_precision(int(mode)), "bgpu_series_set_precision")
+
     def timings(self):
         v = np.zeros(4)
         self.L.bgpu_series_timings(_p(v), 4)
@@ -416,11 +422,14 @@ def autotune_table():
     return [ln for ln in buf.value.decode().split("\n") if ln]
 
 
-def series_run(setups, tune=0, ivisco=1, cg=1.0):
+def series_run(setups, tune=0, ivisco=1, cg=1.0, precision=None):
     """BEST on every mesh of a series through bgpu_series_*: per mesh D_t, D_r, CHI' (11 right-hand
-    sides with ivisco), then their linear extrapolation in 1/N.  Returns (per-mesh list, extrapolated)."""
+    sides with ivisco), then their linear extrapolation in 1/N.  precision: None (FP64) or BGPU_MIXED.
+    Returns (per-mesh list, extrapolated)."""
     S = Series()
     S.create(setups, cg)
+    if precision is not None:
+        S.set_precision(precision)
     xs = S.incenters()
     dms = S.diag_means()
     defl = []

@@ -337,8 +337,17 @@ struct Series {
   unsigned long long graph_kernels = 0;
   bool graph_tried = false, factored = false;
   double ms[4] = {};  // build (graph), of which assembly; last solve; tuning pass
+  // BGPU_MIXED (bgpu_series_set_precision): each mesh's BF16 tensor-core factorisation on a stream
+  // of its own, all enqueued before any is waited for; FP64 GMRES-IR solves
+  int precision = BGPU_FP64;
+  int built_precision = BGPU_FP64;
+  std::vector<std::unique_ptr<MixedSolver>> mixed;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> ev_done;
   ~Series() {
     if (graph) cudaGraphExecDestroy(graph);
+    for (cudaStream_t q : streams) cudaStreamDestroy(q);
+    for (cudaEvent_t e : ev_done) cudaEventDestroy(e);
   }
   DevMesh mesh(int i) const {
     DevMesh m;
@@ -393,6 +402,43 @@ void series_record(Series& S, Runtime& r, cudaStream_t st, cudaEvent_t ev_assemb
                        S.du.as<double>() + S.inv0[i], st),
        "diagonal inverses");
   }
+}
+
+// The mixed-precision series build: every mesh's assembly and BF16 tensor-core factorisation
+// enqueued on its own stream (after the deflation uploads on the runtime stream), then all waited
+// for.  Throws MixedFailure when a mesh cannot be factored without pivoting.
+void series_build_mixed(Series& S, Runtime& r) {
+  if ((int)S.mixed.size() != S.count) {
+    S.mixed.clear();
+    for (int i = 0; i < S.count; ++i) S.mixed.push_back(std::make_unique<MixedSolver>());
+  }
+  while ((int)S.streams.size() < S.count) {
+    cudaStream_t q;
+    cudaEvent_t e;
+    ck(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking), "series stream");
+    ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "series event");
+    S.streams.push_back(q);
+    S.ev_done.push_back(e);
+  }
+  ck(cudaEventRecord(r.ev[2], r.stream), "event");
+  for (int i = 0; i < S.count; ++i) {
+    DevDeflation d;
+    if (S.ndef[i] >= 1) {
+      d.ndef = S.ndef[i];
+      d.gdef = S.gdef.as<double>() + S.gdef0[i];
+      d.xmu = S.xmu.as<double>() + 3 * S.t0[i];
+      if (S.ndef[i] > 1) d.comp = S.comp.as<int>() + S.t0[i];
+    }
+    ck(cudaStreamWaitEvent(S.streams[i], r.ev[2], 0), "series fork");
+    S.mixed[i]->set_refinement(g_refine[0], g_refine[1]);
+    S.mixed[i]->build(S.mesh(i), d, S.gr.as<double>() + S.gr0[i], S.ld[i], 1e-10, S.streams[i], S.ev_done[i],
+                      S.ev_done[i], false);
+  }
+  for (int i = 0; i < S.count; ++i) {
+    S.mixed[i]->finish_build(S.streams[i]);
+    ck(cudaStreamWaitEvent(r.stream, S.ev_done[i], 0), "series join");
+  }
+  ck(cudaEventRecord(r.ev[4], r.stream), "event");
 }
 
 // Assembly (with the deflation defl, on the device), factorisation and the host-side report: the
@@ -880,6 +926,23 @@ int bgpu_series_build(const int* ndef, const double* gdef, const int* comp, cons
       S.perm.ensure(sizeof(int) * 3 * tot, "permutations");
       S.info.ensure(sizeof(int) * kMaxSeries, "info", true);
     }
+    if (S.precision == BGPU_MIXED) {
+      try {
+        series_build_mixed(S, r);
+        r.sync("bgpu_series_build");
+        S.ms[0] = r.elapsed(2, 4);
+        S.ms[1] = 0;
+        S.built_precision = BGPU_MIXED;
+        S.factored = true;
+        note("GPU series build: %d meshes (N = %d .. %d), mixed precision (BF16 tensor-core LU per mesh, one stream "
+             "each), %.1f ms", S.count, *std::min_element(S.n.begin(), S.n.end()),
+             *std::max_element(S.n.begin(), S.n.end()), S.ms[0]);
+        return 0;
+      } catch (const MixedFailure& e) {
+        note("series, mixed precision: %s; building the FP64 series instead", e.what());
+      }
+    }
+    S.built_precision = BGPU_FP64;
     ck(lu_prepare(), "LU kernel attributes");
     if (tune) {
       // a first build with the DGEMM autotuner on (direct launches; the result is overwritten below)
@@ -974,6 +1037,23 @@ int bgpu_series_solve(int nrhs, double* b) {
     S.rhs.ensure((size_t)rows * nrhs * sizeof(double), "series right-hand sides");
     ck(cudaMemcpyAsync(S.rhs.p, b, (size_t)rows * nrhs * sizeof(double), cudaMemcpyHostToDevice, r.stream), "b copy");
     ck(cudaEventRecord(r.ev[5], r.stream), "event");
+    if (S.built_precision == BGPU_MIXED) {
+      MixedReport rep;
+      for (int i = 0; i < S.count; ++i) {
+        double* bi = S.rhs.as<double>() + (size_t)3 * S.t0[i] * nrhs;
+        ck(cudaEventRecord(r.ev[7], r.stream), "event");
+        ck(cudaStreamWaitEvent(S.streams[i], r.ev[7], 0), "series fork");
+        S.mixed[i]->solve(nrhs, bi, 3L * S.n[i], S.streams[i], &rep);
+        ck(cudaEventRecord(S.ev_done[i], S.streams[i]), "event");
+        ck(cudaStreamWaitEvent(r.stream, S.ev_done[i], 0), "series join");
+      }
+      ck(cudaEventRecord(r.ev[6], r.stream), "event");
+      ck(cudaMemcpyAsync(b, S.rhs.p, (size_t)rows * nrhs * sizeof(double), cudaMemcpyDeviceToHost, r.stream),
+         "x copy");
+      r.check_status("bgpu_series_solve");
+      S.ms[2] = r.elapsed(5, 6);
+      return 0;
+    }
     long maxn = 0;
     for (int i = 0; i < S.count; ++i) maxn = std::max<long>(maxn, 3L * S.n[i]);
     r.ensure_trsv((int)maxn);
@@ -1002,6 +1082,18 @@ int bgpu_series_timings(double* ms, int len) {
   const int k = std::min(len, 4);
   for (int i = 0; i < k; ++i) ms[i] = g_series->ms[i];
   return k;
+}
+
+int bgpu_series_set_precision(int mode) {
+  return status_of([&] {
+    Series& S = series();
+    if (mode != BGPU_FP64 && mode != BGPU_MIXED) {
+      note("error: bgpu_series_set_precision: mode %d is neither BGPU_FP64 nor BGPU_MIXED", mode);
+      return 1;
+    }
+    S.precision = mode;
+    return 0;
+  });
 }
 
 void bgpu_series_destroy(void) { g_series.reset(); }

@@ -857,6 +857,8 @@ struct MixedSolver::Impl {
   // per-launch device stamps of the GEMMs (live timing that works inside the graph): slots taken in
   // launch order as the recursion runs (or is captured), with each launch's flops
   std::string host_note;  // host-side times of the last build (allocations, graph capture)
+  int used_slots = 0;     // GEMM stamp slots and work of the last build
+  double used_work = 0;
   Buf stamps;
   int slot_cap = 0, nslots = 0;
   double slot_work = 0;  // GEMM flops
@@ -1108,7 +1110,7 @@ void MixedSolver::set_refinement(int max_restarts, int krylov) {
 const char* MixedSolver::name() const { return "BF16 tensor-core (FP32 factors) + FP64 GMRES-IR"; }
 
 void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, long ld, double eps, cudaStream_t s,
-                        cudaEvent_t ev_assembled, cudaEvent_t ev_factored) {
+                        cudaEvent_t ev_assembled, cudaEvent_t ev_factored, bool wait) {
   Impl& P = *p_;
   using clk = std::chrono::steady_clock;
   const auto ms_since = [](clk::time_point t) {
@@ -1260,17 +1262,28 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     used_work = P.graph_work;
   }
   ck(cudaEventRecord(ev_factored, s), "event");
-  int st = 0;
-  ck(cudaMemcpyAsync(&st, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
-  ck(cudaStreamSynchronize(s), "factorisation");
+  P.used_slots = used_slots;
+  P.used_work = used_work;
   {
     char note[256];
     std::snprintf(note, sizeof note,
                   "mixed build, host side: allocations %.1f ms, graph capture %.1f ms, instantiation %.1f ms, "
-                  "whole call %.1f ms",
+                  "enqueue %.1f ms",
                   ms_alloc, ms_capture, ms_inst, ms_since(t_begin));
     P.host_note = note;
   }
+  if (wait) finish_build(s);
+}
+
+void MixedSolver::finish_build(cudaStream_t s) {
+  Impl& P = *p_;
+  // (the status is read after the wait: a copy to pageable host memory would block the enqueue)
+  ck(cudaStreamSynchronize(s), "factorisation");
+  int st = 0;
+  ck(cudaMemcpyAsync(&st, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
+  ck(cudaStreamSynchronize(s), "status read");
+  const int used_slots = P.used_slots;
+  const double used_work = P.used_work;
   KernelTimer& kt = kernel_timer(1);
   if (kt.on && used_slots > 0) {
     // live GEMM time of this factorisation: each launch's last end minus its first start

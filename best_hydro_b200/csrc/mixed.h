@@ -35,9 +35,12 @@ class MixedSolver {
   MixedSolver& operator=(const MixedSolver&) = delete;
   const char* name() const;
   // Assembles GR + deflation into gr64 (FP64, kept for the residuals) and a reduced-precision copy,
-  // records ev_assembled, factors the copy.  Throws on failure.
+  // records ev_assembled, factors the copy.  Throws on failure.  wait = false: returns once the work
+  // is enqueued on s (other solvers' builds may then run beside it); finish_build(s) completes it.
   void build(const DevMesh& m, const DevDeflation& d, double* gr64, long ld, double eps, cudaStream_t s,
-             cudaEvent_t ev_assembled, cudaEvent_t ev_factored);
+             cudaEvent_t ev_assembled, cudaEvent_t ev_factored, bool wait = true);
+  // Waits for the factorisation enqueued on s, checks its status (throws MixedFailure).
+  void finish_build(cudaStream_t s);
   // With BEST_GPU_PROFILE=1: per-category times of the calls since the last report (log lines).
   std::vector<std::string> profile_report();
   // GMRES restarts (each with a true FP64 residual) and Krylov vectors per restart.

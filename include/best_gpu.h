@@ -144,6 +144,14 @@ int bgpu_series_build(const int *ndef, const double *gdef, const int *comp, cons
 /* Solves every mesh's system for nrhs right-hand sides in place (concatenated blocks). */
 int bgpu_series_solve(int nrhs, double *b);
 
+/* The precision of the next bgpu_series_build: BGPU_FP64 (default: the batched FP64 LU above, each
+ * mesh's solution that of its single plain solve bit for bit) or BGPU_MIXED: every mesh's assembly
+ * and BF16 tensor-core factorisation (the mixed path of bhm_build) enqueued on a stream of its own,
+ * so the meshes' factorisations run side by side, and FP64 GMRES-IR solves to a relative residual of
+ * 1e-12 (each mesh's solution that of its single mixed solve).  A mesh the unpivoted factorisation
+ * cannot handle makes the build fall back to the FP64 series (logged). */
+int bgpu_series_set_precision(int mode);
+
 /* ms[0] last series build (graph replay), ms[1] the assembly of the last direct (tuning or
  * uncaptured) build, ms[2] last series solve, ms[3] the tuning pass (0 when not tuned).  Returns
  * the number of values written. */

@@ -113,6 +113,26 @@ def test_series_at_the_eight_frequencies():
         assert abs(ext[key] - y0) <= 1e-12 * abs(y0), key
 
 
+def test_mixed_series_at_the_eight_frequencies():
+    """The series with every mesh's factorisation on the tensor cores (one stream per mesh, all
+    enqueued together) and FP64 GMRES-IR: each mesh's D_t, D_r, CHI' within 1e-8 of its plain FP64
+    solve, and the 1/N extrapolation likewise."""
+    freqs = (11, 12, 14, 16, 18, 20, 22, 23)
+    setups = []
+    for f in freqs:
+        tri, ta, tv = meshes.ellipsoid(f)
+        setups.append(bh.Setup(tri, 1, ta))
+    per64, ext64, _ = bh.series_run(setups)
+    perm, extm, tm = bh.series_run(setups, precision=bh.BGPU_MIXED)
+    print(f"\nmixed series build {tm['build']:.1f} ms, solve {tm['solve']:.1f} ms")
+    assert any("mixed precision" in ln for ln in bh.log_lines())
+    for a, b in zip(perm, per64):
+        for key in ("D_t", "D_r", "chiprime"):
+            assert abs(a[key] / b[key] - 1) < 1e-8, (a["N"], key)
+    for key in ("D_t", "D_r", "chiprime"):
+        assert abs(extm[key] / ext64[key] - 1) < 1e-8, key
+
+
 def test_adjoint_at_5120():
     verts, faces, ta, tv = meshes.ellipsoid_vf(16)
     from tests.test_gpu_adjoint import check_fd
