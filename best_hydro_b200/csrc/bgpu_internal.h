@@ -173,8 +173,15 @@ cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const doub
 cudaError_t getrs64_trans_inv(const double* LU, long lda, const double* DL, const double* DU, int n, const int* perm,
                               double* X, long ldx, int nrhs, void* scratch, int* d_status, cudaStream_t s);
 // Y := U^-1 L^-1 Y, FP32 factors, right-hand sides and sums (the mixed path's preconditioner)
-cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, float* Y, long ldy,
-                          int nrhs, void* scratch, int* d_status, cudaStream_t s);
+cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, const float* WL,
+                          const float* WU, int n, float* Y, long ldy, int nrhs, void* scratch, int* d_status,
+                          cudaStream_t s);
+// The chain weights of trsv_lu32_inv (WL, WU: chain_weights_elems(n) floats each):
+// W_b = D_b^-1 L_{b,b-1} and D_b^-1 U_{b,b+1} over the 128-row blocks.  (WL = WU = nullptr: the
+// solve without the chain.)
+size_t chain_weights_elems(int n);
+cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const float* DU, int n, float* WL, float* WU,
+                            cudaStream_t s);
 // Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s);
 

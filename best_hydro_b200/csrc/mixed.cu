@@ -851,7 +851,7 @@ struct MixedSolver::Impl {
   int op_rows = 0;     // rows of both operand buffers
   const void* map_key[2] = {};      // the buffers the tensor maps describe
   cudaGraphExec_t graph = nullptr;  // the captured factorisation
-  const void* graph_key[6] = {};
+  const void* graph_key[7] = {};
   int graph_n = 0;
   size_t graph_kernels = 0;
   // per-launch device stamps of the GEMMs (live timing that works inside the graph): slots taken in
@@ -898,6 +898,7 @@ struct MixedSolver::Impl {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool fork = false;
   Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs, dl32, du32, zf;
+  Buf wl32, wu32;  // the preconditioner's chain weights (D_b^-1 L_{b,b-1}, D_b^-1 U_{b,b+1})
   // BF16 mirrors of the factors (L part row-major, U part column-major), written by the triangular
   // solve leaves as the entries become final; the GEMMs read their operands there by position, so no
   // operand copies are made.  Used when the GPU has room for them (4 n^2 bytes), else copies.
@@ -1135,6 +1136,8 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   // solve's scratch (for up to 16 right-hand sides per pass)
   P.dl32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (L)");
   P.du32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (U)");
+  P.wl32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain weights (L)");
+  P.wu32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain weights (U)");
   // BF16 mirrors when they fit with 4 GB to spare, else operand copies per product
   const long ldm = round_up(P.n3, 64);
   const size_t mirror_bytes = (size_t)P.n3 * ldm * 2;
@@ -1212,14 +1215,17 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     P.slot_kind.clear();
     ck(stamps_reset(P.stamps.as<unsigned long long>(), P.slot_cap, s), "stamps");
     P.rlu(0, P.n3, s);  // direct launches in order, each timed
+    ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3, P.wl32.as<float>(),
+                       P.wu32.as<float>(), s),
+       "chain weights");
     used_slots = P.nslots;
     used_work = P.slot_work;
   } else {
     // the recursion's launches depend only on the order and the buffers: capture them once as a
     // CUDA graph and replay it
-    const void* key[6] = {P.lu32.p, P.mirrors ? P.am.p : P.at.p, P.mirrors ? P.bm.p : P.bt.p,
-                          P.dl32.p, P.du32.p, P.stamps.p};
-    if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 6, P.graph_key)) {
+    const void* key[7] = {P.lu32.p, P.mirrors ? P.am.p : P.at.p, P.mirrors ? P.bm.p : P.bt.p,
+                          P.dl32.p, P.du32.p, P.stamps.p, P.wl32.p};
+    if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 7, P.graph_key)) {
       const clk::time_point t_cap = clk::now();
       if (P.graph) cudaGraphExecDestroy(P.graph);
       P.graph = nullptr;
@@ -1234,6 +1240,9 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       P.slot_kind.clear();
       try {
         P.rlu(0, P.n3, cs);
+        ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3,
+                           P.wl32.as<float>(), P.wu32.as<float>(), cs),
+           "chain weights");
       } catch (...) {
         cudaStreamEndCapture(cs, &g);
         if (g) cudaGraphDestroy(g);
@@ -1250,7 +1259,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       ms_inst = ms_since(t_inst);
       cudaGraphDestroy(g);
       cudaStreamDestroy(cs);
-      std::copy(key, key + 6, P.graph_key);
+      std::copy(key, key + 7, P.graph_key);
       P.graph_n = P.n3;
       P.graph_slots = P.nslots;
       P.graph_work = P.slot_work;
@@ -1375,8 +1384,8 @@ void MixedSolver::solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedRe
         P.prof.begin("preconditioner solve", 0, s);
         k_to_f32<<<grid, 256, 0, s>>>(Vj, blk, P.zf.as<float>());
         BGPU_COUNT_LAUNCH();
-        ck(trsv_lu32_inv(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), n, P.zf.as<float>(), n,
-                         q, P.trsv.p, P.d_status(), s),
+        ck(trsv_lu32_inv(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.wl32.as<float>(),
+                         P.wu32.as<float>(), n, P.zf.as<float>(), n, q, P.trsv.p, P.d_status(), s),
            "preconditioner");
         k_to_f64<<<grid, 256, 0, s>>>(P.zf.as<float>(), blk, Zj);
         BGPU_COUNT_LAUNCH();

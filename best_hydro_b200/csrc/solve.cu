@@ -420,12 +420,21 @@ constexpr int kChunk = 16;
 constexpr int kLead = 2;
 
 // V is the type of the right-hand sides and of every sum (double; float for the FP32 preconditioner).
-template <typename F, typename FI, bool LOWER, bool TRANS = false, typename V = double>
+// CHAIN (the FP32 preconditioner): the chain of block rows is taken off the task list.  A final
+// task of row i then stops short of block i-1: it forms c_i = D_i^-1 (b_i - sum_{j <= i-2} L_ij x_j)
+// into a slot of its own and releases cflags[i]; CTA 0 runs the chain alone,
+//     x_i = c_i - W_i x_{i-1},   W_i = D_i^-1 L_{i,i-1}   (chain_weights32, once per factorisation),
+// keeping x_{i-1} in shared memory and W_i (prefetched a step ahead) in registers, and releases
+// flags[i] for the tasks that need x_i.  The chain's step is one 128 x 128 product instead of a
+// handoff through global memory, two products and a wait on the previous block row.  All CTAs of the
+// grid are resident (the grid is sized by occupancy), so CTA 0 always runs.
+template <typename F, typename FI, bool LOWER, bool TRANS = false, typename V = double, bool CHAIN = false>
 __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
                                                   V* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
                                                   unsigned epoch, int* status, unsigned* __restrict__ cnt,
                                                   V* __restrict__ part, int smax, const int4* __restrict__ tasks,
-                                                  int ntasks) {
+                                                  int ntasks, const FI* __restrict__ W, unsigned* cflags,
+                                                  V* __restrict__ cslot) {
   __shared__ V s_y[kIb][kIrhs];
   __shared__ V s_b[kIb][kIrhs];
   __shared__ V s_acc[2][kIb][kIrhs];
@@ -434,6 +443,70 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
   FI* s_di = reinterpret_cast<FI*>(s_dyn);  // the inverted diagonal block, stride kIb + 1
   const int nblk = (n + kIb - 1) / kIb;
   const int tid = threadIdx.x, row = tid & (kIb - 1), half = tid >> 7;
+  if constexpr (CHAIN) {
+    if (blockIdx.x == 0) {
+      // s_y holds x_{i-1}; this thread's 64 entries of W_i: row `row`, columns 64 half .. +63
+      FI wv[64];
+      for (int i = 0; i < nblk; ++i) {
+        const int blk = LOWER ? i : nblk - 1 - i;
+        const int r0 = blk * kIb, nr = min(kIb, n - r0);
+        if (i >= 1) {
+          const FI* wt = W + (size_t)blk * kIb * kIb + (size_t)(half * 64) * kIb + row;  // column-major tile
+#pragma unroll
+          for (int kk = 0; kk < 64; ++kk) wv[kk] = wt[(size_t)kk * kIb];
+        }
+        if (tid == 0) {
+          unsigned spins = 0;
+          int ok = 1;
+          while (ld_acquire_u32(cflags + i) != epoch) {
+            if (++spins > kSpinLimit) {
+              atomicExch(status, (int)kWaitTimeout);
+              ok = 0;
+              break;
+            }
+            __nanosleep(32);
+          }
+          s_cnt = ok;
+        }
+        __syncthreads();
+        if (!s_cnt) return;
+        V c[kIrhs];
+        if (half == 0) {
+          const V* cp = cslot + ((size_t)i * kIb + row) * kIrhs;
+#pragma unroll
+          for (int r = 0; r < kIrhs; ++r) c[r] = __ldcg(cp + r);
+        }
+        V acc[kIrhs];
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) acc[r] = (V)0;
+        if (i >= 1) {
+#pragma unroll
+          for (int kk = 0; kk < 64; ++kk) {
+            const V w = (V)wv[kk];
+#pragma unroll
+            for (int r = 0; r < kIrhs; ++r) acc[r] += w * s_y[half * 64 + kk][r];
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
+        __syncthreads();
+        if (half == 0) {
+#pragma unroll
+          for (int r = 0; r < kIrhs; ++r) {
+            const V x = row < nr ? c[r] - (s_acc[0][row][r] + s_acc[1][row][r]) : (V)0;
+            s_y[row][r] = x;
+            if (row < nr && r < nrhs) Y[(size_t)r * ldy + r0 + row] = x;
+          }
+        }
+        __syncthreads();
+        if (tid == 0) {
+          __threadfence();
+          st_release_u32(flags + blk, epoch);
+        }
+      }
+      return;
+    }
+  }
   for (;;) {
     // task: x = slot (partial task) or -1 - number of partial tasks (final task); y = row; [z, w) blocks
     if (tid == 0) {
@@ -564,16 +637,78 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
     __syncthreads();
-    for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
-      const int rr = idx / kIrhs, r = idx % kIrhs;
-      if (rr < nr && r < nrhs) Y[(size_t)r * ldy + r0 + rr] = s_acc[0][rr][r] + s_acc[1][rr][r];
-    }
-    __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      st_release_u32(flags + blk, epoch);
+    if constexpr (CHAIN) {
+      V* cp = cslot + (size_t)i * kIb * kIrhs;  // c_i, row-major 128 x kIrhs, zero beyond nr and nrhs
+      for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+        const int rr = idx / kIrhs, r = idx % kIrhs;
+        cp[idx] = (rr < nr && r < nrhs) ? s_acc[0][rr][r] + s_acc[1][rr][r] : (V)0;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        st_release_u32(cflags + i, epoch);
+      }
+    } else {
+      for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+        const int rr = idx / kIrhs, r = idx % kIrhs;
+        if (rr < nr && r < nrhs) Y[(size_t)r * ldy + r0 + rr] = s_acc[0][rr][r] + s_acc[1][rr][r];
+      }
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        st_release_u32(flags + blk, epoch);
+      }
     }
   }
+}
+
+// W_b = D_b^-1 L_{b,b-1} (LOWER, b >= 1) or D_b^-1 U_{b,b+1} (upper, b <= nblk - 2), 128 x 128
+// column-major per block row, rows and columns beyond n zero: the chain weights of the FP32
+// preconditioner (see k_trsv_inv, CHAIN).  One CTA per block row and triangle (blockIdx.y).
+__global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict__ LU, long lda, int n,
+                                                          const float* __restrict__ DL, const float* __restrict__ DU,
+                                                          float* __restrict__ WL, float* __restrict__ WU) {
+  extern __shared__ __align__(16) float s_w[];
+  float* sd = s_w;                  // D^-1 (r, k) at sd[k * 129 + r]
+  float* sb = s_w + kIb * (kIb + 1);  // the off-diagonal block (k, c) at sb[c * 129 + k]
+  const int nblk = (n + kIb - 1) / kIb, b = blockIdx.x, lower = blockIdx.y == 0;
+  const int nb = lower ? b - 1 : b + 1;  // the neighbouring block column
+  float* out = (lower ? WL : WU) + (size_t)b * kIb * kIb;
+  const int tid = threadIdx.x;
+  if (nb < 0 || nb >= nblk) {
+    for (int e = tid; e < kIb * kIb; e += 256) out[e] = 0.f;
+    return;
+  }
+  const float* D = (lower ? DL : DU) + (size_t)b * kIb * kIb;
+  const int r0 = b * kIb, nr = min(kIb, n - r0), c0 = nb * kIb, nc = min(kIb, n - c0);
+  for (int e = tid; e < kIb * kIb; e += 256) {
+    const int r = e & (kIb - 1), c = e >> 7;
+    sd[c * (kIb + 1) + r] = D[e];
+    sb[c * (kIb + 1) + r] = (r < nr && c < nc) ? LU[(size_t)(c0 + c) * lda + r0 + r] : 0.f;
+  }
+  __syncthreads();
+  // thread: rows 8 (tid & 15) .. +7, columns 8 (tid >> 4) .. +7
+  const int rb = 8 * (tid & 15), cb = 8 * (tid >> 4);
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+  for (int k = 0; k < kIb; ++k) {
+    float a[8], bv[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = sd[k * (kIb + 1) + rb + i];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) bv[j] = sb[(cb + j) * (kIb + 1) + k];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * bv[j];
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) out[(size_t)(cb + j) * kIb + rb + i] = (rb + i < nr) ? acc[i][j] : 0.f;
 }
 
 // Scratch of the split solves, after the base scratch: per-row partial-task counters, the partial
@@ -585,14 +720,18 @@ struct SplitScratch {
   static size_t base(int n) { return (TrsvScratch::bytes(n) + 255) / 256 * 256; }
   static size_t part_off(int n) { return base(n) + ((size_t)nblk(n) * 4 + 255) / 256 * 256; }
   static size_t task_off(int n) { return part_off(n) + (size_t)nblk(n) * smax(n) * kIb * kIrhs * sizeof(double); }
-  static size_t bytes(int n) { return task_off(n) + max_tasks(n) * sizeof(int4); }
+  // the chain's c_i ready flags (zero when allocated, like the others) and c_i slots
+  static size_t cflag_off(int n) { return (task_off(n) + max_tasks(n) * sizeof(int4) + 255) / 256 * 256; }
+  static size_t cslot_off(int n) { return cflag_off(n) + ((size_t)nblk(n) * 4 + 255) / 256 * 256; }
+  static size_t bytes(int n) { return cslot_off(n) + (size_t)nblk(n) * kIb * kIrhs * sizeof(double); }
 };
 
-// The task list of a triangle with nblk block rows (see k_trsv_inv), built once per size.
-const std::vector<int4>& split_tasks(int nblk) {
-  static std::map<int, std::vector<int4>> cache;
-  auto it = cache.find(nblk);
-  if (it != cache.end()) return it->second;
+// The task list of a triangle with nblk block rows (see k_trsv_inv), built once per size.  chain:
+// the final task of row b stops before block b-1 (the chain's).
+const std::vector<int4>& split_tasks(int nblk, bool chain = false) {
+  static std::map<int, std::vector<int4>> cache[2];
+  auto it = cache[chain].find(nblk);
+  if (it != cache[chain].end()) return it->second;
   std::vector<std::vector<int4>> after(nblk);  // partial tasks issued after F(b)
   std::vector<int> nparts(nblk, 0);
   for (int i = 0; i < nblk; ++i) {
@@ -608,10 +747,60 @@ const std::vector<int4>& split_tasks(int nblk) {
   }
   std::vector<int4> list;
   for (int b = 0; b < nblk; ++b) {
-    list.push_back(make_int4(-1 - nparts[b], b, std::max(0, b - kLead), b));
+    list.push_back(make_int4(-1 - nparts[b], b, std::max(0, b - kLead), chain ? std::max(0, b - 1) : b));
     for (const int4& t : after[b]) list.push_back(t);
   }
-  return cache.emplace(nblk, std::move(list)).first->second;
+  return cache[chain].emplace(nblk, std::move(list)).first->second;
+}
+
+// One triangle of the FP32 preconditioner with the chain (k_trsv_inv, CHAIN): W the chain weights
+// of this triangle (chain_weights32).
+template <bool LOWER>
+cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const float* W, int n, float* Yc, long ldy,
+                           int q, void* scratch, unsigned epoch, int* d_status, cudaStream_t s) {
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  unsigned* ticket = reinterpret_cast<unsigned*>(base);
+  unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
+  unsigned* cnt = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
+  float* part = reinterpret_cast<float*>(base + SplitScratch::part_off(n));
+  int4* tasks = reinterpret_cast<int4*>(base + SplitScratch::task_off(n));
+  unsigned* cflags = reinterpret_cast<unsigned*>(base + SplitScratch::cflag_off(n));
+  float* cslot = reinterpret_cast<float*>(base + SplitScratch::cslot_off(n));
+  const std::vector<int4>& list = split_tasks(SplitScratch::nblk(n), true);
+  if (list.size() > SplitScratch::max_tasks(n)) return cudaErrorInvalidValue;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(cnt, 0, (size_t)SplitScratch::nblk(n) * 4, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(tasks, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return e;
+  const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(float);
+  auto kern = k_trsv_inv<float, float, LOWER, false, float, true>;
+  static bool attr = false;
+  static int per_sm = 0;
+  if (!attr) {
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem)) != cudaSuccess)
+      return e;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, dsmem) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    per_sm = std::min(per_sm, 2);
+    attr = true;
+  }
+  // a cooperative launch: every CTA resident (CTA 0 runs the chain the others wait on); the rest take
+  // tasks in ticket order
+  const float* di = DI;
+  float* y = Yc;
+  long ldy_ = ldy;
+  int n_ = n, q_ = q, smax = SplitScratch::smax(n), nt = (int)list.size();
+  unsigned ep = epoch;
+  void* args[] = {(void*)&LU, (void*)&lda, (void*)&di, (void*)&n_, (void*)&y, (void*)&ldy_, (void*)&q_,
+                  (void*)&flags, (void*)&ticket, (void*)&ep, (void*)&d_status, (void*)&cnt, (void*)&part,
+                  (void*)&smax, (void*)&tasks, (void*)&nt, (void*)&W, (void*)&cflags, (void*)&cslot};
+  e = cudaLaunchCooperativeKernel((const void*)kern, dim3(sms * per_sm), dim3(256), args, dsmem, s);
+  BGPU_COUNT_LAUNCH();
+  return e;
 }
 
 // one triangle: ticket, counters and task list set, then the persistent launch (one CTA per SM)
@@ -653,7 +842,8 @@ cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, V* Yc, long ldy
     per_sm = std::min(per_sm, 2);
   }
   k_trsv_inv<F, FI, LOWER, TRANS, V><<<sms * per_sm, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
-                                                          cnt, part, SplitScratch::smax(n), tasks, (int)list.size());
+                                                          cnt, part, SplitScratch::smax(n), tasks, (int)list.size(),
+                                                          nullptr, nullptr, nullptr);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -760,10 +950,38 @@ cudaError_t getrs64_inv(const double* LU, long lda, const double* DL, const doub
 // Y := U^-1 L^-1 Y with FP32 factors of an unpivoted LU and their FP32 diagonal-block inverses,
 // FP32 right-hand sides and sums (the preconditioner of the refined solve, whose result only
 // steers the iteration: the FP64 products and residuals fix the accuracy)
-cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, int n, float* Y, long ldy,
-                          int nrhs, void* scratch, int* d_status, cudaStream_t s) {
+cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const float* DU, const float* WL,
+                          const float* WU, int n, float* Y, long ldy, int nrhs, void* scratch, int* d_status,
+                          cudaStream_t s) {
   if (n <= 0 || nrhs <= 0) return cudaSuccess;
-  return trsv_inv_pair<float, float, float>(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
+  if (!WL || !WU) return trsv_inv_pair<float, float, float>(LU, lda, DL, DU, n, Y, ldy, nrhs, scratch, d_status, s);
+  for (int c0 = 0; c0 < nrhs; c0 += kIrhs) {
+    const int q = std::min(kIrhs, nrhs - c0);
+    float* Yc = Y + (size_t)c0 * ldy;
+    const unsigned epoch = next_epochs();
+    cudaError_t e = trsv_one_chain<true>(LU, lda, DL, WL, n, Yc, ldy, q, scratch, epoch, d_status, s);
+    if (e != cudaSuccess) return e;
+    if ((e = trsv_one_chain<false>(LU, lda, DU, WU, n, Yc, ldy, q, scratch, epoch + 1, d_status, s)) != cudaSuccess)
+      return e;
+  }
+  return cudaSuccess;
+}
+
+size_t chain_weights_elems(int n) { return (size_t)((n + kIb - 1) / kIb) * kIb * kIb; }
+
+cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const float* DU, int n, float* WL, float* WU,
+                            cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const size_t smem = (size_t)2 * kIb * (kIb + 1) * sizeof(float);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_chain_weights32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_chain_weights32<<<dim3((n + kIb - 1) / kIb, 2), 256, smem, s>>>(LU, lda, n, DL, DU, WL, WU);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
 }
 
 cudaError_t check_finite(const double* X, long ldx, int n, int nrhs, int* d_status, cudaStream_t s) {
