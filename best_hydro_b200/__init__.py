@@ -72,6 +72,7 @@ _SIGS = {
     "bgpu_series_set_precision": (ctypes.c_int, [ctypes.c_int]),
     "bgpu_autotune_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "bgpu_best_gradient": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
+    "bgpu_set_wait_limit": (ctypes.c_int, [ctypes.c_uint]),
     "bgpu_lu32_leaf_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                              ctypes.c_void_p]),
     "bgpu_create_from_triangles": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,

@@ -1526,6 +1526,14 @@ int bgpu_gemm_bf16_minus_device(int m, int n, int k, const float* d_a, int lda, 
   });
 }
 
+int bgpu_set_wait_limit(unsigned spins) {
+  return status_of([&] {
+    rt();
+    ck(set_wait_limit(spins), "wait limit");
+    return 0;
+  });
+}
+
 int bgpu_lu32_leaf_device(int h, float* d_a, int lda, float* d_linv, float* d_uinv) {
   return status_of([&] {
     Runtime& r = rt();

@@ -180,6 +180,8 @@ cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const floa
 // W_b = D_b^-1 L_{b,b-1} and D_b^-1 U_{b,b+1} over the 128-row blocks.  (WL = WU = nullptr: the
 // solve without the chain.)
 size_t chain_weights_elems(int n);
+// The poll limit of every triangular-solve wait (device constant; default 4,194,304).
+cudaError_t set_wait_limit(unsigned spins);
 cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const float* DU, int n, float* WL, float* WU,
                             cudaStream_t s);
 // Sets *d_status = kNotFinite if any of the n x nrhs entries is NaN or Inf.

@@ -34,7 +34,11 @@ namespace {
 constexpr int kBs = 64;           // rows per block
 constexpr int kMaxRhs = 16;       // right-hand sides per call (kernels for 8 and 16)
 constexpr int kThreads = 256;     // 4 quarter-rows of the inner dimension x 64 rows
-constexpr unsigned kSpinLimit = 1u << 22;
+// Polls a triangular-solve wait makes before it gives up (status kWaitTimeout, the kernel returns):
+// 4,194,304 by default; bgpu_set_wait_limit changes it (0: a wait not satisfied at once gives up,
+// which the tests of the failure path use).
+constexpr unsigned kSpinLimitDefault = 1u << 22;
+__constant__ unsigned c_spin_limit = kSpinLimitDefault;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;
@@ -145,7 +149,7 @@ __device__ int wait_ready(const unsigned* flags, int jb, int step, int lo, int h
         if (cnt < 0 || ball == 0xffffffffu) cnt = 32;
         break;
       }
-      if (++spins > kSpinLimit) {
+      if (++spins > c_spin_limit) {
         if (threadIdx.x == 0) atomicExch(status, (int)kWaitTimeout);
         break;
       }
@@ -459,7 +463,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
           unsigned spins = 0;
           int ok = 1;
           while (ld_acquire_u32(cflags + i) != epoch) {
-            if (++spins > kSpinLimit) {
+            if (++spins > c_spin_limit) {
               atomicExch(status, (int)kWaitTimeout);
               ok = 0;
               break;
@@ -542,7 +546,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
         int ok = 1;
         unsigned spins = 0;
         while (nparts > 0 && ld_acquire_u32(cnt + i) < (unsigned)nparts) {
-          if (++spins > kSpinLimit) {
+          if (++spins > c_spin_limit) {
             atomicExch(status, (int)kWaitTimeout);
             ok = 0;
             break;
@@ -966,6 +970,8 @@ cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const floa
   }
   return cudaSuccess;
 }
+
+cudaError_t set_wait_limit(unsigned spins) { return cudaMemcpyToSymbol(c_spin_limit, &spins, sizeof spins); }
 
 size_t chain_weights_elems(int n) { return (size_t)((n + kIb - 1) / kIb) * kIb * kIb; }
 

@@ -100,6 +100,12 @@ int bgpu_create_from_triangles(int n, const double *tri, int iarea, double truea
 int bgpu_build_prepared(double eps, int direct, int single, int nrhs);
 int bgpu_prepared_arrays(double *v1, double *v2, double *v3, double *area, int *icomp, double *xmu, double *gdef);
 
+/* Every wait of the triangular solves (a block row waiting for the rows it depends on) polls at
+ * most `spins` times, then the kernel records a timeout and returns, and the call fails with a
+ * message instead of hanging: 4,194,304 polls by default.  0 makes any wait that is not satisfied at
+ * once give up -- for tests of that failure path.  The solver stays usable afterwards. */
+int bgpu_set_wait_limit(unsigned spins);
+
 /* The mixed-precision LU's diagonal leaf (FP32, device memory): the h x h block d_a (h <= 128,
  * column-major, lda) factored without pivoting in place (unit L below, U on and above the diagonal),
  * L^-1 into d_linv and U^-1 into d_uinv (128 x 128 column-major each, zero outside h x h).  A zero
