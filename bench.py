@@ -329,6 +329,87 @@ def tensors_of(solver, x, st, bh):
                 urc=t["urc"], udr=t["udr"])
 
 
+# ---- DRAM traffic of the tcgen05 GEMM over the LU's launches (profiles/tc_gemm_traffic_lu_shapes.md)
+def lu_gemm_shapes(n3, leaf=128):
+    """The (m, n, k) of every GEMM of the mixed LU's recursion at order n3, in launch order (a replay
+    of MixedSolver's rlu / trsm recursion: the same 3,713 launches at n3 = 61,440)."""
+    out = []
+
+    def split(sz):
+        return max((sz // 2) // leaf * leaf, leaf)
+
+    def trsm_left(h, w):
+        if h <= leaf or w <= 0:
+            return
+        h1 = split(h)
+        trsm_left(h1, w)
+        out.append((h - h1, w, h1))
+        trsm_left(h - h1, w)
+
+    def trsm_right(h, m):
+        if h <= leaf or m <= 0:
+            return
+        h1 = split(h)
+        trsm_right(h1, m)
+        out.append((m, h - h1, h1))
+        trsm_right(h - h1, m)
+
+    def rlu(sz):
+        if sz <= leaf:
+            return
+        h = split(sz)
+        r = sz - h
+        rlu(h)
+        trsm_left(h, r)
+        trsm_right(h, r)
+        out.append((r, r, h))
+        rlu(r)
+
+    rlu(n3)
+    return out
+
+
+def gemm_algorithmic_bytes(m, n, k):
+    """BF16 operands read once, the FP32 C read and written once."""
+    return 2 * (m * k + k * n) + 8 * m * n
+
+
+# DRAM bytes / algorithmic bytes of single k_gemm_bf16_tc launches, from ncu captures on B200
+# (dram__bytes_read.sum + dram__bytes_write.sum; profiles/tc_gemm_traffic_lu_shapes.md)
+GEMM_TRAFFIC_RATIO = {
+    "k<=256": 23675392 / gemm_algorithmic_bytes(128, 30720, 128),
+    "k<=2048": (190902784 + 65673472) / gemm_algorithmic_bytes(1024, 30720, 1024),
+    "square>=8192": (1338633472 + 251912448) / gemm_algorithmic_bytes(8192, 8192, 8192),
+    "k>2048": (2286619392 + 1036582144) / gemm_algorithmic_bytes(16384, 16384, 4096),
+}
+
+
+def small_update(m, n, k):
+    """The products the LU runs on the CUDA cores instead of the tcgen05 kernel (mixed.cu)."""
+    return k <= 256 and m * n * k <= (1 << 26)
+
+
+def gemm_traffic_per_launch(n3):
+    """(estimated DRAM bytes, algorithmic bytes, launches) per tcgen05 GEMM launch of one
+    factorisation at order n3: each launch's algorithmic bytes times the measured ratio of its shape
+    class."""
+    shapes = [sh for sh in lu_gemm_shapes(n3) if not small_update(*sh)]
+    alg = traffic = 0.0
+    for m, n, k in shapes:
+        a = gemm_algorithmic_bytes(m, n, k)
+        if k <= 256:
+            r = GEMM_TRAFFIC_RATIO["k<=256"]
+        elif k <= 2048:
+            r = GEMM_TRAFFIC_RATIO["k<=2048"]
+        elif min(m, n, k) >= 8192:
+            r = GEMM_TRAFFIC_RATIO["square>=8192"]
+        else:
+            r = GEMM_TRAFFIC_RATIO["k>2048"]
+        alg += a
+        traffic += a * r
+    return traffic / len(shapes), alg / len(shapes), len(shapes)
+
+
 def tensor_errors(got, want):
     """Relative differences of BEST's results: D_t, D_r traces and CHI' ([eta] is proportional); the
     full D_tt, D_rr tensors; D_tr relative to sqrt(|D_tt| |D_rr|); the centres of resistance and
@@ -510,12 +591,16 @@ def run_ours(args, rank, world, local_rank):
         achieved = (gflop / max(gl, 1)) / (gms / max(gl, 1) * 1e-3) / 1e12 if gl else None
         if head == "mixed":
             peak = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+            tr_bytes, alg_bytes, nshapes = gemm_traffic_per_launch(n3)
             roof = {"kernel": "k_gemm_bf16_tc (tcgen05.mma kind::f16, TMA, TMEM accumulators): every update of "
                               "the mixed LU", "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": (achieved / peak) if achieved else None, "traffic": None,
+                    "frac": (achieved / peak) if achieved else None, "traffic": tr_bytes,
+                    "traffic_algorithmic": alg_bytes,
                     "peak_source": f"{peak_src} bf16 sustained (MEASURED_PEAKS.json; the GEMM runs inside a long step)",
-                    "traffic_note": "launch shapes vary from 128x128x128 to 30720^3; per-shape DRAM bytes of "
-                                    "captured launches in profiles/"}
+                    "traffic_note": f"DRAM bytes per launch, averaged over the factorisation's {nshapes} launches: each "
+                                    "launch's algorithmic bytes (BF16 A, B read once, FP32 C read and written) times "
+                                    "the DRAM/algorithmic ratio ncu measured for its shape class "
+                                    "(profiles/tc_gemm_traffic_lu_shapes.md)"}
         else:
             p64 = fp64_peak_tflops(torch, dev)
             roof = {"kernel": "FP64 LU trailing-update GEMM (mma.sync f64, k_dgemm_nn_minus)", "bound": "tensor",

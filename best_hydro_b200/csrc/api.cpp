@@ -587,6 +587,8 @@ int bgpu_create_from_triangles(int n, const double* tri, int iarea, double truea
        "set-up on the device");
     ck(cudaMemcpyAsync(s->scal_host, s->scal.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, r.stream), "set-up copy");
     ck(cudaMemcpyAsync(s->counts_host, s->counts.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, r.stream), "counts copy");
+    r.sync("bgpu_create_from_triangles");
+    s->afac = s->scal_host[0];  // the self blocks scale by sqrt(AFAC) (best/tgetgr.f:107-112)
     // what bhm_create does with a mesh given by the caller: self blocks, incenters, DIAGM
     ck(launch_self_blocks(s->mesh(), r.stream), "self blocks");
     ck(launch_diag_mean(s->mesh(), s->diag.as<double>(), r.stream), "diagonal mean");
@@ -601,7 +603,6 @@ int bgpu_create_from_triangles(int n, const double* tri, int iarea, double truea
     r.sync("bgpu_create_from_triangles");
     r.check_status("bgpu_create_from_triangles");
     r.ms[0] = r.elapsed(0, 1);
-    s->afac = s->scal_host[0];
     for (int c = 0; c < 3; ++c) s->v_host[c].assign(v.begin() + (size_t)c * 3 * n, v.begin() + (size_t)(c + 1) * 3 * n);
     s->x_host.resize((size_t)3 * n);
     for (int t = 0; t < n; ++t)

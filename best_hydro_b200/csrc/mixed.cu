@@ -632,37 +632,137 @@ void launch_narrow_leaf(const float* dinv, int h, float* B, long ldb, int len, _
 #undef BGPU_NARROW
 }
 
+// ---- small updates C -= A B in FP32 on the CUDA cores ------------------------------------------
+// The recursion's smallest products (K <= 256, at most 2^26 multiply-adds, e.g. 128 x 128 x 128 or
+// 1024 x 256 x 256) take 15-20 us each on the persistent tcgen05 kernel, whose start-up (TMEM
+// allocation, barrier set-up, the first TMA round trip) is most of it; here 64 x 64 tiles, one per
+// CTA, 4 x 4 results per thread, K in steps of 32 through shared memory.  FP32 operands straight
+// from the factor (more accurate than the BF16 mirrors the tensor cores read).
+constexpr int kSgBk = 32;
+inline bool small_update(int m, int n, int k) { return k <= 256 && (long long)m * n * k <= (1LL << 26); }
+__global__ void __launch_bounds__(256) k_sgemm_small_minus(int m, int n, int k, const float* __restrict__ A, long lda,
+                                                          const float* __restrict__ B, long ldb, float* __restrict__ C,
+                                                          long ldc) {
+  __shared__ __align__(16) float As[kSgBk][64 + 4];  // As[kk][r] = A(m0 + r, k0 + kk)
+  __shared__ __align__(16) float Bs[kSgBk][64 + 4];  // Bs[kk][c] = B(k0 + kk, n0 + c)
+  const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
+  const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+  for (int k0 = 0; k0 < k; k0 += kSgBk) {
+    for (int e = tid; e < kSgBk * 64; e += 256) {
+      const int kk = e >> 6, r = e & 63;
+      As[kk][r] = (m0 + r < m && k0 + kk < k) ? A[(size_t)(k0 + kk) * lda + m0 + r] : 0.f;
+    }
+    for (int e = tid; e < kSgBk * 64; e += 256) {
+      const int kk = e & (kSgBk - 1), c = e / kSgBk;
+      Bs[kk][c] = (n0 + c < n && k0 + kk < k) ? B[(size_t)(n0 + c) * ldb + k0 + kk] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < kSgBk; ++kk) {
+      const float4 a = *reinterpret_cast<const float4*>(&As[kk][4 * tr]);
+      const float4 b = *reinterpret_cast<const float4*>(&Bs[kk][4 * tc]);
+      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += av[i] * bv[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = n0 + 4 * tc + j;
+    if (c >= n) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = m0 + 4 * tr + i;
+      if (r < m) C[(size_t)c * ldc + r] -= acc[i][j];
+    }
+  }
+}
+
 // ---- FP64 mat-vec for the residuals: Y = beta Y + alpha A X (q <= Q columns) ----------------
-// Two rows per thread (16-byte loads; the leading dimension is even and the rows start even), the
-// columns split over blockIdx.y into partial sums P, reduced in a fixed order afterwards.
+// Four rows per thread (two 16-byte loads per column; the leading dimension is a multiple of 32 and
+// the rows start at multiples of 4), the columns split over blockIdx.y into partial sums P, reduced
+// in a fixed order afterwards.  X's chunk of kMvCols columns is staged in shared memory, and the
+// loads of A go four columns ahead through the non-allocating streaming path: GR is read once per
+// product and never reused, so it should not displace anything in L1.  (Measured on B200 at order
+// 61,440, 6 right-hand sides: 4.81 ms, 6.28 TB/s, against 6.79 ms for two rows per thread with X
+// read through L1.)
+constexpr int kMvCols = 128;
+__device__ __forceinline__ double2 ld_stream_f64x2(const double* p) {
+  double2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
 template <int Q>
 __global__ void __launch_bounds__(128) k_matvec64_part(const double* __restrict__ A, long lda, int n,
                                                        const double* __restrict__ X, long ldx, int q, int cols_per,
                                                        double* __restrict__ P) {
-  const int row = 2 * (blockIdx.x * 128 + threadIdx.x), split = blockIdx.y;
+  __shared__ double xs[kMvCols][Q];
+  const int row = 4 * (blockIdx.x * 128 + threadIdx.x), split = blockIdx.y;
   const int c0 = split * cols_per, c1 = min(n, c0 + cols_per);
-  double a0[Q], a1[Q];
+  double acc[4][Q];
 #pragma unroll
-  for (int j = 0; j < Q; ++j) a0[j] = a1[j] = 0.0;
-  if (row < n) {
-    const double* a = A + row;
-#pragma unroll 8
-    for (int c = c0; c < c1; ++c) {
-      const double2 v = *reinterpret_cast<const double2*>(a + (size_t)c * lda);
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < Q; ++j)
-        if (j < q) {
-          const double x = __ldg(&X[(size_t)j * ldx + c]);
-          a0[j] += v.x * x;
-          a1[j] += v.y * x;
-        }
+    for (int j = 0; j < Q; ++j) acc[i][j] = 0.0;
+  const bool live = row < n;
+  const double* a = A + (live ? row : 0);
+  for (int cb = c0; cb < c1; cb += kMvCols) {
+    const int nc = min(kMvCols, c1 - cb);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kMvCols * Q; e += 128) {
+      const int c = e / Q, j = e % Q;
+      xs[c][j] = (c < nc && j < q) ? X[(size_t)j * ldx + cb + c] : 0.0;
     }
+    __syncthreads();
+    if (live) {
+      int c = 0;
+      for (; c + 4 <= nc; c += 4) {
+        double2 v[4][2];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          v[u][0] = ld_stream_f64x2(a + (size_t)(cb + c + u) * lda);
+          v[u][1] = ld_stream_f64x2(a + (size_t)(cb + c + u) * lda + 2);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int j = 0; j < Q; ++j) {
+            const double x = xs[c + u][j];
+            acc[0][j] += v[u][0].x * x;
+            acc[1][j] += v[u][0].y * x;
+            acc[2][j] += v[u][1].x * x;
+            acc[3][j] += v[u][1].y * x;
+          }
+      }
+      for (; c < nc; ++c) {
+        const double2 w0 = ld_stream_f64x2(a + (size_t)(cb + c) * lda);
+        const double2 w1 = ld_stream_f64x2(a + (size_t)(cb + c) * lda + 2);
+#pragma unroll
+        for (int j = 0; j < Q; ++j) {
+          const double x = xs[c][j];
+          acc[0][j] += w0.x * x;
+          acc[1][j] += w0.y * x;
+          acc[2][j] += w1.x * x;
+          acc[3][j] += w1.y * x;
+        }
+      }
+    }
+  }
+  if (live) {
 #pragma unroll
     for (int j = 0; j < Q; ++j)
-      if (j < q) {
-        P[((size_t)split * Q + j) * n + row] = a0[j];
-        if (row + 1 < n) P[((size_t)split * Q + j) * n + row + 1] = a1[j];
-      }
+      if (j < q)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (row + i < n) P[((size_t)split * Q + j) * n + row + i] = acc[i][j];
   }
 }
 
@@ -916,6 +1016,15 @@ struct MixedSolver::Impl {
   void gemm(int m, int n, int k, int ar, int ac, int br, int bc, int cr, int cc, cudaStream_t s) {
     if (m <= 0 || n <= 0 || k <= 0) return;
     float* C = at_(cr, cc);
+    if (small_update(m, n, k)) {
+      prof.begin("small update (FP32 cores)", 2.0 * m * n * k, s);
+      k_sgemm_small_minus<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, s>>>(m, n, k, at_(ar, ac), ld32, at_(br, bc),
+                                                                          ld32, C, ld32);
+      prof.end(s);
+      BGPU_COUNT_LAUNCH();
+      ck(cudaGetLastError(), "small update");
+      return;
+    }
     if (mirrors) {
       prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
       ck(gemm_bf16_tc_minus_at(m, n, k, map_am, ar, ac, map_bm, bc, br, C, ld32, d_status(), s,
@@ -1033,8 +1142,9 @@ struct MixedSolver::Impl {
 
   // Y (n3 x q, ldy) = beta Y + alpha GR X
   void matvec(const double* X, long ldx, int q, double* Y, long ldy, double alpha, double beta, cudaStream_t s) {
-    // 128 threads per block, two rows each (larger blocks measured slower on B200)
-    const int rb = (n3 + 255) / 256;
+    // 128 threads per block, four rows each; 32 column splits at the LU's orders (fewer blocks
+    // would leave SMs idle, more only add partial sums)
+    const int rb = (n3 + 511) / 512;
     const int splits = std::max(1, std::min(32, (4 * sms * 8 + rb - 1) / rb));
     const int per = (n3 + splits - 1) / splits;
     part.ensure((size_t)splits * 16 * n3 * sizeof(double), "residual partials");

@@ -130,6 +130,12 @@ __device__ __forceinline__ void cp_async_elem(void* sdst, const void* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(B) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// asynchronous 16-byte copy global -> shared (both 16-byte aligned), and the commit of a group
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 // Warp 0 waits until flags[jb] == epoch, then counts how many more flags in the direction `step`
 // (+1 or -1) are ready too, up to 32 and within [lo, hi).  Returns that count (>= 1), or 0 when the
@@ -449,16 +455,23 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
   const int tid = threadIdx.x, row = tid & (kIb - 1), half = tid >> 7;
   if constexpr (CHAIN) {
     if (blockIdx.x == 0) {
-      // s_y holds x_{i-1}; this thread's 64 entries of W_i: row `row`, columns 64 half .. +63
+      // s_y holds x_{i-1}; wv this thread's 64 entries of W_i (row `row`, columns 64 half .. +63);
+      // W_{i+1} arrives in shared memory (asynchronous 16-byte copies of the column-major tile)
+      // while step i runs, and moves to registers once x_i is published
       FI wv[64];
+      FI* s_w = s_di;  // 128 x 128, column-major, unpadded (fits the final tasks' 128 x 129 buffer)
+      auto fetch_w = [&](int ii) {
+        if (ii >= 1 && ii < nblk) {
+          const int b = LOWER ? ii : nblk - 1 - ii;
+          const FI* src = W + (size_t)b * kIb * kIb;
+          for (int e = tid; e < kIb * kIb * (int)sizeof(FI) / 16; e += 256) cp_async16(s_w + e * (16 / sizeof(FI)), src + e * (16 / sizeof(FI)));
+        }
+        cp_async_commit();
+      };
+      fetch_w(1);
       for (int i = 0; i < nblk; ++i) {
         const int blk = LOWER ? i : nblk - 1 - i;
         const int r0 = blk * kIb, nr = min(kIb, n - r0);
-        if (i >= 1) {
-          const FI* wt = W + (size_t)blk * kIb * kIb + (size_t)(half * 64) * kIb + row;  // column-major tile
-#pragma unroll
-          for (int kk = 0; kk < 64; ++kk) wv[kk] = wt[(size_t)kk * kIb];
-        }
         if (tid == 0) {
           unsigned spins = 0;
           int ok = 1;
@@ -473,7 +486,10 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
           s_cnt = ok;
         }
         __syncthreads();
-        if (!s_cnt) return;
+        if (!s_cnt) {
+          cp_async_wait_all();
+          return;
+        }
         V c[kIrhs];
         if (half == 0) {
           const V* cp = cslot + ((size_t)i * kIb + row) * kIrhs;
@@ -507,7 +523,16 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
           __threadfence();
           st_release_u32(flags + blk, epoch);
         }
+        if (i + 1 < nblk) {
+          cp_async_wait_all();
+          __syncthreads();
+#pragma unroll
+          for (int kk = 0; kk < 64; ++kk) wv[kk] = s_w[(half * 64 + kk) * kIb + row];
+          __syncthreads();
+          fetch_w(i + 2);
+        }
       }
+      cp_async_wait_all();
       return;
     }
   }

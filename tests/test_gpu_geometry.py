@@ -32,7 +32,7 @@ CASES = {
 
 def _same(a, b):
     a, b = np.asarray(a), np.asarray(b)
-    return a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    return a.shape == b.shape and a.dtype == b.dtype and a.tobytes(order="F") == b.tobytes(order="F")
 
 
 @pytest.mark.parametrize("case", list(CASES))
