@@ -642,7 +642,8 @@ constexpr int kSgBk = 32;
 inline bool small_update(int m, int n, int k) { return k <= 256 && (long long)m * n * k <= (1LL << 26); }
 __global__ void __launch_bounds__(256) k_sgemm_small_minus(int m, int n, int k, const float* __restrict__ A, long lda,
                                                           const float* __restrict__ B, long ldb, float* __restrict__ C,
-                                                          long ldc) {
+                                                          long ldc, unsigned long long* stamp) {
+  stamp_begin(stamp);
   __shared__ __align__(16) float As[kSgBk][64 + 4];  // As[kk][r] = A(m0 + r, k0 + kk)
   __shared__ __align__(16) float Bs[kSgBk][64 + 4];  // Bs[kk][c] = B(k0 + kk, n0 + c)
   const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
@@ -684,6 +685,7 @@ __global__ void __launch_bounds__(256) k_sgemm_small_minus(int m, int n, int k, 
       if (r < m) C[(size_t)c * ldc + r] -= acc[i][j];
     }
   }
+  stamp_end(stamp);
 }
 
 // ---- FP64 mat-vec for the residuals: Y = beta Y + alpha A X (q <= Q columns) ----------------
@@ -904,7 +906,7 @@ struct CallProfile {
 };
 
 // kinds of the factorisation's stamped launches
-constexpr unsigned char kSlotGemm = 0, kSlotLuLeaf = 1, kSlotSolveLeaf = 2;
+constexpr unsigned char kSlotGemm = 0, kSlotLuLeaf = 1, kSlotSolveLeaf = 2, kSlotSmall = 3;
 
 // The factorisation's timeline from its launch stamps: how long some kernel ran, a GEMM ran, only
 // leaves ran (LU leaves among them), and nothing ran, between the first start and the last end.
@@ -917,23 +919,24 @@ std::string timeline_note(const std::vector<unsigned long long>& h, const std::v
     }
   if (ev.empty()) return "";
   std::sort(ev.begin(), ev.end());
-  int cnt[3] = {0, 0, 0};
-  double busy = 0, gemm = 0, leaves_only = 0, lu_only = 0;
+  int cnt[4] = {0, 0, 0, 0};
+  double busy = 0, gemm = 0, small = 0, leaves_only = 0, lu_only = 0;
   for (size_t i = 0; i + 1 < ev.size(); ++i) {
     const int k = std::abs(ev[i].second) - 1;
     cnt[k] += ev[i].second > 0 ? 1 : -1;
     const double dt = (double)(ev[i + 1].first - ev[i].first) * 1e-6;
-    if (cnt[0] + cnt[1] + cnt[2] > 0) busy += dt;
+    if (cnt[0] + cnt[1] + cnt[2] + cnt[3] > 0) busy += dt;
     if (cnt[0] > 0) gemm += dt;
-    if (cnt[0] == 0 && cnt[1] + cnt[2] > 0) leaves_only += dt;
-    if (cnt[0] == 0 && cnt[1] > 0) lu_only += dt;
+    if (cnt[0] == 0 && cnt[3] > 0) small += dt;
+    if (cnt[0] == 0 && cnt[3] == 0 && cnt[1] + cnt[2] > 0) leaves_only += dt;
+    if (cnt[0] == 0 && cnt[3] == 0 && cnt[1] > 0) lu_only += dt;
   }
   const double span = (double)(ev.back().first - ev.front().first) * 1e-6;
-  char note[256];
+  char note[320];
   std::snprintf(note, sizeof note,
-                "factorisation timeline: %.1f ms from first start to last end; a GEMM running %.1f ms, only leaves "
-                "%.1f ms (an LU leaf %.1f ms), nothing %.1f ms",
-                span, gemm, leaves_only, lu_only, span - busy);
+                "factorisation timeline: %.1f ms from first start to last end; a tensor-core GEMM running %.1f ms, "
+                "else a small FP32 update %.1f ms, only leaves %.1f ms (an LU leaf %.1f ms), nothing %.1f ms",
+                span, gemm, small, leaves_only, lu_only, span - busy);
   return note;
 }
 
@@ -1018,8 +1021,8 @@ struct MixedSolver::Impl {
     float* C = at_(cr, cc);
     if (small_update(m, n, k)) {
       prof.begin("small update (FP32 cores)", 2.0 * m * n * k, s);
-      k_sgemm_small_minus<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, s>>>(m, n, k, at_(ar, ac), ld32, at_(br, bc),
-                                                                          ld32, C, ld32);
+      k_sgemm_small_minus<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, s>>>(
+          m, n, k, at_(ar, ac), ld32, at_(br, bc), ld32, C, ld32, next_stamp(2.0 * m * n * k, kSlotSmall));
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "small update");
