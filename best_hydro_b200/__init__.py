@@ -75,6 +75,10 @@ _SIGS = {
     "bgpu_set_wait_limit": (ctypes.c_int, [ctypes.c_uint]),
     "bgpu_lu32_leaf_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                              ctypes.c_void_p]),
+    "bgpu_trsm_leaf_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.c_int]),
+    "bgpu_panel_update_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p] + [ctypes.c_int] * 9),
     "bgpu_create_from_triangles": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                   _dp, _ip]),
     "bgpu_build_prepared": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
@@ -499,6 +503,22 @@ def lu32_leaf_device(h, d_a, lda, d_linv, d_uinv):
     """bgpu_lu32_leaf_device: the mixed LU's 128 x 128 diagonal leaf (see include/best_gpu.h)."""
     _check(lib().bgpu_lu32_leaf_device(int(h), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_linv),
                                        ctypes.c_void_p(d_uinv)), "bgpu_lu32_leaf_device")
+
+
+def trsm_leaf_device(left, n, d_a, lda, d_linv, d_uinv, kd, p0, h, length, d_mirror=None, ldm=0):
+    """bgpu_trsm_leaf_device: the mixed LU's triangular-solve leaf on the tensor cores (see
+    include/best_gpu.h)."""
+    _check(lib().bgpu_trsm_leaf_device(int(bool(left)), int(n), ctypes.c_void_p(d_a), int(lda), ctypes.c_void_p(d_linv),
+                                       ctypes.c_void_p(d_uinv), int(kd), int(p0), int(h), int(length),
+                                       ctypes.c_void_p(d_mirror) if d_mirror else None, int(ldm)),
+           "bgpu_trsm_leaf_device")
+
+
+def panel_update_device(n, d_a, lda, m, nc, ar, ac, br, bc, cr, cc):
+    """bgpu_panel_update_device: the mixed LU's K = 128 update on the tensor cores (see
+    include/best_gpu.h)."""
+    _check(lib().bgpu_panel_update_device(int(n), ctypes.c_void_p(d_a), int(lda), int(m), int(nc), int(ar), int(ac),
+                                          int(br), int(bc), int(cr), int(cc)), "bgpu_panel_update_device")
 
 
 def dgemm_minus_device(m, n, k, d_a, lda, d_b, ldb, d_c, ldc):

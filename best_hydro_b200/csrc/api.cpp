@@ -1548,6 +1548,75 @@ int bgpu_lu32_leaf_device(int h, float* d_a, int lda, float* d_linv, float* d_ui
   });
 }
 
+int bgpu_trsm_leaf_device(int left, int n, float* d_a, int lda, const float* d_linv, const float* d_uinv, int kd,
+                          int p0, int h, int len, void* d_mirror, int ldm) {
+  return status_of([&] {
+    Runtime& r = rt();
+    const bool bad = n < 1 || lda < n || h < 1 || h > 128 || len < 0 || kd < 0 || p0 < 0 || kd % 32 || p0 % 32 ||
+                     kd + h > n || p0 + len > n || (d_mirror && ldm < n);
+    if (bad) {
+      note("error: bgpu_trsm_leaf_device: n %d, lda %d, kd %d, p0 %d, h %d, len %d, ldm %d out of range", n, lda, kd,
+           p0, h, len, ldm);
+      return 1;
+    }
+    ck(tc_gemm_prepare(), "tensor-core attributes");
+    alignas(64) unsigned char maps[4 * kTensorMapBytes];
+    if (!tc_panel_maps(d_a, n, lda, d_linv, d_uinv, maps)) {
+      note("error: bgpu_trsm_leaf_device: cannot build the tensor maps (lda a multiple of 4, 16-byte aligned buffers)");
+      return 1;
+    }
+    float* X = left ? d_a + kd + (size_t)p0 * lda : d_a + p0 + (size_t)kd * lda;
+    void* mir = nullptr;
+    if (d_mirror) {
+      auto* m = static_cast<uint16_t*>(d_mirror);
+      mir = left ? (void*)(m + kd + (size_t)p0 * ldm) : (void*)(m + (size_t)p0 * ldm + kd);
+    }
+    if (left)
+      ck(panel_tf32(true, false, maps, kMapDL, kMapK, 0, kd, kd, p0, h, len, X, lda, mir, ldm, r.status.as<int>(),
+                    r.stream, nullptr),
+         "triangular-solve leaf");
+    else
+      ck(panel_tf32(false, false, maps, kMapDU, kMapMN, 0, kd, p0, kd, h, len, X, lda, mir, ldm, r.status.as<int>(),
+                    r.stream, nullptr),
+         "triangular-solve leaf");
+    r.check_status("triangular-solve leaf");
+    return 0;
+  });
+}
+
+int bgpu_panel_update_device(int n, float* d_a, int lda, int m, int nc, int ar, int ac, int br, int bc, int cr,
+                             int cc) {
+  return status_of([&] {
+    Runtime& r = rt();
+    auto in = [&](int r0, int c0, int rows, int cols) { return r0 >= 0 && c0 >= 0 && r0 + rows <= n && c0 + cols <= n; };
+    const bool bad = n < 1 || lda < n || m < 1 || nc < 1 || std::min(m, nc) > 128 || ar % 4 || br % 4 ||
+                     !in(ar, ac, m, 128) || !in(br, bc, 128, nc) || !in(cr, cc, m, nc);
+    if (bad) {
+      note("error: bgpu_panel_update_device: blocks outside the %d x %d matrix, both sides above 128, or a row offset "
+           "not a multiple of 4", n, n);
+      return 1;
+    }
+    ck(tc_gemm_prepare(), "tensor-core attributes");
+    alignas(64) unsigned char maps[4 * kTensorMapBytes];
+    // the diagonal-block maps are not used: any aligned buffer stands in for them
+    if (!tc_panel_maps(d_a, n, lda, d_a, d_a, maps)) {
+      note("error: bgpu_panel_update_device: cannot build the tensor maps (lda a multiple of 4, 16-byte aligned)");
+      return 1;
+    }
+    float* C = d_a + cr + (size_t)cc * lda;
+    if (m <= nc)
+      ck(panel_tf32(true, true, maps, kMapMN, kMapK, ar, ac, br, bc, m, nc, C, lda, nullptr, 0, r.status.as<int>(),
+                    r.stream, nullptr),
+         "panel update");
+    else
+      ck(panel_tf32(false, true, maps, kMapK, kMapMN, br, bc, ar, ac, nc, m, C, lda, nullptr, 0, r.status.as<int>(),
+                    r.stream, nullptr),
+         "panel update");
+    r.check_status("panel update");
+    return 0;
+  });
+}
+
 static int assemble_device(bool fast, int r0, int r1, int c0, int c1, double* d_out, int ldo) {
   return status_of([&] {
     Solver& s = solver();

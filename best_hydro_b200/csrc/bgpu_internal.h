@@ -25,6 +25,32 @@ enum DevStatus : int {
   kNotFinite = 3,     // a result is NaN or Inf
 };
 
+// Programmatic dependent launch (the factorisation's chain of small launches): a kernel launched
+// by launch_dependent may start while the previous kernel of its stream finishes; it calls
+// pdl_wait() before it touches anything that kernel writes (every kernel so launched does so first),
+// then pdl_trigger() so that the next launch of the stream can start in turn.  Launched the ordinary
+// way, both are no-ops.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                   Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+#endif
+
 // Per-triangle source geometry on the device: p1, p2, p3 (9 doubles), corrected area, 2 pad.
 constexpr int kGeoStride = 12;
 // Incenter: x, y, z, pad.
@@ -221,6 +247,20 @@ cudaError_t stamps_reset(unsigned long long* stamps, int slots, cudaStream_t s);
 // blocks of them named by position (A at rows a_row.., columns a_k..; B at columns b_row..,
 // rows b_k..).
 bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a, void* map_b);
+// Panel products of the FP32 LU on the tensor cores (TF32 operands, FP32 accumulation), a 128 x 128
+// operand R against a panel P of len rows or columns (tc_gemm.cu, k_panel_tf32):
+//   left:  X (h x len) := R P, or -= R P (sub);   right: X (len x h) := P R, or -= P R (sub)
+// maps: four tensor maps (4 kTensorMapBytes, built by tc_panel_maps) over the diagonal-block inverses
+// dl, du (128 x 128 column-major each, one per 128 rows) and the factor (n x n, ld); map_r, map_p pick
+// R's and P's.  The left form reads R through an MN-major map (kMapDL, kMapMN) and P through a K-major
+// one (kMapK); the right form R K-major (kMapDU, kMapK) and P MN-major (kMapMN).  R's block starts at
+// map coordinates (rx0, ry0) (inner, outer), P's at (px0, py0); rx0, px0 multiples of 4.  The assigning
+// form writes the BF16 mirror too (mir: left column-major, right row-major; null: none).
+constexpr int kMapDL = 0, kMapDU = 1, kMapK = 2, kMapMN = 3;
+bool tc_panel_maps(const float* lu32, int n, long ld, const float* dl, const float* du, void* maps);
+cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, int rx0, int ry0, int px0, int py0,
+                       int h, int len, float* X, long ldx, void* mir, long ldm, int* d_status, cudaStream_t s,
+                       unsigned long long* stamp);
 cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
                                   int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s,
                                   unsigned long long* stamp = nullptr);

@@ -94,7 +94,11 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
   asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
   return t;
 }
+// (every kernel of the factorisation's chain starts here: the wait for its predecessor under
+// programmatic dependent launch, the trigger for its successor, then the stamp)
 __device__ __forceinline__ void stamp_begin(unsigned long long* st) {
+  pdl_wait();
+  pdl_trigger();
   if (st && threadIdx.x == 0) atomicMin(st, gtimer_ns());
 }
 __device__ __forceinline__ void stamp_end(unsigned long long* st) {
@@ -619,9 +623,11 @@ void launch_narrow_leaf(const float* dinv, int h, float* B, long ldb, int len, _
   const int nb = len <= 2 * sms * 16 ? 16 : len <= 2 * sms * 32 ? 32 : 64;
 #define BGPU_NARROW(NB)                                                                                  \
   if (LEFT)                                                                                              \
-    k_apply_inv_left<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm, st); \
+    launch_dependent(k_apply_inv_left<NB>, dim3((len + NB - 1) / NB), dim3(256), NarrowLeaf<NB>::smem(), s, dinv, h, \
+                     B, ldb, len, mir, ldm, st);                                                         \
   else                                                                                                   \
-    k_apply_inv_right<NB><<<(len + NB - 1) / NB, 256, NarrowLeaf<NB>::smem(), s>>>(dinv, h, B, ldb, len, mir, ldm, st)
+    launch_dependent(k_apply_inv_right<NB>, dim3((len + NB - 1) / NB), dim3(256), NarrowLeaf<NB>::smem(), s, dinv, \
+                     h, B, ldb, len, mir, ldm, st)
   if (nb == 16) {
     BGPU_NARROW(16);
   } else if (nb == 32) {
@@ -906,10 +912,11 @@ struct CallProfile {
 };
 
 // kinds of the factorisation's stamped launches
-constexpr unsigned char kSlotGemm = 0, kSlotLuLeaf = 1, kSlotSolveLeaf = 2, kSlotSmall = 3;
+constexpr unsigned char kSlotGemm = 0, kSlotLuLeaf = 1, kSlotSolveLeaf = 2, kSlotSmall = 3, kSlotPanel = 4;
 
-// The factorisation's timeline from its launch stamps: how long some kernel ran, a GEMM ran, only
-// leaves ran (LU leaves among them), and nothing ran, between the first start and the last end.
+// The factorisation's timeline from its launch stamps, between the first start and the last end:
+// how long a BF16 GEMM ran, else a TF32 panel update, else a small FP32 update, else only leaves
+// (LU leaves among them), and how long nothing ran.
 std::string timeline_note(const std::vector<unsigned long long>& h, const std::vector<unsigned char>& kind, int n) {
   std::vector<std::pair<unsigned long long, int>> ev;  // (time, +-(1 + kind))
   for (int i = 0; i < n; ++i)
@@ -919,24 +926,27 @@ std::string timeline_note(const std::vector<unsigned long long>& h, const std::v
     }
   if (ev.empty()) return "";
   std::sort(ev.begin(), ev.end());
-  int cnt[4] = {0, 0, 0, 0};
-  double busy = 0, gemm = 0, small = 0, leaves_only = 0, lu_only = 0;
+  int cnt[5] = {0, 0, 0, 0, 0};
+  double busy = 0, gemm = 0, panel = 0, small = 0, leaves_only = 0, lu_only = 0;
   for (size_t i = 0; i + 1 < ev.size(); ++i) {
     const int k = std::abs(ev[i].second) - 1;
     cnt[k] += ev[i].second > 0 ? 1 : -1;
     const double dt = (double)(ev[i + 1].first - ev[i].first) * 1e-6;
-    if (cnt[0] + cnt[1] + cnt[2] + cnt[3] > 0) busy += dt;
-    if (cnt[0] > 0) gemm += dt;
-    if (cnt[0] == 0 && cnt[3] > 0) small += dt;
-    if (cnt[0] == 0 && cnt[3] == 0 && cnt[1] + cnt[2] > 0) leaves_only += dt;
-    if (cnt[0] == 0 && cnt[3] == 0 && cnt[1] > 0) lu_only += dt;
+    const bool any_update = cnt[kSlotGemm] + cnt[kSlotPanel] + cnt[kSlotSmall] > 0;
+    if (cnt[0] + cnt[1] + cnt[2] + cnt[3] + cnt[4] > 0) busy += dt;
+    if (cnt[kSlotGemm] > 0) gemm += dt;
+    if (cnt[kSlotGemm] == 0 && cnt[kSlotPanel] > 0) panel += dt;
+    if (cnt[kSlotGemm] == 0 && cnt[kSlotPanel] == 0 && cnt[kSlotSmall] > 0) small += dt;
+    if (!any_update && cnt[kSlotLuLeaf] + cnt[kSlotSolveLeaf] > 0) leaves_only += dt;
+    if (!any_update && cnt[kSlotLuLeaf] > 0) lu_only += dt;
   }
   const double span = (double)(ev.back().first - ev.front().first) * 1e-6;
-  char note[320];
+  char note[384];
   std::snprintf(note, sizeof note,
-                "factorisation timeline: %.1f ms from first start to last end; a tensor-core GEMM running %.1f ms, "
-                "else a small FP32 update %.1f ms, only leaves %.1f ms (an LU leaf %.1f ms), nothing %.1f ms",
-                span, gemm, small, leaves_only, lu_only, span - busy);
+                "factorisation timeline: %.1f ms from first start to last end; a BF16 tensor-core GEMM running %.1f "
+                "ms, else a TF32 panel update %.1f ms, else a small FP32 update %.1f ms, only leaves %.1f ms (an LU "
+                "leaf %.1f ms), nothing %.1f ms",
+                span, gemm, panel, small, leaves_only, lu_only, span - busy);
   return note;
 }
 
@@ -1010,6 +1020,11 @@ struct MixedSolver::Impl {
   long ldm = 0;
   alignas(64) unsigned char map_am[kTensorMapBytes], map_bm[kTensorMapBytes];
   const void* mirror_key[2] = {};
+  // the triangular-solve leaves on the tensor cores (TF32): tensor maps over the factor and the
+  // diagonal-block inverses; the FP32 CUDA-core leaves when BEST_GPU_SIMT_LEAVES is set
+  bool tc_leaves = true;
+  alignas(64) unsigned char map_leaf[4 * kTensorMapBytes];
+  const void* leaf_key[4] = {};
   int* d_status() { return status.as<int>(); }
   __nv_bfloat16* am_at(int r, int c) const { return am.as<__nv_bfloat16>() + (size_t)r * ldm + c; }
   __nv_bfloat16* bm_at(int r, int c) const { return bm.as<__nv_bfloat16>() + (size_t)c * ldm + r; }
@@ -1019,10 +1034,26 @@ struct MixedSolver::Impl {
   void gemm(int m, int n, int k, int ar, int ac, int br, int bc, int cr, int cc, cudaStream_t s) {
     if (m <= 0 || n <= 0 || k <= 0) return;
     float* C = at_(cr, cc);
+    if (tc_leaves && k == 128 && std::min(m, n) <= 128) {
+      // one side at most 128: the TF32 panel product, the 128-wide operand resident
+      prof.begin(m <= n ? "panel update (TF32, left)" : "panel update (TF32, right)", 2.0 * m * n * k, s);
+      if (m <= n)
+        ck(panel_tf32(true, true, map_leaf, kMapMN, kMapK, ar, ac, br, bc, m, n, C, ld32, nullptr, 0, d_status(), s,
+                      next_stamp(2.0 * m * n * k, kSlotPanel)),
+           "panel update launch");
+      else
+        ck(panel_tf32(false, true, map_leaf, kMapK, kMapMN, br, bc, ar, ac, n, m, C, ld32, nullptr, 0, d_status(), s,
+                      next_stamp(2.0 * m * n * k, kSlotPanel)),
+           "panel update launch");
+      prof.end(s);
+      return;
+    }
     if (small_update(m, n, k)) {
       prof.begin("small update (FP32 cores)", 2.0 * m * n * k, s);
-      k_sgemm_small_minus<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, s>>>(
-          m, n, k, at_(ar, ac), ld32, at_(br, bc), ld32, C, ld32, next_stamp(2.0 * m * n * k, kSlotSmall));
+      ck(launch_dependent(k_sgemm_small_minus, dim3((m + 63) / 64, (n + 63) / 64), dim3(256), 0, s, m, n, k,
+                          (const float*)at_(ar, ac), (long)ld32, (const float*)at_(br, bc), (long)ld32, C, (long)ld32,
+                          next_stamp(2.0 * m * n * k, kSlotSmall)),
+         "small update launch");
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "small update");
@@ -1071,9 +1102,13 @@ struct MixedSolver::Impl {
       const float* dinv = dl32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf;
       __nv_bfloat16* mir = mirrors ? bm_at(kd, c0) : nullptr;
       prof.begin(w >= kWideLeaf ? "trsm leaf (left, wide)" : "trsm leaf (left)", 2.0 * h * h * w, s);
-      if (w >= kWideLeaf)
-        k_leaf_mult<true><<<(w + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(
-            dinv, h, at_(kd, c0), ld32, w, mir, ldm, next_stamp(2.0 * h * h * w, kSlotSolveLeaf));
+      if (tc_leaves)
+        ck(panel_tf32(true, false, map_leaf, kMapDL, kMapK, 0, kd, kd, c0, h, w, at_(kd, c0), ld32, mir, ldm,
+                      d_status(), s, next_stamp(2.0 * h * h * w, kSlotSolveLeaf)),
+           "trsm leaf launch");
+      else if (w >= kWideLeaf)
+        launch_dependent(k_leaf_mult<true>, dim3((w + 127) / 128), dim3(256), (size_t)2 * 128 * kLm * sizeof(float),
+                         s, dinv, h, at_(kd, c0), ld32, w, mir, ldm, next_stamp(2.0 * h * h * w, kSlotSolveLeaf));
       else
         launch_narrow_leaf<true>(dinv, h, at_(kd, c0), ld32, w, mir, ldm, sms, s,
                                  next_stamp(2.0 * h * h * w, kSlotSolveLeaf));
@@ -1095,9 +1130,13 @@ struct MixedSolver::Impl {
       const float* dinv = du32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf;
       __nv_bfloat16* mir = mirrors ? am_at(r0, kd) : nullptr;
       prof.begin(m >= kWideLeaf ? "trsm leaf (right, wide)" : "trsm leaf (right)", 2.0 * h * h * m, s);
-      if (m >= kWideLeaf)
-        k_leaf_mult<false><<<(m + 127) / 128, 256, (size_t)2 * 128 * kLm * sizeof(float), s>>>(
-            dinv, h, at_(r0, kd), ld32, m, mir, ldm, next_stamp(2.0 * h * h * m, kSlotSolveLeaf));
+      if (tc_leaves)
+        ck(panel_tf32(false, false, map_leaf, kMapDU, kMapMN, 0, kd, r0, kd, h, m, at_(r0, kd), ld32, mir, ldm,
+                      d_status(), s, next_stamp(2.0 * h * h * m, kSlotSolveLeaf)),
+           "trsm leaf launch");
+      else if (m >= kWideLeaf)
+        launch_dependent(k_leaf_mult<false>, dim3((m + 127) / 128), dim3(256), (size_t)2 * 128 * kLm * sizeof(float),
+                         s, dinv, h, at_(r0, kd), ld32, m, mir, ldm, next_stamp(2.0 * h * h * m, kSlotSolveLeaf));
       else
         launch_narrow_leaf<false>(dinv, h, at_(r0, kd), ld32, m, mir, ldm, sms, s,
                                   next_stamp(2.0 * h * h * m, kSlotSolveLeaf));
@@ -1119,8 +1158,8 @@ struct MixedSolver::Impl {
       const size_t smem = (size_t)3 * 128 * kS * sizeof(float);
       const size_t off = (size_t)(k0 / kLeaf) * kLeaf * kLeaf;
       prof.begin("LU leaf + inverses", 0, s);
-      k_lu32_leaf_inv<<<1, 512, smem, s>>>(at_(k0, k0), ld32, sz, dl32.as<float>() + off, du32.as<float>() + off,
-                                           d_status(), next_stamp(0, kSlotLuLeaf));
+      launch_dependent(k_lu32_leaf_inv, dim3(1), dim3(512), smem, s, at_(k0, k0), ld32, sz, dl32.as<float>() + off,
+                       du32.as<float>() + off, d_status(), next_stamp(0, kSlotLuLeaf));
       prof.end(s);
       BGPU_COUNT_LAUNCH();
       ck(cudaGetLastError(), "LU leaf");
@@ -1251,6 +1290,16 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   P.du32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (U)");
   P.wl32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain weights (L)");
   P.wu32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain weights (U)");
+  P.tc_leaves = std::getenv("BEST_GPU_SIMT_LEAVES") == nullptr;
+  if (P.tc_leaves && (P.leaf_key[0] != P.lu32.p || P.leaf_key[1] != P.dl32.p || P.leaf_key[2] != P.du32.p ||
+                      P.leaf_key[3] != reinterpret_cast<const void*>((uintptr_t)P.n3))) {
+    if (!tc_panel_maps(P.lu32.as<float>(), P.n3, P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.map_leaf))
+      throw std::runtime_error("cannot build the tensor maps of the triangular-solve leaves");
+    P.leaf_key[0] = P.lu32.p;
+    P.leaf_key[1] = P.dl32.p;
+    P.leaf_key[2] = P.du32.p;
+    P.leaf_key[3] = reinterpret_cast<const void*>((uintptr_t)P.n3);
+  }
   // BF16 mirrors when they fit with 4 GB to spare, else operand copies per product
   const long ldm = round_up(P.n3, 64);
   const size_t mirror_bytes = (size_t)P.n3 * ldm * 2;

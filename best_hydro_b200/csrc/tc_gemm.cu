@@ -140,7 +140,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int m, int n,
                    int k, float* __restrict__ C, long ldc, int tiles_m, int tiles_n, int* status, int a_y0, int a_x0,
                    int b_y0, int b_x0, unsigned long long* stamp) {
-  if (stamp && threadIdx.x == 0) atomicMin(stamp, global_ns());
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;
@@ -177,6 +176,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // the set-up above overlaps the previous launch's tail under programmatic dependent launch; the
+  // operands and C are read only after it has completed
+  pdl_wait();
+  pdl_trigger();
+  if (stamp && threadIdx.x == 0) atomicMin(stamp, global_ns());
 
   if (warp == 0) {
     if (lane == 0) {
@@ -281,6 +285,322 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Panel products of the FP32 LU on the tensor cores (tcgen05 kind::tf32, FP32 accumulation), a
+// 128 x 128 operand R resident in shared memory against a long panel P streamed in 128-long tiles:
+//   left:  X (h x len)  (=|-=)  R (h x 128) P (128 x len)
+//   right: X (len x h)  (=|-=)  P (len x 128) R (128 x h)
+// The triangular-solve leaves are the assigning form (R the inverse of a diagonal block, X = P in
+// place, with the BF16 mirror beside it); the K = 128 updates of the recursion (C -= A B with one
+// side at most 128) the subtracting form.  Both MMA operands must be K-major (kind::tf32 takes no
+// MN-major operand), so the operands that are MN-major in the column-major factor -- the left
+// form's R and the right form's P -- arrive by TMA as four 32 x 32 boxes per 32-deep K chunk and
+// four transposer warps rewrite each chunk K-major (128 rows of 128 bytes, 128-byte swizzle) before
+// the MMA warp uses it.  Shared memory: R (4 chunks of 16 KB), a raw ring (4 x 16 KB, TMA) and an
+// operand ring (4 x 16 KB); two TMEM accumulators of 128 x 128 FP32.
+constexpr int kPtStages = 4;
+constexpr uint32_t kPtChunk = 128 * 32 * 4;  // 16 KB
+constexpr uint32_t kPtSmem = 4 * kPtChunk + 2 * kPtStages * kPtChunk + 1024 + 256;
+constexpr uint32_t kPtTmemCols = 256;
+constexpr int kPtTrWarps = 4;
+constexpr int kPtThreads = 64 + 32 * kEpiWarps + 32 * kPtTrWarps;
+// instruction descriptor, kind::tf32: D FP32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2),
+// both K-major, N = 128 (>> 3 at bits 17-22), M = 128 (>> 4 at bits 24-28)
+constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                                ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdescTf32), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// One 16 KB chunk from four MN-major boxes (box c: MN rows 32 c .. 32 c + 31; K row k at 128 k bytes,
+// 16-byte group g of a row at (g ^ (k & 7)) -- the TMA's 128-byte swizzle) to the K-major layout
+// (MN row r at 128 r bytes, K group g at (g ^ (r & 7))).  t: 0 .. 127 (the transposer threads); each
+// writes 8 groups of 4 K values, a warp 32 consecutive rows (reads and writes free of bank conflicts).
+__device__ __forceinline__ void transpose_chunk(const uint8_t* src, uint8_t* dst, int t) {
+  const int lane = t & 31, w = t >> 5;
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int mn = lane + 32 * (it & 3), kg = w + 4 * (it >> 2);
+    const uint8_t* sb = src + (mn >> 5) * 4096 + (mn & 3) * 4;
+    float v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = 4 * kg + e;
+      v[e] = *reinterpret_cast<const float*>(sb + k * 128 + ((((mn & 31) >> 2) ^ (k & 7)) << 4));
+    }
+    *reinterpret_cast<float4*>(dst + mn * 128 + ((kg ^ (mn & 7)) << 4)) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// tmR, tmP: R's and P's tensor maps (K-major sources: 32 x 128 boxes, one per K chunk; MN-major
+// sources: 32 x 32 boxes).  R starts at (rx0, ry0) of its map, P at (px0, py0): left, R's box
+// (rx0 + 32 c, ry0 + 32 kc) and P's (px0 + 32 kc, py0 + 128 tile); right, R's (rx0 + 32 kc, ry0)
+// and P's (px0 + 128 tile + 32 c, py0 + 32 kc).  X: the result block (ldx), h its extent along R.
+template <bool LEFT, bool SUB>
+__global__ void __launch_bounds__(kPtThreads, 1)
+    k_panel_tf32(const __grid_constant__ CUtensorMap tmR, const __grid_constant__ CUtensorMap tmP, int rx0, int ry0,
+                 int px0, int py0, int h, int len, float* __restrict__ X, long ldx, __nv_bfloat16* __restrict__ mir,
+                 long ldm, int* status, unsigned long long* stamp) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint8_t* sR = smem;                               // R, K-major: 4 chunks
+  uint8_t* sRaw = smem + 4 * kPtChunk;              // TMA ring of MN-major boxes (left: R's, once)
+  uint8_t* sOp = sRaw + kPtStages * kPtChunk;       // P's K-major chunks
+  uint64_t* raw_full = reinterpret_cast<uint64_t*>(sOp + kPtStages * kPtChunk);
+  uint64_t* raw_empty = raw_full + kPtStages;
+  uint64_t* op_full = raw_empty + kPtStages;
+  uint64_t* op_empty = op_full + kPtStages;
+  uint64_t* acc_full = op_empty + kPtStages;  // [2]
+  uint64_t* acc_empty = acc_full + 2;         // [2]
+  uint64_t* r_raw = acc_empty + 2;            // left: R's boxes landed
+  uint64_t* r_full = r_raw + 1;               // R ready (K-major)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(r_full + 1);
+  __shared__ int s_abort;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntiles = (len + 127) / 128;
+  const int tr_first = 2 + kEpiWarps;  // the transposer warps
+
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < kPtStages; ++s) {
+      mbar_init(&raw_full[s], 1);
+      mbar_init(&raw_empty[s], kPtTrWarps);
+      mbar_init(&op_full[s], LEFT ? 1 : kPtTrWarps);
+      mbar_init(&op_empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], kEpiWarps);
+    }
+    mbar_init(r_raw, 1);
+    mbar_init(r_full, LEFT ? kPtTrWarps : 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kPtTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  pdl_wait();
+  pdl_trigger();
+  if (stamp && threadIdx.x == 0) atomicMin(stamp, global_ns());
+
+  if (warp == 0) {
+    if (lane == 0) {
+      if (LEFT) {
+        // R's MN-major boxes into the raw ring (free until the transposers have read them)
+        mbar_expect_tx(r_raw, 4 * kPtChunk);
+        for (int kc = 0; kc < 4; ++kc)
+          for (int c = 0; c < 4; ++c) tma_load_2d(sRaw + kc * kPtChunk + c * 4096, &tmR, rx0 + 32 * c, ry0 + 32 * kc, r_raw);
+      } else {
+        mbar_expect_tx(r_full, 4 * kPtChunk);
+        for (int kc = 0; kc < 4; ++kc) tma_load_2d(sR + kc * kPtChunk, &tmR, rx0 + 32 * kc, ry0, r_full);
+      }
+      uint32_t it = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !*(volatile int*)&s_abort; tile += gridDim.x) {
+        for (int kc = 0; kc < 4; ++kc, ++it) {
+          const uint32_t s = it % kPtStages;
+          uint64_t* freed = LEFT ? &op_empty[s] : &raw_empty[s];
+          if (it >= kPtStages && !mbar_wait(freed, ((it / kPtStages) & 1) ^ 1, status)) {
+            s_abort = 1;
+            break;
+          }
+          if (*(volatile int*)&s_abort) break;
+          if (LEFT) {
+            mbar_expect_tx(&op_full[s], kPtChunk);
+            tma_load_2d(sOp + s * kPtChunk, &tmP, px0 + 32 * kc, py0 + 128 * tile, &op_full[s]);
+          } else {
+            mbar_expect_tx(&raw_full[s], kPtChunk);
+            for (int c = 0; c < 4; ++c)
+              tma_load_2d(sRaw + s * kPtChunk + c * 4096, &tmP, px0 + 128 * tile + 32 * c, py0 + 32 * kc, &raw_full[s]);
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      bool ok = mbar_wait(r_full, 0, status);
+      if (!ok) s_abort = 1;
+      tc_fence_after();
+      uint32_t it = 0, local = 0;
+      for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++local) {
+        const uint32_t b = local & 1, use = local >> 1;
+        if (use >= 1 && !mbar_wait(&acc_empty[b], (use - 1) & 1, status)) {
+          s_abort = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc = tmem + b * 128;
+        for (int kc = 0; kc < 4; ++kc, ++it) {
+          const uint32_t s = it % kPtStages;
+          if (!mbar_wait(&op_full[s], (it / kPtStages) & 1, status)) {
+            s_abort = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t r0s = smem_u32(sR + kc * kPtChunk), p0s = smem_u32(sOp + s * kPtChunk);
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            // K step of 8: 32 bytes along the 128-byte rows of both operands
+            const uint64_t rd = sw128_desc(r0s + kk * 32), pd = sw128_desc(p0s + kk * 32);
+            mma_tf32(acc, LEFT ? rd : pd, LEFT ? pd : rd, (kc > 0 || kk > 0) ? 1u : 0u);
+          }
+          mma_commit(&op_empty[s]);
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[b]);
+      }
+    }
+  } else if (warp >= tr_first) {
+    const int t = threadIdx.x - 32 * tr_first;
+    if (LEFT) {
+      if (mbar_wait(r_raw, 0, status) && !*(volatile int*)&s_abort) {
+        for (int kc = 0; kc < 4; ++kc) transpose_chunk(sRaw + kc * kPtChunk, sR + kc * kPtChunk, t);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(r_full);
+      } else {
+        s_abort = 1;
+      }
+    } else {
+      uint32_t it = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        bool ok = true;
+        for (int kc = 0; kc < 4; ++kc, ++it) {
+          const uint32_t s = it % kPtStages;
+          if (!mbar_wait(&raw_full[s], (it / kPtStages) & 1, status) ||
+              (it >= kPtStages && !mbar_wait(&op_empty[s], ((it / kPtStages) & 1) ^ 1, status)) ||
+              *(volatile int*)&s_abort) {
+            s_abort = 1;
+            ok = false;
+            break;
+          }
+          transpose_chunk(sRaw + s * kPtChunk, sOp + s * kPtChunk, t);
+          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+          __syncwarp();
+          if (lane == 0) {
+            mbar_arrive(&raw_empty[s]);
+            mbar_arrive(&op_full[s]);
+          }
+        }
+        if (!ok) break;
+      }
+    }
+  } else {
+    // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (the tile's rows), columns [64 half, 64 half + 64)
+    const int q = warp & 3, half = (warp - 2) >> 2;
+    const int r = q * 32 + lane;  // accumulator row
+    uint32_t local = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
+      const uint32_t b = local & 1, use = local >> 1;
+      // left: X row r (valid below h), columns 128 tile + j; right: X row 128 tile + r (valid below len),
+      // columns j (valid below h); j = 64 half + 0 .. 63
+      const int xrow = LEFT ? r : 128 * tile + r;
+      const bool rok = LEFT ? r < h : xrow < len;
+      const int jlim = LEFT ? len - 128 * tile : h;  // columns j below jlim are valid
+      float* xp = X + (LEFT ? (size_t)(128 * tile) * ldx : (size_t)0) + xrow;
+      // (sub) C's first 32 columns loaded before the accumulator is ready, the next 32 while the first
+      // are stored
+      float cv[SUB ? 32 : 1], nv[SUB ? 32 : 1];
+      if constexpr (SUB) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int col = 64 * half + j;
+          cv[j] = (rok && col < jlim) ? __ldcs(xp + (size_t)col * ldx) : 0.f;
+        }
+      }
+      if (!mbar_wait(&acc_full[b], use & 1, status) || *(volatile int*)&s_abort) break;
+      tc_fence_after();
+#pragma unroll 1
+      for (int c = 0; c < 2; ++c) {
+        float v[32];
+        const int j0 = 64 * half + 32 * c;
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * 128 + (uint32_t)j0, v);
+        if constexpr (SUB) {
+          if (c == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const int col = j0 + 32 + j;
+              nv[j] = (rok && col < jlim) ? __ldcs(xp + (size_t)col * ldx) : 0.f;
+            }
+          }
+          if (rok) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (j0 + j < jlim) __stcs(xp + (size_t)(j0 + j) * ldx, cv[j] - v[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) cv[j] = nv[j];
+          continue;
+        }
+        if (!rok) continue;
+        if constexpr (SUB) {
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (j0 + j < jlim) xp[(size_t)(j0 + j) * ldx] = v[j];
+          if (mir) {
+            if (LEFT) {
+              // column-major mirror: element (r, 128 tile + j)
+              __nv_bfloat16* mp = mir + (size_t)(128 * tile) * ldm + r;
+#pragma unroll
+              for (int j = 0; j < 32; ++j)
+                if (j0 + j < jlim) mp[(size_t)(j0 + j) * ldm] = __float2bfloat16_rn(v[j]);
+            } else {
+              // row-major mirror: row xrow, 32 consecutive columns
+              __nv_bfloat16* dst = mir + (size_t)xrow * ldm + j0;
+              if (j0 + 32 <= jlim && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0)) {
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                  uint4 pk;
+                  uint32_t* w = reinterpret_cast<uint32_t*>(&pk);
+#pragma unroll
+                  for (int e = 0; e < 4; ++e) {
+                    const __nv_bfloat162 two = __floats2bfloat162_rn(v[8 * g + 2 * e], v[8 * g + 2 * e + 1]);
+                    w[e] = *reinterpret_cast<const uint32_t*>(&two);
+                  }
+                  *reinterpret_cast<uint4*>(dst + 8 * g) = pk;
+                }
+              } else {
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                  if (j0 + j < jlim) dst[j] = __float2bfloat16_rn(v[j]);
+              }
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[b]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kPtTmemCols));
+  }
+  if (stamp && threadIdx.x == 0) {
+    __threadfence();
+    atomicMax(stamp + 1, global_ns());
+  }
+}
+
 __global__ void k_stamps_reset(unsigned long long* stamps, int slots) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < slots; i += gridDim.x * blockDim.x) {
     stamps[2 * i] = ~0ull;
@@ -351,6 +671,20 @@ bool make_map(CUtensorMap* tm, const void* base, int rows, int cols, long ld, in
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2-D FP32 tensor map: `outer` rows of `inner` elements (pitch ld elements), box 32 x box_outer,
+// 128-byte swizzle, zero fill outside.
+bool make_map_f32(CUtensorMap* tm, const void* base, long inner, long outer, long ld, int box_outer) {
+  EncodeTiled fn = encoder();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  cuuint32_t box[2] = {32u, (cuuint32_t)box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // one CTA per SM (at most one per tile)
 int persistent_grid(int tiles) {
   static int sms = 0;
@@ -396,7 +730,53 @@ bool tc_operand_maps(const void* At, int rows_a, long lda_t, const void* Bt, int
 }
 
 cudaError_t tc_gemm_prepare() {
-  return cudaFuncSetAttribute(k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+  cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_panel_tf32<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_panel_tf32<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_panel_tf32<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_panel_tf32<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
+  return e;
+}
+
+bool tc_panel_maps(const float* lu32, int n, long ld, const float* dl, const float* du, void* maps) {
+  if ((ld % 4) || ((uintptr_t)lu32 & 15) || ((uintptr_t)dl & 15) || ((uintptr_t)du & 15) || n <= 0) return false;
+  CUtensorMap* m = static_cast<CUtensorMap*>(maps);
+  const long diag_rows = (long)((n + 127) / 128) * 128;
+  return make_map_f32(&m[kMapDL], dl, 128, diag_rows, 128, 32) &&    // MN-major boxes
+         make_map_f32(&m[kMapDU], du, 128, diag_rows, 128, 128) &&   // K-major boxes
+         make_map_f32(&m[kMapK], lu32, n, n, ld, 128) &&             // K-major boxes
+         make_map_f32(&m[kMapMN], lu32, n, n, ld, 32);               // MN-major boxes
+}
+
+cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, int rx0, int ry0, int px0, int py0,
+                       int h, int len, float* X, long ldx, void* mir, long ldm, int* d_status, cudaStream_t s,
+                       unsigned long long* stamp) {
+  if (len <= 0 || h <= 0) return cudaSuccess;
+  // TMA: the innermost coordinate of every box a multiple of 4 FP32 elements (16 bytes)
+  if (h > 128 || (rx0 % 4) || (px0 % 4) || map_r < 0 || map_r > 3 || map_p < 0 || map_p > 3)
+    return cudaErrorInvalidValue;
+  const CUtensorMap* m = static_cast<const CUtensorMap*>(maps);
+  const dim3 grid(persistent_grid((len + 127) / 128)), block(kPtThreads);
+  __nv_bfloat16* mb = static_cast<__nv_bfloat16*>(mir);
+  cudaError_t e;
+  if (left && !sub)
+    e = launch_dependent(k_panel_tf32<true, false>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0,
+                         h, len, X, ldx, mb, ldm, d_status, stamp);
+  else if (!left && !sub)
+    e = launch_dependent(k_panel_tf32<false, false>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0,
+                         h, len, X, ldx, mb, ldm, d_status, stamp);
+  else if (left)
+    e = launch_dependent(k_panel_tf32<true, true>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0, h,
+                         len, X, ldx, mb, ldm, d_status, stamp);
+  else
+    e = launch_dependent(k_panel_tf32<false, true>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0,
+                         h, len, X, ldx, mb, ldm, d_status, stamp);
+  BGPU_COUNT_LAUNCH();
+  return e;
 }
 
 // (tc_gemm_prepare must have run: the launch may be captured into a graph)
@@ -404,11 +784,12 @@ cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, cons
                                     int* d_status, cudaStream_t s, unsigned long long* stamp) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
-      *static_cast<const CUtensorMap*>(map_a), *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m,
-      tiles_n, d_status, 0, 0, 0, 0, stamp);
+  const cudaError_t e = launch_dependent(k_gemm_bf16_tc, dim3(persistent_grid(tiles_m * tiles_n)), dim3(kThreads),
+                                         kSmem, s, *static_cast<const CUtensorMap*>(map_a),
+                                         *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m, tiles_n,
+                                         d_status, 0, 0, 0, 0, stamp);
   BGPU_COUNT_LAUNCH();
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t stamps_reset(unsigned long long* stamps, int slots, cudaStream_t s) {
@@ -435,11 +816,12 @@ cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   if ((a_k % 8) || (b_k % 8) || (k % BK)) return cudaErrorInvalidValue;
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
-      *static_cast<const CUtensorMap*>(map_a), *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m,
-      tiles_n, d_status, a_row, a_k, b_row, b_k, stamp);
+  const cudaError_t e = launch_dependent(k_gemm_bf16_tc, dim3(persistent_grid(tiles_m * tiles_n)), dim3(kThreads),
+                                         kSmem, s, *static_cast<const CUtensorMap*>(map_a),
+                                         *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m, tiles_n,
+                                         d_status, a_row, a_k, b_row, b_k, stamp);
   BGPU_COUNT_LAUNCH();
-  return cudaGetLastError();
+  return e;
 }
 
 // C (m x n FP32, ldc) -= At^T-major A (m x k, row-major BF16, lda_t) * B (k x n column-major BF16,

@@ -69,6 +69,88 @@ def test_lu32_leaf(h):
     assert np.all(LI[h:, :] == 0) and np.all(LI[:, h:] == 0) and np.all(UI[h:, :] == 0) and np.all(UI[:, h:] == 0)
 
 
+@pytest.mark.parametrize("left,kd,p0,length", [(True, 128, 256, 344), (False, 256, 32, 568), (True, 512, 0, 512),
+                                               (False, 512, 96, 416), (True, 0, 128, 96)])
+def test_trsm_leaf_tc(left, kd, p0, length):
+    """The LU's triangular-solve leaf on the tensor cores (TF32 operands, FP32 accumulation): the
+    block (h rows from kd x length columns from p0, or length rows x h columns) times the inverse
+    diagonal block, against an FP64 product, within 2^-8 of |Dinv| |B| (TF32 rounding of both
+    operands); the BF16 mirror equal to the result rounded to nearest; everything outside the block
+    untouched.  n = 600: the last leaf is ragged (h = 88), as are the last tiles."""
+    torch = _torch()
+    n, lda, ldm = 600, 604, 640
+    nleaves = (n + 127) // 128
+    h = min(128, n - kd)
+    rng = np.random.default_rng(kd * 7 + p0 + length + int(left))
+    A = rng.standard_normal((n, n)).astype(np.float32)  # the matrix, A[i, j]
+    D = np.zeros((nleaves, 128, 128), dtype=np.float32)  # D[b][i, k]: block b's inverse
+    for b in range(nleaves):
+        hb = min(128, n - 128 * b)
+        D[b, :hb, :hb] = rng.standard_normal((hb, hb)).astype(np.float32) / np.sqrt(hb)
+    dA = torch.zeros((n, lda), dtype=torch.float32)
+    dA[:, :n] = torch.from_numpy(np.ascontiguousarray(A.T))  # column j at row j
+    dA = dA.cuda()
+    # column-major 128 x 128 blocks, stacked: element (i, k) of block b at b*16384 + k*128 + i
+    dD = torch.from_numpy(np.ascontiguousarray(np.transpose(D, (0, 2, 1)))).cuda()
+    dZ = torch.full_like(dD, float("nan"))  # the unused inverse: never read
+    mirror = torch.full((n, ldm), 3.0, dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    dl, du = (dD, dZ) if left else (dZ, dD)
+    bh.trsm_leaf_device(left, n, dA.data_ptr(), lda, dl.data_ptr(), du.data_ptr(), kd, p0, h, length,
+                        mirror.data_ptr(), ldm)
+    got_all = dA.cpu().numpy()[:, :n].T.astype(np.float64)  # got_all[i, j]
+    Dk = D[kd // 128, :h, :h].astype(np.float64)
+    A64 = A.astype(np.float64)
+    if left:
+        blk = (slice(kd, kd + h), slice(p0, p0 + length))
+        want = Dk @ A64[blk]
+        bound = np.abs(Dk) @ np.abs(A64[blk])
+    else:
+        blk = (slice(p0, p0 + length), slice(kd, kd + h))
+        want = A64[blk] @ Dk
+        bound = np.abs(A64[blk]) @ np.abs(Dk)
+    got = got_all[blk]
+    assert np.all(np.abs(got - want) <= 2.0 ** -8 * bound + 1e-30), np.max(np.abs(got - want) / bound)
+    outside = np.ones((n, n), dtype=bool)
+    outside[blk] = False
+    assert np.array_equal(got_all[outside], A64[outside])
+    # the mirror: left column-major (element (i, j) at row j of the torch array), right row-major
+    mir = mirror.float().cpu().numpy()
+    mir_blk = mir[:, :n].T[blk] if left else mir[:, :n][blk]
+    want_mir = torch.from_numpy(got.astype(np.float32)).bfloat16().float().numpy()
+    assert np.array_equal(mir_blk, want_mir)
+    mir_out = (mir[:, :n].T if left else mir[:, :n])[outside]
+    assert np.all(mir_out == 3.0)
+
+
+@pytest.mark.parametrize("m,nc", [(128, 300), (300, 100), (50, 384), (128, 128), (384, 7)])
+def test_panel_update_tc(m, nc):
+    """The LU's K = 128 update on the tensor cores (TF32 operands, FP32 accumulation): C -= A B with
+    one side at most 128 (the left form for m <= nc, the right one otherwise), against FP64 within
+    2^-8 of |A| |B|; everything outside C untouched; ragged sizes."""
+    torch = _torch()
+    n, lda = 640, 644
+    ar, ac, br, bc, cr, cc = 0, 0, 128, 128, 256, 256
+    rng = np.random.default_rng(m * 1000 + nc)
+    A = rng.standard_normal((n, n)).astype(np.float32)
+    dA = torch.zeros((n, lda), dtype=torch.float32)
+    dA[:, :n] = torch.from_numpy(np.ascontiguousarray(A.T))
+    dA = dA.cuda()
+    torch.cuda.synchronize()
+    bh.panel_update_device(n, dA.data_ptr(), lda, m, nc, ar, ac, br, bc, cr, cc)
+    got_all = dA.cpu().numpy()[:, :n].T.astype(np.float64)
+    A64 = A.astype(np.float64)
+    a, b = A64[ar:ar + m, ac:ac + 128], A64[br:br + 128, bc:bc + nc]
+    blk = (slice(cr, cr + m), slice(cc, cc + nc))
+    want = A64[blk] - a @ b
+    bound = np.abs(a) @ np.abs(b)
+    err = np.abs(got_all[blk] - want)
+    assert np.all(err <= 2.0 ** -8 * bound + 1e-6 * np.abs(A64[blk])), np.max(err / bound)
+    outside = np.ones((n, n), dtype=bool)
+    outside[blk] = False
+    assert np.array_equal(got_all[outside], A64[outside])
+
+
 def compare(g, o, tol=TOL):
     for key in ("Dtt", "Drr"):
         assert rel(g["tensors"][key], o.tensors[key]) < tol, key
