@@ -160,6 +160,67 @@ __device__ __forceinline__ void small_mm(const float* A, const float* B, float* 
     }
 }
 
+// One doubling step of a 32 x 32 triangular inverse by one warp (T the triangle, X its inverse, both
+// at (o, o) of stride-kS column-major blocks): with the inverses of the S x S diagonal blocks of every
+// 2S x 2S diagonal block already in X, the off-diagonal S x S block of each 2S block's inverse,
+//   lower: X21 = -X22 (T21 X11),   upper: X12 = -X11 (T12 X22),
+// the product in parentheses staged in X21 (X12) itself.  16 S outputs, S / 2 per lane (16 lanes for
+// S = 1); each a full S-term sum (the zero triangles of X take part).
+template <int S, bool LOWER>
+__device__ __forceinline__ void tri_inv_step(const float* T, float* X, int o, int lane) {
+  constexpr int NOUT = 16 * S, Q = NOUT >= 32 ? NOUT / 32 : 1;
+  auto at = [o](int r, int c) { return (o + c) * kS + o + r; };
+  float y[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int e = lane + 32 * q, p = e / (S * S), rem = e % (S * S), i = rem % S, j = rem / S, b = 2 * S * p;
+    float acc = 0.f;
+    if (e < NOUT) {
+#pragma unroll
+      for (int k = 0; k < S; ++k)
+        acc += LOWER ? T[at(b + S + i, b + k)] * X[at(b + k, b + j)] : T[at(b + i, b + S + k)] * X[at(b + S + k, b + S + j)];
+    }
+    y[q] = acc;
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int e = lane + 32 * q, p = e / (S * S), rem = e % (S * S), i = rem % S, j = rem / S, b = 2 * S * p;
+    if (e < NOUT) X[LOWER ? at(b + S + i, b + j) : at(b + i, b + S + j)] = y[q];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int e = lane + 32 * q, p = e / (S * S), rem = e % (S * S), i = rem % S, j = rem / S, b = 2 * S * p;
+    float acc = 0.f;
+    if (e < NOUT) {
+#pragma unroll
+      for (int k = 0; k < S; ++k)
+        acc += LOWER ? X[at(b + S + i, b + S + k)] * X[at(b + S + k, b + j)] : X[at(b + i, b + k)] * X[at(b + k, b + S + j)];
+    }
+    y[q] = -acc;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int e = lane + 32 * q, p = e / (S * S), rem = e % (S * S), i = rem % S, j = rem / S, b = 2 * S * p;
+    if (e < NOUT) X[LOWER ? at(b + S + i, b + j) : at(b + i, b + S + j)] = y[q];
+  }
+  __syncwarp();
+}
+
+// The inverse of the 32 x 32 triangle of T at (o, o) into X (zero there beforehand): lower with unit
+// diagonal, or upper; five doubling steps from the diagonal up (log-depth, no 32-step substitution).
+template <bool LOWER>
+__device__ __forceinline__ void tri_inv32(const float* T, float* X, int o, int lane) {
+  X[(o + lane) * kS + o + lane] = LOWER ? 1.f : 1.f / T[(o + lane) * kS + o + lane];
+  __syncwarp();
+  tri_inv_step<1, LOWER>(T, X, o, lane);
+  tri_inv_step<2, LOWER>(T, X, o, lane);
+  tri_inv_step<4, LOWER>(T, X, o, lane);
+  tri_inv_step<8, LOWER>(T, X, o, lane);
+  tri_inv_step<16, LOWER>(T, X, o, lane);
+}
+
 // The 32 x 32 diagonal block at (o, o): LU by warp 0, then L^-1 by warp 0 and U^-1 by warp 1.
 // Called by all threads (it ends with a block barrier).
 __device__ __noinline__ void leaf_base32(float* M, float* LI, float* UI, int o, int* bad) {
@@ -184,31 +245,10 @@ __device__ __noinline__ void leaf_base32(float* M, float* LI, float* UI, int o, 
     for (int j = 0; j < 32; ++j) M[(o + j) * kS + o + lane] = r[j];
   }
   __syncthreads();
-  if (warp == 0) {
-    // column c = lane of L^-1: x_c = 1, x_i = -sum_{j < i} L_ij x_j (x_j = 0 for j < c)
-    float x[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      float sum = 0.f;
-#pragma unroll
-      for (int j = 0; j < i; ++j) sum += M[(o + j) * kS + o + i] * x[j];
-      x[i] = (i == lane) ? 1.f : (i > lane ? -sum : 0.f);
-    }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) LI[(o + lane) * kS + o + i] = x[i];
-  } else if (warp == 1) {
-    // column c = lane of U^-1: x_i = (delta_ic - sum_{j > i} U_ij x_j) / U_ii, i = 31 .. 0
-    float x[32];
-#pragma unroll
-    for (int i = 31; i >= 0; --i) {
-      float sum = 0.f;
-#pragma unroll
-      for (int j = i + 1; j < 32; ++j) sum += M[(o + j) * kS + o + i] * x[j];
-      x[i] = ((i == lane ? 1.f : 0.f) - sum) / M[(o + i) * kS + o + i];
-    }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) UI[(o + lane) * kS + o + i] = x[i];
-  }
+  if (warp == 0)
+    tri_inv32<true>(M, LI, o, lane);
+  else if (warp == 1)
+    tri_inv32<false>(M, UI, o, lane);
   __syncthreads();
 }
 
@@ -976,6 +1016,7 @@ struct MixedSolver::Impl {
   int slot_cap = 0, nslots = 0;
   double slot_work = 0;  // GEMM flops
   std::vector<unsigned char> slot_kind;  // kSlot* of each slot, in launch order
+  std::vector<double> slot_flop;         // and its flops
   int graph_slots = 0;
   double graph_work = 0;
   // the solve's buffers for q right-hand sides per pass (GMRES vectors, FP32 preconditioner
@@ -995,6 +1036,7 @@ struct MixedSolver::Impl {
     if (nslots >= slot_cap) return nullptr;
     if (kind == kSlotGemm) slot_work += flops;
     slot_kind.push_back(kind);
+    slot_flop.push_back(flops);
     return stamps.as<unsigned long long>() + 2 * (size_t)nslots++;
   }
   int n3 = 0;
@@ -1375,6 +1417,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     P.nslots = 0;
     P.slot_work = 0;
     P.slot_kind.clear();
+    P.slot_flop.clear();
     ck(stamps_reset(P.stamps.as<unsigned long long>(), P.slot_cap, s), "stamps");
     P.rlu(0, P.n3, s);  // direct launches in order, each timed
     ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3, P.wl32.as<float>(),
@@ -1400,6 +1443,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       P.nslots = 0;
       P.slot_work = 0;
       P.slot_kind.clear();
+      P.slot_flop.clear();
       try {
         P.rlu(0, P.n3, cs);
         ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3,
@@ -1470,6 +1514,16 @@ void MixedSolver::finish_build(cudaStream_t s) {
     kt.add(gemms, ns * 1e-6, used_work);
     const std::string tl = timeline_note(h, P.slot_kind, used_slots);
     if (!tl.empty()) P.host_note += "; " + tl;
+    // BEST_GPU_TIMELINE=<file>: every stamped launch of this factorisation appended as
+    // "slot,kind,flops,start_ns,end_ns" (kinds: 0 BF16 GEMM, 1 LU leaf, 2 triangular-solve leaf,
+    // 3 small FP32 update, 4 TF32 panel update)
+    if (const char* path = std::getenv("BEST_GPU_TIMELINE")) {
+      if (FILE* f = std::fopen(path, "a")) {
+        for (int i = 0; i < used_slots && i < (int)P.slot_kind.size(); ++i)
+          std::fprintf(f, "%d,%d,%.0f,%llu,%llu\n", i, (int)P.slot_kind[i], P.slot_flop[i], h[2 * i], h[2 * i + 1]);
+        std::fclose(f);
+      }
+    }
   }
   if (st != 0) {
     ck(cudaMemsetAsync(P.status.p, 0, sizeof(int), s), "status clear");

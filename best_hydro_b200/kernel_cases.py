@@ -6,6 +6,9 @@
                                                              # (mixed: the mixed path's assembly)
     python -m best_hydro_b200.kernel_cases mixed F           # mixed build + solve, ellipsoid frequency F
     python -m best_hydro_b200.kernel_cases adjoint F         # FP64 build + adjoint gradients (k_pair_adjoint)
+    python -m best_hydro_b200.kernel_cases panel left|right leaf|update LEN
+                                                             # k_panel_tf32: a triangular-solve leaf or a
+                                                             # K = 128 update on a 128 x LEN panel
 
 Each case launches its kernel twice (the second launch is the one to capture: `ncu -k <kernel>
 -s 1 -c 1`) and prints the CUDA-event time of the second launch.
@@ -50,6 +53,28 @@ def main(argv):
                   f"(whole call {call:.3f} ms)")
         else:
             print(f"{case} {m}x{n}x{k}: call {call:.3f} ms, {2.0 * m * n * k / call / 1e9:.1f} TFLOP/s")
+        return 0
+    if case == "panel":
+        left, leaf, length = argv[1] == "left", argv[2] == "leaf", int(argv[3])
+        n = length + 256
+        lda = (n + 3) // 4 * 4
+        g = torch.Generator(device=dev).manual_seed(0)
+        a = torch.randn(n, lda, dtype=torch.float32, device=dev, generator=g)  # a[j] = column j
+        nleaves = (n + 127) // 128
+        d = torch.randn(nleaves, 128, 128, dtype=torch.float32, device=dev, generator=g) / 16
+        mir = torch.zeros(n, lda, dtype=torch.bfloat16, device=dev)
+        torch.cuda.synchronize()
+        for _ in range(2):
+            if leaf:
+                # left: rows [0, 128) x columns [256, 256 + LEN); right: rows [256, ..) x columns [0, 128)
+                bh.trsm_leaf_device(left, n, a.data_ptr(), lda, d.data_ptr(), d.data_ptr(), 0, 256, 128, length,
+                                    mir.data_ptr(), lda)
+            elif left:
+                bh.panel_update_device(n, a.data_ptr(), lda, 128, length, 128, 0, 0, 256, 128, 256)
+            else:
+                bh.panel_update_device(n, a.data_ptr(), lda, length, 128, 256, 0, 0, 128, 256, 128)
+        torch.cuda.synchronize()
+        print(f"panel {'left' if left else 'right'} {'leaf' if leaf else 'update'} 128 x {length}: done")
         return 0
     if case == "adjoint":
         from best_hydro_b200 import meshes
