@@ -1567,17 +1567,22 @@ int bgpu_trsm_leaf_device(int left, int n, float* d_a, int lda, const float* d_l
     }
     float* X = left ? d_a + kd + (size_t)p0 * lda : d_a + p0 + (size_t)kd * lda;
     void* mir = nullptr;
+    alignas(64) unsigned char mmaps[2 * kTensorMapBytes];
     if (d_mirror) {
       auto* m = static_cast<uint16_t*>(d_mirror);
       mir = left ? (void*)(m + kd + (size_t)p0 * ldm) : (void*)(m + (size_t)p0 * ldm + kd);
+      if (!tc_mirror_store_maps(d_mirror, d_mirror, n, ldm, mmaps)) {
+        note("error: bgpu_trsm_leaf_device: cannot build the mirror's tensor maps (ldm a multiple of 8, aligned)");
+        return 1;
+      }
     }
     if (left)
-      ck(panel_tf32(true, false, maps, kMapDL, kMapK, 0, kd, kd, p0, h, len, X, lda, mir, ldm, r.status.as<int>(),
-                    r.stream, nullptr),
+      ck(panel_tf32(true, false, maps, kMapDL, kMapK, mmaps, 0, kd, kd, p0, h, len, X, lda, kd, p0, mir, ldm,
+                    r.status.as<int>(), r.stream, nullptr),
          "triangular-solve leaf");
     else
-      ck(panel_tf32(false, false, maps, kMapDU, kMapMN, 0, kd, p0, kd, h, len, X, lda, mir, ldm, r.status.as<int>(),
-                    r.stream, nullptr),
+      ck(panel_tf32(false, false, maps, kMapDU, kMapMN, mmaps, 0, kd, p0, kd, h, len, X, lda, p0, kd, mir, ldm,
+                    r.status.as<int>(), r.stream, nullptr),
          "triangular-solve leaf");
     r.check_status("triangular-solve leaf");
     return 0;
@@ -1589,7 +1594,7 @@ int bgpu_panel_update_device(int n, float* d_a, int lda, int m, int nc, int ar, 
   return status_of([&] {
     Runtime& r = rt();
     auto in = [&](int r0, int c0, int rows, int cols) { return r0 >= 0 && c0 >= 0 && r0 + rows <= n && c0 + cols <= n; };
-    const bool bad = n < 1 || lda < n || m < 1 || nc < 1 || std::min(m, nc) > 128 || ar % 4 || br % 4 ||
+    const bool bad = n < 1 || lda < n || m < 1 || nc < 1 || std::min(m, nc) > 128 || ar % 4 || br % 4 || cr % 4 ||
                      !in(ar, ac, m, 128) || !in(br, bc, 128, nc) || !in(cr, cc, m, nc);
     if (bad) {
       note("error: bgpu_panel_update_device: blocks outside the %d x %d matrix, both sides above 128, or a row offset "
@@ -1605,12 +1610,12 @@ int bgpu_panel_update_device(int n, float* d_a, int lda, int m, int nc, int ar, 
     }
     float* C = d_a + cr + (size_t)cc * lda;
     if (m <= nc)
-      ck(panel_tf32(true, true, maps, kMapMN, kMapK, ar, ac, br, bc, m, nc, C, lda, nullptr, 0, r.status.as<int>(),
-                    r.stream, nullptr),
+      ck(panel_tf32(true, true, maps, kMapMN, kMapK, nullptr, ar, ac, br, bc, m, nc, C, lda, cr, cc, nullptr, 0,
+                    r.status.as<int>(), r.stream, nullptr),
          "panel update");
     else
-      ck(panel_tf32(false, true, maps, kMapK, kMapMN, br, bc, ar, ac, nc, m, C, lda, nullptr, 0, r.status.as<int>(),
-                    r.stream, nullptr),
+      ck(panel_tf32(false, true, maps, kMapK, kMapMN, nullptr, br, bc, ar, ac, nc, m, C, lda, cr, cc, nullptr, 0,
+                    r.status.as<int>(), r.stream, nullptr),
          "panel update");
     r.check_status("panel update");
     return 0;

@@ -258,9 +258,14 @@ bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a
 // form writes the BF16 mirror too (mir: left column-major, right row-major; null: none).
 constexpr int kMapDL = 0, kMapDU = 1, kMapK = 2, kMapMN = 3;
 bool tc_panel_maps(const float* lu32, int n, long ld, const float* dl, const float* du, void* maps);
-cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, int rx0, int ry0, int px0, int py0,
-                       int h, int len, float* X, long ldx, void* mir, long ldm, int* d_status, cudaStream_t s,
-                       unsigned long long* stamp);
+// X sits at row xr0, column xc0 of the factor (multiples of 4; the mirror's position coordinate --
+// xr0 left, xc0 right -- of 8); whole 128 x 128 tiles are stored by TMA through mirror_maps (two
+// tensor maps from tc_mirror_store_maps: [0] the column-major mirror, [1] the row-major one), which
+// must be given when mir is.
+bool tc_mirror_store_maps(const void* Am, const void* Bm, int n, long ldm, void* maps);
+cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, const void* mirror_maps, int rx0,
+                       int ry0, int px0, int py0, int h, int len, float* X, long ldx, int xr0, int xc0, void* mir,
+                       long ldm, int* d_status, cudaStream_t s, unsigned long long* stamp);
 cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
                                   int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s,
                                   unsigned long long* stamp = nullptr);

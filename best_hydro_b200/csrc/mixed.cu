@@ -1061,6 +1061,7 @@ struct MixedSolver::Impl {
   bool mirrors = false;
   long ldm = 0;
   alignas(64) unsigned char map_am[kTensorMapBytes], map_bm[kTensorMapBytes];
+  alignas(64) unsigned char map_mst[2 * kTensorMapBytes];  // the leaves' TMA stores into the mirrors
   const void* mirror_key[2] = {};
   // the triangular-solve leaves on the tensor cores (TF32): tensor maps over the factor and the
   // diagonal-block inverses; the FP32 CUDA-core leaves when BEST_GPU_SIMT_LEAVES is set
@@ -1080,11 +1081,13 @@ struct MixedSolver::Impl {
       // one side at most 128: the TF32 panel product, the 128-wide operand resident
       prof.begin(m <= n ? "panel update (TF32, left)" : "panel update (TF32, right)", 2.0 * m * n * k, s);
       if (m <= n)
-        ck(panel_tf32(true, true, map_leaf, kMapMN, kMapK, ar, ac, br, bc, m, n, C, ld32, nullptr, 0, d_status(), s,
+        ck(panel_tf32(true, true, map_leaf, kMapMN, kMapK, nullptr, ar, ac, br, bc, m, n, C, ld32, cr, cc, nullptr, 0,
+                      d_status(), s,
                       next_stamp(2.0 * m * n * k, kSlotPanel)),
            "panel update launch");
       else
-        ck(panel_tf32(false, true, map_leaf, kMapK, kMapMN, br, bc, ar, ac, n, m, C, ld32, nullptr, 0, d_status(), s,
+        ck(panel_tf32(false, true, map_leaf, kMapK, kMapMN, nullptr, br, bc, ar, ac, n, m, C, ld32, cr, cc, nullptr, 0,
+                      d_status(), s,
                       next_stamp(2.0 * m * n * k, kSlotPanel)),
            "panel update launch");
       prof.end(s);
@@ -1145,7 +1148,8 @@ struct MixedSolver::Impl {
       __nv_bfloat16* mir = mirrors ? bm_at(kd, c0) : nullptr;
       prof.begin(w >= kWideLeaf ? "trsm leaf (left, wide)" : "trsm leaf (left)", 2.0 * h * h * w, s);
       if (tc_leaves)
-        ck(panel_tf32(true, false, map_leaf, kMapDL, kMapK, 0, kd, kd, c0, h, w, at_(kd, c0), ld32, mir, ldm,
+        ck(panel_tf32(true, false, map_leaf, kMapDL, kMapK, mir ? map_mst : nullptr, 0, kd, kd, c0, h, w, at_(kd, c0),
+                      ld32, kd, c0, mir, ldm,
                       d_status(), s, next_stamp(2.0 * h * h * w, kSlotSolveLeaf)),
            "trsm leaf launch");
       else if (w >= kWideLeaf)
@@ -1173,7 +1177,8 @@ struct MixedSolver::Impl {
       __nv_bfloat16* mir = mirrors ? am_at(r0, kd) : nullptr;
       prof.begin(m >= kWideLeaf ? "trsm leaf (right, wide)" : "trsm leaf (right)", 2.0 * h * h * m, s);
       if (tc_leaves)
-        ck(panel_tf32(false, false, map_leaf, kMapDU, kMapMN, 0, kd, r0, kd, h, m, at_(r0, kd), ld32, mir, ldm,
+        ck(panel_tf32(false, false, map_leaf, kMapDU, kMapMN, mir ? map_mst : nullptr, 0, kd, r0, kd, h, m, at_(r0, kd),
+                      ld32, r0, kd, mir, ldm,
                       d_status(), s, next_stamp(2.0 * h * h * m, kSlotSolveLeaf)),
            "trsm leaf launch");
       else if (m >= kWideLeaf)
@@ -1353,7 +1358,8 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     P.am.ensure(mirror_bytes, "BF16 mirror (L)");
     P.bm.ensure(mirror_bytes, "BF16 mirror (U)");
     if (P.ldm != ldm || P.mirror_key[0] != P.am.p || P.mirror_key[1] != P.bm.p) {
-      if (!tc_mirror_maps(P.am.p, P.bm.p, P.n3, ldm, P.map_am, P.map_bm))
+      if (!tc_mirror_maps(P.am.p, P.bm.p, P.n3, ldm, P.map_am, P.map_bm) ||
+          !tc_mirror_store_maps(P.am.p, P.bm.p, P.n3, ldm, P.map_mst))
         throw std::runtime_error("cannot build the tensor maps of the BF16 mirrors");
       P.ldm = ldm;
       P.mirror_key[0] = P.am.p;

@@ -298,9 +298,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 // four transposer warps rewrite each chunk K-major (128 rows of 128 bytes, 128-byte swizzle) before
 // the MMA warp uses it.  Shared memory: R (4 chunks of 16 KB), a raw ring (4 x 16 KB, TMA) and an
 // operand ring (4 x 16 KB); two TMEM accumulators of 128 x 128 FP32.
-constexpr int kPtStages = 4;
+constexpr int kPtStages = 2;
 constexpr uint32_t kPtChunk = 128 * 32 * 4;  // 16 KB
-constexpr uint32_t kPtSmem = 4 * kPtChunk + 2 * kPtStages * kPtChunk + 1024 + 256;
+// R (64 KB), raw and operand rings, the output tile (64 KB: four 32 x 128 FP32 boxes) and its BF16
+// mirror (32 KB: two 64 x 128 boxes), barriers
+constexpr uint32_t kPtOutOff = 4 * kPtChunk + 2 * kPtStages * kPtChunk;
+constexpr uint32_t kPtMirOff = kPtOutOff + 4 * kPtChunk;
+constexpr uint32_t kPtBarOff = kPtMirOff + 2 * kPtChunk;
+constexpr uint32_t kPtSmem = kPtBarOff + 256 + 1024;
 constexpr uint32_t kPtTmemCols = 256;
 constexpr int kPtTrWarps = 4;
 constexpr int kPtThreads = 64 + 32 * kEpiWarps + 32 * kPtTrWarps;
@@ -319,6 +324,17 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
+// TMA store of a box from shared memory (bulk-group completion), its commit and waits
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* tm, const void* src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"((uint64_t)tm),
+               "r"(x), "r"(y), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;\n" ::"r"(32 * kEpiWarps) : "memory"); }
 
 // One 16 KB chunk from four MN-major boxes (box c: MN rows 32 c .. 32 c + 31; K row k at 128 k bytes,
 // 16-byte group g of a row at (g ^ (k & 7)) -- the TMA's 128-byte swizzle) to the K-major layout
@@ -343,18 +359,25 @@ __device__ __forceinline__ void transpose_chunk(const uint8_t* src, uint8_t* dst
 // tmR, tmP: R's and P's tensor maps (K-major sources: 32 x 128 boxes, one per K chunk; MN-major
 // sources: 32 x 32 boxes).  R starts at (rx0, ry0) of its map, P at (px0, py0): left, R's box
 // (rx0 + 32 c, ry0 + 32 kc) and P's (px0 + 32 kc, py0 + 128 tile); right, R's (rx0 + 32 kc, ry0)
-// and P's (px0 + 128 tile + 32 c, py0 + 32 kc).  X: the result block (ldx), h its extent along R.
+// and P's (px0 + 128 tile + 32 c, py0 + 32 kc).  X: the result block (ldx) at row xr0, column xc0
+// of the matrix, h its extent along R.  Whole 128 x 128 tiles of X go out (and, subtracting, come
+// in) as TMA boxes of the factor's K-major map tmX (32 rows x 128 columns) through shared memory,
+// the mirror's as 64 x 128 boxes of tmM (left: column-major mirror at (row, column); right:
+// row-major at (column, row)); ragged tiles by plain loads and stores.
 template <bool LEFT, bool SUB>
 __global__ void __launch_bounds__(kPtThreads, 1)
-    k_panel_tf32(const __grid_constant__ CUtensorMap tmR, const __grid_constant__ CUtensorMap tmP, int rx0, int ry0,
-                 int px0, int py0, int h, int len, float* __restrict__ X, long ldx, __nv_bfloat16* __restrict__ mir,
-                 long ldm, int* status, unsigned long long* stamp) {
+    k_panel_tf32(const __grid_constant__ CUtensorMap tmR, const __grid_constant__ CUtensorMap tmP,
+                 const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmM, int rx0, int ry0,
+                 int px0, int py0, int h, int len, float* __restrict__ X, long ldx, int xr0, int xc0,
+                 __nv_bfloat16* __restrict__ mir, long ldm, int* status, unsigned long long* stamp) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sR = smem;                               // R, K-major: 4 chunks
-  uint8_t* sRaw = smem + 4 * kPtChunk;              // TMA ring of MN-major boxes (left: R's, once)
+  uint8_t* sRaw = smem + 4 * kPtChunk;              // TMA ring of P's MN-major boxes (right)
   uint8_t* sOp = sRaw + kPtStages * kPtChunk;       // P's K-major chunks
-  uint64_t* raw_full = reinterpret_cast<uint64_t*>(sOp + kPtStages * kPtChunk);
+  uint8_t* sOut = smem + kPtOutOff;                 // the output tile (left: R's boxes first)
+  uint8_t* sMir = smem + kPtMirOff;                 // its BF16 mirror
+  uint64_t* raw_full = reinterpret_cast<uint64_t*>(smem + kPtBarOff);
   uint64_t* raw_empty = raw_full + kPtStages;
   uint64_t* op_full = raw_empty + kPtStages;
   uint64_t* op_empty = op_full + kPtStages;
@@ -362,8 +385,10 @@ __global__ void __launch_bounds__(kPtThreads, 1)
   uint64_t* acc_empty = acc_full + 2;         // [2]
   uint64_t* r_raw = acc_empty + 2;            // left: R's boxes landed
   uint64_t* r_full = r_raw + 1;               // R ready (K-major)
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(r_full + 1);
-  __shared__ int s_abort;
+  uint64_t* c_full = r_full + 1;              // (subtracting) the C tile landed
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(c_full + 1);
+  int* s_flags = reinterpret_cast<int*>(tmem_slot + 1);  // [0] abort, [1] the epilogue goes on
+  volatile int& s_abort = s_flags[0];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles = (len + 127) / 128;
@@ -383,6 +408,7 @@ __global__ void __launch_bounds__(kPtThreads, 1)
     }
     mbar_init(r_raw, 1);
     mbar_init(r_full, LEFT ? kPtTrWarps : 1);
+    mbar_init(c_full, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 1) {
@@ -404,7 +430,7 @@ __global__ void __launch_bounds__(kPtThreads, 1)
         // R's MN-major boxes into the raw ring (free until the transposers have read them)
         mbar_expect_tx(r_raw, 4 * kPtChunk);
         for (int kc = 0; kc < 4; ++kc)
-          for (int c = 0; c < 4; ++c) tma_load_2d(sRaw + kc * kPtChunk + c * 4096, &tmR, rx0 + 32 * c, ry0 + 32 * kc, r_raw);
+          for (int c = 0; c < 4; ++c) tma_load_2d(sOut + kc * kPtChunk + c * 4096, &tmR, rx0 + 32 * c, ry0 + 32 * kc, r_raw);
       } else {
         mbar_expect_tx(r_full, 4 * kPtChunk);
         for (int kc = 0; kc < 4; ++kc) tma_load_2d(sR + kc * kPtChunk, &tmR, rx0 + 32 * kc, ry0, r_full);
@@ -469,7 +495,7 @@ __global__ void __launch_bounds__(kPtThreads, 1)
     const int t = threadIdx.x - 32 * tr_first;
     if (LEFT) {
       if (mbar_wait(r_raw, 0, status) && !*(volatile int*)&s_abort) {
-        for (int kc = 0; kc < 4; ++kc) transpose_chunk(sRaw + kc * kPtChunk, sR + kc * kPtChunk, t);
+        for (int kc = 0; kc < 4; ++kc) transpose_chunk(sOut + kc * kPtChunk, sR + kc * kPtChunk, t);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncwarp();
         if (lane == 0) mbar_arrive(r_full);
@@ -501,55 +527,121 @@ __global__ void __launch_bounds__(kPtThreads, 1)
       }
     }
   } else {
-    // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (the tile's rows), columns [64 half, 64 half + 64)
+    // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (the tile's rows), columns [64 half, 64 half + 64);
+    // thread et == 0 leads: the TMA traffic of whole tiles and the waits whose outcome all share
     const int q = warp & 3, half = (warp - 2) >> 2;
+    const int et = threadIdx.x - 64;
     const int r = q * 32 + lane;  // accumulator row
-    uint32_t local = 0;
+    uint32_t local = 0, cuse = 0;
+    bool stored = false;  // (leader) a TMA store from sOut / sMir in flight
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
       const uint32_t b = local & 1, use = local >> 1;
+      const bool whole = h == 128 && 128 * (tile + 1) <= len;
+      const int trow = xr0 + (LEFT ? 0 : 128 * tile), tcol = xc0 + (LEFT ? 128 * tile : 0);  // the tile in X's matrix
+      if (et == 0) {
+        bool ok = true;
+        if (whole) {
+          if (stored) bulk_wait_read();                               // the last stores have read sOut, sMir
+          if (LEFT && local == 0) ok = mbar_wait(r_full, 0, status);  // sOut held R's boxes until then
+          if (SUB && ok) {
+            mbar_expect_tx(c_full, 4 * kPtChunk);
+            for (int c = 0; c < 4; ++c) tma_load_2d(sOut + c * kPtChunk, &tmX, trow + 32 * c, tcol, c_full);
+          }
+        }
+        ok = ok && mbar_wait(&acc_full[b], use & 1, status);
+        if (ok && SUB && whole) ok = mbar_wait(c_full, cuse & 1, status);
+        s_flags[1] = ok && !s_abort;
+      }
+      epi_bar();
+      if (!s_flags[1]) {
+        if (et == 0) s_abort = 1;
+        break;
+      }
+      if (SUB && whole) mbar_wait(c_full, (cuse++) & 1, status);  // (complete: the leader saw it)
+      tc_fence_after();
+      if (whole) {
+        // sOut box c: rows 32 c .. 32 c + 31; column j at 128 j bytes, 16-byte group (row & 31) / 4
+        // swizzled with j & 7 (the TMA's 128-byte swizzle)
+        uint8_t* ob = sOut + q * kPtChunk + (lane & 3) * 4;
+#pragma unroll 1
+        for (int c = 0; c < 2; ++c) {
+          float v[32];
+          const int j0 = 64 * half + 32 * c;
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * 128 + (uint32_t)j0, v);
+#pragma unroll
+          for (int jj = 0; jj < 32; ++jj) {
+            const int j = j0 + jj;
+            float* o = reinterpret_cast<float*>(ob + j * 128 + (((lane >> 2) ^ (j & 7)) << 4));
+            const float x = SUB ? *o - v[jj] : v[jj];
+            *o = x;
+            v[jj] = x;
+            if (!SUB && LEFT && mir) {
+              // column-major mirror box r / 64: column j at 128 j bytes, group (r & 63) / 8 ^ (j & 7)
+              *reinterpret_cast<__nv_bfloat16*>(sMir + (r >> 6) * kPtChunk + j * 128 +
+                                               ((((r & 63) >> 3) ^ (j & 7)) << 4) + (r & 7) * 2) = __float2bfloat16_rn(x);
+            }
+          }
+          if (!SUB && !LEFT && mir) {
+            // row-major mirror box j0 / 64: row r at 128 r bytes, group (j & 63) / 8 ^ (r & 7)
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+              uint4 pk;
+              uint32_t* w = reinterpret_cast<uint32_t*>(&pk);
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const __nv_bfloat162 two = __floats2bfloat162_rn(v[8 * g + 2 * e], v[8 * g + 2 * e + 1]);
+                w[e] = *reinterpret_cast<const uint32_t*>(&two);
+              }
+              *reinterpret_cast<uint4*>(sMir + (j0 >> 6) * kPtChunk + r * 128 +
+                                        (((((j0 & 63) >> 3) + g) ^ (r & 7)) << 4)) = pk;
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[b]);
+        fence_async_smem();
+        epi_bar();
+        if (et == 0) {
+          for (int c = 0; c < 4; ++c) tma_store_2d(&tmX, sOut + c * kPtChunk, trow + 32 * c, tcol);
+          if (!SUB && mir) {
+            for (int c = 0; c < 2; ++c) {
+              if (LEFT)
+                tma_store_2d(&tmM, sMir + c * kPtChunk, trow + 64 * c, tcol);  // (row, column)
+              else
+                tma_store_2d(&tmM, sMir + c * kPtChunk, tcol + 64 * c, trow);  // (column, row)
+            }
+          }
+          bulk_commit();
+          stored = true;
+        }
+        continue;
+      }
       // left: X row r (valid below h), columns 128 tile + j; right: X row 128 tile + r (valid below len),
       // columns j (valid below h); j = 64 half + 0 .. 63
       const int xrow = LEFT ? r : 128 * tile + r;
       const bool rok = LEFT ? r < h : xrow < len;
       const int jlim = LEFT ? len - 128 * tile : h;  // columns j below jlim are valid
       float* xp = X + (LEFT ? (size_t)(128 * tile) * ldx : (size_t)0) + xrow;
-      // (sub) C's first 32 columns loaded before the accumulator is ready, the next 32 while the first
-      // are stored
-      float cv[SUB ? 32 : 1], nv[SUB ? 32 : 1];
-      if constexpr (SUB) {
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = 64 * half + j;
-          cv[j] = (rok && col < jlim) ? __ldcs(xp + (size_t)col * ldx) : 0.f;
-        }
-      }
-      if (!mbar_wait(&acc_full[b], use & 1, status) || *(volatile int*)&s_abort) break;
-      tc_fence_after();
 #pragma unroll 1
       for (int c = 0; c < 2; ++c) {
         float v[32];
         const int j0 = 64 * half + 32 * c;
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * 128 + (uint32_t)j0, v);
         if constexpr (SUB) {
-          if (c == 0) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const int col = j0 + 32 + j;
-              nv[j] = (rok && col < jlim) ? __ldcs(xp + (size_t)col * ldx) : 0.f;
-            }
-          }
+          // (a ragged tile: C by plain loads, 32 columns at a time)
           if (rok) {
+            float cv[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) cv[j] = j0 + j < jlim ? __ldcs(xp + (size_t)(j0 + j) * ldx) : 0.f;
 #pragma unroll
             for (int j = 0; j < 32; ++j)
               if (j0 + j < jlim) __stcs(xp + (size_t)(j0 + j) * ldx, cv[j] - v[j]);
           }
-#pragma unroll
-          for (int j = 0; j < 32; ++j) cv[j] = nv[j];
           continue;
         }
         if (!rok) continue;
-        if constexpr (SUB) {
-        } else {
+        {
 #pragma unroll
           for (int j = 0; j < 32; ++j)
             if (j0 + j < jlim) xp[(size_t)(j0 + j) * ldx] = v[j];
@@ -588,6 +680,7 @@ __global__ void __launch_bounds__(kPtThreads, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[b]);
     }
+    if (et == 0 && stored) bulk_wait_all();
   }
   tc_fence_before();
   __syncthreads();
@@ -752,29 +845,30 @@ bool tc_panel_maps(const float* lu32, int n, long ld, const float* dl, const flo
          make_map_f32(&m[kMapMN], lu32, n, n, ld, 32);               // MN-major boxes
 }
 
-cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, int rx0, int ry0, int px0, int py0,
-                       int h, int len, float* X, long ldx, void* mir, long ldm, int* d_status, cudaStream_t s,
-                       unsigned long long* stamp) {
+bool tc_mirror_store_maps(const void* Am, const void* Bm, int n, long ldm, void* maps) {
+  if ((ldm % 8) || ((uintptr_t)Am & 15) || ((uintptr_t)Bm & 15) || n <= 0) return false;
+  CUtensorMap* m = static_cast<CUtensorMap*>(maps);
+  return make_map(&m[0], Bm, n, n, ldm, 128) &&  // left leaves: column-major mirror, boxes 64 rows x 128
+         make_map(&m[1], Am, n, n, ldm, 128);    // right leaves: row-major mirror, boxes 64 columns x 128
+}
+
+cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, const void* mirror_maps, int rx0,
+                       int ry0, int px0, int py0, int h, int len, float* X, long ldx, int xr0, int xc0, void* mir,
+                       long ldm, int* d_status, cudaStream_t s, unsigned long long* stamp) {
   if (len <= 0 || h <= 0) return cudaSuccess;
-  // TMA: the innermost coordinate of every box a multiple of 4 FP32 elements (16 bytes)
-  if (h > 128 || (rx0 % 4) || (px0 % 4) || map_r < 0 || map_r > 3 || map_p < 0 || map_p > 3)
+  // TMA: the innermost coordinate of every box a multiple of 16 bytes (4 FP32, 8 BF16 elements)
+  if (h > 128 || (rx0 % 4) || (px0 % 4) || (xr0 % 4) || map_r < 0 || map_r > 3 || map_p < 0 || map_p > 3 ||
+      xr0 < 0 || xc0 < 0)
     return cudaErrorInvalidValue;
+  if (mir && (!mirror_maps || (left ? xr0 % 8 : xc0 % 8))) return cudaErrorInvalidValue;
   const CUtensorMap* m = static_cast<const CUtensorMap*>(maps);
+  const CUtensorMap* mm = mir ? static_cast<const CUtensorMap*>(mirror_maps) + (left ? 0 : 1) : &m[kMapK];
   const dim3 grid(persistent_grid((len + 127) / 128)), block(kPtThreads);
   __nv_bfloat16* mb = static_cast<__nv_bfloat16*>(mir);
-  cudaError_t e;
-  if (left && !sub)
-    e = launch_dependent(k_panel_tf32<true, false>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0,
-                         h, len, X, ldx, mb, ldm, d_status, stamp);
-  else if (!left && !sub)
-    e = launch_dependent(k_panel_tf32<false, false>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0,
-                         h, len, X, ldx, mb, ldm, d_status, stamp);
-  else if (left)
-    e = launch_dependent(k_panel_tf32<true, true>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0, h,
-                         len, X, ldx, mb, ldm, d_status, stamp);
-  else
-    e = launch_dependent(k_panel_tf32<false, true>, grid, block, kPtSmem, s, m[map_r], m[map_p], rx0, ry0, px0, py0,
-                         h, len, X, ldx, mb, ldm, d_status, stamp);
+  auto kern = left ? (sub ? k_panel_tf32<true, true> : k_panel_tf32<true, false>)
+                   : (sub ? k_panel_tf32<false, true> : k_panel_tf32<false, false>);
+  const cudaError_t e = launch_dependent(kern, grid, block, kPtSmem, s, m[map_r], m[map_p], m[kMapK], *mm, rx0, ry0, px0,
+                                         py0, h, len, X, ldx, xr0, xc0, mb, ldm, d_status, stamp);
   BGPU_COUNT_LAUNCH();
   return e;
 }

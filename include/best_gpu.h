@@ -119,15 +119,15 @@ int bgpu_lu32_leaf_device(int h, float *d_a, int lda, float *d_linv, float *d_ui
  * [p0, p0 + len) := L_kd^-1 times that block (d_linv's block kd / 128); left == 0: rows [p0, p0 + len) x
  * columns [kd, kd + h) := that block times U_kd^-1 (d_uinv's).  In place; with d_mirror (BF16,
  * n x n, ldm) the result's BF16 copy goes to the same positions of d_mirror, column-major for the
- * left leaf and row-major (element (i, j) at i * ldm + j) for the right one.  kd and p0 multiples of
- * 32, h <= 128. */
+ * left leaf and row-major (element (i, j) at i * ldm + j) for the right one (ldm a multiple of 8).
+ * kd and p0 multiples of 32, h <= 128. */
 int bgpu_trsm_leaf_device(int left, int n, float *d_a, int lda, const float *d_linv, const float *d_uinv, int kd,
                           int p0, int h, int len, void *d_mirror, int ldm);
 
 /* The mixed-precision LU's K = 128 update on the tensor cores (TF32 operands, FP32 accumulation;
  * device memory): in the n x n FP32 matrix d_a (column-major, lda a multiple of 4), the m x nc block
  * at (cr, cc) -= the m x 128 block at (ar, ac) times the 128 x nc block at (br, bc), with m or nc at
- * most 128 and ar, br multiples of 4.  The blocks may lie anywhere in the matrix but the result
+ * most 128 and ar, br, cr multiples of 4.  The blocks may lie anywhere in the matrix but the result
  * block must not overlap the other two. */
 int bgpu_panel_update_device(int n, float *d_a, int lda, int m, int nc, int ar, int ac, int br, int bc, int cr,
                              int cc);
