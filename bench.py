@@ -384,22 +384,18 @@ GEMM_TRAFFIC_RATIO = {
 }
 
 
-def small_update(m, n, k):
-    """The products the LU runs on the CUDA cores instead of the tcgen05 kernel (mixed.cu)."""
-    return k <= 256 and m * n * k <= (1 << 26)
-
-
 def panel_update(m, n, k):
     """The products the LU runs on the TF32 panel kernel (k_panel_tf32, mixed.cu): K = 128 with one
-    side at most 128."""
-    return k == 128 and min(m, n) <= 128
+    side at most 128, or at most 256 with the other at most 3,840; every other product runs on the
+    BF16 tcgen05 GEMM."""
+    return k == 128 and (min(m, n) <= 128 or (min(m, n) <= 256 and max(m, n) <= 3840))
 
 
 def gemm_traffic_per_launch(n3):
     """(estimated DRAM bytes, algorithmic bytes, launches) per tcgen05 GEMM launch of one
     factorisation at order n3: each launch's algorithmic bytes times the measured ratio of its shape
     class."""
-    shapes = [sh for sh in lu_gemm_shapes(n3) if not small_update(*sh) and not panel_update(*sh)]
+    shapes = [sh for sh in lu_gemm_shapes(n3) if not panel_update(*sh)]
     alg = traffic = 0.0
     for m, n, k in shapes:
         a = gemm_algorithmic_bytes(m, n, k)

@@ -1594,10 +1594,10 @@ int bgpu_panel_update_device(int n, float* d_a, int lda, int m, int nc, int ar, 
   return status_of([&] {
     Runtime& r = rt();
     auto in = [&](int r0, int c0, int rows, int cols) { return r0 >= 0 && c0 >= 0 && r0 + rows <= n && c0 + cols <= n; };
-    const bool bad = n < 1 || lda < n || m < 1 || nc < 1 || std::min(m, nc) > 128 || ar % 4 || br % 4 || cr % 4 ||
+    const bool bad = n < 1 || lda < n || m < 1 || nc < 1 || std::min(m, nc) > 256 || ar % 4 || br % 4 || cr % 4 ||
                      !in(ar, ac, m, 128) || !in(br, bc, 128, nc) || !in(cr, cc, m, nc);
     if (bad) {
-      note("error: bgpu_panel_update_device: blocks outside the %d x %d matrix, both sides above 128, or a row offset "
+      note("error: bgpu_panel_update_device: blocks outside the %d x %d matrix, both sides above 256, or a row offset "
            "not a multiple of 4", n, n);
       return 1;
     }

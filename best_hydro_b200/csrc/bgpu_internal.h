@@ -250,6 +250,7 @@ bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a
 // Panel products of the FP32 LU on the tensor cores (TF32 operands, FP32 accumulation), a 128 x 128
 // operand R against a panel P of len rows or columns (tc_gemm.cu, k_panel_tf32):
 //   left:  X (h x len) := R P, or -= R P (sub);   right: X (len x h) := P R, or -= P R (sub)
+// (h <= 128; subtracting, h <= 256: two row groups of R, grid.y)
 // maps: four tensor maps (4 kTensorMapBytes, built by tc_panel_maps) over the diagonal-block inverses
 // dl, du (128 x 128 column-major each, one per 128 rows) and the factor (n x n, ld); map_r, map_p pick
 // R's and P's.  The left form reads R through an MN-major map (kMapDL, kMapMN) and P through a K-major

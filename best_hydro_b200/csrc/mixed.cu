@@ -686,6 +686,10 @@ void launch_narrow_leaf(const float* dinv, int h, float* B, long ldb, int len, _
 // from the factor (more accurate than the BF16 mirrors the tensor cores read).
 constexpr int kSgBk = 32;
 inline bool small_update(int m, int n, int k) { return k <= 256 && (long long)m * n * k <= (1LL << 26); }
+// the K = 128 products of the TF32 panel kernel
+inline bool panel_update(int m, int n, int k) {
+  return k == 128 && (std::min(m, n) <= 128 || (std::min(m, n) <= 256 && std::max(m, n) <= 3840));
+}
 __global__ void __launch_bounds__(256) k_sgemm_small_minus(int m, int n, int k, const float* __restrict__ A, long lda,
                                                           const float* __restrict__ B, long ldb, float* __restrict__ C,
                                                           long ldc, unsigned long long* stamp) {
@@ -1077,8 +1081,9 @@ struct MixedSolver::Impl {
   void gemm(int m, int n, int k, int ar, int ac, int br, int bc, int cr, int cc, cudaStream_t s) {
     if (m <= 0 || n <= 0 || k <= 0) return;
     float* C = at_(cr, cc);
-    if (tc_leaves && k == 128 && std::min(m, n) <= 128) {
-      // one side at most 128: the TF32 panel product, the 128-wide operand resident
+    if (tc_leaves && panel_update(m, n, k)) {
+      // one side at most 128 (at most 256 with the other at most 3,840: wider, the BF16 GEMM is
+      // faster than two row groups): the TF32 panel product, the narrow operand resident
       prof.begin(m <= n ? "panel update (TF32, left)" : "panel update (TF32, right)", 2.0 * m * n * k, s);
       if (m <= n)
         ck(panel_tf32(true, true, map_leaf, kMapMN, kMapK, nullptr, ar, ac, br, bc, m, n, C, ld32, cr, cc, nullptr, 0,
@@ -1093,7 +1098,7 @@ struct MixedSolver::Impl {
       prof.end(s);
       return;
     }
-    if (small_update(m, n, k)) {
+    if (!tc_leaves && small_update(m, n, k)) {
       prof.begin("small update (FP32 cores)", 2.0 * m * n * k, s);
       ck(launch_dependent(k_sgemm_small_minus, dim3((m + 63) / 64, (n + 63) / 64), dim3(256), 0, s, m, n, k,
                           (const float*)at_(ar, ac), (long)ld32, (const float*)at_(br, bc), (long)ld32, C, (long)ld32,

@@ -370,6 +370,19 @@ __global__ void __launch_bounds__(kPtThreads, 1)
                  const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmM, int rx0, int ry0,
                  int px0, int py0, int h, int len, float* __restrict__ X, long ldx, int xr0, int xc0,
                  __nv_bfloat16* __restrict__ mir, long ldm, int* status, unsigned long long* stamp) {
+  // row group blockIdx.y of a 256-wide R: its 128 rows (left) or columns (right), and X's with them
+  if (blockIdx.y) {
+    const int o = 128 * blockIdx.y;
+    h -= o;
+    if (LEFT) {
+      rx0 += o, xr0 += o, X += o;
+      if (mir) mir += o;
+    } else {
+      ry0 += o, xc0 += o, X += (size_t)o * ldx;
+      if (mir) mir += o;
+    }
+  }
+  h = min(h, 128);
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sR = smem;                               // R, K-major: 4 chunks
@@ -857,13 +870,13 @@ cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map
                        long ldm, int* d_status, cudaStream_t s, unsigned long long* stamp) {
   if (len <= 0 || h <= 0) return cudaSuccess;
   // TMA: the innermost coordinate of every box a multiple of 16 bytes (4 FP32, 8 BF16 elements)
-  if (h > 128 || (rx0 % 4) || (px0 % 4) || (xr0 % 4) || map_r < 0 || map_r > 3 || map_p < 0 || map_p > 3 ||
-      xr0 < 0 || xc0 < 0)
+  if (h > 256 || (rx0 % 4) || (px0 % 4) || (xr0 % 4) || map_r < 0 || map_p < 0 || map_r > 3 || map_p > 3 ||
+      xr0 < 0 || xc0 < 0 || (h > 128 && !sub))
     return cudaErrorInvalidValue;
   if (mir && (!mirror_maps || (left ? xr0 % 8 : xc0 % 8))) return cudaErrorInvalidValue;
   const CUtensorMap* m = static_cast<const CUtensorMap*>(maps);
   const CUtensorMap* mm = mir ? static_cast<const CUtensorMap*>(mirror_maps) + (left ? 0 : 1) : &m[kMapK];
-  const dim3 grid(persistent_grid((len + 127) / 128)), block(kPtThreads);
+  const dim3 grid(persistent_grid((len + 127) / 128), (h + 127) / 128), block(kPtThreads);
   __nv_bfloat16* mb = static_cast<__nv_bfloat16*>(mir);
   auto kern = left ? (sub ? k_panel_tf32<true, true> : k_panel_tf32<true, false>)
                    : (sub ? k_panel_tf32<false, true> : k_panel_tf32<false, false>);

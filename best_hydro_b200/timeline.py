@@ -24,17 +24,13 @@ def _split(sz):
 
 
 def _update_kind(m, n, k):
-    if k == 128 and min(m, n) <= 128:
-        return "panel"
-    if k <= 256 and m * n * k <= (1 << 26):
-        return "small"
-    return "gemm"
+    return "panel" if k == 128 and (min(m, n) <= 128 or (min(m, n) <= 256 and max(m, n) <= 3840)) else "gemm"
 
 
 def launch_labels(n3):
     """(kind, m, n, k) of every stamped launch of the factorisation at order n3, in launch order:
-    kind "lu" (diagonal leaf), "leafL" / "leafR" (triangular-solve leaves: h x w, m x h), "panel",
-    "small", "gemm"."""
+    kind "lu" (diagonal leaf), "leafL" / "leafR" (triangular-solve leaves: h x w, m x h), "panel"
+    (TF32 panel update), "gemm" (BF16 tensor-core GEMM)."""
     out = []
 
     def gemm(m, n, k):

@@ -1,6 +1,6 @@
 """CPU checks of bench.py's accounting: the replay of the mixed LU's GEMM shapes gives the launch
-count the library stamps (3,713 at order 61,440: 1,377 BF16 tensor-core GEMMs, 1,920 TF32 panel
-updates, 416 small FP32 updates) and the LU's flop count, and the traffic estimate stays within the
+count the library stamps (3,713 at order 61,440: 1,569 BF16 tensor-core GEMMs and 2,144 TF32 panel
+updates) and the LU's flop count, and the traffic estimate stays within the
 measured per-class ratios."""
 import bench
 
@@ -20,6 +20,5 @@ def test_gemm_traffic_estimate_in_range():
     lo, hi = min(bench.GEMM_TRAFFIC_RATIO.values()), max(bench.GEMM_TRAFFIC_RATIO.values())
     shapes = bench.lu_gemm_shapes(61440)
     panel = sum(1 for sh in shapes if bench.panel_update(*sh))
-    small = sum(1 for sh in shapes if bench.small_update(*sh) and not bench.panel_update(*sh))
-    assert (panel, small) == (1920, 416)
-    assert count == 3713 - small - panel == 1377 and lo * alg <= tr <= hi * alg
+    assert panel == 2144
+    assert count == 3713 - panel == 1569 and lo * alg <= tr <= hi * alg

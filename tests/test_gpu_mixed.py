@@ -123,11 +123,12 @@ def test_trsm_leaf_tc(left, kd, p0, length):
     assert np.all(mir_out == 3.0)
 
 
-@pytest.mark.parametrize("m,nc", [(128, 300), (300, 100), (50, 384), (128, 128), (384, 7)])
+@pytest.mark.parametrize("m,nc", [(128, 300), (300, 100), (50, 384), (128, 128), (384, 7), (256, 384), (384, 200)])
 def test_panel_update_tc(m, nc):
     """The LU's K = 128 update on the tensor cores (TF32 operands, FP32 accumulation): C -= A B with
-    one side at most 128 (the left form for m <= nc, the right one otherwise), against FP64 within
-    2^-8 of |A| |B|; everything outside C untouched; ragged sizes."""
+    one side at most 256 (the left form for m <= nc, the right one otherwise), against FP64 within
+    2^-8 of |A| |B|; everything outside C untouched; ragged sizes; a short side of 129-256 in two
+    row groups."""
     torch = _torch()
     n, lda = 640, 644
     ar, ac, br, bc, cr, cc = 0, 0, 128, 128, 256, 256
