@@ -1560,7 +1560,7 @@ int bgpu_trsm_leaf_device(int left, int n, float* d_a, int lda, const float* d_l
       return 1;
     }
     ck(tc_gemm_prepare(), "tensor-core attributes");
-    alignas(64) unsigned char maps[4 * kTensorMapBytes];
+    alignas(64) unsigned char maps[kPanelMaps * kTensorMapBytes];
     if (!tc_panel_maps(d_a, n, lda, d_linv, d_uinv, maps)) {
       note("error: bgpu_trsm_leaf_device: cannot build the tensor maps (lda a multiple of 4, 16-byte aligned buffers)");
       return 1;
@@ -1602,7 +1602,7 @@ int bgpu_panel_update_device(int n, float* d_a, int lda, int m, int nc, int ar, 
       return 1;
     }
     ck(tc_gemm_prepare(), "tensor-core attributes");
-    alignas(64) unsigned char maps[4 * kTensorMapBytes];
+    alignas(64) unsigned char maps[kPanelMaps * kTensorMapBytes];
     // the diagonal-block maps are not used: any aligned buffer stands in for them
     if (!tc_panel_maps(d_a, n, lda, d_a, d_a, maps)) {
       note("error: bgpu_panel_update_device: cannot build the tensor maps (lda a multiple of 4, 16-byte aligned)");

@@ -251,13 +251,13 @@ bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a
 // operand R against a panel P of len rows or columns (tc_gemm.cu, k_panel_tf32):
 //   left:  X (h x len) := R P, or -= R P (sub);   right: X (len x h) := P R, or -= P R (sub)
 // (h <= 128; subtracting, h <= 256: two row groups of R, grid.y)
-// maps: four tensor maps (4 kTensorMapBytes, built by tc_panel_maps) over the diagonal-block inverses
-// dl, du (128 x 128 column-major each, one per 128 rows) and the factor (n x n, ld); map_r, map_p pick
-// R's and P's.  The left form reads R through an MN-major map (kMapDL, kMapMN) and P through a K-major
+// maps: kPanelMaps tensor maps (kPanelMaps kTensorMapBytes, built by tc_panel_maps) over the
+// diagonal-block inverses dl, du (128 x 128 column-major each, one per 128 rows) and the factor
+// (n x n, ld; kMapC: the BF16 GEMM's C tiles); map_r, map_p pick R's and P's.  The left form reads R through an MN-major map (kMapDL, kMapMN) and P through a K-major
 // one (kMapK); the right form R K-major (kMapDU, kMapK) and P MN-major (kMapMN).  R's block starts at
 // map coordinates (rx0, ry0) (inner, outer), P's at (px0, py0); rx0, px0 multiples of 4.  The assigning
 // form writes the BF16 mirror too (mir: left column-major, right row-major; null: none).
-constexpr int kMapDL = 0, kMapDU = 1, kMapK = 2, kMapMN = 3;
+constexpr int kMapDL = 0, kMapDU = 1, kMapK = 2, kMapMN = 3, kMapC = 4, kPanelMaps = 5;
 bool tc_panel_maps(const float* lu32, int n, long ld, const float* dl, const float* du, void* maps);
 // X sits at row xr0, column xc0 of the factor (multiples of 4; the mirror's position coordinate --
 // xr0 left, xc0 right -- of 8); whole 128 x 128 tiles are stored by TMA through mirror_maps (two
@@ -267,8 +267,12 @@ bool tc_mirror_store_maps(const void* Am, const void* Bm, int n, long ldm, void*
 cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, const void* mirror_maps, int rx0,
                        int ry0, int px0, int py0, int h, int len, float* X, long ldx, int xr0, int xc0, void* mir,
                        long ldm, int* d_status, cudaStream_t s, unsigned long long* stamp);
+// map_c (optional): a tensor map over C's FP32 matrix (tc_panel_maps' kMapC) with C at (c_row, c_col)
+// of it (c_row a multiple of 4): products of at most 8 K tiles then load and store whole C tiles by
+// TMA through shared memory.
 cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
                                   int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s,
-                                  unsigned long long* stamp = nullptr);
+                                  unsigned long long* stamp = nullptr, const void* map_c = nullptr, int c_row = 0,
+                                  int c_col = 0);
 
 }  // namespace bgpu

@@ -1070,7 +1070,7 @@ struct MixedSolver::Impl {
   // the triangular-solve leaves on the tensor cores (TF32): tensor maps over the factor and the
   // diagonal-block inverses; the FP32 CUDA-core leaves when BEST_GPU_SIMT_LEAVES is set
   bool tc_leaves = true;
-  alignas(64) unsigned char map_leaf[4 * kTensorMapBytes];
+  alignas(64) unsigned char map_leaf[kPanelMaps * kTensorMapBytes];
   const void* leaf_key[4] = {};
   int* d_status() { return status.as<int>(); }
   __nv_bfloat16* am_at(int r, int c) const { return am.as<__nv_bfloat16>() + (size_t)r * ldm + c; }
@@ -1112,7 +1112,8 @@ struct MixedSolver::Impl {
     if (mirrors) {
       prof.begin(size_class(m, n, k), 2.0 * m * n * k, s);
       ck(gemm_bf16_tc_minus_at(m, n, k, map_am, ar, ac, map_bm, bc, br, C, ld32, d_status(), s,
-                               next_stamp(2.0 * m * n * k)),
+                               next_stamp(2.0 * m * n * k), tc_leaves ? map_leaf + kMapC * kTensorMapBytes : nullptr,
+                               cr, cc),
          "tensor-core GEMM");
       prof.end(s);
       return;

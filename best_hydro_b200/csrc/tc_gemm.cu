@@ -37,6 +37,11 @@ constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kStageA = BM * BK * 2;  // 16 KB
 constexpr uint32_t kStageB = BN * BK * 2;  // 32 KB
 constexpr uint32_t kSmem = STAGES * (kStageA + kStageB) + 1024 + 256;
+// the small-K variant (at most 8 K tiles): two stages and the C tile staged in shared memory (128 x 256
+// FP32, four 32 x 256 boxes of 32 KB) for TMA loads and stores
+constexpr int kStagesSmallK = 2, kSmallKTiles = 8;
+constexpr uint32_t kCBox = 32 * BN * 4;
+constexpr uint32_t kSmemStaged = kStagesSmallK * (kStageA + kStageB) + 4 * kCBox + 1024 + 256;
 constexpr uint32_t kTmemCols = 512;        // two accumulators of BN columns
 constexpr int kGroupM = 16;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // a wait gives up after 2 s
@@ -86,6 +91,20 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, in
       "l"((uint64_t)tm), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+// TMA store of a box from shared memory (bulk-group completion), its commit and waits
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* tm, const void* src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"((uint64_t)tm),
+               "r"(x), "r"(y), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;\n" ::"r"(32 * kEpiWarps) : "memory"); }
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle; rows of 128 B, 8-row groups 1024 B
 // apart (stride byte offset), version 1 (bits 46-47), layout 2 = SWIZZLE_128B (bits 61-63).
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
@@ -136,20 +155,29 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 // (both 0 for operand buffers that hold just this product).  stamp (optional): the launch's first
 // CTA start and last CTA end on the global nanosecond timer, as atomic min into stamp[0] and max into
 // stamp[1] (live per-launch timing that also works inside a CUDA graph).
+// NST pipeline stages; STAGED: whole C tiles loaded and stored by TMA through shared memory (tmC the
+// C matrix's FP32 map, 32 x 256 boxes; C's element (0, 0) at (c_r0, c_c0) of it), ragged ones by
+// plain loads and stores.
+template <int NST, bool STAGED>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int m, int n,
-                   int k, float* __restrict__ C, long ldc, int tiles_m, int tiles_n, int* status, int a_y0, int a_x0,
-                   int b_y0, int b_x0, unsigned long long* stamp) {
+    k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const __grid_constant__ CUtensorMap tmC, int m, int n, int k, float* __restrict__ C, long ldc,
+                   int c_r0, int c_c0, int tiles_m, int tiles_n, int* status, int a_y0, int a_x0, int b_y0, int b_x0,
+                   unsigned long long* stamp) {
+  constexpr int STAGES = NST;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;
   uint8_t* sB = smem + STAGES * kStageA;
-  uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * kStageB);
+  uint8_t* sC = sB + STAGES * kStageB;  // (staged) the C tile: four 32 x 256 boxes
+  uint64_t* full = reinterpret_cast<uint64_t*>(sC + (STAGED ? 4 * kCBox : 0));
   uint64_t* empty = full + STAGES;
   uint64_t* acc_full = empty + STAGES;   // [2]
   uint64_t* acc_empty = acc_full + 2;    // [2]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
-  __shared__ int s_abort;
+  uint64_t* c_full = acc_empty + 2;      // (staged) the C tile landed
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(c_full + 1);
+  int* s_flags = reinterpret_cast<int*>(tmem_slot + 1);  // [0] abort, [1] the epilogue goes on
+  volatile int& s_abort = s_flags[0];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles = tiles_m * tiles_n;
@@ -165,6 +193,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&acc_full[b], 1);
       mbar_init(&acc_empty[b], kEpiWarps);
     }
+    mbar_init(c_full, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 1) {
@@ -232,45 +261,128 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   } else {
-    // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (tile rows), columns [half * 128, half * 128 + 128)
-    const int q = warp & 3, half = (warp - 2) >> 2;
-    uint32_t local = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
-      const uint32_t b = local & 1, use = local >> 1;
-      int tm, tn;
-      tile_coords(tile, tiles_m, tiles_n, tm, tn);
-      const int row = tm * BM + q * 32 + lane;
-      const int cbase = tn * BN + half * (BN / 2);
-      const bool rok = row < m;
-      float* crow = C + row;
-      // C of the first 32 columns, loaded before the accumulator is ready
-      float cv[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) cv[j] = (rok && cbase + j < n) ? __ldcs(crow + (size_t)(cbase + j) * ldc) : 0.f;
-      if (!mbar_wait(&acc_full[b], use & 1, status) || *(volatile int*)&s_abort) break;
-      tc_fence_after();
+    if constexpr (STAGED) {
+      // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (tile rows), columns [half * 128, half * 128 + 128);
+      // thread et == 0 leads: the TMA traffic of whole tiles and the waits whose outcome all share
+      const int q = warp & 3, half = (warp - 2) >> 2, et = threadIdx.x - 64;
+      uint32_t local = 0, cuse = 0;
+      bool stored = false;  // (leader) a TMA store from sC in flight
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
+        const uint32_t b = local & 1, use = local >> 1;
+        int tm, tn;
+        tile_coords(tile, tiles_m, tiles_n, tm, tn);
+        const bool whole = (tm + 1) * BM <= m && (tn + 1) * BN <= n;
+        const int crow0 = c_r0 + tm * BM, ccol0 = c_c0 + tn * BN;
+        if (et == 0) {
+          bool ok = true;
+          if (whole) {
+            if (stored) bulk_wait_read();  // the last tile's stores have read sC
+            mbar_expect_tx(c_full, 4 * kCBox);
+            for (int c = 0; c < 4; ++c) tma_load_2d(sC + c * kCBox, &tmC, crow0 + 32 * c, ccol0, c_full);
+          }
+          ok = mbar_wait(&acc_full[b], use & 1, status);
+          if (ok && whole) ok = mbar_wait(c_full, cuse & 1, status);
+          s_flags[1] = ok && !s_abort;
+        }
+        epi_bar();
+        if (!s_flags[1]) {
+          if (et == 0) s_abort = 1;
+          break;
+        }
+        tc_fence_after();
+        if (whole) {
+          mbar_wait(c_full, (cuse++) & 1, status);  // (complete: the leader saw it)
+          // sC box q: rows 32 q ..; column j at 128 j bytes, 16-byte group (row & 31) / 4 swizzled with
+          // j & 7 (the TMA's 128-byte swizzle)
+          uint8_t* cb = sC + q * kCBox + (lane & 3) * 4;
 #pragma unroll 1
-      for (int c = 0; c < BN / 2 / 32; ++c) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * BN + (uint32_t)(half * (BN / 2) + c * 32), v);
-        float nv[32];
-        const int c0 = cbase + c * 32, c1 = c0 + 32;
-        if (c + 1 < BN / 2 / 32) {
+          for (int c = 0; c < BN / 2 / 32; ++c) {
+            float v[32];
+            const int j0 = half * (BN / 2) + c * 32;
+            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * BN + (uint32_t)j0, v);
 #pragma unroll
-          for (int j = 0; j < 32; ++j) nv[j] = (rok && c1 + j < n) ? __ldcs(crow + (size_t)(c1 + j) * ldc) : 0.f;
+            for (int jj = 0; jj < 32; ++jj) {
+              const int j = j0 + jj;
+              float* o = reinterpret_cast<float*>(cb + j * 128 + (((lane >> 2) ^ (j & 7)) << 4));
+              *o = *o - v[jj];
+            }
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[b]);
+          fence_async_smem();
+          epi_bar();
+          if (et == 0) {
+            for (int c = 0; c < 4; ++c) tma_store_2d(&tmC, sC + c * kCBox, crow0 + 32 * c, ccol0);
+            bulk_commit();
+            stored = true;
+          }
+          continue;
         }
-        if (rok) {
+        // a ragged tile: plain loads and stores, 32 columns at a time
+        const int row = tm * BM + q * 32 + lane;
+        const bool rok = row < m;
+        float* crow = C + row;
+#pragma unroll 1
+        for (int c = 0; c < BN / 2 / 32; ++c) {
+          float v[32];
+          const int c0 = tn * BN + half * (BN / 2) + c * 32;
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * BN + (uint32_t)(half * (BN / 2) + c * 32), v);
+          if (rok) {
+            float cv[32];
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (c0 + j < n) __stcs(crow + (size_t)(c0 + j) * ldc, cv[j] - v[j]);
+            for (int j = 0; j < 32; ++j) cv[j] = c0 + j < n ? __ldcs(crow + (size_t)(c0 + j) * ldc) : 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (c0 + j < n) __stcs(crow + (size_t)(c0 + j) * ldc, cv[j] - v[j]);
+          }
         }
-#pragma unroll
-        for (int j = 0; j < 32; ++j) cv[j] = nv[j];
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[b]);
       }
-      // every tcgen05.ld of this warp has completed (tmem_ld32 waits): release the accumulator
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acc_empty[b])) : "memory");
+      if (et == 0 && stored) bulk_wait_all();
+    } else {
+      // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (tile rows), columns [half * 128, half * 128 + 128)
+      const int q = warp & 3, half = (warp - 2) >> 2;
+      uint32_t local = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
+        const uint32_t b = local & 1, use = local >> 1;
+        int tm, tn;
+        tile_coords(tile, tiles_m, tiles_n, tm, tn);
+        const int row = tm * BM + q * 32 + lane;
+        const int cbase = tn * BN + half * (BN / 2);
+        const bool rok = row < m;
+        float* crow = C + row;
+        // C of the first 32 columns, loaded before the accumulator is ready
+        float cv[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) cv[j] = (rok && cbase + j < n) ? __ldcs(crow + (size_t)(cbase + j) * ldc) : 0.f;
+        if (!mbar_wait(&acc_full[b], use & 1, status) || *(volatile int*)&s_abort) break;
+        tc_fence_after();
+#pragma unroll 1
+        for (int c = 0; c < BN / 2 / 32; ++c) {
+          float v[32];
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + b * BN + (uint32_t)(half * (BN / 2) + c * 32), v);
+          float nv[32];
+          const int c0 = cbase + c * 32, c1 = c0 + 32;
+          if (c + 1 < BN / 2 / 32) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) nv[j] = (rok && c1 + j < n) ? __ldcs(crow + (size_t)(c1 + j) * ldc) : 0.f;
+          }
+          if (rok) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (c0 + j < n) __stcs(crow + (size_t)(c0 + j) * ldc, cv[j] - v[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) cv[j] = nv[j];
+        }
+        // every tcgen05.ld of this warp has completed (tmem_ld32 waits): release the accumulator
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acc_empty[b])) : "memory");
+      }
     }
   }
   tc_fence_before();
@@ -321,20 +433,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
       " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(kIdescTf32), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-// TMA store of a box from shared memory (bulk-group completion), its commit and waits
-__device__ __forceinline__ void tma_store_2d(const CUtensorMap* tm, const void* src, int x, int y) {
-  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"((uint64_t)tm),
-               "r"(x), "r"(y), "r"(smem_u32(src))
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;\n" ::"r"(32 * kEpiWarps) : "memory"); }
 
 // One 16 KB chunk from four MN-major boxes (box c: MN rows 32 c .. 32 c + 31; K row k at 128 k bytes,
 // 16-byte group g of a row at (g ^ (k & 7)) -- the TMA's 128-byte swizzle) to the K-major layout
@@ -836,7 +934,11 @@ bool tc_operand_maps(const void* At, int rows_a, long lda_t, const void* Bt, int
 }
 
 cudaError_t tc_gemm_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_gemm_bf16_tc<STAGES, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_bf16_tc<kStagesSmallK, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSmemStaged);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_panel_tf32<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
   if (e == cudaSuccess)
@@ -855,7 +957,8 @@ bool tc_panel_maps(const float* lu32, int n, long ld, const float* dl, const flo
   return make_map_f32(&m[kMapDL], dl, 128, diag_rows, 128, 32) &&    // MN-major boxes
          make_map_f32(&m[kMapDU], du, 128, diag_rows, 128, 128) &&   // K-major boxes
          make_map_f32(&m[kMapK], lu32, n, n, ld, 128) &&             // K-major boxes
-         make_map_f32(&m[kMapMN], lu32, n, n, ld, 32);               // MN-major boxes
+         make_map_f32(&m[kMapMN], lu32, n, n, ld, 32) &&             // MN-major boxes
+         make_map_f32(&m[kMapC], lu32, n, n, ld, 256);               // the BF16 GEMM's C tiles
 }
 
 bool tc_mirror_store_maps(const void* Am, const void* Bm, int n, long ldm, void* maps) {
@@ -891,10 +994,10 @@ cudaError_t gemm_bf16_tc_minus_maps(int m, int n, int k, const void* map_a, cons
                                     int* d_status, cudaStream_t s, unsigned long long* stamp) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  const cudaError_t e = launch_dependent(k_gemm_bf16_tc, dim3(persistent_grid(tiles_m * tiles_n)), dim3(kThreads),
-                                         kSmem, s, *static_cast<const CUtensorMap*>(map_a),
-                                         *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m, tiles_n,
-                                         d_status, 0, 0, 0, 0, stamp);
+  const CUtensorMap& ma = *static_cast<const CUtensorMap*>(map_a);
+  const cudaError_t e = launch_dependent(k_gemm_bf16_tc<STAGES, false>, dim3(persistent_grid(tiles_m * tiles_n)),
+                                         dim3(kThreads), kSmem, s, ma, *static_cast<const CUtensorMap*>(map_b), ma, m,
+                                         n, k, C, ldc, 0, 0, tiles_m, tiles_n, d_status, 0, 0, 0, 0, stamp);
   BGPU_COUNT_LAUNCH();
   return e;
 }
@@ -919,14 +1022,22 @@ bool tc_mirror_maps(const void* Am, const void* Bm, int n, long ldm, void* map_a
 // of 64.
 cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
                                   int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s,
-                                  unsigned long long* stamp) {
+                                  unsigned long long* stamp, const void* map_c, int c_row, int c_col) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
-  if ((a_k % 8) || (b_k % 8) || (k % BK)) return cudaErrorInvalidValue;
+  if ((a_k % 8) || (b_k % 8) || (k % BK) || (map_c && ((c_row % 4) || c_row < 0 || c_col < 0)))
+    return cudaErrorInvalidValue;
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  const cudaError_t e = launch_dependent(k_gemm_bf16_tc, dim3(persistent_grid(tiles_m * tiles_n)), dim3(kThreads),
-                                         kSmem, s, *static_cast<const CUtensorMap*>(map_a),
-                                         *static_cast<const CUtensorMap*>(map_b), m, n, k, C, ldc, tiles_m, tiles_n,
-                                         d_status, a_row, a_k, b_row, b_k, stamp);
+  const CUtensorMap& ma = *static_cast<const CUtensorMap*>(map_a);
+  const CUtensorMap& mb = *static_cast<const CUtensorMap*>(map_b);
+  const dim3 grid(persistent_grid(tiles_m * tiles_n));
+  cudaError_t e;
+  if (map_c && k / BK <= kSmallKTiles)
+    e = launch_dependent(k_gemm_bf16_tc<kStagesSmallK, true>, grid, dim3(kThreads), kSmemStaged, s, ma, mb,
+                         *static_cast<const CUtensorMap*>(map_c), m, n, k, C, ldc, c_row, c_col, tiles_m, tiles_n,
+                         d_status, a_row, a_k, b_row, b_k, stamp);
+  else
+    e = launch_dependent(k_gemm_bf16_tc<STAGES, false>, grid, dim3(kThreads), kSmem, s, ma, mb, ma, m, n, k, C, ldc, 0,
+                         0, tiles_m, tiles_n, d_status, a_row, a_k, b_row, b_k, stamp);
   BGPU_COUNT_LAUNCH();
   return e;
 }
@@ -941,13 +1052,14 @@ cudaError_t gemm_bf16_tc_minus(int m, int n, int k, const void* At, long lda_t, 
   if (!make_map(&ta, At, m, k, lda_t, BM) || !make_map(&tb, Bt, n, k, ldb_t, BN)) return cudaErrorInvalidValue;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_gemm_bf16_tc<STAGES, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  k_gemm_bf16_tc<<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(ta, tb, m, n, k, C, ldc, tiles_m,
-                                                                              tiles_n, d_status, 0, 0, 0, 0, nullptr);
+  k_gemm_bf16_tc<STAGES, false><<<persistent_grid(tiles_m * tiles_n), kThreads, kSmem, s>>>(
+      ta, tb, ta, m, n, k, C, ldc, 0, 0, tiles_m, tiles_n, d_status, 0, 0, 0, 0, nullptr);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
