@@ -332,14 +332,15 @@ def tensors_of(solver, x, st, bh):
 # ---- DRAM traffic of the tcgen05 GEMM over the LU's launches (profiles/tc_gemm_traffic_lu_shapes.md)
 def lu_gemm_shapes(n3, leaf=128):
     """The (m, n, k) of every GEMM of the mixed LU's recursion at order n3, in launch order (a replay
-    of MixedSolver's rlu / trsm recursion: the same 3,713 launches at n3 = 61,440)."""
+    of MixedSolver's rlu / trsm recursion: 2,017 launches at n3 = 61,440; a triangular solve 256 deep
+    is one 256-deep leaf, without a GEMM)."""
     out = []
 
     def split(sz):
         return max((sz // 2) // leaf * leaf, leaf)
 
     def trsm_left(h, w):
-        if h <= leaf or w <= 0:
+        if h <= 2 * leaf or w <= 0:
             return
         h1 = split(h)
         trsm_left(h1, w)
@@ -347,7 +348,7 @@ def lu_gemm_shapes(n3, leaf=128):
         trsm_left(h - h1, w)
 
     def trsm_right(h, m):
-        if h <= leaf or m <= 0:
+        if h <= 2 * leaf or m <= 0:
             return
         h1 = split(h)
         trsm_right(h1, m)

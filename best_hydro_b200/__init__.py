@@ -79,6 +79,9 @@ _SIGS = {
                                              ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_void_p, ctypes.c_int]),
     "bgpu_panel_update_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p] + [ctypes.c_int] * 9),
+    "bgpu_trsm_leaf256_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
     "bgpu_create_from_triangles": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                   _dp, _ip]),
     "bgpu_build_prepared": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
@@ -512,6 +515,14 @@ def trsm_leaf_device(left, n, d_a, lda, d_linv, d_uinv, kd, p0, h, length, d_mir
                                        ctypes.c_void_p(d_uinv), int(kd), int(p0), int(h), int(length),
                                        ctypes.c_void_p(d_mirror) if d_mirror else None, int(ldm)),
            "bgpu_trsm_leaf_device")
+
+
+def trsm_leaf256_device(left, n, d_a, lda, d_linv, d_uinv, kd, p0, length, d_mirror=None, ldm=0):
+    """bgpu_trsm_leaf256_device: the mixed LU's 256-deep triangular-solve leaf (see include/best_gpu.h)."""
+    _check(lib().bgpu_trsm_leaf256_device(int(bool(left)), int(n), ctypes.c_void_p(d_a), int(lda),
+                                          ctypes.c_void_p(d_linv), ctypes.c_void_p(d_uinv), int(kd), int(p0),
+                                          int(length), ctypes.c_void_p(d_mirror) if d_mirror else None, int(ldm)),
+           "bgpu_trsm_leaf256_device")
 
 
 def panel_update_device(n, d_a, lda, m, nc, ar, ac, br, bc, cr, cc):

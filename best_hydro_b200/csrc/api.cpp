@@ -1589,6 +1589,45 @@ int bgpu_trsm_leaf_device(int left, int n, float* d_a, int lda, const float* d_l
   });
 }
 
+int bgpu_trsm_leaf256_device(int left, int n, float* d_a, int lda, const float* d_linv, const float* d_uinv, int kd,
+                             int p0, int len, void* d_mirror, int ldm) {
+  return status_of([&] {
+    Runtime& r = rt();
+    const bool bad = n < 1 || lda < n || lda % 4 || len < 1 || kd < 0 || p0 < 0 || kd % 128 || p0 % 32 ||
+                     kd + 256 > n || p0 + len > n || (d_mirror && (ldm < n || ldm % 8));
+    if (bad) {
+      note("error: bgpu_trsm_leaf256_device: n %d, lda %d, kd %d, p0 %d, len %d, ldm %d out of range", n, lda, kd, p0,
+           len, ldm);
+      return 1;
+    }
+    ck(tc_gemm_prepare(), "tensor-core attributes");
+    const int slots = (n + 127) / 128;
+    DevBuf tl, tu;
+    tl.ensure((size_t)slots * 65536 * sizeof(float), "256-block inverses (L)");
+    tu.ensure((size_t)slots * 65536 * sizeof(float), "256-block inverses (U)");
+    alignas(64) unsigned char maps[kPanelMaps * kTensorMapBytes], tmaps[2 * kTensorMapBytes],
+        mmaps[2 * kTensorMapBytes];
+    if (!tc_panel_maps(d_a, n, lda, d_linv, d_uinv, maps) ||
+        !tc_leaf256_maps(tl.as<float>(), tu.as<float>(), slots, tmaps) ||
+        (d_mirror && !tc_mirror_store_maps(d_mirror, d_mirror, n, ldm, mmaps))) {
+      note("error: bgpu_trsm_leaf256_device: cannot build the tensor maps");
+      return 1;
+    }
+    ck(combine256(d_a, lda, kd, d_linv, d_uinv, tl.as<float>(), tu.as<float>(), r.stream), "256-block inverses");
+    float* X = left ? d_a + kd + (size_t)p0 * lda : d_a + p0 + (size_t)kd * lda;
+    void* mir = nullptr;
+    if (d_mirror) {
+      auto* m = static_cast<uint16_t*>(d_mirror);
+      mir = left ? (void*)(m + kd + (size_t)p0 * ldm) : (void*)(m + (size_t)p0 * ldm + kd);
+    }
+    ck(leaf256_tf32(left != 0, maps, tmaps, d_mirror ? mmaps : nullptr, kd / 128, kd, p0, 256, len, X, lda, mir, ldm,
+                    r.status.as<int>(), r.stream, nullptr),
+       "256-deep triangular-solve leaf");
+    r.check_status("256-deep triangular-solve leaf");  // (synchronises before the buffers go)
+    return 0;
+  });
+}
+
 int bgpu_panel_update_device(int n, float* d_a, int lda, int m, int nc, int ar, int ac, int br, int bc, int cr,
                              int cc) {
   return status_of([&] {

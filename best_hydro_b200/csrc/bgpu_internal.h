@@ -270,6 +270,19 @@ cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map
 // map_c (optional): a tensor map over C's FP32 matrix (tc_panel_maps' kMapC) with C at (c_row, c_col)
 // of it (c_row a multiple of 4): products of at most 8 K tiles then load and store whole C tiles by
 // TMA through shared memory.
+// The 256-deep triangular-solve leaf (k_leaf256_tf32): the inverses of 256 x 256 diagonal blocks,
+// column-major, one per slot (256 x 256 floats each; slot = the block's first row / 128), from
+// k_combine256 -- left [[D1, 0], [F, D2]] in dl256, right [[E1, G], [0, E2]] in du256; t_maps: two
+// tensor maps over them (tc_leaf256_maps).  Left: rows [kd, kd + h) x columns [p0, p0 + len) := Tinv
+// times that block; right: rows [p0, p0 + len) x columns [kd, kd + h) := that block times Tinv; in
+// place, with the BF16 mirror as panel_tf32's (kd, p0 multiples of 8; h <= 256).
+bool tc_leaf256_maps(const float* dl256, const float* du256, int slots, void* maps);
+// (mixed.cu) the 256 x 256 inverses of the diagonal block at (k0, k0) into slot k0 / 128 of TL, TU
+cudaError_t combine256(const float* LU, long lda, int k0, const float* DL, const float* DU, float* TL, float* TU,
+                       cudaStream_t s);
+cudaError_t leaf256_tf32(bool left, const void* maps, const void* t_maps, const void* mirror_maps, int slot, int kd,
+                         int p0, int h, int len, float* X, long ldx, void* mir, long ldm, int* d_status, cudaStream_t s,
+                         unsigned long long* stamp);
 cudaError_t gemm_bf16_tc_minus_at(int m, int n, int k, const void* map_a, int a_row, int a_k, const void* map_b,
                                   int b_row, int b_k, float* C, long ldc, int* d_status, cudaStream_t s,
                                   unsigned long long* stamp = nullptr, const void* map_c = nullptr, int c_row = 0,

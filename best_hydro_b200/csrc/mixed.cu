@@ -360,6 +360,77 @@ __device__ __forceinline__ void cp16(void* sdst, const void* gsrc, int src_bytes
 }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// The inverse of the 256 x 256 diagonal block at (k0, k0) from its two 128-block inverses, for the
+// 256-deep triangular-solve leaves (k_leaf256_tf32), column-major 256 x 256 into T:
+//   lower (blockIdx.y == 0): [[D1, 0], [F, D2]],  F = -D2 (L21 D1),  D = the unit-lower inverses (DL)
+//   upper (blockIdx.y == 1): [[E1, G], [0, E2]],  G = -E1 (U12 E2),  E = the upper inverses (DU)
+// L21 = the factor's block (k0 + 128, k0), U12 = (k0, k0 + 128).  CTA x: columns 16 x .. 16 x + 15
+// of each 128-column half; FP32 CUDA cores (two 128 x 128 x 16 products per CTA).
+constexpr size_t kCombineSmem = (size_t)(128 * 129 + 2 * 128 * 16) * sizeof(float);
+__global__ void __launch_bounds__(256) k_combine256(const float* __restrict__ LU, long lda, int k0,
+                                                     const float* __restrict__ DL, const float* __restrict__ DU,
+                                                     float* __restrict__ TL, float* __restrict__ TU,
+                                                     unsigned long long* stamp) {
+  stamp_begin(stamp);
+  extern __shared__ __align__(16) float sm[];
+  float* sA = sm;                     // a 128 x 128 operand, (r, k) at sA[k * 129 + r]
+  float* sB = sm + 128 * 129;         // the 128 x 16 slab operand, (k, c) at sB[k * 16 + c]
+  float* sT = sB + 128 * 16;          // the 128 x 16 intermediate
+  const bool lower = blockIdx.y == 0;
+  const int c0 = 16 * blockIdx.x, tid = threadIdx.x, r = tid & 127, ch = (tid >> 7) * 8;
+  const int b = k0 / 128;
+  const float* X1 = (lower ? DL : DU) + (size_t)b * 16384;        // D1 or E1
+  const float* X2 = (lower ? DL : DU) + (size_t)(b + 1) * 16384;  // D2 or E2
+  const float* off = lower ? LU + (size_t)k0 * lda + k0 + 128 : LU + (size_t)(k0 + 128) * lda + k0;  // L21 or U12
+  float* T = (lower ? TL : TU) + (size_t)b * 65536;
+  // product 1: lower L21 D1[:, slab], upper U12 E2[:, slab]
+  for (int e = tid; e < 128 * 128; e += 256) sA[(e >> 7) * 129 + (e & 127)] = off[(size_t)(e >> 7) * lda + (e & 127)];
+  const float* s1 = lower ? X1 : X2;
+  for (int e = tid; e < 128 * 16; e += 256) sB[(e & 127) * 16 + (e >> 7)] = s1[(size_t)(c0 + (e >> 7)) * 128 + (e & 127)];
+  __syncthreads();
+  float acc[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) acc[c] = 0.f;
+  for (int k = 0; k < 128; ++k) {
+    const float a = sA[k * 129 + r];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] += a * sB[k * 16 + ch + c];
+  }
+#pragma unroll
+  for (int c = 0; c < 8; ++c) sT[r * 16 + ch + c] = acc[c];
+  __syncthreads();
+  // product 2: lower -D2 T, upper -E1 T
+  const float* s2 = lower ? X2 : X1;
+  for (int e = tid; e < 128 * 128; e += 256) sA[(e >> 7) * 129 + (e & 127)] = s2[e];
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < 8; ++c) acc[c] = 0.f;
+  for (int k = 0; k < 128; ++k) {
+    const float a = sA[k * 129 + r];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] += a * sT[k * 16 + ch + c];
+  }
+  // columns c0 + c of the left half and 128 + c0 + c of the right half, all 256 rows
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int j = c0 + ch + c;
+    float* left = T + (size_t)j * 256;
+    float* right = T + (size_t)(128 + j) * 256;
+    if (lower) {
+      left[r] = X1[(size_t)j * 128 + r];
+      left[128 + r] = -acc[c];
+      right[r] = 0.f;
+      right[128 + r] = X2[(size_t)j * 128 + r];
+    } else {
+      left[r] = X1[(size_t)j * 128 + r];
+      left[128 + r] = 0.f;
+      right[r] = -acc[c];
+      right[128 + r] = X2[(size_t)j * 128 + r];
+    }
+  }
+  stamp_end(stamp);
+}
+
 constexpr int kLm = 132;  // row stride of the shared operands (floats)
 constexpr int kWideLeaf = 8192;  // from this many columns (rows) on, k_leaf_mult; below, 64 per CTA
 template <bool LEFT>
@@ -1008,7 +1079,7 @@ struct MixedSolver::Impl {
   int op_rows = 0;     // rows of both operand buffers
   const void* map_key[2] = {};      // the buffers the tensor maps describe
   cudaGraphExec_t graph = nullptr;  // the captured factorisation
-  const void* graph_key[7] = {};
+  const void* graph_key[8] = {};
   int graph_n = 0;
   size_t graph_kernels = 0;
   // per-launch device stamps of the GEMMs (live timing that works inside the graph): slots taken in
@@ -1072,6 +1143,12 @@ struct MixedSolver::Impl {
   bool tc_leaves = true;
   alignas(64) unsigned char map_leaf[kPanelMaps * kTensorMapBytes];
   const void* leaf_key[4] = {};
+  // the inverses of the 256 x 256 diagonal blocks (k_combine256, one slot per 128 rows) for the
+  // 256-deep leaves; has256[b]: formed for the block at row 128 b in this factorisation
+  Buf dl256, du256;
+  alignas(64) unsigned char map_t256[2 * kTensorMapBytes];
+  const void* t256_key[2] = {};
+  std::vector<char> has256;
   int* d_status() { return status.as<int>(); }
   __nv_bfloat16* am_at(int r, int c) const { return am.as<__nv_bfloat16>() + (size_t)r * ldm + c; }
   __nv_bfloat16* bm_at(int r, int c) const { return bm.as<__nv_bfloat16>() + (size_t)c * ldm + r; }
@@ -1149,6 +1226,15 @@ struct MixedSolver::Impl {
   // rows [kd, kd+h) x columns [c0, c0+w) := L^-1 (that block), L the unit lower triangle at (kd, kd)
   void trsm_llu(int kd, int h, int c0, int w, cudaStream_t s) {
     if (h <= 0 || w <= 0) return;
+    if (tc_leaves && h == 256 && has256[kd / kLeaf]) {
+      __nv_bfloat16* mir = mirrors ? bm_at(kd, c0) : nullptr;
+      prof.begin("trsm leaf 256 (left)", 2.0 * h * h * w, s);
+      ck(leaf256_tf32(true, map_leaf, map_t256, mir ? map_mst : nullptr, kd / kLeaf, kd, c0, h, w, at_(kd, c0), ld32,
+                      mir, ldm, d_status(), s, next_stamp(2.0 * h * h * w, kSlotSolveLeaf)),
+         "trsm leaf launch");
+      prof.end(s);
+      return;
+    }
     if (h <= kLeaf) {
       const float* dinv = dl32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf;
       __nv_bfloat16* mir = mirrors ? bm_at(kd, c0) : nullptr;
@@ -1178,6 +1264,15 @@ struct MixedSolver::Impl {
   // rows [r0, r0+m) x columns [kd, kd+h) := (that block) U^-1, U the upper triangle at (kd, kd)
   void trsm_ru(int kd, int h, int r0, int m, cudaStream_t s) {
     if (h <= 0 || m <= 0) return;
+    if (tc_leaves && h == 256 && has256[kd / kLeaf]) {
+      __nv_bfloat16* mir = mirrors ? am_at(r0, kd) : nullptr;
+      prof.begin("trsm leaf 256 (right)", 2.0 * h * h * m, s);
+      ck(leaf256_tf32(false, map_leaf, map_t256, mir ? map_mst : nullptr, kd / kLeaf, kd, r0, h, m, at_(r0, kd), ld32,
+                      mir, ldm, d_status(), s, next_stamp(2.0 * h * h * m, kSlotSolveLeaf)),
+         "trsm leaf launch");
+      prof.end(s);
+      return;
+    }
     if (h <= kLeaf) {
       const float* dinv = du32.as<float>() + (size_t)(kd / kLeaf) * kLeaf * kLeaf;
       __nv_bfloat16* mir = mirrors ? am_at(r0, kd) : nullptr;
@@ -1233,6 +1328,17 @@ struct MixedSolver::Impl {
     }
     gemm(r, r, h, k0 + h, k0, k0, k0 + h, k0 + h, k0 + h, s);
     rlu(k0 + h, r, s);
+    if (tc_leaves && sz == 256) {
+      // the 256 x 256 block's inverses, for the 256-deep leaves below it
+      prof.begin("256-block inverses", 0, s);
+      ck(launch_dependent(k_combine256, dim3(8, 2), dim3(256), kCombineSmem, s, (const float*)lu32.as<float>(),
+                          (long)ld32, k0, (const float*)dl32.as<float>(), (const float*)du32.as<float>(),
+                          dl256.as<float>(), du256.as<float>(), next_stamp(0, kSlotLuLeaf)),
+         "256-block inverses");
+      prof.end(s);
+      BGPU_COUNT_LAUNCH();
+      has256[k0 / kLeaf] = 1;
+    }
   }
 
   // Y (n3 x q, ldy) = beta Y + alpha GR X
@@ -1271,6 +1377,20 @@ struct MixedSolver::Impl {
     return h;
   }
 };
+
+cudaError_t combine256(const float* LU, long lda, int k0, const float* DL, const float* DU, float* TL, float* TU,
+                       cudaStream_t s) {
+  if (k0 < 0 || k0 % 128) return cudaErrorInvalidValue;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_combine256, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCombineSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_combine256<<<dim3(8, 2), 256, kCombineSmem, s>>>(LU, lda, k0, DL, DU, TL, TU, nullptr);
+  BGPU_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
 
 cudaError_t lu32_leaf(float* A, long lda, int h, float* DL, float* DU, int* status, cudaStream_t s) {
   if (h <= 0 || h > 128 || lda < h) return cudaErrorInvalidValue;
@@ -1353,6 +1473,18 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     P.leaf_key[2] = P.du32.p;
     P.leaf_key[3] = reinterpret_cast<const void*>((uintptr_t)P.n3);
   }
+  if (P.tc_leaves) {
+    const int slots = (P.n3 + kLeaf - 1) / kLeaf;
+    P.dl256.ensure((size_t)slots * 65536 * sizeof(float), "256-block inverses (L)");
+    P.du256.ensure((size_t)slots * 65536 * sizeof(float), "256-block inverses (U)");
+    if (P.t256_key[0] != P.dl256.p || P.t256_key[1] != P.du256.p) {
+      if (!tc_leaf256_maps(P.dl256.as<float>(), P.du256.as<float>(), (int)(P.dl256.bytes / (65536 * sizeof(float))),
+                           P.map_t256))
+        throw std::runtime_error("cannot build the tensor maps of the 256-block inverses");
+      P.t256_key[0] = P.dl256.p;
+      P.t256_key[1] = P.du256.p;
+    }
+  }
   // BF16 mirrors when they fit with 4 GB to spare, else operand copies per product
   const long ldm = round_up(P.n3, 64);
   const size_t mirror_bytes = (size_t)P.n3 * ldm * 2;
@@ -1394,6 +1526,8 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     }
   }
   ck(tc_gemm_prepare(), "tensor-core GEMM attributes");
+  ck(cudaFuncSetAttribute(k_combine256, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCombineSmem),
+     "256-block inverse attributes");
   static bool attrs = false;
   if (!attrs) {
     const int big = 200 * 1024;
@@ -1430,6 +1564,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     P.slot_work = 0;
     P.slot_kind.clear();
     P.slot_flop.clear();
+    P.has256.assign((size_t)(P.n3 + kLeaf - 1) / kLeaf, 0);
     ck(stamps_reset(P.stamps.as<unsigned long long>(), P.slot_cap, s), "stamps");
     P.rlu(0, P.n3, s);  // direct launches in order, each timed
     ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3, P.wl32.as<float>(),
@@ -1440,9 +1575,9 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   } else {
     // the recursion's launches depend only on the order and the buffers: capture them once as a
     // CUDA graph and replay it
-    const void* key[7] = {P.lu32.p, P.mirrors ? P.am.p : P.at.p, P.mirrors ? P.bm.p : P.bt.p,
-                          P.dl32.p, P.du32.p, P.stamps.p, P.wl32.p};
-    if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 7, P.graph_key)) {
+    const void* key[8] = {P.lu32.p, P.mirrors ? P.am.p : P.at.p, P.mirrors ? P.bm.p : P.bt.p,
+                          P.dl32.p, P.du32.p, P.stamps.p, P.wl32.p, P.tc_leaves ? P.dl256.p : nullptr};
+    if (!P.graph || P.graph_n != P.n3 || !std::equal(key, key + 8, P.graph_key)) {
       const clk::time_point t_cap = clk::now();
       if (P.graph) cudaGraphExecDestroy(P.graph);
       P.graph = nullptr;
@@ -1456,6 +1591,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       P.slot_work = 0;
       P.slot_kind.clear();
       P.slot_flop.clear();
+      P.has256.assign((size_t)(P.n3 + kLeaf - 1) / kLeaf, 0);
       try {
         P.rlu(0, P.n3, cs);
         ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3,
@@ -1477,7 +1613,7 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       ms_inst = ms_since(t_inst);
       cudaGraphDestroy(g);
       cudaStreamDestroy(cs);
-      std::copy(key, key + 7, P.graph_key);
+      std::copy(key, key + 8, P.graph_key);
       P.graph_n = P.n3;
       P.graph_slots = P.nslots;
       P.graph_work = P.slot_work;

@@ -805,6 +805,297 @@ __global__ void __launch_bounds__(kPtThreads, 1)
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// A triangular-solve leaf 256 deep on the tensor cores (TF32): the inverse of a 256 x 256 diagonal
+// block, T^-1 = [[D1, 0], [F, D2]] (lower) or [[E1, G], [0, E2]] (upper) with F = -D2 L21 D1 and
+// G = -E1 U12 E2 (k_combine256), applied to the 256-deep panel in one launch instead of leaf, K = 128
+// update, leaf:
+//   left:  X (256 x len) := Tinv P      right: X (len x 256) := P Tinv
+// Each CTA owns whole 128-long tiles of the panel and forms both 128-halves of each (row groups on
+// the left, column groups on the right) in two TMEM accumulators before any of the tile is written:
+// the result replaces the panel in place, and the second half reads all 256 of the tile's inputs.
+// The work of a tile is 12 steps of a 32-deep K chunk: half 0 over K 0..127 (the zero quarter of
+// Tinv skipped), half 1 over K 0..255.  Each step brings a K-major chunk by TMA ("direct": P on the
+// left, Tinv on the right) and an MN-major one as four 32 x 32 boxes that the four transposer warps
+// rewrite K-major ("trans": Tinv on the left, P on the right), the MMA's A operand always the trans
+// slot and B the direct one.  The epilogue stages each whole 128 x 128 half through shared memory
+// for TMA stores, with the BF16 mirror; ragged halves and tiles by plain stores.
+constexpr int kL2Stages = 2;
+constexpr uint32_t kL2Stage = 3 * kPtChunk;  // direct, trans, raw
+constexpr uint32_t kL2OutOff = kL2Stages * kL2Stage;
+constexpr uint32_t kL2MirOff = kL2OutOff + 4 * kPtChunk;
+constexpr uint32_t kL2BarOff = kL2MirOff + 2 * kPtChunk;
+constexpr uint32_t kL2Smem = kL2BarOff + 256 + 1024;
+constexpr uint32_t kL2TmemCols = 512;  // two tiles in flight x two halves x 128 columns
+constexpr int kL2Steps = 12;           // (half, K chunk) steps per tile
+
+__device__ __forceinline__ void l2_step(int st, int& half, int& kc) {
+  half = st < 4 ? 0 : 1;
+  kc = st < 4 ? st : st - 4;
+}
+
+// tmT: Tinv's map (left: MN-major 32 x 32 boxes over the column-major 256 x 256 blocks, inner 256;
+// right: K-major 32 x 128 boxes), block at outer coordinate t0 (256 per diagonal block); tmP, tmX, tmM
+// as k_panel_tf32's (the factor's K-major map for the left P and for X, the MN-major one for the
+// right P; the mirror's).  The panel starts at (px0, py0): left P chunk kc at (px0 + 32 kc,
+// py0 + 128 tile); right at (px0 + 128 tile + 32 c, py0 + 32 kc).  X at (xr0, xc0) of the factor;
+// h <= 256 rows (left) or columns (right) of it.
+template <bool LEFT>
+__global__ void __launch_bounds__(kPtThreads, 1)
+    k_leaf256_tf32(const __grid_constant__ CUtensorMap tmT, const __grid_constant__ CUtensorMap tmP,
+                   const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmM, int t0, int px0,
+                   int py0, int h, int len, float* __restrict__ X, long ldx, int xr0, int xc0,
+                   __nv_bfloat16* __restrict__ mir, long ldm, int* status, unsigned long long* stamp) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint8_t* sOut = smem + kL2OutOff;
+  uint8_t* sMir = smem + kL2MirOff;
+  uint64_t* dir_full = reinterpret_cast<uint64_t*>(smem + kL2BarOff);
+  uint64_t* raw_full = dir_full + kL2Stages;
+  uint64_t* raw_empty = raw_full + kL2Stages;
+  uint64_t* tr_full = raw_empty + kL2Stages;
+  uint64_t* st_empty = tr_full + kL2Stages;  // the MMA has read the stage's direct and trans slots
+  uint64_t* acc_full = st_empty + kL2Stages;  // [2]
+  uint64_t* acc_empty = acc_full + 2;         // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  int* s_flags = reinterpret_cast<int*>(tmem_slot + 1);  // [0] abort, [1] the epilogue goes on
+  volatile int& s_abort = s_flags[0];
+  auto dir = [&](uint32_t s) { return smem + s * kL2Stage; };
+  auto trs = [&](uint32_t s) { return smem + s * kL2Stage + kPtChunk; };
+  auto raw = [&](uint32_t s) { return smem + s * kL2Stage + 2 * kPtChunk; };
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntiles = (len + 127) / 128;
+  const int tr_first = 2 + kEpiWarps;
+
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < kL2Stages; ++s) {
+      mbar_init(&dir_full[s], 1);
+      mbar_init(&raw_full[s], 1);
+      mbar_init(&raw_empty[s], kPtTrWarps);
+      mbar_init(&tr_full[s], kPtTrWarps);
+      mbar_init(&st_empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], kEpiWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kL2TmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  pdl_wait();
+  pdl_trigger();
+  if (stamp && threadIdx.x == 0) atomicMin(stamp, global_ns());
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !s_abort; tile += gridDim.x) {
+        for (int st = 0; st < kL2Steps; ++st, ++it) {
+          int g, kc;
+          l2_step(st, g, kc);
+          const uint32_t s = it % kL2Stages, ph = ((it / kL2Stages) & 1) ^ 1;
+          if (it >= kL2Stages && (!mbar_wait(&st_empty[s], ph, status) || !mbar_wait(&raw_empty[s], ph, status))) {
+            s_abort = 1;
+            break;
+          }
+          if (s_abort) break;
+          mbar_expect_tx(&dir_full[s], kPtChunk);
+          mbar_expect_tx(&raw_full[s], kPtChunk);
+          if (LEFT) {
+            tma_load_2d(dir(s), &tmP, px0 + 32 * kc, py0 + 128 * tile, &dir_full[s]);
+            for (int c = 0; c < 4; ++c) tma_load_2d(raw(s) + c * 4096, &tmT, 128 * g + 32 * c, t0 + 32 * kc, &raw_full[s]);
+          } else {
+            tma_load_2d(dir(s), &tmT, 32 * kc, t0 + 128 * g, &dir_full[s]);
+            for (int c = 0; c < 4; ++c)
+              tma_load_2d(raw(s) + c * 4096, &tmP, px0 + 128 * tile + 32 * c, py0 + 32 * kc, &raw_full[s]);
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      uint32_t it = 0, local = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++local) {
+        const uint32_t b = local & 1, use = local >> 1;
+        if (use >= 1 && !mbar_wait(&acc_empty[b], (use - 1) & 1, status)) {
+          s_abort = 1;
+          break;
+        }
+        tc_fence_after();
+        for (int st = 0; st < kL2Steps; ++st, ++it) {
+          int g, kc;
+          l2_step(st, g, kc);
+          const uint32_t s = it % kL2Stages, ph = (it / kL2Stages) & 1;
+          if (!mbar_wait(&dir_full[s], ph, status) || !mbar_wait(&tr_full[s], ph, status)) {
+            s_abort = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t acc = tmem + (b * 2 + g) * 128;
+          const uint32_t a0 = smem_u32(trs(s)), b0 = smem_u32(dir(s));
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+            mma_tf32(acc, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), (kc > 0 || kk > 0) ? 1u : 0u);
+          mma_commit(&st_empty[s]);
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[b]);
+      }
+    }
+  } else if (warp >= tr_first) {
+    const int t = threadIdx.x - 32 * tr_first;
+    uint32_t it = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+      for (int st = 0; st < kL2Steps; ++st, ++it) {
+        const uint32_t s = it % kL2Stages, ph = (it / kL2Stages) & 1;
+        if (!mbar_wait(&raw_full[s], ph, status) || (it >= kL2Stages && !mbar_wait(&st_empty[s], ph ^ 1, status)) ||
+            s_abort) {
+          s_abort = 1;
+          ok = false;
+          break;
+        }
+        transpose_chunk(raw(s), trs(s), t);
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&raw_empty[s]);
+          mbar_arrive(&tr_full[s]);
+        }
+      }
+    }
+  } else {
+    // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (the tile's rows), columns [64 cw, 64 cw + 64) of each
+    // half's accumulator; thread et == 0 leads (the TMA stores and the waits whose outcome all share)
+    const int q = warp & 3, cw = (warp - 2) >> 2;
+    const int et = threadIdx.x - 64;
+    const int r = q * 32 + lane;  // accumulator row
+    uint32_t local = 0;
+    bool stored = false;  // (leader) a TMA store from sOut / sMir in flight
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++local) {
+      const uint32_t b = local & 1, use = local >> 1;
+      if (et == 0) s_flags[1] = mbar_wait(&acc_full[b], use & 1, status) && !s_abort;
+      epi_bar();
+      if (!s_flags[1]) {
+        if (et == 0) s_abort = 1;
+        break;
+      }
+      tc_fence_after();
+      for (int g = 0; g < 2; ++g) {
+        const int hg = min(h - 128 * g, 128);  // rows (left) or columns (right) of X in this half
+        if (hg <= 0) break;
+        const bool whole = hg == 128 && 128 * (tile + 1) <= len;
+        const int trow = xr0 + (LEFT ? 128 * g : 128 * tile), tcol = xc0 + (LEFT ? 128 * tile : 128 * g);
+        const uint32_t accb = tmem + ((uint32_t)(q * 32) << 16) + (b * 2 + g) * 128;
+        if (whole) {
+          if (et == 0 && stored) bulk_wait_read();  // the last stores have read sOut, sMir
+          epi_bar();
+          // sOut box q: rows 32 q ..; column j at 128 j bytes, 16-byte group (row & 31) / 4 swizzled with
+          // j & 7 (the TMA's 128-byte swizzle)
+          uint8_t* ob = sOut + q * kPtChunk + (lane & 3) * 4;
+#pragma unroll 1
+          for (int c = 0; c < 2; ++c) {
+            float v[32];
+            const int j0 = 64 * cw + 32 * c;
+            tmem_ld32(accb + (uint32_t)j0, v);
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj) {
+              const int j = j0 + jj;
+              *reinterpret_cast<float*>(ob + j * 128 + (((lane >> 2) ^ (j & 7)) << 4)) = v[jj];
+              if (LEFT && mir)
+                *reinterpret_cast<__nv_bfloat16*>(sMir + (r >> 6) * kPtChunk + j * 128 +
+                                                 ((((r & 63) >> 3) ^ (j & 7)) << 4) + (r & 7) * 2) =
+                    __float2bfloat16_rn(v[jj]);
+            }
+            if (!LEFT && mir) {
+#pragma unroll
+              for (int gg = 0; gg < 4; ++gg) {
+                uint4 pk;
+                uint32_t* w = reinterpret_cast<uint32_t*>(&pk);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                  const __nv_bfloat162 two = __floats2bfloat162_rn(v[8 * gg + 2 * e], v[8 * gg + 2 * e + 1]);
+                  w[e] = *reinterpret_cast<const uint32_t*>(&two);
+                }
+                *reinterpret_cast<uint4*>(sMir + (j0 >> 6) * kPtChunk + r * 128 +
+                                          (((((j0 & 63) >> 3) + gg) ^ (r & 7)) << 4)) = pk;
+              }
+            }
+          }
+          fence_async_smem();
+          epi_bar();
+          if (et == 0) {
+            for (int c = 0; c < 4; ++c) tma_store_2d(&tmX, sOut + c * kPtChunk, trow + 32 * c, tcol);
+            if (mir) {
+              for (int c = 0; c < 2; ++c) {
+                if (LEFT)
+                  tma_store_2d(&tmM, sMir + c * kPtChunk, trow + 64 * c, tcol);  // (row, column)
+                else
+                  tma_store_2d(&tmM, sMir + c * kPtChunk, tcol + 64 * c, trow);  // (column, row)
+              }
+            }
+            bulk_commit();
+            stored = true;
+          }
+        } else {
+          // a ragged half: plain stores.  Left: X (128 g + r, 128 tile + j); right: X (128 tile + r,
+          // 128 g + j)
+          const int xi = LEFT ? 128 * g + r : 128 * tile + r;
+          const bool rok = LEFT ? r < hg : 128 * tile + r < len;
+          const int jbase = LEFT ? 128 * tile : 128 * g;
+          const int jlim = LEFT ? len - 128 * tile : hg;
+#pragma unroll 1
+          for (int c = 0; c < 2; ++c) {
+            float v[32];
+            const int j0 = 64 * cw + 32 * c;
+            tmem_ld32(accb + (uint32_t)j0, v);
+            if (!rok) continue;
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj) {
+              const int j = j0 + jj;
+              if (j < jlim) {
+                X[(size_t)(jbase + j) * ldx + xi] = v[jj];
+                if (mir) {
+                  if (LEFT)
+                    mir[(size_t)(jbase + j) * ldm + xi] = __float2bfloat16_rn(v[jj]);
+                  else
+                    mir[(size_t)xi * ldm + jbase + j] = __float2bfloat16_rn(v[jj]);
+                }
+              }
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[b]);
+    }
+    if (et == 0 && stored) bulk_wait_all();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kL2TmemCols));
+  }
+  if (stamp && threadIdx.x == 0) {
+    __threadfence();
+    atomicMax(stamp + 1, global_ns());
+  }
+}
+
 __global__ void k_stamps_reset(unsigned long long* stamps, int slots) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < slots; i += gridDim.x * blockDim.x) {
     stamps[2 * i] = ~0ull;
@@ -940,6 +1231,10 @@ cudaError_t tc_gemm_prepare() {
     e = cudaFuncSetAttribute(k_gemm_bf16_tc<kStagesSmallK, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kSmemStaged);
   if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_leaf256_tf32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kL2Smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_leaf256_tf32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kL2Smem);
+  if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_panel_tf32<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_panel_tf32<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
@@ -966,6 +1261,35 @@ bool tc_mirror_store_maps(const void* Am, const void* Bm, int n, long ldm, void*
   CUtensorMap* m = static_cast<CUtensorMap*>(maps);
   return make_map(&m[0], Bm, n, n, ldm, 128) &&  // left leaves: column-major mirror, boxes 64 rows x 128
          make_map(&m[1], Am, n, n, ldm, 128);    // right leaves: row-major mirror, boxes 64 columns x 128
+}
+
+bool tc_leaf256_maps(const float* dl256, const float* du256, int slots, void* maps) {
+  if (((uintptr_t)dl256 & 15) || ((uintptr_t)du256 & 15) || slots <= 0) return false;
+  CUtensorMap* m = static_cast<CUtensorMap*>(maps);
+  return make_map_f32(&m[0], dl256, 256, (long)slots * 256, 256, 32) &&  // left: MN-major boxes
+         make_map_f32(&m[1], du256, 256, (long)slots * 256, 256, 128);   // right: K-major boxes
+}
+
+cudaError_t leaf256_tf32(bool left, const void* maps, const void* t_maps, const void* mirror_maps, int slot, int kd,
+                         int p0, int h, int len, float* X, long ldx, void* mir, long ldm, int* d_status, cudaStream_t s,
+                         unsigned long long* stamp) {
+  if (len <= 0 || h <= 0) return cudaSuccess;
+  const int xr0 = left ? kd : p0, xc0 = left ? p0 : kd;
+  if (h > 256 || (kd % 8) || (p0 % 8) || slot < 0 || (mir && !mirror_maps)) return cudaErrorInvalidValue;
+  const CUtensorMap* m = static_cast<const CUtensorMap*>(maps);
+  const CUtensorMap* tm = static_cast<const CUtensorMap*>(t_maps) + (left ? 0 : 1);
+  const CUtensorMap* mm = mir ? static_cast<const CUtensorMap*>(mirror_maps) + (left ? 0 : 1) : &m[kMapK];
+  const dim3 grid(persistent_grid((len + 127) / 128)), block(kPtThreads);
+  __nv_bfloat16* mb = static_cast<__nv_bfloat16*>(mir);
+  // left P: the K-major map, panel rows kd.., columns p0..; right P: the MN-major map, rows p0..,
+  // columns kd..
+  const cudaError_t e =
+      left ? launch_dependent(k_leaf256_tf32<true>, grid, block, kL2Smem, s, *tm, m[kMapK], m[kMapK], *mm, 256 * slot,
+                              kd, p0, h, len, X, ldx, xr0, xc0, mb, ldm, d_status, stamp)
+           : launch_dependent(k_leaf256_tf32<false>, grid, block, kL2Smem, s, *tm, m[kMapMN], m[kMapK], *mm,
+                              256 * slot, p0, kd, h, len, X, ldx, xr0, xc0, mb, ldm, d_status, stamp);
+  BGPU_COUNT_LAUNCH();
+  return e;
 }
 
 cudaError_t panel_tf32(bool left, bool sub, const void* maps, int map_r, int map_p, const void* mirror_maps, int rx0,

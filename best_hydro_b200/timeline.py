@@ -1,7 +1,7 @@
 """Per-launch durations of the mixed LU's factorisation, from the launch stamps the library writes
 when ``BEST_GPU_TIMELINE=<file>`` is set (one ``slot,kind,flops,start_ns,end_ns`` line per stamped
-launch, appended per factorisation; kinds 0 BF16 GEMM, 1 LU leaf, 2 triangular-solve leaf, 3 small
-FP32 update, 4 TF32 panel update).
+launch, appended per factorisation; kinds 0 BF16 GEMM, 1 LU leaf or 256-block inverses, 2
+triangular-solve leaf, 3 small FP32 update, 4 TF32 panel update).
 
     python -m best_hydro_b200.timeline DUMP.csv N3
 
@@ -29,8 +29,9 @@ def _update_kind(m, n, k):
 
 def launch_labels(n3):
     """(kind, m, n, k) of every stamped launch of the factorisation at order n3, in launch order:
-    kind "lu" (diagonal leaf), "leafL" / "leafR" (triangular-solve leaves: h x w, m x h), "panel"
-    (TF32 panel update), "gemm" (BF16 tensor-core GEMM)."""
+    kind "lu" (diagonal leaf), "inv256" (a 256-block's inverses), "leafL" / "leafR" (triangular-solve
+    leaves: h x w, m x h; k = their depth, 128 or 256), "panel" (TF32 panel update), "gemm" (BF16
+    tensor-core GEMM)."""
     out = []
 
     def gemm(m, n, k):
@@ -40,8 +41,8 @@ def launch_labels(n3):
     def trsm_left(h, w):
         if h <= 0 or w <= 0:
             return
-        if h <= LEAF:
-            out.append(("leafL", h, w, LEAF))
+        if h <= LEAF or h == 2 * LEAF:
+            out.append(("leafL", h, w, h))
             return
         h1 = _split(h)
         trsm_left(h1, w)
@@ -51,8 +52,8 @@ def launch_labels(n3):
     def trsm_right(h, m):
         if h <= 0 or m <= 0:
             return
-        if h <= LEAF:
-            out.append(("leafR", m, h, LEAF))
+        if h <= LEAF or h == 2 * LEAF:
+            out.append(("leafR", m, h, h))
             return
         h1 = _split(h)
         trsm_right(h1, m)
@@ -70,6 +71,8 @@ def launch_labels(n3):
         trsm_right(h, r)
         gemm(r, r, h)
         rlu(r)
+        if sz == 2 * LEAF:
+            out.append(("inv256", sz, sz, sz))
 
     rlu(n3)
     return out
@@ -78,7 +81,7 @@ def launch_labels(n3):
 def _class(kind, m, n, k):
     if kind in ("leafL", "leafR"):
         w = n if kind == "leafL" else m
-        return f"{kind} {'w<=256' if w <= 256 else ('w<=2048' if w <= 2048 else 'w>2048')}"
+        return f"{kind}{k} {'w<=256' if w <= 256 else ('w<=2048' if w <= 2048 else 'w>2048')}"
     if kind == "gemm" and max(m, n) >= 4096:
         return f"gemm large, k={k}"
     if kind in ("gemm", "panel", "small"):

@@ -124,10 +124,20 @@ int bgpu_lu32_leaf_device(int h, float *d_a, int lda, float *d_linv, float *d_ui
 int bgpu_trsm_leaf_device(int left, int n, float *d_a, int lda, const float *d_linv, const float *d_uinv, int kd,
                           int p0, int h, int len, void *d_mirror, int ldm);
 
+/* The mixed-precision LU's 256-deep triangular-solve leaf (TF32 tensor cores; device memory): the
+ * inverse of the 256 x 256 diagonal block at (kd, kd) of the n x n FP32 factor d_a (unit lower L and
+ * upper U packed, column-major, lda a multiple of 4) is formed from the inverses of its two 128-blocks
+ * (d_linv, d_uinv as bgpu_trsm_leaf_device's) and the off-diagonal blocks L21, U12 of d_a, then left
+ * != 0: rows [kd, kd + 256) x columns [p0, p0 + len) := L^-1 times that block; left == 0: rows
+ * [p0, p0 + len) x columns [kd, kd + 256) := that block times U^-1; in place, with the BF16 mirror as
+ * bgpu_trsm_leaf_device's.  kd a multiple of 128, p0 of 32. */
+int bgpu_trsm_leaf256_device(int left, int n, float *d_a, int lda, const float *d_linv, const float *d_uinv, int kd,
+                             int p0, int len, void *d_mirror, int ldm);
+
 /* The mixed-precision LU's K = 128 update on the tensor cores (TF32 operands, FP32 accumulation;
  * device memory): in the n x n FP32 matrix d_a (column-major, lda a multiple of 4), the m x nc block
  * at (cr, cc) -= the m x 128 block at (ar, ac) times the 128 x nc block at (br, bc), with m or nc at
- * most 128 and ar, br, cr multiples of 4.  The blocks may lie anywhere in the matrix but the result
+ * most 256 and ar, br, cr multiples of 4.  The blocks may lie anywhere in the matrix but the result
  * block must not overlap the other two. */
 int bgpu_panel_update_device(int n, float *d_a, int lda, int m, int nc, int ar, int ac, int br, int bc, int cr,
                              int cc);

@@ -1,13 +1,13 @@
 """CPU checks of bench.py's accounting: the replay of the mixed LU's GEMM shapes gives the launch
-count the library stamps (3,713 at order 61,440: 1,569 BF16 tensor-core GEMMs and 2,144 TF32 panel
-updates) and the LU's flop count, and the traffic estimate stays within the
+count the library stamps (2,017 at order 61,440: 1,569 BF16 tensor-core GEMMs and 448 TF32 panel
+updates; a triangular solve 256 deep is one leaf) and the LU's flop count, and the traffic estimate stays within the
 measured per-class ratios."""
 import bench
 
 
 def test_lu_gemm_shapes_replay():
     shapes = bench.lu_gemm_shapes(61440)
-    assert len(shapes) == 3713
+    assert len(shapes) == 2017
     flops = sum(2 * m * n * k for m, n, k in shapes)
     n = 61440
     # (2/3) n^3 minus the diagonal leaves' and triangular-solve leaves' share
@@ -20,5 +20,5 @@ def test_gemm_traffic_estimate_in_range():
     lo, hi = min(bench.GEMM_TRAFFIC_RATIO.values()), max(bench.GEMM_TRAFFIC_RATIO.values())
     shapes = bench.lu_gemm_shapes(61440)
     panel = sum(1 for sh in shapes if bench.panel_update(*sh))
-    assert panel == 2144
-    assert count == 3713 - panel == 1569 and lo * alg <= tr <= hi * alg
+    assert panel == 448
+    assert count == 2017 - panel == 1569 and lo * alg <= tr <= hi * alg

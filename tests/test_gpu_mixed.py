@@ -123,6 +123,64 @@ def test_trsm_leaf_tc(left, kd, p0, length):
     assert np.all(mir_out == 3.0)
 
 
+@pytest.mark.parametrize("left,kd,p0,length", [(True, 256, 512, 256), (False, 128, 384, 384), (True, 0, 256, 200),
+                                               (False, 512, 0, 96), (True, 384, 640, 128)])
+def test_trsm_leaf256_tc(left, kd, p0, length):
+    """The LU's 256-deep triangular-solve leaf (k_combine256 + k_leaf256_tf32): the 256 x 256
+    diagonal block's inverse formed from its two 128-block inverses, applied to the panel in place,
+    against FP64 within 2^-8 of |T^-1| |P| (TF32 operands); the BF16 mirror equal to the result rounded
+    to nearest; everything outside the panel untouched; whole and ragged tiles."""
+    torch = _torch()
+    n, lda, ldm = 768, 772, 768
+    nleaves = n // 128
+    rng = np.random.default_rng(kd + 3 * p0 + length + int(left))
+    A = rng.standard_normal((n, n))
+    for b in range(nleaves):  # well-conditioned diagonal blocks: small L, dominant U diagonal
+        sl = slice(128 * b, 128 * b + 128)
+        blk = A[sl, sl]
+        A[sl, sl] = np.tril(blk, -1) * 0.3 / np.sqrt(128) + np.triu(blk, 1) * 0.3 / np.sqrt(128) + np.diag(
+            2.0 + np.abs(np.diag(blk)))
+    sl2 = slice(kd, kd + 256)
+    A[kd + 128:kd + 256, kd:kd + 128] *= 0.3 / np.sqrt(128)  # L21
+    A[kd:kd + 128, kd + 128:kd + 256] *= 0.3 / np.sqrt(128)  # U12
+    A = A.astype(np.float32).astype(np.float64)
+    DL = np.zeros((nleaves, 128, 128))
+    DU = np.zeros((nleaves, 128, 128))
+    for b in range(nleaves):
+        blk = A[128 * b:128 * b + 128, 128 * b:128 * b + 128]
+        DL[b] = np.linalg.inv(np.tril(blk, -1) + np.eye(128))
+        DU[b] = np.linalg.inv(np.triu(blk))
+    dA = torch.zeros((n, lda), dtype=torch.float32)
+    dA[:, :n] = torch.from_numpy(np.ascontiguousarray(A.T).astype(np.float32))
+    dA = dA.cuda()
+    dDL = torch.from_numpy(np.ascontiguousarray(np.transpose(DL, (0, 2, 1))).astype(np.float32)).cuda()
+    dDU = torch.from_numpy(np.ascontiguousarray(np.transpose(DU, (0, 2, 1))).astype(np.float32)).cuda()
+    mirror = torch.full((n, ldm), 3.0, dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    bh.trsm_leaf256_device(left, n, dA.data_ptr(), lda, dDL.data_ptr(), dDU.data_ptr(), kd, p0, length,
+                           mirror.data_ptr(), ldm)
+    got_all = dA.cpu().numpy()[:, :n].T.astype(np.float64)
+    T = A[sl2, sl2]
+    if left:
+        Tinv = np.linalg.inv(np.tril(T, -1) + np.eye(256))
+        blk = (sl2, slice(p0, p0 + length))
+        want, bound = Tinv @ A[blk], np.abs(Tinv) @ np.abs(A[blk])
+    else:
+        Tinv = np.linalg.inv(np.triu(T))
+        blk = (slice(p0, p0 + length), sl2)
+        want, bound = A[blk] @ Tinv, np.abs(A[blk]) @ np.abs(Tinv)
+    got = got_all[blk]
+    assert np.all(np.abs(got - want) <= 2.0 ** -8 * bound + 1e-30), np.max(np.abs(got - want) / bound)
+    outside = np.ones((n, n), dtype=bool)
+    outside[blk] = False
+    assert np.array_equal(got_all[outside], A[outside])
+    mir = mirror.float().cpu().numpy()
+    mir_blk = mir[:, :n].T[blk] if left else mir[:, :n][blk]
+    want_mir = torch.from_numpy(got.astype(np.float32)).bfloat16().float().numpy()
+    assert np.array_equal(mir_blk, want_mir)
+    assert np.all((mir[:, :n].T if left else mir[:, :n])[outside] == 3.0)
+
+
 @pytest.mark.parametrize("m,nc", [(128, 300), (300, 100), (50, 384), (128, 128), (384, 7), (256, 384), (384, 200)])
 def test_panel_update_tc(m, nc):
     """The LU's K = 128 update on the tensor cores (TF32 operands, FP32 accumulation): C -= A B with
@@ -183,7 +241,8 @@ def test_mixed_solve_vs_oracle(case):
         bh.set_precision(-1)
     print(f"\n{case}: {t} | {' / '.join(l for l in logs if 'solve' in l or 'build' in l)}")
     assert not any("instead" in l for l in logs), logs
-    assert 0 < t["refine_iters"] <= 40 and t["relres"] <= 1e-12
+    # a few GMRES iterations (3-5 at these sizes): a factor gone wrong would still converge, slowly
+    assert 0 < t["refine_iters"] <= 12 and t["relres"] <= 1e-12, t
     o = ob.best_run(tri, ta, tv, iarea=iarea, ivisco=1)
     compare(g, o)
 
@@ -204,7 +263,8 @@ def test_mixed_operand_copies_in_blocks(monkeypatch):
     finally:
         bh.set_precision(-1)
     assert not any("instead" in l for l in logs), logs
-    assert 0 < t["refine_iters"] <= 40 and t["relres"] <= 1e-12
+    # a few GMRES iterations (3-5 at these sizes): a factor gone wrong would still converge, slowly
+    assert 0 < t["refine_iters"] <= 12 and t["relres"] <= 1e-12, t
     compare(g, ob.best_run(tri, ta, tv, iarea=1, ivisco=1))
 
 
