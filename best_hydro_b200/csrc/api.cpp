@@ -31,6 +31,21 @@
 #include "mixed.h"
 
 namespace bgpu {
+
+bool mesh_fast_ok(const double* v, long count, long stride_point, long stride_axis) {
+  double side = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    double lo = INFINITY, hi = -INFINITY;
+    for (long p = 0; p < count; ++p) {
+      const double x = v[a * stride_axis + p * stride_point];
+      lo = std::min(lo, x);
+      hi = std::max(hi, x);
+    }
+    side = std::max(side, hi - lo);
+  }
+  return std::isfinite(side) && side >= 1e-20 && side <= 1e20;
+}
+
 namespace {
 
 // Messages for the caller's log (BEST appends them to its .log, best/besolve.f90:281-292): the
@@ -212,11 +227,13 @@ struct Solver {
   std::unique_ptr<MixedSolver> mixed;
   int precision = BGPU_FP64;
   bool factored = false;
+  bool fast_ok = true;  // mesh_fast_ok of the mesh
   DevMesh mesh() const {
     DevMesh m;
     m.n = n;
     m.cg = cg;
     m.afac = afac;
+    m.fast_ok = fast_ok;
     m.geo = geo.as<double>();
     m.xc = xc.as<double>();
     m.self9 = self9.as<double>();
@@ -349,11 +366,13 @@ struct Series {
     for (cudaStream_t q : streams) cudaStreamDestroy(q);
     for (cudaEvent_t e : ev_done) cudaEventDestroy(e);
   }
+  std::vector<char> fast_ok;  // mesh_fast_ok of each mesh
   DevMesh mesh(int i) const {
     DevMesh m;
     m.n = n[i];
     m.cg = cg;
     m.afac = afac[i];
+    m.fast_ok = fast_ok[i] != 0;
     m.geo = geo.as<double>() + (size_t)t0[i] * kGeoStride;
     m.xc = xc.as<double>() + (size_t)t0[i] * kXcStride;
     m.self9 = self9.as<double>() + (size_t)t0[i] * 9;
@@ -522,6 +541,7 @@ int bhm_create(int n, const double* v1, const double* v2, const double* v3, cons
     s->afac = afac;
     s->cg = cg;
     std::vector<double> h = geo_host(n, v1, v2, v3, area);
+    s->fast_ok = mesh_fast_ok(v1, n, 1, n) && mesh_fast_ok(v2, n, 1, n) && mesh_fast_ok(v3, n, 1, n);
     s->v_host[0].assign(v1, v1 + 3 * (size_t)n);
     s->v_host[1].assign(v2, v2 + 3 * (size_t)n);
     s->v_host[2].assign(v3, v3 + 3 * (size_t)n);
@@ -563,6 +583,7 @@ int bgpu_create_from_triangles(int n, const double* tri, int iarea, double truea
     s->n = n;
     s->cg = cg;
     s->prepared = true;
+    s->fast_ok = mesh_fast_ok(tri, 3 * (long)n, 3, 1);
     s->tri.ensure((size_t)9 * n * sizeof(double), "triangles");
     s->geo.ensure((size_t)n * kGeoStride * sizeof(double), "mesh");
     s->vset.ensure((size_t)9 * n * sizeof(double), "centred corners");
@@ -841,6 +862,8 @@ int bgpu_series_create(int count, const int* n, const double* v1, const double* 
       const long o = S->t0[i];
       std::vector<double> g = geo_host(n[i], v1 + 3 * o, v2 + 3 * o, v3 + 3 * o, area + o);
       h.insert(h.end(), g.begin(), g.end());
+      S->fast_ok.push_back(mesh_fast_ok(v1 + 3 * o, n[i], 1, n[i]) && mesh_fast_ok(v2 + 3 * o, n[i], 1, n[i]) &&
+                           mesh_fast_ok(v3 + 3 * o, n[i], 1, n[i]));
     }
     S->geo.ensure(h.size() * sizeof(double), "series meshes");
     S->xc.ensure((size_t)tot * kXcStride * sizeof(double), "series incenters");

@@ -27,6 +27,7 @@ __global__ void __launch_bounds__(kTgtTile, BGPU_ASM_FAST_MIN_BLOCKS)
 cudaError_t launch_assemble_fast(const DevMesh& m, int r0, int r1, int c0, int c1, double* out, long ld,
                                  const DevDeflation& defl, float* out32, long ld32, cudaStream_t s) {
   if (r1 <= r0 || c1 <= c0) return cudaSuccess;
+  if (!m.fast_ok) return launch_assemble(m, r0, r1, c0, c1, out, ld, defl, out32, ld32, s);
   dim3 grid((r1 - r0 + kTgtTile - 1) / kTgtTile, (c1 - c0 + kSrcTile - 1) / kSrcTile);
   if (grid.y > 65535u) {
     // more source tiles than one grid dimension holds: split along the sources

@@ -198,7 +198,9 @@ __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __re
           const double r1 = rsqrt(a1), r2 = rsqrt(a2);
           const double q1 = a1 * r1, q2 = a2 * r2;
           // the three quotients (log argument, hy/hxy, hx) from one reciprocal of the product of
-          // their denominators
+          // their denominators (that product scales as the 10th power of the mesh's size: meshes
+          // whose extent lies outside [1e-20, 1e20] are assembled by the exact kernel instead,
+          // DevMesh::fast_ok)
           const double den = d211c + d2131 * y + s21 * q1;
           const double dy = cy0 + y * (cy1 + y * cy2), dx = cx0 + y * (cx1 - y * cy2);
           const double dyx = dy * dx;

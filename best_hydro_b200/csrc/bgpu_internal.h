@@ -63,7 +63,14 @@ struct DevMesh {
   const double* geo = nullptr;  // n * kGeoStride
   double* xc = nullptr;         // n * kXcStride (written by the self-block kernel)
   double* self9 = nullptr;      // n * 9, self block of triangle t: self9[9t + 3a + b]
+  // the mesh's extent lies in [1e-20, 1e20] (mesh_fast_ok): the mixed path's assembly may form one
+  // reciprocal of three denominators' product (10th power of the size); otherwise it runs the exact
+  // kernel
+  bool fast_ok = true;
 };
+// true when the bounding box of the points (count coordinates, point p's axis a at
+// p[a * stride_axis + p * stride_point]) has its largest side in [1e-20, 1e20]
+bool mesh_fast_ok(const double* v, long count, long stride_point, long stride_axis);
 
 // The normal-field deflation applied in the assembly epilogue (best/best.f:406-425):
 // GR(I,J) += (gdef[comp[J/3]-1] * xmu[J]) * xmu[I] when comp[I/3] == comp[J/3].

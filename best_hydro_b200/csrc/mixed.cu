@@ -131,22 +131,30 @@ __device__ __forceinline__ void small_mm(const float* A, const float* B, float* 
   for (int i = 0; i < TR; ++i)
 #pragma unroll
     for (int j = 0; j < TC; ++j) acc[i][j] = 0.f;
-#pragma unroll 8
-  for (int k = 0; k < H; ++k) {
-    float a[TR], b[TC];
-    if constexpr (TR == 4) {
-      const float4 v = *reinterpret_cast<const float4*>(A + k * kS + r0);
-      a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
-    } else {
+  // four k at a time: B's columns are contiguous in k (16-byte loads), A's in the row index
+#pragma unroll 2
+  for (int k = 0; k < H; k += 4) {
+    float b[TC][4];
 #pragma unroll
-      for (int i = 0; i < TR; ++i) a[i] = A[k * kS + r0 + i];
+    for (int j = 0; j < TC; ++j) {
+      const float4 v = *reinterpret_cast<const float4*>(B + (c0 + j) * kS + k);
+      b[j][0] = v.x, b[j][1] = v.y, b[j][2] = v.z, b[j][3] = v.w;
     }
 #pragma unroll
-    for (int j = 0; j < TC; ++j) b[j] = B[(c0 + j) * kS + k];
+    for (int kk = 0; kk < 4; ++kk) {
+      float a[TR];
+      if constexpr (TR == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(A + (k + kk) * kS + r0);
+        a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
+      } else {
 #pragma unroll
-    for (int i = 0; i < TR; ++i)
+        for (int i = 0; i < TR; ++i) a[i] = A[(k + kk) * kS + r0 + i];
+      }
 #pragma unroll
-      for (int j = 0; j < TC; ++j) acc[i][j] += a[i] * b[j];
+      for (int i = 0; i < TR; ++i)
+#pragma unroll
+        for (int j = 0; j < TC; ++j) acc[i][j] += a[i] * b[j][kk];
+    }
   }
   if (bar >= 0) group_bar(bar, NT);
 #pragma unroll
@@ -383,10 +391,38 @@ __global__ void __launch_bounds__(256) k_combine256(const float* __restrict__ LU
   const float* X2 = (lower ? DL : DU) + (size_t)(b + 1) * 16384;  // D2 or E2
   const float* off = lower ? LU + (size_t)k0 * lda + k0 + 128 : LU + (size_t)(k0 + 128) * lda + k0;  // L21 or U12
   float* T = (lower ? TL : TU) + (size_t)b * 65536;
+  // a 128 x 128 column-major block (leading dimension ld, 16-byte aligned columns) into sA: sixteen
+  // 16-byte loads in flight per thread
+  auto stage = [&](const float* src, long ld) {
+    float4 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e4 = tid + 256 * q, col = e4 >> 5, row = (e4 & 31) * 4;
+      v[q] = __ldg(reinterpret_cast<const float4*>(src + (size_t)col * ld + row));
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e4 = tid + 256 * q, col = e4 >> 5, row = (e4 & 31) * 4;
+      float* d = sA + col * 129 + row;
+      d[0] = v[q].x, d[1] = v[q].y, d[2] = v[q].z, d[3] = v[q].w;
+    }
+  };
   // product 1: lower L21 D1[:, slab], upper U12 E2[:, slab]
-  for (int e = tid; e < 128 * 128; e += 256) sA[(e >> 7) * 129 + (e & 127)] = off[(size_t)(e >> 7) * lda + (e & 127)];
+  stage(off, lda);
   const float* s1 = lower ? X1 : X2;
-  for (int e = tid; e < 128 * 16; e += 256) sB[(e & 127) * 16 + (e >> 7)] = s1[(size_t)(c0 + (e >> 7)) * 128 + (e & 127)];
+  {
+    float b8[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      b8[q] = __ldg(s1 + (size_t)(c0 + (e >> 7)) * 128 + (e & 127));
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      sB[(e & 127) * 16 + (e >> 7)] = b8[q];
+    }
+  }
   __syncthreads();
   float acc[8];
 #pragma unroll
@@ -400,8 +436,7 @@ __global__ void __launch_bounds__(256) k_combine256(const float* __restrict__ LU
   for (int c = 0; c < 8; ++c) sT[r * 16 + ch + c] = acc[c];
   __syncthreads();
   // product 2: lower -D2 T, upper -E1 T
-  const float* s2 = lower ? X2 : X1;
-  for (int e = tid; e < 128 * 128; e += 256) sA[(e >> 7) * 129 + (e & 127)] = s2[e];
+  stage(lower ? X2 : X1, 128);
   __syncthreads();
 #pragma unroll
   for (int c = 0; c < 8; ++c) acc[c] = 0.f;
@@ -410,23 +445,24 @@ __global__ void __launch_bounds__(256) k_combine256(const float* __restrict__ LU
 #pragma unroll
     for (int c = 0; c < 8; ++c) acc[c] += a * sT[k * 16 + ch + c];
   }
-  // columns c0 + c of the left half and 128 + c0 + c of the right half, all 256 rows
+  // columns c0 + c of the left half and 128 + c0 + c of the right half, all 256 rows (the copies of
+  // D1, D2 / E1, E2 loaded before any store)
+  float x1[8], x2[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int j = c0 + ch + c;
+    x1[c] = __ldg(X1 + (size_t)j * 128 + r);
+    x2[c] = __ldg(X2 + (size_t)j * 128 + r);
+  }
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     const int j = c0 + ch + c;
     float* left = T + (size_t)j * 256;
     float* right = T + (size_t)(128 + j) * 256;
-    if (lower) {
-      left[r] = X1[(size_t)j * 128 + r];
-      left[128 + r] = -acc[c];
-      right[r] = 0.f;
-      right[128 + r] = X2[(size_t)j * 128 + r];
-    } else {
-      left[r] = X1[(size_t)j * 128 + r];
-      left[128 + r] = 0.f;
-      right[r] = -acc[c];
-      right[128 + r] = X2[(size_t)j * 128 + r];
-    }
+    left[r] = x1[c];
+    left[128 + r] = lower ? -acc[c] : 0.f;
+    right[r] = lower ? 0.f : -acc[c];
+    right[128 + r] = x2[c];
   }
   stamp_end(stamp);
 }

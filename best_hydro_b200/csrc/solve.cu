@@ -9,6 +9,7 @@
 // a readiness flag (release/acquire, with a bounded wait).  A block taken from the ticket counter
 // only ever waits on blocks taken before it by CTAs that are already running, so the scheme cannot
 // deadlock however many CTAs are resident.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -136,6 +137,8 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// all but the most recent group of asynchronous copies complete
+__device__ __forceinline__ void cp_async_wait_but_last() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // Warp 0 waits until flags[jb] == epoch, then counts how many more flags in the direction `step`
 // (+1 or -1) are ready too, up to 32 and within [lo, hi).  Returns that count (>= 1), or 0 when the
@@ -431,13 +434,15 @@ constexpr int kLead = 2;
 
 // V is the type of the right-hand sides and of every sum (double; float for the FP32 preconditioner).
 // CHAIN (the FP32 preconditioner): the chain of block rows is taken off the task list.  A final
-// task of row i then stops short of block i-1: it forms c_i = D_i^-1 (b_i - sum_{j <= i-2} L_ij x_j)
+// task of row i then stops short of block i-2: it forms c_i = D_i^-1 (b_i - sum_{j <= i-3} L_ij x_j)
 // into a slot of its own and releases cflags[i]; CTA 0 runs the chain alone,
-//     x_i = c_i - W_i x_{i-1},   W_i = D_i^-1 L_{i,i-1}   (chain_weights32, once per factorisation),
-// keeping x_{i-1} in shared memory and W_i (prefetched a step ahead) in registers, and releases
-// flags[i] for the tasks that need x_i.  The chain's step is one 128 x 128 product instead of a
-// handoff through global memory, two products and a wait on the previous block row.  All CTAs of the
-// grid are resident (the grid is sized by occupancy), so CTA 0 always runs.
+//     x_i = c_i - W_i x_{i-1} - V_i x_{i-2},   W_i = D_i^-1 L_{i,i-1},  V_i = D_i^-1 L_{i,i-2}
+// (chain_weights32, once per factorisation; V in FP16 scaled by its largest entry), keeping x_{i-1}
+// in shared memory and W_i (prefetched a step ahead) in registers, forming V_{i+1} x_{i-1} at the
+// start of step i (before its wait), and releases flags[i] for the tasks that need x_i.  A row's
+// hand-off through global memory (final task, c_i, chain) thus has three chain steps to arrive in
+// instead of two.  All CTAs of the grid are resident (the grid is sized by occupancy), so CTA 0
+// always runs.
 template <typename F, typename FI, bool LOWER, bool TRANS = false, typename V = double, bool CHAIN = false>
 __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
                                                   V* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
@@ -457,9 +462,15 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     if (blockIdx.x == 0) {
       // s_y holds x_{i-1}; wv this thread's 64 entries of W_i (row `row`, columns 64 half .. +63);
       // W_{i+1} arrives in shared memory (asynchronous 16-byte copies of the column-major tile)
-      // while step i runs, and moves to registers once x_i is published
+      // while step i runs, and moves to registers once x_i is published.  The lag-2 term
+      // V_{i+1} x_{i-1} is formed at the start of step i, before the wait for c_i, from V_{i+1} in
+      // shared memory (FP16, scaled; fetched during step i-1): pc holds this thread's half of it
+      // for the next step.
       FI wv[64];
       FI* s_w = s_di;  // 128 x 128, column-major, unpadded (fits the final tasks' 128 x 129 buffer)
+      __half* s_v = reinterpret_cast<__half*>(s_dyn + (size_t)kIb * (kIb + 1) * sizeof(FI));  // 128 x 128 FP16
+      const __half* V16 = reinterpret_cast<const __half*>(W + (size_t)nblk * kIb * kIb);
+      const FI* vscale = W + (size_t)nblk * kIb * kIb + (size_t)nblk * kIb * kIb / 2;
       auto fetch_w = [&](int ii) {
         if (ii >= 1 && ii < nblk) {
           const int b = LOWER ? ii : nblk - 1 - ii;
@@ -468,10 +479,42 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
         }
         cp_async_commit();
       };
+      auto fetch_v = [&](int ii) {
+        if (ii >= 2 && ii < nblk) {
+          const int b = LOWER ? ii : nblk - 1 - ii;
+          const __half* src = V16 + (size_t)b * kIb * kIb;
+          for (int e = tid; e < kIb * kIb * 2 / 16; e += 256) cp_async16(s_v + e * 8, src + e * 8);
+        }
+        cp_async_commit();
+      };
       fetch_w(1);
+      fetch_v(2);
+      V pc[kIrhs];  // (this thread's half of) V_i x_{i-2}, scaled
+#pragma unroll
+      for (int r = 0; r < kIrhs; ++r) pc[r] = (V)0;
       for (int i = 0; i < nblk; ++i) {
         const int blk = LOWER ? i : nblk - 1 - i;
         const int r0 = blk * kIb, nr = min(kIb, n - r0);
+        // the lag-2 term of the next row, V_{i+1} x_{i-1}, while c_i may still be on its way
+        V pn[kIrhs];
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) pn[r] = (V)0;
+        if (i >= 1 && i + 1 < nblk) {
+          cp_async_wait_but_last();  // V_{i+1} (W_{i+1}, fetched last, may still be in flight)
+          __syncthreads();
+          const int bn = LOWER ? i + 1 : nblk - 2 - i;
+          const V sc = (V)vscale[bn];
+#pragma unroll 8
+          for (int kk = 0; kk < 64; ++kk) {
+            const V v = (V)__half2float(s_v[(half * 64 + kk) * kIb + row]);
+#pragma unroll
+            for (int r = 0; r < kIrhs; ++r) pn[r] += v * s_y[half * 64 + kk][r];
+          }
+#pragma unroll
+          for (int r = 0; r < kIrhs; ++r) pn[r] *= sc;
+          __syncthreads();  // s_v read: refill it
+          fetch_v(i + 2);
+        }
         if (tid == 0) {
           unsigned spins = 0;
           int ok = 1;
@@ -498,7 +541,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
         }
         V acc[kIrhs];
 #pragma unroll
-        for (int r = 0; r < kIrhs; ++r) acc[r] = (V)0;
+        for (int r = 0; r < kIrhs; ++r) acc[r] = pc[r];
         if (i >= 1) {
 #pragma unroll
           for (int kk = 0; kk < 64; ++kk) {
@@ -523,8 +566,10 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
           __threadfence();
           st_release_u32(flags + blk, epoch);
         }
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) pc[r] = pn[r];
         if (i + 1 < nblk) {
-          cp_async_wait_all();
+          cp_async_wait_but_last();  // W_{i+1} (V_{i+2}, fetched last, may still be in flight)
           __syncthreads();
 #pragma unroll
           for (int kk = 0; kk < 64; ++kk) wv[kk] = s_w[(half * 64 + kk) * kIb + row];
@@ -691,21 +736,34 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
   }
 }
 
-// W_b = D_b^-1 L_{b,b-1} (LOWER, b >= 1) or D_b^-1 U_{b,b+1} (upper, b <= nblk - 2), 128 x 128
-// column-major per block row, rows and columns beyond n zero: the chain weights of the FP32
-// preconditioner (see k_trsv_inv, CHAIN).  One CTA per block row and triangle (blockIdx.y).
+// The chain weights of the FP32 preconditioner (see k_trsv_inv, CHAIN), one triangle per blockIdx.y,
+// one block row b per blockIdx.x, one lag per blockIdx.z:
+//   lag 1: W_b = D_b^-1 L_{b,b-1} (lower) or D_b^-1 U_{b,b+1} (upper), FP32, 128 x 128 column-major
+//          at out + b * 16384;
+//   lag 2: V_b = D_b^-1 L_{b,b-2} or D_b^-1 U_{b,b+2}, stored as FP16 scaled by its largest magnitude
+//          (the scale at out + nblk * 24576 + b, the halves from out + nblk * 16384)
+// rows and columns beyond n zero; a missing neighbour gives zeros (scale 1).
 __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict__ LU, long lda, int n,
                                                           const float* __restrict__ DL, const float* __restrict__ DU,
                                                           float* __restrict__ WL, float* __restrict__ WU) {
   extern __shared__ __align__(16) float s_w[];
   float* sd = s_w;                  // D^-1 (r, k) at sd[k * 129 + r]
   float* sb = s_w + kIb * (kIb + 1);  // the off-diagonal block (k, c) at sb[c * 129 + k]
-  const int nblk = (n + kIb - 1) / kIb, b = blockIdx.x, lower = blockIdx.y == 0;
-  const int nb = lower ? b - 1 : b + 1;  // the neighbouring block column
-  float* out = (lower ? WL : WU) + (size_t)b * kIb * kIb;
+  __shared__ float s_max[8];
+  const int nblk = (n + kIb - 1) / kIb, b = blockIdx.x, lower = blockIdx.y == 0, lag = 1 + blockIdx.z;
+  const int nb = lower ? b - lag : b + lag;  // the neighbouring block column
+  float* base = lower ? WL : WU;
+  float* out = base + (size_t)b * kIb * kIb;
+  __half* out16 = reinterpret_cast<__half*>(base + (size_t)nblk * kIb * kIb) + (size_t)b * kIb * kIb;
+  float* scale = base + (size_t)nblk * kIb * kIb + (size_t)nblk * kIb * kIb / 2 + b;
   const int tid = threadIdx.x;
   if (nb < 0 || nb >= nblk) {
-    for (int e = tid; e < kIb * kIb; e += 256) out[e] = 0.f;
+    if (lag == 1)
+      for (int e = tid; e < kIb * kIb; e += 256) out[e] = 0.f;
+    else {
+      for (int e = tid; e < kIb * kIb; e += 256) out16[e] = __float2half_rn(0.f);
+      if (tid == 0) *scale = 1.f;
+    }
     return;
   }
   const float* D = (lower ? DL : DU) + (size_t)b * kIb * kIb;
@@ -734,10 +792,34 @@ __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * bv[j];
   }
+  if (lag == 1) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int i = 0; i < 8; ++i) out[(size_t)(cb + j) * kIb + rb + i] = (rb + i < nr) ? acc[i][j] : 0.f;
+    return;
+  }
+  float m = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (rb + i < nr) m = fmaxf(m, fabsf(acc[i][j]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((tid & 31) == 0) s_max[tid >> 5] = m;
+  __syncthreads();
+  float sc = 0.f;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) sc = fmaxf(sc, s_max[w]);
+  sc = sc > 0.f ? sc : 1.f;
+  const float inv = 1.f / sc;
 #pragma unroll
   for (int j = 0; j < 8; ++j)
 #pragma unroll
-    for (int i = 0; i < 8; ++i) out[(size_t)(cb + j) * kIb + rb + i] = (rb + i < nr) ? acc[i][j] : 0.f;
+    for (int i = 0; i < 8; ++i)
+      out16[(size_t)(cb + j) * kIb + rb + i] = __float2half_rn((rb + i < nr) ? acc[i][j] * inv : 0.f);
+  if (tid == 0) *scale = sc;
 }
 
 // Scratch of the split solves, after the base scratch: per-row partial-task counters, the partial
@@ -756,15 +838,16 @@ struct SplitScratch {
 };
 
 // The task list of a triangle with nblk block rows (see k_trsv_inv), built once per size.  chain:
-// the final task of row b stops before block b-1 (the chain's).
+// the final task of row b does block b-3 only (b-2 and b-1 are the chain's).
 const std::vector<int4>& split_tasks(int nblk, bool chain = false) {
   static std::map<int, std::vector<int4>> cache[2];
   auto it = cache[chain].find(nblk);
   if (it != cache[chain].end()) return it->second;
   std::vector<std::vector<int4>> after(nblk);  // partial tasks issued after F(b)
   std::vector<int> nparts(nblk, 0);
+  const int lead = chain ? kLead + 1 : kLead;  // blocks [i - lead, i - (chain ? 2 : 0)) in the final task
   for (int i = 0; i < nblk; ++i) {
-    int e = i - kLead, w = 2, sidx = 0;
+    int e = i - lead, w = 2, sidx = 0;
     while (e > 0) {
       const int lo = std::max(0, e - w);
       after[e - 1].push_back(make_int4(sidx, i, lo, e));
@@ -776,7 +859,7 @@ const std::vector<int4>& split_tasks(int nblk, bool chain = false) {
   }
   std::vector<int4> list;
   for (int b = 0; b < nblk; ++b) {
-    list.push_back(make_int4(-1 - nparts[b], b, std::max(0, b - kLead), chain ? std::max(0, b - 1) : b));
+    list.push_back(make_int4(-1 - nparts[b], b, std::max(0, b - lead), chain ? std::max(0, b - 2) : b));
     for (const int4& t : after[b]) list.push_back(t);
   }
   return cache[chain].emplace(nblk, std::move(list)).first->second;
@@ -805,7 +888,9 @@ cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const flo
   if ((e = cudaMemsetAsync(cnt, 0, (size_t)SplitScratch::nblk(n) * 4, s)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(tasks, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return e;
-  const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(float);
+  // the final tasks' inverted diagonal block (128 x 129 FP32, the chain's W prefetch), then the
+  // chain's V prefetch (128 x 128 FP16)
+  const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(float) + (size_t)kIb * kIb * 2;
   auto kern = k_trsv_inv<float, float, LOWER, false, float, true>;
   static bool attr = false;
   static int per_sm = 0;
@@ -998,7 +1083,10 @@ cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const floa
 
 cudaError_t set_wait_limit(unsigned spins) { return cudaMemcpyToSymbol(c_spin_limit, &spins, sizeof spins); }
 
-size_t chain_weights_elems(int n) { return (size_t)((n + kIb - 1) / kIb) * kIb * kIb; }
+size_t chain_weights_elems(int n) {
+  const size_t nblk = (size_t)((n + kIb - 1) / kIb);
+  return nblk * kIb * kIb + nblk * kIb * kIb / 2 + nblk;  // W (FP32), V (FP16), V's scales
+}
 
 cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const float* DU, int n, float* WL, float* WU,
                             cudaStream_t s) {
@@ -1010,7 +1098,7 @@ cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const fl
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_chain_weights32<<<dim3((n + kIb - 1) / kIb, 2), 256, smem, s>>>(LU, lda, n, DL, DU, WL, WU);
+  k_chain_weights32<<<dim3((n + kIb - 1) / kIb, 2, 2), 256, smem, s>>>(LU, lda, n, DL, DU, WL, WU);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }

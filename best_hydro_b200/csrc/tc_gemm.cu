@@ -410,11 +410,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 // four transposer warps rewrite each chunk K-major (128 rows of 128 bytes, 128-byte swizzle) before
 // the MMA warp uses it.  Shared memory: R (4 chunks of 16 KB), a raw ring (4 x 16 KB, TMA) and an
 // operand ring (4 x 16 KB); two TMEM accumulators of 128 x 128 FP32.
-constexpr int kPtStages = 2;
+constexpr int kPtStages = 4;
 constexpr uint32_t kPtChunk = 128 * 32 * 4;  // 16 KB
 // R (64 KB), raw and operand rings, the output tile (64 KB: four 32 x 128 FP32 boxes) and its BF16
 // mirror (32 KB: two 64 x 128 boxes), barriers
-constexpr uint32_t kPtOutOff = 4 * kPtChunk + 2 * kPtStages * kPtChunk;
+constexpr uint32_t kPtOutOff = 4 * kPtChunk + kPtStages * kPtChunk;
 constexpr uint32_t kPtMirOff = kPtOutOff + 4 * kPtChunk;
 constexpr uint32_t kPtBarOff = kPtMirOff + 2 * kPtChunk;
 constexpr uint32_t kPtSmem = kPtBarOff + 256 + 1024;
@@ -454,6 +454,40 @@ __device__ __forceinline__ void transpose_chunk(const uint8_t* src, uint8_t* dst
   }
 }
 
+// transpose_chunk in place: the four transposer warps read all their values, meet at a named
+// barrier (id 2) that also ANDs their `ok` (the outcome of each thread's wait for the boxes), then --
+// if all were ok -- write (the written places are a permutation of the read ones).  Returns the AND,
+// alike in all 128 threads, so they leave a loop together.
+__device__ __forceinline__ bool transpose_chunk_inplace(uint8_t* buf, int t, bool ok) {
+  const int lane = t & 31, w = t >> 5;
+  float v[8][4];
+  if (ok) {
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+      const int mn = lane + 32 * (it & 3), kg = w + 4 * (it >> 2);
+      const uint8_t* sb = buf + (mn >> 5) * 4096 + (mn & 3) * 4;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int k = 4 * kg + e;
+        v[it][e] = *reinterpret_cast<const float*>(sb + k * 128 + ((((mn & 31) >> 2) ^ (k & 7)) << 4));
+      }
+    }
+  }
+  unsigned all;
+  asm volatile(
+      "{\n .reg .pred pi, po;\n setp.ne.u32 pi, %1, 0;\n bar.red.and.pred po, 2, %2, pi;\n selp.u32 %0, 1, 0, po;\n}\n"
+      : "=r"(all)
+      : "r"((unsigned)ok), "r"(32 * kPtTrWarps)
+      : "memory");
+  if (!all) return false;
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int mn = lane + 32 * (it & 3), kg = w + 4 * (it >> 2);
+    *reinterpret_cast<float4*>(buf + mn * 128 + ((kg ^ (mn & 7)) << 4)) = make_float4(v[it][0], v[it][1], v[it][2], v[it][3]);
+  }
+  return true;
+}
+
 // tmR, tmP: R's and P's tensor maps (K-major sources: 32 x 128 boxes, one per K chunk; MN-major
 // sources: 32 x 32 boxes).  R starts at (rx0, ry0) of its map, P at (px0, py0): left, R's box
 // (rx0 + 32 c, ry0 + 32 kc) and P's (px0 + 32 kc, py0 + 128 tile); right, R's (rx0 + 32 kc, ry0)
@@ -484,13 +518,12 @@ __global__ void __launch_bounds__(kPtThreads, 1)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sR = smem;                               // R, K-major: 4 chunks
-  uint8_t* sRaw = smem + 4 * kPtChunk;              // TMA ring of P's MN-major boxes (right)
-  uint8_t* sOp = sRaw + kPtStages * kPtChunk;       // P's K-major chunks
+  uint8_t* sOp = smem + 4 * kPtChunk;  // P's K-major chunks (right: the MN-major boxes land there and
+                                       // are transposed in place)
   uint8_t* sOut = smem + kPtOutOff;                 // the output tile (left: R's boxes first)
   uint8_t* sMir = smem + kPtMirOff;                 // its BF16 mirror
   uint64_t* raw_full = reinterpret_cast<uint64_t*>(smem + kPtBarOff);
-  uint64_t* raw_empty = raw_full + kPtStages;
-  uint64_t* op_full = raw_empty + kPtStages;
+  uint64_t* op_full = raw_full + kPtStages;
   uint64_t* op_empty = op_full + kPtStages;
   uint64_t* acc_full = op_empty + kPtStages;  // [2]
   uint64_t* acc_empty = acc_full + 2;         // [2]
@@ -509,7 +542,6 @@ __global__ void __launch_bounds__(kPtThreads, 1)
     s_abort = 0;
     for (int s = 0; s < kPtStages; ++s) {
       mbar_init(&raw_full[s], 1);
-      mbar_init(&raw_empty[s], kPtTrWarps);
       mbar_init(&op_full[s], LEFT ? 1 : kPtTrWarps);
       mbar_init(&op_empty[s], 1);
     }
@@ -550,8 +582,7 @@ __global__ void __launch_bounds__(kPtThreads, 1)
       for (int tile = blockIdx.x; tile < ntiles && !*(volatile int*)&s_abort; tile += gridDim.x) {
         for (int kc = 0; kc < 4; ++kc, ++it) {
           const uint32_t s = it % kPtStages;
-          uint64_t* freed = LEFT ? &op_empty[s] : &raw_empty[s];
-          if (it >= kPtStages && !mbar_wait(freed, ((it / kPtStages) & 1) ^ 1, status)) {
+          if (it >= kPtStages && !mbar_wait(&op_empty[s], ((it / kPtStages) & 1) ^ 1, status)) {
             s_abort = 1;
             break;
           }
@@ -562,7 +593,7 @@ __global__ void __launch_bounds__(kPtThreads, 1)
           } else {
             mbar_expect_tx(&raw_full[s], kPtChunk);
             for (int c = 0; c < 4; ++c)
-              tma_load_2d(sRaw + s * kPtChunk + c * 4096, &tmP, px0 + 128 * tile + 32 * c, py0 + 32 * kc, &raw_full[s]);
+              tma_load_2d(sOp + s * kPtChunk + c * 4096, &tmP, px0 + 128 * tile + 32 * c, py0 + 32 * kc, &raw_full[s]);
           }
         }
       }
@@ -619,20 +650,16 @@ __global__ void __launch_bounds__(kPtThreads, 1)
         bool ok = true;
         for (int kc = 0; kc < 4; ++kc, ++it) {
           const uint32_t s = it % kPtStages;
-          if (!mbar_wait(&raw_full[s], (it / kPtStages) & 1, status) ||
-              (it >= kPtStages && !mbar_wait(&op_empty[s], ((it / kPtStages) & 1) ^ 1, status)) ||
-              *(volatile int*)&s_abort) {
+          // (the transposition's barrier makes the four warps agree on the waits' outcome)
+          if (!transpose_chunk_inplace(sOp + s * kPtChunk, t,
+                                       mbar_wait(&raw_full[s], (it / kPtStages) & 1, status) && !s_abort)) {
             s_abort = 1;
             ok = false;
             break;
           }
-          transpose_chunk(sRaw + s * kPtChunk, sOp + s * kPtChunk, t);
-          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+          fence_async_smem();
           __syncwarp();
-          if (lane == 0) {
-            mbar_arrive(&raw_empty[s]);
-            mbar_arrive(&op_full[s]);
-          }
+          if (lane == 0) mbar_arrive(&op_full[s]);
         }
         if (!ok) break;
       }
@@ -820,8 +847,9 @@ __global__ void __launch_bounds__(kPtThreads, 1)
 // rewrite K-major ("trans": Tinv on the left, P on the right), the MMA's A operand always the trans
 // slot and B the direct one.  The epilogue stages each whole 128 x 128 half through shared memory
 // for TMA stores, with the BF16 mirror; ragged halves and tiles by plain stores.
-constexpr int kL2Stages = 2;
-constexpr uint32_t kL2Stage = 3 * kPtChunk;  // direct, trans, raw
+constexpr int kL2Stages = 4;
+constexpr uint32_t kL2Stage = 2 * kPtChunk;  // direct, trans (the MN-major boxes land there and are
+                                             // transposed in place)
 constexpr uint32_t kL2OutOff = kL2Stages * kL2Stage;
 constexpr uint32_t kL2MirOff = kL2OutOff + 4 * kPtChunk;
 constexpr uint32_t kL2BarOff = kL2MirOff + 2 * kPtChunk;
@@ -851,10 +879,9 @@ __global__ void __launch_bounds__(kPtThreads, 1)
   uint8_t* sOut = smem + kL2OutOff;
   uint8_t* sMir = smem + kL2MirOff;
   uint64_t* dir_full = reinterpret_cast<uint64_t*>(smem + kL2BarOff);
-  uint64_t* raw_full = dir_full + kL2Stages;
-  uint64_t* raw_empty = raw_full + kL2Stages;
-  uint64_t* tr_full = raw_empty + kL2Stages;
-  uint64_t* st_empty = tr_full + kL2Stages;  // the MMA has read the stage's direct and trans slots
+  uint64_t* raw_full = dir_full + kL2Stages;  // the MN-major boxes landed in the trans slot
+  uint64_t* tr_full = raw_full + kL2Stages;   // ... and are transposed
+  uint64_t* st_empty = tr_full + kL2Stages;   // the MMA has read the stage's direct and trans slots
   uint64_t* acc_full = st_empty + kL2Stages;  // [2]
   uint64_t* acc_empty = acc_full + 2;         // [2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
@@ -862,7 +889,6 @@ __global__ void __launch_bounds__(kPtThreads, 1)
   volatile int& s_abort = s_flags[0];
   auto dir = [&](uint32_t s) { return smem + s * kL2Stage; };
   auto trs = [&](uint32_t s) { return smem + s * kL2Stage + kPtChunk; };
-  auto raw = [&](uint32_t s) { return smem + s * kL2Stage + 2 * kPtChunk; };
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles = (len + 127) / 128;
@@ -873,7 +899,6 @@ __global__ void __launch_bounds__(kPtThreads, 1)
     for (int s = 0; s < kL2Stages; ++s) {
       mbar_init(&dir_full[s], 1);
       mbar_init(&raw_full[s], 1);
-      mbar_init(&raw_empty[s], kPtTrWarps);
       mbar_init(&tr_full[s], kPtTrWarps);
       mbar_init(&st_empty[s], 1);
     }
@@ -904,7 +929,7 @@ __global__ void __launch_bounds__(kPtThreads, 1)
           int g, kc;
           l2_step(st, g, kc);
           const uint32_t s = it % kL2Stages, ph = ((it / kL2Stages) & 1) ^ 1;
-          if (it >= kL2Stages && (!mbar_wait(&st_empty[s], ph, status) || !mbar_wait(&raw_empty[s], ph, status))) {
+          if (it >= kL2Stages && !mbar_wait(&st_empty[s], ph, status)) {
             s_abort = 1;
             break;
           }
@@ -913,11 +938,11 @@ __global__ void __launch_bounds__(kPtThreads, 1)
           mbar_expect_tx(&raw_full[s], kPtChunk);
           if (LEFT) {
             tma_load_2d(dir(s), &tmP, px0 + 32 * kc, py0 + 128 * tile, &dir_full[s]);
-            for (int c = 0; c < 4; ++c) tma_load_2d(raw(s) + c * 4096, &tmT, 128 * g + 32 * c, t0 + 32 * kc, &raw_full[s]);
+            for (int c = 0; c < 4; ++c) tma_load_2d(trs(s) + c * 4096, &tmT, 128 * g + 32 * c, t0 + 32 * kc, &raw_full[s]);
           } else {
             tma_load_2d(dir(s), &tmT, 32 * kc, t0 + 128 * g, &dir_full[s]);
             for (int c = 0; c < 4; ++c)
-              tma_load_2d(raw(s) + c * 4096, &tmP, px0 + 128 * tile + 32 * c, py0 + 32 * kc, &raw_full[s]);
+              tma_load_2d(trs(s) + c * 4096, &tmP, px0 + 128 * tile + 32 * c, py0 + 32 * kc, &raw_full[s]);
           }
         }
       }
@@ -961,19 +986,15 @@ __global__ void __launch_bounds__(kPtThreads, 1)
     for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
       for (int st = 0; st < kL2Steps; ++st, ++it) {
         const uint32_t s = it % kL2Stages, ph = (it / kL2Stages) & 1;
-        if (!mbar_wait(&raw_full[s], ph, status) || (it >= kL2Stages && !mbar_wait(&st_empty[s], ph ^ 1, status)) ||
-            s_abort) {
+        // the in-place transposition's barrier makes the four warps agree on the waits' outcome
+        if (!transpose_chunk_inplace(trs(s), t, mbar_wait(&raw_full[s], ph, status) && !s_abort)) {
           s_abort = 1;
           ok = false;
           break;
         }
-        transpose_chunk(raw(s), trs(s), t);
         fence_async_smem();
         __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(&raw_empty[s]);
-          mbar_arrive(&tr_full[s]);
-        }
+        if (lane == 0) mbar_arrive(&tr_full[s]);
       }
     }
   } else {

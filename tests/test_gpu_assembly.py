@@ -210,3 +210,29 @@ def test_mixed_assembly_entries(case):
           f"exact {e_exact.max():.2e}")
     assert e_fast.max() <= 4 * e_exact.max() + 1e-13
     assert np.median(e_fast) <= 4 * np.median(e_exact) + 1e-13
+
+
+@pytest.mark.parametrize("scale", [1e15, 1e-15, 1e30, 1e-33])
+def test_mixed_assembly_extreme_scales(scale):
+    """The mixed assembly forms one reciprocal of the product of three denominators, which scales as
+    the 10th power of the mesh's size: meshes whose extent lies in [1e-20, 1e20] take that path
+    (scaled by 1e15 and 1e-15 here: every entry finite and within 1e-8 of the row scale of the exact
+    kernel's, as on the unscaled mesh); beyond, the exact kernel assembles them (1e30, 1e-33: equal bit
+    for bit)."""
+    torch = _torch()
+    tri, ta, tv = meshes.icosphere(2, 15.0)
+    tri = tri * scale
+    s = ob.setup(tri, 1, ta * scale ** 2)
+    solver, gr = gpu_gr(s, 1.0)
+    n3 = 3 * s.n
+    d = torch.empty((n3, n3), dtype=torch.float64, device="cuda")
+    assemble_device(0, s.n, 0, s.n, d.data_ptr(), n3, mixed=True)
+    torch.cuda.synchronize()
+    fast = d.cpu().numpy().reshape(n3, n3).T
+    solver.destroy()
+    assert np.all(np.isfinite(gr)) and np.all(np.isfinite(fast))
+    if 1e-20 <= 30.0 * scale <= 1e20:
+        scale_r = np.abs(gr).max(axis=1, keepdims=True)
+        assert (np.abs(fast - gr) / scale_r).max() < 1e-8
+    else:
+        assert np.array_equal(fast.view(np.int64), gr.view(np.int64))
