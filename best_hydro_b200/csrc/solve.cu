@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
                                                   V* __restrict__ part, int smax, const int4* __restrict__ tasks,
                                                   int ntasks, const FI* __restrict__ W, unsigned* cflags,
                                                   V* __restrict__ cslot) {
-  __shared__ V s_y[kIb][kIrhs];
+  __shared__ __align__(16) V s_y[kIb][kIrhs];
   __shared__ V s_b[kIb][kIrhs];
   __shared__ V s_acc[2][kIb][kIrhs];
   __shared__ int s_task[4], s_cnt;
@@ -638,6 +638,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
       }
     }
     int confirmed = q0;
+    bool have_x = false;  // s_y already holds this block's x (loaded during the previous block)
     for (int q = q0; q < q1; ++q) {
       const int jb = LOWER ? q : nblk - 1 - q;
       const int c0 = jb * kIb, nc = min(kIb, n - c0);
@@ -661,18 +662,52 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
         }
         confirmed = q + c;
       }
-      for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
-        const int rr = idx / kIrhs, r = idx % kIrhs;
-        s_y[rr][r] = (rr < nc && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + c0 + rr]) : (V)0;
+      if (!have_x)
+        for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+          const int rr = idx / kIrhs, r = idx % kIrhs;
+          s_y[rr][r] = (rr < nc && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + c0 + rr]) : (V)0;
+        }
+      __syncthreads();
+      // the next block's x, when its flag is already known to be set, loaded while this block's
+      // product runs (to shared memory after it)
+      const bool pre = q + 1 < q1 && q + 1 < confirmed;
+      V xn[kIb * kIrhs / 256];
+      if (pre) {
+        const int jn = LOWER ? q + 1 : nblk - 2 - q;
+        const int cn = jn * kIb, nn = min(kIb, n - cn);
+#pragma unroll
+        for (int e = 0; e < kIb * kIrhs / 256; ++e) {
+          const int idx = tid + 256 * e, rr = idx / kIrhs, r = idx % kIrhs;
+          xn[e] = (rr < nn && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + cn + rr]) : (V)0;
+        }
+      }
+      if constexpr (sizeof(V) == 4 && kIrhs == 8) {
+        // (FP32: the 8 right-hand sides of a row of x as two 16-byte reads)
+        const float4* sy = reinterpret_cast<const float4*>(&s_y[half * 64][0]);
+#pragma unroll
+        for (int kk = 0; kk < 64; ++kk) {
+          const V l = (V)lv[kk];
+          const float4 a = sy[2 * kk], b = sy[2 * kk + 1];
+          acc[0] -= l * a.x, acc[1] -= l * a.y, acc[2] -= l * a.z, acc[3] -= l * a.w;
+          acc[4] -= l * b.x, acc[5] -= l * b.y, acc[6] -= l * b.z, acc[7] -= l * b.w;
+        }
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < 64; ++kk) {
+          const V l = (V)lv[kk];
+#pragma unroll
+          for (int r = 0; r < kIrhs; ++r) acc[r] -= l * s_y[half * 64 + kk][r];
+        }
       }
       __syncthreads();
+      if (pre) {
 #pragma unroll
-      for (int kk = 0; kk < 64; ++kk) {
-        const V l = (V)lv[kk];
-#pragma unroll
-        for (int r = 0; r < kIrhs; ++r) acc[r] -= l * s_y[half * 64 + kk][r];
+        for (int e = 0; e < kIb * kIrhs / 256; ++e) {
+          const int idx = tid + 256 * e;
+          s_y[idx / kIrhs][idx % kIrhs] = xn[e];
+        }
       }
-      __syncthreads();
+      have_x = pre;
     }
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
