@@ -630,9 +630,24 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
         cp_async_wait_all();
         return;
       }
-      if (half == 0) {
+      {
+        // the partial sums of this row: half 0 adds slots [0, mid), half 1 [mid, nparts), four
+        // slots' loads in flight at a time (the two halves meet in the fixed order of the final sum)
         const V* p = part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs;
-        for (int sp = 0; sp < nparts; ++sp)
+        const int mid = (nparts + 1) / 2, s1 = half ? nparts : mid;
+        int sp = half ? mid : 0;
+        for (; sp + 4 <= s1; sp += 4) {
+          V t[4][kIrhs];
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int r = 0; r < kIrhs; ++r) t[u][r] = __ldcg(p + (size_t)(sp + u) * kIb * kIrhs + r);
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int r = 0; r < kIrhs; ++r) acc[r] += t[u][r];
+        }
+        for (; sp < s1; ++sp)
 #pragma unroll
           for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + (size_t)sp * kIb * kIrhs + r);
       }
