@@ -137,6 +137,21 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// the same copies with the bytes from `bytes` (0..16, or 0..4) on zero-filled; no bytes are read
+// when it is 0
+__device__ __forceinline__ void cp_async16z(void* sdst, const void* gsrc, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async4z(void* sdst, const void* gsrc, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+}
+// all but the N most recent groups of asynchronous copies complete
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 // all but the most recent group of asynchronous copies complete
 __device__ __forceinline__ void cp_async_wait_but_last() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
@@ -168,6 +183,28 @@ __device__ int wait_ready(const unsigned* flags, int jb, int step, int lo, int h
   }
   __syncthreads();
   return *s_cnt;
+}
+
+// Thread 0 waits until f[lo .. hi) all equal epoch, each wait bounded (status set, the rest skipped,
+// when one runs out).  Every thread of the block must call it; false when a wait ran out.
+__device__ bool wait_all(const unsigned* f, int lo, int hi, unsigned epoch, int* status, int* s_ok) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    for (int k = lo; k < hi && ok; ++k) {
+      unsigned spins = 0;
+      while (ld_acquire_u32(f + k) != epoch) {
+        if (++spins > c_spin_limit) {
+          atomicExch(status, (int)kWaitTimeout);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
 }
 
 // One triangle of the solve on Y (n x nrhs <= RHS, ldy).  LOWER: unit lower L, blocks in increasing
@@ -424,13 +461,15 @@ __global__ void __launch_bounds__(kIb) k_diag_inverses(const F* __restrict__ LU,
 // fixed order (so results do not depend on scheduling), applies the inverted diagonal block and
 // publishes x_i.  The blocks before are cut, walking away from the diagonal, into chunks of 2, 4,
 // 8 and then kChunk blocks, each a partial task P(i, s) that streams its blocks into a slot of its
-// own.  A chunk is issued right after the final task of its newest block row (the last x it needs):
+// own and releases that slot's flag.  A chunk is issued right after the final task of its newest
+// block row (the last x it needs):
 // the chunks near the diagonal, which become ready last, are short, so they finish within the few
 // rows the chain advances meanwhile, and the far ones, ready long before, stream the bulk of the
 // factor.  The host builds the task list (every task after all tasks it waits for, so the waits
 // always end; each is bounded anyway) and CTAs take it in ticket order.
 constexpr int kChunk = 16;
 constexpr int kLead = 2;
+constexpr int kRing = 3;  // stages of the FP32 partial tasks' factor ring (32 KB each)
 
 // V is the type of the right-hand sides and of every sum (double; float for the FP32 preconditioner).
 // CHAIN (the FP32 preconditioner): the chain of block rows is taken off the task list.  A final
@@ -444,9 +483,9 @@ constexpr int kLead = 2;
 // instead of two.  All CTAs of the grid are resident (the grid is sized by occupancy), so CTA 0
 // always runs.
 template <typename F, typename FI, bool LOWER, bool TRANS = false, typename V = double, bool CHAIN = false>
-__global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
+__global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
                                                   V* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
-                                                  unsigned epoch, int* status, unsigned* __restrict__ cnt,
+                                                  unsigned epoch, int* status, unsigned* __restrict__ pflags,
                                                   V* __restrict__ part, int smax, const int4* __restrict__ tasks,
                                                   int ntasks, const FI* __restrict__ W, unsigned* cflags,
                                                   V* __restrict__ cslot) {
@@ -581,6 +620,12 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
       return;
     }
   }
+  // The FP32 factor's partial tasks (column-major blocks, 8 right-hand sides) stream through a ring
+  // of kRing stages in s_dyn, each 64 columns x 128 rows of a block (32 KB), filled by asynchronous
+  // copies issued kRing - 1 stages ahead, so the factor's loads run under the waits for x and under
+  // the products; other tasks hold their block in registers.
+  constexpr bool kRingPath = sizeof(F) == 4 && sizeof(V) == 4 && kIrhs == 8 && !TRANS;
+  const bool vec16 = lda % 4 == 0 && (reinterpret_cast<uintptr_t>(LU) & 15) == 0;
   for (;;) {
     // task: x = slot (partial task) or -1 - number of partial tasks (final task); y = row; [z, w) blocks
     if (tid == 0) {
@@ -602,40 +647,49 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
     V acc[kIrhs];
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) acc[r] = (V)0;
+    // this thread's 64 entries of block (blk, block of q) (register path)
+    F lv[64];
+    auto load_lv = [&](int q) {
+      const int jb = LOWER ? q : nblk - 1 - q;
+      const int c0 = jb * kIb, nc = min(kIb, n - c0);
+      if (TRANS) {
+        const F* rowp = LU + (size_t)(r0 + row) * lda + c0 + half * 64;
+#pragma unroll
+        for (int kk = 0; kk < 64; ++kk) lv[kk] = (live && half * 64 + kk < nc) ? rowp[kk] : (F)0;
+      } else {
+        const F* col = LU + (size_t)(c0 + half * 64) * lda + r0 + row;
+#pragma unroll
+        for (int kk = 0; kk < 64; ++kk) lv[kk] = (live && half * 64 + kk < nc) ? col[(size_t)kk * lda] : (F)0;
+      }
+    };
+    bool lv_ready = false;  // lv already holds block q0
     if (fin) {
       // before any wait: the inverted diagonal block into shared memory (asynchronous copies), the
-      // block's right-hand sides, and the partial sums of the earlier chunks
+      // block's right-hand sides, and this thread's entries of the first block
       const FI* dblk = DI + (size_t)blk * kIb * kIb;
       for (int e = tid; e < kIb * kIb; e += 256) cp_async_elem<sizeof(FI)>(s_di + (e >> 7) * (kIb + 1) + (e & 127), dblk + e);
       for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
         const int rr = idx / kIrhs, r = idx % kIrhs;
         s_b[rr][r] = (rr < nr && r < nrhs) ? Y[(size_t)r * ldy + r0 + rr] : (V)0;
       }
-      const int nparts = -1 - code;
-      if (tid == 0) {
-        int ok = 1;
-        unsigned spins = 0;
-        while (nparts > 0 && ld_acquire_u32(cnt + i) < (unsigned)nparts) {
-          if (++spins > c_spin_limit) {
-            atomicExch(status, (int)kWaitTimeout);
-            ok = 0;
-            break;
-          }
-          __nanosleep(32);
-        }
-        s_cnt = ok;
+      if (q0 < q1) {
+        load_lv(q0);
+        lv_ready = true;
       }
-      __syncthreads();
-      if (!s_cnt) {
+      // the partial sums of this row: the far chunks' slots 1 .. nparts-1 (ready first) as soon as
+      // they are all in, half 0 adding [1, mid) and half 1 [mid, nparts), four slots' loads in
+      // flight at a time; then slot 0 (the chunk next to the final blocks, ready last) by half 0.
+      // The order of the sum is fixed.
+      const int nparts = -1 - code;
+      const unsigned* pf = pflags + (size_t)i * smax;
+      const V* p = part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs;
+      if (!wait_all(pf, 1, nparts, epoch, status, &s_cnt)) {
         cp_async_wait_all();
         return;
       }
       {
-        // the partial sums of this row: half 0 adds slots [0, mid), half 1 [mid, nparts), four
-        // slots' loads in flight at a time (the two halves meet in the fixed order of the final sum)
-        const V* p = part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs;
-        const int mid = (nparts + 1) / 2, s1 = half ? nparts : mid;
-        int sp = half ? mid : 0;
+        const int mid = 1 + nparts / 2, s1 = half ? nparts : mid;
+        int sp = half ? mid : 1;
         for (; sp + 4 <= s1; sp += 4) {
           V t[4][kIrhs];
 #pragma unroll
@@ -651,6 +705,120 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
 #pragma unroll
           for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + (size_t)sp * kIb * kIrhs + r);
       }
+      if (!wait_all(pf, 0, min(nparts, 1), epoch, status, &s_cnt)) {
+        cp_async_wait_all();
+        return;
+      }
+      if (nparts > 0 && half == 0)
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + r);
+    }
+    if constexpr (kRingPath) {
+      if (!fin) {
+        // stage st: columns 64 (st & 1) .. +63 of the block of q0 + st / 2, column-major 128 x 64 at
+        // ring + (st % kRing) * 8192; rows beyond nr and columns beyond n zero-filled
+        float* ring = reinterpret_cast<float*>(s_dyn);
+        const int nst = 2 * (q1 - q0);
+        auto issue = [&](int st) {
+          if (st < nst) {
+            const int jb = LOWER ? q0 + (st >> 1) : nblk - 1 - q0 - (st >> 1);
+            const int cs = jb * kIb + (st & 1) * 64, ncs = min(64, n - cs);
+            float* dst = ring + (st % kRing) * (64 * kIb);
+            const float* src = reinterpret_cast<const float*>(LU);
+            if (vec16) {
+              for (int e = tid; e < 64 * kIb / 4; e += 256) {
+                const int c = e >> 5, rr = (e & 31) * 4;
+                const int ok = c < ncs ? max(0, min(4, nr - rr)) : 0;
+                cp_async16z(dst + c * kIb + rr, ok ? src + (size_t)(cs + c) * lda + r0 + rr : src, ok * 4);
+              }
+            } else {
+              for (int e = tid; e < 64 * kIb; e += 256) {
+                const int c = e >> 7, rr = e & 127;
+                const bool ok = c < ncs && rr < nr;
+                cp_async4z(dst + c * kIb + rr, ok ? src + (size_t)(cs + c) * lda + r0 + rr : src, ok ? 4 : 0);
+              }
+            }
+          }
+          cp_async_commit();
+        };
+#pragma unroll
+        for (int st = 0; st < kRing - 1; ++st) issue(st);
+        int confirmed = q0;
+        bool have_x = false;  // xn holds the x of the next block
+        float xn[kIb * kIrhs / 256];
+        for (int st = 0; st < nst; ++st) {
+          const int q = q0 + (st >> 1);
+          const bool head = (st & 1) == 0;
+          if (head && q >= confirmed) {
+            const int jb = LOWER ? q : nblk - 1 - q;
+            const int c = LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, &s_cnt)
+                                : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, &s_cnt);
+            if (c == 0) {
+              cp_async_wait_all();
+              return;
+            }
+            confirmed = q + c;
+          }
+          cp_async_wait_group<kRing - 2>();
+          // stage st is in for every thread; nobody reads stage st - 1 (nor, at a block's head, the
+          // previous block's x) any more
+          __syncthreads();
+          issue(st + kRing - 1);
+          if (head) {
+            const int jb = LOWER ? q : nblk - 1 - q;
+            const int c0 = jb * kIb, nc = min(kIb, n - c0);
+            if (have_x) {
+#pragma unroll
+              for (int e = 0; e < kIb * kIrhs / 256; ++e) {
+                const int idx = tid + 256 * e;
+                s_y[idx / kIrhs][idx % kIrhs] = xn[e];
+              }
+            } else {
+              for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+                const int rr = idx / kIrhs, r = idx % kIrhs;
+                s_y[rr][r] = (rr < nc && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + c0 + rr]) : 0.f;
+              }
+            }
+            have_x = false;
+            __syncthreads();
+          } else if (q + 1 < q1 && q + 1 < confirmed) {
+            // the next block's x (its flag already seen), to registers while this product runs
+            const int jn = LOWER ? q + 1 : nblk - 2 - q;
+            const int cn = jn * kIb, nn = min(kIb, n - cn);
+#pragma unroll
+            for (int e = 0; e < kIb * kIrhs / 256; ++e) {
+              const int idx = tid + 256 * e, rr = idx / kIrhs, r = idx % kIrhs;
+              xn[e] = (rr < nn && r < nrhs) ? __ldcg(&Y[(size_t)r * ldy + cn + rr]) : 0.f;
+            }
+            have_x = true;
+          }
+          // columns 32 half .. +31 of the stage against the matching 32 rows of x (two 16-byte reads
+          // of the 8 right-hand sides per row)
+          const float* sl = ring + (st % kRing) * (64 * kIb) + half * 32 * kIb + row;
+          const float4* sy = reinterpret_cast<const float4*>(&s_y[(st & 1) * 64 + half * 32][0]);
+#pragma unroll
+          for (int kk = 0; kk < 32; ++kk) {
+            const float l = sl[kk * kIb];
+            const float4 a = sy[2 * kk], b = sy[2 * kk + 1];
+            acc[0] -= l * a.x, acc[1] -= l * a.y, acc[2] -= l * a.z, acc[3] -= l * a.w;
+            acc[4] -= l * b.x, acc[5] -= l * b.y, acc[6] -= l * b.z, acc[7] -= l * b.w;
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
+        __syncthreads();
+        V* slot = part + ((size_t)i * smax + sidx) * kIb * kIrhs;
+        for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
+          const int rr = idx / kIrhs, r = idx % kIrhs;
+          slot[idx] = s_acc[0][rr][r] + s_acc[1][rr][r];
+        }
+        __syncthreads();
+        if (tid == 0) {
+          __threadfence();
+          st_release_u32(pflags + (size_t)i * smax + sidx, epoch);
+        }
+        continue;
+      }
     }
     int confirmed = q0;
     bool have_x = false;  // s_y already holds this block's x (loaded during the previous block)
@@ -658,16 +826,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
       const int jb = LOWER ? q : nblk - 1 - q;
       const int c0 = jb * kIb, nc = min(kIb, n - c0);
       // this thread's 64 entries of block (blk, jb), loaded before the wait
-      F lv[64];
-      if (TRANS) {
-        const F* rowp = LU + (size_t)(r0 + row) * lda + c0 + half * 64;
-#pragma unroll
-        for (int kk = 0; kk < 64; ++kk) lv[kk] = (live && half * 64 + kk < nc) ? rowp[kk] : (F)0;
-      } else {
-        const F* col = LU + (size_t)(c0 + half * 64) * lda + r0 + row;
-#pragma unroll
-        for (int kk = 0; kk < 64; ++kk) lv[kk] = (live && half * 64 + kk < nc) ? col[(size_t)kk * lda] : (F)0;
-      }
+      if (!(lv_ready && q == q0)) load_lv(q);
       if (q >= confirmed) {
         const int c = LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, &s_cnt)
                             : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, &s_cnt);
@@ -736,7 +895,7 @@ __global__ void __launch_bounds__(256) k_trsv_inv(const F* __restrict__ LU, long
       __syncthreads();
       if (tid == 0) {
         __threadfence();
-        atomicAdd(cnt + i, 1u);
+        st_release_u32(pflags + (size_t)i * smax + sidx, epoch);
       }
       continue;
     }
@@ -872,14 +1031,15 @@ __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict
   if (tid == 0) *scale = sc;
 }
 
-// Scratch of the split solves, after the base scratch: per-row partial-task counters, the partial
-// sums [nblk][smax][128][kIrhs], and the task list.
+// Scratch of the split solves, after the base scratch: the partial sums' ready flags [nblk][smax]
+// (zero when allocated; a slot is ready when its flag equals the solve's epoch), the partial sums
+// [nblk][smax][128][kIrhs], and the task list.
 struct SplitScratch {
   static int nblk(int n) { return (n + kIb - 1) / kIb; }
   static int smax(int n) { return 4 + nblk(n) / kChunk; }
   static size_t max_tasks(int n) { return (size_t)nblk(n) * (1 + smax(n)); }
   static size_t base(int n) { return (TrsvScratch::bytes(n) + 255) / 256 * 256; }
-  static size_t part_off(int n) { return base(n) + ((size_t)nblk(n) * 4 + 255) / 256 * 256; }
+  static size_t part_off(int n) { return base(n) + ((size_t)nblk(n) * smax(n) * 4 + 255) / 256 * 256; }
   static size_t task_off(int n) { return part_off(n) + (size_t)nblk(n) * smax(n) * kIb * kIrhs * sizeof(double); }
   // the chain's c_i ready flags (zero when allocated, like the others) and c_i slots
   static size_t cflag_off(int n) { return (task_off(n) + max_tasks(n) * sizeof(int4) + 255) / 256 * 256; }
@@ -923,7 +1083,7 @@ cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const flo
   unsigned char* base = static_cast<unsigned char*>(scratch);
   unsigned* ticket = reinterpret_cast<unsigned*>(base);
   unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
-  unsigned* cnt = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
+  unsigned* pflags = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
   float* part = reinterpret_cast<float*>(base + SplitScratch::part_off(n));
   int4* tasks = reinterpret_cast<int4*>(base + SplitScratch::task_off(n));
   unsigned* cflags = reinterpret_cast<unsigned*>(base + SplitScratch::cflag_off(n));
@@ -935,12 +1095,12 @@ cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const flo
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
   if (e != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(cnt, 0, (size_t)SplitScratch::nblk(n) * 4, s)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(tasks, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return e;
   // the final tasks' inverted diagonal block (128 x 129 FP32, the chain's W prefetch), then the
-  // chain's V prefetch (128 x 128 FP16)
+  // chain's V prefetch (128 x 128 FP16); the partial tasks' ring (kRing x 32 KB) fits in the same
   const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(float) + (size_t)kIb * kIb * 2;
+  static_assert((size_t)kIb * (kIb + 1) * 4 + (size_t)kIb * kIb * 2 >= (size_t)kRing * 64 * kIb * 4, "ring");
   auto kern = k_trsv_inv<float, float, LOWER, false, float, true>;
   static bool attr = false;
   static int per_sm = 0;
@@ -960,7 +1120,7 @@ cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const flo
   int n_ = n, q_ = q, smax = SplitScratch::smax(n), nt = (int)list.size();
   unsigned ep = epoch;
   void* args[] = {(void*)&LU, (void*)&lda, (void*)&di, (void*)&n_, (void*)&y, (void*)&ldy_, (void*)&q_,
-                  (void*)&flags, (void*)&ticket, (void*)&ep, (void*)&d_status, (void*)&cnt, (void*)&part,
+                  (void*)&flags, (void*)&ticket, (void*)&ep, (void*)&d_status, (void*)&pflags, (void*)&part,
                   (void*)&smax, (void*)&tasks, (void*)&nt, (void*)&W, (void*)&cflags, (void*)&cslot};
   e = cudaLaunchCooperativeKernel((const void*)kern, dim3(sms * per_sm), dim3(256), args, dsmem, s);
   BGPU_COUNT_LAUNCH();
@@ -974,7 +1134,7 @@ cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, V* Yc, long ldy
   unsigned char* base = static_cast<unsigned char*>(scratch);
   unsigned* ticket = reinterpret_cast<unsigned*>(base);
   unsigned* flags = reinterpret_cast<unsigned*>(base + TrsvScratch::flags_off());
-  unsigned* cnt = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
+  unsigned* pflags = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
   V* part = reinterpret_cast<V*>(base + SplitScratch::part_off(n));
   int4* tasks = reinterpret_cast<int4*>(base + SplitScratch::task_off(n));
   const std::vector<int4>& list = split_tasks(SplitScratch::nblk(n));
@@ -984,10 +1144,11 @@ cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, V* Yc, long ldy
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaMemsetAsync(ticket, 0, 4, s);
   if (e != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(cnt, 0, (size_t)SplitScratch::nblk(n) * 4, s)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(tasks, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return e;
-  const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(FI);
+  // the final tasks' inverted diagonal block; for the FP32 factor at least the partial tasks' ring
+  const size_t dsmem = std::max((size_t)kIb * (kIb + 1) * sizeof(FI),
+                                sizeof(F) == 4 && !TRANS ? (size_t)kRing * 64 * kIb * 4 : (size_t)0);
   static bool attr = false;
   if (!attr) {
     if ((e = cudaFuncSetAttribute(k_trsv_inv<F, FI, LOWER, TRANS, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1006,7 +1167,7 @@ cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, V* Yc, long ldy
     per_sm = std::min(per_sm, 2);
   }
   k_trsv_inv<F, FI, LOWER, TRANS, V><<<sms * per_sm, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
-                                                          cnt, part, SplitScratch::smax(n), tasks, (int)list.size(),
+                                                          pflags, part, SplitScratch::smax(n), tasks, (int)list.size(),
                                                           nullptr, nullptr, nullptr);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
