@@ -210,7 +210,8 @@ cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const floa
                           const float* WU, int n, float* Y, long ldy, int nrhs, void* scratch, int* d_status,
                           cudaStream_t s);
 // The chain weights of trsv_lu32_inv (WL, WU: chain_weights_elems(n) floats each):
-// W_b = D_b^-1 L_{b,b-1} and D_b^-1 U_{b,b+1} over the 128-row blocks.  (WL = WU = nullptr: the
+// W_b = D_b^-1 L_{b,b-1}, V_b = D_b^-1 L_{b,b-2} (and the same with U) over the 128-row blocks,
+// FP16 scaled, in the order the chain's tensor-core products read them.  (WL = WU = nullptr: the
 // solve without the chain.)
 size_t chain_weights_elems(int n);
 // The poll limit of every triangular-solve wait (device constant; default 4,194,304).

@@ -131,14 +131,10 @@ __device__ __forceinline__ void cp_async_elem(void* sdst, const void* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(B) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-// asynchronous 16-byte copy global -> shared (both 16-byte aligned), and the commit of a group
-__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
-}
+// the commit of a group of asynchronous copies
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// the same copies with the bytes from `bytes` (0..16, or 0..4) on zero-filled; no bytes are read
-// when it is 0
+// asynchronous 16-byte (both addresses 16-byte aligned) or 4-byte copies global -> shared, the
+// bytes from `bytes` (0..16, or 0..4) on zero-filled; no bytes are read when it is 0
 __device__ __forceinline__ void cp_async16z(void* sdst, const void* gsrc, int bytes) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
@@ -152,8 +148,6 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait_group() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
-// all but the most recent group of asynchronous copies complete
-__device__ __forceinline__ void cp_async_wait_but_last() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // Warp 0 waits until flags[jb] == epoch, then counts how many more flags in the direction `step`
 // (+1 or -1) are ready too, up to 32 and within [lo, hi).  Returns that count (>= 1), or 0 when the
@@ -471,24 +465,186 @@ constexpr int kChunk = 16;
 constexpr int kLead = 2;
 constexpr int kRing = 3;  // stages of the FP32 partial tasks' factor ring (32 KB each)
 
+// D += A B on the tensor cores (mma.sync m16n8k8, TF32 operands, FP32 accumulators).  Fragments:
+// lane = 4 g + t; A (16 x 8): a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4); B (8 x 8):
+// b0 (t, g), b1 (t + 4, g); D (16 x 8): d0 (g, 2t), d1 (g, 2t + 1), d2 (g + 8, 2t), d3 (g + 8, 2t + 1).
+__device__ __forceinline__ void mma_tf32(float (&d)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
+                                         unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+// x rounded to TF32 (nearest, ties away), as the bits of an FP32 value
+__device__ __forceinline__ unsigned to_tf32(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
+
+// The chain weights' layout: a 128 x 128 block M in FP16, scaled by its largest magnitude, in the
+// order the chain's tensor-core products read it: warp w (rows 16 w .. +15) and k-step s (columns
+// 8 s .. +7) give lane l the A fragment (a0, a1, a2, a3) of M's 16 x 8 tile, two k-steps per 16
+// bytes, so each lane loads its fragments of a block with eight 16-byte reads.  Half index of M(r, k):
+__device__ __forceinline__ int chain_frag_off(int r, int k) {
+  const int w = r >> 4, g = r & 7, rhi = (r >> 3) & 1, s = k >> 3, t = k & 3, khi = (k >> 2) & 1;
+  return (((w * 8 + (s >> 1)) * 32 + g * 4 + t) * 2 + (s & 1)) * 4 + rhi + 2 * khi;
+}
+constexpr int kChainBlockHalves = kIb * kIb;  // 16,384 halves (32 KB) per block
+
+// The chain of the FP32 preconditioner (one CTA of k_trsv_inv, all 256 threads; see there):
+//     x_i = c_i - W_i x_{i-1} - V_i x_{i-2}
+// over the chain steps i = 0 .. nblk-1 (block row i, or nblk-1-i for the upper triangle).  Warp w
+// owns rows 16 w .. +15 of every step: both products on the tensor cores (W_i x_{i-1} for x_i, and
+// V_{i+1} x_{i-1} for the next step, sharing x_{i-1}'s fragments), x split into two TF32 parts
+// (hi + lo) so that only the weights carry TF32/FP16 rounding.  The weights of the next step are
+// loaded into registers while the current step runs; c_i (entries tagged with the solve's epoch by
+// the final tasks) is loaded a step ahead and taken entry by entry once its tags match, so a step
+// waits on no flag.  x_{i-1}, x_i live in a ring of three 128 x 8 buffers; one barrier per step,
+// after which thread 0 releases flags[block] for the tasks that need x_i.  Wt: chain_weights32's
+// output for this triangle; cslot: the tagged c slots [nblk][128][8].
+template <bool LOWER>
+__device__ void chain_run(const float* __restrict__ Wt, int n, int nblk, float* Y, long ldy, int nrhs, unsigned* flags,
+                          unsigned epoch, int* status, const unsigned long long* cslot, float* xb0, float* xb1,
+                          float* xb2) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const __half* Wh = reinterpret_cast<const __half*>(Wt);
+  const __half* Vh = Wh + (size_t)nblk * kChainBlockHalves;
+  const float* scales = Wt + (size_t)nblk * kChainBlockHalves;  // W's scales [nblk], then V's
+  auto bl = [&](int ii) { return LOWER ? ii : nblk - 1 - ii; };
+  auto xbuf = [&](int k) { return k == 0 ? xb0 : (k == 1 ? xb1 : xb2); };
+  uint4 aw[8], av[8];  // this lane's fragments of W_i and V_{i+1} (FP16, two k-steps per uint4)
+  auto load_frags = [&](uint4 (&a)[8], const __half* base, int ii) {
+    const uint4* p = reinterpret_cast<const uint4*>(base + (size_t)bl(ii) * kChainBlockHalves) + warp * 256 + lane;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) a[m] = __ldg(p + m * 32);
+  };
+  const int ra = 16 * warp + g, rb = ra + 8, n0 = 2 * t;
+  unsigned long long cv[4];
+  auto load_c = [&](int ii) {
+    const unsigned long long* p = cslot + (size_t)ii * kIb * kIrhs;
+    cv[0] = ld_relaxed_u64(p + ra * kIrhs + n0);
+    cv[1] = ld_relaxed_u64(p + ra * kIrhs + n0 + 1);
+    cv[2] = ld_relaxed_u64(p + rb * kIrhs + n0);
+    cv[3] = ld_relaxed_u64(p + rb * kIrhs + n0 + 1);
+  };
+  for (int e = tid; e < kIb * kIrhs; e += 256) xb2[e] = 0.f;  // x_{-1}
+  load_frags(aw, Wh, 0);
+  float sw = scales[bl(0)], sv = 0.f;
+  if (nblk > 1) {
+    load_frags(av, Vh, 1);
+    sv = scales[nblk + bl(1)];
+  }
+  load_c(0);
+  float pc[4] = {0.f, 0.f, 0.f, 0.f};  // sv_i V_i x_{i-2}, this lane's D fragment
+  __syncthreads();
+  for (int i = 0; i < nblk; ++i) {
+    const int blk = bl(i), r0 = blk * kIb, nr = min(kIb, n - r0);
+    const float* xp = xbuf((i + 2) % 3);  // x_{i-1}
+    float dw[4] = {0.f, 0.f, 0.f, 0.f}, dw2[4] = {0.f, 0.f, 0.f, 0.f};
+    float dv[4] = {0.f, 0.f, 0.f, 0.f}, dv2[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = 16 * m + 8 * h + t;
+        const float x0 = xp[k * kIrhs + g], x1 = xp[(k + 4) * kIrhs + g];
+        const unsigned h0 = to_tf32(x0), h1 = to_tf32(x1);
+        const unsigned l0 = to_tf32(x0 - __uint_as_float(h0)), l1 = to_tf32(x1 - __uint_as_float(h1));
+        const unsigned pw0 = h ? aw[m].z : aw[m].x, pw1 = h ? aw[m].w : aw[m].y;
+        const unsigned pv0 = h ? av[m].z : av[m].x, pv1 = h ? av[m].w : av[m].y;
+        const float2 w01 = __half22float2(*reinterpret_cast<const __half2*>(&pw0));
+        const float2 w23 = __half22float2(*reinterpret_cast<const __half2*>(&pw1));
+        const float2 v01 = __half22float2(*reinterpret_cast<const __half2*>(&pv0));
+        const float2 v23 = __half22float2(*reinterpret_cast<const __half2*>(&pv1));
+        mma_tf32(dw, __float_as_uint(w01.x), __float_as_uint(w01.y), __float_as_uint(w23.x), __float_as_uint(w23.y), h0,
+                 h1);
+        mma_tf32(dw2, __float_as_uint(w01.x), __float_as_uint(w01.y), __float_as_uint(w23.x), __float_as_uint(w23.y),
+                 l0, l1);
+        mma_tf32(dv, __float_as_uint(v01.x), __float_as_uint(v01.y), __float_as_uint(v23.x), __float_as_uint(v23.y), h0,
+                 h1);
+        mma_tf32(dv2, __float_as_uint(v01.x), __float_as_uint(v01.y), __float_as_uint(v23.x), __float_as_uint(v23.y),
+                 l0, l1);
+      }
+    const float sw_i = sw, sv_next = sv;
+    // the next step's weights, into the registers just read
+    if (i + 1 < nblk) {
+      load_frags(aw, Wh, i + 1);
+      sw = scales[bl(i + 1)];
+    }
+    if (i + 2 < nblk) {
+      load_frags(av, Vh, i + 2);
+      sv = scales[nblk + bl(i + 2)];
+    }
+    // c_i: every entry must carry this solve's epoch (reloaded until it does, bounded)
+    int fail = 0;
+    {
+      const unsigned long long* p = cslot + (size_t)i * kIb * kIrhs;
+      unsigned spins = 0;
+      while (!((unsigned)(cv[0] >> 32) == epoch && (unsigned)(cv[1] >> 32) == epoch &&
+               (unsigned)(cv[2] >> 32) == epoch && (unsigned)(cv[3] >> 32) == epoch)) {
+        if (++spins > c_spin_limit) {
+          fail = 1;
+          break;
+        }
+        __nanosleep(32);
+        cv[0] = ld_relaxed_u64(p + ra * kIrhs + n0);
+        cv[1] = ld_relaxed_u64(p + ra * kIrhs + n0 + 1);
+        cv[2] = ld_relaxed_u64(p + rb * kIrhs + n0);
+        cv[3] = ld_relaxed_u64(p + rb * kIrhs + n0 + 1);
+      }
+    }
+    float x[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = __uint_as_float((unsigned)cv[j]) - pc[j] - sw_i * (dw[j] + dw2[j]);
+    float* xo = xbuf(i % 3);
+    *reinterpret_cast<float2*>(xo + ra * kIrhs + n0) = make_float2(x[0], x[1]);
+    *reinterpret_cast<float2*>(xo + rb * kIrhs + n0) = make_float2(x[2], x[3]);
+    if (ra < nr) {
+      if (n0 < nrhs) Y[(size_t)n0 * ldy + r0 + ra] = x[0];
+      if (n0 + 1 < nrhs) Y[(size_t)(n0 + 1) * ldy + r0 + ra] = x[1];
+    }
+    if (rb < nr) {
+      if (n0 < nrhs) Y[(size_t)n0 * ldy + r0 + rb] = x[2];
+      if (n0 + 1 < nrhs) Y[(size_t)(n0 + 1) * ldy + r0 + rb] = x[3];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) pc[j] = sv_next * (dv[j] + dv2[j]);
+    if (i + 1 < nblk) load_c(i + 1);
+    // x_i complete in shared memory and in Y; x_{i-1}'s buffer free for x_{i+2}
+    if (__syncthreads_or(fail)) {
+      if (tid == 0) atomicExch(status, (int)kWaitTimeout);
+      return;
+    }
+    if (tid == 0) st_release_u32(flags + blk, epoch);
+  }
+}
+
 // V is the type of the right-hand sides and of every sum (double; float for the FP32 preconditioner).
 // CHAIN (the FP32 preconditioner): the chain of block rows is taken off the task list.  A final
 // task of row i then stops short of block i-2: it forms c_i = D_i^-1 (b_i - sum_{j <= i-3} L_ij x_j)
-// into a slot of its own and releases cflags[i]; CTA 0 runs the chain alone,
+// into a slot of its own (entries tagged with the solve's epoch); CTA 0 runs the chain (chain_run),
 //     x_i = c_i - W_i x_{i-1} - V_i x_{i-2},   W_i = D_i^-1 L_{i,i-1},  V_i = D_i^-1 L_{i,i-2}
-// (chain_weights32, once per factorisation; V in FP16 scaled by its largest entry), keeping x_{i-1}
-// in shared memory and W_i (prefetched a step ahead) in registers, forming V_{i+1} x_{i-1} at the
-// start of step i (before its wait), and releases flags[i] for the tasks that need x_i.  A row's
-// hand-off through global memory (final task, c_i, chain) thus has three chain steps to arrive in
-// instead of two.  All CTAs of the grid are resident (the grid is sized by occupancy), so CTA 0
-// always runs.
+// (chain_weights32, once per factorisation), and releases flags[i] for the tasks that need x_i.
+// A row's hand-off through global memory (final task, c_i, chain) thus has three chain steps to
+// arrive in instead of two.  All CTAs of the grid are resident (the grid is sized by occupancy), so
+// CTA 0 always runs.
 template <typename F, typename FI, bool LOWER, bool TRANS = false, typename V = double, bool CHAIN = false>
 __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
                                                   V* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
                                                   unsigned epoch, int* status, unsigned* __restrict__ pflags,
                                                   V* __restrict__ part, int smax, const int4* __restrict__ tasks,
-                                                  int ntasks, const FI* __restrict__ W, unsigned* cflags,
-                                                  V* __restrict__ cslot) {
+                                                  int ntasks, const FI* __restrict__ W,
+                                                  unsigned long long* cslot) {
   __shared__ __align__(16) V s_y[kIb][kIrhs];
   __shared__ V s_b[kIb][kIrhs];
   __shared__ V s_acc[2][kIb][kIrhs];
@@ -499,124 +655,8 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
   const int tid = threadIdx.x, row = tid & (kIb - 1), half = tid >> 7;
   if constexpr (CHAIN) {
     if (blockIdx.x == 0) {
-      // s_y holds x_{i-1}; wv this thread's 64 entries of W_i (row `row`, columns 64 half .. +63);
-      // W_{i+1} arrives in shared memory (asynchronous 16-byte copies of the column-major tile)
-      // while step i runs, and moves to registers once x_i is published.  The lag-2 term
-      // V_{i+1} x_{i-1} is formed at the start of step i, before the wait for c_i, from V_{i+1} in
-      // shared memory (FP16, scaled; fetched during step i-1): pc holds this thread's half of it
-      // for the next step.
-      FI wv[64];
-      FI* s_w = s_di;  // 128 x 128, column-major, unpadded (fits the final tasks' 128 x 129 buffer)
-      __half* s_v = reinterpret_cast<__half*>(s_dyn + (size_t)kIb * (kIb + 1) * sizeof(FI));  // 128 x 128 FP16
-      const __half* V16 = reinterpret_cast<const __half*>(W + (size_t)nblk * kIb * kIb);
-      const FI* vscale = W + (size_t)nblk * kIb * kIb + (size_t)nblk * kIb * kIb / 2;
-      auto fetch_w = [&](int ii) {
-        if (ii >= 1 && ii < nblk) {
-          const int b = LOWER ? ii : nblk - 1 - ii;
-          const FI* src = W + (size_t)b * kIb * kIb;
-          for (int e = tid; e < kIb * kIb * (int)sizeof(FI) / 16; e += 256) cp_async16(s_w + e * (16 / sizeof(FI)), src + e * (16 / sizeof(FI)));
-        }
-        cp_async_commit();
-      };
-      auto fetch_v = [&](int ii) {
-        if (ii >= 2 && ii < nblk) {
-          const int b = LOWER ? ii : nblk - 1 - ii;
-          const __half* src = V16 + (size_t)b * kIb * kIb;
-          for (int e = tid; e < kIb * kIb * 2 / 16; e += 256) cp_async16(s_v + e * 8, src + e * 8);
-        }
-        cp_async_commit();
-      };
-      fetch_w(1);
-      fetch_v(2);
-      V pc[kIrhs];  // (this thread's half of) V_i x_{i-2}, scaled
-#pragma unroll
-      for (int r = 0; r < kIrhs; ++r) pc[r] = (V)0;
-      for (int i = 0; i < nblk; ++i) {
-        const int blk = LOWER ? i : nblk - 1 - i;
-        const int r0 = blk * kIb, nr = min(kIb, n - r0);
-        // the lag-2 term of the next row, V_{i+1} x_{i-1}, while c_i may still be on its way
-        V pn[kIrhs];
-#pragma unroll
-        for (int r = 0; r < kIrhs; ++r) pn[r] = (V)0;
-        if (i >= 1 && i + 1 < nblk) {
-          cp_async_wait_but_last();  // V_{i+1} (W_{i+1}, fetched last, may still be in flight)
-          __syncthreads();
-          const int bn = LOWER ? i + 1 : nblk - 2 - i;
-          const V sc = (V)vscale[bn];
-#pragma unroll 8
-          for (int kk = 0; kk < 64; ++kk) {
-            const V v = (V)__half2float(s_v[(half * 64 + kk) * kIb + row]);
-#pragma unroll
-            for (int r = 0; r < kIrhs; ++r) pn[r] += v * s_y[half * 64 + kk][r];
-          }
-#pragma unroll
-          for (int r = 0; r < kIrhs; ++r) pn[r] *= sc;
-          __syncthreads();  // s_v read: refill it
-          fetch_v(i + 2);
-        }
-        if (tid == 0) {
-          unsigned spins = 0;
-          int ok = 1;
-          while (ld_acquire_u32(cflags + i) != epoch) {
-            if (++spins > c_spin_limit) {
-              atomicExch(status, (int)kWaitTimeout);
-              ok = 0;
-              break;
-            }
-            __nanosleep(32);
-          }
-          s_cnt = ok;
-        }
-        __syncthreads();
-        if (!s_cnt) {
-          cp_async_wait_all();
-          return;
-        }
-        V c[kIrhs];
-        if (half == 0) {
-          const V* cp = cslot + ((size_t)i * kIb + row) * kIrhs;
-#pragma unroll
-          for (int r = 0; r < kIrhs; ++r) c[r] = __ldcg(cp + r);
-        }
-        V acc[kIrhs];
-#pragma unroll
-        for (int r = 0; r < kIrhs; ++r) acc[r] = pc[r];
-        if (i >= 1) {
-#pragma unroll
-          for (int kk = 0; kk < 64; ++kk) {
-            const V w = (V)wv[kk];
-#pragma unroll
-            for (int r = 0; r < kIrhs; ++r) acc[r] += w * s_y[half * 64 + kk][r];
-          }
-        }
-#pragma unroll
-        for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
-        __syncthreads();
-        if (half == 0) {
-#pragma unroll
-          for (int r = 0; r < kIrhs; ++r) {
-            const V x = row < nr ? c[r] - (s_acc[0][row][r] + s_acc[1][row][r]) : (V)0;
-            s_y[row][r] = x;
-            if (row < nr && r < nrhs) Y[(size_t)r * ldy + r0 + row] = x;
-          }
-        }
-        __syncthreads();
-        if (tid == 0) {
-          __threadfence();
-          st_release_u32(flags + blk, epoch);
-        }
-#pragma unroll
-        for (int r = 0; r < kIrhs; ++r) pc[r] = pn[r];
-        if (i + 1 < nblk) {
-          cp_async_wait_but_last();  // W_{i+1} (V_{i+2}, fetched last, may still be in flight)
-          __syncthreads();
-#pragma unroll
-          for (int kk = 0; kk < 64; ++kk) wv[kk] = s_w[(half * 64 + kk) * kIb + row];
-          __syncthreads();
-          fetch_w(i + 2);
-        }
-      }
-      cp_async_wait_all();
+      chain_run<LOWER>(reinterpret_cast<const float*>(W), n, nblk, reinterpret_cast<float*>(Y), ldy, nrhs, flags, epoch,
+                       status, cslot, &s_acc[0][0][0], &s_acc[1][0][0], &s_y[0][0]);
       return;
     }
   }
@@ -921,15 +961,13 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
     __syncthreads();
     if constexpr (CHAIN) {
-      V* cp = cslot + (size_t)i * kIb * kIrhs;  // c_i, row-major 128 x kIrhs, zero beyond nr and nrhs
+      // c_i, row-major 128 x kIrhs, zero beyond nr and nrhs, each entry tagged with the solve's epoch
+      // in its upper 32 bits (the chain takes the entries once their tags match; no flag)
+      unsigned long long* cp = cslot + (size_t)i * kIb * kIrhs;
       for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
         const int rr = idx / kIrhs, r = idx % kIrhs;
-        cp[idx] = (rr < nr && r < nrhs) ? s_acc[0][rr][r] + s_acc[1][rr][r] : (V)0;
-      }
-      __syncthreads();
-      if (tid == 0) {
-        __threadfence();
-        st_release_u32(cflags + i, epoch);
+        const float c = (rr < nr && r < nrhs) ? (float)(s_acc[0][rr][r] + s_acc[1][rr][r]) : 0.f;
+        st_relaxed_u64(cp + idx, ((unsigned long long)epoch << 32) | __float_as_uint(c));
       }
     } else {
       for (int idx = tid; idx < kIb * kIrhs; idx += 256) {
@@ -945,13 +983,14 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
   }
 }
 
-// The chain weights of the FP32 preconditioner (see k_trsv_inv, CHAIN), one triangle per blockIdx.y,
-// one block row b per blockIdx.x, one lag per blockIdx.z:
-//   lag 1: W_b = D_b^-1 L_{b,b-1} (lower) or D_b^-1 U_{b,b+1} (upper), FP32, 128 x 128 column-major
-//          at out + b * 16384;
-//   lag 2: V_b = D_b^-1 L_{b,b-2} or D_b^-1 U_{b,b+2}, stored as FP16 scaled by its largest magnitude
-//          (the scale at out + nblk * 24576 + b, the halves from out + nblk * 16384)
-// rows and columns beyond n zero; a missing neighbour gives zeros (scale 1).
+// The chain weights of the FP32 preconditioner (see chain_run), one triangle per blockIdx.y, one
+// block row b per blockIdx.x, one lag per blockIdx.z:
+//   lag 1: W_b = D_b^-1 L_{b,b-1} (lower) or D_b^-1 U_{b,b+1} (upper),
+//   lag 2: V_b = D_b^-1 L_{b,b-2} or D_b^-1 U_{b,b+2},
+// each in FP16 scaled by its largest magnitude, in the fragment order of chain_frag_off: W_b's halves
+// from out + b * 8192 floats, V_b's from out + nblk * 8192 + b * 8192 floats; the scales at
+// out + nblk * 16384 + b (W) and + nblk + b (V).  Rows and columns beyond n zero; a missing
+// neighbour gives zeros (scale 1).
 __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict__ LU, long lda, int n,
                                                           const float* __restrict__ DL, const float* __restrict__ DU,
                                                           float* __restrict__ WL, float* __restrict__ WU) {
@@ -962,17 +1001,12 @@ __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict
   const int nblk = (n + kIb - 1) / kIb, b = blockIdx.x, lower = blockIdx.y == 0, lag = 1 + blockIdx.z;
   const int nb = lower ? b - lag : b + lag;  // the neighbouring block column
   float* base = lower ? WL : WU;
-  float* out = base + (size_t)b * kIb * kIb;
-  __half* out16 = reinterpret_cast<__half*>(base + (size_t)nblk * kIb * kIb) + (size_t)b * kIb * kIb;
-  float* scale = base + (size_t)nblk * kIb * kIb + (size_t)nblk * kIb * kIb / 2 + b;
+  __half* out16 = reinterpret_cast<__half*>(base) + ((size_t)(lag - 1) * nblk + b) * kChainBlockHalves;
+  float* scale = base + (size_t)nblk * kChainBlockHalves + (size_t)(lag - 1) * nblk + b;
   const int tid = threadIdx.x;
   if (nb < 0 || nb >= nblk) {
-    if (lag == 1)
-      for (int e = tid; e < kIb * kIb; e += 256) out[e] = 0.f;
-    else {
-      for (int e = tid; e < kIb * kIb; e += 256) out16[e] = __float2half_rn(0.f);
-      if (tid == 0) *scale = 1.f;
-    }
+    for (int e = tid; e < kChainBlockHalves; e += 256) out16[e] = __float2half_rn(0.f);
+    if (tid == 0) *scale = 1.f;
     return;
   }
   const float* D = (lower ? DL : DU) + (size_t)b * kIb * kIb;
@@ -1001,13 +1035,6 @@ __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * bv[j];
   }
-  if (lag == 1) {
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-#pragma unroll
-      for (int i = 0; i < 8; ++i) out[(size_t)(cb + j) * kIb + rb + i] = (rb + i < nr) ? acc[i][j] : 0.f;
-    return;
-  }
   float m = 0.f;
 #pragma unroll
   for (int i = 0; i < 8; ++i)
@@ -1027,7 +1054,7 @@ __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict
   for (int j = 0; j < 8; ++j)
 #pragma unroll
     for (int i = 0; i < 8; ++i)
-      out16[(size_t)(cb + j) * kIb + rb + i] = __float2half_rn((rb + i < nr) ? acc[i][j] * inv : 0.f);
+      out16[chain_frag_off(rb + i, cb + j)] = __float2half_rn((rb + i < nr) ? acc[i][j] * inv : 0.f);
   if (tid == 0) *scale = sc;
 }
 
@@ -1041,10 +1068,9 @@ struct SplitScratch {
   static size_t base(int n) { return (TrsvScratch::bytes(n) + 255) / 256 * 256; }
   static size_t part_off(int n) { return base(n) + ((size_t)nblk(n) * smax(n) * 4 + 255) / 256 * 256; }
   static size_t task_off(int n) { return part_off(n) + (size_t)nblk(n) * smax(n) * kIb * kIrhs * sizeof(double); }
-  // the chain's c_i ready flags (zero when allocated, like the others) and c_i slots
-  static size_t cflag_off(int n) { return (task_off(n) + max_tasks(n) * sizeof(int4) + 255) / 256 * 256; }
-  static size_t cslot_off(int n) { return cflag_off(n) + ((size_t)nblk(n) * 4 + 255) / 256 * 256; }
-  static size_t bytes(int n) { return cslot_off(n) + (size_t)nblk(n) * kIb * kIrhs * sizeof(double); }
+  // the chain's c_i slots (entries tagged with the solve's epoch; zero when allocated)
+  static size_t cslot_off(int n) { return (task_off(n) + max_tasks(n) * sizeof(int4) + 255) / 256 * 256; }
+  static size_t bytes(int n) { return cslot_off(n) + (size_t)nblk(n) * kIb * kIrhs * sizeof(unsigned long long); }
 };
 
 // The task list of a triangle with nblk block rows (see k_trsv_inv), built once per size.  chain:
@@ -1086,8 +1112,7 @@ cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const flo
   unsigned* pflags = reinterpret_cast<unsigned*>(base + SplitScratch::base(n));
   float* part = reinterpret_cast<float*>(base + SplitScratch::part_off(n));
   int4* tasks = reinterpret_cast<int4*>(base + SplitScratch::task_off(n));
-  unsigned* cflags = reinterpret_cast<unsigned*>(base + SplitScratch::cflag_off(n));
-  float* cslot = reinterpret_cast<float*>(base + SplitScratch::cslot_off(n));
+  unsigned long long* cslot = reinterpret_cast<unsigned long long*>(base + SplitScratch::cslot_off(n));
   const std::vector<int4>& list = split_tasks(SplitScratch::nblk(n), true);
   if (list.size() > SplitScratch::max_tasks(n)) return cudaErrorInvalidValue;
   int dev = 0, sms = 0;
@@ -1097,10 +1122,9 @@ cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const flo
   if (e != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(tasks, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return e;
-  // the final tasks' inverted diagonal block (128 x 129 FP32, the chain's W prefetch), then the
-  // chain's V prefetch (128 x 128 FP16); the partial tasks' ring (kRing x 32 KB) fits in the same
-  const size_t dsmem = (size_t)kIb * (kIb + 1) * sizeof(float) + (size_t)kIb * kIb * 2;
-  static_assert((size_t)kIb * (kIb + 1) * 4 + (size_t)kIb * kIb * 2 >= (size_t)kRing * 64 * kIb * 4, "ring");
+  // the final tasks' inverted diagonal block (128 x 129 FP32) or the partial tasks' ring (kRing x
+  // 32 KB); the chain uses none
+  const size_t dsmem = std::max((size_t)kIb * (kIb + 1) * sizeof(float), (size_t)kRing * 64 * kIb * 4);
   auto kern = k_trsv_inv<float, float, LOWER, false, float, true>;
   static bool attr = false;
   static int per_sm = 0;
@@ -1121,7 +1145,7 @@ cudaError_t trsv_one_chain(const float* LU, long lda, const float* DI, const flo
   unsigned ep = epoch;
   void* args[] = {(void*)&LU, (void*)&lda, (void*)&di, (void*)&n_, (void*)&y, (void*)&ldy_, (void*)&q_,
                   (void*)&flags, (void*)&ticket, (void*)&ep, (void*)&d_status, (void*)&pflags, (void*)&part,
-                  (void*)&smax, (void*)&tasks, (void*)&nt, (void*)&W, (void*)&cflags, (void*)&cslot};
+                  (void*)&smax, (void*)&tasks, (void*)&nt, (void*)&W, (void*)&cslot};
   e = cudaLaunchCooperativeKernel((const void*)kern, dim3(sms * per_sm), dim3(256), args, dsmem, s);
   BGPU_COUNT_LAUNCH();
   return e;
@@ -1168,7 +1192,7 @@ cudaError_t trsv_one(const F* LU, long lda, const FI* DI, int n, V* Yc, long ldy
   }
   k_trsv_inv<F, FI, LOWER, TRANS, V><<<sms * per_sm, 256, dsmem, s>>>(LU, lda, DI, n, Yc, ldy, q, flags, ticket, epoch, d_status,
                                                           pflags, part, SplitScratch::smax(n), tasks, (int)list.size(),
-                                                          nullptr, nullptr, nullptr);
+                                                          nullptr, nullptr);
   BGPU_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -1296,7 +1320,7 @@ cudaError_t set_wait_limit(unsigned spins) { return cudaMemcpyToSymbol(c_spin_li
 
 size_t chain_weights_elems(int n) {
   const size_t nblk = (size_t)((n + kIb - 1) / kIb);
-  return nblk * kIb * kIb + nblk * kIb * kIb / 2 + nblk;  // W (FP32), V (FP16), V's scales
+  return nblk * kChainBlockHalves + 2 * nblk;  // W and V (FP16, two halves per float), their scales
 }
 
 cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const float* DU, int n, float* WL, float* WU,
