@@ -63,6 +63,11 @@ struct Buf {
     }
     bytes = need;
   }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
   template <class T>
   T* as() const {
     return static_cast<T*>(p);
@@ -1164,7 +1169,7 @@ struct MixedSolver::Impl {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool fork = false;
   Buf lu32, at, bt, status, part, pdots, dots, trsv, vecs, dl32, du32, zf;
-  Buf wl32, wu32;  // the preconditioner's chain weights (D_b^-1 L_{b,b-1}, D_b^-1 U_{b,b+1})
+  Buf wl32, wu32;  // the preconditioner's chain data per triangle (weights, FP16 copy of the off-diagonal blocks)
   // BF16 mirrors of the factors (L part row-major, U part column-major), written by the triangular
   // solve leaves as the entries become final; the GEMMs read their operands there by position, so no
   // operand copies are made.  Used when the GPU has room for them (4 n^2 bytes), else copies.
@@ -1497,8 +1502,15 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   // solve's scratch (for up to 16 right-hand sides per pass)
   P.dl32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (L)");
   P.du32.ensure(diag_inverse_elems(P.n3) * sizeof(float), "diagonal-block inverses (U)");
-  P.wl32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain weights (L)");
-  P.wu32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain weights (U)");
+  // the preconditioner's chain data (weights and the FP16 copy of the off-diagonal blocks, half the
+  // FP32 factor's size); without room for it the preconditioner runs without the chain
+  try {
+    P.wl32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain data (L)");
+    P.wu32.ensure(chain_weights_elems(P.n3) * sizeof(float), "preconditioner chain data (U)");
+  } catch (const std::runtime_error&) {
+    P.wl32.release();
+    P.wu32.release();
+  }
   P.tc_leaves = std::getenv("BEST_GPU_SIMT_LEAVES") == nullptr;
   if (P.tc_leaves && (P.leaf_key[0] != P.lu32.p || P.leaf_key[1] != P.dl32.p || P.leaf_key[2] != P.du32.p ||
                       P.leaf_key[3] != reinterpret_cast<const void*>((uintptr_t)P.n3))) {
@@ -1603,9 +1615,10 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
     P.has256.assign((size_t)(P.n3 + kLeaf - 1) / kLeaf, 0);
     ck(stamps_reset(P.stamps.as<unsigned long long>(), P.slot_cap, s), "stamps");
     P.rlu(0, P.n3, s);  // direct launches in order, each timed
-    ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3, P.wl32.as<float>(),
-                       P.wu32.as<float>(), s),
-       "chain weights");
+    if (P.wl32.p)
+      ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3, P.wl32.as<float>(),
+                         P.wu32.as<float>(), s),
+         "chain weights");
     used_slots = P.nslots;
     used_work = P.slot_work;
   } else {
@@ -1630,9 +1643,10 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
       P.has256.assign((size_t)(P.n3 + kLeaf - 1) / kLeaf, 0);
       try {
         P.rlu(0, P.n3, cs);
-        ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3,
-                           P.wl32.as<float>(), P.wu32.as<float>(), cs),
-           "chain weights");
+        if (P.wl32.p)
+          ck(chain_weights32(P.lu32.as<float>(), P.ld32, P.dl32.as<float>(), P.du32.as<float>(), P.n3,
+                             P.wl32.as<float>(), P.wu32.as<float>(), cs),
+             "chain weights");
       } catch (...) {
         cudaStreamEndCapture(cs, &g);
         if (g) cudaGraphDestroy(g);

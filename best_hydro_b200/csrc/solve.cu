@@ -134,14 +134,25 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the commit of a group of asynchronous copies
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 // asynchronous 16-byte (both addresses 16-byte aligned) or 4-byte copies global -> shared, the
-// bytes from `bytes` (0..16, or 0..4) on zero-filled; no bytes are read when it is 0
-__device__ __forceinline__ void cp_async16z(void* sdst, const void* gsrc, int bytes) {
+// bytes from `bytes` (0..16, or 0..4) on zero-filled, no bytes read when it is 0; `policy` an L2
+// cache policy (l2_evict_first)
+__device__ __forceinline__ void cp_async16z(void* sdst, const void* gsrc, int bytes, unsigned long long policy) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;\n" ::"r"(d), "l"(gsrc), "r"(bytes),
+               "l"(policy)
+               : "memory");
 }
-__device__ __forceinline__ void cp_async4z(void* sdst, const void* gsrc, int bytes) {
+__device__ __forceinline__ void cp_async4z(void* sdst, const void* gsrc, int bytes, unsigned long long policy) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2, %3;\n" ::"r"(d), "l"(gsrc), "r"(bytes),
+               "l"(policy)
+               : "memory");
+}
+// an L2 policy that evicts the lines it touches first (streams read once)
+__device__ __forceinline__ unsigned long long l2_evict_first() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
 }
 // all but the N most recent groups of asynchronous copies complete
 template <int N>
@@ -490,6 +501,13 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
 }
+__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+// bytes (a multiple of 16, from a 16-byte aligned address) fetched into L2 ahead of their use
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
 
 // The chain weights' layout: a 128 x 128 block M in FP16, scaled by its largest magnitude, in the
 // order the chain's tensor-core products read it: warp w (rows 16 w .. +15) and k-step s (columns
@@ -501,12 +519,32 @@ __device__ __forceinline__ int chain_frag_off(int r, int k) {
 }
 constexpr int kChainBlockHalves = kIb * kIb;  // 16,384 halves (32 KB) per block
 
+// A triangle's chain data (one buffer per triangle, offsets in floats), all blocks in the fragment
+// order above, FP16, each row scaled by its largest magnitude (128 row scales per block):
+//   [0, kLags * nblk * 8192)       the weights D_b^-1 L_{b,b-l} (or D_b^-1 U_{b,b+l}) of the lags
+//                                  l = 1 .. kLags: block ((l-1) nblk + b) at that many 16,384 halves
+//                                  (l = 1: the chain's W_b; 2: its V_b; 3 .. 5: the final tasks')
+//   wscale_off: [+ kLags nblk 128) their row scales, block ((l-1) nblk + b) at that many 128 floats
+//   bscale_off: [+ nb2 * 128)      the row scales of the off-diagonal blocks
+//   blocks_off: [+ nb2 * 8192)     the off-diagonal blocks of the triangle in the order of the solve:
+//                                  block (i, q), q < i in q-space (q-row i is block row i of L, or
+//                                  nblk-1-i of U; q-column q likewise), number i (i-1) / 2 + q
+constexpr int kLags = 5;
+struct ChainLayout {
+  __host__ __device__ static size_t nb2(int nblk) { return (size_t)nblk * (nblk - 1) / 2; }
+  __host__ __device__ static size_t wscale_off(int nblk) { return (size_t)kLags * nblk * kChainBlockHalves / 2; }
+  __host__ __device__ static size_t bscale_off(int nblk) { return wscale_off(nblk) + (size_t)kLags * nblk * kIb; }
+  __host__ __device__ static size_t blocks_off(int nblk) { return (bscale_off(nblk) + nb2(nblk) * kIb + 63) / 64 * 64; }
+  __host__ __device__ static size_t elems(int nblk) { return blocks_off(nblk) + nb2(nblk) * kChainBlockHalves / 2; }
+};
+
 // The chain of the FP32 preconditioner (one CTA of k_trsv_inv, all 256 threads; see there):
 //     x_i = c_i - W_i x_{i-1} - V_i x_{i-2}
 // over the chain steps i = 0 .. nblk-1 (block row i, or nblk-1-i for the upper triangle).  Warp w
 // owns rows 16 w .. +15 of every step: both products on the tensor cores (W_i x_{i-1} for x_i, and
-// V_{i+1} x_{i-1} for the next step, sharing x_{i-1}'s fragments), x split into two TF32 parts
-// (hi + lo) so that only the weights carry TF32/FP16 rounding.  The weights of the next step are
+// V_{i+1} x_{i-1} for the next step, sharing x_{i-1}'s fragments; x rounded to TF32, the weights
+// carrying FP16 rounding with a scale per row).  The chain has its SM to itself (k_trsv_inv).  The
+// weights of the next step are
 // loaded into registers while the current step runs; c_i (entries tagged with the solve's epoch by
 // the final tasks) is loaded a step ahead and taken entry by entry once its tags match, so a step
 // waits on no flag.  x_{i-1}, x_i live in a ring of three 128 x 8 buffers; one barrier per step,
@@ -514,12 +552,12 @@ constexpr int kChainBlockHalves = kIb * kIb;  // 16,384 halves (32 KB) per block
 // output for this triangle; cslot: the tagged c slots [nblk][128][8].
 template <bool LOWER>
 __device__ void chain_run(const float* __restrict__ Wt, int n, int nblk, float* Y, long ldy, int nrhs, unsigned* flags,
-                          unsigned epoch, int* status, const unsigned long long* cslot, float* xb0, float* xb1,
-                          float* xb2) {
+                          unsigned epoch, int* status, const unsigned long long* cslot, unsigned long long* xt,
+                          float* xb0, float* xb1, float* xb2) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
   const __half* Wh = reinterpret_cast<const __half*>(Wt);
   const __half* Vh = Wh + (size_t)nblk * kChainBlockHalves;
-  const float* scales = Wt + (size_t)nblk * kChainBlockHalves;  // W's scales [nblk], then V's
+  const float* scales = Wt + ChainLayout::wscale_off(nblk);  // row scales: W's [nblk][128], then V's
   auto bl = [&](int ii) { return LOWER ? ii : nblk - 1 - ii; };
   auto xbuf = [&](int k) { return k == 0 ? xb0 : (k == 1 ? xb1 : xb2); };
   uint4 aw[8], av[8];  // this lane's fragments of W_i and V_{i+1} (FP16, two k-steps per uint4)
@@ -538,52 +576,68 @@ __device__ void chain_run(const float* __restrict__ Wt, int n, int nblk, float* 
     cv[3] = ld_relaxed_u64(p + rb * kIrhs + n0 + 1);
   };
   for (int e = tid; e < kIb * kIrhs; e += 256) xb2[e] = 0.f;  // x_{-1}
+  // row scales of this lane's rows ra, rb: W_i's (swa, swb) and V_{i+1}'s (sva, svb)
+  auto wsc = [&](int ii, int r) { return scales[(size_t)bl(ii) * kIb + r]; };
+  auto vsc = [&](int ii, int r) { return scales[((size_t)nblk + bl(ii)) * kIb + r]; };
   load_frags(aw, Wh, 0);
-  float sw = scales[bl(0)], sv = 0.f;
+  float swa = wsc(0, ra), swb = wsc(0, rb), sva = 0.f, svb = 0.f;
   if (nblk > 1) {
     load_frags(av, Vh, 1);
-    sv = scales[nblk + bl(1)];
+    sva = vsc(1, ra);
+    svb = vsc(1, rb);
   }
   load_c(0);
+  if (tid == 0) {
+    for (int ii = 1; ii < 4 && ii < nblk; ++ii) prefetch_l2(Wh + (size_t)bl(ii) * kChainBlockHalves, kChainBlockHalves * 2);
+    for (int ii = 2; ii < 5 && ii < nblk; ++ii) prefetch_l2(Vh + (size_t)bl(ii) * kChainBlockHalves, kChainBlockHalves * 2);
+  }
   float pc[4] = {0.f, 0.f, 0.f, 0.f};  // sv_i V_i x_{i-2}, this lane's D fragment
   __syncthreads();
   for (int i = 0; i < nblk; ++i) {
     const int blk = bl(i), r0 = blk * kIb, nr = min(kIb, n - r0);
     const float* xp = xbuf((i + 2) % 3);  // x_{i-1}
-    float dw[4] = {0.f, 0.f, 0.f, 0.f}, dw2[4] = {0.f, 0.f, 0.f, 0.f};
-    float dv[4] = {0.f, 0.f, 0.f, 0.f}, dv2[4] = {0.f, 0.f, 0.f, 0.f};
+    // two independent accumulators per product (the two k-steps of a 16-byte fragment load into
+    // m & 1)
+    float dw[2][4], dv[2][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dw[a][j] = dv[a][j] = 0.f;
 #pragma unroll
     for (int m = 0; m < 8; ++m)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int k = 16 * m + 8 * h + t;
-        const float x0 = xp[k * kIrhs + g], x1 = xp[(k + 4) * kIrhs + g];
-        const unsigned h0 = to_tf32(x0), h1 = to_tf32(x1);
-        const unsigned l0 = to_tf32(x0 - __uint_as_float(h0)), l1 = to_tf32(x1 - __uint_as_float(h1));
+        const unsigned h0 = to_tf32(xp[k * kIrhs + g]), h1 = to_tf32(xp[(k + 4) * kIrhs + g]);
         const unsigned pw0 = h ? aw[m].z : aw[m].x, pw1 = h ? aw[m].w : aw[m].y;
         const unsigned pv0 = h ? av[m].z : av[m].x, pv1 = h ? av[m].w : av[m].y;
         const float2 w01 = __half22float2(*reinterpret_cast<const __half2*>(&pw0));
         const float2 w23 = __half22float2(*reinterpret_cast<const __half2*>(&pw1));
         const float2 v01 = __half22float2(*reinterpret_cast<const __half2*>(&pv0));
         const float2 v23 = __half22float2(*reinterpret_cast<const __half2*>(&pv1));
-        mma_tf32(dw, __float_as_uint(w01.x), __float_as_uint(w01.y), __float_as_uint(w23.x), __float_as_uint(w23.y), h0,
-                 h1);
-        mma_tf32(dw2, __float_as_uint(w01.x), __float_as_uint(w01.y), __float_as_uint(w23.x), __float_as_uint(w23.y),
-                 l0, l1);
-        mma_tf32(dv, __float_as_uint(v01.x), __float_as_uint(v01.y), __float_as_uint(v23.x), __float_as_uint(v23.y), h0,
-                 h1);
-        mma_tf32(dv2, __float_as_uint(v01.x), __float_as_uint(v01.y), __float_as_uint(v23.x), __float_as_uint(v23.y),
-                 l0, l1);
+        const int a = m & 1;
+        mma_tf32(dw[a], __float_as_uint(w01.x), __float_as_uint(w01.y), __float_as_uint(w23.x), __float_as_uint(w23.y),
+                 h0, h1);
+        mma_tf32(dv[a], __float_as_uint(v01.x), __float_as_uint(v01.y), __float_as_uint(v23.x), __float_as_uint(v23.y),
+                 h0, h1);
       }
-    const float sw_i = sw, sv_next = sv;
+    float pw[4], pv[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      pw[j] = dw[0][j] + dw[1][j];
+      pv[j] = dv[0][j] + dv[1][j];
+    }
+    const float swa_i = swa, swb_i = swb, sva_n = sva, svb_n = svb;
     // the next step's weights, into the registers just read
     if (i + 1 < nblk) {
       load_frags(aw, Wh, i + 1);
-      sw = scales[bl(i + 1)];
+      swa = wsc(i + 1, ra);
+      swb = wsc(i + 1, rb);
     }
     if (i + 2 < nblk) {
       load_frags(av, Vh, i + 2);
-      sv = scales[nblk + bl(i + 2)];
+      sva = vsc(i + 2, ra);
+      svb = vsc(i + 2, rb);
     }
     // c_i: every entry must carry this solve's epoch (reloaded until it does, bounded)
     int fail = 0;
@@ -605,7 +659,7 @@ __device__ void chain_run(const float* __restrict__ Wt, int n, int nblk, float* 
     }
     float x[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) x[j] = __uint_as_float((unsigned)cv[j]) - pc[j] - sw_i * (dw[j] + dw2[j]);
+    for (int j = 0; j < 4; ++j) x[j] = __uint_as_float((unsigned)cv[j]) - pc[j] - (j < 2 ? swa_i : swb_i) * pw[j];
     float* xo = xbuf(i % 3);
     *reinterpret_cast<float2*>(xo + ra * kIrhs + n0) = make_float2(x[0], x[1]);
     *reinterpret_cast<float2*>(xo + rb * kIrhs + n0) = make_float2(x[2], x[3]);
@@ -617,15 +671,324 @@ __device__ void chain_run(const float* __restrict__ Wt, int n, int nblk, float* 
       if (n0 < nrhs) Y[(size_t)n0 * ldy + r0 + rb] = x[2];
       if (n0 + 1 < nrhs) Y[(size_t)(n0 + 1) * ldy + r0 + rb] = x[3];
     }
+    {
+      // the tagged copy the tasks read (every entry of the block, zeros included)
+      unsigned long long* xq = xt + (size_t)blk * kIb * kIrhs;
+      const unsigned long long tag = (unsigned long long)epoch << 32;
+      st_relaxed_u64(xq + ra * kIrhs + n0, tag | __float_as_uint(x[0]));
+      st_relaxed_u64(xq + ra * kIrhs + n0 + 1, tag | __float_as_uint(x[1]));
+      st_relaxed_u64(xq + rb * kIrhs + n0, tag | __float_as_uint(x[2]));
+      st_relaxed_u64(xq + rb * kIrhs + n0 + 1, tag | __float_as_uint(x[3]));
+    }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) pc[j] = sv_next * (dv[j] + dv2[j]);
+    for (int j = 0; j < 4; ++j) pc[j] = (j < 2 ? sva_n : svb_n) * pv[j];
     if (i + 1 < nblk) load_c(i + 1);
-    // x_i complete in shared memory and in Y; x_{i-1}'s buffer free for x_{i+2}
+    // x_i complete in shared memory, in Y and in the tagged copy; x_{i-1}'s buffer free for x_{i+2}
     if (__syncthreads_or(fail)) {
       if (tid == 0) atomicExch(status, (int)kWaitTimeout);
       return;
     }
-    if (tid == 0) st_release_u32(flags + blk, epoch);
+    if (tid == 0) {
+      // the flag is a hint (the tasks check the tags of what they read), so no fence
+      st_relaxed_u32(flags + blk, epoch);
+      // the weights four steps ahead into L2 (each is read once per sweep, from HBM otherwise)
+      if (i + 4 < nblk) prefetch_l2(Wh + (size_t)bl(i + 4) * kChainBlockHalves, kChainBlockHalves * 2);
+      if (i + 5 < nblk) prefetch_l2(Vh + (size_t)bl(i + 5) * kChainBlockHalves, kChainBlockHalves * 2);
+    }
+  }
+}
+
+// This lane's product of a 128 x 128 FP16 block (fragments fr, chain_frag_off order) with x
+// (128 x 8, row-major in shared memory), x rounded to TF32 (the block itself carries FP16 rounding):
+// d = M x (unscaled).  Four independent accumulators (k-step s into s & 3).
+__device__ __forceinline__ void block_mma(const uint4 (&fr)[8], const float* xs, float (&d)[4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float da[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) da[a][j] = 0.f;
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = 16 * m + 8 * h + t;
+      const unsigned h0 = to_tf32(xs[k * kIrhs + g]), h1 = to_tf32(xs[(k + 4) * kIrhs + g]);
+      const unsigned p0 = h ? fr[m].z : fr[m].x, p1 = h ? fr[m].w : fr[m].y;
+      const float2 a01 = __half22float2(*reinterpret_cast<const __half2*>(&p0));
+      const float2 a23 = __half22float2(*reinterpret_cast<const __half2*>(&p1));
+      mma_tf32(da[(2 * m + h) & 3], __float_as_uint(a01.x), __float_as_uint(a01.y), __float_as_uint(a23.x),
+               __float_as_uint(a23.y), h0, h1);
+    }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) d[j] = (da[0][j] + da[1][j]) + (da[2][j] + da[3][j]);
+}
+
+// The tasks of the FP32 preconditioner's chained triangle, run by every CTA but the chain's (the
+// task list and its order as in k_trsv_inv).  The off-diagonal blocks come from the triangle's FP16
+// copy (ChainLayout, k_pblocks32) and are multiplied on the tensor cores, x rounded to TF32.  Warp w,
+// lane 4 g + t owns rows ra = 16 w + g and rb = ra + 8, right-hand sides 2t and 2t + 1 of its block
+// row (the D fragment).
+//   partial task: its blocks stream through a ring of kRing 32 KB stages (asynchronous copies
+//     issued kRing - 1 blocks ahead, evict-first); each block's x goes to shared memory once its
+//     flag is set; the sum into the task's slot, then the slot's flag.
+//   final task: b and the slots (far ones first; the nearest covers blocks up to i-6, so all are in
+//     before the final blocks' x), e = D_i^-1 (b - sum) with three TF32 products per k-step (D and
+//     the sum both split: FP32-accurate), then c_i = e - sum_{l=3..5} (D_i^-1 L_{i,i-l}) x_{i-l}
+//     through the lag weights (chain_weights32), each term as soon as its x is set: after x_{i-3}
+//     only one 128 x 128 x 8 product remains.  c_i goes to the c slot, each entry tagged with the
+//     solve's epoch.
+// s_x, s_y2: 128 x 8 floats each; s_dyn: kRing x 32 KB (the ring, or D^-1 with column stride 136).
+template <bool LOWER>
+__device__ void chain_tasks(const float* __restrict__ Wt, const float* __restrict__ DI, int n, int nblk,
+                            const float* Y, long ldy, int nrhs, const unsigned* flags, unsigned* ticket,
+                            unsigned epoch, int* status, unsigned* pflags, float* part, int smax,
+                            const int4* __restrict__ tasks, int ntasks, unsigned long long* cslot,
+                            const unsigned long long* xt, unsigned char* s_dyn, float* s_x, float* s_y2, int* s_task,
+                            int* s_cnt) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const int ra = 16 * warp + g, rb = ra + 8, n0 = 2 * t;
+  const __half* blocks = reinterpret_cast<const __half*>(Wt + ChainLayout::blocks_off(nblk));
+  const float* bscale = Wt + ChainLayout::bscale_off(nblk);
+  const unsigned long long pol = l2_evict_first();  // the factor and D^-1 are read once per sweep
+  // x of block jb from the chain's tagged copy into this thread's four entries of the 128 x 8
+  // row-major tile; true when all four carry this solve's epoch
+  auto fetch_x = [&](int jb, float (&xr)[4]) {
+    const unsigned long long* p = xt + (size_t)jb * kIb * kIrhs + tid;
+    bool ok = true;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const unsigned long long v = ld_relaxed_u64(p + 256 * e);
+      ok = ok && (unsigned)(v >> 32) == epoch;
+      xr[e] = __uint_as_float((unsigned)v);
+    }
+    return ok;
+  };
+  // every thread's entries valid (refetched until they are, bounded); a barrier of the whole CTA
+  auto settle_x = [&](int jb, float (&xr)[4], bool ok) {
+    unsigned spins = 0;
+    while (!__syncthreads_and(ok)) {
+      if (++spins > c_spin_limit) {
+        if (tid == 0) atomicExch(status, (int)kWaitTimeout);
+        return false;
+      }
+      __nanosleep(64);
+      if (!ok) ok = fetch_x(jb, xr);
+    }
+    return true;
+  };
+  auto wait_x = [&](int jb, int blk) {
+    return LOWER ? wait_ready(flags, jb, +1, 0, blk, epoch, status, s_cnt)
+                 : wait_ready(flags, jb, -1, blk + 1, nblk, epoch, status, s_cnt);
+  };
+  for (;;) {
+    if (tid == 0) {
+      const unsigned tk_ = atomicAdd(ticket, 1u);
+      const int4 tk = tk_ < (unsigned)ntasks ? tasks[tk_] : make_int4(0, -1, 0, 0);
+      s_task[0] = tk.x;
+      s_task[1] = tk.y;
+      s_task[2] = tk.z;
+      s_task[3] = tk.w;
+    }
+    __syncthreads();
+    const int code = s_task[0], i = s_task[1], q0 = s_task[2], q1 = s_task[3];
+    if (i < 0) return;
+    const int blk = LOWER ? i : nblk - 1 - i;
+    const int r0 = blk * kIb, nr = min(kIb, n - r0);
+    const size_t tri = (size_t)i * (i - 1) / 2;  // the first block of q-row i in the copy
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    if (code >= 0) {
+      // partial task: blocks [q0, q1) through the ring (stage st = block q0 + st)
+      const int nst = q1 - q0;
+      uint4* ring = reinterpret_cast<uint4*>(s_dyn);
+      auto issue = [&](int st) {
+        if (st < nst) {
+          const uint4* src = reinterpret_cast<const uint4*>(blocks + (tri + q0 + st) * kChainBlockHalves);
+          uint4* dst = ring + (st % kRing) * (kChainBlockHalves / 8);
+          for (int e = tid; e < kChainBlockHalves / 8; e += 256) cp_async16z(dst + e, src + e, 16, pol);
+        }
+        cp_async_commit();
+      };
+#pragma unroll
+      for (int st = 0; st < kRing - 1; ++st) issue(st);
+      int confirmed = q0;
+      bool have_x = false, xok = false;  // xr already holds the x of block q0 + st (all valid: xok)
+      float xr[4];
+      for (int st = 0; st < nst; ++st) {
+        const int q = q0 + st, jb = LOWER ? q : nblk - 1 - q;
+        if (q >= confirmed) {
+          const int c = wait_x(jb, blk);
+          if (c == 0) {
+            cp_async_wait_all();
+            return;
+          }
+          confirmed = q + c;
+        }
+        if (!have_x) xok = fetch_x(jb, xr);
+        cp_async_wait_group<kRing - 2>();
+        // x valid everywhere and stage st in for every thread; nobody reads the previous stage or x
+        // any more
+        if (!settle_x(jb, xr, xok)) {
+          cp_async_wait_all();
+          return;
+        }
+        issue(st + kRing - 1);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) s_x[tid + 256 * e] = xr[e];
+        __syncthreads();
+        have_x = q + 1 < q1 && q + 1 < confirmed;
+        if (have_x) xok = fetch_x(LOWER ? q + 1 : nblk - 2 - q, xr);  // the next block's x, its flag seen
+        uint4 fr[8];
+        const uint4* sp = ring + (st % kRing) * (kChainBlockHalves / 8) + warp * 256 + lane;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) fr[m] = sp[m * 32];
+        float d[4];
+        block_mma(fr, s_x, d);
+        const float sca = bscale[(tri + q) * kIb + ra], scb = bscale[(tri + q) * kIb + rb];
+        acc[0] -= sca * d[0];
+        acc[1] -= sca * d[1];
+        acc[2] -= scb * d[2];
+        acc[3] -= scb * d[3];
+      }
+      float* slot = part + ((size_t)i * smax + code) * kIb * kIrhs;
+      *reinterpret_cast<float2*>(slot + ra * kIrhs + n0) = make_float2(acc[0], acc[1]);
+      *reinterpret_cast<float2*>(slot + rb * kIrhs + n0) = make_float2(acc[2], acc[3]);
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        st_release_u32(pflags + (size_t)i * smax + code, epoch);
+      }
+      continue;
+    }
+    // final task.  Before any wait: D^-1 into shared memory (column stride 136), b, and the first
+    // lag weight's fragments
+    float* sd = reinterpret_cast<float*>(s_dyn);
+    {
+      const float* dblk = DI + (size_t)blk * kIb * kIb;
+      for (int e = tid; e < kIb * kIb / 4; e += 256) {
+        const int c = e >> 5, r4 = (e & 31) * 4;
+        cp_async16z(sd + c * 136 + r4, dblk + c * kIb + r4, 16, pol);
+      }
+      cp_async_commit();
+    }
+    acc[0] = (ra < nr && n0 < nrhs) ? Y[(size_t)n0 * ldy + r0 + ra] : 0.f;
+    acc[1] = (ra < nr && n0 + 1 < nrhs) ? Y[(size_t)(n0 + 1) * ldy + r0 + ra] : 0.f;
+    acc[2] = (rb < nr && n0 < nrhs) ? Y[(size_t)n0 * ldy + r0 + rb] : 0.f;
+    acc[3] = (rb < nr && n0 + 1 < nrhs) ? Y[(size_t)(n0 + 1) * ldy + r0 + rb] : 0.f;
+    // the weight D_i^-1 L_{i,q} of q-block q (lag i - q) of this block row: fragments and row scales
+    uint4 fr[8];
+    float swa = 0.f, swb = 0.f;
+    auto load_weight = [&](int q) {
+      const size_t wb = (size_t)(i - q - 1) * nblk + blk;
+      const uint4* p = reinterpret_cast<const uint4*>(reinterpret_cast<const __half*>(Wt) + wb * kChainBlockHalves) +
+                       warp * 256 + lane;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) fr[m] = __ldg(p + m * 32);
+      swa = Wt[ChainLayout::wscale_off(nblk) + wb * kIb + ra];
+      swb = Wt[ChainLayout::wscale_off(nblk) + wb * kIb + rb];
+    };
+    if (q0 < q1) load_weight(q0);
+    // the slots: [2, nparts) in batches of up to eight from the top, each added once all its slots
+    // are in, then slot 1 and slot 0 (all ready before the final blocks' x).  The order of the sum is
+    // fixed.
+    const int nparts = -1 - code;
+    const unsigned* pf = pflags + (size_t)i * smax;
+    const float* ps = part + (size_t)i * smax * kIb * kIrhs;
+    for (int hi = nparts; hi > 2; hi -= 8) {
+      const int lo = max(2, hi - 8);
+      if (!wait_all(pf, lo, hi, epoch, status, s_cnt)) {
+        cp_async_wait_all();
+        return;
+      }
+      float2 va[8], vb[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int sp = lo + u;
+        va[u] = sp < hi ? __ldcg(reinterpret_cast<const float2*>(ps + (size_t)sp * kIb * kIrhs + ra * kIrhs + n0))
+                        : make_float2(0.f, 0.f);
+        vb[u] = sp < hi ? __ldcg(reinterpret_cast<const float2*>(ps + (size_t)sp * kIb * kIrhs + rb * kIrhs + n0))
+                        : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        acc[0] += va[u].x;
+        acc[1] += va[u].y;
+        acc[2] += vb[u].x;
+        acc[3] += vb[u].y;
+      }
+    }
+    for (int sp = min(nparts, 2) - 1; sp >= 0; --sp) {
+      if (!wait_all(pf, sp, sp + 1, epoch, status, s_cnt)) {
+        cp_async_wait_all();
+        return;
+      }
+      const float2 a = __ldcg(reinterpret_cast<const float2*>(ps + (size_t)sp * kIb * kIrhs + ra * kIrhs + n0));
+      const float2 b = __ldcg(reinterpret_cast<const float2*>(ps + (size_t)sp * kIb * kIrhs + rb * kIrhs + n0));
+      acc[0] += a.x;
+      acc[1] += a.y;
+      acc[2] += b.x;
+      acc[3] += b.y;
+    }
+    // e = D^-1 (b - sum): three TF32 products per k-step (D and the sum both split: FP32-accurate),
+    // four independent accumulators (k-step s into s & 3)
+    *reinterpret_cast<float2*>(s_y2 + ra * kIrhs + n0) = make_float2(acc[0], acc[1]);
+    *reinterpret_cast<float2*>(s_y2 + rb * kIrhs + n0) = make_float2(acc[2], acc[3]);
+    cp_async_wait_all();
+    __syncthreads();
+    float ca[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) ca[a][j] = 0.f;
+#pragma unroll
+    for (int s = 0; s < kIb / 8; ++s) {
+      const int k = 8 * s + t;
+      const float a0 = sd[k * 136 + ra], a1 = sd[k * 136 + rb], a2 = sd[(k + 4) * 136 + ra], a3 = sd[(k + 4) * 136 + rb];
+      const unsigned ah0 = to_tf32(a0), ah1 = to_tf32(a1), ah2 = to_tf32(a2), ah3 = to_tf32(a3);
+      const unsigned al0 = to_tf32(a0 - __uint_as_float(ah0)), al1 = to_tf32(a1 - __uint_as_float(ah1));
+      const unsigned al2 = to_tf32(a2 - __uint_as_float(ah2)), al3 = to_tf32(a3 - __uint_as_float(ah3));
+      const float y0 = s_y2[k * kIrhs + g], y1 = s_y2[(k + 4) * kIrhs + g];
+      const unsigned yh0 = to_tf32(y0), yh1 = to_tf32(y1);
+      const unsigned yl0 = to_tf32(y0 - __uint_as_float(yh0)), yl1 = to_tf32(y1 - __uint_as_float(yh1));
+      mma_tf32(ca[s & 3], al0, al1, al2, al3, yh0, yh1);
+      mma_tf32(ca[s & 3], ah0, ah1, ah2, ah3, yl0, yl1);
+      mma_tf32(ca[s & 3], ah0, ah1, ah2, ah3, yh0, yh1);
+    }
+    float cc[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cc[j] = (ca[0][j] + ca[1][j]) + (ca[2][j] + ca[3][j]);
+    // c_i = e - sum over the final blocks q of D_i^-1 L_{i,q} x_q, each as soon as x_q is set (the
+    // next weight's fragments loaded after each product)
+    for (int q = q0; q < q1; ++q) {
+      const int jb = LOWER ? q : nblk - 1 - q;
+      float xr[4];
+      // x_q polled in the tagged copy itself (no flag); settle_x's barriers also end every read of
+      // s_x and s_y2
+      if (!settle_x(jb, xr, fetch_x(jb, xr))) {
+        cp_async_wait_all();
+        return;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; ++e) s_x[tid + 256 * e] = xr[e];
+      __syncthreads();
+      float d[4];
+      block_mma(fr, s_x, d);
+      cc[0] -= swa * d[0];
+      cc[1] -= swa * d[1];
+      cc[2] -= swb * d[2];
+      cc[3] -= swb * d[3];
+      if (q + 1 < q1) load_weight(q + 1);
+    }
+    // c_i, row-major 128 x 8, zero beyond nr and nrhs, each entry tagged with the solve's epoch in
+    // its upper 32 bits (the chain takes the entries once their tags match; no flag)
+    unsigned long long* cp = cslot + (size_t)i * kIb * kIrhs;
+    const unsigned long long tag = (unsigned long long)epoch << 32;
+    st_relaxed_u64(cp + ra * kIrhs + n0, tag | __float_as_uint((ra < nr && n0 < nrhs) ? cc[0] : 0.f));
+    st_relaxed_u64(cp + ra * kIrhs + n0 + 1, tag | __float_as_uint((ra < nr && n0 + 1 < nrhs) ? cc[1] : 0.f));
+    st_relaxed_u64(cp + rb * kIrhs + n0, tag | __float_as_uint((rb < nr && n0 < nrhs) ? cc[2] : 0.f));
+    st_relaxed_u64(cp + rb * kIrhs + n0 + 1, tag | __float_as_uint((rb < nr && n0 + 1 < nrhs) ? cc[3] : 0.f));
+    // s_y2, s_x and D^-1 are read: the next task may overwrite them
+    __syncthreads();
   }
 }
 
@@ -636,8 +999,9 @@ __device__ void chain_run(const float* __restrict__ Wt, int n, int nblk, float* 
 //     x_i = c_i - W_i x_{i-1} - V_i x_{i-2},   W_i = D_i^-1 L_{i,i-1},  V_i = D_i^-1 L_{i,i-2}
 // (chain_weights32, once per factorisation), and releases flags[i] for the tasks that need x_i.
 // A row's hand-off through global memory (final task, c_i, chain) thus has three chain steps to
-// arrive in instead of two.  All CTAs of the grid are resident (the grid is sized by occupancy), so
-// CTA 0 always runs.
+// arrive in instead of two.  The other CTAs run chain_tasks (the factor's blocks from an FP16 copy,
+// products on the tensor cores).  All CTAs of the grid are resident (a cooperative launch), so CTA 0
+// always runs.
 template <typename F, typename FI, bool LOWER, bool TRANS = false, typename V = double, bool CHAIN = false>
 __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const F* __restrict__ LU, long lda, const FI* __restrict__ DI, int n,
                                                   V* Y, long ldy, int nrhs, unsigned* flags, unsigned* ticket,
@@ -654,11 +1018,38 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
   const int nblk = (n + kIb - 1) / kIb;
   const int tid = threadIdx.x, row = tid & (kIb - 1), half = tid >> 7;
   if constexpr (CHAIN) {
+    // the chain's SM is left to the chain: CTA 0 publishes its SM (tagged with the epoch, after the
+    // c slots) and a task CTA on the same SM leaves at once (if the tag does not show up within the
+    // wait limit, the CTA simply takes tasks)
+    unsigned long long* chain_sm = cslot + (size_t)nblk * kIb * kIrhs;
+    unsigned long long* xt = chain_sm + 32;  // the chain's tagged copy of x, [nblk][128][8]
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;\n" : "=r"(smid));
+    if (blockIdx.x != 0) {
+      if (tid == 0) {
+        unsigned spins = 0;
+        unsigned long long v = ld_relaxed_u64(chain_sm);
+        while ((unsigned)(v >> 32) != epoch && ++spins <= c_spin_limit) {
+          __nanosleep(64);
+          v = ld_relaxed_u64(chain_sm);
+        }
+        s_cnt = (unsigned)(v >> 32) == epoch && (unsigned)v == smid;
+      }
+      __syncthreads();
+      if (s_cnt) return;
+    } else if (tid == 0) {
+      st_relaxed_u64(chain_sm, ((unsigned long long)epoch << 32) | smid);
+    }
     if (blockIdx.x == 0) {
       chain_run<LOWER>(reinterpret_cast<const float*>(W), n, nblk, reinterpret_cast<float*>(Y), ldy, nrhs, flags, epoch,
-                       status, cslot, &s_acc[0][0][0], &s_acc[1][0][0], &s_y[0][0]);
-      return;
+                       status, cslot, xt, &s_acc[0][0][0], &s_acc[1][0][0], &s_y[0][0]);
+    } else {
+      chain_tasks<LOWER>(reinterpret_cast<const float*>(W), reinterpret_cast<const float*>(DI), n, nblk,
+                         reinterpret_cast<const float*>(Y), ldy, nrhs, flags, ticket, epoch, status, pflags,
+                         reinterpret_cast<float*>(part), smax, tasks, ntasks, cslot, xt, s_dyn, &s_y[0][0],
+                         &s_b[0][0], s_task, &s_cnt);
     }
+    return;
   }
   // The FP32 factor's partial tasks (column-major blocks, 8 right-hand sides) stream through a ring
   // of kRing stages in s_dyn, each 64 columns x 128 rows of a block (32 KB), filled by asynchronous
@@ -716,42 +1107,39 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
         load_lv(q0);
         lv_ready = true;
       }
-      // the partial sums of this row: the far chunks' slots 1 .. nparts-1 (ready first) as soon as
-      // they are all in, half 0 adding [1, mid) and half 1 [mid, nparts), four slots' loads in
-      // flight at a time; then slot 0 (the chunk next to the final blocks, ready last) by half 0.
-      // The order of the sum is fixed.
+      // the partial sums of this row, far chunks first (ready long before): slots [2, nparts) in
+      // batches of up to eight from the top, each added once all of its slots are in, half 0 taking
+      // a batch's even and half 1 its odd offsets; then slot 1 (half 1).  Slot 0, the chunk next to
+      // the final blocks and ready last, is added after the final blocks' product.  The order of the
+      // sum is fixed.
       const int nparts = -1 - code;
       const unsigned* pf = pflags + (size_t)i * smax;
       const V* p = part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs;
-      if (!wait_all(pf, 1, nparts, epoch, status, &s_cnt)) {
-        cp_async_wait_all();
-        return;
-      }
-      {
-        const int mid = 1 + nparts / 2, s1 = half ? nparts : mid;
-        int sp = half ? mid : 1;
-        for (; sp + 4 <= s1; sp += 4) {
-          V t[4][kIrhs];
-#pragma unroll
-          for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int r = 0; r < kIrhs; ++r) t[u][r] = __ldcg(p + (size_t)(sp + u) * kIb * kIrhs + r);
-#pragma unroll
-          for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int r = 0; r < kIrhs; ++r) acc[r] += t[u][r];
+      for (int hi = nparts; hi > 2; hi -= 8) {
+        const int lo = max(2, hi - 8);
+        if (!wait_all(pf, lo, hi, epoch, status, &s_cnt)) {
+          cp_async_wait_all();
+          return;
         }
-        for (; sp < s1; ++sp)
+        V t[4][kIrhs];
 #pragma unroll
-          for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + (size_t)sp * kIb * kIrhs + r);
+        for (int u = 0; u < 4; ++u) {
+          const int sp = lo + half + 2 * u;
+#pragma unroll
+          for (int r = 0; r < kIrhs; ++r) t[u][r] = sp < hi ? __ldcg(p + (size_t)sp * kIb * kIrhs + r) : (V)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int r = 0; r < kIrhs; ++r) acc[r] += t[u][r];
       }
-      if (!wait_all(pf, 0, min(nparts, 1), epoch, status, &s_cnt)) {
+      if (!wait_all(pf, 1, min(nparts, 2), epoch, status, &s_cnt)) {
         cp_async_wait_all();
         return;
       }
-      if (nparts > 0 && half == 0)
+      if (nparts > 1 && half == 1)
 #pragma unroll
-        for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + r);
+        for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(p + (size_t)kIb * kIrhs + r);
     }
     if constexpr (kRingPath) {
       if (!fin) {
@@ -759,6 +1147,7 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
         // ring + (st % kRing) * 8192; rows beyond nr and columns beyond n zero-filled
         float* ring = reinterpret_cast<float*>(s_dyn);
         const int nst = 2 * (q1 - q0);
+        const unsigned long long pol = l2_evict_first();  // the factor is read once per sweep
         auto issue = [&](int st) {
           if (st < nst) {
             const int jb = LOWER ? q0 + (st >> 1) : nblk - 1 - q0 - (st >> 1);
@@ -769,13 +1158,13 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
               for (int e = tid; e < 64 * kIb / 4; e += 256) {
                 const int c = e >> 5, rr = (e & 31) * 4;
                 const int ok = c < ncs ? max(0, min(4, nr - rr)) : 0;
-                cp_async16z(dst + c * kIb + rr, ok ? src + (size_t)(cs + c) * lda + r0 + rr : src, ok * 4);
+                cp_async16z(dst + c * kIb + rr, ok ? src + (size_t)(cs + c) * lda + r0 + rr : src, ok * 4, pol);
               }
             } else {
               for (int e = tid; e < 64 * kIb; e += 256) {
                 const int c = e >> 7, rr = e & 127;
                 const bool ok = c < ncs && rr < nr;
-                cp_async4z(dst + c * kIb + rr, ok ? src + (size_t)(cs + c) * lda + r0 + rr : src, ok ? 4 : 0);
+                cp_async4z(dst + c * kIb + rr, ok ? src + (size_t)(cs + c) * lda + r0 + rr : src, ok ? 4 : 0, pol);
               }
             }
           }
@@ -923,6 +1312,17 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
       }
       have_x = pre;
     }
+    if (fin) {
+      // slot 0 (see above)
+      const int nparts = -1 - code;
+      if (!wait_all(pflags + (size_t)i * smax, 0, min(nparts, 1), epoch, status, &s_cnt)) {
+        cp_async_wait_all();
+        return;
+      }
+      if (nparts > 0 && half == 0)
+#pragma unroll
+        for (int r = 0; r < kIrhs; ++r) acc[r] += __ldcg(part + (size_t)i * smax * kIb * kIrhs + (size_t)row * kIrhs + r);
+    }
 #pragma unroll
     for (int r = 0; r < kIrhs; ++r) s_acc[half][row][r] = acc[r];
     __syncthreads();
@@ -983,32 +1383,30 @@ __global__ void __launch_bounds__(256, sizeof(F) == 4 ? 2 : 1) k_trsv_inv(const 
   }
 }
 
-// The chain weights of the FP32 preconditioner (see chain_run), one triangle per blockIdx.y, one
-// block row b per blockIdx.x, one lag per blockIdx.z:
-//   lag 1: W_b = D_b^-1 L_{b,b-1} (lower) or D_b^-1 U_{b,b+1} (upper),
-//   lag 2: V_b = D_b^-1 L_{b,b-2} or D_b^-1 U_{b,b+2},
-// each in FP16 scaled by its largest magnitude, in the fragment order of chain_frag_off: W_b's halves
-// from out + b * 8192 floats, V_b's from out + nblk * 8192 + b * 8192 floats; the scales at
-// out + nblk * 16384 + b (W) and + nblk + b (V).  Rows and columns beyond n zero; a missing
-// neighbour gives zeros (scale 1).
+// The chain weights of the FP32 preconditioner (see chain_run, chain_tasks), one triangle per
+// blockIdx.y, one block row b per blockIdx.x, one lag l = 1 + blockIdx.z (1 .. kLags):
+//   D_b^-1 L_{b,b-l} (lower) or D_b^-1 U_{b,b+l} (upper)
+// in FP16 with every row scaled by its largest magnitude, in the fragment order of chain_frag_off
+// (ChainLayout).  Rows and columns beyond n zero; a missing neighbour gives zeros (scales 1).
 __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict__ LU, long lda, int n,
                                                           const float* __restrict__ DL, const float* __restrict__ DU,
                                                           float* __restrict__ WL, float* __restrict__ WU) {
   extern __shared__ __align__(16) float s_w[];
   float* sd = s_w;                  // D^-1 (r, k) at sd[k * 129 + r]
   float* sb = s_w + kIb * (kIb + 1);  // the off-diagonal block (k, c) at sb[c * 129 + k]
-  __shared__ float s_max[8];
+  __shared__ unsigned s_rmax[kIb];  // each row's largest magnitude (FP32 bits)
   const int nblk = (n + kIb - 1) / kIb, b = blockIdx.x, lower = blockIdx.y == 0, lag = 1 + blockIdx.z;
   const int nb = lower ? b - lag : b + lag;  // the neighbouring block column
   float* base = lower ? WL : WU;
   __half* out16 = reinterpret_cast<__half*>(base) + ((size_t)(lag - 1) * nblk + b) * kChainBlockHalves;
-  float* scale = base + (size_t)nblk * kChainBlockHalves + (size_t)(lag - 1) * nblk + b;
+  float* scale = base + ChainLayout::wscale_off(nblk) + ((size_t)(lag - 1) * nblk + b) * kIb;
   const int tid = threadIdx.x;
   if (nb < 0 || nb >= nblk) {
     for (int e = tid; e < kChainBlockHalves; e += 256) out16[e] = __float2half_rn(0.f);
-    if (tid == 0) *scale = 1.f;
+    if (tid < kIb) scale[tid] = 1.f;
     return;
   }
+  if (tid < kIb) s_rmax[tid] = 0u;
   const float* D = (lower ? DL : DU) + (size_t)b * kIb * kIb;
   const int r0 = b * kIb, nr = min(kIb, n - r0), c0 = nb * kIb, nc = min(kIb, n - c0);
   for (int e = tid; e < kIb * kIb; e += 256) {
@@ -1035,27 +1433,84 @@ __global__ void __launch_bounds__(256) k_chain_weights32(const float* __restrict
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * bv[j];
   }
-  float m = 0.f;
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 8; ++i) {
+    float m = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) m = fmaxf(m, fabsf(acc[i][j]));
+    if (rb + i < nr) atomicMax(&s_rmax[rb + i], __float_as_uint(m));  // non-negative: ordered as integers
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const float mx = __uint_as_float(s_rmax[rb + i]), sc = mx > 0.f ? mx : 1.f, inv = 1.f / sc;
 #pragma unroll
     for (int j = 0; j < 8; ++j)
-      if (rb + i < nr) m = fmaxf(m, fabsf(acc[i][j]));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((tid & 31) == 0) s_max[tid >> 5] = m;
-  __syncthreads();
-  float sc = 0.f;
-#pragma unroll
-  for (int w = 0; w < 8; ++w) sc = fmaxf(sc, s_max[w]);
-  sc = sc > 0.f ? sc : 1.f;
-  const float inv = 1.f / sc;
-#pragma unroll
-  for (int j = 0; j < 8; ++j)
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
       out16[chain_frag_off(rb + i, cb + j)] = __float2half_rn((rb + i < nr) ? acc[i][j] * inv : 0.f);
-  if (tid == 0) *scale = sc;
+  }
+  if (tid < kIb) {
+    const float mx = __uint_as_float(s_rmax[tid]);
+    scale[tid] = mx > 0.f ? mx : 1.f;
+  }
+}
+
+// The off-diagonal blocks of both triangles of the FP32 factor LU, copied in FP16 (each row scaled
+// by its largest magnitude) in the chain's fragment order (ChainLayout): block blockIdx.x of
+// triangle blockIdx.y (0: L, into WL; 1: U, into WU).  Rows and columns beyond n zero; an all-zero
+// row gets scale 1.
+__global__ void __launch_bounds__(256) k_pblocks32(const float* __restrict__ LU, long lda, int n, float* __restrict__ WL,
+                                                    float* __restrict__ WU) {
+  extern __shared__ __align__(16) float s_blk[];  // element (r, k) at k * 129 + r
+  __shared__ float s_rm[2][kIb], s_inv[kIb];
+  const int nblk = (n + kIb - 1) / kIb, tid = threadIdx.x;
+  const long idx = blockIdx.x;
+  // q-row i and q-column q of the block: idx = i (i-1) / 2 + q, q < i
+  int i = (int)((1.0 + sqrt(1.0 + 8.0 * (double)idx)) * 0.5);
+  while ((long)i * (i - 1) / 2 > idx) --i;
+  while ((long)(i + 1) * i / 2 <= idx) ++i;
+  const int q = (int)(idx - (long)i * (i - 1) / 2);
+  const bool lower = blockIdx.y == 0;
+  const int blk = lower ? i : nblk - 1 - i, jb = lower ? q : nblk - 1 - q;
+  const int r0 = blk * kIb, nr = min(kIb, n - r0), c0 = jb * kIb, nc = min(kIb, n - c0);
+  for (int e = tid; e < kIb * kIb; e += 256) {
+    const int r = e & (kIb - 1), k = e >> 7;
+    s_blk[k * (kIb + 1) + r] = (r < nr && k < nc) ? LU[(size_t)(c0 + k) * lda + r0 + r] : 0.f;
+  }
+  __syncthreads();
+  {
+    // row r's largest magnitude: thread (r, half) over columns 64 half .. +63
+    const int r = tid & (kIb - 1), h = tid >> 7;
+    float m = 0.f;
+    for (int k = 64 * h; k < 64 * h + 64; ++k) m = fmaxf(m, fabsf(s_blk[k * (kIb + 1) + r]));
+    s_rm[h][r] = m;
+  }
+  __syncthreads();
+  float* base = lower ? WL : WU;
+  if (tid < kIb) {
+    const float mx = fmaxf(s_rm[0][tid], s_rm[1][tid]), sc = mx > 0.f ? mx : 1.f;
+    s_inv[tid] = 1.f / sc;
+    base[ChainLayout::bscale_off(nblk) + (size_t)idx * kIb + tid] = sc;
+  }
+  __syncthreads();
+  uint4* out = reinterpret_cast<uint4*>(base + ChainLayout::blocks_off(nblk)) + (size_t)idx * (kChainBlockHalves / 8);
+  // 16-byte chunk c = halves 8c .. 8c+7: warp w, two k-steps 2m, 2m+1, lane 4g + t (chain_frag_off)
+  for (int c = tid; c < kChainBlockHalves / 8; c += 256) {
+    const int w = c >> 8, mm = (c >> 5) & 7, lane = c & 31, g = lane >> 2, t = lane & 3;
+    unsigned u[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      __half2 h2;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int jj = 2 * p + e, s = 2 * mm + (jj >> 2), j = jj & 3;
+        const int r = 16 * w + g + 8 * (j & 1), k = 8 * s + t + 4 * (j >> 1);
+        const __half h = __float2half_rn(s_blk[k * (kIb + 1) + r] * s_inv[r]);
+        if (e == 0) h2.x = h; else h2.y = h;
+      }
+      u[p] = *reinterpret_cast<unsigned*>(&h2);
+    }
+    out[c] = make_uint4(u[0], u[1], u[2], u[3]);
+  }
 }
 
 // Scratch of the split solves, after the base scratch: the partial sums' ready flags [nblk][smax]
@@ -1068,20 +1523,24 @@ struct SplitScratch {
   static size_t base(int n) { return (TrsvScratch::bytes(n) + 255) / 256 * 256; }
   static size_t part_off(int n) { return base(n) + ((size_t)nblk(n) * smax(n) * 4 + 255) / 256 * 256; }
   static size_t task_off(int n) { return part_off(n) + (size_t)nblk(n) * smax(n) * kIb * kIrhs * sizeof(double); }
-  // the chain's c_i slots (entries tagged with the solve's epoch; zero when allocated)
+  // the chain's c_i slots (entries tagged with the solve's epoch; zero when allocated), the chain
+  // CTA's SM (tagged likewise, in a 256-byte slot) and the chain's tagged copy of x
   static size_t cslot_off(int n) { return (task_off(n) + max_tasks(n) * sizeof(int4) + 255) / 256 * 256; }
-  static size_t bytes(int n) { return cslot_off(n) + (size_t)nblk(n) * kIb * kIrhs * sizeof(unsigned long long); }
+  static size_t bytes(int n) {
+    return cslot_off(n) + ((size_t)nblk(n) * kIb * kIrhs * 2 + 32) * sizeof(unsigned long long);
+  }
 };
 
 // The task list of a triangle with nblk block rows (see k_trsv_inv), built once per size.  chain:
-// the final task of row b does block b-3 only (b-2 and b-1 are the chain's).
+// the final task of row b takes blocks b-5 .. b-3 through the weights D_b^-1 L_{b,b-l} (see
+// chain_tasks; b-2 and b-1 are the chain's), the partial tasks the blocks before b-5.
 const std::vector<int4>& split_tasks(int nblk, bool chain = false) {
   static std::map<int, std::vector<int4>> cache[2];
   auto it = cache[chain].find(nblk);
   if (it != cache[chain].end()) return it->second;
   std::vector<std::vector<int4>> after(nblk);  // partial tasks issued after F(b)
   std::vector<int> nparts(nblk, 0);
-  const int lead = chain ? kLead + 1 : kLead;  // blocks [i - lead, i - (chain ? 2 : 0)) in the final task
+  const int lead = chain ? kLags : kLead;  // blocks [i - lead, i - (chain ? 2 : 0)) in the final task
   for (int i = 0; i < nblk; ++i) {
     int e = i - lead, w = 2, sidx = 0;
     while (e > 0) {
@@ -1318,10 +1777,7 @@ cudaError_t trsv_lu32_inv(const float* LU, long lda, const float* DL, const floa
 
 cudaError_t set_wait_limit(unsigned spins) { return cudaMemcpyToSymbol(c_spin_limit, &spins, sizeof spins); }
 
-size_t chain_weights_elems(int n) {
-  const size_t nblk = (size_t)((n + kIb - 1) / kIb);
-  return nblk * kChainBlockHalves + 2 * nblk;  // W and V (FP16, two halves per float), their scales
-}
+size_t chain_weights_elems(int n) { return ChainLayout::elems((n + kIb - 1) / kIb); }
 
 cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const float* DU, int n, float* WL, float* WU,
                             cudaStream_t s) {
@@ -1333,8 +1789,21 @@ cudaError_t chain_weights32(const float* LU, long lda, const float* DL, const fl
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_chain_weights32<<<dim3((n + kIb - 1) / kIb, 2, 2), 256, smem, s>>>(LU, lda, n, DL, DU, WL, WU);
+  const int nblk = (n + kIb - 1) / kIb;
+  k_chain_weights32<<<dim3(nblk, 2, kLags), 256, smem, s>>>(LU, lda, n, DL, DU, WL, WU);
   BGPU_COUNT_LAUNCH();
+  const size_t nb2 = ChainLayout::nb2(nblk);
+  if (nb2 > 0) {
+    static bool attr_b = false;
+    if (!attr_b) {
+      cudaError_t e = cudaFuncSetAttribute(k_pblocks32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(kIb * (kIb + 1) * sizeof(float)));
+      if (e != cudaSuccess) return e;
+      attr_b = true;
+    }
+    k_pblocks32<<<dim3((unsigned)nb2, 2), 256, kIb * (kIb + 1) * sizeof(float), s>>>(LU, lda, n, WL, WU);
+    BGPU_COUNT_LAUNCH();
+  }
   return cudaGetLastError();
 }
 
