@@ -924,6 +924,54 @@ def star45_record(warmup=1, steps=1, fp64=True):
     return rec
 
 
+def hmatrix_record(big=64, small=32, eps=1e-4):
+    """The path for meshes beyond HBM: the star body at geodesic frequency `big` (64: N = 81,920, order
+    245,760, whose dense FP64 GR would need 483 GB) through BEST's seam, where bhm_build takes the
+    H-matrix path by itself; and at `small` (32: the headline mesh), where the dense paths also run,
+    the H-matrix results against the mixed dense path's.  eps = 1e-4 is BEST's default -he accuracy.
+    Host wall time of bhm_build + bhm_solve (6 RHS, host buffers); the 11-RHS solve for the tensors is
+    untimed."""
+    import torch
+    import best_hydro_b200 as bh
+    from best_hydro_b200 import meshes
+
+    rec = {"eps": eps}
+    for f, prec in ((small, bh.BGPU_HMATRIX), (small, bh.BGPU_MIXED), (big, -1)):
+        tri, ta, tv = meshes.star(f)
+        st = bh.Setup(tri, 0, ta)
+        s = bh.BhmSolver()
+        s.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        x = s.incenters()
+        xmu, gdef = st.deflation(s.diag_mean())
+        bh.set_precision(prec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.build(eps=eps, direct=0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+        t1 = time.perf_counter()
+        s.solve(bh.rhs6(x))
+        t2 = time.perf_counter()
+        bh.set_precision(-1)
+        path = {0: "fp64", 1: "mixed", 2: "hmatrix"}[bh.lib().bgpu_precision()]
+        leg = {"N": st.n, "order": 3 * st.n, "path": path, "build_s": t1 - t0, "solve_s": t2 - t1,
+               "value": t2 - t0, "unit": "s", "dense_fp64_gb": 72.0 * st.n * st.n / 1e9}
+        if path == "hmatrix":
+            hs = bh.hmatrix_stats()
+            leg["hmatrix"] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in hs.items()}
+            leg["stored_gb"] = 8 * (hs["dense_entries"] + hs["lowrank_entries"]) / 1e9
+        t = tensors_of(s, x, st, bh)
+        leg.update(D_t=t["D_t"], D_r=t["D_r"], chiprime=t["chiprime"])
+        rec[f"f{f}_{path}"] = (leg, t)
+        s.destroy()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    out = {k: v[0] for k, v in rec.items() if k != "eps"}
+    hm, mx = rec.get(f"f{small}_hmatrix"), rec.get(f"f{small}_mixed")
+    if hm and mx:
+        out[f"accuracy_f{small}_hmatrix_vs_mixed"] = tensor_errors(hm[1], mx[1])
+    out["eps"] = eps
+    return out
+
+
 def collect_records(args, local_rank, t_start):
     """The other workloads' records in the default run (each guarded; skipped past the time budget)."""
     import torch
@@ -931,7 +979,8 @@ def collect_records(args, local_rank, t_start):
     recs = {}
     for name, fn in (("ellipsoid_series", lambda: series_record(1, 1, local_rank)),
                      ("ellipsoid_adjoint", lambda: adjoint_record(1, 1, fd_vertices=4, fit_steps=0)),
-                     ("star_f45", lambda: star45_record())):
+                     ("star_f45", lambda: star45_record()),
+                     ("star_f64_hmatrix", lambda: hmatrix_record())):
         if time.perf_counter() - t_start > args.records_budget_s:
             recs[name] = {"skipped": f"bench time budget of {args.records_budget_s:.0f} s reached"}
             continue

@@ -25,6 +25,7 @@ LIBPATH = os.path.join(HERE, "lib", "libbestgpu.so")
 
 BGPU_FP64 = 0
 BGPU_MIXED = 1
+BGPU_HMATRIX = 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -88,6 +89,12 @@ _SIGS = {
     "bgpu_prepared_arrays": (ctypes.c_int, [_dp, _dp, _dp, _dp, _ip, _dp, _dp]),
     "bgpu_launch_count": (ctypes.c_ulonglong, []),
     "bgpu_kernel_stats": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, _dp, _dp]),
+    "bgpu_hmatrix_set_options": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "bgpu_hmatrix_stats": (ctypes.c_int, [_dp, ctypes.c_int]),
+    "bgpu_hmatrix_matvec_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_int]),
+    "bgpu_hmatrix_plan": (ctypes.c_int, [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int, _ip, _ip]),
     # include/best_driver.h: BEST's host side around the seam
     "bgpu_best_setup": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, _dp,
                                        _dp, _ip, _ip, _ip, _ip]),
@@ -481,6 +488,39 @@ def set_refinement(max_restarts=8, krylov=10):
 
 def set_precision(mode):
     _check(lib().bgpu_set_precision(int(mode)), "bgpu_set_precision")
+
+
+HMATRIX_STATS = ("n", "leaves", "dense_blocks", "lowrank_blocks", "dense_entries", "lowrank_entries", "mean_rank",
+                 "max_rank", "capped_blocks", "fill_ms", "aca_ms", "precond_ms", "gmres_steps", "relres",
+                 "device_bytes")
+
+
+def hmatrix_set_options(leaf=128, eta=2.0, kmax=90):
+    """bgpu_hmatrix_set_options: leaf size, admissibility and rank cap of later H-matrix builds."""
+    _check(lib().bgpu_hmatrix_set_options(int(leaf), float(eta), int(kmax)), "bgpu_hmatrix_set_options")
+
+
+def hmatrix_stats():
+    """bgpu_hmatrix_stats as a dict (HMATRIX_STATS)."""
+    out = np.zeros(len(HMATRIX_STATS))
+    _check(lib().bgpu_hmatrix_stats(_p(out), len(out)), "bgpu_hmatrix_stats")
+    return dict(zip(HMATRIX_STATS, out.tolist()))
+
+
+def hmatrix_matvec_device(nrhs, d_x, ldx, d_y, ldy):
+    _check(lib().bgpu_hmatrix_matvec_device(int(nrhs), ctypes.c_void_p(d_x), int(ldx), ctypes.c_void_p(d_y),
+                                            int(ldy)), "bgpu_hmatrix_matvec_device")
+
+
+def hmatrix_plan(x, v1, v2, v3, leaf=128, eta=2.0, kmax=90):
+    """bgpu_hmatrix_plan (host only): (perm, {depth, leaves, dense, lowrank, admissible})."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, v1, v2, v3)]
+    n = arrs[0].size // 3
+    perm = np.zeros(n, dtype=np.int32)
+    counts = np.zeros(5, dtype=np.int32)
+    _check(lib().bgpu_hmatrix_plan(n, *(_p(a) for a in arrs), int(leaf), float(eta), int(kmax),
+                                   perm.ctypes.data_as(_ip), counts.ctypes.data_as(_ip)), "bgpu_hmatrix_plan")
+    return perm, dict(zip(("depth", "leaves", "dense", "lowrank", "admissible"), counts.tolist()))
 
 
 def dgetrf_device(n, d_a, lda, d_ipiv):

@@ -27,6 +27,7 @@ SOURCES = [
     ("solve.cu", []),
     ("tc_gemm.cu", []),
     ("mixed.cu", []),
+    ("hmatrix.cu", ["-fmad=false"]),
     ("adjoint.cu", []),
     ("api.cpp", []),
     ("driver.cpp", []),

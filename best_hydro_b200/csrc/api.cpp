@@ -28,6 +28,7 @@
 #include "../../include/best_gpu.h"
 #include "../../include/best_hmatrix.h"
 #include "bgpu_internal.h"
+#include "hmatrix.h"
 #include "mixed.h"
 
 namespace bgpu {
@@ -225,6 +226,7 @@ struct Solver {
   double scal_host[5] = {0, 0, 0, 0, 0};
   DevBuf tri, vset, area, scal, counts, setup_scratch;
   std::unique_ptr<MixedSolver> mixed;
+  std::unique_ptr<HMatrixSolver> hmat;  // the H-matrix path (BGPU_HMATRIX)
   int precision = BGPU_FP64;
   bool factored = false;
   bool fast_ok = true;  // mesh_fast_ok of the mesh
@@ -245,6 +247,11 @@ std::unique_ptr<Solver> g;
 int g_prec_override = -1;
 int g_refine[2] = {8, 10};  // GMRES restarts, Krylov vectors per restart
 double g_solve_info[2] = {0, 0};  // refinement iterations, relative residual of the last solve
+struct HOpts {
+  int leaf = 128;
+  double eta = 2.0;
+  int kmax = 90;
+} g_hm_opts;  // H-matrix settings (bgpu_hmatrix_set_options)
 
 Solver& solver() {
   if (!g) throw std::runtime_error("bhm_create has not been called");
@@ -256,6 +263,7 @@ int precision_for(int direct, int single) {
   if (const char* e = std::getenv("BEST_GPU_PRECISION")) {
     if (!std::strcmp(e, "fp64")) return BGPU_FP64;
     if (!std::strcmp(e, "mixed")) return BGPU_MIXED;
+    if (!std::strcmp(e, "hmatrix")) return BGPU_HMATRIX;
   }
   if (direct && !single) return BGPU_FP64;
   return BGPU_MIXED;
@@ -280,7 +288,16 @@ void solve_device(Solver& s, Runtime& r, int nrhs, double* d_b, long ldb) {
   if (!s.factored) throw std::runtime_error("bhm_build has not factored GR");
   const int n3 = 3 * s.n;
   ck(cudaEventRecord(r.ev[6], r.stream), "event");
-  if (s.precision == BGPU_MIXED && s.mixed) {
+  if (s.precision == BGPU_HMATRIX && s.hmat) {
+    HReport rep{};
+    try {
+      s.hmat->solve(nrhs, d_b, ldb, r.stream, &rep);
+    } catch (const std::runtime_error& e) {
+      throw CudaError(e.what());
+    }
+    g_solve_info[0] = rep.iterations;
+    g_solve_info[1] = rep.relres;
+  } else if (s.precision == BGPU_MIXED && s.mixed) {
     MixedReport rep{};
     // keep the right-hand sides: a failed refinement falls back to the FP64 LU on the same input
     s.rhs_keep.ensure((size_t)n3 * nrhs * sizeof(double), "right-hand sides (copy)");
@@ -466,6 +483,44 @@ int build_common(Solver& s, Runtime& r, double eps, int direct, int single, cons
   const int n = s.n, n3 = 3 * n;
   s.factored = false;
   s.precision = precision_for(direct, single);
+  if (s.precision != BGPU_HMATRIX) {
+    // the dense paths hold the FP64 GR (72 N^2 bytes; the mixed path an FP32 copy beside it):
+    // beyond the free device memory, the H-matrix path takes over (as the reference switches to
+    // its H-matrix for large N, best/best.f:138)
+    size_t fr = 0, tot = 0;
+    ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+    const double need = (s.precision == BGPU_FP64 ? 72.0 : 108.0) * (double)n * n * 1.02 + 5.12e8 - (double)s.gr.bytes;
+    if (need > (double)fr) {
+      note("dense GR of order %d needs %.1f GB, %.1f GB free on the GPU: H-matrix path", n3, need / 1e9, fr / 1e9);
+      s.precision = BGPU_HMATRIX;
+    }
+  }
+  if (s.precision == BGPU_HMATRIX) {
+    s.gr.reset();
+    s.mixed.reset();
+    if (!s.hmat) s.hmat = std::make_unique<HMatrixSolver>();
+    s.hmat->set_options(g_hm_opts.leaf, g_hm_opts.eta, g_hm_opts.kmax);
+    ck(cudaEventRecord(r.ev[2], r.stream), "event");
+    try {
+      s.hmat->build(s.mesh(), defl, defl.ndef, eps, r.stream);
+    } catch (const std::runtime_error& e) {
+      throw CudaError(e.what());
+    }
+    ck(cudaEventRecord(r.ev[5], r.stream), "event");
+    r.sync("bhm_build");
+    const std::vector<double> st = s.hmat->stats();
+    r.ms[1] = st[9] + st[10];
+    r.ms[2] = st[11];
+    r.ms[4] = r.elapsed(2, 5);
+    s.factored = true;
+    note("GPU build: H-matrix of order %d at eps %.0e: %d leaves, %d dense blocks (%.2f GB), %d low-rank blocks "
+         "(%.2f GB, mean rank %.1f, largest %d, %d at the cap), fill %.1f ms, cross approximation %.1f ms, "
+         "block-Jacobi preconditioner %.1f ms",
+         n3, eps, (int)st[1], (int)st[2], st[4] * 8e-9, (int)st[3], st[5] * 8e-9, st[6], (int)st[7], (int)st[8], st[9],
+         st[10], st[11]);
+    return 0;
+  }
+  s.hmat.reset();
   s.ld = padded_ld(n3);
   s.gr.ensure((size_t)s.ld * n3 * sizeof(double), "GR (FP64)");
   ck(cudaEventRecord(r.ev[2], r.stream), "event");
@@ -790,7 +845,10 @@ int bhm_solve(int nrhs, double* b) {
     r.sync("bhm_solve");
     if (s.precision == BGPU_MIXED && s.mixed)
       for (auto& line : s.mixed->profile_report()) note("%s", line.c_str());
-    if (s.precision == BGPU_MIXED && s.mixed)
+    if (s.precision == BGPU_HMATRIX)
+      note("solve: %d right-hand sides by GMRES on the H-matrix, %d steps, relative residual %.1e, %.2f ms", nrhs,
+           (int)g_solve_info[0], g_solve_info[1], r.ms[3]);
+    else if (s.precision == BGPU_MIXED && s.mixed)
       note("solve: %d right-hand sides, %d refinement steps, relative residual %.1e, %.2f ms", nrhs,
           (int)g_solve_info[0], g_solve_info[1], r.ms[3]);
     else
@@ -811,7 +869,7 @@ void bhm_destroy(void) {
 // ---------------------------------------------------------------------------------------------
 
 int bgpu_set_precision(int mode) {
-  if (mode != -1 && mode != BGPU_FP64 && mode != BGPU_MIXED) {
+  if (mode != -1 && mode != BGPU_FP64 && mode != BGPU_MIXED && mode != BGPU_HMATRIX) {
     note("error: unknown precision %d", mode);
     return 1;
   }
@@ -1422,6 +1480,73 @@ int bgpu_best_gradient(int iarea, double truearea, double wm, double* values, do
         "adjoint solve %.1f, pair adjoint %.1f, deflation/area/triangles %.1f, total %.1f ms",
         values[0], values[1], wm > 0 ? "[eta]" : "CHI'", values[2], r.ms[5], hms[0], hms[1] - hms[0], hms[2] - hms[1],
         hms[3] - hms[2], hms[4] - hms[3], hms[5]);
+    return 0;
+  });
+}
+
+int bgpu_hmatrix_set_options(int leaf, double eta, int kmax) {
+  return status_of([&] {
+    HMatrixSolver probe;
+    probe.set_options(leaf, eta, kmax);  // validates
+    g_hm_opts.leaf = leaf;
+    g_hm_opts.eta = eta;
+    g_hm_opts.kmax = kmax;
+    return 0;
+  });
+}
+
+int bgpu_hmatrix_stats(double* out, int len) {
+  return status_of([&] {
+    Solver& s = solver();
+    if (!s.hmat) throw std::runtime_error("bgpu_hmatrix_stats: the last bhm_build did not take the H-matrix path");
+    const std::vector<double> st = s.hmat->stats();
+    for (int i = 0; i < len && i < (int)st.size(); ++i) out[i] = st[i];
+    return 0;
+  });
+}
+
+int bgpu_hmatrix_matvec_device(int nrhs, const double* d_x, int ldx, double* d_y, int ldy) {
+  return status_of([&] {
+    Solver& s = solver();
+    Runtime& r = rt();
+    if (!s.hmat || s.precision != BGPU_HMATRIX)
+      throw std::runtime_error("bgpu_hmatrix_matvec_device: the last bhm_build did not take the H-matrix path");
+    if (nrhs < 0 || ldx < 3 * s.n || ldy < 3 * s.n) throw std::runtime_error("bgpu_hmatrix_matvec_device: bad sizes");
+    try {
+      s.hmat->matvec(nrhs, d_x, ldx, d_y, ldy, r.stream);
+    } catch (const std::runtime_error& e) {
+      throw CudaError(e.what());
+    }
+    r.sync("bgpu_hmatrix_matvec_device");
+    return 0;
+  });
+}
+
+int bgpu_hmatrix_plan(int n, const double* x, const double* v1, const double* v2, const double* v3, int leaf,
+                      double eta, int kmax, int* perm, int* counts) {
+  return status_of([&] {
+    if (n < 1) throw std::runtime_error("bgpu_hmatrix_plan: n < 1");
+    std::vector<double> geo((size_t)n * kGeoStride, 0.0), xc((size_t)n * kXcStride, 0.0);
+    for (int t = 0; t < n; ++t)
+      for (int c = 0; c < 3; ++c) {
+        geo[(size_t)t * kGeoStride + c] = v1[(size_t)c * n + t];
+        geo[(size_t)t * kGeoStride + 3 + c] = v2[(size_t)c * n + t];
+        geo[(size_t)t * kGeoStride + 6 + c] = v3[(size_t)c * n + t];
+        xc[(size_t)t * kXcStride + c] = x[(size_t)c * n + t];
+      }
+    const HPlan p = hplan_build(n, geo.data(), xc.data(), leaf, eta, kmax);
+    for (int k = 0; k < n; ++k) perm[k] = p.perm[k];
+    int nd = 0, nl = 0, na = 0;
+    for (const auto& b : p.blocks) {
+      nd += !b.lowrank;
+      nl += b.lowrank;
+      na += b.admissible;
+    }
+    counts[0] = p.depth;
+    counts[1] = (int)p.leaves.size();
+    counts[2] = nd;
+    counts[3] = nl;
+    counts[4] = na;
     return 0;
   });
 }

@@ -38,6 +38,180 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
   return a0 * b0 + a1 * b1 + a2 * b2;
 }
 
+// Target-independent terms of source triangle gp (kGeoStride doubles: p1, p2, p3, ..., area at 9):
+// P = p1, p2, p3; V = v21, v31, v32; D = d2121 d2131 d2132 d3131 d3232 d3231 s21 area 1/s21 (the
+// last for Fast only).  triangleint.f:110-120 (kernel.cpp:160-172).
+template <bool Fast>
+__device__ __forceinline__ void source_terms(const double* __restrict__ gp, double* P, double* V, double* D) {
+  double p[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) p[q] = gp[q];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) P[q] = p[q];
+  double v21[3], v31[3], v32[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    v21[c] = p[3 + c] - p[c];
+    v31[c] = p[6 + c] - p[c];
+    v32[c] = p[6 + c] - p[3 + c];
+    V[c] = v21[c];
+    V[3 + c] = v31[c];
+    V[6 + c] = v32[c];
+  }
+  const double d2121 = dot3(v21[0], v21[1], v21[2], v21[0], v21[1], v21[2]);
+  D[0] = d2121;
+  D[1] = dot3(v21[0], v21[1], v21[2], v31[0], v31[1], v31[2]);
+  D[2] = dot3(v21[0], v21[1], v21[2], v32[0], v32[1], v32[2]);
+  D[3] = dot3(v31[0], v31[1], v31[2], v31[0], v31[1], v31[2]);
+  D[4] = dot3(v32[0], v32[1], v32[2], v32[0], v32[1], v32[2]);
+  D[5] = dot3(v32[0], v32[1], v32[2], v31[0], v31[1], v31[2]);
+  D[6] = sqrt(d2121);
+  D[7] = gp[9];
+  if constexpr (Fast) D[8] = 1.0 / D[6];
+}
+
+// The 3 x 3 block G(target, source) of one pair of distinct triangles (triangleint.f:110-188,
+// kernel.cpp:148-249): P, V, D the source's terms (source_terms), xc the target's incenter;
+// blk[3a + b] = G_ab.  Fast = false needs s_logtab (the shared copy of the log's table).
+template <bool Fast>
+__device__ __forceinline__ void pair_gr(const double* P, const double* V, const double* D, double xcx, double xcy,
+                                        double xcz, double cg, const double* s_logtab, double* blk) {
+  const double v21[3] = {V[0], V[1], V[2]};
+  const double v31[3] = {V[3], V[4], V[5]};
+  const double v32[3] = {V[6], V[7], V[8]};
+  const double v1c[3] = {P[0] - xcx, P[1] - xcy, P[2] - xcz};
+  const double v2c[3] = {P[3] - xcx, P[4] - xcy, P[5] - xcz};
+  const double v3c[3] = {P[6] - xcx, P[7] - xcy, P[8] - xcz};
+  const double d2121 = D[0], d2131 = D[1], d2132 = D[2], d3131 = D[3], d3232 = D[4], d3231 = D[5];
+  const double s21 = D[6];
+  const double d211c = dot3(v21[0], v21[1], v21[2], v1c[0], v1c[1], v1c[2]);
+  const double d212c = dot3(v21[0], v21[1], v21[2], v2c[0], v2c[1], v2c[2]);
+  const double d322c = dot3(v32[0], v32[1], v32[2], v2c[0], v2c[1], v2c[2]);
+  const double d1c1c = dot3(v1c[0], v1c[1], v1c[2], v1c[0], v1c[1], v1c[2]);
+  const double d1c31 = dot3(v1c[0], v1c[1], v1c[2], v31[0], v31[1], v31[2]);
+  const double d2c2c = dot3(v2c[0], v2c[1], v2c[2], v2c[0], v2c[1], v2c[2]);
+  const double d2c1c = dot3(v2c[0], v2c[1], v2c[2], v1c[0], v1c[1], v1c[2]);
+  const double d3c31 = dot3(v3c[0], v3c[1], v3c[2], v31[0], v31[1], v31[2]);
+  const double d3c32 = dot3(v3c[0], v3c[1], v3c[2], v32[0], v32[1], v32[2]);
+  const double d3c3c = dot3(v3c[0], v3c[1], v3c[2], v3c[0], v3c[1], v3c[2]);
+  double t0 = 0.0, s0 = 0.0, sx = 0.0, sy = 0.0, sxy = 0.0, syy = 0.0, sxx = 0.0;
+  if constexpr (!Fast) {
+    // j-independent terms of the hy/hxy/hx denominators (each is recomputed identically on every
+    // quadrature point in the reference, so evaluating it once gives the same double)
+    const double p211 = d211c * d211c;
+    const double p1121 = d1c1c * d2121;
+    const double p3131sq = d1c31 * d1c31;
+    const double p1131 = d1c1c * d3131;
+#pragma unroll 3
+    for (int j = 0; j < 21; ++j) {
+      const double y = c_gy[j], w = c_gw[j];
+      const double y2 = 2.0 * y, yy = y * y;
+      const double q1 = sqrt(d1c1c + y2 * d1c31 + yy * d3131);
+      const double q2 = sqrt(d2c2c + y2 * d322c + yy * d3232);
+      // h (triangleint.f:198-206): the denominator's root is d1c1c + (2 d1c31) y + (d3131 y) y
+      const double hv = dd::cr_log_tab((d212c + d2132 * y + s21 * q2) /
+                                           (d211c + d2131 * y + s21 * sqrt(d1c1c + 2 * d1c31 * y + d3131 * y * y)),
+                                       s_logtab) /
+                        s21;
+      // hy (:222-234)
+      const double hya = (d211c + y * d2131) / q1;
+      const double hyb = (y * d2132 + d212c) / q2;
+      const double hyc = (p211 - p1121 - y2 * d1c31 * d2121 + y2 * d211c * d2131 + yy * d2131 * d2131 -
+                          yy * d2121 * d3131);
+      const double hyv = (hya - hyb) / hyc;
+      // hxy (:236-247)
+      const double hxyb = (y * d211c - d2c1c - y2 * d1c31 - y * d2131 - yy * d3231) / q2;
+      const double hxyc =
+          (-p211 + p1121 + y2 * d1c31 * d2121 - y2 * d211c * d2131 - yy * (d2131 * d2131) + yy * d2121 * d3131);
+      const double hxyv = (q1 + hxyb) / hxyc;
+      // hx (:208-220)
+      const double hxa = (-d1c31 - y * d2131) / sqrt(d1c1c + y2 * d211c + yy * d2121);
+      const double hxb = (-(y * d3231) + d3c31) / sqrt(yy * d3232 - y2 * d3c32 + d3c3c);
+      const double hxc = (-p3131sq - y2 * d1c31 * d2131 - yy * d2131 * d2131 + p1131 + y2 * d211c * d3131 +
+                          yy * d2121 * d3131);
+      const double hxv = (hxa + hxb) / hxc;
+      // :122-130
+      const double wy = w * y, wyy = wy * y;
+      t0 = t0 + w * hv;
+      s0 = s0 + w * hyv;
+      sx = sx + w * hxyv;
+      sy = sy + wy * hyv;
+      sxy = sxy + wy * hxyv;
+      syy = syy + wyy * hyv;
+      sxx = sxx + wyy * hxv;
+    }
+  } else {
+    // 1/sqrt as rsqrt (q = a rsqrt(a)); the denominators of hy and hxy (exact negatives of each
+    // other in triangleint.f) and of hx as quadratics in y with per-pair coefficients; one
+    // reciprocal per quadrature point for all three quotients; 1/s21 once per source triangle
+    const double inv_s21 = D[8];
+    const double cy0 = d211c * d211c - d1c1c * d2121;
+    const double cy1 = 2.0 * (d211c * d2131 - d1c31 * d2121);
+    const double cy2 = d2131 * d2131 - d2121 * d3131;
+    const double cx0 = d1c1c * d3131 - d1c31 * d1c31;
+    const double cx1 = 2.0 * (d211c * d3131 - d1c31 * d2131);
+#pragma unroll 3
+    for (int j = 0; j < 21; ++j) {
+      const double y = c_gy[j], w = c_gw[j];
+      const double a1 = d1c1c + y * (2.0 * d1c31 + y * d3131);
+      const double a2 = d2c2c + y * (2.0 * d322c + y * d3232);
+      const double a3 = d1c1c + y * (2.0 * d211c + y * d2121);
+      const double a4 = d3c3c + y * (y * d3232 - 2.0 * d3c32);
+      const double r1 = rsqrt(a1), r2 = rsqrt(a2);
+      const double q1 = a1 * r1, q2 = a2 * r2;
+      // the three quotients (log argument, hy/hxy, hx) from one reciprocal of the product of
+      // their denominators (that product scales as the 10th power of the mesh's size: meshes
+      // whose extent lies outside [1e-20, 1e20] are assembled by the exact kernel instead,
+      // DevMesh::fast_ok)
+      const double den = d211c + d2131 * y + s21 * q1;
+      const double dy = cy0 + y * (cy1 + y * cy2), dx = cx0 + y * (cx1 - y * cy2);
+      const double dyx = dy * dx;
+      const double r = 1.0 / (dyx * den);
+      const double ry = dx * den * r, rx = dy * den * r, rden = dyx * r;
+      const double hv = log((d212c + d2132 * y + s21 * q2) * rden) * inv_s21;
+      const double hyv = ((d211c + y * d2131) * r1 - (y * d2132 + d212c) * r2) * ry;
+      const double hxyv = -(q1 + (y * d211c - d2c1c - 2.0 * y * d1c31 - y * d2131 - y * y * d3231) * r2) * ry;
+      const double hxv = ((-d1c31 - y * d2131) * rsqrt(a3) + (d3c31 - y * d3231) * rsqrt(a4)) * rx;
+      const double wy = w * y, wyy = wy * y;
+      t0 = t0 + w * hv;
+      s0 = s0 + w * hyv;
+      sx = sx + w * hxyv;
+      sy = sy + wy * hyv;
+      sxy = sxy + wy * hxyv;
+      syy = syy + wyy * hyv;
+      sxx = sxx + wyy * hxv;
+    }
+  }
+  t0 = 0.5 * t0;
+  s0 = 0.5 * s0;
+  sx = 0.5 * sx;
+  sy = 0.5 * sy;
+  sxy = 0.5 * sxy;
+  syy = 0.5 * syy;
+  sxx = 0.5 * sxx;
+  // tensor (:149-177) and G (:180-188)
+  double tt[6];
+  int q = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = a; b < 3; ++b)
+      tt[q++] = v1c[a] * v1c[b] * s0 + (v1c[a] * v21[b] + v21[a] * v1c[b]) * sx +
+                (v31[a] * v1c[b] + v1c[a] * v31[b]) * sy + (v21[a] * v31[b] + v31[a] * v21[b]) * sxy +
+                v21[a] * v21[b] * sxx + v31[a] * v31[b] * syy;
+  // tt: t11 t12 t13 t22 t23 t33
+  const double ar2 = 2.0 * D[7];
+  const double g11 = ar2 * (t0 + cg * tt[0]);
+  const double g21 = ar2 * tt[1] * cg;
+  const double g22 = ar2 * (t0 + cg * tt[3]);
+  const double g31 = ar2 * tt[2] * cg;
+  const double g32 = ar2 * tt[4] * cg;
+  const double g33 = ar2 * (t0 + cg * tt[5]);
+  blk[0] = g11; blk[1] = g21; blk[2] = g31;
+  blk[3] = g21; blk[4] = g22; blk[5] = g32;
+  blk[6] = g31; blk[7] = g32; blk[8] = g33;
+}
+
 // One tile: targets [r0 + 128 bx, +128) x sources [c0 + 16 by, +16) of one mesh.  Fast = false:
 // triangleint.f's operations in its order with a correctly rounded log (bit for bit TGETGR's
 // arithmetic with correctly rounded functions; the including file is compiled with -fmad=false);
@@ -58,32 +232,7 @@ __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __re
   const int ns = min(kSrcTile, c1 - sbase);
   if (threadIdx.x < ns) {
     const int t = sbase + threadIdx.x;
-    const double* gp = geo + (size_t)t * kGeoStride;
-    double p[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) p[q] = gp[q];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) s_p[threadIdx.x][q] = p[q];
-    double v21[3], v31[3], v32[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      v21[c] = p[3 + c] - p[c];
-      v31[c] = p[6 + c] - p[c];
-      v32[c] = p[6 + c] - p[3 + c];
-      s_v[threadIdx.x][c] = v21[c];
-      s_v[threadIdx.x][3 + c] = v31[c];
-      s_v[threadIdx.x][6 + c] = v32[c];
-    }
-    const double d2121 = dot3(v21[0], v21[1], v21[2], v21[0], v21[1], v21[2]);
-    s_d[threadIdx.x][0] = d2121;
-    s_d[threadIdx.x][1] = dot3(v21[0], v21[1], v21[2], v31[0], v31[1], v31[2]);
-    s_d[threadIdx.x][2] = dot3(v21[0], v21[1], v21[2], v32[0], v32[1], v32[2]);
-    s_d[threadIdx.x][3] = dot3(v31[0], v31[1], v31[2], v31[0], v31[1], v31[2]);
-    s_d[threadIdx.x][4] = dot3(v32[0], v32[1], v32[2], v32[0], v32[1], v32[2]);
-    s_d[threadIdx.x][5] = dot3(v32[0], v32[1], v32[2], v31[0], v31[1], v31[2]);
-    s_d[threadIdx.x][6] = sqrt(d2121);
-    s_d[threadIdx.x][7] = gp[9];
-    if constexpr (Fast) s_d[threadIdx.x][8] = 1.0 / s_d[threadIdx.x][6];
+    source_terms<Fast>(geo + (size_t)t * kGeoStride, s_p[threadIdx.x], s_v[threadIdx.x], s_d[threadIdx.x]);
     s_comp[threadIdx.x] = (defl.ndef > 1) ? defl.comp[t] : 1;
   }
   if constexpr (!Fast) {
@@ -111,143 +260,7 @@ __device__ __forceinline__ void assemble_tile(int bx, int by, const double* __re
 #pragma unroll
       for (int q = 0; q < 9; ++q) blk[q] = self9[(size_t)n1 * 9 + q];
     } else {
-      const double* P = s_p[si];
-      const double* V = s_v[si];
-      const double* D = s_d[si];
-      const double v21[3] = {V[0], V[1], V[2]};
-      const double v31[3] = {V[3], V[4], V[5]};
-      const double v32[3] = {V[6], V[7], V[8]};
-      const double v1c[3] = {P[0] - xcx, P[1] - xcy, P[2] - xcz};
-      const double v2c[3] = {P[3] - xcx, P[4] - xcy, P[5] - xcz};
-      const double v3c[3] = {P[6] - xcx, P[7] - xcy, P[8] - xcz};
-      const double d2121 = D[0], d2131 = D[1], d2132 = D[2], d3131 = D[3], d3232 = D[4], d3231 = D[5];
-      const double s21 = D[6];
-      const double d211c = dot3(v21[0], v21[1], v21[2], v1c[0], v1c[1], v1c[2]);
-      const double d212c = dot3(v21[0], v21[1], v21[2], v2c[0], v2c[1], v2c[2]);
-      const double d322c = dot3(v32[0], v32[1], v32[2], v2c[0], v2c[1], v2c[2]);
-      const double d1c1c = dot3(v1c[0], v1c[1], v1c[2], v1c[0], v1c[1], v1c[2]);
-      const double d1c31 = dot3(v1c[0], v1c[1], v1c[2], v31[0], v31[1], v31[2]);
-      const double d2c2c = dot3(v2c[0], v2c[1], v2c[2], v2c[0], v2c[1], v2c[2]);
-      const double d2c1c = dot3(v2c[0], v2c[1], v2c[2], v1c[0], v1c[1], v1c[2]);
-      const double d3c31 = dot3(v3c[0], v3c[1], v3c[2], v31[0], v31[1], v31[2]);
-      const double d3c32 = dot3(v3c[0], v3c[1], v3c[2], v32[0], v32[1], v32[2]);
-      const double d3c3c = dot3(v3c[0], v3c[1], v3c[2], v3c[0], v3c[1], v3c[2]);
-      double t0 = 0.0, s0 = 0.0, sx = 0.0, sy = 0.0, sxy = 0.0, syy = 0.0, sxx = 0.0;
-      if constexpr (!Fast) {
-        // j-independent terms of the hy/hxy/hx denominators (each is recomputed identically on every
-        // quadrature point in the reference, so evaluating it once gives the same double)
-        const double p211 = d211c * d211c;
-        const double p1121 = d1c1c * d2121;
-        const double p3131sq = d1c31 * d1c31;
-        const double p1131 = d1c1c * d3131;
-  #pragma unroll 3
-        for (int j = 0; j < 21; ++j) {
-          const double y = c_gy[j], w = c_gw[j];
-          const double y2 = 2.0 * y, yy = y * y;
-          const double q1 = sqrt(d1c1c + y2 * d1c31 + yy * d3131);
-          const double q2 = sqrt(d2c2c + y2 * d322c + yy * d3232);
-          // h (triangleint.f:198-206): the denominator's root is d1c1c + (2 d1c31) y + (d3131 y) y
-          const double hv = dd::cr_log_tab((d212c + d2132 * y + s21 * q2) /
-                                               (d211c + d2131 * y + s21 * sqrt(d1c1c + 2 * d1c31 * y + d3131 * y * y)),
-                                           s_logtab) /
-                            s21;
-          // hy (:222-234)
-          const double hya = (d211c + y * d2131) / q1;
-          const double hyb = (y * d2132 + d212c) / q2;
-          const double hyc = (p211 - p1121 - y2 * d1c31 * d2121 + y2 * d211c * d2131 + yy * d2131 * d2131 -
-                              yy * d2121 * d3131);
-          const double hyv = (hya - hyb) / hyc;
-          // hxy (:236-247)
-          const double hxyb = (y * d211c - d2c1c - y2 * d1c31 - y * d2131 - yy * d3231) / q2;
-          const double hxyc =
-              (-p211 + p1121 + y2 * d1c31 * d2121 - y2 * d211c * d2131 - yy * (d2131 * d2131) + yy * d2121 * d3131);
-          const double hxyv = (q1 + hxyb) / hxyc;
-          // hx (:208-220)
-          const double hxa = (-d1c31 - y * d2131) / sqrt(d1c1c + y2 * d211c + yy * d2121);
-          const double hxb = (-(y * d3231) + d3c31) / sqrt(yy * d3232 - y2 * d3c32 + d3c3c);
-          const double hxc = (-p3131sq - y2 * d1c31 * d2131 - yy * d2131 * d2131 + p1131 + y2 * d211c * d3131 +
-                              yy * d2121 * d3131);
-          const double hxv = (hxa + hxb) / hxc;
-          // :122-130
-          const double wy = w * y, wyy = wy * y;
-          t0 = t0 + w * hv;
-          s0 = s0 + w * hyv;
-          sx = sx + w * hxyv;
-          sy = sy + wy * hyv;
-          sxy = sxy + wy * hxyv;
-          syy = syy + wyy * hyv;
-          sxx = sxx + wyy * hxv;
-        }
-      } else {
-        // 1/sqrt as rsqrt (q = a rsqrt(a)); the denominators of hy and hxy (exact negatives of each
-        // other in triangleint.f) and of hx as quadratics in y with per-pair coefficients; one
-        // reciprocal per quadrature point for all three quotients; 1/s21 once per source triangle
-        const double inv_s21 = D[8];
-        const double cy0 = d211c * d211c - d1c1c * d2121;
-        const double cy1 = 2.0 * (d211c * d2131 - d1c31 * d2121);
-        const double cy2 = d2131 * d2131 - d2121 * d3131;
-        const double cx0 = d1c1c * d3131 - d1c31 * d1c31;
-        const double cx1 = 2.0 * (d211c * d3131 - d1c31 * d2131);
-#pragma unroll 3
-        for (int j = 0; j < 21; ++j) {
-          const double y = c_gy[j], w = c_gw[j];
-          const double a1 = d1c1c + y * (2.0 * d1c31 + y * d3131);
-          const double a2 = d2c2c + y * (2.0 * d322c + y * d3232);
-          const double a3 = d1c1c + y * (2.0 * d211c + y * d2121);
-          const double a4 = d3c3c + y * (y * d3232 - 2.0 * d3c32);
-          const double r1 = rsqrt(a1), r2 = rsqrt(a2);
-          const double q1 = a1 * r1, q2 = a2 * r2;
-          // the three quotients (log argument, hy/hxy, hx) from one reciprocal of the product of
-          // their denominators (that product scales as the 10th power of the mesh's size: meshes
-          // whose extent lies outside [1e-20, 1e20] are assembled by the exact kernel instead,
-          // DevMesh::fast_ok)
-          const double den = d211c + d2131 * y + s21 * q1;
-          const double dy = cy0 + y * (cy1 + y * cy2), dx = cx0 + y * (cx1 - y * cy2);
-          const double dyx = dy * dx;
-          const double r = 1.0 / (dyx * den);
-          const double ry = dx * den * r, rx = dy * den * r, rden = dyx * r;
-          const double hv = log((d212c + d2132 * y + s21 * q2) * rden) * inv_s21;
-          const double hyv = ((d211c + y * d2131) * r1 - (y * d2132 + d212c) * r2) * ry;
-          const double hxyv = -(q1 + (y * d211c - d2c1c - 2.0 * y * d1c31 - y * d2131 - y * y * d3231) * r2) * ry;
-          const double hxv = ((-d1c31 - y * d2131) * rsqrt(a3) + (d3c31 - y * d3231) * rsqrt(a4)) * rx;
-          const double wy = w * y, wyy = wy * y;
-          t0 = t0 + w * hv;
-          s0 = s0 + w * hyv;
-          sx = sx + w * hxyv;
-          sy = sy + wy * hyv;
-          sxy = sxy + wy * hxyv;
-          syy = syy + wyy * hyv;
-          sxx = sxx + wyy * hxv;
-        }
-      }
-      t0 = 0.5 * t0;
-      s0 = 0.5 * s0;
-      sx = 0.5 * sx;
-      sy = 0.5 * sy;
-      sxy = 0.5 * sxy;
-      syy = 0.5 * syy;
-      sxx = 0.5 * sxx;
-      // tensor (:149-177) and G (:180-188)
-      double tt[6];
-      int q = 0;
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = a; b < 3; ++b)
-          tt[q++] = v1c[a] * v1c[b] * s0 + (v1c[a] * v21[b] + v21[a] * v1c[b]) * sx +
-                    (v31[a] * v1c[b] + v1c[a] * v31[b]) * sy + (v21[a] * v31[b] + v31[a] * v21[b]) * sxy +
-                    v21[a] * v21[b] * sxx + v31[a] * v31[b] * syy;
-      // tt: t11 t12 t13 t22 t23 t33
-      const double ar2 = 2.0 * D[7];
-      const double g11 = ar2 * (t0 + cg * tt[0]);
-      const double g21 = ar2 * tt[1] * cg;
-      const double g22 = ar2 * (t0 + cg * tt[3]);
-      const double g31 = ar2 * tt[2] * cg;
-      const double g32 = ar2 * tt[4] * cg;
-      const double g33 = ar2 * (t0 + cg * tt[5]);
-      blk[0] = g11; blk[1] = g21; blk[2] = g31;
-      blk[3] = g21; blk[4] = g22; blk[5] = g32;
-      blk[6] = g31; blk[7] = g32; blk[8] = g33;
+      pair_gr<Fast>(s_p[si], s_v[si], s_d[si], xcx, xcy, xcz, cg, s_logtab, blk);
     }
     const size_t col0 = 3 * (size_t)(n2 - c0);
     if (defl.ndef > 0) {

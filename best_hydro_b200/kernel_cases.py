@@ -6,6 +6,9 @@
                                                              # (mixed: the mixed path's assembly)
     python -m best_hydro_b200.kernel_cases mixed F           # mixed build + solve, ellipsoid frequency F
     python -m best_hydro_b200.kernel_cases adjoint F         # FP64 build + adjoint gradients (k_pair_adjoint)
+    python -m best_hydro_b200.kernel_cases hmatrix F [EPS]  # H-matrix build + 6-RHS GMRES solve of the star
+                                                             # body at geodesic frequency F (eps 1e-4), then
+                                                             # five timed 6-column products
     python -m best_hydro_b200.kernel_cases panel left|right leaf|update LEN
                                                              # k_panel_tf32: a triangular-solve leaf or a
                                                              # K = 128 update on a 128 x LEN panel
@@ -89,6 +92,42 @@ def main(argv):
         for _ in range(2):
             s.gradient(iarea=1, truearea=ta)
         print([ln for ln in bh.log_lines() if ln.startswith("gradient")][-1])
+        return 0
+    if case == "hmatrix":
+        from best_hydro_b200 import meshes
+        f = int(argv[1])
+        eps = float(argv[2]) if len(argv) > 2 else 1e-4
+        tri, ta, tv = meshes.star(f)
+        st = bh.Setup(tri, 0, ta)
+        s = bh.BhmSolver()
+        s.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        x = s.incenters()
+        xmu, gdef = st.deflation(s.diag_mean())
+        bh.set_precision(bh.BGPU_HMATRIX)
+        s.build(eps=eps, direct=0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+        s.solve(bh.rhs6(x))
+        t = bh.timings()
+        hs = bh.hmatrix_stats()
+        n3 = 3 * st.n
+        xs = torch.randn(6, n3, dtype=torch.float64, device=dev)
+        ys = torch.empty_like(xs)
+        ls = torch.cuda.ExternalStream(bh.lib().bgpu_stream())  # the library's stream, where it launches
+        e0, e1 = _ev(torch)
+        torch.cuda.synchronize()
+        e0.record(ls)
+        for _ in range(5):
+            bh.hmatrix_matvec_device(6, xs.data_ptr(), n3, ys.data_ptr(), n3)
+        e1.record(ls)
+        torch.cuda.synchronize()
+        mv = e0.elapsed_time(e1) / 5
+        gb = 8 * (hs["dense_entries"] + hs["lowrank_entries"]) / 1e9
+        print(f"hmatrix N={st.n} eps={eps:g}: build {t['build']:.1f} ms (fill {hs['fill_ms']:.1f}, ACA "
+              f"{hs['aca_ms']:.1f}, preconditioner {hs['precond_ms']:.1f}), solve {t['solve']:.1f} ms "
+              f"({int(hs['gmres_steps'])} GMRES steps); product of 6 columns {mv:.3f} ms over {gb:.2f} GB "
+              f"({gb / mv * 1e3:.0f} GB/s of stored blocks)")
+        for line in bh.log_lines():
+            print(line)
+        bh.set_precision(-1)
         return 0
     if case in ("assemble", "mixed"):
         f = int(argv[1])

@@ -17,11 +17,14 @@ extern "C" {
 
 /* Factorisation precisions for bhm_build. */
 enum {
-  BGPU_FP64 = 0,   /* FP64 LU with partial pivoting (the plain path) */
-  BGPU_MIXED = 1   /* reduced-precision tensor-core LU + FP64 GMRES refinement */
+  BGPU_FP64 = 0,    /* FP64 LU with partial pivoting (the plain path) */
+  BGPU_MIXED = 1,   /* reduced-precision tensor-core LU + FP64 GMRES refinement */
+  BGPU_HMATRIX = 2  /* H-matrix (dense near field, low-rank far field) + FP64 GMRES: N beyond HBM */
 };
 
-/* Overrides the precision bhm_build derives from direct/single (-1: back to that rule). */
+/* Overrides the precision bhm_build derives from direct/single (-1: back to that rule).  Without an
+ * override, bhm_build takes BGPU_HMATRIX by itself when the dense GR of the chosen path does not fit
+ * in the GPU's free memory (logged). */
 int bgpu_set_precision(int mode);
 
 /* The precision of the last bhm_build. */
@@ -31,6 +34,35 @@ int bgpu_precision(void);
  * FP64 residual) of krylov <= 16 vectors; defaults 8 and 10.  When the refinement does not reach its
  * tolerance, bhm_solve factors the kept FP64 matrix on the GPU and solves with it instead (logged). */
 int bgpu_set_refinement(int max_restarts, int krylov);
+
+/* The H-matrix path (the GPU counterpart of the reference's H-matrix solver, hmatrix/src/api.cpp:582-771,
+ * selected by BEST's -hm or N > 10,000 there; here by bgpu_set_precision(BGPU_HMATRIX) or when the dense
+ * GR does not fit).  bhm_build's eps is the relative accuracy of the far-field blocks (BEST's -he,
+ * default 1e-4); bhm_solve runs GMRES(30) to a relative residual of 0.1 eps (hmatrix/src/api.cpp:39-41).
+ * Every entry the H-matrix evaluates equals bhm_entries' entry bit for bit; the deflation is applied as
+ * a low-rank term of every product (api.cpp:641-646).
+ *
+ * Settings of later builds: leaf clusters of at most `leaf` triangles (8..128; default 128), the
+ * admissibility eta (default 2.0, cluster.cpp:115-117), at most kmax (multiple of 3, <= 120; default
+ * 90) terms per low-rank block. */
+int bgpu_hmatrix_set_options(int leaf, double eta, int kmax);
+
+/* Figures of the last H-matrix build and solve, up to len of: n, leaves, dense blocks, low-rank blocks,
+ * dense entries, low-rank entries (at their ranks), mean rank, largest rank, blocks that reached kmax,
+ * fill ms, cross-approximation ms, preconditioner ms, GMRES steps of the last solve, its largest
+ * relative residual, device bytes held. */
+int bgpu_hmatrix_stats(double *out, int len);
+
+/* y = (H + deflation) x on device data (3n x nrhs, leading dimensions ldx, ldy >= 3n), original
+ * triangle order: the product GMRES uses. */
+int bgpu_hmatrix_matvec_device(int nrhs, const double *d_x, int ldx, double *d_y, int ldy);
+
+/* The H-matrix's cluster tree and block partition alone, on the host (no GPU used): x the incenters
+ * and v1, v2, v3 the corners (n x 3 column-major, as bhm_create takes them).  perm[k] receives the
+ * triangle at tree position k (0-based); counts[0..4]: depth, leaves, dense blocks, low-rank blocks,
+ * admissible blocks. */
+int bgpu_hmatrix_plan(int n, const double *x, const double *v1, const double *v2, const double *v3, int leaf,
+                      double eta, int kmax, int *perm, int *counts);
 
 /* Stage times of the last calls in milliseconds, measured with CUDA events on the library's
  * stream: ms[0] self blocks + incenters (bhm_create), ms[1] assembly + deflation, ms[2] LU,

@@ -1,0 +1,101 @@
+"""GPU tests of the H-matrix path (bgpu_set_precision(BGPU_HMATRIX); the GPU counterpart of the
+reference's H-matrix solver, hmatrix/src/api.cpp:582-771, which BEST runs for large N):
+
+* its product (H + deflation) x against the dense deflated GR (bhm_entries + best.f:406-425) at
+  eps = 1e-4 and 1e-6: relative error per column <= 3 eps;
+* BEST's results (D_t, D_r, D_tr, centres, CHI') from its GMRES solves against the plain FP64 path on
+  the same mesh: relative difference <= eps;
+* the reference's golden results of 2eu7 (one surface, area correction) and of the two-surface case
+  (NDEF = 2, the deflation per surface) within their 2e-4 tolerance, as the reference's H-matrix
+  path meets them (test/run_tests.sh).
+"""
+import numpy as np
+import pytest
+import torch
+
+import best_hydro_b200 as bh
+from best_hydro_b200 import BhmSolver, meshes
+from oracle import best as ob
+from tests.helpers import expected_cases, golden_mesh, rel, run_gpu, value_for_label
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(tri, ta, precision, eps=1e-4, ivisco=1, **kw):
+    bh.set_precision(precision)
+    solver = BhmSolver()
+    try:
+        g = run_gpu(solver, tri, ta, eps=eps, direct=1 if precision == bh.BGPU_FP64 else 0, ivisco=ivisco, **kw)
+        g["stats"] = bh.hmatrix_stats() if precision == bh.BGPU_HMATRIX else None
+        g["precision"] = bh.lib().bgpu_precision()
+    finally:
+        bh.set_precision(-1)
+    return solver, g
+
+
+def _results_diff(a, b):
+    ta, tb = a["tensors"], b["tensors"]
+    out = {k: rel(ta[k], tb[k]) for k in ("Dtt", "Drr")}
+    scale = np.sqrt(np.max(np.abs(tb["Dtt"])) * np.max(np.abs(tb["Drr"])))
+    out["Dtr"] = float(np.max(np.abs(ta["Dtr"] - tb["Dtr"])) / scale)
+    size = np.sqrt(np.mean(b["x"].reshape(3, -1) ** 2) * 3)
+    for k in ("urc", "udr"):
+        out[k] = float(np.max(np.abs(ta[k] - tb[k])) / size)
+    if a.get("chiprime") is not None:
+        out["chiprime"] = abs(a["chiprime"] / b["chiprime"] - 1)
+    return out
+
+
+@pytest.mark.parametrize("eps", [1e-4, 1e-6])
+def test_product_against_dense(eps):
+    tri, ta, tv = meshes.ellipsoid(12)  # N = 2,880
+    solver, g = _run(tri, ta, bh.BGPU_HMATRIX, eps=eps, ivisco=0)
+    assert g["precision"] == bh.BGPU_HMATRIX
+    s = g["setup"]
+    n3 = 3 * s.n
+    gr = solver.entries(0, n3, 0, n3)
+    ob.deflate(s, gr, g["xmu"], g["gdef"])
+    rng = np.random.default_rng(7)
+    X = np.asfortranarray(rng.standard_normal((n3, 3)))
+    Y = gr @ X
+    dx = torch.from_numpy(X.T.copy()).cuda()  # column-major 3n x 3: row c of the torch tensor is column c
+    dy = torch.zeros_like(dx)
+    bh.hmatrix_matvec_device(3, dx.data_ptr(), n3, dy.data_ptr(), n3)
+    torch.cuda.synchronize()
+    Yh = dy.cpu().numpy().T
+    err = np.linalg.norm(Yh - Y, axis=0) / np.linalg.norm(Y, axis=0)
+    st = g["stats"]
+    print(f"eps {eps}: product error {err.max():.2e}; {st}")
+    assert st["lowrank_blocks"] > 0 and st["dense_blocks"] > 0
+    assert st["dense_entries"] + st["lowrank_entries"] < 0.9 * n3 * n3
+    assert err.max() <= 3 * eps, err
+    solver.destroy()
+
+
+@pytest.mark.parametrize("eps", [1e-4, 1e-6])
+def test_results_against_fp64_path(eps):
+    tri, ta, tv = meshes.ellipsoid(16)  # N = 5,120
+    s1, h = _run(tri, ta, bh.BGPU_HMATRIX, eps=eps)
+    s1.destroy()
+    s2, d = _run(tri, ta, bh.BGPU_FP64)
+    s2.destroy()
+    diff = _results_diff(h, d)
+    print(f"eps {eps}: {diff}; GMRES steps {h['stats']['gmres_steps']:.0f}; {h['stats']}")
+    assert h["stats"]["relres"] <= 0.1 * eps
+    for k, v in diff.items():
+        assert v <= eps, (k, v)
+
+
+@pytest.mark.parametrize("key", ["2eu7", "two"])
+def test_golden_results_on_the_hmatrix(key):
+    c = expected_cases()[key]
+    tri, ta, tv = golden_mesh(c["mesh"])
+    solver, g = _run(tri, ta, bh.BGPU_HMATRIX, eps=1e-4, ivisco=c["ivisco"], iarea=c["iarea"], icov=c["icov"],
+                     truevol=tv, wm=c["wm"])
+    for e in c["expected"]:
+        if e["label"] in ("Dx", "Dy", "Dz"):
+            got = g["dvisc"]["xyz".index(e["label"][1])]
+        else:
+            got = value_for_label(g["report"], e["label"])
+        assert abs(got - e["value"]) <= e["tol"] * abs(e["value"]), (e["label"], got, e["value"])
+    solver.destroy()
