@@ -489,7 +489,9 @@ int build_common(Solver& s, Runtime& r, double eps, int direct, int single, cons
     // its H-matrix for large N, best/best.f:138)
     size_t fr = 0, tot = 0;
     ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
-    const double need = (s.precision == BGPU_FP64 ? 72.0 : 108.0) * (double)n * n * 1.02 + 5.12e8 - (double)s.gr.bytes;
+    // memory this solver holds now is reused or freed by the build: count it as available
+    const double held = (double)s.gr.bytes + (s.mixed ? (double)s.mixed->device_bytes() : 0.0);
+    const double need = (s.precision == BGPU_FP64 ? 72.0 : 108.0) * (double)n * n * 1.02 + 5.12e8 - held;
     if (need > (double)fr) {
       note("dense GR of order %d needs %.1f GB, %.1f GB free on the GPU: H-matrix path", n3, need / 1e9, fr / 1e9);
       s.precision = BGPU_HMATRIX;

@@ -547,33 +547,66 @@ __global__ void __launch_bounds__(kFixThreads)
 // Rows and columns of earlier pivots are not excluded beyond the current row: the cross
 // approximation reproduces them exactly, so their residuals are zero up to rounding.
 
-// Product, first part: t[toff + q', c] = V[:, q']^T xt[3 c0 .., c] for every term of every low-rank
-// block (a warp per term).
-__global__ void k_lr_vt(const HLow* __restrict__ lb, const int2* __restrict__ terms, int nterms,
-                        const double* __restrict__ Vp, const double* __restrict__ xt, long ldx, int nq,
-                        double* __restrict__ tbuf) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
-  if (w >= nterms) return;
-  const int2 tm = terms[w];
-  const HLow B = lb[tm.x];
+// Product, first part: t[toff + j, c] = V[:, j]^T xt[3 c0 .., c] for every term of every low-rank
+// block.  One CTA per block, each warp four terms at a time (four independent loads of V per lane),
+// the columns of x in passes of eight; the block's rows of x are read through L1 by all its warps.
+constexpr int kVtThreads = 128;
+template <int QC>
+__global__ void __launch_bounds__(kVtThreads)
+    k_lr_vt(const HLow* __restrict__ lb, const double* __restrict__ Vp, const double* __restrict__ xt, long ldx,
+            int nq, double* __restrict__ tbuf) {
+  const HLow B = lb[blockIdx.x];
+  const int kr = B.kcap;  // after the fill, the block's rank
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   const long ldv = 3L * B.nc;
-  const double* v = Vp + B.voff + (size_t)tm.y * ldv;
+  const int rows = 3 * B.nc;
   const double* x = xt + 3L * B.c0;
-  double acc[kHQ];
+  for (int j0 = 4 * w; j0 < kr; j0 += 4 * (kVtThreads / 32)) {
+    const double* v = Vp + B.voff + (size_t)j0 * ldv;
+    const int nj = min(4, kr - j0);
+    for (int c0 = 0; c0 < nq; c0 += QC) {
+      const int qc = min(QC, nq - c0);
+      double acc[4][QC];
 #pragma unroll
-  for (int c = 0; c < kHQ; ++c) acc[c] = 0.0;
-  for (int r = l; r < 3 * B.nc; r += 32) {
-    const double vr = __ldg(v + r);
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int c = 0; c < kHQ; ++c)
-      if (c < nq) acc[c] += vr * x[(size_t)c * ldx + r];
-  }
+        for (int c = 0; c < QC; ++c) acc[a][c] = 0.0;
+      int r = l;
+      for (; r + 32 < rows; r += 64) {  // two rows per lane in flight
+        double vr[2][4];
 #pragma unroll
-  for (int c = 0; c < kHQ; ++c) {
-    if (c >= nq) break;
-    double a = acc[c];
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-    if (l == 0) tbuf[(size_t)(B.toff + tm.y) * kHQ + c] = a;
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int a = 0; a < 4; ++a) vr[h][a] = a < nj ? __ldg(v + (size_t)a * ldv + r + 32 * h) : 0.0;
+#pragma unroll
+        for (int c = 0; c < QC; ++c)
+          if (c < qc) {
+            const double x0 = __ldg(x + (size_t)(c0 + c) * ldx + r), x1 = __ldg(x + (size_t)(c0 + c) * ldx + r + 32);
+#pragma unroll
+            for (int a = 0; a < 4; ++a) acc[a][c] += vr[0][a] * x0 + vr[1][a] * x1;
+          }
+      }
+      for (; r < rows; r += 32) {
+        double vr[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) vr[a] = a < nj ? __ldg(v + (size_t)a * ldv + r) : 0.0;
+#pragma unroll
+        for (int c = 0; c < QC; ++c)
+          if (c < qc) {
+            const double xv = __ldg(x + (size_t)(c0 + c) * ldx + r);
+#pragma unroll
+            for (int a = 0; a < 4; ++a) acc[a][c] += vr[a] * xv;
+          }
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < QC; ++c) {
+          double t = acc[a][c];
+          for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+          if (l == 0 && a < nj && c < qc) tbuf[(size_t)(B.toff + j0 + a) * kHQ + c0 + c] = t;
+        }
+    }
   }
 }
 
@@ -601,11 +634,12 @@ __global__ void k_defl_sums(int n, int ndef, const double* __restrict__ gdef, co
 
 constexpr int kLeafThreads = 3 * kHMaxLeaf;  // the most threads per CTA (one per row of the largest leaf)
 constexpr int kColChunk = 128;               // source triangles of x staged at a time
-constexpr int kSegments = 4;                 // CTAs per leaf row cluster in the product
+constexpr int kSegments = 8;                 // CTAs per leaf row cluster in the product
 
 // Product, second part: CTA (leaf L, segment g) sums the rows of L of every g-th of L's blocks (dense:
 // rows times x; low-rank: rows of U times that block's t) into part[g]; four independent loads per
 // thread in flight, and kSegments CTAs per leaf, to keep enough bytes moving.
+template <int NQ>
 __global__ void __launch_bounds__(kLeafThreads)
     k_leaf_mv(const HLeaf* __restrict__ leaves, const HEntry* __restrict__ dent, const HEntry* __restrict__ lent,
               const HDense* __restrict__ db, const HLow* __restrict__ lb, const double* __restrict__ Dp,
@@ -616,9 +650,9 @@ __global__ void __launch_bounds__(kLeafThreads)
   const int g = blockIdx.y;
   const int row = threadIdx.x;
   const int m = 3 * L.cnt;
-  double acc[kHQ];
+  double acc[NQ];
 #pragma unroll
-  for (int c = 0; c < kHQ; ++c) acc[c] = 0.0;
+  for (int c = 0; c < NQ; ++c) acc[c] = 0.0;
   for (int e = L.d0 + g; e < L.d1; e += kSegments) {
     const HEntry E = dent[e];
     const HDense B = db[E.blk];
@@ -640,8 +674,7 @@ __global__ void __launch_bounds__(kLeafThreads)
           const double a0 = __ldg(a + (size_t)r * ld), a1 = __ldg(a + (size_t)(r + 1) * ld);
           const double a2 = __ldg(a + (size_t)(r + 2) * ld), a3 = __ldg(a + (size_t)(r + 3) * ld);
 #pragma unroll
-          for (int c = 0; c < kHQ; ++c)
-            if (c < nq) {
+          for (int c = 0; c < NQ; ++c) {
               acc[c] += a0 * sx[r * kHQ + c];
               acc[c] += a1 * sx[(r + 1) * kHQ + c];
               acc[c] += a2 * sx[(r + 2) * kHQ + c];
@@ -651,8 +684,7 @@ __global__ void __launch_bounds__(kLeafThreads)
         for (; r < rn; ++r) {
           const double av = __ldg(a + (size_t)r * ld);
 #pragma unroll
-          for (int c = 0; c < kHQ; ++c)
-            if (c < nq) acc[c] += av * sx[r * kHQ + c];
+          for (int c = 0; c < NQ; ++c) acc[c] += av * sx[r * kHQ + c];
         }
       }
     }
@@ -675,8 +707,7 @@ __global__ void __launch_bounds__(kLeafThreads)
         const double u0 = __ldg(u + (size_t)j * ld), u1 = __ldg(u + (size_t)(j + 1) * ld);
         const double u2 = __ldg(u + (size_t)(j + 2) * ld), u3 = __ldg(u + (size_t)(j + 3) * ld);
 #pragma unroll
-        for (int c = 0; c < kHQ; ++c)
-          if (c < nq) {
+        for (int c = 0; c < NQ; ++c) {
             acc[c] += u0 * sx[j * kHQ + c];
             acc[c] += u1 * sx[(j + 1) * kHQ + c];
             acc[c] += u2 * sx[(j + 2) * kHQ + c];
@@ -686,16 +717,14 @@ __global__ void __launch_bounds__(kLeafThreads)
       for (; j < kr; ++j) {
         const double uv = __ldg(u + (size_t)j * ld);
 #pragma unroll
-        for (int c = 0; c < kHQ; ++c)
-          if (c < nq) acc[c] += uv * sx[j * kHQ + c];
+        for (int c = 0; c < NQ; ++c) acc[c] += uv * sx[j * kHQ + c];
       }
     }
   }
   if (row >= m) return;
   const size_t gr = 3L * L.beg + row;
 #pragma unroll
-  for (int c = 0; c < kHQ; ++c)
-    if (c < nq) part[((size_t)g * nq + c) * ldp + gr] = acc[c];
+  for (int c = 0; c < NQ; ++c) part[((size_t)g * nq + c) * ldp + gr] = acc[c];
 }
 
 // y = the segments' partial sums in order, plus the deflation term xmu_i s[comp(i)].
@@ -976,7 +1005,7 @@ struct HMatrixSolver::Impl {
   double ms_fill = 0, ms_aca = 0, ms_pre = 0;
   HReport last;
   Buf perm, geo_t, xc_t, self9_t, xmu_t, comp_t, gdef;
-  Buf d_dense, d_low, d_leaves, d_dent, d_lent, d_terms, d_dtile, d_rtile, d_ctile, d_state, status;
+  Buf d_dense, d_low, d_leaves, d_dent, d_lent, d_dtile, d_rtile, d_ctile, d_state, status;
   Buf D, Up, Vp, inv;
   Buf xt, yt, tb, sdef, part;         // product scratch
   int threads = kLeafThreads;         // CTA size of the per-leaf kernels: 3 x the largest leaf, rounded up to 32
@@ -984,7 +1013,7 @@ struct HMatrixSolver::Impl {
   size_t held() const {
     size_t s = 0;
     for (const Buf* b : {&perm, &geo_t, &xc_t, &self9_t, &xmu_t, &comp_t, &gdef, &d_dense, &d_low, &d_leaves, &d_dent,
-                         &d_lent, &d_terms, &d_dtile, &d_rtile, &d_ctile, &d_state, &status, &D, &Up, &Vp, &inv, &xt, &yt,
+                         &d_lent, &d_dtile, &d_rtile, &d_ctile, &d_state, &status, &D, &Up, &Vp, &inv, &xt, &yt,
                          &tb, &sdef, &part, &gV, &gW, &gZ, &gX, &gR, &gB, &gh, &gn})
       s += b->bytes;
     return s;
@@ -993,8 +1022,9 @@ struct HMatrixSolver::Impl {
   // y_t = (H + deflation) x_t, both in tree order (column stride ld)
   void apply_tree(int nq, const double* x, long ldx, double* y, long ldy, cudaStream_t s) {
     if (nterms > 0) {
-      k_lr_vt<<<blocks_for(32L * nterms, 256), 256, 0, s>>>(d_low.as<HLow>(), d_terms.as<int2>(), nterms, Vp.as<double>(),
-                                                             x, ldx, nq, tb.as<double>());
+      auto vt = nq >= 8 ? k_lr_vt<8> : nq == 7 ? k_lr_vt<7> : nq == 6 ? k_lr_vt<6> : nq == 5 ? k_lr_vt<5>
+              : nq == 4 ? k_lr_vt<4> : nq == 3 ? k_lr_vt<3> : nq == 2 ? k_lr_vt<2> : k_lr_vt<1>;
+      vt<<<(unsigned)low.size(), kVtThreads, 0, s>>>(d_low.as<HLow>(), Vp.as<double>(), x, ldx, nq, tb.as<double>());
       BGPU_COUNT_LAUNCH();
     }
     if (ndef > 0) {
@@ -1004,7 +1034,20 @@ struct HMatrixSolver::Impl {
     }
     const size_t smem = sizeof(double) * std::max(3 * kColChunk, kHMaxRank) * kHQ;
     const long n3 = 3L * n;
-    k_leaf_mv<<<dim3((unsigned)leaves.size(), kSegments), threads, smem, s>>>(
+    decltype(&k_leaf_mv<1>) mv = nullptr;
+    switch (nq) {
+#define BGPU_HQ_CASE(q) \
+  case q:               \
+    mv = k_leaf_mv<q>;  \
+    break;
+      BGPU_HQ_CASE(1) BGPU_HQ_CASE(2) BGPU_HQ_CASE(3) BGPU_HQ_CASE(4) BGPU_HQ_CASE(5) BGPU_HQ_CASE(6)
+      BGPU_HQ_CASE(7) BGPU_HQ_CASE(8) BGPU_HQ_CASE(9) BGPU_HQ_CASE(10) BGPU_HQ_CASE(11) BGPU_HQ_CASE(12)
+      BGPU_HQ_CASE(13) BGPU_HQ_CASE(14) BGPU_HQ_CASE(15) BGPU_HQ_CASE(16)
+#undef BGPU_HQ_CASE
+      default:
+        throw std::runtime_error("H-matrix: 1 to 16 columns per product");
+    }
+    mv<<<dim3((unsigned)leaves.size(), kSegments), threads, smem, s>>>(
         d_leaves.as<HLeaf>(), d_dent.as<HEntry>(), d_lent.as<HEntry>(), d_dense.as<HDense>(), d_low.as<HLow>(),
         D.as<double>(), Up.as<double>(), x, ldx, tb.as<double>(), nq, part.as<double>(), n3);
     BGPU_COUNT_LAUNCH();
@@ -1159,7 +1202,10 @@ void HMatrixSolver::build(const DevMesh& m, const DevDeflation& d, int ndef, dou
   static bool attrs = false;
   if (!attrs) {
     const int smem = (int)(sizeof(double) * std::max(3 * kColChunk, kHMaxRank) * kHQ);
-    hck(cudaFuncSetAttribute(k_leaf_mv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "kernel attributes");
+    for (auto f : {k_leaf_mv<1>, k_leaf_mv<2>, k_leaf_mv<3>, k_leaf_mv<4>, k_leaf_mv<5>, k_leaf_mv<6>, k_leaf_mv<7>,
+                   k_leaf_mv<8>, k_leaf_mv<9>, k_leaf_mv<10>, k_leaf_mv<11>, k_leaf_mv<12>, k_leaf_mv<13>,
+                   k_leaf_mv<14>, k_leaf_mv<15>, k_leaf_mv<16>})
+      hck(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "kernel attributes");
     hck(cudaFuncSetAttribute(k_bj_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(double) * 3 * kHMaxLeaf * kHQ)),
         "kernel attributes");
@@ -1222,7 +1268,7 @@ void HMatrixSolver::build(const DevMesh& m, const DevDeflation& d, int ndef, dou
       "ACA state");
   hck(cudaStreamSynchronize(s), "cross approximation");
   // final ranks into the block list (kcap := rank), product term list
-  std::vector<int2> terms;
+  int nterms = 0;
   I.capped = 0;
   I.max_rank = 0;
   I.low_entries = 0;
@@ -1230,18 +1276,17 @@ void HMatrixSolver::build(const DevMesh& m, const DevDeflation& d, int ndef, dou
   for (int b = 0; b < nlb; ++b) {
     HLow& L = I.low[b];
     const int r = st[b].rank;
-    L.toff = (int)terms.size();
+    L.toff = nterms;
     L.kcap = r;
-    for (int j = 0; j < r; ++j) terms.push_back(make_int2(b, j));
+    nterms += r;
     I.capped += st[b].capped;
     I.max_rank = std::max(I.max_rank, r);
     rsum += r;
     I.low_entries += 3.0 * (L.nr + L.nc) * r;
   }
   I.mean_rank = nlb ? (double)rsum / nlb : 0.0;
-  I.nterms = (int)terms.size();
+  I.nterms = nterms;
   upload(I.d_low, I.low, "low-rank block list", s);
-  upload(I.d_terms, terms, "term list", s);
   // block-Jacobi preconditioner
   k_bj_copy<<<(unsigned)I.leaves.size(), 256, 0, s>>>(I.d_leaves.as<HLeaf>(), I.d_dense.as<HDense>(), I.D.as<double>(),
                                                        I.ndef, I.gdef.as<double>(), I.xmu_t.as<double>(),

@@ -1688,6 +1688,15 @@ void MixedSolver::build(const DevMesh& m, const DevDeflation& d, double* gr64, l
   if (wait) finish_build(s);
 }
 
+size_t MixedSolver::device_bytes() const {
+  const Impl& P = *p_;
+  size_t b = 0;
+  for (const Buf* q : {&P.stamps, &P.lu32, &P.at, &P.bt, &P.status, &P.part, &P.pdots, &P.dots, &P.trsv, &P.vecs,
+                       &P.dl32, &P.du32, &P.zf, &P.wl32, &P.wu32, &P.am, &P.bm, &P.dl256, &P.du256})
+    b += q->p ? q->bytes : 0;
+  return b;
+}
+
 void MixedSolver::finish_build(cudaStream_t s) {
   Impl& P = *p_;
   // (the status is read after the wait: a copy to pageable host memory would block the enqueue)

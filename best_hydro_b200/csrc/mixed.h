@@ -47,6 +47,8 @@ class MixedSolver {
   void set_refinement(int max_restarts, int krylov);
   // Solves GR x = b in place (d_b: 3n x nrhs, ldb) to the relative residual of build's eps.
   void solve(int nrhs, double* d_b, long ldb, cudaStream_t s, MixedReport* rep);
+  // Device memory the solver holds (its factor, mirrors, inverses and scratch), reused by the next build.
+  size_t device_bytes() const;
 
  private:
   struct Impl;
