@@ -405,17 +405,56 @@ __global__ void __launch_bounds__(kFixThreads)
   const double* V = Vp + B.voff;
   for (int q = threadIdx.x; q < 3 * k; q += blockDim.x) sv[q % 3][q / 3] = V[(size_t)(q / 3) * ldv + 3 * j + q % 3];
   if (threadIdx.x == 0) {
-    // P[a][c] = residual row a at the pivot triangle's column c
-    double P[9];
+    // P[a][c] = residual row a at the pivot triangle's column c.  The residual's 3 x 3 block is often
+    // nearly rank-deficient after a few steps, so its usable part is chosen by complete pivoting (up
+    // to three rank-one terms, as hmatrix/src/hmatrix.cpp:56-60 takes them): index sets I (rows) and
+    // J (columns) with P_IJ well conditioned, and the generalised inverse G (3 x 3) with
+    // G[J[q]][I[p]] = (P_IJ^-1)[q][p], zero elsewhere, so that C G R = C_J P_IJ^-1 R_I.
+    double P[9], W[9];
     for (int a = 0; a < 3; ++a)
-      for (int c = 0; c < 3; ++c) P[3 * a + c] = V[(size_t)(k + a) * ldv + 3 * j + c];
-    const double c00 = P[4] * P[8] - P[5] * P[7], c01 = P[5] * P[6] - P[3] * P[8], c02 = P[3] * P[7] - P[4] * P[6];
-    const double det = P[0] * c00 + P[1] * c01 + P[2] * c02;
+      for (int c = 0; c < 3; ++c) P[3 * a + c] = W[3 * a + c] = V[(size_t)(k + a) * ldv + 3 * j + c];
     double pmax = 0.0;
     for (int q = 0; q < 9; ++q) pmax = fmax(pmax, fabs(P[q]));
-    s_ok = isfinite(det) && fabs(det) > 1e-12 * pmax * pmax * pmax && pmax > 0.0;
-    if (s_ok) {
-      const double id = 1.0 / det;
+    int I[3], J[3], r = 0;
+    bool usedr[3] = {false, false, false}, usedc[3] = {false, false, false};
+    if (isfinite(pmax) && pmax > 0.0) {
+      for (; r < 3; ++r) {
+        int ba = -1, bc = -1;
+        double bv = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c)
+            if (!usedr[a] && !usedc[c] && fabs(W[3 * a + c]) > bv) {
+              bv = fabs(W[3 * a + c]);
+              ba = a;
+              bc = c;
+            }
+        if (ba < 0 || !(bv > 1e-10 * pmax)) break;
+        I[r] = ba;
+        J[r] = bc;
+        usedr[ba] = usedc[bc] = true;
+        const double piv = W[3 * ba + bc];
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c)
+            if (!usedr[a] && !usedc[c]) W[3 * a + c] -= W[3 * a + bc] * W[3 * ba + c] / piv;
+      }
+    }
+    for (int q = 0; q < 9; ++q) s_pinv[q] = 0.0;
+    s_ok = r > 0;
+    if (r == 1) {
+      s_pinv[3 * J[0] + I[0]] = 1.0 / P[3 * I[0] + J[0]];
+    } else if (r == 2) {
+      const double m00 = P[3 * I[0] + J[0]], m01 = P[3 * I[0] + J[1]], m10 = P[3 * I[1] + J[0]],
+                   m11 = P[3 * I[1] + J[1]];
+      const double id = 1.0 / (m00 * m11 - m01 * m10);
+      // M^-1 = [[m11, -m01], [-m10, m00]] / det, rows indexed by J, columns by I
+      s_pinv[3 * J[0] + I[0]] = m11 * id;
+      s_pinv[3 * J[0] + I[1]] = -m01 * id;
+      s_pinv[3 * J[1] + I[0]] = -m10 * id;
+      s_pinv[3 * J[1] + I[1]] = m00 * id;
+    } else if (r == 3) {
+      const double c00 = P[4] * P[8] - P[5] * P[7], c01 = P[5] * P[6] - P[3] * P[8], c02 = P[3] * P[7] - P[4] * P[6];
+      const double id = 1.0 / (P[0] * c00 + P[1] * c01 + P[2] * c02);
+      // the full inverse, stored as G[c][a] = (P^-1)[c][a]
       s_pinv[0] = c00 * id;
       s_pinv[1] = (P[2] * P[7] - P[1] * P[8]) * id;
       s_pinv[2] = (P[1] * P[5] - P[2] * P[4]) * id;
@@ -426,6 +465,8 @@ __global__ void __launch_bounds__(kFixThreads)
       s_pinv[7] = (P[1] * P[6] - P[0] * P[7]) * id;
       s_pinv[8] = (P[0] * P[4] - P[1] * P[3]) * id;
     }
+    for (int q = 0; q < 9; ++q)
+      if (!isfinite(s_pinv[q])) s_ok = 0;
   }
   __syncthreads();
   if (!s_ok) {

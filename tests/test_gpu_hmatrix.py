@@ -99,3 +99,45 @@ def test_golden_results_on_the_hmatrix(key):
             got = value_for_label(g["report"], e["label"])
         assert abs(got - e["value"]) <= e["tol"] * abs(e["value"]), (e["label"], got, e["value"])
     solver.destroy()
+
+
+def test_product_at_the_headline_size():
+    """The star body at N = 20,480 (the benchmark's mesh; trees of depth 8, blocks up to 10,240
+    triangles a side) at eps = 1e-6: the product against the dense deflated GR, formed in row blocks
+    by the exact assembly, within 3 eps; no block row is missed."""
+    tri, ta, tv = meshes.star(32)
+    st = bh.Setup(tri, 0, ta)
+    s = BhmSolver()
+    s.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+    x = s.incenters()
+    xmu, gdef = st.deflation(s.diag_mean())
+    n = st.n
+    n3 = 3 * n
+    bh.set_precision(bh.BGPU_HMATRIX)
+    try:
+        s.build(eps=1e-6, direct=0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+    finally:
+        bh.set_precision(-1)
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((n3, 2))
+    dx = torch.from_numpy(X.T.copy()).cuda()
+    dy = torch.zeros_like(dx)
+    bh.hmatrix_matvec_device(2, dx.data_ptr(), n3, dy.data_ptr(), n3)
+    torch.cuda.synchronize()
+    Yh = dy.cpu().numpy().T
+    Y = np.zeros((n3, 2))
+    for r0 in range(0, n, 2048):
+        r1 = min(n, r0 + 2048)
+        blk = torch.empty((n3, 3 * (r1 - r0)), dtype=torch.float64, device="cuda")  # rows of r0..r1, column-major
+        bh.assemble_device(r0, r1, 0, n, blk.data_ptr(), 3 * (r1 - r0))
+        Y[3 * r0:3 * r1] = (dx @ blk).cpu().numpy().T
+        del blk
+    xm = xmu.reshape(-1)
+    Y += np.outer(xm, gdef[0] * (xm @ X))  # one surface
+    err = np.linalg.norm(Yh - Y, axis=0) / np.linalg.norm(Y, axis=0)
+    rows = np.abs(Yh - Y).max(axis=1) / (np.linalg.norm(Y) / np.sqrt(n3))
+    print(f"N={n}: product error {err.max():.2e}, worst row {rows.max():.2e}; {bh.hmatrix_stats()}")
+    assert st.ndef == 1
+    assert err.max() <= 3e-6, err
+    assert rows.max() <= 1e-3
+    s.destroy()
