@@ -928,7 +928,8 @@ def hmatrix_record(big=64, small=32, eps=1e-4):
     """The path for meshes beyond HBM: the star body at geodesic frequency `big` (64: N = 81,920, order
     245,760, whose dense FP64 GR would need 483 GB) through BEST's seam, where bhm_build takes the
     H-matrix path by itself; and at `small` (32: the headline mesh), where the dense paths also run,
-    the H-matrix results against the mixed dense path's.  eps = 1e-4 is BEST's default -he accuracy.
+    the H-matrix results against the mixed dense path's, at eps = 1e-4 (BEST's default -he accuracy) and
+    at 1e-7 (at most 120 terms a block), against the dense paths' 1e-8 bar.
     Host wall time of bhm_build + bhm_solve (6 RHS, host buffers); the 11-RHS solve for the tensors is
     untimed."""
     import torch
@@ -936,7 +937,9 @@ def hmatrix_record(big=64, small=32, eps=1e-4):
     from best_hydro_b200 import meshes
 
     rec = {"eps": eps}
-    for f, prec in ((small, bh.BGPU_HMATRIX), (small, bh.BGPU_MIXED), (big, -1)):
+    legs = ((small, bh.BGPU_HMATRIX, eps, 90), (small, bh.BGPU_HMATRIX, 1e-7, 120), (small, bh.BGPU_MIXED, eps, 90),
+            (big, -1, eps, 90))
+    for f, prec, leps, kmax in legs:
         tri, ta, tv = meshes.star(f)
         st = bh.Setup(tri, 0, ta)
         s = bh.BhmSolver()
@@ -944,13 +947,15 @@ def hmatrix_record(big=64, small=32, eps=1e-4):
         x = s.incenters()
         xmu, gdef = st.deflation(s.diag_mean())
         bh.set_precision(prec)
+        bh.hmatrix_set_options(128, 2.0, kmax)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        s.build(eps=eps, direct=0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+        s.build(eps=leps, direct=0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
         t1 = time.perf_counter()
         s.solve(bh.rhs6(x))
         t2 = time.perf_counter()
         bh.set_precision(-1)
+        bh.hmatrix_set_options()
         path = {0: "fp64", 1: "mixed", 2: "hmatrix"}[bh.lib().bgpu_precision()]
         leg = {"N": st.n, "order": 3 * st.n, "path": path, "build_s": t1 - t0, "solve_s": t2 - t1,
                "value": t2 - t0, "unit": "s", "dense_fp64_gb": 72.0 * st.n * st.n / 1e9}
@@ -959,15 +964,16 @@ def hmatrix_record(big=64, small=32, eps=1e-4):
             leg["hmatrix"] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in hs.items()}
             leg["stored_gb"] = 8 * (hs["dense_entries"] + hs["lowrank_entries"]) / 1e9
         t = tensors_of(s, x, st, bh)
-        leg.update(D_t=t["D_t"], D_r=t["D_r"], chiprime=t["chiprime"])
-        rec[f"f{f}_{path}"] = (leg, t)
+        leg.update(D_t=t["D_t"], D_r=t["D_r"], chiprime=t["chiprime"], eps=leps, kmax=kmax)
+        rec[f"f{f}_{path}" + ("" if leps == eps else f"_eps{leps:.0e}")] = (leg, t)
         s.destroy()
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     out = {k: v[0] for k, v in rec.items() if k != "eps"}
-    hm, mx = rec.get(f"f{small}_hmatrix"), rec.get(f"f{small}_mixed")
-    if hm and mx:
-        out[f"accuracy_f{small}_hmatrix_vs_mixed"] = tensor_errors(hm[1], mx[1])
+    mx = rec.get(f"f{small}_mixed")
+    for key in (f"f{small}_hmatrix", f"f{small}_hmatrix_eps1e-07"):
+        if rec.get(key) and mx:
+            out[f"accuracy_{key}_vs_mixed"] = tensor_errors(rec[key][1], mx[1])
     out["eps"] = eps
     return out
 
