@@ -1,4 +1,4 @@
-// The hierarchical-matrix path for meshes beyond the dense path's reach: GR held as dense
+// The hierarchical-matrix path for meshes beyond the dense paths' reach (N above ~40,000 on one B200): GR held as dense
 // near-field blocks and low-rank far-field blocks, solved by FP64 GMRES.
 //
 // Compiled with -fmad=false: every entry this path evaluates (the dense blocks in full, the rows

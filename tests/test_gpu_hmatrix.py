@@ -132,6 +132,7 @@ def test_product_at_the_headline_size():
         bh.assemble_device(r0, r1, 0, n, blk.data_ptr(), 3 * (r1 - r0))
         Y[3 * r0:3 * r1] = (dx @ blk).cpu().numpy().T
         del blk
+    torch.cuda.empty_cache()  # later tests size their paths by the device's free memory
     xm = xmu.reshape(-1)
     Y += np.outer(xm, gdef[0] * (xm @ X))  # one surface
     err = np.linalg.norm(Yh - Y, axis=0) / np.linalg.norm(Y, axis=0)
@@ -141,3 +142,34 @@ def test_product_at_the_headline_size():
     assert err.max() <= 3e-6, err
     assert rows.max() <= 1e-3
     s.destroy()
+
+
+def test_device_setup_path_and_determinism():
+    """The H-matrix path behind the device set-up (bgpu_create_from_triangles + bgpu_build_prepared)
+    on the two-surface mesh (NDEF = 2) gives, bit for bit, the solution of the host path (bhm_create +
+    bhm_build with the host's arrays): the set-up's arrays are equal, and the H-matrix build and its
+    GMRES solve are deterministic (fixed summation orders, no atomics)."""
+    tri, ta, tv = golden_mesh(expected_cases()["two"]["mesh"])
+    tri = np.ascontiguousarray(tri, dtype=np.float64)
+    st = bh.Setup(tri, 1, ta)
+    assert st.ndef == 2
+    bh.set_precision(bh.BGPU_HMATRIX)
+    try:
+        s = BhmSolver()
+        s.create_from_triangles(tri, 1, ta)
+        x_dev, dm_dev = s.incenters(), s.diag_mean()
+        s.build_prepared(eps=1e-5, direct=0)
+        assert bh.lib().bgpu_precision() == bh.BGPU_HMATRIX
+        B_dev = s.solve(bh.rhs6(x_dev))
+        s.destroy()
+        s2 = BhmSolver()
+        s2.create(st.v1, st.v2, st.v3, st.area, st.afac, 1.0)
+        x = s2.incenters()
+        xmu, gdef = st.deflation(s2.diag_mean())
+        s2.build(eps=1e-5, direct=0, ndef=st.ndef, gdef=gdef, comp=st.icomp, xmu=xmu)
+        B = s2.solve(bh.rhs6(x))
+        s2.destroy()
+    finally:
+        bh.set_precision(-1)
+    assert np.array_equal(x, x_dev)
+    assert np.array_equal(B, B_dev)
