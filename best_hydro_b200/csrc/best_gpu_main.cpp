@@ -1,5 +1,7 @@
 // best_gpu: BEST's command line (best/input.f:26-68) on the GPU backend, for machines without a
-// Fortran compiler.  best_gpu -f file [-na] [-p] [-v] [-vc] [-mw W] [-fp64 | -mixed]
+// Fortran compiler.  best_gpu -f file [-na] [-p] [-v] [-vc] [-mw W] [-fp64 | -mixed | -hm]
+// (-hm: the H-matrix path at BEST's default accuracy 1e-4, as BEST's own -hm flag selects its H-matrix
+// solver; without a flag, meshes whose dense matrix does not fit on the GPU take it by themselves)
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -19,9 +21,10 @@ int main(int argc, char** argv) {
     else if (!std::strcmp(argv[k], "-mw") && k + 1 < argc) wm = std::atof(argv[++k]);
     else if (!std::strcmp(argv[k], "-fp64")) prec = 0;
     else if (!std::strcmp(argv[k], "-mixed")) prec = 1;
+    else if (!std::strcmp(argv[k], "-hm")) prec = 2;
   }
   if (!file) {
-    std::printf("Usage : best_gpu -f input_filename [-na] [-p] [-v] [-vc] [-mw W] [-fp64 | -mixed]\n");
+    std::printf("Usage : best_gpu -f input_filename [-na] [-p] [-v] [-vc] [-mw W] [-fp64 | -mixed | -hm]\n");
     return 0;
   }
   const int rc = bgpu_best_run(file, iarea, cgz, iv, icov, wm, prec, nullptr);

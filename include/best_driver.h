@@ -46,7 +46,7 @@ void bgpu_best_traces(const double *tensors, double *out);
 double bgpu_best_extrapolate(int count, const int *n, const double *y, double *slope);
 
 /* The whole program (best/best.f:184-510 through the seam, as with -hm): reads the mesh file, solves,
- * writes <infile><flags>.be and .log.  precision: 0 FP64 LU, 1 mixed, -1 BEST's rule.  results
+ * writes <infile><flags>.be and .log.  precision: 0 FP64 LU, 1 mixed, 2 H-matrix, -1 BEST's rule.  results
  * (may be NULL, 68 doubles): bgpu_best_difco's 60, then CHI', Dx, Dy, Dz, D_t, D_r, CHI, ETA. */
 int bgpu_best_run(const char *infile, int iarea, int cg_zero, int ivisco, int icov, double wm, int precision,
                   double *results);

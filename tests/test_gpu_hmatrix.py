@@ -173,3 +173,28 @@ def test_device_setup_path_and_determinism():
         bh.set_precision(-1)
     assert np.array_equal(x, x_dev)
     assert np.array_equal(B, B_dev)
+
+
+@pytest.mark.parametrize("precision", [-1, bh.BGPU_HMATRIX])
+def test_whole_program_on_golden_mesh(tmp_path, precision):
+    """BEST's whole program through the seam (bgpu_best_run, the best_gpu command; -hm selects the
+    H-matrix path) on 2eu7 with -v and a molecular weight: the reference's golden values within their
+    tolerance, and the .be and .log files written."""
+    c = expected_cases()["2eu7"]
+    tri, ta, tv = golden_mesh(c["mesh"])
+    path = tmp_path / "2eu7.txt"
+    meshes.write_best(str(path), tri, ta, tv)
+    bh.log_lines()  # the program's .log takes the library's queued messages: start from an empty queue
+    rep = bh.best_run(path, iarea=c["iarea"], ivisco=c["ivisco"], icov=c["icov"], wm=c["wm"], precision=precision)
+    bh.set_precision(-1)
+    for e in c["expected"]:
+        if e["label"] in ("Dx", "Dy", "Dz"):
+            got = rep["dvisc"]["xyz".index(e["label"][1])]
+        else:
+            got = value_for_label(rep, e["label"])
+        assert got is not None, e["label"]
+        assert abs(got - e["value"]) <= e["tol"] * abs(e["value"]), (e["label"], got, e["value"])
+    outs = sorted(p.name for p in tmp_path.iterdir())
+    assert any(n.endswith(".be") for n in outs) and any(n.endswith(".log") for n in outs), outs
+    log = "".join(p.read_text() for p in tmp_path.iterdir() if p.name.endswith(".log"))
+    assert ("GPU build: H-matrix of order 7686" in log) == (precision == bh.BGPU_HMATRIX), log[-2000:]
