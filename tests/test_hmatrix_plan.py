@@ -13,6 +13,8 @@ from oracle import hplan
 def _mesh(kind):
     if kind == "ellipsoid":
         tri, ta, tv = meshes.ellipsoid(8)
+    elif kind == "star32":
+        tri, ta, tv = meshes.star(32)  # the benchmark's mesh, N = 20,480
     else:
         tri, ta, tv = meshes.star(10)
     s = ob.setup(tri, 1, ta)
@@ -20,7 +22,7 @@ def _mesh(kind):
     return s, x
 
 
-@pytest.mark.parametrize("kind,leaf", [("ellipsoid", 32), ("ellipsoid", 128), ("star", 64)])
+@pytest.mark.parametrize("kind,leaf", [("ellipsoid", 32), ("ellipsoid", 128), ("star", 64), ("star32", 128)])
 def test_plan_matches_reference_tree(kind, leaf):
     s, x = _mesh(kind)
     n = s.n
